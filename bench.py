@@ -1,0 +1,350 @@
+"""Benchmark of the blocked matrix product over Blosc2-compressed containers on B200.
+
+Workload (one step = one iarray_opt_gemm call on resident compressed containers:
+decode A, decode B, product, re-encode C):
+  precision_f64: A, B 8192 x 8192 float64, entries uniform(-1,1) * 2^U{-8..8}
+  (numpy default_rng(3), A then B), chunkshape 2048 x 2048, blockshape 256 x 256,
+  Blosc2 LZ4 clevel 5 + SHUFFLE; output with the same partition.
+The headline `value` is effective TFLOP/s (2*M*N*K per step) of the split-precision
+form when the library supports it, else of the native FP64 form; both forms are timed
+and their normwise errors against a double-double oracle (sampled rows) are reported.
+
+Contract: `python bench.py --gpus N --steps K --warmup W` prints one JSON line (rank 0).
+`--impl reference` times the reference algorithm on the host cores instead (the
+oracle's restatement of iarray_opt_gemm's block-pair loop with OpenBLAS dgemm and
+liblz4), on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "iron-array_b200"))
+
+import numpy as np  # noqa: E402
+
+M = N = K = 8192
+CHUNK, BLOCK = (2048, 2048), (256, 256)
+FLOP = 2.0 * M * N * K
+METRIC = "GEMM TFLOP/s split-precision vs native FP64 at stated error; decode GB/s"
+
+
+def make_inputs():
+    rng = np.random.default_rng(3)
+    A = rng.uniform(-1, 1, (M, K)) * np.exp2(rng.integers(-8, 9, (M, K)))
+    B = rng.uniform(-1, 1, (K, N)) * np.exp2(rng.integers(-8, 9, (K, N)))
+    return A, B
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.p = None
+        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
+                                 f".clocks_{os.getpid()}.csv")
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in open(self.path):
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.remove(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+# ============================================================================ reference arm
+def run_reference(args):
+    world, rank, local, pg = dist_setup(args)
+    if rank != 0:
+        barrier(pg)
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    A, B = make_inputs()
+    ga, ach = O.encode_array(A, CHUNK, BLOCK)
+    gb, bch = O.encode_array(B, CHUNK, BLOCK)
+    gc = O.Geom((M, N), CHUNK, BLOCK, 8)
+    del A, B
+    cores = os.cpu_count() or 1
+    times = []
+    for s in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        O.cpu_opt_gemm_chunk(ga, ach, gb, bch, gc, s % gc.nchunks, cores)
+        if s >= args.warmup:
+            times.append(time.perf_counter() - t)
+    chunk_flop = 2.0 * CHUNK[0] * CHUNK[1] * K
+    sec_full = float(np.mean(times)) * gc.nchunks
+    v = FLOP / sec_full / 1e12
+    sample = (f"one 2048x2048 output chunk of the 8192^3 opt_gemm per step (1/{gc.nchunks} of the work, "
+              f"{chunk_flop / 1e9:.1f} GFLOP), block-pair loop with per-pair LZ4 block decode, "
+              f"single-threaded OpenBLAS dgemm per worker, LZ4 re-encode; scaled to the full product")
+    line = {"metric": METRIC, "value": v, "unit": "TFLOP/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_full * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "precision_f64 8192^3, chunk 2048^2, block 256^2, LZ4+SHUFFLE",
+                       "M": M, "N": N, "K": K},
+            "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    barrier(pg)
+
+
+# ============================================================================ our arm
+def run_ours(args):
+    world, rank, local, pg = dist_setup(args)
+    import torch
+    torch.cuda.set_device(local)
+    import iarray_b200 as ia
+    ia.init()
+    ctx = ia.Context()
+    stream = torch.cuda.ExternalStream(ctx.stream())
+
+    A, B = make_inputs()
+    Ac = ia.Container.from_numpy(ctx, A, CHUNK, BLOCK)
+    Bc = ia.Container.from_numpy(ctx, B, CHUNK, BLOCK)
+    a_nb, a_cb = Ac.info()
+    b_nb, b_cb = Bc.info()
+
+    forms = {"native": ia.FORM_NATIVE, "split": ia.FORM_SPLIT}
+    results = {}
+    for name, form in forms.items():
+        ctx.set_form(form)
+        try:
+            C = ia.opt_gemm(ctx, Ac, Bc, CHUNK, BLOCK)
+        except ia.IArrayError as e:
+            if e.name == "NOT_SUPPORTED":
+                continue
+            raise
+        for _ in range(max(args.warmup - 1, 0)):
+            C.free()
+            C = ia.opt_gemm(ctx, Ac, Bc, CHUNK, BLOCK)
+        C.free()
+        barrier(pg)
+        torch.cuda.synchronize()
+        clk = Clocks(local)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        parts = np.zeros(5)
+        l0 = ia.lib().iarray_b200_kernel_launches()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            C = ia.opt_gemm(ctx, Ac, Bc, CHUNK, BLOCK)
+            t = ctx.timings()
+            parts += [t["decode_a"], t["decode_b"], t["product"], t["encode"], t["total"]]
+            C.free()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        launches = ia.lib().iarray_b200_kernel_launches() - l0
+        clocks = clk.stop()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        ms = max_over_ranks(pg, ms)
+        parts /= args.steps
+        results[name] = dict(ms=ms, parts=parts, launches=launches, clocks=clocks, form=form)
+
+    # errors vs double-double on sampled rows (outside the timed region)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    if rank == 0:
+        import oracle as O
+        rows = np.sort(np.random.default_rng(99).choice(M, args.err_rows, replace=False))
+        hi, lo = O.dd_rows(A, B, rows)
+        for name, r in results.items():
+            ctx.set_form(r["form"])
+            C = ia.opt_gemm(ctx, Ac, Bc, CHUNK, BLOCK)
+            c = C.to_numpy()
+            r["err"] = O.normwise_error(c, hi, lo, rows)
+            _, c_cb = C.info()
+            r["c_cbytes"] = c_cb
+            C.free()
+            del c
+
+    # end-to-end through the C ABI with host frames: H2D of A and B frames, product,
+    # D2H of C's frame, every step
+    head = "split" if "split" in results else "native"
+    ctx.set_form(results[head]["form"])
+    fa, fb = Ac.to_cframe(), Bc.to_cframe()
+    e2e_t, d2h = [], 0
+    for s in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        a2 = ia.Container.from_cframe(ctx, fa)
+        b2 = ia.Container.from_cframe(ctx, fb)
+        C = ia.opt_gemm(ctx, a2, b2, CHUNK, BLOCK)
+        fc = C.to_cframe()
+        torch.cuda.synchronize()
+        if s >= args.warmup:
+            e2e_t.append(time.perf_counter() - t)
+        d2h = len(fc)
+        for x in (a2, b2, C):
+            x.free()
+    e2e_ms = max_over_ranks(pg, float(np.mean(e2e_t)) * 1e3)
+
+    # cuBLAS DGEMM on the same dense shapes: the measured FP64 tensor roof
+    dgemm_tflops = None
+    if rank == 0:
+        x = torch.randn(M, K, dtype=torch.float64, device="cuda")
+        y = torch.randn(K, N, dtype=torch.float64, device="cuda")
+        for _ in range(2):
+            torch.matmul(x, y)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            torch.matmul(x, y)
+        e1.record()
+        torch.cuda.synchronize()
+        dgemm_tflops = FLOP / (e0.elapsed_time(e1) / 3 * 1e-3) / 1e12
+        del x, y
+        torch.cuda.empty_cache()
+
+    # CPU baseline: the reference's loop on a bounded sample (rank 0, N = 1 only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle as O
+        ga, ach = O.Geom((M, K), CHUNK, BLOCK, 8), Ac.chunks()
+        gb, bch = O.Geom((K, N), CHUNK, BLOCK, 8), Bc.chunks()
+        gc = O.Geom((M, N), CHUNK, BLOCK, 8)
+        cores = os.cpu_count() or 1
+        ts = []
+        for s in range(2):
+            t = time.perf_counter()
+            O.cpu_opt_gemm_chunk(ga, ach, gb, bch, gc, s, cores)
+            ts.append(time.perf_counter() - t)
+        v = FLOP / (min(ts[1:] or ts) * gc.nchunks) / 1e12
+        cpu = {"value": v, "unit": "TFLOP/s", "cores": cores, "kind": "port",
+               "sample": "one 2048x2048 output chunk (1/16 of the 8192^3 opt_gemm) with the reference's block-pair "
+                         "loop: per-pair LZ4 block decode, single-threaded OpenBLAS dgemm per worker thread, LZ4 "
+                         "re-encode; rate scaled to the full product"}
+
+    if rank != 0:
+        barrier(pg)
+        return
+    barrier(pg)
+    pk = peaks()
+    hr = results[head]
+    value = world * FLOP / (hr["ms"] * 1e-3) / 1e12
+    prod_ms = hr["parts"][2]
+    if head == "native":
+        roof = {"bound": "tensor", "kernel": "k_gemm_f64 (DMMA m16n8k4)", "achieved": FLOP / (prod_ms * 1e-3) / 1e12,
+                "peak": dgemm_tflops, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor roof)",
+                "unit": "TFLOP/s"}
+    else:
+        roof = {"bound": "tensor", "kernel": "split-precision product", "achieved": FLOP / (prod_ms * 1e-3) / 1e12,
+                "peak": dgemm_tflops, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run", "unit": "TFLOP/s"}
+    roof["frac"] = roof["achieved"] / roof["peak"] if roof["peak"] else None
+    roof["traffic"] = None
+    tf = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tf):
+        roof["traffic"] = json.load(open(tf)).get(roof["kernel"].split()[0])
+    decode_ms = hr["parts"][0]
+    line = {
+        "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": hr["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (numpy default_rng(3))",
+        "config": {"workload": "precision_f64 opt_gemm 8192^3, chunk 2048^2, block 256^2, LZ4 clevel5 + SHUFFLE",
+                   "form": head, "M": M, "N": N, "K": K, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (compressed A+B %.0f MB)" % ((a_cb + b_cb) / 1e6)},
+        "forms": {k: {"tflops": world * FLOP / (r["ms"] * 1e-3) / 1e12, "ms_per_step": r["ms"],
+                      "ms_parts": {"decode_a": r["parts"][0], "decode_b": r["parts"][1], "product": r["parts"][2],
+                                   "encode": r["parts"][3]},
+                      "normwise_err_vs_dd": r.get("err"), "kernel_launches": int(r["launches"])}
+                  for k, r in results.items()},
+        "decode_gbs": (a_nb + a_cb) / (decode_ms * 1e-3) / 1e9,
+        "compression": {"a_ratio": a_nb / a_cb, "b_ratio": b_nb / b_cb,
+                        "c_ratio": (M * N * 8) / hr["c_cbytes"] if hr.get("c_cbytes") else None},
+        "roofline": roof,
+        "cublas_dgemm_tflops": dgemm_tflops,
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * FLOP / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
+                "h2d_bytes_per_step": len(fa) + len(fb), "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "gpu_launches": int(hr["launches"]),
+        "clocks": hr["clocks"],
+        "peaks_used": {"hbm_gbs": pk.get("hbm_gbs"), "bf16_tflops": pk.get("bf16_tflops")},
+    }
+    if "split" in results and "native" in results:
+        line["split_vs_native"] = {"speedup": results["native"]["ms"] / results["split"]["ms"],
+                                   "err_ratio": (results["split"].get("err") or 0) /
+                                                max(results["native"].get("err") or 1e-300, 1e-300)}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--err-rows", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1081 @@
+// Host runtime behind include/iarray_b200.h: contexts, GPU-resident containers,
+// persistence, and the matmul entry points of ironArray (src/linalg/matmul.c,
+// src/linalg/matmul/gemm.c, gemv.c, src/linalg/iarray_gemm.c, iarray_gemm_a.c,
+// iarray_gemm_b.c, iarray_gemv.c).
+//
+// A container keeps its Blosc2 chunks in device memory, back to back, with host-side
+// offsets.  A product decodes each operand once into a dense row-major device array
+// (the reference decodes every A block N_blocks x N_chunks times), runs one product
+// kernel over the whole matrices, and re-encodes the result into `storage`'s
+// partition.  Calls are synchronous on one internal CUDA stream per context.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/iarray_b200.h"
+#include "common.cuh"
+#include "frame.h"
+
+using iab::DevBuf;
+using iab::Geom;
+
+// ============================================================================ pool + geometry
+namespace iab {
+
+std::atomic<uint64_t> g_launches{0};
+
+DevicePool &DevicePool::get(int device)
+{
+    static std::mutex mu;
+    static std::map<int, DevicePool *> pools;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = pools.find(device);
+    if (it != pools.end()) return *it->second;
+    DevicePool *p = new DevicePool();
+    pools[device] = p;
+    return *p;
+}
+
+static size_t size_class(size_t n)
+{
+    if (n <= (1u << 20)) {
+        size_t s = 256;
+        while (s < n) s <<= 1;
+        return s;
+    }
+    return round_up((int64_t)n, (int64_t)2 << 20);
+}
+
+void *DevicePool::alloc(size_t bytes)
+{
+    const size_t sc = size_class(std::max<size_t>(bytes, 1));
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = free_.lower_bound(sc);
+        if (it != free_.end() && it->first <= sc + sc / 4) {
+            void *p = it->second;
+            used_[p] = it->first;
+            free_.erase(it);
+            return p;
+        }
+    }
+    void *p = nullptr;
+    if (cudaMalloc(&p, sc) != cudaSuccess) {
+        cudaGetLastError();
+        trim();
+        if (cudaMalloc(&p, sc) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    }
+    std::lock_guard<std::mutex> lk(mu_);
+    used_[p] = sc;
+    return p;
+}
+
+void DevicePool::release(void *p)
+{
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(mu_);
+    auto it = used_.find(p);
+    if (it == used_.end()) return;
+    free_.emplace(it->second, p);
+    used_.erase(it);
+}
+
+void DevicePool::trim()
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    cudaDeviceSynchronize();
+    for (auto &kv : free_) cudaFree(kv.second);
+    free_.clear();
+}
+
+bool DevBuf::allocate(size_t bytes, int device)
+{
+    reset();
+    dev = device;
+    p = DevicePool::get(device).alloc(bytes);
+    n = p ? bytes : 0;
+    return p != nullptr;
+}
+
+void DevBuf::reset()
+{
+    if (p) DevicePool::get(dev).release(p);
+    p = nullptr;
+    n = 0;
+}
+
+bool make_geom(int ndim, const int64_t *shape, const int64_t *chunk, const int64_t *block, int itemsize, Geom *g)
+{
+    if (ndim < 1 || ndim > 2) return false;
+    memset(g, 0, sizeof(*g));
+    g->itemsize = itemsize;
+    g->ndim = ndim;
+    for (int d = 0; d < 2; d++) {
+        const int s = d - (2 - ndim);   // 1-D arrays are 1 x n
+        g->shape[d] = s < 0 ? 1 : shape[s];
+        g->chunk[d] = s < 0 ? 1 : chunk[s];
+        g->block[d] = s < 0 ? 1 : block[s];
+        if (g->shape[d] < 0 || g->chunk[d] <= 0 || g->block[d] <= 0) return false;
+        if (g->block[d] > g->chunk[d]) return false;
+        g->extc[d] = round_up(g->chunk[d], g->block[d]);
+        g->cgrid[d] = g->shape[d] == 0 ? 0 : ceil_div(g->shape[d], g->chunk[d]);
+        g->bgrid[d] = g->extc[d] / g->block[d];
+    }
+    g->nchunks = g->cgrid[0] * g->cgrid[1];
+    g->nblocks = g->bgrid[0] * g->bgrid[1];
+    g->blockn = g->block[0] * g->block[1];
+    g->blocksize = g->blockn * itemsize;
+    g->chunk_nbytes = g->extc[0] * g->extc[1] * itemsize;
+    if (g->chunk_nbytes > (int64_t)INT32_MAX - 64) return false;   // Blosc2 chunks are < 2 GiB
+    return true;
+}
+
+}  // namespace iab
+
+// ============================================================================ objects
+struct ChunkStore {
+    int device = 0;
+    DevBuf buf;                    // chunk bytes, back to back
+    DevBuf d_off, d_len;           // device copies of off / len
+    std::vector<int64_t> off;      // byte offset of each chunk in buf
+    std::vector<int32_t> len;      // cbytes of each chunk
+    int64_t cbytes = 0;
+    bool upload_index()
+    {
+        const size_t n = off.size();
+        if (!d_off.allocate(std::max<size_t>(n, 1) * 8, device) || !d_len.allocate(std::max<size_t>(n, 1) * 4, device))
+            return false;
+        if (n) {
+            cudaMemcpy(d_off.p, off.data(), n * 8, cudaMemcpyHostToDevice);
+            cudaMemcpy(d_len.p, len.data(), n * 4, cudaMemcpyHostToDevice);
+        }
+        cbytes = 0;
+        for (int32_t l : len) cbytes += l;
+        return true;
+    }
+};
+
+struct iarray_context_s {
+    iarray_config_t cfg;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int form = IARRAY_B200_FORM_NATIVE;
+    int split_terms = 0;
+    double timings[5] = {0, 0, 0, 0, 0};
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+};
+
+struct iarray_container_s {
+    iarray_dtshape_t dtshape;      // logical shape (a transposed view has it reversed)
+    iarray_storage_t storage;      // partition of the stored chunks
+    std::string urlpath;
+    Geom geom;                     // geometry of the stored chunks
+    std::shared_ptr<ChunkStore> store;
+    bool transposed = false;
+    bool view = false;
+    bool shuffle = true;
+    int splitmode = IARRAY_AUTO_SPLIT;
+    int clevel = 5;
+};
+
+// ============================================================================ errors
+static ina_rc_t rc_err(uint32_t msg) { return INA_RC_ERROR_BIT | (ina_rc_t)msg; }
+
+static bool g_initialized = false;
+static int g_device = -1;
+
+INA_API(const char *) iarray_err_strerror(ina_rc_t error)
+{
+    if (!INA_FAILED(error)) return "Success";
+    switch (INA_RC_MSG(error)) {
+    case IARRAY_ERR_INVALID_DTYPE: return "Invalid dtype";
+    case IARRAY_ERR_INVALID_SHAPE: return "Invalid shape";
+    case IARRAY_ERR_INVALID_CHUNKSHAPE: return "Invalid chunkshape";
+    case IARRAY_ERR_INVALID_BLOCKSHAPE: return "Invalid blockshape";
+    case IARRAY_ERR_INVALID_NDIM: return "Invalid ndim";
+    case IARRAY_ERR_INVALID_STORAGE: return "Invalid storage";
+    case IARRAY_ERR_TOO_SMALL_BUFFER: return "Buffer too small";
+    case IARRAY_ERR_BLOSC_FAILED: return "Blosc chunk failed to encode or decode";
+    case IARRAY_ERR_ASSERTION_FAILED: return "Assertion failed";
+    case IARRAY_ERR_PERSISTENCY_FAILED: return "Persistence failed";
+    case IARRAY_ERR_GPU_FAILED: return "GPU failed or unavailable";
+    case IARRAY_ERR_GPU_OUT_OF_MEMORY: return "GPU out of memory";
+    case IARRAY_ERR_NOT_SUPPORTED: return "Not supported";
+    case INA_ERR_INVALID_ARGUMENT: return "Invalid argument";
+    case INA_ERR_NOT_INITIALIZED: return "Library not initialized";
+    default: return "Error";
+    }
+}
+
+#define CHECK_ARG(x) do { if (!(x)) return rc_err(INA_ERR_INVALID_ARGUMENT); } while (0)
+
+static ina_rc_t cuda_rc(cudaError_t e)
+{
+    if (e == cudaSuccess) return INA_SUCCESS;
+    if (e == cudaErrorMemoryAllocation) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    return rc_err(IARRAY_ERR_GPU_FAILED);
+}
+
+// ============================================================================ runtime
+INA_API(ina_rc_t) iarray_init(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        return rc_err(IARRAY_ERR_GPU_FAILED);
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    g_device = dev;
+    g_initialized = true;
+    return INA_SUCCESS;
+}
+
+INA_API(void) iarray_destroy(void)
+{
+    if (g_initialized && g_device >= 0) iab::DevicePool::get(g_device).trim();
+    g_initialized = false;
+}
+
+INA_API(ina_rc_t) iarray_context_new(iarray_config_t *cfg, iarray_context_t **ctx)
+{
+    CHECK_ARG(cfg && ctx);
+    if (!g_initialized) return rc_err(INA_ERR_NOT_INITIALIZED);
+    if (cfg->compression_codec != IARRAY_COMPRESSION_LZ4) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
+    if (cfg->filter_flags & ~IARRAY_COMP_SHUFFLE) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
+    if (cfg->compression_level <= 0 || cfg->compression_level > 9) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
+    iarray_context_t *c = new iarray_context_t();
+    c->cfg = *cfg;
+    c->device = g_device;
+    cudaSetDevice(c->device);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return rc_err(IARRAY_ERR_GPU_FAILED);
+    }
+    for (auto &e : c->ev) cudaEventCreate(&e);
+    *ctx = c;
+    return INA_SUCCESS;
+}
+
+INA_API(void) iarray_context_free(iarray_context_t **ctx)
+{
+    if (!ctx || !*ctx) return;
+    iarray_context_t *c = *ctx;
+    if (c->stream) { cudaStreamSynchronize(c->stream); cudaStreamDestroy(c->stream); }
+    for (auto &e : c->ev) if (e) cudaEventDestroy(e);
+    delete c;
+    *ctx = nullptr;
+}
+
+INA_API(ina_rc_t) iarray_b200_set_form(iarray_context_t *ctx, iarray_b200_form_t form)
+{
+    CHECK_ARG(ctx && (form == IARRAY_B200_FORM_NATIVE || form == IARRAY_B200_FORM_SPLIT));
+    ctx->form = form;
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_b200_set_split_terms(iarray_context_t *ctx, int nterms)
+{
+    CHECK_ARG(ctx && nterms >= 0 && nterms <= 32);
+    ctx->split_terms = nterms;
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_b200_last_timings(iarray_context_t *ctx, double *ms5)
+{
+    CHECK_ARG(ctx && ms5);
+    for (int i = 0; i < 5; i++) ms5[i] = ctx->timings[i];
+    return INA_SUCCESS;
+}
+
+INA_API(uint64_t) iarray_b200_kernel_launches(void) { return iab::g_launches.load(); }
+
+INA_API(ina_rc_t) iarray_b200_get_stream(iarray_context_t *ctx, void **stream)
+{
+    CHECK_ARG(ctx && stream);
+    *stream = (void *)ctx->stream;
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_b200_synchronize(iarray_context_t *ctx)
+{
+    CHECK_ARG(ctx);
+    return cuda_rc(cudaStreamSynchronize(ctx->stream));
+}
+
+// ============================================================================ containers
+static int dtype_size(int dtype)
+{
+    switch (dtype) {
+    case IARRAY_DATA_TYPE_DOUBLE: case IARRAY_DATA_TYPE_INT64: case IARRAY_DATA_TYPE_UINT64: return 8;
+    case IARRAY_DATA_TYPE_FLOAT: case IARRAY_DATA_TYPE_INT32: case IARRAY_DATA_TYPE_UINT32: return 4;
+    case IARRAY_DATA_TYPE_INT16: case IARRAY_DATA_TYPE_UINT16: return 2;
+    case IARRAY_DATA_TYPE_INT8: case IARRAY_DATA_TYPE_UINT8: case IARRAY_DATA_TYPE_BOOL: return 1;
+    default: return 0;
+    }
+}
+
+static ina_rc_t new_container(iarray_context_t *ctx, iarray_dtshape_t *dtshape, iarray_storage_t *storage,
+                              iarray_container_t **out)
+{
+    CHECK_ARG(ctx && dtshape && storage && out);
+    const int isz = dtype_size(dtshape->dtype);
+    if (!isz) return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    if (dtshape->ndim < 1 || dtshape->ndim > 2) return rc_err(IARRAY_ERR_INVALID_NDIM);
+    for (int i = 0; i < dtshape->ndim; i++) {
+        if (dtshape->shape[i] < 0) return rc_err(IARRAY_ERR_INVALID_SHAPE);
+        if (storage->chunkshape[i] <= 0) return rc_err(IARRAY_ERR_INVALID_CHUNKSHAPE);
+        if (storage->blockshape[i] <= 0 || storage->blockshape[i] > storage->chunkshape[i])
+            return rc_err(IARRAY_ERR_INVALID_BLOCKSHAPE);
+    }
+    Geom g;
+    if (!iab::make_geom(dtshape->ndim, dtshape->shape, storage->chunkshape, storage->blockshape, isz, &g))
+        return rc_err(IARRAY_ERR_INVALID_CHUNKSHAPE);
+    iarray_container_t *c = new iarray_container_t();
+    c->dtshape = *dtshape;
+    c->dtshape.dtype_size = isz;
+    c->storage = *storage;
+    c->storage.urlpath = nullptr;
+    if (storage->urlpath) c->urlpath = storage->urlpath;
+    c->geom = g;
+    c->store = std::make_shared<ChunkStore>();
+    c->store->device = ctx->device;
+    c->shuffle = (ctx->cfg.filter_flags & IARRAY_COMP_SHUFFLE) != 0;
+    c->splitmode = ctx->cfg.splitmode;
+    c->clevel = ctx->cfg.compression_level;
+    *out = c;
+    return INA_SUCCESS;
+}
+
+static ina_rc_t save_if_urlpath(iarray_context_t *ctx, iarray_container_t *c);
+
+// Fill a container with Blosc2 special-zero chunks (header only).
+static ina_rc_t fill_zero_chunks(iarray_container_t *c)
+{
+    const Geom &g = c->geom;
+    std::vector<uint8_t> h((size_t)g.nchunks * 32, 0);
+    for (int64_t k = 0; k < g.nchunks; k++) {
+        uint8_t *p = &h[k * 32];
+        p[0] = 5; p[1] = 1; p[2] = 0x05 | (1 << 5); p[3] = (uint8_t)g.itemsize;
+        const int32_t nb = (int32_t)g.chunk_nbytes, bs = (int32_t)g.blocksize, cb = 32;
+        memcpy(p + 4, &nb, 4); memcpy(p + 8, &bs, 4); memcpy(p + 12, &cb, 4);
+        p[21] = c->shuffle ? 1 : 0;
+        p[22] = 1;
+        p[31] = 1 << 4;   // special value: zeros
+    }
+    ChunkStore &s = *c->store;
+    if (!s.buf.allocate(std::max<size_t>(h.size(), 1), s.device)) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    if (!h.empty() && cudaMemcpy(s.buf.p, h.data(), h.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return rc_err(IARRAY_ERR_GPU_FAILED);
+    s.off.resize((size_t)g.nchunks);
+    s.len.assign((size_t)g.nchunks, 32);
+    for (int64_t k = 0; k < g.nchunks; k++) s.off[k] = k * 32;
+    if (!s.upload_index()) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_empty(iarray_context_t *ctx, iarray_dtshape_t *dtshape, iarray_storage_t *storage,
+                               iarray_container_t **container)
+{
+    ina_rc_t rc = new_container(ctx, dtshape, storage, container);
+    if (INA_FAILED(rc)) return rc;
+    rc = fill_zero_chunks(*container);
+    if (INA_FAILED(rc)) { iarray_container_free(ctx, container); return rc; }
+    return save_if_urlpath(ctx, *container);
+}
+
+INA_API(ina_rc_t) iarray_zeros(iarray_context_t *ctx, iarray_dtshape_t *dtshape, iarray_storage_t *storage,
+                               iarray_container_t **container)
+{
+    return iarray_empty(ctx, dtshape, storage, container);
+}
+
+INA_API(void) iarray_container_free(iarray_context_t *ctx, iarray_container_t **container)
+{
+    (void)ctx;
+    if (!container || !*container) return;
+    delete *container;
+    *container = nullptr;
+}
+
+// Encode a dense device array (row-major, leading dimension ld) into c's store.
+static ina_rc_t encode_into(iarray_context_t *ctx, iarray_container_t *c, const void *dense, int64_t ld)
+{
+    ChunkStore &s = *c->store;
+    DevBuf out;
+    std::vector<int64_t> off;
+    std::vector<int32_t> len;
+    int r = iab::encode_container(c->geom, dense, ld, c->shuffle, c->splitmode, &out, &off, &len, ctx->stream);
+    if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    if (r != 0) return rc_err(IARRAY_ERR_GPU_FAILED);
+    s.buf = std::move(out);
+    s.off = std::move(off);
+    s.len = std::move(len);
+    if (!s.upload_index()) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    return INA_SUCCESS;
+}
+
+// Decode the stored chunks of c (its base geometry, not the view) into dense memory.
+static ina_rc_t decode_store(iarray_context_t *ctx, const iarray_container_t *c, void *dense, int64_t ld)
+{
+    const Geom &g = c->geom;
+    if (g.nchunks == 0) return INA_SUCCESS;
+    if (ld != g.shape[1] || g.nchunks * g.nblocks == 0) {
+        // padding columns must read as zero for the products
+        cudaMemsetAsync(dense, 0, (size_t)(g.shape[0] * ld * g.itemsize), ctx->stream);
+    }
+    const ChunkStore &s = *c->store;
+    const int r = iab::decode_container(g, s.buf.as<uint8_t>(), s.d_off.as<int64_t>(), s.d_len.as<int32_t>(), dense, ld,
+                                        ctx->stream);
+    if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    if (r < 0) return rc_err(IARRAY_ERR_GPU_FAILED);
+    if (r > 0) return rc_err(IARRAY_ERR_BLOSC_FAILED);
+    return INA_SUCCESS;
+}
+
+static int64_t rows_of(const iarray_dtshape_t &d) { return d.ndim == 2 ? d.shape[0] : 1; }
+static int64_t cols_of(const iarray_dtshape_t &d) { return d.ndim == 2 ? d.shape[1] : d.shape[0]; }
+static int64_t pad_ld(int64_t cols) { return std::max<int64_t>(iab::round_up(cols, 32), 32); }
+
+// Decode a container (honouring a transposed view) into dense memory, logical
+// rows x cols with leading dimension ld.
+static ina_rc_t decode_logical(iarray_context_t *ctx, const iarray_container_t *c, void *dense, int64_t ld)
+{
+    if (!c->transposed) return decode_store(ctx, c, dense, ld);
+    const Geom &g = c->geom;
+    DevBuf tmp;
+    const int64_t bld = pad_ld(g.shape[1]);
+    if (!tmp.allocate((size_t)(std::max<int64_t>(g.shape[0], 1) * bld * g.itemsize), ctx->device))
+        return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    ina_rc_t rc = decode_store(ctx, c, tmp.p, bld);
+    if (INA_FAILED(rc)) return rc;
+    if (ld != g.shape[0]) cudaMemsetAsync(dense, 0, (size_t)(g.shape[1] * ld * g.itemsize), ctx->stream);
+    iab::transpose_dense(g.itemsize, g.shape[0], g.shape[1], tmp.p, bld, dense, ld, ctx->stream);
+    return cuda_rc(cudaStreamSynchronize(ctx->stream));
+}
+
+INA_API(ina_rc_t) iarray_from_buffer(iarray_context_t *ctx, iarray_dtshape_t *dtshape, void *buffer, int64_t buflen,
+                                     iarray_storage_t *storage, iarray_container_t **container)
+{
+    CHECK_ARG(buffer);
+    ina_rc_t rc = new_container(ctx, dtshape, storage, container);
+    if (INA_FAILED(rc)) return rc;
+    iarray_container_t *c = *container;
+    const int64_t n = rows_of(c->dtshape) * cols_of(c->dtshape);
+    if (buflen < n * c->geom.itemsize) { iarray_container_free(ctx, container); return rc_err(IARRAY_ERR_TOO_SMALL_BUFFER); }
+    DevBuf dense;
+    if (!dense.allocate((size_t)std::max<int64_t>(n * c->geom.itemsize, 1), ctx->device)) {
+        iarray_container_free(ctx, container);
+        return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    }
+    cudaMemcpyAsync(dense.p, buffer, (size_t)(n * c->geom.itemsize), cudaMemcpyHostToDevice, ctx->stream);
+    if (c->geom.nchunks == 0) rc = fill_zero_chunks(c);
+    else rc = encode_into(ctx, c, dense.p, cols_of(c->dtshape));
+    if (INA_FAILED(rc)) { iarray_container_free(ctx, container); return rc; }
+    return save_if_urlpath(ctx, c);
+}
+
+INA_API(ina_rc_t) iarray_to_buffer(iarray_context_t *ctx, iarray_container_t *container, void *buffer, int64_t buflen)
+{
+    CHECK_ARG(ctx && container && buffer);
+    const iarray_container_t *c = container;
+    const int64_t rows = rows_of(c->dtshape), cols = cols_of(c->dtshape);
+    const int64_t nb = rows * cols * c->geom.itemsize;
+    if (buflen < nb) return rc_err(IARRAY_ERR_TOO_SMALL_BUFFER);
+    if (nb == 0) return INA_SUCCESS;
+    DevBuf dense;
+    if (!dense.allocate((size_t)nb, ctx->device)) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    ina_rc_t rc = decode_logical(ctx, c, dense.p, cols);
+    if (INA_FAILED(rc)) return rc;
+    cudaMemcpyAsync(buffer, dense.p, (size_t)nb, cudaMemcpyDeviceToHost, ctx->stream);
+    return cuda_rc(cudaStreamSynchronize(ctx->stream));
+}
+
+INA_API(ina_rc_t) iarray_arange(iarray_context_t *ctx, iarray_dtshape_t *dtshape, double start, double step,
+                                iarray_storage_t *storage, iarray_container_t **container)
+{
+    ina_rc_t rc = new_container(ctx, dtshape, storage, container);
+    if (INA_FAILED(rc)) return rc;
+    iarray_container_t *c = *container;
+    if (c->dtshape.dtype != IARRAY_DATA_TYPE_DOUBLE && c->dtshape.dtype != IARRAY_DATA_TYPE_FLOAT) {
+        iarray_container_free(ctx, container);
+        return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    }
+    const int64_t rows = rows_of(c->dtshape), cols = cols_of(c->dtshape);
+    DevBuf dense;
+    if (!dense.allocate((size_t)std::max<int64_t>(rows * cols * c->geom.itemsize, 1), ctx->device)) {
+        iarray_container_free(ctx, container);
+        return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    }
+    iab::fill_arange(c->dtshape.dtype == IARRAY_DATA_TYPE_DOUBLE ? 0 : 1, rows, cols, cols, start, step, dense.p,
+                     ctx->stream);
+    rc = c->geom.nchunks ? encode_into(ctx, c, dense.p, cols) : fill_zero_chunks(c);
+    if (INA_FAILED(rc)) { iarray_container_free(ctx, container); return rc; }
+    return save_if_urlpath(ctx, c);
+}
+
+INA_API(ina_rc_t) iarray_linspace(iarray_context_t *ctx, iarray_dtshape_t *dtshape, double start, double stop,
+                                  iarray_storage_t *storage, iarray_container_t **container)
+{
+    CHECK_ARG(dtshape);
+    int64_t n = 1;
+    for (int i = 0; i < dtshape->ndim; i++) n *= dtshape->shape[i];
+    const double step = n > 1 ? (stop - start) / (double)(n - 1) : 0.0;
+    return iarray_arange(ctx, dtshape, start, step, storage, container);
+}
+
+INA_API(ina_rc_t) iarray_container_info(iarray_container_t *container, int64_t *nbytes, int64_t *cbytes)
+{
+    CHECK_ARG(container && nbytes && cbytes);
+    *nbytes = container->geom.nchunks * container->geom.chunk_nbytes;
+    *cbytes = container->store->cbytes;
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_get_dtshape(iarray_context_t *ctx, iarray_container_t *c, iarray_dtshape_t *dtshape)
+{
+    (void)ctx;
+    CHECK_ARG(c && dtshape);
+    *dtshape = c->dtshape;
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_get_storage(iarray_context_t *ctx, iarray_container_t *c, iarray_storage_t *storage)
+{
+    (void)ctx;
+    CHECK_ARG(c && storage);
+    *storage = c->storage;
+    storage->urlpath = c->urlpath.empty() ? nullptr : (char *)c->urlpath.c_str();
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_is_view(iarray_context_t *ctx, iarray_container_t *c, bool *view)
+{
+    (void)ctx;
+    CHECK_ARG(c && view);
+    *view = c->view;
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_b200_nchunks(iarray_container_t *c, int64_t *nchunks)
+{
+    CHECK_ARG(c && nchunks);
+    *nchunks = c->geom.nchunks;
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_b200_get_chunk(iarray_context_t *ctx, iarray_container_t *c, int64_t nchunk, uint8_t *buf,
+                                        int64_t *len)
+{
+    CHECK_ARG(ctx && c && len && nchunk >= 0 && nchunk < c->geom.nchunks);
+    const ChunkStore &s = *c->store;
+    const int32_t l = s.len[nchunk];
+    if (!buf) { *len = l; return INA_SUCCESS; }
+    if (*len < l) return rc_err(IARRAY_ERR_TOO_SMALL_BUFFER);
+    *len = l;
+    cudaMemcpyAsync(buf, s.buf.as<uint8_t>() + s.off[nchunk], (size_t)l, cudaMemcpyDeviceToHost, ctx->stream);
+    return cuda_rc(cudaStreamSynchronize(ctx->stream));
+}
+
+static ina_rc_t upload_chunks(iarray_context_t *ctx, iarray_container_t *c, const uint8_t *const *chunks,
+                              const int64_t *lens)
+{
+    const Geom &g = c->geom;
+    ChunkStore &s = *c->store;
+    int64_t total = 0;
+    for (int64_t k = 0; k < g.nchunks; k++) {
+        if (lens[k] < 32 || lens[k] > g.chunk_nbytes + 64) return rc_err(IARRAY_ERR_BLOSC_FAILED);
+        total += lens[k];
+    }
+    if (!s.buf.allocate((size_t)std::max<int64_t>(total, 1), s.device)) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    // one staging copy keeps the H2D transfer to a single large cudaMemcpyAsync
+    std::vector<uint8_t> stage((size_t)total);
+    s.off.resize((size_t)g.nchunks);
+    s.len.resize((size_t)g.nchunks);
+    int64_t acc = 0;
+    for (int64_t k = 0; k < g.nchunks; k++) {
+        memcpy(stage.data() + acc, chunks[k], (size_t)lens[k]);
+        s.off[k] = acc;
+        s.len[k] = (int32_t)lens[k];
+        acc += lens[k];
+    }
+    if (total) cudaMemcpyAsync(s.buf.p, stage.data(), (size_t)total, cudaMemcpyHostToDevice, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    if (!s.upload_index()) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_b200_from_chunks(iarray_context_t *ctx, iarray_dtshape_t *dtshape, iarray_storage_t *storage,
+                                          int64_t nchunks, const uint8_t *const *chunks, const int64_t *chunk_lens,
+                                          iarray_container_t **container)
+{
+    CHECK_ARG(chunks && chunk_lens);
+    ina_rc_t rc = new_container(ctx, dtshape, storage, container);
+    if (INA_FAILED(rc)) return rc;
+    if (nchunks != (*container)->geom.nchunks) {
+        iarray_container_free(ctx, container);
+        return rc_err(IARRAY_ERR_INVALID_STORAGE);
+    }
+    rc = upload_chunks(ctx, *container, chunks, chunk_lens);
+    if (INA_FAILED(rc)) iarray_container_free(ctx, container);
+    return rc;
+}
+
+INA_API(ina_rc_t) iarray_b200_decode_to_device(iarray_context_t *ctx, iarray_container_t *c, void *dptr, int64_t ld)
+{
+    CHECK_ARG(ctx && c && dptr && ld >= cols_of(c->dtshape));
+    return decode_logical(ctx, c, dptr, ld);
+}
+
+INA_API(ina_rc_t) iarray_b200_encode_from_device(iarray_context_t *ctx, iarray_dtshape_t *dtshape, const void *dptr,
+                                                 int64_t ld, iarray_storage_t *storage, iarray_container_t **container)
+{
+    CHECK_ARG(dptr);
+    ina_rc_t rc = new_container(ctx, dtshape, storage, container);
+    if (INA_FAILED(rc)) return rc;
+    if (ld < cols_of((*container)->dtshape)) { iarray_container_free(ctx, container); return rc_err(INA_ERR_INVALID_ARGUMENT); }
+    rc = (*container)->geom.nchunks ? encode_into(ctx, *container, dptr, ld) : fill_zero_chunks(*container);
+    if (INA_FAILED(rc)) iarray_container_free(ctx, container);
+    return rc;
+}
+
+INA_API(ina_rc_t) iarray_container_almost_equal(iarray_container_t *a, iarray_container_t *b, double tol)
+{
+    CHECK_ARG(a && b);
+    if (a->dtshape.dtype != b->dtshape.dtype) return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    if (a->dtshape.ndim != b->dtshape.ndim) return rc_err(IARRAY_ERR_INVALID_NDIM);
+    for (int i = 0; i < a->dtshape.ndim; i++)
+        if (a->dtshape.shape[i] != b->dtshape.shape[i]) return rc_err(IARRAY_ERR_INVALID_SHAPE);
+    iarray_config_t cfg = IARRAY_CONFIG_DEFAULTS;
+    iarray_context_t *ctx = nullptr;
+    ina_rc_t rc = iarray_context_new(&cfg, &ctx);
+    if (INA_FAILED(rc)) return rc;
+    const int64_t n = rows_of(a->dtshape) * cols_of(a->dtshape);
+    const int isz = a->geom.itemsize;
+    std::vector<uint8_t> ha((size_t)(n * isz)), hb((size_t)(n * isz));
+    rc = iarray_to_buffer(ctx, a, ha.data(), n * isz);
+    if (INA_SUCCEED(rc)) rc = iarray_to_buffer(ctx, b, hb.data(), n * isz);
+    iarray_context_free(&ctx);
+    if (INA_FAILED(rc)) return rc;
+    // relative difference |a - b| / a, as src/iarray_container.c:1252-1279 computes it
+    for (int64_t i = 0; i < n; i++) {
+        double va, vb;
+        if (isz == 8) { va = ((double *)ha.data())[i]; vb = ((double *)hb.data())[i]; }
+        else { va = ((float *)ha.data())[i]; vb = ((float *)hb.data())[i]; }
+        const double r = fabs(va - vb) / va;
+        if (r > tol) return rc_err(IARRAY_ERR_ASSERTION_FAILED);
+    }
+    return INA_SUCCESS;
+}
+
+// ============================================================================ persistence
+static ina_rc_t to_frame(iarray_context_t *ctx, iarray_container_t *c, std::vector<uint8_t> *out)
+{
+    const Geom &g = c->geom;
+    const ChunkStore &s = *c->store;
+    std::vector<uint8_t> host((size_t)std::max<int64_t>(s.cbytes, 1));
+    if (s.cbytes) {
+        cudaMemcpyAsync(host.data(), s.buf.p, (size_t)s.cbytes, cudaMemcpyDeviceToHost, ctx->stream);
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return rc_err(IARRAY_ERR_GPU_FAILED);
+    }
+    // chunks are stored back to back in logical order: s.off[k] is a running sum
+    std::vector<const uint8_t *> ptrs;
+    for (int64_t k = 0; k < g.nchunks; k++) ptrs.push_back(host.data() + s.off[k]);
+    iab::FrameInfo fi;
+    fi.ndim = c->dtshape.ndim;
+    const iarray_dtshape_t &d = c->dtshape;
+    for (int i = 0; i < fi.ndim; i++) {
+        fi.shape[i] = d.shape[i];
+        fi.chunk[i] = c->storage.chunkshape[i];
+        fi.block[i] = c->storage.blockshape[i];
+    }
+    fi.dtype = d.dtype;
+    fi.typesize = g.itemsize;
+    fi.nbytes = g.nchunks * g.chunk_nbytes;
+    fi.blocksize = (int32_t)g.blocksize;
+    fi.chunksize = (int32_t)g.chunk_nbytes;
+    fi.codec = 1;
+    fi.clevel = c->clevel;
+    fi.nthreads = std::max(1, ctx->cfg.max_num_threads);
+    fi.shuffle = c->shuffle;
+    iab::write_frame(fi, ptrs, s.len, out);
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_to_cframe(iarray_context_t *ctx, iarray_container_t *src, uint8_t **frame, int64_t *frame_len,
+                                   bool *needs_free)
+{
+    CHECK_ARG(ctx && src && frame && frame_len && needs_free);
+    if (src->view) return rc_err(IARRAY_ERR_INVALID_STORAGE);
+    std::vector<uint8_t> f;
+    ina_rc_t rc = to_frame(ctx, src, &f);
+    if (INA_FAILED(rc)) return rc;
+    uint8_t *p = (uint8_t *)malloc(f.size());
+    if (!p) return rc_err(INA_ERR_OUT_OF_MEMORY);
+    memcpy(p, f.data(), f.size());
+    *frame = p;
+    *frame_len = (int64_t)f.size();
+    *needs_free = true;
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_from_cframe(iarray_context_t *ctx, uint8_t *frame, int64_t frame_len, bool copy,
+                                     iarray_container_t **container)
+{
+    (void)copy;   // chunks are always copied to the GPU
+    CHECK_ARG(ctx && frame && container && frame_len > 0);
+    iab::FrameInfo fi;
+    std::vector<std::pair<int64_t, int32_t>> chunks;
+    std::string why;
+    if (!iab::read_frame(frame, (size_t)frame_len, &fi, &chunks, &why)) return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+    iarray_dtshape_t d;
+    memset(&d, 0, sizeof(d));
+    d.dtype = (iarray_data_type_t)fi.dtype;
+    d.ndim = (int8_t)fi.ndim;
+    iarray_storage_t st;
+    memset(&st, 0, sizeof(st));
+    for (int i = 0; i < fi.ndim; i++) { d.shape[i] = fi.shape[i]; st.chunkshape[i] = fi.chunk[i]; st.blockshape[i] = fi.block[i]; }
+    ina_rc_t rc = new_container(ctx, &d, &st, container);
+    if (INA_FAILED(rc)) return rc;
+    iarray_container_t *c = *container;
+    if (fi.typesize != c->geom.itemsize || fi.chunksize != c->geom.chunk_nbytes ||
+        (int64_t)chunks.size() != c->geom.nchunks) {
+        iarray_container_free(ctx, container);
+        return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+    }
+    c->shuffle = fi.shuffle;
+    c->clevel = fi.clevel;
+    std::vector<const uint8_t *> ptrs;
+    std::vector<int64_t> lens;
+    for (auto &pr : chunks) { ptrs.push_back(frame + pr.first); lens.push_back(pr.second); }
+    rc = upload_chunks(ctx, c, ptrs.data(), lens.data());
+    if (INA_FAILED(rc)) iarray_container_free(ctx, container);
+    return rc;
+}
+
+static ina_rc_t write_file(const char *path, const std::vector<uint8_t> &f)
+{
+    FILE *fp = fopen(path, "wb");
+    if (!fp) return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+    const size_t w = fwrite(f.data(), 1, f.size(), fp);
+    fclose(fp);
+    return w == f.size() ? INA_SUCCESS : rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+}
+
+static ina_rc_t save_if_urlpath(iarray_context_t *ctx, iarray_container_t *c)
+{
+    if (c->urlpath.empty()) return INA_SUCCESS;
+    std::vector<uint8_t> f;
+    ina_rc_t rc = to_frame(ctx, c, &f);
+    if (INA_FAILED(rc)) return rc;
+    return write_file(c->urlpath.c_str(), f);
+}
+
+INA_API(ina_rc_t) iarray_container_save(iarray_context_t *ctx, iarray_container_t *container, char *urlpath)
+{
+    CHECK_ARG(ctx && container && urlpath);
+    if (container->view) return rc_err(IARRAY_ERR_INVALID_STORAGE);   // src/iarray_container.c:57-61
+    if (!container->urlpath.empty()) return rc_err(IARRAY_ERR_INVALID_STORAGE);
+    std::vector<uint8_t> f;
+    ina_rc_t rc = to_frame(ctx, container, &f);
+    if (INA_FAILED(rc)) return rc;
+    return write_file(urlpath, f);
+}
+
+static ina_rc_t load_file(iarray_context_t *ctx, char *urlpath, iarray_container_t **container, bool keep_path)
+{
+    CHECK_ARG(ctx && urlpath && container);
+    FILE *fp = fopen(urlpath, "rb");
+    if (!fp) return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+    fseek(fp, 0, SEEK_END);
+    const long n = ftell(fp);
+    fseek(fp, 0, SEEK_SET);
+    std::vector<uint8_t> f((size_t)std::max(n, 0L));
+    const size_t r = n > 0 ? fread(f.data(), 1, (size_t)n, fp) : 0;
+    fclose(fp);
+    if (n <= 0 || r != (size_t)n) return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+    ina_rc_t rc = iarray_from_cframe(ctx, f.data(), (int64_t)f.size(), true, container);
+    if (INA_SUCCEED(rc) && keep_path) (*container)->urlpath = urlpath;
+    return rc;
+}
+
+INA_API(ina_rc_t) iarray_container_open(iarray_context_t *ctx, char *urlpath, iarray_container_t **container)
+{
+    return load_file(ctx, urlpath, container, true);
+}
+
+INA_API(ina_rc_t) iarray_container_load(iarray_context_t *ctx, char *urlpath, iarray_container_t **container)
+{
+    return load_file(ctx, urlpath, container, false);
+}
+
+// ============================================================================ linear algebra
+INA_API(ina_rc_t) iarray_linalg_transpose(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t **b)
+{
+    (void)ctx;
+    CHECK_ARG(a && b);
+    if (a->view) return rc_err(IARRAY_ERR_NOT_SUPPORTED);          // src/linalg/transpose.c:23-26
+    if (a->dtshape.ndim != 2) return rc_err(IARRAY_ERR_INVALID_NDIM);
+    iarray_container_t *v = new iarray_container_t(*a);
+    v->dtshape.shape[0] = a->dtshape.shape[1];
+    v->dtshape.shape[1] = a->dtshape.shape[0];
+    v->transposed = true;
+    v->view = true;
+    v->urlpath.clear();
+    *b = v;
+    return INA_SUCCESS;
+}
+
+struct Timer {
+    iarray_context_t *ctx;
+    explicit Timer(iarray_context_t *c) : ctx(c) { cudaEventRecord(ctx->ev[0], ctx->stream); }
+    void mark(int i) { cudaEventRecord(ctx->ev[i], ctx->stream); }
+    void finish()
+    {
+        cudaEventSynchronize(ctx->ev[4]);
+        float t;
+        for (int i = 0; i < 4; i++) {
+            cudaEventElapsedTime(&t, ctx->ev[i], ctx->ev[i + 1]);
+            ctx->timings[i] = t;
+        }
+        cudaEventElapsedTime(&t, ctx->ev[0], ctx->ev[4]);
+        ctx->timings[4] = t;
+    }
+};
+
+// Run the product on dense device operands with the context's form.
+static ina_rc_t dense_product(iarray_context_t *ctx, int dtype, int64_t M, int64_t N, int64_t K, const void *A,
+                              int64_t lda, const void *B, int64_t ldb, void *C, int64_t ldc)
+{
+    if (ctx->form == IARRAY_B200_FORM_SPLIT) {
+        int r;
+        if (dtype == IARRAY_DATA_TYPE_DOUBLE)
+            r = iab::gemm_f64_ozaki(M, N, K, (const double *)A, lda, (const double *)B, ldb, (double *)C, ldc,
+                                    ctx->split_terms, ctx->stream);
+        else
+            r = iab::gemm_f32_bf16x3(M, N, K, (const float *)A, lda, (const float *)B, ldb, (float *)C, ldc, ctx->stream);
+        if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+        if (r != 0) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
+    } else if (dtype == IARRAY_DATA_TYPE_DOUBLE) {
+        iab::gemm_f64_native(M, N, K, (const double *)A, lda, (const double *)B, ldb, (double *)C, ldc, ctx->stream);
+    } else {
+        iab::gemm_f32_native(M, N, K, (const float *)A, lda, (const float *)B, ldb, (float *)C, ldc, ctx->stream);
+    }
+    return cuda_rc(cudaGetLastError());
+}
+
+INA_API(ina_rc_t) iarray_b200_dense_gemm(iarray_context_t *ctx, int dtype, int64_t M, int64_t N, int64_t K,
+                                         const void *A, int64_t lda, const void *B, int64_t ldb, void *C, int64_t ldc)
+{
+    CHECK_ARG(ctx && A && B && C && M >= 0 && N >= 0 && K >= 0);
+    CHECK_ARG(dtype == IARRAY_DATA_TYPE_DOUBLE || dtype == IARRAY_DATA_TYPE_FLOAT);
+    const int64_t align = dtype == IARRAY_DATA_TYPE_DOUBLE ? 2 : 4;
+    CHECK_ARG(lda % align == 0 && ldb % align == 0 && ldc % align == 0);
+    CHECK_ARG(lda >= K && ldb >= N && ldc >= N);
+    if (M == 0 || N == 0) return INA_SUCCESS;
+    return dense_product(ctx, dtype, M, N, K, A, lda, B, ldb, C, ldc);
+}
+
+// Decode -> product -> encode into the already-created container c.
+static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b, iarray_container_t *c)
+{
+    const int dtype = a->dtshape.dtype;
+    const int isz = a->geom.itemsize;
+    const int64_t M = a->dtshape.shape[0], K = a->dtshape.shape[1];
+    const bool vec = b->dtshape.ndim == 1;
+    const int64_t N = vec ? 1 : b->dtshape.shape[1];
+    const int64_t lda = pad_ld(K), ldb = vec ? 1 : pad_ld(N), ldc = vec ? 1 : pad_ld(N);
+    Timer tm(ctx);
+    DevBuf dA, dB, dC;
+    if (!dA.allocate((size_t)std::max<int64_t>(M * lda * isz, 16), ctx->device) ||
+        !dB.allocate((size_t)std::max<int64_t>((vec ? pad_ld(K) : K * ldb) * isz, 16), ctx->device) ||
+        !dC.allocate((size_t)std::max<int64_t>((vec ? pad_ld(M) : M * ldc) * isz, 16), ctx->device))
+        return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    ina_rc_t rc = decode_logical(ctx, a, dA.p, lda);
+    if (INA_FAILED(rc)) return rc;
+    tm.mark(1);
+    if (vec) cudaMemsetAsync(dB.p, 0, (size_t)(pad_ld(K) * isz), ctx->stream);
+    rc = decode_logical(ctx, b, dB.p, vec ? K : ldb);
+    if (INA_FAILED(rc)) return rc;
+    tm.mark(2);
+    if (K == 0) {
+        cudaMemsetAsync(dC.p, 0, (size_t)((vec ? M : M * ldc) * isz), ctx->stream);
+    } else if (vec) {
+        iab::gemv_native(dtype == IARRAY_DATA_TYPE_DOUBLE ? 0 : 1, M, K, dA.p, lda, dB.p, dC.p, ctx->stream);
+        rc = cuda_rc(cudaGetLastError());
+    } else {
+        rc = dense_product(ctx, dtype, M, N, K, dA.p, lda, dB.p, ldb, dC.p, ldc);
+    }
+    if (INA_FAILED(rc)) return rc;
+    tm.mark(3);
+    dA.reset();
+    dB.reset();
+    rc = c->geom.nchunks ? encode_into(ctx, c, dC.p, vec ? M : ldc) : fill_zero_chunks(c);
+    if (INA_FAILED(rc)) return rc;
+    tm.mark(4);
+    tm.finish();
+    return save_if_urlpath(ctx, c);
+}
+
+static ina_rc_t output_container(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b,
+                                 iarray_storage_t *storage, iarray_container_t **c)
+{
+    iarray_dtshape_t d;
+    memset(&d, 0, sizeof(d));
+    d.dtype = a->dtshape.dtype;
+    d.ndim = b->dtshape.ndim;
+    d.shape[0] = a->dtshape.shape[0];
+    if (d.ndim > 1) d.shape[1] = b->dtshape.shape[1];
+    ina_rc_t rc = new_container(ctx, &d, storage, c);
+    if (INA_FAILED(rc)) return rc;
+    (*c)->shuffle = true;   // blosc2 cparams defaults keep SHUFFLE in the last filter slot
+    return INA_SUCCESS;
+}
+
+static ina_rc_t check_operands(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b, iarray_storage_t *storage,
+                               iarray_container_t **c)
+{
+    CHECK_ARG(ctx && a && b && storage && c);
+    if (a->dtshape.dtype != IARRAY_DATA_TYPE_DOUBLE && a->dtshape.dtype != IARRAY_DATA_TYPE_FLOAT)
+        return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_linalg_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b,
+                                       iarray_storage_t *storage, iarray_container_t **c)
+{
+    CHECK_ARG(ctx && a && b && storage && c);
+    // src/linalg/matmul.c:31-55
+    if (a->dtshape.ndim != 2 || (b->dtshape.ndim != 1 && b->dtshape.ndim != 2)) return rc_err(IARRAY_ERR_INVALID_NDIM);
+    if (a->dtshape.shape[1] != b->dtshape.shape[0]) return rc_err(IARRAY_ERR_INVALID_SHAPE);
+    if (a->dtshape.dtype != b->dtshape.dtype) return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    ina_rc_t rc = check_operands(ctx, a, b, storage, c);
+    if (INA_FAILED(rc)) return rc;
+    const int64_t oshape[2] = {a->dtshape.shape[0], b->dtshape.ndim > 1 ? b->dtshape.shape[1] : 0};
+    for (int i = 0; i < b->dtshape.ndim; i++)
+        if (oshape[i] < storage->chunkshape[i]) return rc_err(IARRAY_ERR_INVALID_CHUNKSHAPE);
+    rc = output_container(ctx, a, b, storage, c);
+    if (INA_FAILED(rc)) return rc;
+    rc = run_matmul(ctx, a, b, *c);
+    if (INA_FAILED(rc)) iarray_container_free(ctx, c);
+    return rc;
+}
+
+INA_API(ina_rc_t) iarray_gemm(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b, iarray_container_t *c)
+{
+    CHECK_ARG(ctx && a && b && c);
+    if (a->dtshape.ndim != 2 || b->dtshape.ndim != 2 || c->dtshape.ndim != 2) return rc_err(IARRAY_ERR_INVALID_NDIM);
+    if (a->dtshape.shape[1] != b->dtshape.shape[0] || c->dtshape.shape[0] != a->dtshape.shape[0] ||
+        c->dtshape.shape[1] != b->dtshape.shape[1])
+        return rc_err(IARRAY_ERR_INVALID_SHAPE);
+    if (a->dtshape.dtype != b->dtshape.dtype || c->dtshape.dtype != a->dtshape.dtype) return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    c->shuffle = true;
+    return run_matmul(ctx, a, b, c);
+}
+
+INA_API(ina_rc_t) iarray_gemv(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b, iarray_container_t *c)
+{
+    CHECK_ARG(ctx && a && b && c);
+    if (a->dtshape.ndim != 2 || b->dtshape.ndim != 1 || c->dtshape.ndim != 1) return rc_err(IARRAY_ERR_INVALID_NDIM);
+    if (a->dtshape.shape[1] != b->dtshape.shape[0] || c->dtshape.shape[0] != a->dtshape.shape[0])
+        return rc_err(IARRAY_ERR_INVALID_SHAPE);
+    if (a->dtshape.dtype != b->dtshape.dtype || c->dtshape.dtype != a->dtshape.dtype) return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    c->shuffle = true;
+    return run_matmul(ctx, a, b, c);
+}
+
+// Partition checks of iarray_opt_gemm (src/linalg/iarray_gemm.c:327-364).
+INA_API(ina_rc_t) iarray_opt_gemm(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b,
+                                  iarray_storage_t *storage, iarray_container_t **c)
+{
+    ina_rc_t rc = check_operands(ctx, a, b, storage, c);
+    if (INA_FAILED(rc)) return rc;
+    if (a->dtshape.ndim != 2 || b->dtshape.ndim != 2) return rc_err(IARRAY_ERR_INVALID_NDIM);
+    if (a->dtshape.shape[1] != b->dtshape.shape[0]) return rc_err(IARRAY_ERR_INVALID_SHAPE);
+    if (a->dtshape.dtype != b->dtshape.dtype) return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    const int64_t *ac = a->storage.chunkshape, *bc = b->storage.chunkshape, *ab = a->storage.blockshape,
+                  *bb = b->storage.blockshape;
+    if (a->transposed || b->transposed) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
+    if (ac[0] != storage->chunkshape[0] || ac[1] != bc[0] || bc[1] != storage->chunkshape[1])
+        return rc_err(IARRAY_ERR_INVALID_CHUNKSHAPE);
+    if (ab[0] != storage->blockshape[0] || ab[1] != bb[0] || bb[1] != storage->blockshape[1])
+        return rc_err(IARRAY_ERR_INVALID_BLOCKSHAPE);
+    rc = output_container(ctx, a, b, storage, c);
+    if (INA_FAILED(rc)) return rc;
+    rc = run_matmul(ctx, a, b, *c);
+    if (INA_FAILED(rc)) iarray_container_free(ctx, c);
+    return rc;
+}
+
+// Partition checks of iarray_opt_gemm_a (src/linalg/iarray_gemm_a.c:212-263); with
+// `swap`, the mirrored checks of iarray_opt_gemm_b (src/linalg/iarray_gemm_b.c).
+static ina_rc_t opt_gemm_ab(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b,
+                            iarray_storage_t *storage, iarray_container_t **c, bool swap)
+{
+    ina_rc_t rc = check_operands(ctx, a, b, storage, c);
+    if (INA_FAILED(rc)) return rc;
+    if (a->dtshape.ndim != 2 || b->dtshape.ndim != 2) return rc_err(IARRAY_ERR_INVALID_NDIM);
+    if (a->dtshape.shape[1] != b->dtshape.shape[0]) return rc_err(IARRAY_ERR_INVALID_SHAPE);
+    if (a->dtshape.dtype != b->dtshape.dtype) return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    if (a->transposed || b->transposed) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
+    const int64_t *ac = a->storage.chunkshape, *bc = b->storage.chunkshape, *ab = a->storage.blockshape,
+                  *bb = b->storage.blockshape, *as = a->dtshape.shape, *bs = b->dtshape.shape;
+    const int64_t *cc = storage->chunkshape, *cb = storage->blockshape;
+    if (!swap) {
+        if (ac[1] < as[1] || bc[0] < bs[0] || ac[1] != bc[0]) return rc_err(IARRAY_ERR_INVALID_CHUNKSHAPE);
+        if (ac[0] != cc[0] || bs[1] > cc[1]) return rc_err(IARRAY_ERR_INVALID_CHUNKSHAPE);
+        if (ac[0] != cb[0] || bc[1] != cb[1] || ac[0] != ab[0] || bc[1] != bb[1] || ab[1] != bb[0])
+            return rc_err(IARRAY_ERR_INVALID_BLOCKSHAPE);
+    } else {
+        if (ac[1] < as[1] || bc[0] < bs[0] || ac[1] != bc[0]) return rc_err(IARRAY_ERR_INVALID_CHUNKSHAPE);
+        if (bc[1] != cc[1] || as[0] > cc[0]) return rc_err(IARRAY_ERR_INVALID_CHUNKSHAPE);
+        if (ac[0] != cb[0] || bc[1] != cb[1] || ac[0] != ab[0] || bc[1] != bb[1] || ab[1] != bb[0])
+            return rc_err(IARRAY_ERR_INVALID_BLOCKSHAPE);
+    }
+    rc = output_container(ctx, a, b, storage, c);
+    if (INA_FAILED(rc)) return rc;
+    rc = run_matmul(ctx, a, b, *c);
+    if (INA_FAILED(rc)) iarray_container_free(ctx, c);
+    return rc;
+}
+
+INA_API(ina_rc_t) iarray_opt_gemm_a(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b,
+                                    iarray_storage_t *storage, iarray_container_t **c)
+{
+    return opt_gemm_ab(ctx, a, b, storage, c, false);
+}
+
+INA_API(ina_rc_t) iarray_opt_gemm_b(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b,
+                                    iarray_storage_t *storage, iarray_container_t **c)
+{
+    return opt_gemm_ab(ctx, a, b, storage, c, true);
+}
+
+// Partition checks of iarray_opt_gemv (src/linalg/iarray_gemv.c:261-286).
+INA_API(ina_rc_t) iarray_opt_gemv(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b,
+                                  iarray_storage_t *storage, iarray_container_t **c)
+{
+    ina_rc_t rc = check_operands(ctx, a, b, storage, c);
+    if (INA_FAILED(rc)) return rc;
+    if (a->dtshape.ndim != 2 || b->dtshape.ndim != 1) return rc_err(IARRAY_ERR_INVALID_NDIM);
+    if (a->dtshape.shape[1] != b->dtshape.shape[0]) return rc_err(IARRAY_ERR_INVALID_SHAPE);
+    if (a->dtshape.dtype != b->dtshape.dtype) return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    if (a->transposed) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
+    const int64_t *ac = a->storage.chunkshape, *bc = b->storage.chunkshape, *ab = a->storage.blockshape,
+                  *bb = b->storage.blockshape;
+    if (ac[0] != storage->chunkshape[0] || ac[1] != bc[0]) return rc_err(IARRAY_ERR_INVALID_CHUNKSHAPE);
+    if (ab[0] != storage->blockshape[0] || ab[1] != bb[0]) return rc_err(IARRAY_ERR_INVALID_BLOCKSHAPE);
+    rc = output_container(ctx, a, b, storage, c);
+    if (INA_FAILED(rc)) return rc;
+    rc = run_matmul(ctx, a, b, *c);
+    if (INA_FAILED(rc)) iarray_container_free(ctx, c);
+    return rc;
+}

@@ -1,0 +1,796 @@
+// Blosc2 LZ4+SHUFFLE chunk decoder and encoder on the GPU.
+//
+// Replaces, for ironArray's matmul path, the Blosc2 block decode done by
+// blosc2_getitem_ctx / blosc2_decompress_ctx (src/linalg/iarray_gemm.c:259-274,
+// src/linalg/iarray_gemm_a.c:316, src/linalg/iarray_gemv.c:194-209, and the panel
+// slices of src/iarray_container.c:628-737) and the output encode done by
+// blosc2_compress_ctx (src/linalg/iarray_gemm.c:405-422, src/linalg/matmul/gemm.c:216-233),
+// plus Caterva's padded blocked layout (iarray_from_buffer / iarray_to_buffer,
+// src/iarray_constructor.c:218-305).
+//
+// Decode = parse (one thread per block walks its stream headers) -> LZ4 (one warp per
+// LZ4 stream, 8 KiB shared-memory history ring) -> unshuffle/scatter (one CTA per
+// block tile, byte planes staged in shared memory, items written to the dense
+// row-major array).  Raw and run streams are never copied before the scatter.
+//
+// Encode = gather/shuffle (dense -> byte-plane image) -> LZ4 (one warp per stream,
+// 16 KiB hash table in shared memory, 32 match probes evaluated per step) -> layout
+// (per chunk: stream kinds, offsets, memcpy fallback; exclusive scan of chunk sizes)
+// -> emit (copy payloads into the final contiguous chunk buffer).
+// The LZ4 encoder reproduces liblz4 1.9.4 LZ4_compress_fast(acceleration 1) output
+// byte for byte (the codec c-blosc2 calls for BLOSC_LZ4); stream-kind selection
+// (zero/run, raw when LZ4 does not fit, memcpyed chunk when the output would exceed
+// nbytes + 32) follows c-blosc2's blosc_c rules.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace iab {
+
+#define FULLMASK 0xffffffffu
+
+__device__ __forceinline__ int32_t ld_s32(const uint8_t *p)
+{
+    return (int32_t)((uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24));
+}
+
+__device__ __forceinline__ void dev_fail(int *err, int code) { atomicCAS(err, 0, code); }
+
+// ============================================================================ decode
+// D0: parse one (chunk, block) per thread.
+__global__ void k_parse(Geom g, const uint8_t *__restrict__ ch, const int64_t *__restrict__ off,
+                        const int32_t *__restrict__ len, BlockDesc *bd, StreamDesc *sd, Lz4Job *jobs,
+                        int *njobs, int *err)
+{
+    const int64_t total = g.nchunks * g.nblocks;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = t / g.nblocks, b = t % g.nblocks;
+        const uint8_t *p = ch + off[c];
+        const int32_t clen = len[c];
+        BlockDesc d;
+        d.mode = BM_PLAIN; d.nstreams = 1; d.neblock = (int32_t)g.blocksize; d.pad = 0; d.value_src = 0;
+        StreamDesc *s = sd + t * 8;
+        for (int j = 0; j < 8; j++) { s[j].kind = SK_RUN; s[j].len = 0; s[j].src = 0; }
+        bool ok = clen >= 32;
+        int32_t nbytes = 0, bsz = 0, cbytes = 0;
+        uint8_t flags = 0, ts = 0, bflags = 0;
+        if (ok) {
+            flags = p[2]; ts = p[3]; bflags = p[31];
+            nbytes = ld_s32(p + 4); bsz = ld_s32(p + 8); cbytes = ld_s32(p + 12);
+            ok = (flags & 0x05) == 0x05 && nbytes == g.chunk_nbytes && cbytes >= 32 && cbytes <= clen;
+        }
+        if (!ok) { dev_fail(err, DE_HEADER); bd[t] = d; continue; }
+        const int special = (bflags >> 4) & 7;
+        if (special) {
+            if (special == 2) d.mode = BM_NAN;
+            else if (special == 3) {
+                if (cbytes < 32 + (int32_t)g.itemsize) dev_fail(err, DE_HEADER);
+                d.mode = BM_VALUE; d.value_src = off[c] + 32;
+            } else if (special != 1 && special != 4) dev_fail(err, DE_HEADER);
+            bd[t] = d;
+            continue;
+        }
+        if (flags & 0x02) {                      // memcpyed: raw blocked items
+            if (cbytes < 32 + nbytes) { dev_fail(err, DE_BOUNDS); bd[t] = d; continue; }
+            s[0].kind = SK_RAW; s[0].len = (int32_t)g.blocksize; s[0].src = off[c] + 32 + b * g.blocksize;
+            bd[t] = d;
+            continue;
+        }
+        // filters: only SHUFFLE (slot 5 == 1) or none are produced on this path
+        bool filt_ok = p[16] == 0 && p[17] == 0 && p[18] == 0 && p[19] == 0 && p[20] == 0 && p[21] <= 1;
+        if (bsz != g.blocksize || ts != g.itemsize || !filt_ok) { dev_fail(err, DE_HEADER); bd[t] = d; continue; }
+        const bool split = !(flags & 0x10);
+        const bool shuffle = p[21] == 1 && ts > 1;
+        const int nstreams = split ? ts : 1;
+        const int neblock = (int)(g.blocksize / nstreams);
+        d.mode = shuffle ? BM_SHUFFLED : BM_PLAIN;
+        d.nstreams = nstreams; d.neblock = neblock;
+        const int64_t bs_end = 32 + 4 * g.nblocks;
+        if (bs_end > cbytes) { d.mode = BM_PLAIN; dev_fail(err, DE_BOUNDS); bd[t] = d; continue; }
+        int64_t q = ld_s32(p + 32 + 4 * b);
+        if (q < bs_end || q >= cbytes) { d.mode = BM_PLAIN; dev_fail(err, DE_BOUNDS); bd[t] = d; continue; }
+        for (int j = 0; j < nstreams; j++) {
+            if (q + 4 > cbytes) { dev_fail(err, DE_BOUNDS); ok = false; break; }
+            const int32_t cs = ld_s32(p + q);
+            q += 4;
+            if (cs == 0) { s[j].kind = SK_RUN; s[j].len = 0; s[j].src = 0; continue; }
+            if (cs < 0) {
+                if (q + 1 > cbytes || !(p[q] & 1) || cs < -255) { dev_fail(err, DE_RUN_TOKEN); ok = false; break; }
+                q += 1;
+                s[j].kind = SK_RUN; s[j].len = -cs; s[j].src = 0;
+                continue;
+            }
+            if (q + cs > cbytes || cs > neblock) { dev_fail(err, DE_BOUNDS); ok = false; break; }
+            s[j].src = off[c] + q;
+            s[j].len = cs;
+            if (cs == neblock) {
+                s[j].kind = SK_RAW;
+            } else {
+                s[j].kind = SK_LZ4;
+                const int k = atomicAdd(njobs, 1);
+                Lz4Job jb;
+                jb.src = off[c] + q; jb.csize = cs; jb.dst = t * g.blocksize + (int64_t)j * neblock; jb.dlen = neblock;
+                jobs[k] = jb;
+            }
+            q += cs;
+        }
+        if (!ok) { for (int j = 0; j < nstreams; j++) { s[j].kind = SK_RUN; s[j].len = 0; } }
+        bd[t] = d;
+    }
+}
+
+// D1: one warp per LZ4 stream.  The 32 input bytes at the parse position are held one
+// per lane and read with shuffles; output goes to the scratch image and to a
+// shared-memory ring that serves matches whose source lies in the last RING bytes.
+template <int RING>
+__global__ void __launch_bounds__(256) k_lz4_decode(const uint8_t *__restrict__ ch, const Lz4Job *__restrict__ jobs,
+                                                    const int *__restrict__ njobs_p, uint8_t *scratch, int *err)
+{
+    extern __shared__ uint8_t sm_ring[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    uint8_t *ring = sm_ring + warp * RING;
+    const int njobs = *njobs_p;
+    for (int jid = blockIdx.x * wpb + warp; jid < njobs; jid += gridDim.x * wpb) {
+        const Lz4Job jb = jobs[jid];
+        const uint8_t *__restrict__ in = ch + jb.src;
+        const int isz = jb.csize;
+        uint8_t *out = scratch + jb.dst;
+        const int osz = jb.dlen;
+        int wbase = 0;
+        uint32_t win = lane < isz ? __ldg(in + lane) : 0u;
+        auto byte_at = [&](int pos) -> int {
+            if ((unsigned)(pos - wbase) >= 32u) {
+                wbase = pos;
+                win = (pos + lane < isz) ? __ldg(in + pos + lane) : 0u;
+            }
+            return (int)__shfl_sync(FULLMASK, win, pos - wbase);
+        };
+        int ip = 0, op = 0;
+        bool bad = false;
+        for (;;) {
+            if (ip >= isz) { bad = true; break; }
+            const int token = byte_at(ip++);
+            int lit = token >> 4;
+            if (lit == 15) {
+                int s;
+                do {
+                    if (ip >= isz) { bad = true; break; }
+                    s = byte_at(ip++);
+                    lit += s;
+                } while (s == 255);
+                if (bad) break;
+            }
+            if (lit > isz - ip || lit > osz - op) { bad = true; break; }
+            for (int x = lane; x < lit; x += 32) {
+                const uint8_t v = __ldg(in + ip + x);
+                out[op + x] = v;
+                ring[(op + x) & (RING - 1)] = v;
+            }
+            ip += lit;
+            op += lit;
+            if (ip == isz) break;
+            if (isz - ip < 2) { bad = true; break; }
+            const int mo = byte_at(ip) | (byte_at(ip + 1) << 8);
+            ip += 2;
+            int ml = token & 15;
+            if (ml == 15) {
+                int s;
+                do {
+                    if (ip >= isz) { bad = true; break; }
+                    s = byte_at(ip++);
+                    ml += s;
+                } while (s == 255);
+                if (bad) break;
+            }
+            ml += 4;
+            if (mo == 0 || mo > op || ml > osz - op) { bad = true; break; }
+            __syncwarp();
+            if (mo + ml <= RING) {
+                for (int x = lane; x < ml; x += 32) {
+                    const int sp = op - mo + (mo >= ml ? x : x % mo);
+                    const uint8_t v = ring[sp & (RING - 1)];
+                    out[op + x] = v;
+                    ring[(op + x) & (RING - 1)] = v;
+                }
+            } else {
+                for (int x = lane; x < ml; x += 32) {
+                    const int sp = op - mo + (mo >= ml ? x : x % mo);
+                    const uint8_t v = __ldcg(out + sp);
+                    out[op + x] = v;
+                    ring[(op + x) & (RING - 1)] = v;
+                }
+            }
+            op += ml;
+            __syncwarp();
+        }
+        if (!bad && op != osz) bad = true;
+        if (bad && lane == 0) dev_fail(err, DE_LZ4);
+        __syncwarp();
+    }
+}
+
+constexpr int TILE = 1024;
+
+__device__ __forceinline__ void store_item(uint8_t *o, int ts, uint64_t v)
+{
+    switch (ts) {
+    case 8: *reinterpret_cast<uint64_t *>(o) = v; break;
+    case 4: *reinterpret_cast<uint32_t *>(o) = (uint32_t)v; break;
+    case 2: *reinterpret_cast<uint16_t *>(o) = (uint16_t)v; break;
+    default: for (int j = 0; j < ts; j++) o[j] = (uint8_t)(v >> (8 * j)); break;
+    }
+}
+
+__device__ __forceinline__ uint64_t load_item(const uint8_t *o, int ts)
+{
+    switch (ts) {
+    case 8: return *reinterpret_cast<const uint64_t *>(o);
+    case 4: return *reinterpret_cast<const uint32_t *>(o);
+    case 2: return *reinterpret_cast<const uint16_t *>(o);
+    default: { uint64_t v = 0; for (int j = 0; j < ts; j++) v |= (uint64_t)o[j] << (8 * j); return v; }
+    }
+}
+
+// Map item i of block b of chunk c to its logical (row, col); false if it is padding.
+__device__ __forceinline__ bool item_pos(const Geom &g, int64_t c, int64_t b, int64_t i, int64_t &row, int64_t &col)
+{
+    const int64_t ci0 = c / g.cgrid[1], ci1 = c - ci0 * g.cgrid[1];
+    const int64_t bi0 = b / g.bgrid[1], bi1 = b - bi0 * g.bgrid[1];
+    const int64_t r = i / g.block[1], cc = i - r * g.block[1];
+    const int64_t rin = bi0 * g.block[0] + r, cin = bi1 * g.block[1] + cc;
+    if (rin >= g.chunk[0] || cin >= g.chunk[1]) return false;
+    row = ci0 * g.chunk[0] + rin;
+    col = ci1 * g.chunk[1] + cin;
+    return row < g.shape[0] && col < g.shape[1];
+}
+
+// D2: unshuffle one tile of TILE items of one block and scatter it to the dense array.
+__global__ void __launch_bounds__(256) k_scatter(Geom g, const uint8_t *__restrict__ ch,
+                                                 const BlockDesc *__restrict__ bd, const StreamDesc *__restrict__ sd,
+                                                 const uint8_t *__restrict__ scratch, uint8_t *__restrict__ out, int64_t ld)
+{
+    __shared__ __align__(16) uint8_t planes[8 * TILE];
+    const int ts = g.itemsize;
+    const int64_t tpb = (g.blockn + TILE - 1) / TILE;
+    const int64_t nwork = g.nchunks * g.nblocks * tpb;
+    for (int64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int64_t t = w / tpb, i0 = (w - t * tpb) * TILE;
+        const int cnt = (int)min((int64_t)TILE, g.blockn - i0);
+        const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
+        const BlockDesc d = bd[t];
+        const StreamDesc *s = sd + t * 8;
+        const uint8_t *blk_scratch = scratch + t * g.blocksize;
+        if (d.mode == BM_SHUFFLED) {
+            for (int j = 0; j < ts; j++) {
+                const int64_t pos = (int64_t)j * g.blockn + i0;
+                const int sidx = (int)(pos / d.neblock);
+                const int64_t so = pos - (int64_t)sidx * d.neblock;
+                const StreamDesc q = s[sidx];
+                uint8_t *pl = planes + j * TILE;
+                if (q.kind == SK_RUN) {
+                    for (int x = threadIdx.x; x < cnt; x += blockDim.x) pl[x] = (uint8_t)q.len;
+                } else if (q.kind == SK_RAW) {
+                    const uint8_t *src = ch + q.src + so;
+                    for (int x = threadIdx.x; x < cnt; x += blockDim.x) pl[x] = __ldg(src + x);
+                } else {
+                    const uint8_t *src = blk_scratch + (int64_t)sidx * d.neblock + so;
+                    for (int x = threadIdx.x; x < cnt; x += blockDim.x) pl[x] = __ldcg(src + x);
+                }
+            }
+        } else if (d.mode == BM_PLAIN) {
+            for (int x = threadIdx.x; x < cnt * ts; x += blockDim.x) {
+                const int64_t pos = i0 * ts + x;
+                const int sidx = (int)(pos / d.neblock);
+                const int64_t so = pos - (int64_t)sidx * d.neblock;
+                const StreamDesc q = s[sidx];
+                uint8_t v;
+                if (q.kind == SK_RUN) v = (uint8_t)q.len;
+                else if (q.kind == SK_RAW) v = __ldg(ch + q.src + so);
+                else v = __ldcg(blk_scratch + (int64_t)sidx * d.neblock + so);
+                planes[x] = v;
+            }
+        }
+        __syncthreads();
+        for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
+            int64_t row, col;
+            if (!item_pos(g, c, b, i0 + x, row, col)) continue;
+            uint8_t *o = out + (row * ld + col) * ts;
+            uint64_t v = 0;
+            if (d.mode == BM_SHUFFLED) {
+                for (int j = 0; j < ts; j++) v |= (uint64_t)planes[j * TILE + x] << (8 * j);
+            } else if (d.mode == BM_PLAIN) {
+                for (int j = 0; j < ts; j++) v |= (uint64_t)planes[x * ts + j] << (8 * j);
+            } else if (d.mode == BM_NAN) {
+                v = ts == 8 ? 0x7FF8000000000000ull : 0x7FC00000ull;
+            } else {
+                v = load_item(ch + d.value_src, ts);
+            }
+            store_item(o, ts, v);
+        }
+        __syncthreads();
+    }
+}
+
+// ============================================================================ encode
+// E1: dense -> byte-plane image (shuffled: plane j holds byte j of every item;
+// plain: items back to back).  Padding items are zero, as in Caterva.
+__global__ void __launch_bounds__(256) k_gather(Geom g, const uint8_t *__restrict__ in, int64_t ld, bool shuffle,
+                                                uint8_t *__restrict__ img)
+{
+    __shared__ __align__(16) uint8_t planes[8 * TILE];
+    const int ts = g.itemsize;
+    const int64_t tpb = (g.blockn + TILE - 1) / TILE;
+    const int64_t nwork = g.nchunks * g.nblocks * tpb;
+    for (int64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int64_t t = w / tpb, i0 = (w - t * tpb) * TILE;
+        const int cnt = (int)min((int64_t)TILE, g.blockn - i0);
+        const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
+        for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
+            int64_t row, col;
+            uint64_t v = 0;
+            if (item_pos(g, c, b, i0 + x, row, col)) v = load_item(in + (row * ld + col) * ts, ts);
+            if (shuffle) {
+                for (int j = 0; j < ts; j++) planes[j * TILE + x] = (uint8_t)(v >> (8 * j));
+            } else {
+                for (int j = 0; j < ts; j++) planes[x * ts + j] = (uint8_t)(v >> (8 * j));
+            }
+        }
+        __syncthreads();
+        uint8_t *blk = img + t * g.blocksize;
+        if (shuffle) {
+            for (int j = 0; j < ts; j++) {
+                uint8_t *dst = blk + (int64_t)j * g.blockn + i0;
+                for (int x = threadIdx.x; x < cnt; x += blockDim.x) dst[x] = planes[j * TILE + x];
+            }
+        } else {
+            uint8_t *dst = blk + i0 * ts;
+            for (int x = threadIdx.x; x < cnt * ts; x += blockDim.x) dst[x] = planes[x];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- LZ4 encoder (warp)
+__device__ __forceinline__ uint32_t ld4u(const uint8_t *p)
+{
+    return (uint32_t)__ldg(p) | ((uint32_t)__ldg(p + 1) << 8) | ((uint32_t)__ldg(p + 2) << 16) |
+           ((uint32_t)__ldg(p + 3) << 24);
+}
+
+__device__ __forceinline__ uint32_t lz_hash(const uint8_t *p, bool small)
+{
+    if (small) return (ld4u(p) * 2654435761u) >> (32 - 13);
+    const uint64_t v = (uint64_t)ld4u(p) | ((uint64_t)__ldg(p + 4) << 32);
+    return (uint32_t)(((v << 24) * 889523592379ull) >> (64 - 12));
+}
+
+// Position offset of the t-th probe of a search, relative to its start: the step is
+// 1 for probes 0..64 and grows by one every 64 probes after that.
+__device__ __forceinline__ int64_t probe_offset(int64_t t)
+{
+    if (t <= 0) return 0;
+    const int64_t m = 62 + t, q = m >> 6, r = m - (q << 6);
+    return 1 + 64 * (q * (q - 1) / 2) + q * (r + 1);
+}
+
+// Warp-cooperative LZ4 block compressor in limited-output mode with capacity `cap`.
+// Returns the compressed size, or 0 when it does not fit; *need_out receives the
+// smallest capacity for which it would have fit.  All lanes must call it.
+__device__ int warp_lz4_compress(const uint8_t *__restrict__ src, int n, uint8_t *__restrict__ dst, int cap,
+                                 uint32_t *tab, int *need_out)
+{
+    const int lane = threadIdx.x & 31;
+    const bool small = n < 65536 + 12 - 1;
+    uint16_t *tab16 = reinterpret_cast<uint16_t *>(tab);
+    for (int i = lane; i < 4096; i += 32) tab[i] = 0u;
+    __syncwarp();
+    int need = 0, op = 0, anchor = 0, ip = 1, mt = 0;
+    int token_pos = 0, token_val = 0;
+    const int mfl1 = n - 12 + 1, mlimit = n - 5;
+#define TGET(h) (small ? (uint32_t)tab16[h] : tab[h])
+#define TPUT(h, v) do { if (small) tab16[h] = (uint16_t)(v); else tab[h] = (uint32_t)(v); } while (0)
+#define NEED(x) do { const int nx_ = (x); need = max(need, nx_); if (nx_ > cap) { *need_out = need; return 0; } } while (0)
+    if (n < 13) goto last_literals;
+    if (lane == 0) TPUT(lz_hash(src, small), 0);
+    __syncwarp();
+    for (;;) {
+        {   // search: 32 probes per step
+            const int p0 = ip;
+            int64_t t0 = 0;
+            bool found = false;
+            for (;;) {
+                const int64_t t = t0 + lane;
+                const int64_t p = p0 + probe_offset(t), pn = p0 + probe_offset(t + 1);
+                const bool valid = pn <= mfl1;
+                const uint32_t h = valid ? lz_hash(src + p, small) : (0x80000000u | (uint32_t)lane);
+                const uint32_t ctab = valid ? TGET(h) : 0u;
+                const unsigned peers = __match_any_sync(FULLMASK, h);
+                const unsigned lower = peers & ((1u << lane) - 1u);
+                const int srcl = lower ? 31 - __clz(lower) : lane;
+                const int pl = __shfl_sync(FULLMASK, (int)p, srcl);
+                const uint32_t cand = lower ? (uint32_t)pl : ctab;
+                const bool m = valid && (small || cand + 65535u >= (uint32_t)p) && ld4u(src + cand) == ld4u(src + p);
+                const unsigned mm = __ballot_sync(FULLMASK, m), em = __ballot_sync(FULLMASK, !valid);
+                const int W = mm ? __ffs(mm) - 1 : 32, E = em ? __ffs(em) - 1 : 32;
+                const int lastw = min(W, E - 1);
+                __syncwarp();
+                if (lane <= lastw) {
+                    const unsigned upto = (lastw >= 31) ? FULLMASK : ((2u << lastw) - 1u);
+                    const unsigned higher = peers & ~((2u << lane) - 1u) & upto;
+                    if (!higher) TPUT(h, (uint32_t)p);
+                }
+                __syncwarp();
+                if (W < E) {
+                    ip = __shfl_sync(FULLMASK, (int)p, W);
+                    mt = (int)__shfl_sync(FULLMASK, cand, W);
+                    found = true;
+                    break;
+                }
+                if (E < 32) break;
+                t0 += 32;
+            }
+            if (!found) goto last_literals;
+        }
+        for (;;) {   // extend the match backwards
+            const int k = lane + 1;
+            const bool ok = (ip - k >= anchor) && (mt - k >= 0) && __ldg(src + ip - k) == __ldg(src + mt - k);
+            const unsigned badm = __ballot_sync(FULLMASK, !ok);
+            const int ext = badm ? __ffs(badm) - 1 : 32;
+            ip -= ext;
+            mt -= ext;
+            if (ext < 32) break;
+        }
+        {   // literals
+            const int lit = ip - anchor;
+            token_pos = op;
+            op += 1;
+            NEED(op + lit + 8 + lit / 255);
+            if (lit >= 15) {
+                token_val = 15 << 4;
+                const int rem = lit - 15, nff = rem / 255;
+                for (int x = lane; x < nff; x += 32) dst[op + x] = 255;
+                if (lane == 0) dst[op + nff] = (uint8_t)(rem % 255);
+                op += nff + 1;
+            } else {
+                token_val = lit << 4;
+            }
+            for (int x = lane; x < lit; x += 32) dst[op + x] = __ldg(src + anchor + x);
+            op += lit;
+        }
+    next_match:
+        {
+            const int mo = ip - mt;
+            if (lane == 0) { dst[op] = (uint8_t)mo; dst[op + 1] = (uint8_t)(mo >> 8); }
+            op += 2;
+            int mc = 0;
+            for (int a = ip + 4, bpos = mt + 4;; a += 32, bpos += 32) {
+                const int pa = a + lane;
+                const bool eq = pa < mlimit && __ldg(src + pa) == __ldg(src + bpos + lane);
+                const unsigned ne = __ballot_sync(FULLMASK, !eq);
+                const int cnum = ne ? __ffs(ne) - 1 : 32;
+                mc += cnum;
+                if (cnum < 32) break;
+            }
+            ip += mc + 4;
+            NEED(op + 6 + (mc + 240) / 255);
+            if (mc >= 15) {
+                token_val += 15;
+                const int rem = mc - 15, nff = rem / 255;
+                for (int x = lane; x < nff; x += 32) dst[op + x] = 255;
+                if (lane == 0) dst[op + nff] = (uint8_t)(rem % 255);
+                op += nff + 1;
+            } else {
+                token_val += mc;
+            }
+            if (lane == 0) dst[token_pos] = (uint8_t)token_val;
+        }
+        anchor = ip;
+        if (ip >= mfl1) break;
+        if (lane == 0) TPUT(lz_hash(src + ip - 2, small), ip - 2);
+        __syncwarp();
+        {   // immediate re-match at ip
+            const uint32_t h = lz_hash(src + ip, small);
+            const uint32_t midx = TGET(h);
+            __syncwarp();
+            if (lane == 0) TPUT(h, ip);
+            __syncwarp();
+            if ((small || midx + 65535u >= (uint32_t)ip) && ld4u(src + midx) == ld4u(src + ip)) {
+                token_pos = op;
+                token_val = 0;
+                op += 1;
+                mt = (int)midx;
+                goto next_match;
+            }
+        }
+        ip++;
+    }
+last_literals:
+    {
+        const int last = n - anchor;
+        NEED(op + last + 1 + (last + 255 - 15) / 255);
+        if (last >= 15) {
+            const int rem = last - 15, nff = rem / 255;
+            if (lane == 0) dst[op] = 15 << 4;
+            for (int x = lane; x < nff; x += 32) dst[op + 1 + x] = 255;
+            if (lane == 0) dst[op + 1 + nff] = (uint8_t)(rem % 255);
+            op += nff + 2;
+        } else {
+            if (lane == 0) dst[op] = (uint8_t)(last << 4);
+            op += 1;
+        }
+        for (int x = lane; x < last; x += 32) dst[op + x] = __ldg(src + anchor + x);
+        op += last;
+    }
+#undef TGET
+#undef TPUT
+#undef NEED
+    __syncwarp();
+    *need_out = need;
+    return op;
+}
+
+// E2: one warp per stream: run check, then LZ4 into the stream's slot (capacity =
+// stream length; a stream that does not shrink is stored raw).
+__global__ void __launch_bounds__(128) k_lz4_encode(const uint8_t *__restrict__ img, int64_t nstreams_total,
+                                                    int neblock, uint8_t *slots, EncStream *es)
+{
+    extern __shared__ uint32_t sm_tab[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    uint32_t *tab = sm_tab + warp * 4096;
+    for (int64_t sid = (int64_t)blockIdx.x * wpb + warp; sid < nstreams_total; sid += (int64_t)gridDim.x * wpb) {
+        const uint8_t *src = img + sid * neblock;
+        const uint8_t first = __ldg(src);
+        bool run = true;
+        for (int base = 0; base < neblock && run; base += 32 * 16) {
+            bool mine = true;
+            for (int k = 0; k < 16; k++) {
+                const int x = base + k * 32 + lane;
+                if (x < neblock && __ldg(src + x) != first) mine = false;
+            }
+            run = __all_sync(FULLMASK, mine);
+        }
+        EncStream e;
+        e.out = -1;
+        if (run) {
+            e.kind = SK_RUN; e.csize = first; e.need = 0;
+        } else {
+            int need = 0;
+            const int cs = warp_lz4_compress(src, neblock, slots + sid * neblock, neblock, tab, &need);
+            if (cs > 0 && cs < neblock) { e.kind = SK_LZ4; e.csize = cs; e.need = need; }
+            else { e.kind = SK_RAW; e.csize = neblock; e.need = need; }
+        }
+        if (lane == 0) es[sid] = e;
+        __syncwarp();
+    }
+}
+
+// E3: per chunk, walk streams in order as blosc_c does, assigning offsets and deciding
+// the memcpy fallback (destination capacity nbytes + 32); then scan chunk sizes.
+__global__ void k_layout(Geom g, int nstreams, int neblock, EncStream *es, EncChunk *ec, int64_t *total)
+{
+    const int64_t destsize = g.chunk_nbytes + 32;
+    for (int64_t c = threadIdx.x; c < g.nchunks; c += blockDim.x) {
+        int64_t ntb = 32 + 4 * g.nblocks;
+        bool ok = ntb <= destsize;
+        for (int64_t b = 0; ok && b < g.nblocks; b++) {
+            for (int j = 0; j < nstreams; j++) {
+                EncStream &e = es[(c * g.nblocks + b) * nstreams + j];
+                ntb += 4;
+                if (e.kind == SK_RUN) {
+                    if (ntb > destsize) { ok = false; break; }
+                    e.out = (int32_t)(ntb - 4);
+                    if (e.csize != 0) {
+                        if (ntb + 1 > destsize) { ok = false; break; }
+                        ntb += 1;
+                    }
+                    continue;
+                }
+                int64_t maxout = neblock;
+                if (ntb + maxout > destsize) {
+                    maxout = destsize - ntb;
+                    if (maxout <= 0) { ok = false; break; }
+                }
+                int64_t sz;
+                if (e.kind == SK_LZ4 && e.need <= maxout) {
+                    sz = e.csize;
+                } else {
+                    if (ntb + neblock > destsize) { ok = false; break; }
+                    e.kind = SK_RAW;
+                    sz = neblock;
+                }
+                e.out = (int32_t)(ntb - 4);
+                ntb += sz;
+            }
+        }
+        ec[c].memcpyed = ok ? 0 : 1;
+        ec[c].cbytes = (int32_t)(ok ? ntb : destsize);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t acc = 0;
+        for (int64_t c = 0; c < g.nchunks; c++) { ec[c].offset = acc; acc += ec[c].cbytes; }
+        *total = acc;
+    }
+}
+
+// E5: write headers, bstarts, csize words and payloads.  One CTA per (chunk, block).
+__global__ void __launch_bounds__(256) k_emit(Geom g, int nstreams, int neblock, bool shuffle, int splitflag,
+                                              const uint8_t *__restrict__ img, const uint8_t *__restrict__ slots,
+                                              const EncStream *__restrict__ es, const EncChunk *__restrict__ ec,
+                                              uint8_t *__restrict__ outbuf)
+{
+    const int ts = g.itemsize;
+    for (int64_t t = blockIdx.x; t < g.nchunks * g.nblocks; t += gridDim.x) {
+        const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
+        const EncChunk cc = ec[c];
+        uint8_t *chunk = outbuf + cc.offset;
+        if (b == 0 && threadIdx.x < 32) {
+            const int flags = 0x05 | (1 << 5) | (splitflag ? 0 : 0x10) | (cc.memcpyed ? 0x02 : 0);
+            uint8_t hb = 0;
+            const int x = threadIdx.x;
+            if (x == 0) hb = 5;
+            else if (x == 1) hb = 1;
+            else if (x == 2) hb = (uint8_t)flags;
+            else if (x == 3) hb = (uint8_t)ts;
+            else if (x >= 4 && x < 8) hb = (uint8_t)(g.chunk_nbytes >> (8 * (x - 4)));
+            else if (x >= 8 && x < 12) hb = (uint8_t)(g.blocksize >> (8 * (x - 8)));
+            else if (x >= 12 && x < 16) hb = (uint8_t)((uint32_t)cc.cbytes >> (8 * (x - 12)));
+            else if (x == 21) hb = shuffle ? 1 : 0;
+            else if (x == 22) hb = 1;   // compcode LZ4
+            chunk[x] = hb;
+        }
+        const uint8_t *blk_img = img + t * g.blocksize;
+        if (cc.memcpyed) {
+            uint8_t *dst = chunk + 32 + b * g.blocksize;
+            for (int64_t x = threadIdx.x; x < g.blocksize; x += blockDim.x) {
+                uint8_t v;
+                if (shuffle) { const int64_t i = x / ts, j = x - i * ts; v = blk_img[j * g.blockn + i]; }
+                else v = blk_img[x];
+                dst[x] = v;
+            }
+            continue;
+        }
+        const EncStream *bs = es + t * nstreams;
+        if (threadIdx.x == 0) {
+            const int32_t bstart = bs[0].out;
+            uint8_t *p = chunk + 32 + 4 * b;
+            p[0] = (uint8_t)bstart; p[1] = (uint8_t)(bstart >> 8); p[2] = (uint8_t)(bstart >> 16); p[3] = (uint8_t)(bstart >> 24);
+        }
+        for (int j = 0; j < nstreams; j++) {
+            const EncStream e = bs[j];
+            uint8_t *w = chunk + e.out;
+            int32_t word;
+            const uint8_t *payload = nullptr;
+            int plen = 0;
+            if (e.kind == SK_RUN) { word = -e.csize; }
+            else if (e.kind == SK_LZ4) { word = e.csize; payload = slots + (t * nstreams + j) * (int64_t)neblock; plen = e.csize; }
+            else { word = neblock; payload = blk_img + (int64_t)j * neblock; plen = neblock; }
+            if (threadIdx.x < 4) w[threadIdx.x] = (uint8_t)((uint32_t)word >> (8 * threadIdx.x));
+            if (e.kind == SK_RUN && e.csize != 0 && threadIdx.x == 4) w[4] = 1;
+            for (int x = threadIdx.x; x < plen; x += blockDim.x) w[4 + x] = payload[x];
+        }
+    }
+}
+
+// ============================================================================ host launchers
+static int sm_count()
+{
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+constexpr int DEC_RING = 8192;
+
+int decode_container(const Geom &g, const uint8_t *d_chunks, const int64_t *d_off, const int32_t *d_len,
+                     void *out, int64_t ld, cudaStream_t st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int64_t nbl = g.nchunks * g.nblocks;
+    DevBuf bd, sd, jobs, scratch, counters;
+    if (!bd.allocate(sizeof(BlockDesc) * nbl, dev) || !sd.allocate(sizeof(StreamDesc) * nbl * 8, dev) ||
+        !jobs.allocate(sizeof(Lz4Job) * nbl * 8, dev) || !scratch.allocate((size_t)(nbl * g.blocksize), dev) ||
+        !counters.allocate(64, dev))
+        return -100;
+    int *njobs = counters.as<int>(), *err = counters.as<int>() + 1;
+    cudaMemsetAsync(counters.p, 0, 64, st);
+    const int sms = sm_count();
+    {
+        const int threads = 128;
+        const int64_t blocks = std::min<int64_t>((nbl + threads - 1) / threads, (int64_t)sms * 16);
+        IAB_LAUNCHED(1);
+        k_parse<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, st>>>(g, d_chunks, d_off, d_len, bd.as<BlockDesc>(),
+                                                                          sd.as<StreamDesc>(), jobs.as<Lz4Job>(), njobs, err);
+    }
+    {
+        static bool attr = false;
+        const int smem = 8 * DEC_RING;
+        if (!attr) {
+            cudaFuncSetAttribute(k_lz4_decode<DEC_RING>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            attr = true;
+        }
+        IAB_LAUNCHED(1);
+        k_lz4_decode<DEC_RING><<<sms * 3, 256, smem, st>>>(d_chunks, jobs.as<Lz4Job>(), njobs, scratch.as<uint8_t>(), err);
+    }
+    {
+        const int64_t tpb = (g.blockn + TILE - 1) / TILE;
+        const int64_t nwork = nbl * tpb;
+        const int64_t blocks = std::min<int64_t>(nwork, (int64_t)sms * 8);
+        IAB_LAUNCHED(1);
+        k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, d_chunks, bd.as<BlockDesc>(), sd.as<StreamDesc>(),
+                                                                        scratch.as<uint8_t>(), (uint8_t *)out, ld);
+    }
+    int h_err = 0;
+    cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return -101;
+    return h_err;
+}
+
+int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, DevBuf *d_out,
+                     std::vector<int64_t> *h_off, std::vector<int32_t> *h_len, cudaStream_t st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int ts = g.itemsize;
+    const int64_t nbl = g.nchunks * g.nblocks;
+    const int64_t img_bytes = nbl * g.blocksize;
+    // c-blosc2's split rule for LZ4 (always / never / automatic: LZ4 + shuffle,
+    // typesize <= 16 and at least 32 items per block)
+    bool split;
+    if (splitmode == 1) split = true;
+    else if (splitmode == 2) split = false;
+    else split = shuffle && ts <= 16 && (g.blocksize / ts) >= 32;
+    const int nstreams = split ? ts : 1;
+    const int neblock = (int)(g.blocksize / nstreams);
+    DevBuf img, slots, es, ec, tot;
+    if (!img.allocate(img_bytes, dev) || !slots.allocate(img_bytes, dev) ||
+        !es.allocate(sizeof(EncStream) * nbl * nstreams, dev) || !ec.allocate(sizeof(EncChunk) * g.nchunks, dev) ||
+        !tot.allocate(64, dev) || !d_out->allocate((size_t)(g.nchunks * (g.chunk_nbytes + 32)), dev))
+        return -100;
+    const int sms = sm_count();
+    {
+        const int64_t tpb = (g.blockn + TILE - 1) / TILE;
+        const int64_t blocks = std::min<int64_t>(nbl * tpb, (int64_t)sms * 8);
+        IAB_LAUNCHED(1);
+        k_gather<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, (const uint8_t *)in, ld, shuffle, img.as<uint8_t>());
+    }
+    {
+        static bool attr = false;
+        const int wpb = 4, smem = wpb * 4096 * 4;
+        if (!attr) {
+            cudaFuncSetAttribute(k_lz4_encode, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            attr = true;
+        }
+        const int64_t ns = nbl * nstreams;
+        const int64_t blocks = std::min<int64_t>((ns + wpb - 1) / wpb, (int64_t)sms * 3);
+        IAB_LAUNCHED(1);
+        k_lz4_encode<<<(unsigned)std::max<int64_t>(blocks, 1), wpb * 32, smem, st>>>(img.as<uint8_t>(), ns, neblock,
+                                                                                   slots.as<uint8_t>(), es.as<EncStream>());
+    }
+    IAB_LAUNCHED(1);
+    k_layout<<<1, 1024, 0, st>>>(g, nstreams, neblock, es.as<EncStream>(), ec.as<EncChunk>(), tot.as<int64_t>());
+    {
+        const int64_t blocks = std::min<int64_t>(nbl, (int64_t)sms * 8);
+        IAB_LAUNCHED(1);
+        k_emit<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, nstreams, neblock, shuffle, split ? 1 : 0,
+                                                                      img.as<uint8_t>(), slots.as<uint8_t>(),
+                                                                      es.as<EncStream>(), ec.as<EncChunk>(), d_out->as<uint8_t>());
+    }
+    std::vector<EncChunk> hc((size_t)g.nchunks);
+    cudaMemcpyAsync(hc.data(), ec.p, sizeof(EncChunk) * g.nchunks, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return -101;
+    h_off->resize((size_t)g.nchunks);
+    h_len->resize((size_t)g.nchunks);
+    for (int64_t c = 0; c < g.nchunks; c++) { (*h_off)[c] = hc[c].offset; (*h_len)[c] = hc[c].cbytes; }
+    return 0;
+}
+
+}  // namespace iab

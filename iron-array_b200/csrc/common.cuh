@@ -1,0 +1,151 @@
+// Shared definitions for the B200 kernels and the host runtime.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <atomic>
+#include <mutex>
+#include <map>
+#include <vector>
+
+namespace iab {
+
+// ------------------------------------------------------------------ geometry
+// A container's partition, viewed as 2-D: 1-D arrays of n items are 1 x n with
+// chunk 1 x c and block 1 x b (Caterva's 1-D layout is the same byte sequence).
+struct Geom {
+    int itemsize;
+    int ndim;
+    int64_t shape[2], chunk[2], block[2];
+    int64_t extc[2];       // extchunkshape = chunk rounded up to block
+    int64_t cgrid[2];      // chunks per dimension (extshape / chunkshape)
+    int64_t bgrid[2];      // blocks per dimension inside a chunk
+    int64_t nchunks;       // cgrid[0] * cgrid[1]
+    int64_t nblocks;       // blocks per chunk
+    int64_t blockn;        // items per block
+    int64_t blocksize;     // bytes per block
+    int64_t chunk_nbytes;  // bytes per (padded) chunk
+};
+
+static inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+static inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
+
+// Builds the geometry; returns false when the partition is invalid.
+bool make_geom(int ndim, const int64_t *shape, const int64_t *chunk, const int64_t *block,
+               int itemsize, Geom *g);
+
+// ------------------------------------------------------------------ codec descriptors
+enum StreamKind : int32_t { SK_RUN = 0, SK_RAW = 1, SK_LZ4 = 2 };
+enum BlockMode : int32_t { BM_SHUFFLED = 0, BM_PLAIN = 1, BM_NAN = 2, BM_VALUE = 3 };
+
+struct StreamDesc {   // one compressed stream of one block, found by the parse kernel
+    int32_t kind;     // StreamKind
+    int32_t len;      // csize for LZ4 / raw, byte value for runs
+    int64_t src;      // byte offset of the payload in the container's chunk buffer
+};
+
+struct BlockDesc {
+    int32_t mode;      // BlockMode
+    int32_t nstreams;  // typesize when split, else 1
+    int32_t neblock;   // bytes per stream
+    int32_t pad;
+    int64_t value_src; // BM_VALUE: offset of the repeated item
+};
+
+struct Lz4Job {       // decode job: one LZ4 stream
+    int64_t src;      // payload offset in chunk buffer
+    int64_t dst;      // offset in the scratch image
+    int32_t csize;
+    int32_t dlen;
+};
+
+struct EncStream {    // per-stream result of the LZ4 encoder
+    int32_t kind;     // SK_RUN / SK_RAW / SK_LZ4
+    int32_t csize;    // LZ4: compressed size; RUN: byte value
+    int32_t need;     // LZ4: the smallest output capacity for which limited mode succeeds
+    int32_t out;      // final offset of the stream's csize word inside its chunk (-1: none)
+};
+
+struct EncChunk {
+    int32_t cbytes;
+    int32_t memcpyed;
+    int64_t offset;   // byte offset of the chunk in the container buffer
+};
+
+// Error codes reported by kernels through a device status word (first error wins).
+enum DevErr : int32_t {
+    DE_OK = 0,
+    DE_HEADER = 1,      // chunk header does not match the container geometry
+    DE_BOUNDS = 2,      // a bstart / csize points outside the chunk
+    DE_LZ4 = 3,         // malformed LZ4 stream
+    DE_RUN_TOKEN = 4,   // negative csize without a valid run token
+};
+
+// ------------------------------------------------------------------ device memory pool
+// Caching allocator: freed blocks are kept per size class and reused, so steady-state
+// calls do no cudaMalloc.  One pool per device, shared by all contexts.
+class DevicePool {
+public:
+    static DevicePool &get(int device);
+    void *alloc(size_t bytes);
+    void release(void *p);
+    void trim();
+private:
+    std::mutex mu_;
+    std::multimap<size_t, void *> free_;
+    std::map<void *, size_t> used_;
+};
+
+struct DevBuf {   // RAII handle over a pool allocation
+    void *p = nullptr;
+    size_t n = 0;
+    int dev = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept { p = o.p; n = o.n; dev = o.dev; o.p = nullptr; o.n = 0; }
+    DevBuf &operator=(DevBuf &&o) noexcept { reset(); p = o.p; n = o.n; dev = o.dev; o.p = nullptr; o.n = 0; return *this; }
+    ~DevBuf() { reset(); }
+    bool allocate(size_t bytes, int device);
+    void reset();
+    template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+// ------------------------------------------------------------------ kernel entry points
+// Every kernel launch of the library adds to this counter (read through the C ABI).
+extern std::atomic<uint64_t> g_launches;
+#define IAB_LAUNCHED(n) (::iab::g_launches.fetch_add((n), std::memory_order_relaxed))
+
+struct CodecStats { int32_t err; };
+
+// Decode `g.nchunks` chunks (buffer d_chunks, offsets d_off) into a dense row-major
+// array `out` with leading dimension `ld` items.  Returns a DevErr (synchronises).
+int decode_container(const Geom &g, const uint8_t *d_chunks, const int64_t *d_off,
+                     const int32_t *d_len, void *out, int64_t ld, cudaStream_t st);
+
+// Encode a dense row-major array into Blosc2 chunks.  On return *d_out holds the
+// chunks back-to-back, h_off / h_len (host) their offsets and lengths.
+int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode,
+                     DevBuf *d_out, std::vector<int64_t> *h_off, std::vector<int32_t> *h_len,
+                     cudaStream_t st);
+
+// Dense products (row-major, leading dimensions in items).
+void gemm_f64_native(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda,
+                     const double *B, int64_t ldb, double *C, int64_t ldc, cudaStream_t st);
+void gemm_f32_native(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda,
+                     const float *B, int64_t ldb, float *C, int64_t ldc, cudaStream_t st);
+void gemv_native(int dtype, int64_t M, int64_t K, const void *A, int64_t lda, const void *x,
+                 void *y, cudaStream_t st);
+// Split-precision forms; return 0 on success, < 0 when unsupported on this device.
+int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda,
+                   const double *B, int64_t ldb, double *C, int64_t ldc, int nterms, cudaStream_t st);
+int gemm_f32_bf16x3(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda,
+                    const float *B, int64_t ldb, float *C, int64_t ldc, cudaStream_t st);
+
+void fill_arange(int dtype, int64_t M, int64_t N, int64_t ld, double start, double step, void *out,
+                 cudaStream_t st);
+void transpose_dense(int itemsize, int64_t rows, int64_t cols, const void *in, int64_t ldin, void *out,
+                     int64_t ldout, cudaStream_t st);
+
+}  // namespace iab

@@ -1,0 +1,194 @@
+"""GPU parity of the Blosc2 decoder/encoder (through the C ABI) against the oracle and
+the reference's golden chunks.  Bar: bit-exact."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+DIGESTS = json.load(open(os.path.join(GOLD, "golden_digests.json")))
+GOLDEN = {
+    "test_binomial_int32_n1_p0.7": np.int32,
+    "test_poisson_int32_lam3": np.int32,
+    "test_rand_float32": np.float32,
+}
+
+
+def _golden(name):
+    return open(os.path.join(GOLD, f"chunk_{name}_0.bin"), "rb").read()
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN))
+def test_gpu_decodes_golden_chunk(ctx, ia, name):
+    chunk = _golden(name)
+    c = ia.Container.from_chunks(ctx, (100000,), GOLDEN[name], (100000,), (10000,), [chunk])
+    out = c.to_numpy()
+    assert hashlib.sha256(out.tobytes()).hexdigest() == DIGESTS[name]["chunks"][0]["sha_decoded"]
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN))
+def test_gpu_reencodes_golden_chunk_byte_identical(ctx, ia, name):
+    chunk = _golden(name)
+    data = np.frombuffer(O.chunk_decompress(chunk), GOLDEN[name])
+    c = ia.Container.from_numpy(ctx, data, (100000,), (10000,))
+    mine = c.chunk(0)
+    assert mine[:32] == chunk[:32]
+    gb, mb = O.chunk_blocks(chunk), O.chunk_blocks(mine)
+    for (s, e), (s2, e2) in zip(gb, mb):
+        assert chunk[s:e] == mine[s2:e2]
+
+
+def _data(kind, shape, dtype, seed=0):
+    rng = np.random.default_rng(seed)
+    n = int(np.prod(shape))
+    if kind == "uniform":
+        a = rng.uniform(-1, 1, n)
+    elif kind == "scaled":
+        a = rng.uniform(-1, 1, n) * 2.0 ** rng.integers(-8, 9, n)
+    elif kind == "smooth":
+        i = np.arange(n)
+        a = np.sin(0.001 * (i // shape[-1])) + np.cos(0.002 * (i % shape[-1]))
+    elif kind == "zeros":
+        a = np.zeros(n)
+    elif kind == "const":
+        a = np.full(n, -2.5)
+    elif kind == "bytes":
+        return np.frombuffer(rng.bytes(n * np.dtype(dtype).itemsize), dtype).reshape(shape).copy()
+    elif kind == "sparse":
+        a = np.where(rng.random(n) < 0.02, rng.standard_normal(n), 0.0)
+    return a.astype(dtype).reshape(shape)
+
+
+GEOMS = [
+    ((300, 670), (28, 300), (11, 31)),      # ragged chunks and blocks (tests/test_linalg_gemm.c:208-218)
+    ((1000, 1000), (500, 500), (100, 100)),
+    ((257, 129), (64, 64), (64, 64)),
+    ((5000,), (1200,), (256,)),
+    ((37,), (40,), (8,)),                   # chunk larger than the array
+]
+
+
+@pytest.mark.parametrize("geom", GEOMS, ids=lambda g: "x".join(map(str, g[0])))
+@pytest.mark.parametrize("kind", ["uniform", "scaled", "smooth", "zeros", "const", "bytes", "sparse"])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_gpu_roundtrip_matches_oracle_bytes(ctx, ia, geom, kind, dtype):
+    shape, chunk, block = geom
+    a = _data(kind, shape, dtype)
+    c = ia.Container.from_numpy(ctx, a, chunk, block)
+    back = c.to_numpy()
+    assert back.tobytes() == a.tobytes()
+    g, ref_chunks = O.encode_array(a, chunk, block)
+    mine = c.chunks()
+    assert len(mine) == len(ref_chunks)
+    for m, r in zip(mine, ref_chunks):
+        assert m == r
+    # the oracle reads what the GPU wrote, and the GPU reads what the oracle wrote
+    assert O.decode_array(g, mine, dtype).tobytes() == a.tobytes()
+    c2 = ia.Container.from_chunks(ctx, shape, dtype, chunk, block, ref_chunks)
+    assert c2.to_numpy().tobytes() == a.tobytes()
+
+
+@pytest.mark.parametrize("dtype", [np.int64, np.int32, np.int16, np.uint8])
+def test_gpu_roundtrip_integer_types(ctx, ia, dtype):
+    rng = np.random.default_rng(3)
+    a = rng.integers(0, 50, (400, 300)).astype(dtype)
+    c = ia.Container.from_numpy(ctx, a, (128, 128), (32, 64))
+    assert np.array_equal(c.to_numpy(), a)
+    _, ref_chunks = O.encode_array(a, (128, 128), (32, 64))
+    assert c.chunks() == ref_chunks
+
+
+def test_gpu_never_split_chunks(ia):
+    cfg = ia.Config.defaults()
+    cfg.splitmode = ia.NEVER_SPLIT
+    ctx = ia.Context(cfg)
+    a = _data("smooth", (512, 512), np.float64)
+    c = ia.Container.from_numpy(ctx, a, (256, 256), (64, 64))
+    assert np.array_equal(c.to_numpy(), a)
+    _, ref = O.encode_array(a, (256, 256), (64, 64), splitmode=O.SPLIT_NEVER)
+    assert c.chunks() == ref
+    assert not O.chunk_header(ref[0])["split"]
+
+
+def test_gpu_decodes_special_and_memcpyed_chunks(ctx, ia):
+    shape, chunk, block = (64, 64), (64, 64), (16, 16)
+    g = O.Geom(shape, chunk, block, 8)
+
+    def special(v):
+        z = bytearray(32)
+        z[0], z[1], z[2], z[3] = 5, 1, 0x25, 8
+        z[4:8] = g.chunk_nbytes.to_bytes(4, "little")
+        z[8:12] = g.blocksize.to_bytes(4, "little")
+        z[12:16] = (32).to_bytes(4, "little")
+        z[31] = v << 4
+        return bytes(z)
+    assert not ia.Container.from_chunks(ctx, shape, np.float64, chunk, block, [special(1)]).to_numpy().any()
+    assert np.isnan(ia.Container.from_chunks(ctx, shape, np.float64, chunk, block, [special(2)]).to_numpy()).all()
+    rnd = _data("bytes", shape, np.float64)
+    memc = O.chunk_compress(g.chunk_from_array(rnd, 0).tobytes(), 8, g.blocksize)
+    assert O.chunk_header(memc)["memcpyed"]
+    out = ia.Container.from_chunks(ctx, shape, np.float64, chunk, block, [memc]).to_numpy()
+    assert out.tobytes() == rnd.tobytes()
+
+
+def test_gpu_rejects_corrupted_chunks_without_faulting(ctx, ia):
+    a = _data("smooth", (256, 256), np.float64)
+    _, (chunk,) = O.encode_array(a, (256, 256), (64, 64))
+    bad_bstart = bytearray(chunk)
+    bad_bstart[32:36] = (len(chunk) + 100).to_bytes(4, "little")        # bstart past cbytes
+    bad_csize = bytearray(chunk)
+    s, _ = O.chunk_blocks(chunk)[1]
+    bad_csize[s:s + 4] = (10 ** 7).to_bytes(4, "little")                 # stream past the chunk
+    bad_lz4 = bytearray(chunk)
+    for blk in O.chunk_blocks(chunk):
+        p = blk[0]
+        cs = int.from_bytes(chunk[p:p + 4], "little", signed=True)
+        if 0 < cs < 64 * 64:                                             # an LZ4 stream: break its offsets
+            bad_lz4[p + 4:p + 4 + cs] = bytes([0x0f]) + bytes(cs - 1)
+            break
+    for bad in (bad_bstart, bad_csize, bad_lz4):
+        c = ia.Container.from_chunks(ctx, (256, 256), np.float64, (256, 256), (64, 64), [bytes(bad)])
+        with pytest.raises(ia.IArrayError) as e:
+            c.to_numpy()
+        assert e.value.name == "BLOSC_FAILED"
+    # the context still works afterwards
+    ok = ia.Container.from_chunks(ctx, (256, 256), np.float64, (256, 256), (64, 64), [chunk])
+    assert np.array_equal(ok.to_numpy(), a)
+
+
+def test_gpu_frames_roundtrip(ctx, ia, tmp_path):
+    a = _data("scaled", (300, 200), np.float64)
+    c = ia.Container.from_numpy(ctx, a, (128, 64), (32, 32))
+    frame = c.to_cframe()
+    fr = O.read_frame(frame)
+    assert fr["chunks"] == c.chunks()
+    ndim, shape, chunk, block = O.parse_caterva_meta(fr["metalayers"]["caterva"])
+    assert (ndim, shape, chunk, block) == (2, [300, 200], [128, 64], [32, 32])
+    assert fr["metalayers"]["iarray"] == bytes([0x93, 0, 0, 0])
+    assert fr["typesize"] == 8 and fr["blocksize"] == 32 * 32 * 8 and fr["chunksize"] == 128 * 64 * 8
+    # header layout matches the reference's frames (same field encodings and flags)
+    gold = bytes.fromhex(DIGESTS["test_rand_float32"]["header_hex"])
+    assert frame[:10] == gold[:10] and frame[24:29] == gold[24:29]
+    assert frame[-35:-16] == bytes.fromhex(DIGESTS["test_rand_float32"]["trailer_hex"])[:19]
+    c2 = ia.Container.from_cframe(ctx, frame)
+    assert np.array_equal(c2.to_numpy(), a)
+    p = str(tmp_path / "a.iarray")
+    c.save(p)
+    assert open(p, "rb").read() == frame
+    assert np.array_equal(ia.Container.open(ctx, p).to_numpy(), a)
+    assert np.array_equal(ia.Container.open(ctx, p, load=True).to_numpy(), a)
+
+
+def test_gpu_container_info_and_empty(ctx, ia):
+    a = _data("smooth", (1000, 1000), np.float64)
+    c = ia.Container.from_numpy(ctx, a, (500, 500), (100, 100))
+    nb, cb = c.info()
+    assert nb == 1000 * 1000 * 8 and cb == sum(len(x) for x in c.chunks())
+    e = ia.Container.empty(ctx, (130, 70), np.float32, (64, 64), (16, 16))
+    assert not e.to_numpy().any()
