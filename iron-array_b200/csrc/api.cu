@@ -170,6 +170,8 @@ struct iarray_context_s {
     int split_terms = 0;
     double timings[5] = {0, 0, 0, 0, 0};
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t stream2 = nullptr;          // second stream for concurrent operand decode
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 struct iarray_container_s {
@@ -261,6 +263,9 @@ INA_API(ina_rc_t) iarray_context_new(iarray_config_t *cfg, iarray_context_t **ct
         return rc_err(IARRAY_ERR_GPU_FAILED);
     }
     for (auto &e : c->ev) cudaEventCreate(&e);
+    cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming);
     *ctx = c;
     return INA_SUCCESS;
 }
@@ -270,6 +275,9 @@ INA_API(void) iarray_context_free(iarray_context_t **ctx)
     if (!ctx || !*ctx) return;
     iarray_context_t *c = *ctx;
     if (c->stream) { cudaStreamSynchronize(c->stream); cudaStreamDestroy(c->stream); }
+    if (c->stream2) { cudaStreamSynchronize(c->stream2); cudaStreamDestroy(c->stream2); }
+    if (c->fork) cudaEventDestroy(c->fork);
+    if (c->join) cudaEventDestroy(c->join);
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
     delete c;
     *ctx = nullptr;
@@ -439,6 +447,39 @@ static ina_rc_t decode_store(iarray_context_t *ctx, const iarray_container_t *c,
     if (r < 0) return rc_err(IARRAY_ERR_GPU_FAILED);
     if (r > 0) return rc_err(IARRAY_ERR_BLOSC_FAILED);
     return INA_SUCCESS;
+}
+
+static ina_rc_t decode_rc(int r)
+{
+    if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    if (r < 0) return rc_err(IARRAY_ERR_GPU_FAILED);
+    if (r > 0) return rc_err(IARRAY_ERR_BLOSC_FAILED);
+    return INA_SUCCESS;
+}
+
+// Decode two stored (non-view) containers concurrently: the first on the context's
+// stream, the second on its second stream; returns after both finished.
+static ina_rc_t decode_pair(iarray_context_t *ctx, const iarray_container_t *a, void *da, int64_t lda,
+                            const iarray_container_t *b, void *db, int64_t ldb)
+{
+    const Geom &ga = a->geom, &gb = b->geom;
+    if (lda != ga.shape[1]) cudaMemsetAsync(da, 0, (size_t)(ga.shape[0] * lda * ga.itemsize), ctx->stream);
+    if (ldb != gb.shape[1]) cudaMemsetAsync(db, 0, (size_t)(gb.shape[0] * ldb * gb.itemsize), ctx->stream);
+    cudaEventRecord(ctx->fork, ctx->stream);
+    cudaStreamWaitEvent(ctx->stream2, ctx->fork, 0);
+    iab::DecodeWork wa, wb;
+    int ra = 0, rb = 0;
+    if (ga.nchunks) ra = iab::decode_launch(ga, a->store->buf.as<uint8_t>(), a->store->d_off.as<int64_t>(),
+                                            a->store->d_len.as<int32_t>(), da, lda, ctx->stream, &wa);
+    if (gb.nchunks) rb = iab::decode_launch(gb, b->store->buf.as<uint8_t>(), b->store->d_off.as<int64_t>(),
+                                            b->store->d_len.as<int32_t>(), db, ldb, ctx->stream2, &wb);
+    cudaEventRecord(ctx->join, ctx->stream2);
+    cudaStreamWaitEvent(ctx->stream, ctx->join, 0);
+    if (ga.nchunks && !ra) ra = iab::decode_finish(&wa, ctx->stream);
+    if (gb.nchunks && !rb) rb = iab::decode_finish(&wb, ctx->stream2);
+    cudaStreamSynchronize(ctx->stream);
+    ina_rc_t rc = decode_rc(ra);
+    return INA_FAILED(rc) ? rc : decode_rc(rb);
 }
 
 static int64_t rows_of(const iarray_dtshape_t &d) { return d.ndim == 2 ? d.shape[0] : 1; }
@@ -899,13 +940,22 @@ static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_
         !dB.allocate((size_t)std::max<int64_t>((vec ? pad_ld(K) : K * ldb) * isz, 16), ctx->device) ||
         !dC.allocate((size_t)std::max<int64_t>((vec ? pad_ld(M) : M * ldc) * isz, 16), ctx->device))
         return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
-    ina_rc_t rc = decode_logical(ctx, a, dA.p, lda);
-    if (INA_FAILED(rc)) return rc;
-    tm.mark(1);
     if (vec) cudaMemsetAsync(dB.p, 0, (size_t)(pad_ld(K) * isz), ctx->stream);
-    rc = decode_logical(ctx, b, dB.p, vec ? K : ldb);
-    if (INA_FAILED(rc)) return rc;
-    tm.mark(2);
+    ina_rc_t rc;
+    if (!a->transposed && !b->transposed) {
+        // both operands at once: A on the context stream, B on the second stream
+        rc = decode_pair(ctx, a, dA.p, lda, b, dB.p, vec ? K : ldb);
+        if (INA_FAILED(rc)) return rc;
+        tm.mark(1);
+        tm.mark(2);
+    } else {
+        rc = decode_logical(ctx, a, dA.p, lda);
+        if (INA_FAILED(rc)) return rc;
+        tm.mark(1);
+        rc = decode_logical(ctx, b, dB.p, vec ? K : ldb);
+        if (INA_FAILED(rc)) return rc;
+        tm.mark(2);
+    }
     if (K == 0) {
         cudaMemsetAsync(dC.p, 0, (size_t)((vec ? M : M * ldc) * isz), ctx->stream);
     } else if (vec) {

@@ -533,13 +533,21 @@ last_literals:
 
 // E2: one warp per stream: run check, then LZ4 into the stream's slot (capacity =
 // stream length; a stream that does not shrink is stored raw).
+// Streams are handed out dynamically (one atomic per stream): compressible streams cost
+// far more than incompressible ones, and in shuffled float data they recur at a fixed
+// stride, which a static round-robin assignment would pile onto the same warps.
 __global__ void __launch_bounds__(128) k_lz4_encode(const uint8_t *__restrict__ img, int64_t nstreams_total,
-                                                    int neblock, uint8_t *slots, EncStream *es)
+                                                    int neblock, uint8_t *slots, EncStream *es,
+                                                    unsigned long long *next)
 {
     extern __shared__ uint32_t sm_tab[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t *tab = sm_tab + warp * 4096;
-    for (int64_t sid = (int64_t)blockIdx.x * wpb + warp; sid < nstreams_total; sid += (int64_t)gridDim.x * wpb) {
+    for (;;) {
+        unsigned long long got = 0;
+        if (lane == 0) got = atomicAdd(next, 1ull);
+        const int64_t sid = (int64_t)__shfl_sync(FULLMASK, got, 0);
+        if (sid >= nstreams_total) break;
         const uint8_t *src = img + sid * neblock;
         const uint8_t first = __ldg(src);
         bool run = true;
@@ -692,10 +700,27 @@ constexpr int DEC_RING = 8192;
 int decode_container(const Geom &g, const uint8_t *d_chunks, const int64_t *d_off, const int32_t *d_len,
                      void *out, int64_t ld, cudaStream_t st)
 {
+    DecodeWork w;
+    int r = decode_launch(g, d_chunks, d_off, d_len, out, ld, st, &w);
+    if (r) return r;
+    return decode_finish(&w, st);
+}
+
+int decode_finish(DecodeWork *w, cudaStream_t st)
+{
+    int h_err = 0;
+    cudaMemcpyAsync(&h_err, w->counters.as<int>() + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return -101;
+    return h_err;
+}
+
+int decode_launch(const Geom &g, const uint8_t *d_chunks, const int64_t *d_off, const int32_t *d_len, void *out,
+                  int64_t ld, cudaStream_t st, DecodeWork *w)
+{
     int dev = 0;
     cudaGetDevice(&dev);
     const int64_t nbl = g.nchunks * g.nblocks;
-    DevBuf bd, sd, jobs, scratch, counters;
+    DevBuf &bd = w->bd, &sd = w->sd, &jobs = w->jobs, &scratch = w->scratch, &counters = w->counters;
     if (!bd.allocate(sizeof(BlockDesc) * nbl, dev) || !sd.allocate(sizeof(StreamDesc) * nbl * 8, dev) ||
         !jobs.allocate(sizeof(Lz4Job) * nbl * 8, dev) || !scratch.allocate((size_t)(nbl * g.blocksize), dev) ||
         !counters.allocate(64, dev))
@@ -728,10 +753,7 @@ int decode_container(const Geom &g, const uint8_t *d_chunks, const int64_t *d_of
         k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, d_chunks, bd.as<BlockDesc>(), sd.as<StreamDesc>(),
                                                                         scratch.as<uint8_t>(), (uint8_t *)out, ld);
     }
-    int h_err = 0;
-    cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (cudaStreamSynchronize(st) != cudaSuccess) return -101;
-    return h_err;
+    return 0;
 }
 
 int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, DevBuf *d_out,
@@ -755,6 +777,7 @@ int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, in
         !es.allocate(sizeof(EncStream) * nbl * nstreams, dev) || !ec.allocate(sizeof(EncChunk) * g.nchunks, dev) ||
         !tot.allocate(64, dev) || !d_out->allocate((size_t)(g.nchunks * (g.chunk_nbytes + 32)), dev))
         return -100;
+    cudaMemsetAsync(tot.p, 0, 64, st);
     const int sms = sm_count();
     {
         const int64_t tpb = (g.blockn + TILE - 1) / TILE;
@@ -772,8 +795,9 @@ int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, in
         const int64_t ns = nbl * nstreams;
         const int64_t blocks = std::min<int64_t>((ns + wpb - 1) / wpb, (int64_t)sms * 3);
         IAB_LAUNCHED(1);
-        k_lz4_encode<<<(unsigned)std::max<int64_t>(blocks, 1), wpb * 32, smem, st>>>(img.as<uint8_t>(), ns, neblock,
-                                                                                   slots.as<uint8_t>(), es.as<EncStream>());
+        k_lz4_encode<<<(unsigned)std::max<int64_t>(blocks, 1), wpb * 32, smem, st>>>(
+            img.as<uint8_t>(), ns, neblock, slots.as<uint8_t>(), es.as<EncStream>(),
+            reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1));
     }
     IAB_LAUNCHED(1);
     k_layout<<<1, 1024, 0, st>>>(g, nstreams, neblock, es.as<EncStream>(), ec.as<EncChunk>(), tot.as<int64_t>());

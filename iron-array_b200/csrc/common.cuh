@@ -124,6 +124,15 @@ struct CodecStats { int32_t err; };
 int decode_container(const Geom &g, const uint8_t *d_chunks, const int64_t *d_off,
                      const int32_t *d_len, void *out, int64_t ld, cudaStream_t st);
 
+// Asynchronous form: decode_launch enqueues the kernels on `st` (work buffers held in
+// *w until decode_finish, which synchronises `st` and returns the DevErr).
+struct DecodeWork {
+    DevBuf bd, sd, jobs, scratch, counters;
+};
+int decode_launch(const Geom &g, const uint8_t *d_chunks, const int64_t *d_off, const int32_t *d_len,
+                  void *out, int64_t ld, cudaStream_t st, DecodeWork *w);
+int decode_finish(DecodeWork *w, cudaStream_t st);
+
 // Encode a dense row-major array into Blosc2 chunks.  On return *d_out holds the
 // chunks back-to-back, h_off / h_len (host) their offsets and lengths.
 int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode,

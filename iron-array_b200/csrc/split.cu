@@ -1,12 +1,572 @@
-// Split-precision forms (filled in by the Ozaki INT8 and 3xBF16 kernels).
+// Split-precision float64 product on the INT8 tensor cores (Ozaki scheme II, the
+// Chinese-remainder form), for the block-pair GEMM of ironArray's matmul path
+// (src/linalg/iarray_gemm.c:276-290 computes the same product with cblas_dgemm).
+//
+//   1. Scaling.  Row i of A is scaled by 2^sA_i and rounded to an integer matrix A'
+//      (|A'_ik| < 2^52), column j of B by 2^sB_j -> B'.  The shifts are chosen from the
+//      row / column 2-norms so that ||A'_i||_2 * ||B'_j||_2 < P / 2, where P is the
+//      product of the moduli; by Cauchy-Schwarz every entry of C' = A' B' then lies in
+//      (-P/2, P/2) and is recovered exactly from its residues.
+//   2. Residues.  For each modulus m_l (pairwise coprime, <= 256) the symmetric residues
+//      A'_l = A' mod m_l and B'_l = B' mod m_l fit in int8 (B'_l is stored transposed,
+//      K-major, for the tensor-core operand layout).
+//   3. INT8 GEMM per modulus on tcgen05 (kind::i8, INT32 accumulate in TMEM, exact since
+//      K * 128 * 128 < 2^31), fused epilogue reducing every entry modulo m_l to a byte.
+//   4. Reconstruction.  C'_ij = sum_l r_l w_l mod P (w_l the CRT basis, 128-bit integer
+//      arithmetic), centred, converted to float64 and scaled back by 2^-(sA_i + sB_j).
+// FP64 is used only for the scaling, the residue arithmetic and the final conversion.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
 #include "common.cuh"
+#include "tc_common.cuh"
 
 namespace iab {
 
-int gemm_f64_ozaki(int64_t, int64_t, int64_t, const double *, int64_t, const double *, int64_t, double *, int64_t, int,
-                   cudaStream_t)
+// ============================================================================ tensor maps
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn()
 {
-    return -1;
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    });
+    return fn;
+}
+
+bool make_tmap_3d(CUtensorMap *map, CUtensorMapDataType dt, const void *base, uint64_t d0, uint64_t d1, uint64_t d2,
+                  uint64_t stride1, uint64_t stride2, uint32_t box0, uint32_t box1, CUtensorMapSwizzle sw)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[3] = {d0, d1, d2};
+    const cuuint64_t strides[2] = {stride1, stride2};
+    const cuuint32_t box[3] = {box0, box1, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return fn(map, dt, 3, const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// ============================================================================ moduli + CRT basis
+constexpr int MAX_MODULI = 20;
+static const int kModuli[MAX_MODULI] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
+                                        223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
+
+struct CrtConst {
+    int L;
+    int mod[MAX_MODULI];
+    double inv_mod[MAX_MODULI];
+    float inv_modf[MAX_MODULI];
+    uint64_t w_lo[MAX_MODULI], w_hi[MAX_MODULI];   // CRT basis w_l = (P/m_l) * ((P/m_l)^-1 mod m_l) mod P
+    uint64_t p_lo, p_hi, h_lo, h_hi;               // P and floor(P/2)
+    double inv_p;                                  // 1/P (rounded)
+    double log2p;
+};
+
+__constant__ CrtConst c_crt;
+
+static bool build_crt(int L, CrtConst *c)
+{
+    if (L < 2 || L > 16) return false;   // P < 2^126 keeps the reconstruction in two limbs + sign
+    typedef unsigned __int128 u128;
+    u128 P = 1;
+    for (int l = 0; l < L; l++) P *= (u128)kModuli[l];
+    memset(c, 0, sizeof(*c));
+    c->L = L;
+    double lp = 0;
+    for (int l = 0; l < L; l++) {
+        const int m = kModuli[l];
+        c->mod[l] = m;
+        c->inv_mod[l] = 1.0 / m;
+        c->inv_modf[l] = 1.0f / (float)m;
+        lp += log2((double)m);
+        const u128 Ml = P / (u128)m;
+        const int a = (int)(Ml % (u128)m);
+        int inv = 0;
+        for (int x = 1; x < m; x++)
+            if ((a * x) % m == 1) { inv = x; break; }
+        if (!inv) return false;
+        const u128 w = (Ml * (u128)inv) % P;
+        c->w_lo[l] = (uint64_t)w;
+        c->w_hi[l] = (uint64_t)(w >> 64);
+    }
+    c->p_lo = (uint64_t)P;
+    c->p_hi = (uint64_t)(P >> 64);
+    const u128 H = P / 2;
+    c->h_lo = (uint64_t)H;
+    c->h_hi = (uint64_t)(H >> 64);
+    c->inv_p = 1.0 / ((double)c->p_hi * 18446744073709551616.0 + (double)c->p_lo);
+    c->log2p = lp;
+    return true;
+}
+
+// ============================================================================ scaling
+// Shift for one row / column: the largest s with max|x| * 2^s < 2^52 and
+// ||x||_2 * 2^s <= 2^(gamma - 1).
+__device__ __forceinline__ int pick_shift(double amax, double sumsq, double gamma)
+{
+    if (!(amax > 0.0)) return 0;
+    int e;
+    frexp(amax, &e);                      // amax < 2^e
+    const int s1 = 52 - e;
+    const double nrm = sqrt(sumsq);
+    const int s2 = (int)floor(gamma - log2(nrm)) - 1;
+    return min(s1, s2);
+}
+
+__global__ void __launch_bounds__(256) k_row_shift(int M, int K, const double *__restrict__ A, int64_t lda, double gamma,
+                                                   int *__restrict__ shift)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= M) return;
+    const double *row = A + (int64_t)warp * lda;
+    double mx = 0.0, ss = 0.0;
+    for (int k = lane; k < K; k += 32) {
+        const double v = fabs(row[k]);
+        mx = fmax(mx, v);
+        ss = fma(v, v, ss);
+    }
+    for (int o = 16; o; o >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    }
+    if (lane == 0) shift[warp] = pick_shift(mx, ss, gamma);
+}
+
+constexpr int COL_SEGS = 64;
+
+__global__ void __launch_bounds__(256) k_col_partial(int K, int N, const double *__restrict__ B, int64_t ldb,
+                                                     double *__restrict__ pmax, double *__restrict__ pss)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x, seg = blockIdx.y;
+    if (j >= N) return;
+    const int per = (K + COL_SEGS - 1) / COL_SEGS, k0 = seg * per, k1 = min(K, k0 + per);
+    double mx = 0.0, ss = 0.0;
+    for (int k = k0; k < k1; k++) {
+        const double v = fabs(B[(int64_t)k * ldb + j]);
+        mx = fmax(mx, v);
+        ss = fma(v, v, ss);
+    }
+    pmax[(int64_t)seg * N + j] = mx;
+    pss[(int64_t)seg * N + j] = ss;
+}
+
+__global__ void k_col_shift(int N, const double *__restrict__ pmax, const double *__restrict__ pss, double gamma,
+                            int *__restrict__ shift)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N) return;
+    double mx = 0.0, ss = 0.0;
+    for (int s = 0; s < COL_SEGS; s++) {
+        mx = fmax(mx, pmax[(int64_t)s * N + j]);
+        ss += pss[(int64_t)s * N + j];
+    }
+    shift[j] = pick_shift(mx, ss, gamma);
+}
+
+// ============================================================================ residues
+__device__ __forceinline__ int sym_residue(double x, int l)
+{
+    const int m = c_crt.mod[l];
+    const double q = rint(x * c_crt.inv_mod[l]);
+    int r = (int)fma(-q, (double)m, x);            // exact: small integer
+    const int hi = (m == 256) ? 127 : (m - 1) / 2;
+    const int lo = (m == 256) ? -128 : -(m - 1) / 2;
+    if (r > hi) r -= m;
+    if (r < lo) r += m;
+    return r;
+}
+
+// A (M x K, row-major) -> res[l][i][k] (int8, row pitch Kp), 8 consecutive k per thread.
+__global__ void __launch_bounds__(256) k_residues_rows(int M, int K, int Kp, const double *__restrict__ A, int64_t lda,
+                                                       const int *__restrict__ shift, int8_t *__restrict__ res)
+{
+    const int groups = Kp / 8;
+    const int64_t total = (int64_t)M * groups;
+    const int L = c_crt.L;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(t / groups), k0 = (int)(t - (int64_t)i * groups) * 8;
+        const int s = shift[i];
+        double x[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int k = k0 + u;
+            x[u] = k < K ? rint(ldexp(A[(int64_t)i * lda + k], s)) : 0.0;
+        }
+        for (int l = 0; l < L; l++) {
+            uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+            for (int u = 0; u < 4; u++) w0 |= (uint32_t)(uint8_t)sym_residue(x[u], l) << (8 * u);
+#pragma unroll
+            for (int u = 0; u < 4; u++) w1 |= (uint32_t)(uint8_t)sym_residue(x[4 + u], l) << (8 * u);
+            *reinterpret_cast<uint2 *>(res + ((int64_t)l * M + i) * Kp + k0) = make_uint2(w0, w1);
+        }
+    }
+}
+
+// B (K x N, row-major) -> res[l][j][k] (int8, transposed, row pitch Kp), via 64x64 tiles.
+__global__ void __launch_bounds__(256) k_residues_cols(int K, int N, int Kp, const double *__restrict__ B, int64_t ldb,
+                                                       const int *__restrict__ shift, int8_t *__restrict__ res)
+{
+    __shared__ double tile[64][65];
+    const int k0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
+    for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+        const int r = e >> 6, c = e & 63;
+        const int k = k0 + r, j = j0 + c;
+        tile[r][c] = (k < K && j < N) ? B[(int64_t)k * ldb + j] : 0.0;
+    }
+    __syncthreads();
+    const int L = c_crt.L;
+    for (int e = threadIdx.x; e < 64 * 8; e += blockDim.x) {
+        const int c = e >> 3, kg = (e & 7) * 8;
+        const int j = j0 + c;
+        if (j >= N || k0 + kg >= Kp) continue;
+        const int s = shift[j];
+        double x[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) x[u] = rint(ldexp(tile[kg + u][c], s));
+        for (int l = 0; l < L; l++) {
+            uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+            for (int u = 0; u < 4; u++) w0 |= (uint32_t)(uint8_t)sym_residue(x[u], l) << (8 * u);
+#pragma unroll
+            for (int u = 0; u < 4; u++) w1 |= (uint32_t)(uint8_t)sym_residue(x[4 + u], l) << (8 * u);
+            *reinterpret_cast<uint2 *>(res + ((int64_t)l * N + j) * Kp + k0 + kg) = make_uint2(w0, w1);
+        }
+    }
+}
+
+// ============================================================================ INT8 tcgen05 GEMM
+namespace oz {
+constexpr int BM = 128, BN = 256, BK = 128, STAGES = 4;
+constexpr int A_BYTES = BM * BK, B_BYTES = BN * BK, STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int THREADS = 192;
+constexpr int SMEM = 1024 + STAGES * STAGE_BYTES + 256;
+constexpr uint32_t IDESC = tc::make_idesc(2 /*S32*/, 1 /*s8*/, 1 /*s8*/, BM, BN);
+}
+
+struct I8Params {
+    int M, N, Kp, L, tiles_m, tiles_n;
+    uint8_t *R;        // [L][M][ldr] residues of the products
+    int64_t ldr;
+    int *err;
+};
+
+// Persistent, warp-specialised: warp 0 issues TMA loads, warp 1 issues tcgen05.mma into
+// one of two TMEM accumulators (128 x 256 int32 each), warps 2-5 drain the other
+// accumulator: r = C mod m_l in [0, m_l), stored as one byte per entry.
+__global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_constant__ CUtensorMap tmA,
+                                                                const __grid_constant__ CUtensorMap tmB, I8Params p)
+{
+    using namespace oz;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t *sA = smem, *sB = smem + STAGES * A_BYTES;
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+    uint64_t *tfull = empty + STAGES;
+    uint64_t *tempty = tfull + 2;
+    uint64_t *drain = tempty + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) { tc::mbar_init(&full[s], 1); tc::mbar_init(&empty[s], 1); }
+        for (int b = 0; b < 2; b++) { tc::mbar_init(&tfull[b], 1); tc::mbar_init(&tempty[b], 4); }
+        tc::mbar_init(drain, 1);
+        tc::fence_barrier_init();
+        tc::tma_prefetch_desc(&tmA);
+        tc::tma_prefetch_desc(&tmB);
+    }
+    if (warp == 1) {
+        tc::tmem_alloc(tmem_slot, 512);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const int total = p.L * p.tiles_m * p.tiles_n;
+    const int ktiles = p.Kp / BK;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int64_t issued = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+                const int l = t / (p.tiles_m * p.tiles_n), rem = t - l * p.tiles_m * p.tiles_n;
+                const int tm = rem / p.tiles_n, tn = rem - tm * p.tiles_n;
+                for (int kt = 0; kt < ktiles; kt++) {
+                    if (!tc::mbar_wait(&empty[stage], phase ^ 1, p.err)) { ok = false; break; }
+                    tc::mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
+                    tc::tma_load_3d(sA + stage * A_BYTES, &tmA, kt * BK, tm * BM, l, &full[stage]);
+                    tc::tma_load_3d(sB + stage * B_BYTES, &tmB, kt * BK, tn * BN, l, &full[stage]);
+                    issued++;
+                    if (++stage == STAGES) { stage = 0; phase ^= 1; }
+                }
+            }
+            // every load issued has landed before the CTA may exit (bounded waits on the
+            // full barriers of the last STAGES loads)
+            for (int64_t it = issued > STAGES ? issued - STAGES : 0; it < issued; it++)
+                tc::mbar_wait(&full[it % STAGES], (uint32_t)((it / STAGES) & 1), p.err, 1u << 20);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int stage = 0, acc = 0;
+            uint32_t phase = 0, acc_phase = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+                if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, p.err)) { ok = false; break; }
+                tc::tc_fence_after();
+                const uint32_t dt = tmem_base + (uint32_t)(acc * BN);
+                for (int kt = 0; kt < ktiles; kt++) {
+                    if (!tc::mbar_wait(&full[stage], phase, p.err)) { ok = false; break; }
+                    tc::tc_fence_after();
+                    const uint32_t a0 = tc::smem_addr(sA + stage * A_BYTES), b0 = tc::smem_addr(sB + stage * B_BYTES);
+#pragma unroll
+                    for (int kk = 0; kk < BK / 32; kk++) {
+                        tc::mma_i8(dt, tc::sw128_kmajor_desc(a0 + kk * 32), tc::sw128_kmajor_desc(b0 + kk * 32), IDESC,
+                                   (kt | kk) != 0);
+                    }
+                    tc::tc_commit(&empty[stage]);
+                    if (++stage == STAGES) { stage = 0; phase ^= 1; }
+                }
+                if (!ok) break;
+                tc::tc_commit(&tfull[acc]);
+                if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+            }
+            // all issued MMAs complete before TMEM is released
+            tc::tc_commit(drain);
+            tc::mbar_wait(drain, 0, p.err, 1u << 20);
+        }
+    } else {
+        const int q = warp & 3;   // TMEM lane quarter this warp may access
+        int acc = 0;
+        uint32_t acc_phase = 0;
+        for (int t = blockIdx.x; t < total; t += gridDim.x) {
+            const int l = t / (p.tiles_m * p.tiles_n), rem = t - l * p.tiles_m * p.tiles_n;
+            const int tm = rem / p.tiles_n, tn = rem - tm * p.tiles_n;
+            if (!tc::mbar_wait(&tfull[acc], acc_phase, p.err)) break;
+            tc::tc_fence_after();
+            const int m = c_crt.mod[l];
+            const float invm = c_crt.inv_modf[l];
+            const int row = tm * BM + q * 32 + lane;
+            uint8_t *out = p.R + ((int64_t)l * p.M + row) * p.ldr + (int64_t)tn * BN;
+            for (int c = 0; c < BN; c += 32) {
+                uint32_t v[32];
+                tc::tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + c), v);
+                uint32_t w[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    uint32_t packed = 0;
+#pragma unroll
+                    for (int b = 0; b < 4; b++) {
+                        const int x = (int)v[u * 4 + b];
+                        const int qq = __float2int_rn((float)x * invm);
+                        int r = x - qq * m;
+                        r += (r < 0) ? m : 0;
+                        r -= (r >= m) ? m : 0;
+                        packed |= (uint32_t)r << (8 * b);
+                    }
+                    w[u] = packed;
+                }
+                const int col = tn * BN + c;
+                if (row < p.M) {
+                    if (col + 32 <= p.N) {
+                        uint4 *o4 = reinterpret_cast<uint4 *>(out + c);
+                        o4[0] = make_uint4(w[0], w[1], w[2], w[3]);
+                        o4[1] = make_uint4(w[4], w[5], w[6], w[7]);
+                    } else {
+                        for (int b = 0; b < 32 && col + b < p.N; b++) out[c + b] = (uint8_t)(w[b >> 2] >> (8 * (b & 3)));
+                    }
+                }
+            }
+            tc::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&tempty[acc]);
+            if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    if (warp == 1) tc::tmem_dealloc(tmem_base, 512);
+}
+
+// ============================================================================ reconstruction
+// C_ij = 2^-(sA_i + sB_j) * centred( sum_l r_l w_l mod P ).
+__global__ void __launch_bounds__(256) k_crt(int M, int N, const uint8_t *__restrict__ R, int64_t ldr,
+                                             const int *__restrict__ sA, const int *__restrict__ sB,
+                                             double *__restrict__ C, int64_t ldc)
+{
+    const int L = c_crt.L;
+    const int64_t plane = (int64_t)M * ldr;
+    const int64_t total = (int64_t)M * N;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e / N), j = (int)(e - (int64_t)i * N);
+        const uint8_t *rp = R + (int64_t)i * ldr + j;
+        // S = sum_l r_l w_l < L * 256 * P needs up to 2^134: three 64-bit limbs
+        uint64_t s0 = 0, s1 = 0, s2 = 0;
+        for (int l = 0; l < L; l++) {
+            const uint64_t r = rp[l * plane];
+            const uint64_t t0 = r * c_crt.w_lo[l], c0 = __umul64hi(r, c_crt.w_lo[l]);
+            const uint64_t t1 = r * c_crt.w_hi[l], c1 = __umul64hi(r, c_crt.w_hi[l]);
+            s0 += t0;
+            const uint64_t k0 = s0 < t0 ? 1 : 0;
+            const uint64_t u1 = t1 + c0;                    // no overflow: t1 < 2^64 - 2^8, c0 < 2^8
+            const uint64_t k1a = u1 < t1 ? 1 : 0;
+            s1 += u1;
+            const uint64_t k1 = (s1 < u1 ? 1 : 0) + k1a;
+            s1 += k0;
+            const uint64_t k2 = (s1 < k0 ? 1 : 0);
+            s2 += c1 + k1 + k2;
+        }
+        // reduce modulo P: quotient estimate from the leading bits, then one correction
+        const double sd = ((double)s2 * 18446744073709551616.0 + (double)s1) * 18446744073709551616.0 + (double)s0;
+        const uint64_t qe = (uint64_t)(sd * c_crt.inv_p);
+        // q * P as three limbs
+        const uint64_t q0 = qe * c_crt.p_lo, q0h = __umul64hi(qe, c_crt.p_lo);
+        const uint64_t q1l = qe * c_crt.p_hi, q1h = __umul64hi(qe, c_crt.p_hi);
+        const uint64_t q1 = q1l + q0h;
+        const uint64_t q2 = q1h + (q1 < q1l ? 1 : 0);
+        uint64_t xlo = s0 - q0;
+        const uint64_t b0 = s0 < q0 ? 1 : 0;
+        const uint64_t m1 = s1 - q1;
+        const uint64_t b1 = (s1 < q1 ? 1 : 0) + (m1 < b0 ? 1 : 0);
+        // X = S - qP lies in [-P, 2P) with P < 2^126, so the two low limbs hold it in two's
+        // complement (the third limb is its sign extension)
+        uint64_t xhi = m1 - b0;
+        (void)s2; (void)q2; (void)b1;
+        if ((int64_t)xhi < 0) {                                  // estimate one too large
+            const uint64_t t = xlo + c_crt.p_lo;
+            xhi += c_crt.p_hi + (t < xlo ? 1 : 0);
+            xlo = t;
+        } else if (xhi > c_crt.p_hi || (xhi == c_crt.p_hi && xlo >= c_crt.p_lo)) {   // one too small
+            const uint64_t t = xlo - c_crt.p_lo;
+            xhi -= c_crt.p_hi + (xlo < c_crt.p_lo ? 1 : 0);
+            xlo = t;
+        }
+        // centre into (-P/2, P/2]
+        bool neg = false;
+        if (xhi > c_crt.h_hi || (xhi == c_crt.h_hi && xlo > c_crt.h_lo)) {
+            // x - P < 0: magnitude P - x
+            const uint64_t t = c_crt.p_lo - xlo;
+            xhi = c_crt.p_hi - xhi - (c_crt.p_lo < xlo ? 1 : 0);
+            xlo = t;
+            neg = true;
+        }
+        double v = (double)xhi * 18446744073709551616.0 + (double)xlo;
+        v = ldexp(neg ? -v : v, -(sA[i] + sB[j]));
+        C[(int64_t)i * ldc + j] = v;
+    }
+}
+
+// ============================================================================ host driver
+static int sms()
+{
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+}
+
+static bool device_is_sm100()
+{
+    int dev = 0, major = 0, minor = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+    return major == 10 && minor == 0;
+}
+
+int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B, int64_t ldb,
+                   double *C, int64_t ldc, int nterms, cudaStream_t st)
+{
+    if (!device_is_sm100()) return -1;
+    if (M <= 0 || N <= 0 || K <= 0) return 0;
+    // |sum_k a*b| <= K * 2^14 must keep the epilogue's float quotient within one of the
+    // true quotient (K * 2^14 * 2^-24 / 173 < 0.5) and the int32 accumulator exact
+    if (K > 65536 || M > (1 << 30) || N > (1 << 30)) return -1;
+    const int L = nterms > 0 ? nterms : 14;
+    static std::mutex mu;
+    static CrtConst cached;
+    static int cached_L = -1;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (cached_L != L) {
+            if (!build_crt(L, &cached)) return -1;
+            cached_L = L;
+        }
+        if (cudaMemcpyToSymbolAsync(c_crt, &cached, sizeof(CrtConst), 0, cudaMemcpyHostToDevice, st) != cudaSuccess)
+            return -1;
+    }
+    const double gamma = (cached.log2p - 1.0) / 2.0 - 0.01;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int64_t Kp = round_up(K, oz::BK);
+    const int64_t ldr = round_up(N, 16);
+    DevBuf ra, rb, rr, sa, sb, pm, ps, err;
+    if (!ra.allocate((size_t)(L * M * Kp), dev) || !rb.allocate((size_t)(L * N * Kp), dev) ||
+        !rr.allocate((size_t)(L * M * ldr), dev) || !sa.allocate((size_t)M * 4, dev) ||
+        !sb.allocate((size_t)N * 4, dev) || !pm.allocate((size_t)COL_SEGS * N * 8, dev) ||
+        !ps.allocate((size_t)COL_SEGS * N * 8, dev) || !err.allocate(16, dev))
+        return -100;
+    cudaMemsetAsync(err.p, 0, 16, st);
+    const int nsm = sms();
+    IAB_LAUNCHED(1);
+    k_row_shift<<<(unsigned)((M * 32 + 255) / 256), 256, 0, st>>>((int)M, (int)K, A, lda, gamma, sa.as<int>());
+    IAB_LAUNCHED(1);
+    k_col_partial<<<dim3((unsigned)((N + 255) / 256), COL_SEGS), 256, 0, st>>>((int)K, (int)N, B, ldb, pm.as<double>(),
+                                                                               ps.as<double>());
+    IAB_LAUNCHED(1);
+    k_col_shift<<<(unsigned)((N + 255) / 256), 256, 0, st>>>((int)N, pm.as<double>(), ps.as<double>(), gamma, sb.as<int>());
+    IAB_LAUNCHED(1);
+    k_residues_rows<<<(unsigned)(nsm * 16), 256, 0, st>>>((int)M, (int)K, (int)Kp, A, lda, sa.as<int>(), ra.as<int8_t>());
+    IAB_LAUNCHED(1);
+    k_residues_cols<<<dim3((unsigned)((N + 63) / 64), (unsigned)((Kp + 63) / 64)), 256, 0, st>>>(
+        (int)K, (int)N, (int)Kp, B, ldb, sb.as<int>(), rb.as<int8_t>());
+
+    CUtensorMap tmA, tmB;
+    if (!make_tmap_3d(&tmA, CU_TENSOR_MAP_DATA_TYPE_UINT8, ra.p, (uint64_t)Kp, (uint64_t)M, (uint64_t)L, (uint64_t)Kp,
+                      (uint64_t)(Kp * M), oz::BK, oz::BM, CU_TENSOR_MAP_SWIZZLE_128B) ||
+        !make_tmap_3d(&tmB, CU_TENSOR_MAP_DATA_TYPE_UINT8, rb.p, (uint64_t)Kp, (uint64_t)N, (uint64_t)L, (uint64_t)Kp,
+                      (uint64_t)(Kp * N), oz::BK, oz::BN, CU_TENSOR_MAP_SWIZZLE_128B))
+        return -1;
+    I8Params prm;
+    prm.M = (int)M; prm.N = (int)N; prm.Kp = (int)Kp; prm.L = L;
+    prm.tiles_m = (int)ceil_div(M, oz::BM); prm.tiles_n = (int)ceil_div(N, oz::BN);
+    prm.R = rr.as<uint8_t>(); prm.ldr = ldr; prm.err = err.as<int>();
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_i8gemm_mod, cudaFuncAttributeMaxDynamicSharedMemorySize, oz::SMEM);
+        attr = true;
+    }
+    const int tiles = L * prm.tiles_m * prm.tiles_n;
+    IAB_LAUNCHED(1);
+    k_i8gemm_mod<<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm);
+    IAB_LAUNCHED(1);
+    k_crt<<<(unsigned)(nsm * 16), 256, 0, st>>>((int)M, (int)N, rr.as<uint8_t>(), ldr, sa.as<int>(), sb.as<int>(), C, ldc);
+    int h_err = 0;
+    cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return -2;
+    return h_err ? -3 : 0;
 }
 
 int gemm_f32_bf16x3(int64_t, int64_t, int64_t, const float *, int64_t, const float *, int64_t, float *, int64_t,

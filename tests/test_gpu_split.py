@@ -1,0 +1,84 @@
+"""GPU tests of the split-precision forms through the C ABI.
+
+float64 (Ozaki scheme II on INT8 tensor cores): integer-valued products are exact; for
+wide-range random data the normwise error against the double-double oracle must stay
+within 4x the native FP64 path's error (the project's acceptance bar), and below 1e-14.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from ref_fixtures import GEMM
+
+pytestmark = pytest.mark.gpu
+
+
+def _split_ctx(ia):
+    c = ia.Context()
+    c.set_form(ia.FORM_SPLIT)
+    return c
+
+
+def _scaled(rng, shape):
+    return rng.uniform(-1, 1, shape) * np.exp2(rng.integers(-8, 9, shape))
+
+
+@pytest.mark.parametrize("M,K,N,cs,bs", [
+    (300, 257, 200, 128, 32),        # ragged: M, N not tile multiples, K not a multiple of 128
+    (256, 1024, 512, 256, 64),
+    (129, 130, 257, 64, 16),
+    (1000, 1000, 1000, 500, 100),
+])
+def test_split_f64_error_within_bar(ia, M, K, N, cs, bs):
+    rng = np.random.default_rng(M + K + N)
+    A, B = _scaled(rng, (M, K)), _scaled(rng, (K, N))
+    sctx, nctx = _split_ctx(ia), ia.Context()
+    Ac = ia.Container.from_numpy(nctx, A, (cs, cs), (bs, bs))
+    Bc = ia.Container.from_numpy(nctx, B, (cs, cs), (bs, bs))
+    cn = ia.opt_gemm(nctx, Ac, Bc, (cs, cs), (bs, bs)).to_numpy()
+    cs_ = ia.opt_gemm(sctx, Ac, Bc, (cs, cs), (bs, bs)).to_numpy()
+    rows = np.arange(M)
+    hi, lo = O.dd_rows(A, B, rows)
+    en = O.normwise_error(cn, hi, lo, rows)
+    es = O.normwise_error(cs_, hi, lo, rows)
+    assert es <= 1e-14, es
+    assert es <= 4 * max(en, 1e-17), (es, en)
+
+
+@pytest.mark.parametrize("fx", [f for f in GEMM if f[1] == "f8"], ids=lambda f: f[0])
+def test_split_f64_exact_on_integer_fixtures(ia, fx):
+    """The reference's arange fixtures: every product is an integer below 2^53, so the
+    split form must reproduce it exactly."""
+    name, dt, (xs, xc, xb), (ys, yc, yb), (zs, zc, zb) = fx
+    ctx = _split_ctx(ia)
+    X = ia.Container.arange(ctx, xs, np.float64, 0, 1, xc, xb)
+    Y = ia.Container.arange(ctx, ys, np.float64, 0, 1, yc, yb)
+    z = ia.matmul(ctx, X, Y, zc, zb).to_numpy()
+    x, y = X.to_numpy(), Y.to_numpy()
+    assert np.array_equal(z, O.dense_gemm(x, y))
+
+
+def test_split_f64_zero_rows_and_signs(ia):
+    rng = np.random.default_rng(3)
+    A = _scaled(rng, (200, 300))
+    A[5] = 0.0
+    A[:, 7] = 0.0
+    B = -_scaled(rng, (300, 150))
+    B[:, 3] = 0.0
+    ctx = _split_ctx(ia)
+    C = ia.matmul(ctx, ia.Container.from_numpy(ctx, A, (128, 128), (32, 32)),
+                  ia.Container.from_numpy(ctx, B, (128, 128), (32, 32)), (128, 128), (32, 32)).to_numpy()
+    hi, lo = O.dd_rows(A, B, np.arange(200))
+    assert not C[5].any() and not C[:, 3].any()
+    assert O.normwise_error(C, hi, lo, np.arange(200)) <= 1e-14
+
+
+@pytest.mark.parametrize("nterms", [14, 15, 16])
+def test_split_f64_more_moduli_is_at_least_as_accurate(ia, nterms):
+    rng = np.random.default_rng(nterms)
+    A, B = _scaled(rng, (256, 512)), _scaled(rng, (512, 256))
+    ctx = ia.Context(form=ia.FORM_SPLIT, split_terms=nterms)
+    C = ia.matmul(ctx, ia.Container.from_numpy(ctx, A, (256, 256), (64, 64)),
+                  ia.Container.from_numpy(ctx, B, (256, 256), (64, 64)), (256, 256), (64, 64)).to_numpy()
+    hi, lo = O.dd_rows(A, B, np.arange(256))
+    assert O.normwise_error(C, hi, lo, np.arange(256)) <= 2e-15
