@@ -211,6 +211,140 @@ __global__ void __launch_bounds__(256) k_lz4_decode(const uint8_t *__restrict__ 
     }
 }
 
+// D1 (batched): one warp per LZ4 stream, 32 sequences per step.  Every lane parses the
+// same token stream from a shared-memory input window (uniform control flow, so the
+// parse costs one instruction stream per warp); lane s keeps sequence s.  The copy
+// phase then runs the 32 sequences in parallel: literals first (no dependencies),
+// then matches in rounds - a lane copies once every earlier lane whose match output
+// overlaps its source has finished.  History for matches within RING bytes comes from
+// a shared-memory ring; older sources are read back from the output in global memory.
+template <int RING, int IWIN>
+__global__ void __launch_bounds__(256) k_lz4_decode_batched(const uint8_t *__restrict__ ch,
+                                                            const Lz4Job *__restrict__ jobs,
+                                                            const int *__restrict__ njobs_p, uint8_t *scratch,
+                                                            int *err, unsigned *next)
+{
+    extern __shared__ uint8_t sm_dec[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint8_t *ring = sm_dec + warp * (RING + IWIN);
+    uint8_t *iwin = ring + RING;
+    const int njobs = *njobs_p;
+    for (;;) {
+        unsigned got = 0;
+        if (lane == 0) got = atomicAdd(next, 1u);
+        const int jid = (int)__shfl_sync(FULLMASK, got, 0);
+        if (jid >= njobs) break;
+        const Lz4Job jb = jobs[jid];
+        const uint8_t *__restrict__ in = ch + jb.src;
+        const int isz = jb.csize;
+        uint8_t *out = scratch + jb.dst;
+        const int osz = jb.dlen;
+        // input window: bytes [wlo, wlo + IWIN) of the stream staged in iwin (ring-indexed)
+        int wlo = 0, whi = 0;
+        auto stage = [&](int from) {
+            wlo = from;
+            whi = min(isz, from + IWIN);
+            for (int x = from + lane; x < whi; x += 32) iwin[x & (IWIN - 1)] = __ldg(in + x);
+            __syncwarp();
+        };
+        auto rd = [&](int q) -> int {
+            if (q >= whi) stage(q);
+            return iwin[q & (IWIN - 1)];
+        };
+        stage(0);
+        int p = 0, op = 0;
+        bool bad = false, done = false;
+        while (!done && !bad) {
+            int my_lp = 0, my_lit = 0, my_op = 0, my_off = 1, my_ml = 0, nseq = 0;
+            const int batch_op0 = op;
+            for (int s = 0; s < 32; s++) {
+                if (p >= isz) { bad = true; break; }
+                const int tok = rd(p++);
+                int lit = tok >> 4;
+                if (lit == 15) {
+                    int b;
+                    do {
+                        if (p >= isz) { bad = true; break; }
+                        b = rd(p++);
+                        lit += b;
+                    } while (b == 255);
+                    if (bad) break;
+                }
+                if (lit > isz - p || lit > osz - op) { bad = true; break; }
+                const int lp = p;
+                p += lit;
+                int off = 1, ml = 0;
+                const bool last = p == isz;
+                if (!last) {
+                    if (isz - p < 2) { bad = true; break; }
+                    const int o0 = rd(p);          // in order: a restage may move the window
+                    const int o1 = rd(p + 1);
+                    off = o0 | (o1 << 8);
+                    p += 2;
+                    ml = tok & 15;
+                    if (ml == 15) {
+                        int b;
+                        do {
+                            if (p >= isz) { bad = true; break; }
+                            b = rd(p++);
+                            ml += b;
+                        } while (b == 255);
+                        if (bad) break;
+                    }
+                    ml += 4;
+                    if (off == 0 || off > op + lit || ml > osz - op - lit) { bad = true; break; }
+                }
+                if (lane == s) { my_lp = lp; my_lit = lit; my_op = op; my_off = off; my_ml = ml; }
+                op += lit + ml;
+                nseq = s + 1;
+                if (last) { done = true; break; }
+            }
+            if (bad) break;
+            const bool active = lane < nseq;
+            // literals
+            if (active) {
+                for (int i = 0; i < my_lit; i++) {
+                    const uint8_t v = __ldg(in + my_lp + i);
+                    out[my_op + i] = v;
+                    ring[(my_op + i) & (RING - 1)] = v;
+                }
+            }
+            __syncwarp();
+            // matches in dependency rounds
+            const int mstart = my_op + my_lit;
+            const int src = mstart - my_off;
+            const int src_end = src + min(my_ml, my_off);
+            unsigned dep = 0;
+            for (int t = 0; t < 31; t++) {
+                const int ms = __shfl_sync(FULLMASK, mstart, t);
+                const int me = ms + __shfl_sync(FULLMASK, my_ml, t);
+                if (t < lane && ms < src_end && me > src) dep |= 1u << t;
+            }
+            // sources this far back are never overwritten in the ring during this batch
+            const bool from_ring = src >= op - RING;
+            bool mine = !(active && my_ml > 0);
+            unsigned donem = __ballot_sync(FULLMASK, mine);
+            for (int round = 0; donem != FULLMASK && round < 33; round++) {
+                if (!mine && (dep & ~donem) == 0) {
+                    for (int i = 0; i < my_ml; i++) {
+                        const int sp = src + (my_off >= my_ml ? i : i % my_off);
+                        const uint8_t v = from_ring ? ring[sp & (RING - 1)] : __ldcg(out + sp);
+                        out[mstart + i] = v;
+                        ring[(mstart + i) & (RING - 1)] = v;
+                    }
+                    mine = true;
+                }
+                __syncwarp();
+                donem = __ballot_sync(FULLMASK, mine);
+            }
+            (void)batch_op0;
+        }
+        if (!bad && op != osz) bad = true;
+        if (bad && lane == 0) dev_fail(err, DE_LZ4);
+        __syncwarp();
+    }
+}
+
 constexpr int TILE = 1024;
 
 __device__ __forceinline__ void store_item(uint8_t *o, int ts, uint64_t v)
@@ -353,10 +487,14 @@ __global__ void __launch_bounds__(256) k_gather(Geom g, const uint8_t *__restric
 }
 
 // ---------------------------------------------------------------- LZ4 encoder (warp)
+// Unaligned little-endian reads from a source whose stream base is 4-byte aligned: two
+// aligned word loads and a funnel shift.  Callers only read where p + 7 stays inside the
+// stream (hash positions are at most n - 12; match candidates lie before them).
 __device__ __forceinline__ uint32_t ld4u(const uint8_t *p)
 {
-    return (uint32_t)__ldg(p) | ((uint32_t)__ldg(p + 1) << 8) | ((uint32_t)__ldg(p + 2) << 16) |
-           ((uint32_t)__ldg(p + 3) << 24);
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~uintptr_t(3));
+    return __funnelshift_r(__ldg(w), __ldg(w + 1), (uint32_t)(a & 3) * 8);
 }
 
 __device__ __forceinline__ uint32_t lz_hash(const uint8_t *p, bool small)
@@ -402,7 +540,9 @@ __device__ int warp_lz4_compress(const uint8_t *__restrict__ src, int n, uint8_t
             bool found = false;
             for (;;) {
                 const int64_t t = t0 + lane;
-                const int64_t p = p0 + probe_offset(t), pn = p0 + probe_offset(t + 1);
+                // the step is 1 for the first 65 probes: positions are p0 + t there
+                const int64_t p = t0 + 32 <= 64 ? p0 + t : p0 + probe_offset(t);
+                const int64_t pn = t0 + 32 <= 64 ? p + 1 : p0 + probe_offset(t + 1);
                 const bool valid = pn <= mfl1;
                 const uint32_t h = valid ? lz_hash(src + p, small) : (0x80000000u | (uint32_t)lane);
                 const uint32_t ctab = valid ? TGET(h) : 0u;
@@ -737,13 +877,16 @@ int decode_launch(const Geom &g, const uint8_t *d_chunks, const int64_t *d_off, 
     }
     {
         static bool attr = false;
-        const int smem = 8 * DEC_RING;
+        constexpr int IWIN = 1024;
+        const int smem = 8 * (DEC_RING + IWIN);
         if (!attr) {
-            cudaFuncSetAttribute(k_lz4_decode<DEC_RING>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            cudaFuncSetAttribute(k_lz4_decode_batched<DEC_RING, IWIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             attr = true;
         }
         IAB_LAUNCHED(1);
-        k_lz4_decode<DEC_RING><<<sms * 3, 256, smem, st>>>(d_chunks, jobs.as<Lz4Job>(), njobs, scratch.as<uint8_t>(), err);
+        k_lz4_decode_batched<DEC_RING, IWIN><<<sms * 3, 256, smem, st>>>(d_chunks, jobs.as<Lz4Job>(), njobs,
+                                                                       scratch.as<uint8_t>(), err,
+                                                                       reinterpret_cast<unsigned *>(counters.as<int>() + 2));
     }
     {
         const int64_t tpb = (g.blockn + TILE - 1) / TILE;
