@@ -9,7 +9,7 @@
 // src/iarray_constructor.c:218-305).
 //
 // Decode = parse (one thread per block walks its stream headers) -> LZ4 (one warp per
-// LZ4 stream, 8 KiB shared-memory history ring) -> unshuffle/scatter (one CTA per
+// LZ4 stream, sequences located 32 at a time by pointer doubling) -> unshuffle/scatter (one CTA per
 // block tile, byte planes staged in shared memory, items written to the dense
 // row-major array).  Raw and run streams are never copied before the scatter.
 //
@@ -121,117 +121,35 @@ __global__ void k_parse(Geom g, const uint8_t *__restrict__ ch, const int64_t *_
     }
 }
 
-// D1: one warp per LZ4 stream.  The 32 input bytes at the parse position are held one
-// per lane and read with shuffles; output goes to the scratch image and to a
-// shared-memory ring that serves matches whose source lies in the last RING bytes.
-template <int RING>
-__global__ void __launch_bounds__(256) k_lz4_decode(const uint8_t *__restrict__ ch, const Lz4Job *__restrict__ jobs,
-                                                    const int *__restrict__ njobs_p, uint8_t *scratch, int *err)
-{
-    extern __shared__ uint8_t sm_ring[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-    uint8_t *ring = sm_ring + warp * RING;
-    const int njobs = *njobs_p;
-    for (int jid = blockIdx.x * wpb + warp; jid < njobs; jid += gridDim.x * wpb) {
-        const Lz4Job jb = jobs[jid];
-        const uint8_t *__restrict__ in = ch + jb.src;
-        const int isz = jb.csize;
-        uint8_t *out = scratch + jb.dst;
-        const int osz = jb.dlen;
-        int wbase = 0;
-        uint32_t win = lane < isz ? __ldg(in + lane) : 0u;
-        auto byte_at = [&](int pos) -> int {
-            if ((unsigned)(pos - wbase) >= 32u) {
-                wbase = pos;
-                win = (pos + lane < isz) ? __ldg(in + pos + lane) : 0u;
-            }
-            return (int)__shfl_sync(FULLMASK, win, pos - wbase);
-        };
-        int ip = 0, op = 0;
-        bool bad = false;
-        for (;;) {
-            if (ip >= isz) { bad = true; break; }
-            const int token = byte_at(ip++);
-            int lit = token >> 4;
-            if (lit == 15) {
-                int s;
-                do {
-                    if (ip >= isz) { bad = true; break; }
-                    s = byte_at(ip++);
-                    lit += s;
-                } while (s == 255);
-                if (bad) break;
-            }
-            if (lit > isz - ip || lit > osz - op) { bad = true; break; }
-            for (int x = lane; x < lit; x += 32) {
-                const uint8_t v = __ldg(in + ip + x);
-                out[op + x] = v;
-                ring[(op + x) & (RING - 1)] = v;
-            }
-            ip += lit;
-            op += lit;
-            if (ip == isz) break;
-            if (isz - ip < 2) { bad = true; break; }
-            const int mo = byte_at(ip) | (byte_at(ip + 1) << 8);
-            ip += 2;
-            int ml = token & 15;
-            if (ml == 15) {
-                int s;
-                do {
-                    if (ip >= isz) { bad = true; break; }
-                    s = byte_at(ip++);
-                    ml += s;
-                } while (s == 255);
-                if (bad) break;
-            }
-            ml += 4;
-            if (mo == 0 || mo > op || ml > osz - op) { bad = true; break; }
-            __syncwarp();
-            if (mo + ml <= RING) {
-                for (int x = lane; x < ml; x += 32) {
-                    const int sp = op - mo + (mo >= ml ? x : x % mo);
-                    const uint8_t v = ring[sp & (RING - 1)];
-                    out[op + x] = v;
-                    ring[(op + x) & (RING - 1)] = v;
-                }
-            } else {
-                for (int x = lane; x < ml; x += 32) {
-                    const int sp = op - mo + (mo >= ml ? x : x % mo);
-                    const uint8_t v = __ldcg(out + sp);
-                    out[op + x] = v;
-                    ring[(op + x) & (RING - 1)] = v;
-                }
-            }
-            op += ml;
-            __syncwarp();
-        }
-        if (!bad && op != osz) bad = true;
-        if (bad && lane == 0) dev_fail(err, DE_LZ4);
-        __syncwarp();
-    }
-}
+// D1 (parallel parse): one warp per LZ4 stream.  The stream is consumed in windows of W
+// input bytes staged in shared memory.  For every byte position q of the window the
+// warp computes next[q] = where the following token would start if a sequence began at
+// q (STOP if that sequence does not end inside the window, ENDS if it is the stream's
+// last sequence).  Five pointer-doubling levels (next^1, ^2, ^4, ^8, ^16) then let lane l
+// locate the l-th sequence after a known token position with five table reads, so 32
+// sequences are parsed in parallel per step.  Copies run per batch of <= 32 sequences:
+// literals first, then matches in rounds; a lane copies once its source lies below the
+// lowest output position still owed by an unfinished lane (the frontier).  A batch never
+// spans more than RING output bytes, so within a batch no two output positions share a
+// slot of the shared-memory history ring; older history is read back from global memory.
+// A sequence too long for a window is decoded on its own (header read from global).
+constexpr uint16_t SEQ_STOP = 0xFFFF, SEQ_ENDS = 0xFFFE;
 
-// D1 (batched): one warp per LZ4 stream, 32 sequences per step.  Every lane parses the
-// same token stream from a shared-memory input window (uniform control flow, so the
-// parse costs one instruction stream per warp); lane s keeps sequence s.  The copy
-// phase then runs the 32 sequences in parallel: literals first (no dependencies),
-// then matches in rounds - a lane copies once every earlier lane whose match output
-// overlaps its source has finished.  History for matches within RING bytes comes from
-// a shared-memory ring; older sources are read back from the output in global memory.
-template <int RING, int IWIN>
-__global__ void __launch_bounds__(256) k_lz4_decode_batched(const uint8_t *__restrict__ ch,
-                                                            const Lz4Job *__restrict__ jobs,
-                                                            const int *__restrict__ njobs_p, uint8_t *scratch,
-                                                            int *err, unsigned *next)
+template <int RING, int W>
+__global__ void __launch_bounds__(128) k_lz4_decode_jump(const uint8_t *__restrict__ ch, const Lz4Job *__restrict__ jobs,
+                                                         const int *__restrict__ njobs_p, uint8_t *scratch, int *err,
+                                                         unsigned *next_job)
 {
-    extern __shared__ uint8_t sm_dec[];
+    extern __shared__ __align__(16) uint8_t sm_jump[];
+    constexpr int PER_WARP = RING + W + 16 + 5 * W * 2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint8_t *ring = sm_dec + warp * (RING + IWIN);
+    uint8_t *ring = sm_jump + warp * PER_WARP;
     uint8_t *iwin = ring + RING;
+    uint16_t *J = reinterpret_cast<uint16_t *>(iwin + W + 16);   // J[b * W + q], b = 0..4
     const int njobs = *njobs_p;
     for (;;) {
         unsigned got = 0;
-        if (lane == 0) got = atomicAdd(next, 1u);
+        if (lane == 0) got = atomicAdd(next_job, 1u);
         const int jid = (int)__shfl_sync(FULLMASK, got, 0);
         if (jid >= njobs) break;
         const Lz4Job jb = jobs[jid];
@@ -239,105 +157,208 @@ __global__ void __launch_bounds__(256) k_lz4_decode_batched(const uint8_t *__res
         const int isz = jb.csize;
         uint8_t *out = scratch + jb.dst;
         const int osz = jb.dlen;
-        // input window: bytes [wlo, wlo + IWIN) of the stream staged in iwin (ring-indexed)
-        int wlo = 0, whi = 0;
-        auto stage = [&](int from) {
-            wlo = from;
-            whi = min(isz, from + IWIN);
-            for (int x = from + lane; x < whi; x += 32) iwin[x & (IWIN - 1)] = __ldg(in + x);
-            __syncwarp();
-        };
-        auto rd = [&](int q) -> int {
-            if (q >= whi) stage(q);
-            return iwin[q & (IWIN - 1)];
-        };
-        stage(0);
         int p = 0, op = 0;
         bool bad = false, done = false;
         while (!done && !bad) {
-            int my_lp = 0, my_lit = 0, my_op = 0, my_off = 1, my_ml = 0, nseq = 0;
-            const int batch_op0 = op;
-            for (int s = 0; s < 32; s++) {
-                if (p >= isz) { bad = true; break; }
-                const int tok = rd(p++);
-                int lit = tok >> 4;
-                if (lit == 15) {
-                    int b;
-                    do {
-                        if (p >= isz) { bad = true; break; }
-                        b = rd(p++);
-                        lit += b;
-                    } while (b == 255);
-                    if (bad) break;
-                }
-                if (lit > isz - p || lit > osz - op) { bad = true; break; }
-                const int lp = p;
-                p += lit;
-                int off = 1, ml = 0;
-                const bool last = p == isz;
-                if (!last) {
-                    if (isz - p < 2) { bad = true; break; }
-                    const int o0 = rd(p);          // in order: a restage may move the window
-                    const int o1 = rd(p + 1);
-                    off = o0 | (o1 << 8);
-                    p += 2;
-                    ml = tok & 15;
-                    if (ml == 15) {
-                        int b;
-                        do {
-                            if (p >= isz) { bad = true; break; }
-                            b = rd(p++);
-                            ml += b;
-                        } while (b == 255);
-                        if (bad) break;
+            const int n = min(W, isz - p);            // valid bytes in this window
+            const int rem = isz - p;                  // bytes left in the stream
+            for (int x = lane; x < n; x += 32) iwin[x] = __ldg(in + p + x);
+            __syncwarp();
+            // next[q]: parse one sequence header at q inside the window
+            for (int q = lane; q < W; q += 32) {
+                uint16_t nx = SEQ_STOP;
+                if (q < n) {
+                    int r = q + 1;
+                    const int tok = iwin[q];
+                    int lit = tok >> 4;
+                    bool ok = true;
+                    if (lit == 15) {
+                        int b = 255;
+                        while (b == 255) {
+                            if (r >= n) { ok = false; break; }
+                            b = iwin[r++];
+                            lit += b;
+                        }
                     }
-                    ml += 4;
-                    if (off == 0 || off > op + lit || ml > osz - op - lit) { bad = true; break; }
+                    if (ok) {
+                        r += lit;
+                        if (r == rem) nx = SEQ_ENDS;             // literals reach the stream end: last sequence
+                        else if (r + 2 <= n) {
+                            r += 2;
+                            int ml = tok & 15;
+                            if (ml == 15) {
+                                int b = 255;
+                                while (b == 255) {
+                                    if (r >= n) { ok = false; break; }
+                                    b = iwin[r++];
+                                }
+                            }
+                            if (ok && r <= n) nx = (uint16_t)r;
+                        }
+                    }
                 }
-                if (lane == s) { my_lp = lp; my_lit = lit; my_op = op; my_off = off; my_ml = ml; }
-                op += lit + ml;
-                nseq = s + 1;
-                if (last) { done = true; break; }
-            }
-            if (bad) break;
-            const bool active = lane < nseq;
-            // literals
-            if (active) {
-                for (int i = 0; i < my_lit; i++) {
-                    const uint8_t v = __ldg(in + my_lp + i);
-                    out[my_op + i] = v;
-                    ring[(my_op + i) & (RING - 1)] = v;
-                }
+                J[q] = nx;
             }
             __syncwarp();
-            // matches in dependency rounds
-            const int mstart = my_op + my_lit;
-            const int src = mstart - my_off;
-            const int src_end = src + min(my_ml, my_off);
-            unsigned dep = 0;
-            for (int t = 0; t < 31; t++) {
-                const int ms = __shfl_sync(FULLMASK, mstart, t);
-                const int me = ms + __shfl_sync(FULLMASK, my_ml, t);
-                if (t < lane && ms < src_end && me > src) dep |= 1u << t;
-            }
-            // sources this far back are never overwritten in the ring during this batch
-            const bool from_ring = src >= op - RING;
-            bool mine = !(active && my_ml > 0);
-            unsigned donem = __ballot_sync(FULLMASK, mine);
-            for (int round = 0; donem != FULLMASK && round < 33; round++) {
-                if (!mine && (dep & ~donem) == 0) {
-                    for (int i = 0; i < my_ml; i++) {
-                        const int sp = src + (my_off >= my_ml ? i : i % my_off);
-                        const uint8_t v = from_ring ? ring[sp & (RING - 1)] : __ldcg(out + sp);
-                        out[mstart + i] = v;
-                        ring[(mstart + i) & (RING - 1)] = v;
-                    }
-                    mine = true;
+            for (int b = 1; b < 5; b++) {
+                const uint16_t *Jp = J + (b - 1) * W;
+                uint16_t *Jb = J + b * W;
+                for (int q = lane; q < W; q += 32) {
+                    const uint16_t v = Jp[q];
+                    Jb[q] = v < n ? Jp[v] : v;
                 }
                 __syncwarp();
-                donem = __ballot_sync(FULLMASK, mine);
             }
-            (void)batch_op0;
+            // batches of up to 32 sequences, starting at relative position `start`
+            int start = 0;
+            while (!done && !bad) {
+                if (start >= n || J[start] == SEQ_STOP) break;    // next sequence not complete here
+                int pos = start;
+#pragma unroll
+                for (int b = 0; b < 5; b++)
+                    if (((lane >> b) & 1) && pos < n) pos = J[b * W + pos];
+                const bool have = pos < n && J[pos] != SEQ_STOP;
+                int nb = __popc(__ballot_sync(FULLMASK, have));   // sequences present: a prefix of lanes
+                // parse my sequence
+                int lit = 0, ml = 0, off = 1, lp = 0;
+                bool last = false;
+                if (have) {
+                    int r = pos + 1;
+                    const int tok = iwin[pos];
+                    lit = tok >> 4;
+                    if (lit == 15) {
+                        int b = 255;
+                        while (b == 255) { b = iwin[r++]; lit += b; }
+                    }
+                    lp = p + r;
+                    r += lit;
+                    last = J[pos] == SEQ_ENDS;
+                    if (!last) {
+                        off = iwin[r] | (iwin[r + 1] << 8);
+                        r += 2;
+                        ml = tok & 15;
+                        if (ml == 15) {
+                            int b = 255;
+                            while (b == 255) { b = iwin[r++]; ml += b; }
+                        }
+                        ml += 4;
+                    }
+                }
+                // output positions: exclusive prefix of lit + ml
+                const int span = lit + ml;
+                int incl = span;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(FULLMASK, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const int my_op = op + incl - span;
+                // cut the batch where its output span would exceed RING (lane 0 always stays)
+                const unsigned over = __ballot_sync(FULLMASK, lane > 0 && lane < nb && incl > RING);
+                if (over) nb = min(nb, __ffs(over) - 1);
+                // a sequence after the stream's last one is malformed
+                const unsigned lastm = __ballot_sync(FULLMASK, lane < nb && last);
+                if (lastm) {
+                    const int li = __ffs(lastm) - 1;
+                    nb = li + 1;
+                    done = true;
+                }
+                const bool act = lane < nb;
+                const bool badme = act && (lit > osz - my_op || (!last && (off == 0 || off > my_op + lit ||
+                                                                           ml > osz - my_op - lit)));
+                if (__any_sync(FULLMASK, badme)) { bad = true; break; }
+                const int bspan = __shfl_sync(FULLMASK, incl, nb - 1);
+                // literals
+                if (act) {
+                    for (int i = 0; i < lit; i++) {
+                        const uint8_t v = __ldg(in + lp + i);
+                        out[my_op + i] = v;
+                        ring[(my_op + i) & (RING - 1)] = v;
+                    }
+                }
+                __syncwarp();
+                // matches in frontier rounds
+                const int mstart = my_op + lit;
+                const int src = mstart - off;
+                const int src_end = src + min(ml, off);
+                const int batch_end = op + bspan;
+                const bool from_ring = src >= batch_end - RING;
+                bool mine = !(act && ml > 0);
+                for (int round = 0; round < 33; round++) {
+                    const int frontier = (int)__reduce_min_sync(FULLMASK, mine ? 0x7FFFFFFFu : (unsigned)mstart);
+                    if (frontier == 0x7FFFFFFF) break;
+                    if (!mine && src_end <= frontier) {
+                        for (int i = 0; i < ml; i++) {
+                            const int sp = src + (off >= ml ? i : i % off);
+                            const uint8_t v = from_ring ? ring[sp & (RING - 1)] : __ldcg(out + sp);
+                            out[mstart + i] = v;
+                            ring[(mstart + i) & (RING - 1)] = v;
+                        }
+                        mine = true;
+                    }
+                    __syncwarp();
+                }
+                // advance past the batch
+                const int nxt = __shfl_sync(FULLMASK, have ? (int)J[pos] : 0, nb - 1);
+                op += bspan;
+                if (done) break;
+                start = nxt;
+            }
+            if (done || bad) break;
+            if (start > 0) {
+                p += start;      // restage at the first sequence not decoded yet
+                continue;
+            }
+            // the sequence at p does not fit in a window: decode it alone, header from global
+            {
+                int r = p;
+                const int tok = __ldg(in + r++);
+                int lit = tok >> 4;
+                if (lit == 15) {
+                    int b = 255;
+                    while (b == 255) {
+                        if (r >= isz) { bad = true; break; }
+                        b = __ldg(in + r++);
+                        lit += b;
+                    }
+                    if (bad) break;
+                }
+                if (lit > isz - r || lit > osz - op) { bad = true; break; }
+                for (int x = lane; x < lit; x += 32) {
+                    const uint8_t v = __ldg(in + r + x);
+                    out[op + x] = v;
+                    ring[(op + x) & (RING - 1)] = v;
+                }
+                r += lit;
+                op += lit;
+                __syncwarp();
+                if (r == isz) { done = true; break; }
+                if (isz - r < 2) { bad = true; break; }
+                const int mo = __ldg(in + r) | (__ldg(in + r + 1) << 8);
+                r += 2;
+                int ml = tok & 15;
+                if (ml == 15) {
+                    int b = 255;
+                    while (b == 255) {
+                        if (r >= isz) { bad = true; break; }
+                        b = __ldg(in + r++);
+                        ml += b;
+                    }
+                    if (bad) break;
+                }
+                ml += 4;
+                if (mo == 0 || mo > op || ml > osz - op) { bad = true; break; }
+                const bool ringok = mo + ml <= RING;
+                for (int x = lane; x < ml; x += 32) {
+                    const int sp = op - mo + (mo >= ml ? x : x % mo);
+                    const uint8_t v = ringok ? ring[sp & (RING - 1)] : __ldcg(out + sp);
+                    out[op + x] = v;
+                    ring[(op + x) & (RING - 1)] = v;
+                }
+                op += ml;
+                p = r;
+                __syncwarp();
+            }
         }
         if (!bad && op != osz) bad = true;
         if (bad && lane == 0) dev_fail(err, DE_LZ4);
@@ -835,8 +856,6 @@ static int sm_count()
     return n;
 }
 
-constexpr int DEC_RING = 8192;
-
 int decode_container(const Geom &g, const uint8_t *d_chunks, const int64_t *d_off, const int32_t *d_len,
                      void *out, int64_t ld, cudaStream_t st)
 {
@@ -877,16 +896,16 @@ int decode_launch(const Geom &g, const uint8_t *d_chunks, const int64_t *d_off, 
     }
     {
         static bool attr = false;
-        constexpr int IWIN = 1024;
-        const int smem = 8 * (DEC_RING + IWIN);
+        constexpr int RING = 4096, WIN = 1024, WARPS = 4;
+        const int smem = WARPS * (RING + WIN + 16 + 5 * WIN * 2);
         if (!attr) {
-            cudaFuncSetAttribute(k_lz4_decode_batched<DEC_RING, IWIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            cudaFuncSetAttribute(k_lz4_decode_jump<RING, WIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             attr = true;
         }
         IAB_LAUNCHED(1);
-        k_lz4_decode_batched<DEC_RING, IWIN><<<sms * 3, 256, smem, st>>>(d_chunks, jobs.as<Lz4Job>(), njobs,
-                                                                       scratch.as<uint8_t>(), err,
-                                                                       reinterpret_cast<unsigned *>(counters.as<int>() + 2));
+        k_lz4_decode_jump<RING, WIN><<<sms * 3, WARPS * 32, smem, st>>>(d_chunks, jobs.as<Lz4Job>(), njobs,
+                                                                      scratch.as<uint8_t>(), err,
+                                                                      reinterpret_cast<unsigned *>(counters.as<int>() + 2));
     }
     {
         const int64_t tpb = (g.blockn + TILE - 1) / TILE;
