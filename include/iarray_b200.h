@@ -334,6 +334,11 @@ INA_API(uint64_t) iarray_b200_kernel_launches(void);
 /* The context's CUDA stream (a cudaStream_t), for callers that record their own
  * events around library calls. */
 INA_API(ina_rc_t) iarray_b200_get_stream(iarray_context_t *ctx, void **stream);
+/* Serialise a container as a contiguous frame (the layout of iarray_to_cframe) into a
+ * caller buffer of `cap` bytes, e.g. pinned host memory; *len receives the frame size.
+ * buf = NULL only queries the size. */
+INA_API(ina_rc_t) iarray_b200_to_cframe_into(iarray_context_t *ctx, iarray_container_t *c, uint8_t *buf,
+                                             int64_t cap, int64_t *len);
 
 #ifdef __cplusplus
 }

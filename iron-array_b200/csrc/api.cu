@@ -441,7 +441,7 @@ static ina_rc_t decode_store(iarray_context_t *ctx, const iarray_container_t *c,
         cudaMemsetAsync(dense, 0, (size_t)(g.shape[0] * ld * g.itemsize), ctx->stream);
     }
     const ChunkStore &s = *c->store;
-    const int r = iab::decode_container(g, s.buf.as<uint8_t>(), s.d_off.as<int64_t>(), s.d_len.as<int32_t>(), dense, ld,
+    const int r = iab::decode_container(g, s.buf.as<uint8_t>(), (int64_t)s.buf.n, s.d_off.as<int64_t>(), s.d_len.as<int32_t>(), dense, ld,
                                         ctx->stream);
     if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
     if (r < 0) return rc_err(IARRAY_ERR_GPU_FAILED);
@@ -469,9 +469,9 @@ static ina_rc_t decode_pair(iarray_context_t *ctx, const iarray_container_t *a, 
     cudaStreamWaitEvent(ctx->stream2, ctx->fork, 0);
     iab::DecodeWork wa, wb;
     int ra = 0, rb = 0;
-    if (ga.nchunks) ra = iab::decode_launch(ga, a->store->buf.as<uint8_t>(), a->store->d_off.as<int64_t>(),
+    if (ga.nchunks) ra = iab::decode_launch(ga, a->store->buf.as<uint8_t>(), (int64_t)a->store->buf.n, a->store->d_off.as<int64_t>(),
                                             a->store->d_len.as<int32_t>(), da, lda, ctx->stream, &wa);
-    if (gb.nchunks) rb = iab::decode_launch(gb, b->store->buf.as<uint8_t>(), b->store->d_off.as<int64_t>(),
+    if (gb.nchunks) rb = iab::decode_launch(gb, b->store->buf.as<uint8_t>(), (int64_t)b->store->buf.n, b->store->d_off.as<int64_t>(),
                                             b->store->d_len.as<int32_t>(), db, ldb, ctx->stream2, &wb);
     cudaEventRecord(ctx->join, ctx->stream2);
     cudaStreamWaitEvent(ctx->stream, ctx->join, 0);
@@ -718,18 +718,9 @@ INA_API(ina_rc_t) iarray_container_almost_equal(iarray_container_t *a, iarray_co
 }
 
 // ============================================================================ persistence
-static ina_rc_t to_frame(iarray_context_t *ctx, iarray_container_t *c, std::vector<uint8_t> *out)
+static iab::FrameInfo frame_info(iarray_context_t *ctx, const iarray_container_t *c)
 {
     const Geom &g = c->geom;
-    const ChunkStore &s = *c->store;
-    std::vector<uint8_t> host((size_t)std::max<int64_t>(s.cbytes, 1));
-    if (s.cbytes) {
-        cudaMemcpyAsync(host.data(), s.buf.p, (size_t)s.cbytes, cudaMemcpyDeviceToHost, ctx->stream);
-        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return rc_err(IARRAY_ERR_GPU_FAILED);
-    }
-    // chunks are stored back to back in logical order: s.off[k] is a running sum
-    std::vector<const uint8_t *> ptrs;
-    for (int64_t k = 0; k < g.nchunks; k++) ptrs.push_back(host.data() + s.off[k]);
     iab::FrameInfo fi;
     fi.ndim = c->dtshape.ndim;
     const iarray_dtshape_t &d = c->dtshape;
@@ -747,8 +738,60 @@ static ina_rc_t to_frame(iarray_context_t *ctx, iarray_container_t *c, std::vect
     fi.clevel = c->clevel;
     fi.nthreads = std::max(1, ctx->cfg.max_num_threads);
     fi.shuffle = c->shuffle;
-    iab::write_frame(fi, ptrs, s.len, out);
+    return fi;
+}
+
+// Serialise c as a contiguous frame into buf (capacity cap bytes); *len receives the
+// frame size (buf == NULL only queries it).  Chunk bytes go device -> buf directly.
+static ina_rc_t frame_into(iarray_context_t *ctx, iarray_container_t *c, uint8_t *buf, int64_t cap, int64_t *len)
+{
+    const Geom &g = c->geom;
+    const ChunkStore &s = *c->store;
+    const iab::FrameInfo fi = frame_info(ctx, c);
+    const std::vector<uint8_t> head = iab::frame_header(fi, s.cbytes, g.nchunks);
+    const std::vector<uint8_t> tail = iab::frame_tail(s.len);
+    const int64_t total = (int64_t)head.size() + s.cbytes + (int64_t)tail.size();
+    *len = total;
+    if (!buf) return INA_SUCCESS;
+    if (cap < total) return rc_err(IARRAY_ERR_TOO_SMALL_BUFFER);
+    memcpy(buf, head.data(), head.size());
+    uint8_t *data = buf + head.size();
+    bool in_order = true;
+    int64_t acc = 0;
+    for (int64_t k = 0; k < g.nchunks; k++) {
+        if (s.off[k] != acc) in_order = false;
+        acc += s.len[k];
+    }
+    if (in_order) {
+        if (s.cbytes) cudaMemcpyAsync(data, s.buf.p, (size_t)s.cbytes, cudaMemcpyDeviceToHost, ctx->stream);
+    } else {
+        acc = 0;
+        for (int64_t k = 0; k < g.nchunks; k++) {
+            cudaMemcpyAsync(data + acc, s.buf.as<uint8_t>() + s.off[k], (size_t)s.len[k], cudaMemcpyDeviceToHost,
+                            ctx->stream);
+            acc += s.len[k];
+        }
+    }
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return rc_err(IARRAY_ERR_GPU_FAILED);
+    memcpy(data + s.cbytes, tail.data(), tail.size());
     return INA_SUCCESS;
+}
+
+static ina_rc_t to_frame(iarray_context_t *ctx, iarray_container_t *c, std::vector<uint8_t> *out)
+{
+    int64_t n = 0;
+    ina_rc_t rc = frame_into(ctx, c, nullptr, 0, &n);
+    if (INA_FAILED(rc)) return rc;
+    out->resize((size_t)n);
+    return frame_into(ctx, c, out->data(), n, &n);
+}
+
+INA_API(ina_rc_t) iarray_b200_to_cframe_into(iarray_context_t *ctx, iarray_container_t *c, uint8_t *buf, int64_t cap,
+                                             int64_t *len)
+{
+    CHECK_ARG(ctx && c && len);
+    if (c->view) return rc_err(IARRAY_ERR_INVALID_STORAGE);
+    return frame_into(ctx, c, buf, cap, len);
 }
 
 INA_API(ina_rc_t) iarray_to_cframe(iarray_context_t *ctx, iarray_container_t *src, uint8_t **frame, int64_t *frame_len,
@@ -756,14 +799,15 @@ INA_API(ina_rc_t) iarray_to_cframe(iarray_context_t *ctx, iarray_container_t *sr
 {
     CHECK_ARG(ctx && src && frame && frame_len && needs_free);
     if (src->view) return rc_err(IARRAY_ERR_INVALID_STORAGE);
-    std::vector<uint8_t> f;
-    ina_rc_t rc = to_frame(ctx, src, &f);
+    int64_t n = 0;
+    ina_rc_t rc = frame_into(ctx, src, nullptr, 0, &n);
     if (INA_FAILED(rc)) return rc;
-    uint8_t *p = (uint8_t *)malloc(f.size());
+    uint8_t *p = (uint8_t *)malloc((size_t)n);
     if (!p) return rc_err(INA_ERR_OUT_OF_MEMORY);
-    memcpy(p, f.data(), f.size());
+    rc = frame_into(ctx, src, p, n, &n);
+    if (INA_FAILED(rc)) { free(p); return rc; }
     *frame = p;
-    *frame_len = (int64_t)f.size();
+    *frame_len = n;
     *needs_free = true;
     return INA_SUCCESS;
 }
@@ -794,12 +838,28 @@ INA_API(ina_rc_t) iarray_from_cframe(iarray_context_t *ctx, uint8_t *frame, int6
     }
     c->shuffle = fi.shuffle;
     c->clevel = fi.clevel;
-    std::vector<const uint8_t *> ptrs;
-    std::vector<int64_t> lens;
-    for (auto &pr : chunks) { ptrs.push_back(frame + pr.first); lens.push_back(pr.second); }
-    rc = upload_chunks(ctx, c, ptrs.data(), lens.data());
-    if (INA_FAILED(rc)) iarray_container_free(ctx, container);
-    return rc;
+    // the chunks occupy one region of the frame: copy it once, keep the frame's offsets
+    int64_t lo = INT64_MAX, hi = 0;
+    for (auto &pr : chunks) {
+        if (pr.second > c->geom.chunk_nbytes + 64) { iarray_container_free(ctx, container); return rc_err(IARRAY_ERR_BLOSC_FAILED); }
+        lo = std::min(lo, pr.first);
+        hi = std::max(hi, pr.first + (int64_t)pr.second);
+    }
+    ChunkStore &s = *c->store;
+    if (chunks.empty()) lo = hi = 0;
+    if (!s.buf.allocate((size_t)std::max<int64_t>(hi - lo, 1), s.device)) {
+        iarray_container_free(ctx, container);
+        return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    }
+    if (hi > lo) cudaMemcpyAsync(s.buf.p, frame + lo, (size_t)(hi - lo), cudaMemcpyHostToDevice, ctx->stream);
+    s.off.clear();
+    s.len.clear();
+    for (auto &pr : chunks) { s.off.push_back(pr.first - lo); s.len.push_back(pr.second); }
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess || !s.upload_index()) {
+        iarray_container_free(ctx, container);
+        return rc_err(IARRAY_ERR_GPU_FAILED);
+    }
+    return INA_SUCCESS;
 }
 
 static ina_rc_t write_file(const char *path, const std::vector<uint8_t> &f)

@@ -401,8 +401,102 @@ __device__ __forceinline__ bool item_pos(const Geom &g, int64_t c, int64_t b, in
     return row < g.shape[0] && col < g.shape[1];
 }
 
-// D2: unshuffle one tile of TILE items of one block and scatter it to the dense array.
-__global__ void __launch_bounds__(256) k_scatter(Geom g, const uint8_t *__restrict__ ch,
+// True when every item of block b of chunk c is a logical item (no chunk or array
+// padding inside the block), block rows hold whole groups of 4 items and items are 4 or
+// 8 bytes: such blocks take the word-level fast paths below.
+__device__ __forceinline__ bool block_fast(const Geom &g, int64_t c, int64_t b)
+{
+    if ((g.block[1] & 3) || (g.itemsize != 4 && g.itemsize != 8)) return false;
+    const int64_t ci0 = c / g.cgrid[1], ci1 = c - ci0 * g.cgrid[1];
+    const int64_t bi0 = b / g.bgrid[1], bi1 = b - bi0 * g.bgrid[1];
+    const int64_t r1 = (bi0 + 1) * g.block[0], c1 = (bi1 + 1) * g.block[1];
+    return r1 <= g.chunk[0] && c1 <= g.chunk[1] && ci0 * g.chunk[0] + r1 <= g.shape[0] &&
+           ci1 * g.chunk[1] + c1 <= g.shape[1];
+}
+
+// 4x4 byte transpose: o_i holds byte i of a, b, c, d (in that order).
+__device__ __forceinline__ void transpose4x4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t &o0, uint32_t &o1,
+                                             uint32_t &o2, uint32_t &o3)
+{
+    const uint32_t ab_lo = __byte_perm(a, b, 0x5140), ab_hi = __byte_perm(a, b, 0x7362);
+    const uint32_t cd_lo = __byte_perm(c, d, 0x5140), cd_hi = __byte_perm(c, d, 0x7362);
+    o0 = __byte_perm(ab_lo, cd_lo, 0x5410);
+    o1 = __byte_perm(ab_lo, cd_lo, 0x7632);
+    o2 = __byte_perm(ab_hi, cd_hi, 0x5410);
+    o3 = __byte_perm(ab_hi, cd_hi, 0x7632);
+}
+
+// 4 bytes at any address p < lim - 3: two aligned word loads and a funnel shift when the
+// second word still lies below lim, byte loads otherwise.
+__device__ __forceinline__ uint32_t ld4_any(const uint8_t *p, const uint8_t *lim)
+{
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p) & ~uintptr_t(3);
+    if (a + 8 <= reinterpret_cast<uintptr_t>(lim)) {
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(a);
+        return __funnelshift_r(__ldg(w), __ldg(w + 1), (uint32_t)(reinterpret_cast<uintptr_t>(p) & 3) * 8);
+    }
+    return (uint32_t)__ldg(p) | ((uint32_t)__ldg(p + 1) << 8) | ((uint32_t)__ldg(p + 2) << 16) |
+           ((uint32_t)__ldg(p + 3) << 24);
+}
+
+// D2 fast path: one CTA per interior, shuffled, split block; each thread rebuilds 4
+// consecutive items from one 4-byte word per byte plane (read in place from raw streams
+// or the LZ4 scratch) and writes them to the dense row.
+template <int TS>
+__global__ void __launch_bounds__(256) k_scatter_fast(Geom g, const uint8_t *__restrict__ ch, const uint8_t *ch_end,
+                                                      const BlockDesc *__restrict__ bd,
+                                                      const StreamDesc *__restrict__ sd,
+                                                      const uint8_t *__restrict__ scratch, const uint8_t *scratch_end,
+                                                      uint8_t *__restrict__ out, int64_t ld)
+{
+    const int64_t nbl = g.nchunks * g.nblocks;
+    const int qpr = (int)(g.block[1] / 4), nq = (int)(g.blockn / 4);
+    for (int64_t t = blockIdx.x; t < nbl; t += gridDim.x) {
+        const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
+        const BlockDesc d = bd[t];
+        if (d.mode != BM_SHUFFLED || d.nstreams != TS || !block_fast(g, c, b)) continue;
+        const uint8_t *base[TS];
+        const uint8_t *lim[TS];
+        uint32_t fill[TS];
+#pragma unroll
+        for (int j = 0; j < TS; j++) {
+            const StreamDesc q = sd[t * 8 + j];
+            fill[j] = q.kind == SK_RUN ? (uint32_t)q.len * 0x01010101u : 0u;
+            if (q.kind == SK_RAW) { base[j] = ch + q.src; lim[j] = ch_end; }
+            else if (q.kind == SK_LZ4) { base[j] = scratch + t * g.blocksize + (int64_t)j * d.neblock; lim[j] = scratch_end; }
+            else { base[j] = nullptr; lim[j] = nullptr; }
+        }
+        const int64_t ci0 = c / g.cgrid[1], ci1 = c - ci0 * g.cgrid[1];
+        const int64_t bi0 = b / g.bgrid[1], bi1 = b - bi0 * g.bgrid[1];
+        const int64_t row0 = ci0 * g.chunk[0] + bi0 * g.block[0], col0 = ci1 * g.chunk[1] + bi1 * g.block[1];
+        for (int qd = threadIdx.x; qd < nq; qd += blockDim.x) {
+            const int i0 = qd * 4, r = qd / qpr, cc = (qd - r * qpr) * 4;
+            uint32_t w[TS];
+#pragma unroll
+            for (int j = 0; j < TS; j++) w[j] = base[j] ? ld4_any(base[j] + i0, lim[j]) : fill[j];
+            uint8_t *o = out + ((row0 + r) * ld + col0 + cc) * TS;
+            uint32_t v0, v1, v2, v3;
+            transpose4x4(w[0], w[1], w[2], w[3], v0, v1, v2, v3);
+            if constexpr (TS == 8) {
+                uint32_t h0, h1, h2, h3;
+                transpose4x4(w[4], w[5], w[6], w[7], h0, h1, h2, h3);
+                uint64_t *o8 = reinterpret_cast<uint64_t *>(o);
+                o8[0] = ((uint64_t)h0 << 32) | v0;
+                o8[1] = ((uint64_t)h1 << 32) | v1;
+                o8[2] = ((uint64_t)h2 << 32) | v2;
+                o8[3] = ((uint64_t)h3 << 32) | v3;
+            } else {
+                uint32_t *o4 = reinterpret_cast<uint32_t *>(o);
+                o4[0] = v0; o4[1] = v1; o4[2] = v2; o4[3] = v3;
+            }
+        }
+    }
+}
+
+// D2 general path: unshuffle one tile of TILE items of one block through shared memory
+// and scatter it to the dense array (padded edge blocks, other item sizes, plain and
+// special chunks).  With skip_fast, blocks the fast path handles are skipped.
+__global__ void __launch_bounds__(256) k_scatter(Geom g, bool skip_fast, const uint8_t *__restrict__ ch,
                                                  const BlockDesc *__restrict__ bd, const StreamDesc *__restrict__ sd,
                                                  const uint8_t *__restrict__ scratch, uint8_t *__restrict__ out, int64_t ld)
 {
@@ -415,6 +509,7 @@ __global__ void __launch_bounds__(256) k_scatter(Geom g, const uint8_t *__restri
         const int cnt = (int)min((int64_t)TILE, g.blockn - i0);
         const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
         const BlockDesc d = bd[t];
+        if (skip_fast && d.mode == BM_SHUFFLED && d.nstreams == ts && block_fast(g, c, b)) continue;
         const StreamDesc *s = sd + t * 8;
         const uint8_t *blk_scratch = scratch + t * g.blocksize;
         if (d.mode == BM_SHUFFLED) {
@@ -469,10 +564,46 @@ __global__ void __launch_bounds__(256) k_scatter(Geom g, const uint8_t *__restri
 }
 
 // ============================================================================ encode
-// E1: dense -> byte-plane image (shuffled: plane j holds byte j of every item;
-// plain: items back to back).  Padding items are zero, as in Caterva.
-__global__ void __launch_bounds__(256) k_gather(Geom g, const uint8_t *__restrict__ in, int64_t ld, bool shuffle,
-                                                uint8_t *__restrict__ img)
+// E1 fast path: interior blocks, shuffle on; each thread reads 4 consecutive items of a
+// block row and writes one 4-byte word into each byte plane of the image.
+template <int TS>
+__global__ void __launch_bounds__(256) k_gather_fast(Geom g, const uint8_t *__restrict__ in, int64_t ld,
+                                                     uint8_t *__restrict__ img)
+{
+    const int64_t nbl = g.nchunks * g.nblocks;
+    const int qpr = (int)(g.block[1] / 4), nq = (int)(g.blockn / 4);
+    for (int64_t t = blockIdx.x; t < nbl; t += gridDim.x) {
+        const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
+        if (!block_fast(g, c, b)) continue;
+        const int64_t ci0 = c / g.cgrid[1], ci1 = c - ci0 * g.cgrid[1];
+        const int64_t bi0 = b / g.bgrid[1], bi1 = b - bi0 * g.bgrid[1];
+        const int64_t row0 = ci0 * g.chunk[0] + bi0 * g.block[0], col0 = ci1 * g.chunk[1] + bi1 * g.block[1];
+        uint8_t *blk = img + t * g.blocksize;
+        for (int qd = threadIdx.x; qd < nq; qd += blockDim.x) {
+            const int i0 = qd * 4, r = qd / qpr, cc = (qd - r * qpr) * 4;
+            const uint8_t *src = in + ((row0 + r) * ld + col0 + cc) * TS;
+            uint32_t o[TS];
+            if constexpr (TS == 8) {
+                const uint64_t *s8 = reinterpret_cast<const uint64_t *>(src);
+                const uint64_t x0 = __ldg(s8), x1 = __ldg(s8 + 1), x2 = __ldg(s8 + 2), x3 = __ldg(s8 + 3);
+                transpose4x4((uint32_t)x0, (uint32_t)x1, (uint32_t)x2, (uint32_t)x3, o[0], o[1], o[2], o[3]);
+                transpose4x4((uint32_t)(x0 >> 32), (uint32_t)(x1 >> 32), (uint32_t)(x2 >> 32), (uint32_t)(x3 >> 32),
+                             o[4], o[5], o[6], o[7]);
+            } else {
+                const uint32_t *s4 = reinterpret_cast<const uint32_t *>(src);
+                transpose4x4(__ldg(s4), __ldg(s4 + 1), __ldg(s4 + 2), __ldg(s4 + 3), o[0], o[1], o[2], o[3]);
+            }
+#pragma unroll
+            for (int j = 0; j < TS; j++) *reinterpret_cast<uint32_t *>(blk + (int64_t)j * g.blockn + i0) = o[j];
+        }
+    }
+}
+
+// E1 general path: dense -> byte-plane image (shuffled: plane j holds byte j of every
+// item; plain: items back to back).  Padding items are zero, as in Caterva.  With
+// skip_fast, blocks the fast path handles are skipped.
+__global__ void __launch_bounds__(256) k_gather(Geom g, bool skip_fast, const uint8_t *__restrict__ in, int64_t ld,
+                                                bool shuffle, uint8_t *__restrict__ img)
 {
     __shared__ __align__(16) uint8_t planes[8 * TILE];
     const int ts = g.itemsize;
@@ -482,6 +613,7 @@ __global__ void __launch_bounds__(256) k_gather(Geom g, const uint8_t *__restric
         const int64_t t = w / tpb, i0 = (w - t * tpb) * TILE;
         const int cnt = (int)min((int64_t)TILE, g.blockn - i0);
         const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
+        if (skip_fast && block_fast(g, c, b)) continue;
         for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
             int64_t row, col;
             uint64_t v = 0;
@@ -554,45 +686,70 @@ __device__ int warp_lz4_compress(const uint8_t *__restrict__ src, int n, uint8_t
     if (n < 13) goto last_literals;
     if (lane == 0) TPUT(lz_hash(src, small), 0);
     __syncwarp();
+    {
+    // One 32-lane step evaluates consecutive table operations of the serial algorithm.
+    // Right after a match (`after`), lane 0 is the insert of ip-2, lane 1 the immediate
+    // re-match probe at ip, and lanes 2.. the first probes of the search that follows
+    // from ip+1; otherwise all lanes are search probes.  Insertions happen in increasing
+    // position order, so each probe sees the latest earlier insert of its hash: the
+    // table before the step, or a lower lane of the same hash within it.
+    int p0 = 1;
+    int64_t t0 = 0;
+    bool after = false;
     for (;;) {
-        {   // search: 32 probes per step
-            const int p0 = ip;
-            int64_t t0 = 0;
-            bool found = false;
-            for (;;) {
-                const int64_t t = t0 + lane;
-                // the step is 1 for the first 65 probes: positions are p0 + t there
-                const int64_t p = t0 + 32 <= 64 ? p0 + t : p0 + probe_offset(t);
-                const int64_t pn = t0 + 32 <= 64 ? p + 1 : p0 + probe_offset(t + 1);
-                const bool valid = pn <= mfl1;
-                const uint32_t h = valid ? lz_hash(src + p, small) : (0x80000000u | (uint32_t)lane);
-                const uint32_t ctab = valid ? TGET(h) : 0u;
-                const unsigned peers = __match_any_sync(FULLMASK, h);
-                const unsigned lower = peers & ((1u << lane) - 1u);
-                const int srcl = lower ? 31 - __clz(lower) : lane;
-                const int pl = __shfl_sync(FULLMASK, (int)p, srcl);
-                const uint32_t cand = lower ? (uint32_t)pl : ctab;
-                const bool m = valid && (small || cand + 65535u >= (uint32_t)p) && ld4u(src + cand) == ld4u(src + p);
-                const unsigned mm = __ballot_sync(FULLMASK, m), em = __ballot_sync(FULLMASK, !valid);
-                const int W = mm ? __ffs(mm) - 1 : 32, E = em ? __ffs(em) - 1 : 32;
-                const int lastw = min(W, E - 1);
-                __syncwarp();
-                if (lane <= lastw) {
-                    const unsigned upto = (lastw >= 31) ? FULLMASK : ((2u << lastw) - 1u);
-                    const unsigned higher = peers & ~((2u << lane) - 1u) & upto;
-                    if (!higher) TPUT(h, (uint32_t)p);
-                }
-                __syncwarp();
-                if (W < E) {
-                    ip = __shfl_sync(FULLMASK, (int)p, W);
-                    mt = (int)__shfl_sync(FULLMASK, cand, W);
-                    found = true;
-                    break;
-                }
-                if (E < 32) break;
-                t0 += 32;
+        bool rematch = false;
+        for (;;) {
+            int kind = 2;                       // 0 insert only, 1 re-match probe, 2 search probe
+            int64_t t = t0 + lane;
+            if (after) {
+                kind = lane == 0 ? 0 : (lane == 1 ? 1 : 2);
+                t = t0 + lane - 2;
             }
-            if (!found) goto last_literals;
+            int64_t p;
+            bool valid;
+            if (kind == 0) { p = ip - 2; valid = true; }
+            else if (kind == 1) { p = ip; valid = true; }
+            else {
+                // the step is 1 for the first 66 probes: positions are p0 + t there
+                const bool dense = t0 + 32 <= 65;
+                p = dense ? p0 + t : p0 + probe_offset(t);
+                const int64_t pn = dense ? p + 1 : p0 + probe_offset(t + 1);
+                valid = pn <= mfl1;
+            }
+            const bool probe = kind != 0 && valid;
+            const uint32_t h = valid ? lz_hash(src + p, small) : (0x80000000u | (uint32_t)lane);
+            const uint32_t ctab = probe ? TGET(h) : 0u;
+            const unsigned peers = __match_any_sync(FULLMASK, h);
+            const unsigned lower = peers & ((1u << lane) - 1u);
+            const int srcl = lower ? 31 - __clz(lower) : lane;
+            const int pl = __shfl_sync(FULLMASK, (int)p, srcl);
+            const uint32_t cand = lower ? (uint32_t)pl : ctab;
+            const bool m = probe && (small || cand + 65535u >= (uint32_t)p) && ld4u(src + cand) == ld4u(src + p);
+            const unsigned mm = __ballot_sync(FULLMASK, m), em = __ballot_sync(FULLMASK, kind != 0 && !valid);
+            const int W = mm ? __ffs(mm) - 1 : 32, E = em ? __ffs(em) - 1 : 32;
+            const int lastw = min(W, E - 1);
+            __syncwarp();
+            if (lane <= lastw) {
+                const unsigned upto = (lastw >= 31) ? FULLMASK : ((2u << lastw) - 1u);
+                const unsigned higher = peers & ~((2u << lane) - 1u) & upto;
+                if (!higher) TPUT(h, (uint32_t)p);
+            }
+            __syncwarp();
+            if (W < E) {
+                ip = __shfl_sync(FULLMASK, (int)p, W);
+                mt = (int)__shfl_sync(FULLMASK, cand, W);
+                rematch = after && W == 1;
+                break;
+            }
+            if (E < 32) goto last_literals;
+            t0 += after ? 30 : 32;
+            after = false;
+        }
+        if (rematch) {   // a match right at the previous match's end: no literals
+            token_pos = op;
+            token_val = 0;
+            op += 1;
+            goto next_match;
         }
         for (;;) {   // extend the match backwards
             const int k = lane + 1;
@@ -649,23 +806,10 @@ __device__ int warp_lz4_compress(const uint8_t *__restrict__ src, int n, uint8_t
         }
         anchor = ip;
         if (ip >= mfl1) break;
-        if (lane == 0) TPUT(lz_hash(src + ip - 2, small), ip - 2);
-        __syncwarp();
-        {   // immediate re-match at ip
-            const uint32_t h = lz_hash(src + ip, small);
-            const uint32_t midx = TGET(h);
-            __syncwarp();
-            if (lane == 0) TPUT(h, ip);
-            __syncwarp();
-            if ((small || midx + 65535u >= (uint32_t)ip) && ld4u(src + midx) == ld4u(src + ip)) {
-                token_pos = op;
-                token_val = 0;
-                op += 1;
-                mt = (int)midx;
-                goto next_match;
-            }
-        }
-        ip++;
+        after = true;
+        p0 = ip + 1;
+        t0 = 0;
+    }
     }
 last_literals:
     {
@@ -856,11 +1000,11 @@ static int sm_count()
     return n;
 }
 
-int decode_container(const Geom &g, const uint8_t *d_chunks, const int64_t *d_off, const int32_t *d_len,
+int decode_container(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, const int64_t *d_off, const int32_t *d_len,
                      void *out, int64_t ld, cudaStream_t st)
 {
     DecodeWork w;
-    int r = decode_launch(g, d_chunks, d_off, d_len, out, ld, st, &w);
+    int r = decode_launch(g, d_chunks, chunks_bytes, d_off, d_len, out, ld, st, &w);
     if (r) return r;
     return decode_finish(&w, st);
 }
@@ -873,7 +1017,7 @@ int decode_finish(DecodeWork *w, cudaStream_t st)
     return h_err;
 }
 
-int decode_launch(const Geom &g, const uint8_t *d_chunks, const int64_t *d_off, const int32_t *d_len, void *out,
+int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, const int64_t *d_off, const int32_t *d_len, void *out,
                   int64_t ld, cudaStream_t st, DecodeWork *w)
 {
     int dev = 0;
@@ -911,8 +1055,20 @@ int decode_launch(const Geom &g, const uint8_t *d_chunks, const int64_t *d_off, 
         const int64_t tpb = (g.blockn + TILE - 1) / TILE;
         const int64_t nwork = nbl * tpb;
         const int64_t blocks = std::min<int64_t>(nwork, (int64_t)sms * 8);
+        const bool fast = g.itemsize == 4 || g.itemsize == 8;
+        if (fast) {
+            const int64_t fb = std::min<int64_t>(nbl, (int64_t)sms * 8);
+            const uint8_t *cend = d_chunks + chunks_bytes, *send = scratch.as<uint8_t>() + nbl * g.blocksize;
+            IAB_LAUNCHED(1);
+            if (g.itemsize == 8)
+                k_scatter_fast<8><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
+                    g, d_chunks, cend, bd.as<BlockDesc>(), sd.as<StreamDesc>(), scratch.as<uint8_t>(), send, (uint8_t *)out, ld);
+            else
+                k_scatter_fast<4><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
+                    g, d_chunks, cend, bd.as<BlockDesc>(), sd.as<StreamDesc>(), scratch.as<uint8_t>(), send, (uint8_t *)out, ld);
+        }
         IAB_LAUNCHED(1);
-        k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, d_chunks, bd.as<BlockDesc>(), sd.as<StreamDesc>(),
+        k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, fast, d_chunks, bd.as<BlockDesc>(), sd.as<StreamDesc>(),
                                                                         scratch.as<uint8_t>(), (uint8_t *)out, ld);
     }
     return 0;
@@ -945,7 +1101,14 @@ int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, in
         const int64_t tpb = (g.blockn + TILE - 1) / TILE;
         const int64_t blocks = std::min<int64_t>(nbl * tpb, (int64_t)sms * 8);
         IAB_LAUNCHED(1);
-        k_gather<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, (const uint8_t *)in, ld, shuffle, img.as<uint8_t>());
+        const bool fast = shuffle && (ts == 4 || ts == 8);
+        if (fast) {
+            const int64_t fb = std::min<int64_t>(nbl, (int64_t)sms * 8);
+            IAB_LAUNCHED(1);
+            if (ts == 8) k_gather_fast<8><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(g, (const uint8_t *)in, ld, img.as<uint8_t>());
+            else k_gather_fast<4><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(g, (const uint8_t *)in, ld, img.as<uint8_t>());
+        }
+        k_gather<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, fast, (const uint8_t *)in, ld, shuffle, img.as<uint8_t>());
     }
     {
         static bool attr = false;

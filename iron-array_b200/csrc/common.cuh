@@ -121,7 +121,7 @@ struct CodecStats { int32_t err; };
 
 // Decode `g.nchunks` chunks (buffer d_chunks, offsets d_off) into a dense row-major
 // array `out` with leading dimension `ld` items.  Returns a DevErr (synchronises).
-int decode_container(const Geom &g, const uint8_t *d_chunks, const int64_t *d_off,
+int decode_container(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, const int64_t *d_off,
                      const int32_t *d_len, void *out, int64_t ld, cudaStream_t st);
 
 // Asynchronous form: decode_launch enqueues the kernels on `st` (work buffers held in
@@ -129,7 +129,7 @@ int decode_container(const Geom &g, const uint8_t *d_chunks, const int64_t *d_of
 struct DecodeWork {
     DevBuf bd, sd, jobs, scratch, counters;
 };
-int decode_launch(const Geom &g, const uint8_t *d_chunks, const int64_t *d_off, const int32_t *d_len,
+int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, const int64_t *d_off, const int32_t *d_len,
                   void *out, int64_t ld, cudaStream_t st, DecodeWork *w);
 int decode_finish(DecodeWork *w, cudaStream_t st);
 

@@ -58,15 +58,26 @@ std::vector<uint8_t> memcpyed_chunk(const uint8_t *data, int32_t nbytes, int typ
     return c;
 }
 
-bool write_frame(const FrameInfo &fi, const std::vector<const uint8_t *> &chunks, const std::vector<int32_t> &lens,
-                 std::vector<uint8_t> *out)
+static const uint8_t kTrailer[35] = {0x94, 0x01, 0x93, 0xcd, 0x00, 0x06, 0xde, 0x00, 0x00, 0xdc, 0x00, 0x00,
+                                     0xce, 0x00, 0x00, 0x00, 0x23, 0xd8, 0x00};
+
+std::vector<uint8_t> frame_tail(const std::vector<int32_t> &lens)
 {
-    std::vector<uint8_t> &h = *out;
-    h.clear();
+    std::vector<int64_t> offsets;
+    int64_t acc = 0;
+    for (int32_t l : lens) { offsets.push_back(acc); acc += l; }
+    std::vector<uint8_t> t = memcpyed_chunk(reinterpret_cast<const uint8_t *>(offsets.data()),
+                                            (int32_t)(offsets.size() * 8), 8);
+    // trailer: [version, [vlmeta index size, {}, []], trailer length, fingerprint]
+    t.insert(t.end(), kTrailer, kTrailer + 35);
+    return t;
+}
+
+std::vector<uint8_t> frame_header(const FrameInfo &fi, int64_t data_cbytes, int64_t nchunks)
+{
+    std::vector<uint8_t> h;
     const std::vector<uint8_t> cat = caterva_meta(fi.ndim, fi.shape, fi.chunk, fi.block);
     const std::vector<uint8_t> ia = iarray_meta(fi.dtype);
-    int64_t data_cbytes = 0;
-    for (int32_t l : lens) data_cbytes += l;
     h.push_back(0x9e);
     h.push_back(0xa8);
     const char magic[8] = {'b', '2', 'f', 'r', 'a', 'm', 'e', 0};
@@ -119,22 +130,20 @@ bool write_frame(const FrameInfo &fi, const std::vector<const uint8_t *> &chunks
     }
     const uint32_t header_size = (uint32_t)h.size();
     for (int k = 0; k < 4; k++) h[11 + k] = (uint8_t)(header_size >> (8 * (3 - k)));
-    std::vector<int64_t> offsets;
-    int64_t acc = 0;
-    for (size_t i = 0; i < chunks.size(); i++) {
-        offsets.push_back(acc);
-        h.insert(h.end(), chunks[i], chunks[i] + lens[i]);
-        acc += lens[i];
-    }
-    const std::vector<uint8_t> oc = memcpyed_chunk(reinterpret_cast<const uint8_t *>(offsets.data()),
-                                                   (int32_t)(offsets.size() * 8), 8);
-    h.insert(h.end(), oc.begin(), oc.end());
-    // trailer: [version, [vlmeta index size, {}, []], trailer length, fingerprint]
-    const uint8_t trailer[35] = {0x94, 0x01, 0x93, 0xcd, 0x00, 0x06, 0xde, 0x00, 0x00, 0xdc, 0x00, 0x00,
-                                 0xce, 0x00, 0x00, 0x00, 0x23, 0xd8, 0x00};
-    h.insert(h.end(), trailer, trailer + 35);
-    const uint64_t fs = h.size();
+    const uint64_t fs = (uint64_t)h.size() + (uint64_t)data_cbytes + 32 + 8 * (uint64_t)nchunks + 35;
     for (int k = 0; k < 8; k++) h[16 + k] = (uint8_t)(fs >> (8 * (7 - k)));
+    return h;
+}
+
+bool write_frame(const FrameInfo &fi, const std::vector<const uint8_t *> &chunks, const std::vector<int32_t> &lens,
+                 std::vector<uint8_t> *out)
+{
+    int64_t data_cbytes = 0;
+    for (int32_t l : lens) data_cbytes += l;
+    *out = frame_header(fi, data_cbytes, (int64_t)lens.size());
+    for (size_t i = 0; i < chunks.size(); i++) out->insert(out->end(), chunks[i], chunks[i] + lens[i]);
+    const std::vector<uint8_t> t = frame_tail(lens);
+    out->insert(out->end(), t.begin(), t.end());
     return true;
 }
 

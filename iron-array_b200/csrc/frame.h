@@ -22,6 +22,10 @@ struct FrameInfo {
 
 bool write_frame(const FrameInfo &fi, const std::vector<const uint8_t *> &chunks, const std::vector<int32_t> &lens,
                  std::vector<uint8_t> *out);
+// The frame pieces around the chunk bytes: header (depends on the total frame size) and
+// tail (offsets chunk + trailer).  A frame is header | chunks back to back | tail.
+std::vector<uint8_t> frame_header(const FrameInfo &fi, int64_t data_cbytes, int64_t nchunks);
+std::vector<uint8_t> frame_tail(const std::vector<int32_t> &lens);
 // Parses a frame; `chunks` receives (byte offset in the frame, cbytes) in logical order.
 bool read_frame(const uint8_t *buf, size_t n, FrameInfo *fi, std::vector<std::pair<int64_t, int32_t>> *chunks,
                 std::string *why);

@@ -73,6 +73,8 @@ struct CrtConst {
     double inv_mod[MAX_MODULI];
     float inv_modf[MAX_MODULI];
     uint64_t w_lo[MAX_MODULI], w_hi[MAX_MODULI];   // CRT basis w_l = (P/m_l) * ((P/m_l)^-1 mod m_l) mod P
+    uint32_t w32[MAX_MODULI][4];                   // the same, as 32-bit limbs (least significant first)
+    uint32_t p32[4], h32[4];                       // P and floor(P/2) as 32-bit limbs
     uint64_t p_lo, p_hi, h_lo, h_hi;               // P and floor(P/2)
     double inv_p;                                  // 1/P (rounded)
     double log2p;
@@ -104,12 +106,17 @@ static bool build_crt(int L, CrtConst *c)
         const u128 w = (Ml * (u128)inv) % P;
         c->w_lo[l] = (uint64_t)w;
         c->w_hi[l] = (uint64_t)(w >> 64);
+        for (int k = 0; k < 4; k++) c->w32[l][k] = (uint32_t)(w >> (32 * k));
     }
     c->p_lo = (uint64_t)P;
     c->p_hi = (uint64_t)(P >> 64);
     const u128 H = P / 2;
     c->h_lo = (uint64_t)H;
     c->h_hi = (uint64_t)(H >> 64);
+    for (int k = 0; k < 4; k++) {
+        c->p32[k] = (uint32_t)(P >> (32 * k));
+        c->h32[k] = (uint32_t)(H >> (32 * k));
+    }
     c->inv_p = 1.0 / ((double)c->p_hi * 18446744073709551616.0 + (double)c->p_lo);
     c->log2p = lp;
     return true;
@@ -411,70 +418,109 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
 }
 
 // ============================================================================ reconstruction
-// C_ij = 2^-(sA_i + sB_j) * centred( sum_l r_l w_l mod P ).
+// X = sum_l r_l w_l mod P, centred into (-P/2, P/2], as a float64 (32-bit limbs: every
+// r_l * limb product is one 32x32->64 multiply-add; L * 2^8 * 2^32 < 2^45 per limb).
+__device__ __forceinline__ double crt_value(const uint32_t (&w)[16], int u, int L)
+{
+    uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+    for (int l = 0; l < 16; l++) {
+        if (l < L) {
+            const uint64_t v = (w[l] >> (8 * u)) & 0xffu;
+            a0 += v * c_crt.w32[l][0];
+            a1 += v * c_crt.w32[l][1];
+            a2 += v * c_crt.w32[l][2];
+            a3 += v * c_crt.w32[l][3];
+        }
+    }
+    // S in five 32-bit limbs
+    uint32_t s0 = (uint32_t)a0;
+    a1 += a0 >> 32;
+    uint32_t s1 = (uint32_t)a1;
+    a2 += a1 >> 32;
+    uint32_t s2 = (uint32_t)a2;
+    a3 += a2 >> 32;
+    uint32_t s3 = (uint32_t)a3;
+    uint32_t s4 = (uint32_t)(a3 >> 32);
+    // quotient estimate (within one of floor(S / P)), then X = S - qP with a signed carry
+    const double sd = ((((double)s4 * 4294967296.0 + (double)s3) * 4294967296.0 + (double)s2) * 4294967296.0 +
+                       (double)s1) * 4294967296.0 + (double)s0;
+    const uint32_t q = (uint32_t)(sd * c_crt.inv_p);
+    int64_t x[5];
+    int64_t carry = 0;
+    const uint32_t sv[4] = {s0, s1, s2, s3};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const uint64_t m = (uint64_t)q * c_crt.p32[k];
+        const int64_t d = (int64_t)sv[k] + carry - (int64_t)(m & 0xffffffffu);
+        x[k] = d & 0xffffffff;
+        carry = (d >> 32) - (int64_t)(m >> 32);
+    }
+    x[4] = (int64_t)s4 + carry;                  // sign of X lives here
+    // one correction either way, then centre
+    auto add_p = [&](int sgn) {
+        int64_t c = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int64_t d = x[k] + sgn * (int64_t)c_crt.p32[k] + c;
+            x[k] = d & 0xffffffff;
+            c = d >> 32;
+        }
+        x[4] += c;
+    };
+    auto ge = [&](const uint32_t (&v)[4]) -> bool {   // X >= v (X non-negative, v < 2^128)
+        if (x[4] > 0) return true;
+        for (int k = 3; k >= 0; k--) {
+            if ((uint64_t)x[k] != v[k]) return (uint64_t)x[k] > v[k];
+        }
+        return true;
+    };
+    if (x[4] < 0) add_p(1);
+    else if (ge(c_crt.p32)) add_p(-1);
+    bool neg = false;
+    if (!ge(c_crt.h32)) {
+        // X <= P/2 - 1 ... keep
+    } else {
+        bool eq = x[4] == 0;
+        for (int k = 0; k < 4 && eq; k++) eq = (uint64_t)x[k] == c_crt.h32[k];
+        if (!eq) {       // X > floor(P/2): use X - P < 0, magnitude P - X
+            int64_t c = 0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int64_t d = (int64_t)c_crt.p32[k] - x[k] + c;
+                x[k] = d & 0xffffffff;
+                c = d >> 32;
+            }
+            x[4] = 0;
+            neg = true;
+        }
+    }
+    const double v = (((double)x[3] * 4294967296.0 + (double)x[2]) * 4294967296.0 + (double)x[1]) * 4294967296.0 +
+                     (double)x[0];
+    return neg ? -v : v;
+}
+
+// C_ij = 2^-(sA_i + sB_j) * centred( sum_l r_l w_l mod P ); four entries per thread.
 __global__ void __launch_bounds__(256) k_crt(int M, int N, const uint8_t *__restrict__ R, int64_t ldr,
                                              const int *__restrict__ sA, const int *__restrict__ sB,
                                              double *__restrict__ C, int64_t ldc)
 {
     const int L = c_crt.L;
     const int64_t plane = (int64_t)M * ldr;
-    const int64_t total = (int64_t)M * N;
+    const int nq = (N + 3) / 4;
+    const int64_t total = (int64_t)M * nq;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(e / N), j = (int)(e - (int64_t)i * N);
-        const uint8_t *rp = R + (int64_t)i * ldr + j;
-        // S = sum_l r_l w_l < L * 256 * P needs up to 2^134: three 64-bit limbs
-        uint64_t s0 = 0, s1 = 0, s2 = 0;
-        for (int l = 0; l < L; l++) {
-            const uint64_t r = rp[l * plane];
-            const uint64_t t0 = r * c_crt.w_lo[l], c0 = __umul64hi(r, c_crt.w_lo[l]);
-            const uint64_t t1 = r * c_crt.w_hi[l], c1 = __umul64hi(r, c_crt.w_hi[l]);
-            s0 += t0;
-            const uint64_t k0 = s0 < t0 ? 1 : 0;
-            const uint64_t u1 = t1 + c0;                    // no overflow: t1 < 2^64 - 2^8, c0 < 2^8
-            const uint64_t k1a = u1 < t1 ? 1 : 0;
-            s1 += u1;
-            const uint64_t k1 = (s1 < u1 ? 1 : 0) + k1a;
-            s1 += k0;
-            const uint64_t k2 = (s1 < k0 ? 1 : 0);
-            s2 += c1 + k1 + k2;
+        const int i = (int)(e / nq), j0 = (int)(e - (int64_t)i * nq) * 4;
+        const uint8_t *rp = R + (int64_t)i * ldr + j0;
+        uint32_t w[16];
+#pragma unroll
+        for (int l = 0; l < 16; l++) w[l] = l < L ? *reinterpret_cast<const uint32_t *>(rp + l * plane) : 0u;  // ldr % 16 == 0
+        const int si = sA[i];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int j = j0 + u;
+            if (j < N) C[(int64_t)i * ldc + j] = ldexp(crt_value(w, u, L), -(si + sB[j]));
         }
-        // reduce modulo P: quotient estimate from the leading bits, then one correction
-        const double sd = ((double)s2 * 18446744073709551616.0 + (double)s1) * 18446744073709551616.0 + (double)s0;
-        const uint64_t qe = (uint64_t)(sd * c_crt.inv_p);
-        // q * P as three limbs
-        const uint64_t q0 = qe * c_crt.p_lo, q0h = __umul64hi(qe, c_crt.p_lo);
-        const uint64_t q1l = qe * c_crt.p_hi, q1h = __umul64hi(qe, c_crt.p_hi);
-        const uint64_t q1 = q1l + q0h;
-        const uint64_t q2 = q1h + (q1 < q1l ? 1 : 0);
-        uint64_t xlo = s0 - q0;
-        const uint64_t b0 = s0 < q0 ? 1 : 0;
-        const uint64_t m1 = s1 - q1;
-        const uint64_t b1 = (s1 < q1 ? 1 : 0) + (m1 < b0 ? 1 : 0);
-        // X = S - qP lies in [-P, 2P) with P < 2^126, so the two low limbs hold it in two's
-        // complement (the third limb is its sign extension)
-        uint64_t xhi = m1 - b0;
-        (void)s2; (void)q2; (void)b1;
-        if ((int64_t)xhi < 0) {                                  // estimate one too large
-            const uint64_t t = xlo + c_crt.p_lo;
-            xhi += c_crt.p_hi + (t < xlo ? 1 : 0);
-            xlo = t;
-        } else if (xhi > c_crt.p_hi || (xhi == c_crt.p_hi && xlo >= c_crt.p_lo)) {   // one too small
-            const uint64_t t = xlo - c_crt.p_lo;
-            xhi -= c_crt.p_hi + (xlo < c_crt.p_lo ? 1 : 0);
-            xlo = t;
-        }
-        // centre into (-P/2, P/2]
-        bool neg = false;
-        if (xhi > c_crt.h_hi || (xhi == c_crt.h_hi && xlo > c_crt.h_lo)) {
-            // x - P < 0: magnitude P - x
-            const uint64_t t = c_crt.p_lo - xlo;
-            xhi = c_crt.p_hi - xhi - (c_crt.p_lo < xlo ? 1 : 0);
-            xlo = t;
-            neg = true;
-        }
-        double v = (double)xhi * 18446744073709551616.0 + (double)xlo;
-        v = ldexp(neg ? -v : v, -(sA[i] + sB[j]));
-        C[(int64_t)i * ldc + j] = v;
     }
 }
 
@@ -562,7 +608,7 @@ int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda
     IAB_LAUNCHED(1);
     k_i8gemm_mod<<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm);
     IAB_LAUNCHED(1);
-    k_crt<<<(unsigned)(nsm * 16), 256, 0, st>>>((int)M, (int)N, rr.as<uint8_t>(), ldr, sa.as<int>(), sb.as<int>(), C, ldc);
+    k_crt<<<(unsigned)(nsm * 8), 256, 0, st>>>((int)M, (int)N, rr.as<uint8_t>(), ldr, sa.as<int>(), sb.as<int>(), C, ldc);
     int h_err = 0;
     cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return -2;

@@ -121,6 +121,7 @@ def _lib():
             "iarray_b200_synchronize": ([P], RC),
             "iarray_b200_kernel_launches": ([], ctypes.c_uint64),
             "iarray_b200_get_stream": ([P, P], RC),
+            "iarray_b200_to_cframe_into": ([P, P, P, I64, P], RC),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -254,10 +255,14 @@ class Container:
         return cls(ctx, p)
 
     @classmethod
-    def from_cframe(cls, ctx, frame: bytes):
-        buf = ctypes.create_string_buffer(frame, len(frame))
+    def from_cframe(cls, ctx, frame):
+        """frame: bytes, or a numpy uint8 array (e.g. in pinned memory); not copied."""
+        if isinstance(frame, np.ndarray):
+            ptr, n = frame.ctypes.data, frame.nbytes
+        else:
+            ptr, n = ctypes.cast(ctypes.c_char_p(frame), ctypes.c_void_p), len(frame)
         p = ctypes.c_void_p()
-        check(_lib().iarray_from_cframe(ctx.ptr, buf, len(frame), True, ctypes.byref(p)), "iarray_from_cframe")
+        check(_lib().iarray_from_cframe(ctx.ptr, ptr, n, True, ctypes.byref(p)), "iarray_from_cframe")
         return cls(ctx, p)
 
     @classmethod
@@ -315,6 +320,18 @@ class Container:
         if nf.value:
             ctypes.CDLL(None).free(fp)
         return data
+
+    def cframe_len(self) -> int:
+        n = ctypes.c_int64()
+        check(_lib().iarray_b200_to_cframe_into(self.ctx.ptr, self.ptr, None, 0, ctypes.byref(n)))
+        return n.value
+
+    def to_cframe_into(self, buf: np.ndarray) -> int:
+        """Write the frame into a caller numpy uint8 buffer; returns its length."""
+        n = ctypes.c_int64()
+        check(_lib().iarray_b200_to_cframe_into(self.ctx.ptr, self.ptr, buf.ctypes.data, buf.nbytes, ctypes.byref(n)),
+              "iarray_b200_to_cframe_into")
+        return n.value
 
     def save(self, path):
         check(_lib().iarray_container_save(self.ctx.ptr, self.ptr, path.encode()), "iarray_container_save")

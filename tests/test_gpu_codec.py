@@ -94,6 +94,21 @@ def test_gpu_roundtrip_matches_oracle_bytes(ctx, ia, geom, kind, dtype):
     assert c2.to_numpy().tobytes() == a.tobytes()
 
 
+@pytest.mark.parametrize("n", [4096, 65535, 65546, 65547, 70000, 250000])
+def test_gpu_lz4_encoder_stress_matches_oracle(ctx, ia, n):
+    """One uint8 stream per block, sizes around the 2^16 + 11 switch between the 16-bit
+    and 32-bit hash tables, entropy from 1 to 8 bits per byte: every chunk must equal
+    the oracle's (liblz4-identical) encoding byte for byte."""
+    rng = np.random.default_rng(n)
+    for bits in (1, 2, 3, 5, 8):
+        a = rng.integers(0, 1 << bits, n).astype(np.uint8)
+        a[n // 3: n // 3 + n // 10] = a[: n // 10]             # a long repeat
+        c = ia.Container.from_numpy(ctx, a, (n,), (n,))
+        _, ref = O.encode_array(a, (n,), (n,))
+        assert c.chunks() == ref, (n, bits)
+        assert np.array_equal(c.to_numpy(), a)
+
+
 @pytest.mark.parametrize("dtype", [np.int64, np.int32, np.int16, np.uint8])
 def test_gpu_roundtrip_integer_types(ctx, ia, dtype):
     rng = np.random.default_rng(3)
