@@ -61,9 +61,18 @@ class Clocks:
         try:
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+            return
+        # nvidia-smi takes a moment to start: wait for its first sample so that the
+        # timed region that follows is covered
+        t0 = time.time()
+        while time.time() - t0 < 10 and self.p.poll() is None:
+            self.f.flush()
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.p is None:
@@ -154,6 +163,48 @@ def run_reference(args):
     barrier(pg)
 
 
+# ============================================================================ roofline
+L_MODULI = 14          # moduli of the split-precision product (library default)
+
+
+def roofline(kprof, pk, dgemm_tflops, c_cbytes, a_cb, b_cb):
+    """Roofline of the kernel with the largest device time in the timed steps.
+    achieved = algorithmic work of one launch / its mean CUDA-event duration."""
+    name, (cnt, tot) = max(kprof.items(), key=lambda kv: kv[1][1])
+    avg_s = tot / cnt * 1e-3
+    img = M * N * 8                              # bytes of one dense 8192^2 float64 matrix
+    if name == "k_i8gemm_mod":
+        work, unit, bound = 2.0 * M * N * K * L_MODULI / 1e12, "TOP/s", "tensor"
+        peak, src = 2 * pk["bf16_tflops"], "2 x measured dense BF16 (sm_100 dense INT8 rate is twice BF16)"
+    elif name == "k_gemm_f64":
+        work, unit, bound = FLOP / 1e12, "TFLOP/s", "tensor"
+        peak, src = dgemm_tflops, "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor roof)"
+    else:
+        bytes_per_launch = {
+            "k_lz4_encode": img + (c_cbytes or img),            # read the byte-plane image, write LZ4 streams
+            "k_lz4_decode_jump": (a_cb + b_cb) / 2 + img,       # upper bound: all streams LZ4
+            "k_crt": L_MODULI * M * N + img,                    # residue planes in, float64 out
+            "k_residues_rows": img + L_MODULI * M * K,
+            "k_residues_cols": img + L_MODULI * K * N,
+            "k_scatter_fast": 2 * img, "k_scatter": 2 * img,
+            "k_gather_fast": 2 * img, "k_gather": 2 * img,
+            "k_emit": 2 * (c_cbytes or img),
+        }.get(name)
+        if bytes_per_launch is None:
+            return {"bound": None, "kernel": name, "achieved": None, "peak": None, "unit": None, "frac": None,
+                    "traffic": None}
+        work, unit, bound = bytes_per_launch / 1e9, "GB/s", "hbm"
+        peak, src = pk["hbm_gbs"], "measured HBM copy bandwidth"
+    achieved = work / avg_s
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get(name)
+    return {"bound": bound, "kernel": name, "launches": cnt, "avg_ms": tot / cnt, "achieved": achieved,
+            "peak": peak, "peak_source": src, "unit": unit, "frac": achieved / peak if peak else None,
+            "traffic": traffic}
+
+
 # ============================================================================ our arm
 def run_ours(args):
     world, rank, local, pg = dist_setup(args)
@@ -190,6 +241,7 @@ def run_ours(args):
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         parts = np.zeros(5)
         l0 = ia.lib().iarray_b200_kernel_launches()
+        ia.profile_kernels(True)            # CUDA events around every launch, on its stream
         ev0.record(stream)
         for _ in range(args.steps):
             C = ia.opt_gemm(ctx, Ac, Bc, CHUNK, BLOCK)
@@ -198,12 +250,14 @@ def run_ours(args):
             C.free()
         ev1.record(stream)
         torch.cuda.synchronize()
+        ia.profile_kernels(False)
+        kprof = ia.kernel_profile()
         launches = ia.lib().iarray_b200_kernel_launches() - l0
         clocks = clk.stop()
         ms = ev0.elapsed_time(ev1) / args.steps
         ms = max_over_ranks(pg, ms)
         parts /= args.steps
-        results[name] = dict(ms=ms, parts=parts, launches=launches, clocks=clocks, form=form)
+        results[name] = dict(ms=ms, parts=parts, launches=launches, clocks=clocks, form=form, kprof=kprof)
 
     # errors vs double-double on sampled rows (outside the timed region)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -247,6 +301,25 @@ def run_ours(args):
         for x in (a2, b2, C):
             x.free()
     e2e_ms = max_over_ranks(pg, float(np.mean(e2e_t)) * 1e3)
+
+    # standalone decode of A (compressed chunks resident in HBM -> dense float64 array in
+    # HBM) through iarray_b200_decode_to_device; bytes = compressed read + decoded written
+    dense = torch.empty((M, K), dtype=torch.float64, device="cuda")
+    for _ in range(args.warmup):
+        Ac.decode_to_device(dense.data_ptr(), K)
+    ctx.synchronize()
+    d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ia.profile_kernels(True)
+    d0.record(stream)
+    for _ in range(args.steps):
+        Ac.decode_to_device(dense.data_ptr(), K)
+    d1.record(stream)
+    ctx.synchronize()
+    ia.profile_kernels(False)
+    dec_prof = ia.kernel_profile()
+    dec_ms = max_over_ranks(pg, d0.elapsed_time(d1) / args.steps)
+    del dense
+    torch.cuda.empty_cache()
 
     # cuBLAS DGEMM on the same dense shapes: the measured FP64 tensor roof
     dgemm_tflops = None
@@ -292,20 +365,7 @@ def run_ours(args):
     pk = peaks()
     hr = results[head]
     value = world * FLOP / (hr["ms"] * 1e-3) / 1e12
-    prod_ms = hr["parts"][2]
-    if head == "native":
-        roof = {"bound": "tensor", "kernel": "k_gemm_f64 (DMMA m16n8k4)", "achieved": FLOP / (prod_ms * 1e-3) / 1e12,
-                "peak": dgemm_tflops, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor roof)",
-                "unit": "TFLOP/s"}
-    else:
-        roof = {"bound": "tensor", "kernel": "split-precision product", "achieved": FLOP / (prod_ms * 1e-3) / 1e12,
-                "peak": dgemm_tflops, "peak_source": "cuBLAS DGEMM 8192^3 measured in this run", "unit": "TFLOP/s"}
-    roof["frac"] = roof["achieved"] / roof["peak"] if roof["peak"] else None
-    roof["traffic"] = None
-    tf = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(tf):
-        roof["traffic"] = json.load(open(tf)).get(roof["kernel"].split()[0])
-    decode_ms = hr["parts"][0]
+    roof = roofline(hr["kprof"], pk, dgemm_tflops, c_cbytes=hr.get("c_cbytes"), a_cb=a_cb, b_cb=b_cb)
     line = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": hr["ms"], "higher_is_better": True, "scaling": "weak",
@@ -318,7 +378,14 @@ def run_ours(args):
                                    "encode": r["parts"][3]},
                       "normwise_err_vs_dd": r.get("err"), "kernel_launches": int(r["launches"])}
                   for k, r in results.items()},
-        "decode_gbs": (a_nb + a_cb) / (decode_ms * 1e-3) / 1e9,
+        "decode": {"gbs": (a_nb + a_cb) / (dec_ms * 1e-3) / 1e9,
+                   "frac_of_measured_hbm": (a_nb + a_cb) / (dec_ms * 1e-3) / 1e9 / pk["hbm_gbs"],
+                   "ms": dec_ms, "bytes": a_nb + a_cb,
+                   "what": "A (8192^2 float64, 16 chunks) compressed in HBM -> dense in HBM, "
+                           "bytes = compressed read + decoded written",
+                   "kernel_ms": {k: v[1] / args.steps for k, v in sorted(dec_prof.items())}},
+        "kernel_ms_per_step": {k: {kk: v[1] / args.steps for kk, v in sorted(r["kprof"].items())}
+                               for k, r in results.items()},
         "compression": {"a_ratio": a_nb / a_cb, "b_ratio": b_nb / b_cb,
                         "c_ratio": (M * N * 8) / hr["c_cbytes"] if hr.get("c_cbytes") else None},
         "roofline": roof,
@@ -340,7 +407,7 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--err-rows", type=int, default=64)

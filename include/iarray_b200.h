@@ -340,6 +340,14 @@ INA_API(ina_rc_t) iarray_b200_get_stream(iarray_context_t *ctx, void **stream);
 INA_API(ina_rc_t) iarray_b200_to_cframe_into(iarray_context_t *ctx, iarray_container_t *c, uint8_t *buf,
                                              int64_t cap, int64_t *len);
 
+/* Per-kernel device time (B200 addition; the reference has no counterpart).  While
+ * enabled, every kernel launch of the library is bracketed by CUDA events on its stream;
+ * iarray_b200_profile_kernels(1) clears the totals and starts, (0) stops.
+ * iarray_b200_kernel_profile writes one line per kernel, "name launches total_ms\n",
+ * NUL-terminated, into `buf` (cap bytes; buf = NULL only queries *len). */
+INA_API(ina_rc_t) iarray_b200_profile_kernels(int on);
+INA_API(ina_rc_t) iarray_b200_kernel_profile(char *buf, int64_t cap, int64_t *len);
+
 #ifdef __cplusplus
 }
 #endif

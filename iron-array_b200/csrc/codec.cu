@@ -1034,9 +1034,8 @@ int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, 
     {
         const int threads = 128;
         const int64_t blocks = std::min<int64_t>((nbl + threads - 1) / threads, (int64_t)sms * 16);
-        IAB_LAUNCHED(1);
-        k_parse<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, st>>>(g, d_chunks, d_off, d_len, bd.as<BlockDesc>(),
-                                                                          sd.as<StreamDesc>(), jobs.as<Lz4Job>(), njobs, err);
+        IAB_TIMED("k_parse", st, k_parse<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, st>>>(g, d_chunks, d_off, d_len, bd.as<BlockDesc>(),
+                                                                          sd.as<StreamDesc>(), jobs.as<Lz4Job>(), njobs, err));
     }
     {
         static bool attr = false;
@@ -1046,10 +1045,9 @@ int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, 
             cudaFuncSetAttribute(k_lz4_decode_jump<RING, WIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             attr = true;
         }
-        IAB_LAUNCHED(1);
-        k_lz4_decode_jump<RING, WIN><<<sms * 3, WARPS * 32, smem, st>>>(d_chunks, jobs.as<Lz4Job>(), njobs,
+        IAB_TIMED("k_lz4_decode_jump", st, k_lz4_decode_jump<RING, WIN><<<sms * 3, WARPS * 32, smem, st>>>(d_chunks, jobs.as<Lz4Job>(), njobs,
                                                                       scratch.as<uint8_t>(), err,
-                                                                      reinterpret_cast<unsigned *>(counters.as<int>() + 2));
+                                                                      reinterpret_cast<unsigned *>(counters.as<int>() + 2)));
     }
     {
         const int64_t tpb = (g.blockn + TILE - 1) / TILE;
@@ -1059,17 +1057,15 @@ int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, 
         if (fast) {
             const int64_t fb = std::min<int64_t>(nbl, (int64_t)sms * 8);
             const uint8_t *cend = d_chunks + chunks_bytes, *send = scratch.as<uint8_t>() + nbl * g.blocksize;
-            IAB_LAUNCHED(1);
             if (g.itemsize == 8)
-                k_scatter_fast<8><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
-                    g, d_chunks, cend, bd.as<BlockDesc>(), sd.as<StreamDesc>(), scratch.as<uint8_t>(), send, (uint8_t *)out, ld);
+                IAB_TIMED("k_scatter_fast", st, k_scatter_fast<8><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
+                    g, d_chunks, cend, bd.as<BlockDesc>(), sd.as<StreamDesc>(), scratch.as<uint8_t>(), send, (uint8_t *)out, ld));
             else
-                k_scatter_fast<4><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
-                    g, d_chunks, cend, bd.as<BlockDesc>(), sd.as<StreamDesc>(), scratch.as<uint8_t>(), send, (uint8_t *)out, ld);
+                IAB_TIMED("k_scatter_fast", st, k_scatter_fast<4><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
+                    g, d_chunks, cend, bd.as<BlockDesc>(), sd.as<StreamDesc>(), scratch.as<uint8_t>(), send, (uint8_t *)out, ld));
         }
-        IAB_LAUNCHED(1);
-        k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, fast, d_chunks, bd.as<BlockDesc>(), sd.as<StreamDesc>(),
-                                                                        scratch.as<uint8_t>(), (uint8_t *)out, ld);
+        IAB_TIMED("k_scatter", st, k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, fast, d_chunks, bd.as<BlockDesc>(), sd.as<StreamDesc>(),
+                                                                        scratch.as<uint8_t>(), (uint8_t *)out, ld));
     }
     return 0;
 }
@@ -1100,15 +1096,18 @@ int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, in
     {
         const int64_t tpb = (g.blockn + TILE - 1) / TILE;
         const int64_t blocks = std::min<int64_t>(nbl * tpb, (int64_t)sms * 8);
-        IAB_LAUNCHED(1);
         const bool fast = shuffle && (ts == 4 || ts == 8);
         if (fast) {
             const int64_t fb = std::min<int64_t>(nbl, (int64_t)sms * 8);
-            IAB_LAUNCHED(1);
-            if (ts == 8) k_gather_fast<8><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(g, (const uint8_t *)in, ld, img.as<uint8_t>());
-            else k_gather_fast<4><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(g, (const uint8_t *)in, ld, img.as<uint8_t>());
+            if (ts == 8)
+                IAB_TIMED("k_gather_fast", st, k_gather_fast<8><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
+                    g, (const uint8_t *)in, ld, img.as<uint8_t>()));
+            else
+                IAB_TIMED("k_gather_fast", st, k_gather_fast<4><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
+                    g, (const uint8_t *)in, ld, img.as<uint8_t>()));
         }
-        k_gather<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, fast, (const uint8_t *)in, ld, shuffle, img.as<uint8_t>());
+        IAB_TIMED("k_gather", st, k_gather<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
+            g, fast, (const uint8_t *)in, ld, shuffle, img.as<uint8_t>()));
     }
     {
         static bool attr = false;
@@ -1119,19 +1118,16 @@ int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, in
         }
         const int64_t ns = nbl * nstreams;
         const int64_t blocks = std::min<int64_t>((ns + wpb - 1) / wpb, (int64_t)sms * 3);
-        IAB_LAUNCHED(1);
-        k_lz4_encode<<<(unsigned)std::max<int64_t>(blocks, 1), wpb * 32, smem, st>>>(
+        IAB_TIMED("k_lz4_encode", st, k_lz4_encode<<<(unsigned)std::max<int64_t>(blocks, 1), wpb * 32, smem, st>>>(
             img.as<uint8_t>(), ns, neblock, slots.as<uint8_t>(), es.as<EncStream>(),
-            reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1));
+            reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1)));
     }
-    IAB_LAUNCHED(1);
-    k_layout<<<1, 1024, 0, st>>>(g, nstreams, neblock, es.as<EncStream>(), ec.as<EncChunk>(), tot.as<int64_t>());
+    IAB_TIMED("k_layout", st, k_layout<<<1, 1024, 0, st>>>(g, nstreams, neblock, es.as<EncStream>(), ec.as<EncChunk>(), tot.as<int64_t>()));
     {
         const int64_t blocks = std::min<int64_t>(nbl, (int64_t)sms * 8);
-        IAB_LAUNCHED(1);
-        k_emit<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, nstreams, neblock, shuffle, split ? 1 : 0,
+        IAB_TIMED("k_emit", st, k_emit<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, nstreams, neblock, shuffle, split ? 1 : 0,
                                                                       img.as<uint8_t>(), slots.as<uint8_t>(),
-                                                                      es.as<EncStream>(), ec.as<EncChunk>(), d_out->as<uint8_t>());
+                                                                      es.as<EncStream>(), ec.as<EncChunk>(), d_out->as<uint8_t>()));
     }
     std::vector<EncChunk> hc((size_t)g.nchunks);
     cudaMemcpyAsync(hc.data(), ec.p, sizeof(EncChunk) * g.nchunks, cudaMemcpyDeviceToHost, st);

@@ -116,6 +116,28 @@ struct DevBuf {   // RAII handle over a pool allocation
 // Every kernel launch of the library adds to this counter (read through the C ABI).
 extern std::atomic<uint64_t> g_launches;
 #define IAB_LAUNCHED(n) (::iab::g_launches.fetch_add((n), std::memory_order_relaxed))
+// Counts and (while kernel profiling is on) times one launch statement on stream `st`.
+#define IAB_TIMED(name, st, ...)                   \
+    do {                                           \
+        ::iab::KernelTimer iab_kt_((name), (st));  \
+        IAB_LAUNCHED(1);                           \
+        __VA_ARGS__;                               \
+    } while (0)
+
+// Brackets one kernel launch with CUDA events on its stream while kernel profiling is on
+// (iarray_b200_profile_kernels); does nothing otherwise.  Construct it right before the
+// launch, in the launch's scope.
+class KernelTimer {
+public:
+    KernelTimer(const char *name, cudaStream_t st);
+    ~KernelTimer();
+    KernelTimer(const KernelTimer &) = delete;
+    KernelTimer &operator=(const KernelTimer &) = delete;
+private:
+    const char *name_;
+    cudaStream_t st_;
+    cudaEvent_t e0_ = nullptr;
+};
 
 struct CodecStats { int32_t err; };
 

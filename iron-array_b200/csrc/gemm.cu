@@ -151,8 +151,7 @@ void gemm_f64_native(int64_t M, int64_t N, int64_t K, const double *A, int64_t l
         attr = true;
     }
     dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM));
-    IAB_LAUNCHED(1);
-    k_gemm_f64<<<grid, 256, SMEM, st>>>((int)M, (int)N, (int)K, A, lda, B, ldb, C, ldc);
+    IAB_TIMED("k_gemm_f64", st, k_gemm_f64<<<grid, 256, SMEM, st>>>((int)M, (int)N, (int)K, A, lda, B, ldb, C, ldc));
 }
 
 // ============================================================================ FP32 FFMA
@@ -260,8 +259,7 @@ void gemm_f32_native(int64_t M, int64_t N, int64_t K, const float *A, int64_t ld
 {
     using namespace f32k;
     dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM));
-    IAB_LAUNCHED(1);
-    k_gemm_f32<<<grid, 256, 0, st>>>((int)M, (int)N, (int)K, A, lda, B, ldb, C, ldc);
+    IAB_TIMED("k_gemm_f32", st, k_gemm_f32<<<grid, 256, 0, st>>>((int)M, (int)N, (int)K, A, lda, B, ldb, C, ldc));
 }
 
 // ============================================================================ GEMV
@@ -299,8 +297,8 @@ __global__ void __launch_bounds__(256) k_gemv(int M, int K, const T *__restrict_
 void gemv_native(int dtype, int64_t M, int64_t K, const void *A, int64_t lda, const void *x, void *y, cudaStream_t st)
 {
     const int blocks = (int)((M * 32 + 255) / 256);
-    if (dtype == 0) { IAB_LAUNCHED(1); k_gemv<double><<<blocks, 256, 0, st>>>((int)M, (int)K, (const double *)A, lda, (const double *)x, (double *)y); }
-    else { IAB_LAUNCHED(1); k_gemv<float><<<blocks, 256, 0, st>>>((int)M, (int)K, (const float *)A, lda, (const float *)x, (float *)y); }
+    if (dtype == 0) { IAB_TIMED("k_gemv", st, k_gemv<double><<<blocks, 256, 0, st>>>((int)M, (int)K, (const double *)A, lda, (const double *)x, (double *)y)); }
+    else { IAB_TIMED("k_gemv", st, k_gemv<float><<<blocks, 256, 0, st>>>((int)M, (int)K, (const float *)A, lda, (const float *)x, (float *)y)); }
 }
 
 // ============================================================================ helpers
@@ -318,8 +316,8 @@ void fill_arange(int dtype, int64_t M, int64_t N, int64_t ld, double start, doub
     const int64_t n = M * N;
     const unsigned blocks = (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 32);
     if (n == 0) return;
-    if (dtype == 0) { IAB_LAUNCHED(1); k_arange<double><<<blocks, 256, 0, st>>>(M, N, ld, start, step, (double *)out); }
-    else { IAB_LAUNCHED(1); k_arange<float><<<blocks, 256, 0, st>>>(M, N, ld, start, step, (float *)out); }
+    if (dtype == 0) { IAB_TIMED("k_arange", st, k_arange<double><<<blocks, 256, 0, st>>>(M, N, ld, start, step, (double *)out)); }
+    else { IAB_TIMED("k_arange", st, k_arange<float><<<blocks, 256, 0, st>>>(M, N, ld, start, step, (float *)out)); }
 }
 
 template <typename T>
@@ -343,8 +341,8 @@ void transpose_dense(int itemsize, int64_t rows, int64_t cols, const void *in, i
                      cudaStream_t st)
 {
     dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32)), block(32, 8);
-    if (itemsize == 8) { IAB_LAUNCHED(1); k_transpose<double><<<grid, block, 0, st>>>(rows, cols, (const double *)in, ldin, (double *)out, ldout); }
-    else { IAB_LAUNCHED(1); k_transpose<float><<<grid, block, 0, st>>>(rows, cols, (const float *)in, ldin, (float *)out, ldout); }
+    if (itemsize == 8) { IAB_TIMED("k_transpose", st, k_transpose<double><<<grid, block, 0, st>>>(rows, cols, (const double *)in, ldin, (double *)out, ldout)); }
+    else { IAB_TIMED("k_transpose", st, k_transpose<float><<<grid, block, 0, st>>>(rows, cols, (const float *)in, ldin, (float *)out, ldout)); }
 }
 
 }  // namespace iab

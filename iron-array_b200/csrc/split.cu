@@ -576,18 +576,13 @@ int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda
         return -100;
     cudaMemsetAsync(err.p, 0, 16, st);
     const int nsm = sms();
-    IAB_LAUNCHED(1);
-    k_row_shift<<<(unsigned)((M * 32 + 255) / 256), 256, 0, st>>>((int)M, (int)K, A, lda, gamma, sa.as<int>());
-    IAB_LAUNCHED(1);
-    k_col_partial<<<dim3((unsigned)((N + 255) / 256), COL_SEGS), 256, 0, st>>>((int)K, (int)N, B, ldb, pm.as<double>(),
-                                                                               ps.as<double>());
-    IAB_LAUNCHED(1);
-    k_col_shift<<<(unsigned)((N + 255) / 256), 256, 0, st>>>((int)N, pm.as<double>(), ps.as<double>(), gamma, sb.as<int>());
-    IAB_LAUNCHED(1);
-    k_residues_rows<<<(unsigned)(nsm * 16), 256, 0, st>>>((int)M, (int)K, (int)Kp, A, lda, sa.as<int>(), ra.as<int8_t>());
-    IAB_LAUNCHED(1);
-    k_residues_cols<<<dim3((unsigned)((N + 63) / 64), (unsigned)((Kp + 63) / 64)), 256, 0, st>>>(
-        (int)K, (int)N, (int)Kp, B, ldb, sb.as<int>(), rb.as<int8_t>());
+    IAB_TIMED("k_row_shift", st, k_row_shift<<<(unsigned)((M * 32 + 255) / 256), 256, 0, st>>>((int)M, (int)K, A, lda, gamma, sa.as<int>()));
+    IAB_TIMED("k_col_partial", st, k_col_partial<<<dim3((unsigned)((N + 255) / 256), COL_SEGS), 256, 0, st>>>((int)K, (int)N, B, ldb, pm.as<double>(),
+                                                                               ps.as<double>()));
+    IAB_TIMED("k_col_shift", st, k_col_shift<<<(unsigned)((N + 255) / 256), 256, 0, st>>>((int)N, pm.as<double>(), ps.as<double>(), gamma, sb.as<int>()));
+    IAB_TIMED("k_residues_rows", st, k_residues_rows<<<(unsigned)(nsm * 16), 256, 0, st>>>((int)M, (int)K, (int)Kp, A, lda, sa.as<int>(), ra.as<int8_t>()));
+    IAB_TIMED("k_residues_cols", st, k_residues_cols<<<dim3((unsigned)((N + 63) / 64), (unsigned)((Kp + 63) / 64)), 256, 0, st>>>(
+        (int)K, (int)N, (int)Kp, B, ldb, sb.as<int>(), rb.as<int8_t>()));
 
     CUtensorMap tmA, tmB;
     if (!make_tmap_3d(&tmA, CU_TENSOR_MAP_DATA_TYPE_UINT8, ra.p, (uint64_t)Kp, (uint64_t)M, (uint64_t)L, (uint64_t)Kp,
@@ -605,10 +600,8 @@ int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda
         attr = true;
     }
     const int tiles = L * prm.tiles_m * prm.tiles_n;
-    IAB_LAUNCHED(1);
-    k_i8gemm_mod<<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm);
-    IAB_LAUNCHED(1);
-    k_crt<<<(unsigned)(nsm * 8), 256, 0, st>>>((int)M, (int)N, rr.as<uint8_t>(), ldr, sa.as<int>(), sb.as<int>(), C, ldc);
+    IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
+    IAB_TIMED("k_crt", st, k_crt<<<(unsigned)(nsm * 8), 256, 0, st>>>((int)M, (int)N, rr.as<uint8_t>(), ldr, sa.as<int>(), sb.as<int>(), C, ldc));
     int h_err = 0;
     cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return -2;

@@ -122,6 +122,8 @@ def _lib():
             "iarray_b200_kernel_launches": ([], ctypes.c_uint64),
             "iarray_b200_get_stream": ([P, P], RC),
             "iarray_b200_to_cframe_into": ([P, P, P, I64, P], RC),
+            "iarray_b200_profile_kernels": ([ctypes.c_int], RC),
+            "iarray_b200_kernel_profile": ([P, I64, P], RC),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -133,6 +135,24 @@ def _lib():
 
 def lib():
     return _lib()
+
+
+def profile_kernels(on):
+    """Start (clearing the totals) or stop per-kernel CUDA-event timing."""
+    check(_lib().iarray_b200_profile_kernels(1 if on else 0), "profile_kernels")
+
+
+def kernel_profile():
+    """{kernel name: (launches, total device ms)} since profiling was last started."""
+    n = ctypes.c_int64()
+    check(_lib().iarray_b200_kernel_profile(None, 0, ctypes.byref(n)), "kernel_profile")
+    buf = ctypes.create_string_buffer(n.value + 1)
+    check(_lib().iarray_b200_kernel_profile(buf, n.value + 1, ctypes.byref(n)), "kernel_profile")
+    out = {}
+    for ln in buf.value.decode().splitlines():
+        name, cnt, ms = ln.split()
+        out[name] = (int(cnt), float(ms))
+    return out
 
 
 def check(rc, where=""):
@@ -273,6 +293,11 @@ class Container:
         return cls(ctx, p)
 
     # ------------------------------------------------------------------ accessors
+    def decode_to_device(self, dptr, ld):
+        """Decode into device memory at `dptr` (row-major, leading dimension `ld` items)
+        on the context's stream."""
+        check(_lib().iarray_b200_decode_to_device(self.ctx.ptr, self.ptr, dptr, ld), "decode_to_device")
+
     def dtshape(self):
         d = DtShape()
         check(_lib().iarray_get_dtshape(self.ctx.ptr, self.ptr, ctypes.byref(d)))

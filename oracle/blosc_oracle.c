@@ -11,7 +11,7 @@
  *     greedy encoder in "limited output" mode.  c-blosc2 (the reference's codec,
  *     an un-vendored submodule `contribs/caterva/contribs/c-blosc2`, version not
  *     pinned in the checkout) bundles liblz4 and always calls it with acceleration 1.
- *     Parity pin: the reference's golden frames the tests/data directory frames (every LZ4 stream
+ *     Parity pin: the reference's golden frames (tests/data/*.iarray: every LZ4 stream
  *     re-encodes byte-identically) and liblz4.so.1 itself (random + structured inputs).
  *   - Blosc2 chunk format v5 with the 32-byte extended header, SHUFFLE filter,
  *     split streams, zero / run / raw / LZ4 stream kinds, memcpyed chunks and the
