@@ -348,6 +348,36 @@ INA_API(ina_rc_t) iarray_b200_to_cframe_into(iarray_context_t *ctx, iarray_conta
 INA_API(ina_rc_t) iarray_b200_profile_kernels(int on);
 INA_API(ina_rc_t) iarray_b200_kernel_profile(char *buf, int64_t cap, int64_t *len);
 
+/* Decode without allocating.  No counterpart in the reference (whose decoders allocate
+ * through Blosc2 contexts): this entry point is for callers that cannot call cudaMalloc,
+ * such as engines whose device memory is owned by their own arena or memory-budget
+ * manager and that hand the library only buffers they already hold, or latency-bound
+ * loops that must not pay the device synchronisation cudaMalloc / cudaFree bring.
+ *
+ * Decodes `nchunks = prod(ceil(shape / chunkshape))` Blosc2 chunks stored back to back
+ * in device memory (`chunks`, `chunks_len` bytes, row-major chunk order, the layout of a
+ * frame's chunk region) into the device array `dptr` (row-major, leading dimension `ld`
+ * items, ld >= last dimension; columns past the last dimension are left untouched), on
+ * the CUDA stream `stream` (a cudaStream_t; NULL = the legacy default stream), and
+ * waits for it.  The kernels are the ones iarray_b200_decode_to_device runs; their work
+ * buffers live in one fixed device array of the library instead of allocations, so the
+ * call allocates nothing.  Limits per call: nchunks x padded chunk bytes <=
+ * IARRAY_B200_NOALLOC_MAX_BYTES and nchunks x blocks per chunk <=
+ * IARRAY_B200_NOALLOC_MAX_BLOCKS; larger geometries return IARRAY_ERR_NOALLOC_TOO_LARGE
+ * (decode a large container chunk by chunk, passing chunkshape as the shape).
+ * The fixed array (about 9.4 MiB) is held by every GPU that loads the library's kernels
+ * until the process exits.  The first call on each device looks up the array's device
+ * address and sets a kernel attribute; make that first call before any stream capture.
+ * All calls share the array and it keeps the last call's contents: calls whose work
+ * overlaps on the GPU (other streams, other host threads) race on it and must be
+ * serialised by the caller. */
+#define IARRAY_B200_NOALLOC_MAX_BYTES (8LL << 20)
+#define IARRAY_B200_NOALLOC_MAX_BLOCKS 4096LL
+#define IARRAY_ERR_NOALLOC_TOO_LARGE (INA_ERR_OUT_OF_RANGE | IARRAY_ES_BUFFER)
+INA_API(ina_rc_t) iarray_b200_decode_noalloc(int8_t ndim, const int64_t *shape, const int64_t *chunkshape,
+                                             const int64_t *blockshape, int32_t itemsize, const void *chunks,
+                                             int64_t chunks_len, void *dptr, int64_t ld, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -212,6 +212,7 @@ INA_API(const char *) iarray_err_strerror(ina_rc_t error)
     case IARRAY_ERR_NOT_SUPPORTED: return "Not supported";
     case INA_ERR_INVALID_ARGUMENT: return "Invalid argument";
     case INA_ERR_NOT_INITIALIZED: return "Library not initialized";
+    case IARRAY_ERR_NOALLOC_TOO_LARGE: return "Geometry exceeds the fixed scratch of iarray_b200_decode_noalloc";
     default: return "Error";
     }
 }
@@ -674,6 +675,27 @@ INA_API(ina_rc_t) iarray_b200_decode_to_device(iarray_context_t *ctx, iarray_con
 {
     CHECK_ARG(ctx && c && dptr && ld >= cols_of(c->dtshape));
     return decode_logical(ctx, c, dptr, ld);
+}
+
+INA_API(ina_rc_t) iarray_b200_decode_noalloc(int8_t ndim, const int64_t *shape, const int64_t *chunkshape,
+                                             const int64_t *blockshape, int32_t itemsize, const void *chunks,
+                                             int64_t chunks_len, void *dptr, int64_t ld, void *stream)
+{
+    CHECK_ARG(shape && chunkshape && blockshape && chunks && dptr && chunks_len >= 0);
+    CHECK_ARG(itemsize == 1 || itemsize == 2 || itemsize == 4 || itemsize == 8);
+    Geom g;
+    if (!iab::make_geom(ndim, shape, chunkshape, blockshape, itemsize, &g)) return rc_err(INA_ERR_INVALID_ARGUMENT);
+    CHECK_ARG(ld >= g.shape[1]);
+    static_assert(IARRAY_B200_NOALLOC_MAX_BYTES == iab::NOALLOC_MAX_BYTES &&
+                  IARRAY_B200_NOALLOC_MAX_BLOCKS == iab::NOALLOC_MAX_BLOCKS, "no-allocation limits");
+    if (g.nchunks * g.chunk_nbytes > iab::NOALLOC_MAX_BYTES || g.nchunks * g.nblocks > iab::NOALLOC_MAX_BLOCKS)
+        return rc_err(IARRAY_ERR_NOALLOC_TOO_LARGE);
+    const int r = iab::decode_noalloc(g, static_cast<const uint8_t *>(chunks), chunks_len, dptr, ld,
+                                      static_cast<cudaStream_t>(stream));
+    if (r == -102) return rc_err(IARRAY_ERR_NOALLOC_TOO_LARGE);
+    if (r < 0) return rc_err(IARRAY_ERR_GPU_FAILED);
+    if (r > 0) return rc_err(IARRAY_ERR_BLOSC_FAILED);
+    return INA_SUCCESS;
 }
 
 INA_API(ina_rc_t) iarray_b200_encode_from_device(iarray_context_t *ctx, iarray_dtshape_t *dtshape, const void *dptr,

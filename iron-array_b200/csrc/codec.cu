@@ -1138,4 +1138,122 @@ int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, in
     return 0;
 }
 
+// ============================================================================ decode without allocation
+// For callers that cannot call cudaMalloc: engines whose device memory belongs to their own
+// arena or memory-budget manager and that hand the library only buffers they already hold,
+// and latency-bound loops that must not pay the device synchronisation of cudaMalloc and
+// cudaFree.  decode_noalloc runs the same kernels as decode_launch, but its work buffers (chunk
+// index, block and stream descriptors, LZ4 jobs, the decoded-stream image and the
+// status counters) live in one file-scope device array instead of pool allocations.
+// The array is part of the library's device image: every GPU on which the library's
+// kernels are loaded holds it until the process exits, and every call shares it, so
+// calls whose kernels overlap on the GPU (two streams, two host threads) race on it.
+constexpr int64_t NA_MAX_BLOCKS = NOALLOC_MAX_BLOCKS;
+constexpr size_t na_align(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr size_t NA_COUNTERS = 0;
+constexpr size_t NA_OFF = 256;
+constexpr size_t NA_LEN = na_align(NA_OFF + sizeof(int64_t) * NA_MAX_BLOCKS);
+constexpr size_t NA_BD = na_align(NA_LEN + sizeof(int32_t) * NA_MAX_BLOCKS);
+constexpr size_t NA_SD = na_align(NA_BD + sizeof(BlockDesc) * NA_MAX_BLOCKS);
+constexpr size_t NA_JOBS = na_align(NA_SD + sizeof(StreamDesc) * 8 * NA_MAX_BLOCKS);
+constexpr size_t NA_IMG = na_align(NA_JOBS + sizeof(Lz4Job) * 8 * NA_MAX_BLOCKS);
+constexpr size_t NA_TOTAL = NA_IMG + (size_t)NOALLOC_MAX_BYTES;
+
+static __device__ __align__(256) uint8_t g_noalloc_scratch[NA_TOTAL];
+
+// Chunk index of back-to-back chunks: one thread walks the headers (cbytes at byte 12).
+// A header that does not fit the buffer yields length 0, which the parse kernel reports
+// as a header error.
+__global__ void k_chunk_walk(const uint8_t *__restrict__ ch, int64_t bytes, int64_t n, int64_t *off, int32_t *len)
+{
+    if (blockIdx.x || threadIdx.x) return;
+    int64_t pos = 0;
+    for (int64_t c = 0; c < n; c++) {
+        int32_t cb = 0;
+        if (pos + 32 <= bytes) {
+            cb = ld_s32(ch + pos + 12);
+            if (cb < 32 || (int64_t)cb > bytes - pos) cb = 0;
+        }
+        off[c] = pos;
+        len[c] = cb;
+        pos = cb ? pos + cb : bytes;
+    }
+}
+
+// Device address of g_noalloc_scratch on the current device.  The first call on a device
+// looks the address up (the symbol's host name is only a stand-in, not a device address)
+// and sets the decoder's shared-memory attribute; later calls reuse the cached address.
+static uint8_t *noalloc_scratch()
+{
+    constexpr int MAXDEV = 64;
+    static std::mutex mu;
+    static uint8_t *ptr[MAXDEV] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAXDEV) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) { cudaGetLastError(); return nullptr; }
+        constexpr int RING = 4096, WIN = 1024, WARPS = 4;
+        const int smem = WARPS * (RING + WIN + 16 + 5 * WIN * 2);
+        if (cudaFuncSetAttribute(k_lz4_decode_jump<RING, WIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+            cudaSuccess) { cudaGetLastError(); return nullptr; }
+        ptr[dev] = static_cast<uint8_t *>(p);
+    }
+    return ptr[dev];
+}
+
+int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, void *out, int64_t ld, cudaStream_t st)
+{
+    const int64_t nbl = g.nchunks * g.nblocks;
+    if (g.nchunks * g.chunk_nbytes > NOALLOC_MAX_BYTES || nbl > NOALLOC_MAX_BLOCKS) return -102;
+    if (nbl == 0) return 0;
+    uint8_t *base = noalloc_scratch();
+    if (!base) return -101;
+    int *counters = reinterpret_cast<int *>(base + NA_COUNTERS);
+    int64_t *off = reinterpret_cast<int64_t *>(base + NA_OFF);
+    int32_t *len = reinterpret_cast<int32_t *>(base + NA_LEN);
+    BlockDesc *bd = reinterpret_cast<BlockDesc *>(base + NA_BD);
+    StreamDesc *sd = reinterpret_cast<StreamDesc *>(base + NA_SD);
+    Lz4Job *jobs = reinterpret_cast<Lz4Job *>(base + NA_JOBS);
+    uint8_t *img = base + NA_IMG;
+    int *njobs = counters, *err = counters + 1;
+    // the job count, the status word and the job cursor must start at zero; descriptors,
+    // the chunk index and the image are fully rewritten before they are read
+    cudaMemsetAsync(counters, 0, 64, st);
+    const int sms = sm_count();
+    IAB_TIMED("k_chunk_walk", st, k_chunk_walk<<<1, 32, 0, st>>>(d_chunks, chunks_bytes, g.nchunks, off, len));
+    {
+        const int threads = 128;
+        const int64_t blocks = std::min<int64_t>((nbl + threads - 1) / threads, (int64_t)sms * 16);
+        IAB_TIMED("k_parse", st, k_parse<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, st>>>(g, d_chunks, off, len, bd, sd, jobs, njobs, err));
+    }
+    {
+        constexpr int RING = 4096, WIN = 1024, WARPS = 4;
+        const int smem = WARPS * (RING + WIN + 16 + 5 * WIN * 2);
+        IAB_TIMED("k_lz4_decode_jump", st, k_lz4_decode_jump<RING, WIN><<<sms * 3, WARPS * 32, smem, st>>>(d_chunks, jobs, njobs, img, err,
+                                                                      reinterpret_cast<unsigned *>(counters + 2)));
+    }
+    {
+        const int64_t tpb = (g.blockn + TILE - 1) / TILE;
+        const int64_t blocks = std::min<int64_t>(nbl * tpb, (int64_t)sms * 8);
+        const bool fast = g.itemsize == 4 || g.itemsize == 8;
+        if (fast) {
+            const int64_t fb = std::min<int64_t>(nbl, (int64_t)sms * 8);
+            const uint8_t *cend = d_chunks + chunks_bytes, *send = img + nbl * g.blocksize;
+            if (g.itemsize == 8)
+                IAB_TIMED("k_scatter_fast", st, k_scatter_fast<8><<<(unsigned)fb, 256, 0, st>>>(
+                    g, d_chunks, cend, bd, sd, img, send, (uint8_t *)out, ld));
+            else
+                IAB_TIMED("k_scatter_fast", st, k_scatter_fast<4><<<(unsigned)fb, 256, 0, st>>>(
+                    g, d_chunks, cend, bd, sd, img, send, (uint8_t *)out, ld));
+        }
+        IAB_TIMED("k_scatter", st, k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, fast, d_chunks, bd, sd, img, (uint8_t *)out, ld));
+    }
+    int h_err = 0;
+    if (cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return -101;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return -101;
+    return h_err;
+}
+
 }  // namespace iab

@@ -155,6 +155,14 @@ int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, 
                   void *out, int64_t ld, cudaStream_t st, DecodeWork *w);
 int decode_finish(DecodeWork *w, cudaStream_t st);
 
+// Decode without allocating: the work buffers live in a fixed device array of the library
+// (at most NOALLOC_MAX_BYTES decoded bytes and NOALLOC_MAX_BLOCKS blocks per call; larger
+// geometries return -102).  d_chunks holds g.nchunks chunks back to back.  Returns a
+// DevErr (synchronises `st`), -101 on a CUDA error.
+constexpr int64_t NOALLOC_MAX_BYTES = int64_t(8) << 20;
+constexpr int64_t NOALLOC_MAX_BLOCKS = 4096;
+int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, void *out, int64_t ld, cudaStream_t st);
+
 // Encode a dense row-major array into Blosc2 chunks.  On return *d_out holds the
 // chunks back-to-back, h_off / h_len (host) their offsets and lengths.
 int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode,

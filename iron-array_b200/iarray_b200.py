@@ -49,6 +49,7 @@ ERR = {
     "NOT_SUPPORTED": (_code(10) | NEGATE) | (ES + 1),
     "INVALID_ARGUMENT": _code(1) | 1,
     "NOT_INITIALIZED": (_code(11) | NEGATE),
+    "NOALLOC_TOO_LARGE": _code(6) | (ES + 9),
 }
 ERR_NAME = {v: k for k, v in ERR.items()}
 
@@ -124,6 +125,7 @@ def _lib():
             "iarray_b200_to_cframe_into": ([P, P, P, I64, P], RC),
             "iarray_b200_profile_kernels": ([ctypes.c_int], RC),
             "iarray_b200_kernel_profile": ([P, I64, P], RC),
+            "iarray_b200_decode_noalloc": ([ctypes.c_int8, P, P, P, ctypes.c_int32, P, I64, P, I64, P], RC),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
