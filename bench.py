@@ -182,7 +182,7 @@ def roofline(kprof, pk, dgemm_tflops, c_cbytes, a_cb, b_cb):
     else:
         bytes_per_launch = {
             "k_lz4_encode": img + (c_cbytes or img),            # read the byte-plane image, write LZ4 streams
-            "k_lz4_decode_jump": (a_cb + b_cb) / 2 + img,       # upper bound: all streams LZ4
+            "k_lz4_decode_cta": (a_cb + b_cb) / 2 + img,        # upper bound: all streams LZ4
             "k_crt": L_MODULI * M * N + img,                    # residue planes in, float64 out
             "k_residues_rows": img + L_MODULI * M * K,
             "k_residues_cols": img + L_MODULI * K * N,

@@ -121,248 +121,315 @@ __global__ void k_parse(Geom g, const uint8_t *__restrict__ ch, const int64_t *_
     }
 }
 
-// D1 (parallel parse): one warp per LZ4 stream.  The stream is consumed in windows of W
-// input bytes staged in shared memory.  For every byte position q of the window the
-// warp computes next[q] = where the following token would start if a sequence began at
-// q (STOP if that sequence does not end inside the window, ENDS if it is the stream's
-// last sequence).  Five pointer-doubling levels (next^1, ^2, ^4, ^8, ^16) then let lane l
-// locate the l-th sequence after a known token position with five table reads, so 32
-// sequences are parsed in parallel per step.  Copies run per batch of <= 32 sequences:
-// literals first, then matches in rounds; a lane copies once its source lies below the
-// lowest output position still owed by an unfinished lane (the frontier).  A batch never
-// spans more than RING output bytes, so within a batch no two output positions share a
-// slot of the shared-memory history ring; older history is read back from global memory.
-// A sequence too long for a window is decoded on its own (header read from global).
-constexpr uint16_t SEQ_STOP = 0xFFFF, SEQ_ENDS = 0xFFFE;
+// D1: LZ4 stream decode, one CTA (256 threads) per stream, streams handed out
+// dynamically.  The stream is consumed in windows of up to DW compressed bytes staged in
+// shared memory, and each window is decoded without any serial walk:
+//  1. for every byte q of the window, next[q] = where the following token would start if
+//     a sequence began at q (STOP when that sequence does not end inside the window,
+//     ENDS when it is the stream's last, literal-only sequence);
+//  2. the chain of token positions from the window start is built by pointer doubling
+//     (next, next^2, next^4, ... composed in two ping-pong tables, the chain doubled
+//     alongside), so the window's sequences are all located in O(log) parallel steps;
+//  3. their literal and match lengths are read in parallel and an exclusive scan gives
+//     each sequence's output offset;
+//  4. the output is resolved in groups of at most DCAP bytes in shared memory: a literal
+//     byte takes its value from the window, a match byte points at its source (a source
+//     inside the same match is folded back below the match start modulo the offset), and
+//     pointer jumping settles every byte in O(log depth) rounds; sources before the group
+//     are read from the already written output;
+//  5. a sequence with more than DCAP output bytes is copied straight in global memory
+//     (all its sources lie before its own match start), and a sequence too long for a
+//     window is decoded alone with its header read from global memory.
+namespace dcta {
+constexpr int THREADS = 256;
+constexpr int DW = 2048;                   // compressed bytes per window
+constexpr int MAXS = DW / 3 + 2;           // sequences per window (a non-final one takes >= 3 bytes)
+constexpr int PATH = 1024;                 // >= 2 * the largest power of two below MAXS + 1
+constexpr int DCAP = 8192;                 // output bytes resolved in shared memory at once
+constexpr uint16_t STOP = 0xFFFF, ENDS = 0xFFFE;
+constexpr uint32_t RES = 0x80000000u;      // resolved output byte (value in the low 8 bits)
+struct Smem {
+    uint32_t st[DCAP];                     // per output byte: RES | value, or the source's index
+    int32_t ostart[MAXS + 1];              // output offset of each sequence in the window
+    int32_t llen[MAXS];
+    int32_t mlen[MAXS];
+    uint16_t lpos[MAXS];
+    uint16_t off[MAXS];
+    uint16_t J[2][DW];
+    uint16_t path[PATH];
+    uint8_t win[DW + 16];
+    int32_t wsum[THREADS / 32];
+    int32_t scal[8];
+};
+}  // namespace dcta
 
-template <int RING, int W>
-__global__ void __launch_bounds__(128) k_lz4_decode_jump(const uint8_t *__restrict__ ch, const Lz4Job *__restrict__ jobs,
-                                                         const int *__restrict__ njobs_p, uint8_t *scratch, int *err,
-                                                         unsigned *next_job)
+// next[q] for a sequence starting at window offset q (n valid bytes, rem bytes left in
+// the stream from the window start).
+__device__ __forceinline__ uint16_t dcta_next(const uint8_t *win, int q, int n, int rem)
 {
-    extern __shared__ __align__(16) uint8_t sm_jump[];
-    constexpr int PER_WARP = RING + W + 16 + 5 * W * 2;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint8_t *ring = sm_jump + warp * PER_WARP;
-    uint8_t *iwin = ring + RING;
-    uint16_t *J = reinterpret_cast<uint16_t *>(iwin + W + 16);   // J[b * W + q], b = 0..4
+    int r = q + 1;
+    const int tok = win[q];
+    int lit = tok >> 4;
+    if (lit == 15) {
+        int b = 255;
+        while (b == 255) {
+            if (r >= n) return dcta::STOP;
+            b = win[r++];
+            lit += b;
+        }
+    }
+    r += lit;
+    if (r > n) return dcta::STOP;
+    if (r == rem) return dcta::ENDS;      // literals reach the stream end: the last sequence
+    if (r + 2 > n) return dcta::STOP;
+    r += 2;
+    if ((tok & 15) == 15) {
+        int b = 255;
+        while (b == 255) {
+            if (r >= n) return dcta::STOP;
+            b = win[r++];
+        }
+    }
+    return (uint16_t)r;                   // r <= n; r == n: the next token starts the next window
+}
+
+__global__ void __launch_bounds__(dcta::THREADS, 4) k_lz4_decode_cta(const uint8_t *__restrict__ ch,
+                                                                  const Lz4Job *__restrict__ jobs,
+                                                                  const int *__restrict__ njobs_p, uint8_t *scratch,
+                                                                  int *err, unsigned *next_job)
+{
+    using namespace dcta;
+    extern __shared__ __align__(16) uint8_t sm_dcta[];
+    Smem &S = *reinterpret_cast<Smem *>(sm_dcta);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int njobs = *njobs_p;
     for (;;) {
-        unsigned got = 0;
-        if (lane == 0) got = atomicAdd(next_job, 1u);
-        const int jid = (int)__shfl_sync(FULLMASK, got, 0);
+        __syncthreads();
+        if (tid == 0) S.scal[0] = (int)atomicAdd(next_job, 1u);
+        __syncthreads();
+        const int jid = S.scal[0];
         if (jid >= njobs) break;
         const Lz4Job jb = jobs[jid];
         const uint8_t *__restrict__ in = ch + jb.src;
         const int isz = jb.csize;
         uint8_t *out = scratch + jb.dst;
         const int osz = jb.dlen;
-        int p = 0, op = 0;
-        bool bad = false, done = false;
+        int p = 0, op = 0;                 // window start in the input, output written so far
+        bool bad = false, done = false;    // block-uniform
         while (!done && !bad) {
-            const int n = min(W, isz - p);            // valid bytes in this window
-            const int rem = isz - p;                  // bytes left in the stream
-            for (int x = lane; x < n; x += 32) iwin[x] = __ldg(in + p + x);
-            __syncwarp();
-            // next[q]: parse one sequence header at q inside the window
-            for (int q = lane; q < W; q += 32) {
-                uint16_t nx = SEQ_STOP;
-                if (q < n) {
-                    int r = q + 1;
-                    const int tok = iwin[q];
-                    int lit = tok >> 4;
-                    bool ok = true;
+            const int rem = isz - p, n = min(DW, rem);
+            __syncthreads();
+            for (int x = tid; x < n; x += THREADS) S.win[x] = __ldg(in + p + x);
+            __syncthreads();
+            for (int q = tid; q < n; q += THREADS) S.J[0][q] = dcta_next(S.win, q, n, rem);
+            if (tid == 0) { S.path[0] = 0; S.scal[1] = PATH; }
+            __syncthreads();
+            // chain of token positions by doubling: after level k, path[0 .. 2^(k+1)) known
+            int len = 1, cur = 0, cnt = 0;
+            for (;;) {
+                for (int j = tid; j < len; j += THREADS) {
+                    const uint16_t pj = S.path[j];
+                    const uint16_t v = pj < n ? S.J[cur][pj] : pj;
+                    S.path[len + j] = v;
+                    if (v >= n) atomicMin(&S.scal[1], len + j);
+                }
+                __syncthreads();
+                const int t = S.scal[1];
+                if (t < 2 * len) { cnt = t; break; }
+                // J_{k+1} = J_k o J_k
+                for (int q = tid; q < n; q += THREADS) {
+                    const uint16_t v = S.J[cur][q];
+                    S.J[cur ^ 1][q] = v < n ? S.J[cur][v] : v;
+                }
+                cur ^= 1;
+                len *= 2;
+                __syncthreads();
+            }
+            const uint16_t term = S.path[cnt];          // n, ENDS or STOP
+            const int nseq = term == STOP ? cnt - 1 : cnt;
+            if (nseq > 0) {
+                // sequence fields and validity
+                if (tid == 0) S.scal[2] = 0;
+                int part = 0;
+                constexpr int PER = (MAXS + THREADS - 1) / THREADS;
+                const int i0 = tid * PER;
+                for (int i = i0; i < min(i0 + PER, nseq); i++) {
+                    const int q = S.path[i];
+                    const int tok = S.win[q];
+                    int r = q + 1, lit = tok >> 4;
                     if (lit == 15) {
                         int b = 255;
-                        while (b == 255) {
-                            if (r >= n) { ok = false; break; }
-                            b = iwin[r++];
-                            lit += b;
-                        }
+                        while (b == 255) { b = S.win[r++]; lit += b; }
                     }
-                    if (ok) {
-                        r += lit;
-                        if (r == rem) nx = SEQ_ENDS;             // literals reach the stream end: last sequence
-                        else if (r + 2 <= n) {
-                            r += 2;
-                            int ml = tok & 15;
-                            if (ml == 15) {
-                                int b = 255;
-                                while (b == 255) {
-                                    if (r >= n) { ok = false; break; }
-                                    b = iwin[r++];
-                                }
-                            }
-                            if (ok && r <= n) nx = (uint16_t)r;
-                        }
-                    }
-                }
-                J[q] = nx;
-            }
-            __syncwarp();
-            for (int b = 1; b < 5; b++) {
-                const uint16_t *Jp = J + (b - 1) * W;
-                uint16_t *Jb = J + b * W;
-                for (int q = lane; q < W; q += 32) {
-                    const uint16_t v = Jp[q];
-                    Jb[q] = v < n ? Jp[v] : v;
-                }
-                __syncwarp();
-            }
-            // batches of up to 32 sequences, starting at relative position `start`
-            int start = 0;
-            while (!done && !bad) {
-                if (start >= n || J[start] == SEQ_STOP) break;    // next sequence not complete here
-                int pos = start;
-#pragma unroll
-                for (int b = 0; b < 5; b++)
-                    if (((lane >> b) & 1) && pos < n) pos = J[b * W + pos];
-                const bool have = pos < n && J[pos] != SEQ_STOP;
-                int nb = __popc(__ballot_sync(FULLMASK, have));   // sequences present: a prefix of lanes
-                // parse my sequence
-                int lit = 0, ml = 0, off = 1, lp = 0;
-                bool last = false;
-                if (have) {
-                    int r = pos + 1;
-                    const int tok = iwin[pos];
-                    lit = tok >> 4;
-                    if (lit == 15) {
-                        int b = 255;
-                        while (b == 255) { b = iwin[r++]; lit += b; }
-                    }
-                    lp = p + r;
+                    S.lpos[i] = (uint16_t)r;
+                    S.llen[i] = lit;
                     r += lit;
-                    last = J[pos] == SEQ_ENDS;
-                    if (!last) {
-                        off = iwin[r] | (iwin[r + 1] << 8);
+                    int ml = 0, mo = 0;
+                    if (!(i == nseq - 1 && term == ENDS)) {
+                        mo = S.win[r] | (S.win[r + 1] << 8);
                         r += 2;
                         ml = tok & 15;
                         if (ml == 15) {
                             int b = 255;
-                            while (b == 255) { b = iwin[r++]; ml += b; }
+                            while (b == 255) { b = S.win[r++]; ml += b; }
                         }
                         ml += 4;
                     }
+                    S.off[i] = (uint16_t)mo;
+                    S.mlen[i] = ml;
+                    part += lit + ml;
                 }
-                // output positions: exclusive prefix of lit + ml
-                const int span = lit + ml;
-                int incl = span;
+                // exclusive scan of the output lengths
+                int incl = part;
 #pragma unroll
                 for (int o = 1; o < 32; o <<= 1) {
                     const int v = __shfl_up_sync(FULLMASK, incl, o);
                     if (lane >= o) incl += v;
                 }
-                const int my_op = op + incl - span;
-                // cut the batch where its output span would exceed RING (lane 0 always stays)
-                const unsigned over = __ballot_sync(FULLMASK, lane > 0 && lane < nb && incl > RING);
-                if (over) nb = min(nb, __ffs(over) - 1);
-                // a sequence after the stream's last one is malformed
-                const unsigned lastm = __ballot_sync(FULLMASK, lane < nb && last);
-                if (lastm) {
-                    const int li = __ffs(lastm) - 1;
-                    nb = li + 1;
-                    done = true;
+                if (lane == 31) S.wsum[warp] = incl;
+                __syncthreads();
+                int wbase = 0;
+                for (int w = 0; w < warp; w++) wbase += S.wsum[w];
+                int acc = wbase + incl - part;
+                for (int i = i0; i < min(i0 + PER, nseq); i++) {
+                    S.ostart[i] = acc;
+                    const int ms = op + acc + S.llen[i];             // absolute match start
+                    if (S.mlen[i] > 0 && (S.off[i] == 0 || S.off[i] > ms)) S.scal[2] = 1;
+                    acc += S.llen[i] + S.mlen[i];
                 }
-                const bool act = lane < nb;
-                const bool badme = act && (lit > osz - my_op || (!last && (off == 0 || off > my_op + lit ||
-                                                                           ml > osz - my_op - lit)));
-                if (__any_sync(FULLMASK, badme)) { bad = true; break; }
-                const int bspan = __shfl_sync(FULLMASK, incl, nb - 1);
-                // literals
-                if (act) {
-                    for (int i = 0; i < lit; i++) {
-                        const uint8_t v = __ldg(in + lp + i);
-                        out[my_op + i] = v;
-                        ring[(my_op + i) & (RING - 1)] = v;
+                if (tid == THREADS - 1) S.ostart[nseq] = acc;      // nseq <= MAXS: the last thread holds the total
+                __syncthreads();
+                const int total = S.ostart[nseq];
+                if (S.scal[2] || total > osz - op) { bad = true; break; }
+                // output in groups of at most DCAP bytes
+                int a = 0;
+                while (a < nseq) {
+                    const int base = S.ostart[a];
+                    int lo = a + 1, hi = nseq;                      // largest b with ostart[b] - base <= DCAP
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (S.ostart[mid] - base <= DCAP) lo = mid; else hi = mid - 1;
                     }
-                }
-                __syncwarp();
-                // matches in frontier rounds
-                const int mstart = my_op + lit;
-                const int src = mstart - off;
-                const int src_end = src + min(ml, off);
-                const int batch_end = op + bspan;
-                const bool from_ring = src >= batch_end - RING;
-                bool mine = !(act && ml > 0);
-                for (int round = 0; round < 33; round++) {
-                    const int frontier = (int)__reduce_min_sync(FULLMASK, mine ? 0x7FFFFFFFu : (unsigned)mstart);
-                    if (frontier == 0x7FFFFFFF) break;
-                    if (!mine && src_end <= frontier) {
-                        for (int i = 0; i < ml; i++) {
-                            const int sp = src + (off >= ml ? i : i % off);
-                            const uint8_t v = from_ring ? ring[sp & (RING - 1)] : __ldcg(out + sp);
-                            out[mstart + i] = v;
-                            ring[(mstart + i) & (RING - 1)] = v;
+                    const int b = lo;
+                    if (S.ostart[b] - base <= DCAP) {
+                        const int span = S.ostart[b] - base;
+                        // each thread fills a contiguous run of output bytes: one binary search
+                        // for the sequence holding its first byte, then a forward walk
+                        const int per = (span + THREADS - 1) / THREADS;
+                        const int x0 = tid * per, x1 = min(span, x0 + per);
+                        if (x0 < x1) {
+                            int l2 = a, h2 = b - 1;
+                            while (l2 < h2) {
+                                const int mid = (l2 + h2 + 1) >> 1;
+                                if (S.ostart[mid] - base <= x0) l2 = mid; else h2 = mid - 1;
+                            }
+                            int s0 = S.ostart[l2] - base, s1 = S.ostart[l2 + 1] - base;
+                            int lit = S.llen[l2], d = S.off[l2], lp = S.lpos[l2];
+                            for (int x = x0; x < x1; x++) {
+                                while (x >= s1) {                   // next non-empty sequence
+                                    l2++;
+                                    s0 = s1;
+                                    s1 = S.ostart[l2 + 1] - base;
+                                    lit = S.llen[l2]; d = S.off[l2]; lp = S.lpos[l2];
+                                }
+                                const int rel = x - s0;
+                                uint32_t v;
+                                if (rel < lit) {
+                                    v = RES | S.win[lp + rel];
+                                } else {
+                                    const int m0 = s0 + lit, k = x - m0;
+                                    const int src = d > k ? x - d : m0 - d + k % d;
+                                    v = src >= 0 ? (uint32_t)src : (RES | __ldcg(out + op + base + src));
+                                }
+                                S.st[x] = v;
+                            }
                         }
-                        mine = true;
+                        __syncthreads();
+                        for (;;) {                                 // pointer jumping
+                            int open = 0;
+                            for (int x = tid; x < span; x += THREADS) {
+                                const uint32_t v = S.st[x];
+                                if (!(v & RES)) {
+                                    const uint32_t t = S.st[v];
+                                    S.st[x] = t;
+                                    open |= !(t & RES);
+                                }
+                            }
+                            if (!__syncthreads_or(open)) break;
+                        }
+                        uint8_t *o = out + op + base;
+                        for (int x = tid; x < span; x += THREADS) o[x] = (uint8_t)S.st[x];
+                        a = b;
+                    } else {
+                        // one sequence larger than DCAP: literals, then the match from global memory
+                        const int abs0 = op + base, lit = S.llen[a], ml = S.mlen[a], d = S.off[a];
+                        for (int x = tid; x < lit; x += THREADS) out[abs0 + x] = S.win[S.lpos[a] + x];
+                        __syncthreads();
+                        const int m0 = abs0 + lit;
+                        for (int x = tid; x < ml; x += THREADS) out[m0 + x] = __ldcg(out + m0 - d + (d > x ? x : x % d));
+                        a = a + 1;
                     }
-                    __syncwarp();
+                    __syncthreads();
                 }
-                // advance past the batch
-                const int nxt = __shfl_sync(FULLMASK, have ? (int)J[pos] : 0, nb - 1);
-                op += bspan;
-                if (done) break;
-                start = nxt;
-            }
-            if (done || bad) break;
-            if (start > 0) {
-                p += start;      // restage at the first sequence not decoded yet
+                op += total;
+                if (term == ENDS) { done = true; break; }
+                p += term == STOP ? S.path[cnt - 1] : n;
                 continue;
             }
             // the sequence at p does not fit in a window: decode it alone, header from global
-            {
-                int r = p;
+            if (tid == 0) {
+                int r = p, f = 0, lit = 0, mo = 0, ml = 0, fin = 0;
                 const int tok = __ldg(in + r++);
-                int lit = tok >> 4;
+                lit = tok >> 4;
                 if (lit == 15) {
-                    int b = 255;
-                    while (b == 255) {
-                        if (r >= isz) { bad = true; break; }
-                        b = __ldg(in + r++);
-                        lit += b;
+                    int bb = 255;
+                    while (bb == 255) {
+                        if (r >= isz) { f = 1; break; }
+                        bb = __ldg(in + r++);
+                        lit += bb;
                     }
-                    if (bad) break;
                 }
-                if (lit > isz - r || lit > osz - op) { bad = true; break; }
-                for (int x = lane; x < lit; x += 32) {
-                    const uint8_t v = __ldg(in + r + x);
-                    out[op + x] = v;
-                    ring[(op + x) & (RING - 1)] = v;
-                }
-                r += lit;
-                op += lit;
-                __syncwarp();
-                if (r == isz) { done = true; break; }
-                if (isz - r < 2) { bad = true; break; }
-                const int mo = __ldg(in + r) | (__ldg(in + r + 1) << 8);
-                r += 2;
-                int ml = tok & 15;
-                if (ml == 15) {
-                    int b = 255;
-                    while (b == 255) {
-                        if (r >= isz) { bad = true; break; }
-                        b = __ldg(in + r++);
-                        ml += b;
+                const int lp = r;
+                if (!f && (lit > isz - r || lit > osz - op)) f = 1;
+                if (!f) {
+                    r += lit;
+                    if (r == isz) {
+                        fin = 1;
+                    } else if (isz - r < 2) {
+                        f = 1;
+                    } else {
+                        mo = __ldg(in + r) | (__ldg(in + r + 1) << 8);
+                        r += 2;
+                        ml = tok & 15;
+                        if (ml == 15) {
+                            int bb = 255;
+                            while (bb == 255) {
+                                if (r >= isz) { f = 1; break; }
+                                bb = __ldg(in + r++);
+                                ml += bb;
+                            }
+                        }
+                        ml += 4;
+                        if (!f && (mo == 0 || mo > op + lit || ml > osz - op - lit)) f = 1;
                     }
-                    if (bad) break;
                 }
-                ml += 4;
-                if (mo == 0 || mo > op || ml > osz - op) { bad = true; break; }
-                const bool ringok = mo + ml <= RING;
-                for (int x = lane; x < ml; x += 32) {
-                    const int sp = op - mo + (mo >= ml ? x : x % mo);
-                    const uint8_t v = ringok ? ring[sp & (RING - 1)] : __ldcg(out + sp);
-                    out[op + x] = v;
-                    ring[(op + x) & (RING - 1)] = v;
-                }
-                op += ml;
-                p = r;
-                __syncwarp();
+                S.scal[2] = f; S.scal[3] = lit; S.scal[4] = lp; S.scal[5] = mo; S.scal[6] = ml; S.scal[7] = fin ? -1 : r;
+            }
+            __syncthreads();
+            if (S.scal[2]) { bad = true; break; }
+            {
+                const int lit = S.scal[3], lp = S.scal[4], mo = S.scal[5], ml = S.scal[6], nr = S.scal[7];
+                for (int x = tid; x < lit; x += THREADS) out[op + x] = __ldg(in + lp + x);
+                __syncthreads();
+                const int m0 = op + lit;
+                for (int x = tid; x < ml; x += THREADS) out[m0 + x] = __ldcg(out + m0 - mo + (mo > x ? x : x % mo));
+                __syncthreads();
+                op += lit + ml;
+                if (nr < 0) done = true; else p = nr;
             }
         }
         if (!bad && op != osz) bad = true;
-        if (bad && lane == 0) dev_fail(err, DE_LZ4);
-        __syncwarp();
+        if (bad && tid == 0) dev_fail(err, DE_LZ4);
     }
 }
 
@@ -477,17 +544,28 @@ __global__ void __launch_bounds__(256) k_scatter_fast(Geom g, const uint8_t *__r
             uint8_t *o = out + ((row0 + r) * ld + col0 + cc) * TS;
             uint32_t v0, v1, v2, v3;
             transpose4x4(w[0], w[1], w[2], w[3], v0, v1, v2, v3);
+            const bool a16 = (reinterpret_cast<uintptr_t>(o) & 15) == 0;
             if constexpr (TS == 8) {
                 uint32_t h0, h1, h2, h3;
                 transpose4x4(w[4], w[5], w[6], w[7], h0, h1, h2, h3);
-                uint64_t *o8 = reinterpret_cast<uint64_t *>(o);
-                o8[0] = ((uint64_t)h0 << 32) | v0;
-                o8[1] = ((uint64_t)h1 << 32) | v1;
-                o8[2] = ((uint64_t)h2 << 32) | v2;
-                o8[3] = ((uint64_t)h3 << 32) | v3;
+                if (a16) {
+                    uint4 *o16 = reinterpret_cast<uint4 *>(o);
+                    o16[0] = make_uint4(v0, h0, v1, h1);
+                    o16[1] = make_uint4(v2, h2, v3, h3);
+                } else {
+                    uint64_t *o8 = reinterpret_cast<uint64_t *>(o);
+                    o8[0] = ((uint64_t)h0 << 32) | v0;
+                    o8[1] = ((uint64_t)h1 << 32) | v1;
+                    o8[2] = ((uint64_t)h2 << 32) | v2;
+                    o8[3] = ((uint64_t)h3 << 32) | v3;
+                }
             } else {
-                uint32_t *o4 = reinterpret_cast<uint32_t *>(o);
-                o4[0] = v0; o4[1] = v1; o4[2] = v2; o4[3] = v3;
+                if (a16) {
+                    *reinterpret_cast<uint4 *>(o) = make_uint4(v0, v1, v2, v3);
+                } else {
+                    uint32_t *o4 = reinterpret_cast<uint32_t *>(o);
+                    o4[0] = v0; o4[1] = v1; o4[2] = v2; o4[3] = v3;
+                }
             }
         }
     }
@@ -666,94 +744,184 @@ __device__ __forceinline__ int64_t probe_offset(int64_t t)
     return 1 + 64 * (q * (q - 1) / 2) + q * (r + 1);
 }
 
-// Warp-cooperative LZ4 block compressor in limited-output mode with capacity `cap`.
-// Returns the compressed size, or 0 when it does not fit; *need_out receives the
-// smallest capacity for which it would have fit.  All lanes must call it.
-__device__ int warp_lz4_compress(const uint8_t *__restrict__ src, int n, uint8_t *__restrict__ dst, int cap,
-                                 uint32_t *tab, int *need_out)
+// Shared-memory window over one stream for the encoder: positions [lo, hi) sit at
+// r[x & (ERING - 1)], the first 16 ring bytes mirrored past its end so that 4-byte reads
+// never wrap.  The window follows the parse position; reads outside it (far search
+// probes, old match candidates) go to global memory.  Without it the candidate reads of
+// low-entropy streams, spread over the last few KiB, mostly miss L1.
+constexpr int ERING = 8192, ESEG = 1024, ELOOK = 512;
+
+struct EncSrc {
+    const uint8_t *g;   // the stream in global memory
+    uint8_t *r;         // ERING + 16 bytes, 16-byte aligned
+    int lo, hi, n;
+};
+
+__device__ __forceinline__ uint32_t es_byte(const EncSrc &s, int x)
+{
+    return (x >= s.lo && x < s.hi) ? (uint32_t)s.r[x & (ERING - 1)] : (uint32_t)__ldg(s.g + x);
+}
+
+__device__ __forceinline__ uint32_t es_rd32(const EncSrc &s, int x)
+{
+    if (x >= s.lo && x + 4 <= s.hi) {
+        const int o = x & (ERING - 1);
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(s.r) + (o >> 2);
+        return __funnelshift_r(w[0], w[1], (uint32_t)(o & 3) * 8);
+    }
+    return ld4u(s.g + x);
+}
+
+// liblz4's hash of the 4 (byU16 tables) or 5 (byU32 tables) bytes at p.
+__device__ __forceinline__ uint32_t es_hash(const EncSrc &s, int p, bool small)
+{
+    if (small) return (es_rd32(s, p) * 2654435761u) >> (32 - 13);
+    const uint64_t v = (uint64_t)es_rd32(s, p) | ((uint64_t)es_byte(s, p + 4) << 32);
+    return (uint32_t)(((v << 24) * 889523592379ull) >> (64 - 12));
+}
+
+// Extends the window up to position `want` (warp-uniform) in ESEG pieces.
+__device__ __forceinline__ void es_fill(EncSrc &s, int want)
 {
     const int lane = threadIdx.x & 31;
-    const bool small = n < 65536 + 12 - 1;
+    while (s.hi < s.n && s.hi < want) {
+        const int base = s.hi, cnt = min(ESEG, s.n - base);
+        __syncwarp();                                    // reads of the slots being replaced are done
+        for (int x = lane * 4; x < cnt; x += 128) {
+            uint32_t v = 0;
+            if (base + x + 8 <= s.n) {
+                v = ld4u(s.g + base + x);
+            } else {
+                for (int k = 0; k < 4; k++)
+                    if (base + x + k < s.n) v |= (uint32_t)__ldg(s.g + base + x + k) << (8 * k);
+            }
+            const int o = (base + x) & (ERING - 1);
+            *reinterpret_cast<uint32_t *>(s.r + o) = v;
+            if (o < 16) *reinterpret_cast<uint32_t *>(s.r + ERING + o) = v;
+        }
+        s.hi = base + cnt;
+        s.lo = max(s.lo, base + ESEG - ERING);
+        __syncwarp();
+    }
+}
+
+// Shared-memory accesses through 32-bit shared-window addresses (volatile: they keep
+// their order relative to each other, which the table updates rely on).
+__device__ __forceinline__ uint32_t lds32(uint32_t a)
+{
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ uint32_t lds_tab(uint32_t a, bool small)
+{
+    uint32_t v;
+    if (small) {
+        uint16_t h;
+        asm volatile("ld.shared.u16 %0, [%1];" : "=h"(h) : "r"(a) : "memory");
+        v = h;
+    } else {
+        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+    }
+    return v;
+}
+__device__ __forceinline__ void sts_tab(uint32_t a, uint32_t v, bool small)
+{
+    if (small) asm volatile("st.shared.u16 [%0], %1;" ::"r"(a), "h"((uint16_t)v) : "memory");
+    else asm volatile("st.shared.u32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+
+// liblz4's hash of the 4 bytes v4 at a position (byU16 tables) or of those and the fifth
+// byte b4 (byU32 tables).
+template <bool SMALL>
+__device__ __forceinline__ uint32_t lz_hash_v(uint32_t v4, uint32_t b4)
+{
+    if (SMALL) return (v4 * 2654435761u) >> (32 - 13);
+    const uint64_t v = (uint64_t)v4 | ((uint64_t)b4 << 32);
+    return (uint32_t)(((v << 24) * 889523592379ull) >> (64 - 12));
+}
+
+// Warp-cooperative LZ4 block compressor in limited-output mode with capacity `cap`.
+// Returns the compressed size, or 0 when it does not fit; *need_out receives the
+// smallest capacity for which it would have fit.  All lanes must call it; every
+// position, candidate and output offset below is warp-uniform.  SMALL selects liblz4's
+// byU16 table (inputs below 64 KiB + 11 bytes: 13-bit hash of 4 bytes) over its byU32
+// table (12-bit hash of 5 bytes, 65535-byte distance limit).
+//
+// Two regimes.  Searching (no match at the parse position): one step evaluates 32
+// consecutive probes of liblz4's search (its step schedule), resolving probes that share
+// a hash bucket in probe order with __match_any_sync.  Right after a match liblz4
+// inserts ip - 2 and tests ip itself; on low-entropy data that test nearly always
+// succeeds, so it runs as a short scalar path that every lane executes identically (the
+// window bytes around ip and around the candidate come from a few aligned shared-memory
+// words, the match length from one 64-bit compare, table updates written by all lanes
+// with the same value), leaving the warp-wide machinery for long matches and searches.
+template <bool SMALL>
+__device__ __forceinline__ int warp_lz4_compress(const uint8_t *__restrict__ src, int n, uint8_t *__restrict__ dst,
+                                                 int cap, uint32_t *tab, uint8_t *ring, int *need_out)
+{
+    const int lane = threadIdx.x & 31;
     uint16_t *tab16 = reinterpret_cast<uint16_t *>(tab);
     for (int i = lane; i < 4096; i += 32) tab[i] = 0u;
+    EncSrc s;
+    s.g = src; s.r = ring; s.lo = 0; s.hi = 0; s.n = n;
+    const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(ring), tab_s = (uint32_t)__cvta_generic_to_shared(tab);
+    constexpr uint32_t TSH = SMALL ? 1 : 2;             // table entry size: 2 or 4 bytes
     __syncwarp();
     int need = 0, op = 0, anchor = 0, ip = 1, mt = 0;
     int token_pos = 0, token_val = 0;
     const int mfl1 = n - 12 + 1, mlimit = n - 5;
-#define TGET(h) (small ? (uint32_t)tab16[h] : tab[h])
-#define TPUT(h, v) do { if (small) tab16[h] = (uint16_t)(v); else tab[h] = (uint32_t)(v); } while (0)
+#define TGET(h) (SMALL ? (uint32_t)tab16[h] : tab[h])
+#define TPUT(h, v) do { if (SMALL) tab16[h] = (uint16_t)(v); else tab[h] = (uint32_t)(v); } while (0)
 #define NEED(x) do { const int nx_ = (x); need = max(need, nx_); if (nx_ > cap) { *need_out = need; return 0; } } while (0)
     if (n < 13) goto last_literals;
-    if (lane == 0) TPUT(lz_hash(src, small), 0);
+    es_fill(s, ELOOK);
+    if (lane == 0) TPUT(es_hash(s, 0, SMALL), 0);
     __syncwarp();
-    {
-    // One 32-lane step evaluates consecutive table operations of the serial algorithm.
-    // Right after a match (`after`), lane 0 is the insert of ip-2, lane 1 the immediate
-    // re-match probe at ip, and lanes 2.. the first probes of the search that follows
-    // from ip+1; otherwise all lanes are search probes.  Insertions happen in increasing
-    // position order, so each probe sees the latest earlier insert of its hash: the
-    // table before the step, or a lower lane of the same hash within it.
-    int p0 = 1;
-    int64_t t0 = 0;
-    bool after = false;
     for (;;) {
-        bool rematch = false;
-        for (;;) {
-            int kind = 2;                       // 0 insert only, 1 re-match probe, 2 search probe
-            int64_t t = t0 + lane;
-            if (after) {
-                kind = lane == 0 ? 0 : (lane == 1 ? 1 : 2);
-                t = t0 + lane - 2;
-            }
-            int64_t p;
-            bool valid;
-            if (kind == 0) { p = ip - 2; valid = true; }
-            else if (kind == 1) { p = ip; valid = true; }
-            else {
+        // ---- search from ip: probes p0 + probe_offset(t), t = 0, 1, ...
+        {
+            const int p0 = ip;
+            int64_t t0 = 0;
+            for (;;) {
+                es_fill(s, p0 + (int)(probe_offset(t0) < n ? probe_offset(t0) : (int64_t)n) + ELOOK);
+                const int64_t t = t0 + lane;
                 // the step is 1 for the first 66 probes: positions are p0 + t there
                 const bool dense = t0 + 32 <= 65;
-                p = dense ? p0 + t : p0 + probe_offset(t);
+                const int64_t p = dense ? p0 + t : p0 + probe_offset(t);
                 const int64_t pn = dense ? p + 1 : p0 + probe_offset(t + 1);
-                valid = pn <= mfl1;
+                const bool valid = pn <= mfl1;
+                const uint32_t h = valid ? es_hash(s, (int)p, SMALL) : (0x80000000u | (uint32_t)lane);
+                const uint32_t ctab = valid ? TGET(h) : 0u;
+                const unsigned peers = __match_any_sync(FULLMASK, h);
+                const unsigned lower = peers & ((1u << lane) - 1u);
+                const int srcl = lower ? 31 - __clz(lower) : lane;
+                const int pl = __shfl_sync(FULLMASK, (int)p, srcl);
+                const uint32_t cand = lower ? (uint32_t)pl : ctab;
+                const bool m = valid && (SMALL || cand + 65535u >= (uint32_t)p) &&
+                               es_rd32(s, (int)cand) == es_rd32(s, (int)p);
+                const unsigned mm = __ballot_sync(FULLMASK, m), em = __ballot_sync(FULLMASK, !valid);
+                const int W = mm ? __ffs(mm) - 1 : 32, E = em ? __ffs(em) - 1 : 32;
+                const int lastw = min(W, E - 1);
+                __syncwarp();
+                if (lane <= lastw) {
+                    const unsigned upto = (lastw >= 31) ? FULLMASK : ((2u << lastw) - 1u);
+                    const unsigned higher = peers & ~((2u << lane) - 1u) & upto;
+                    if (!higher) TPUT(h, (uint32_t)p);
+                }
+                __syncwarp();
+                if (W < E) {
+                    ip = __shfl_sync(FULLMASK, (int)p, W);
+                    mt = (int)__shfl_sync(FULLMASK, cand, W);
+                    break;
+                }
+                if (E < 32) goto last_literals;
+                t0 += 32;
             }
-            const bool probe = kind != 0 && valid;
-            const uint32_t h = valid ? lz_hash(src + p, small) : (0x80000000u | (uint32_t)lane);
-            const uint32_t ctab = probe ? TGET(h) : 0u;
-            const unsigned peers = __match_any_sync(FULLMASK, h);
-            const unsigned lower = peers & ((1u << lane) - 1u);
-            const int srcl = lower ? 31 - __clz(lower) : lane;
-            const int pl = __shfl_sync(FULLMASK, (int)p, srcl);
-            const uint32_t cand = lower ? (uint32_t)pl : ctab;
-            const bool m = probe && (small || cand + 65535u >= (uint32_t)p) && ld4u(src + cand) == ld4u(src + p);
-            const unsigned mm = __ballot_sync(FULLMASK, m), em = __ballot_sync(FULLMASK, kind != 0 && !valid);
-            const int W = mm ? __ffs(mm) - 1 : 32, E = em ? __ffs(em) - 1 : 32;
-            const int lastw = min(W, E - 1);
-            __syncwarp();
-            if (lane <= lastw) {
-                const unsigned upto = (lastw >= 31) ? FULLMASK : ((2u << lastw) - 1u);
-                const unsigned higher = peers & ~((2u << lane) - 1u) & upto;
-                if (!higher) TPUT(h, (uint32_t)p);
-            }
-            __syncwarp();
-            if (W < E) {
-                ip = __shfl_sync(FULLMASK, (int)p, W);
-                mt = (int)__shfl_sync(FULLMASK, cand, W);
-                rematch = after && W == 1;
-                break;
-            }
-            if (E < 32) goto last_literals;
-            t0 += after ? 30 : 32;
-            after = false;
-        }
-        if (rematch) {   // a match right at the previous match's end: no literals
-            token_pos = op;
-            token_val = 0;
-            op += 1;
-            goto next_match;
         }
         for (;;) {   // extend the match backwards
             const int k = lane + 1;
-            const bool ok = (ip - k >= anchor) && (mt - k >= 0) && __ldg(src + ip - k) == __ldg(src + mt - k);
+            const bool ok = (ip - k >= anchor) && (mt - k >= 0) && es_byte(s, ip - k) == es_byte(s, mt - k);
             const unsigned badm = __ballot_sync(FULLMASK, !ok);
             const int ext = badm ? __ffs(badm) - 1 : 32;
             ip -= ext;
@@ -774,18 +942,18 @@ __device__ int warp_lz4_compress(const uint8_t *__restrict__ src, int n, uint8_t
             } else {
                 token_val = lit << 4;
             }
-            for (int x = lane; x < lit; x += 32) dst[op + x] = __ldg(src + anchor + x);
+            for (int x = lane; x < lit; x += 32) dst[op + x] = (uint8_t)es_byte(s, anchor + x);
             op += lit;
         }
-    next_match:
-        {
+        {   // the match found by the search: offset, length (warp-wide compare), token
             const int mo = ip - mt;
             if (lane == 0) { dst[op] = (uint8_t)mo; dst[op + 1] = (uint8_t)(mo >> 8); }
             op += 2;
             int mc = 0;
             for (int a = ip + 4, bpos = mt + 4;; a += 32, bpos += 32) {
+                es_fill(s, a + 32 + ELOOK);
                 const int pa = a + lane;
-                const bool eq = pa < mlimit && __ldg(src + pa) == __ldg(src + bpos + lane);
+                const bool eq = pa < mlimit && es_byte(s, pa) == es_byte(s, bpos + lane);
                 const unsigned ne = __ballot_sync(FULLMASK, !eq);
                 const int cnum = ne ? __ffs(ne) - 1 : 32;
                 mc += cnum;
@@ -804,12 +972,82 @@ __device__ int warp_lz4_compress(const uint8_t *__restrict__ src, int n, uint8_t
             }
             if (lane == 0) dst[token_pos] = (uint8_t)token_val;
         }
-        anchor = ip;
-        if (ip >= mfl1) break;
-        after = true;
-        p0 = ip + 1;
-        t0 = 0;
-    }
+        // ---- after each match: insert ip - 2, look ip up, insert it; a hit is a match with
+        // no literals (scalar path, identical on every lane)
+        for (;;) {
+            anchor = ip;
+            if (ip >= mfl1) goto last_literals;
+            if (ip + 64 > s.hi) es_fill(s, ip + ELOOK);
+            uint32_t a0, a1, a2, a3;                         // bytes ip-2 .. ip+13
+            {
+                const uint32_t o = (uint32_t)(ip - 2) & (ERING - 1);
+                const uint32_t wa = ring_s + (o & ~3u);
+                const uint32_t sh = (o & 3) * 8;
+                const uint32_t w0 = lds32(wa), w1 = lds32(wa + 4), w2 = lds32(wa + 8), w3 = lds32(wa + 12),
+                               w4 = lds32(wa + 16);
+                a0 = __funnelshift_r(w0, w1, sh);
+                a1 = __funnelshift_r(w1, w2, sh);
+                a2 = __funnelshift_r(w2, w3, sh);
+                a3 = __funnelshift_r(w3, w4, sh);
+            }
+            const uint32_t v0 = __funnelshift_r(a0, a1, 16);   // bytes ip .. ip+3
+            const uint32_t h2 = lz_hash_v<SMALL>(a0, a1 & 0xffu), h0 = lz_hash_v<SMALL>(v0, (a1 >> 16) & 0xffu);
+            const uint32_t c = (h0 == h2) ? (uint32_t)(ip - 2) : lds_tab(tab_s + (h0 << TSH), SMALL);
+            sts_tab(tab_s + (h2 << TSH), (uint32_t)(ip - 2), SMALL);
+            sts_tab(tab_s + (h0 << TSH), (uint32_t)ip, SMALL);
+            uint32_t cv, cn0, cn1;                            // bytes c .. c+11
+            if ((int)c >= s.lo) {
+                const uint32_t o = c & (ERING - 1);
+                const uint32_t wa = ring_s + (o & ~3u);
+                const uint32_t sh = (o & 3) * 8;
+                const uint32_t w0 = lds32(wa), w1 = lds32(wa + 4), w2 = lds32(wa + 8), w3 = lds32(wa + 12);
+                cv = __funnelshift_r(w0, w1, sh);
+                cn0 = __funnelshift_r(w1, w2, sh);
+                cn1 = __funnelshift_r(w2, w3, sh);
+            } else {
+                cv = ld4u(src + c);
+                cn0 = ld4u(src + c + 4);
+                cn1 = ld4u(src + c + 8);
+            }
+            if (!((SMALL || c + 65535u >= (uint32_t)ip) && cv == v0)) {
+                ip += 1;
+                __syncwarp();
+                break;                                        // back to searching from ip + 1
+            }
+            const uint64_t nx = ((uint64_t)__funnelshift_r(a2, a3, 16) << 32) | __funnelshift_r(a1, a2, 16);
+            const uint64_t x = nx ^ (((uint64_t)cn1 << 32) | cn0);
+            const int lim = mlimit - (ip + 4);
+            int mc = x ? (__ffsll((long long)x) - 1) >> 3 : 8;
+            if (mc >= lim) {
+                mc = lim;
+            } else if (mc == 8) {                            // long match: warp-wide compare from ip + 12
+                for (int a = ip + 12, bpos = (int)c + 12;; a += 32, bpos += 32) {
+                    es_fill(s, a + 32 + ELOOK);
+                    const int pa = a + lane;
+                    const bool eq = pa < mlimit && es_byte(s, pa) == es_byte(s, bpos + lane);
+                    const unsigned ne = __ballot_sync(FULLMASK, !eq);
+                    const int cnum = ne ? __ffs(ne) - 1 : 32;
+                    mc += cnum;
+                    if (cnum < 32) break;
+                }
+            }
+            const int mo = ip - (int)c;
+            NEED(op + 9 + (mc >= 15 ? (mc + 240) / 255 : 0));
+            if (lane == 0) {
+                uint8_t *dp = dst + op;
+                dp[0] = (uint8_t)(mc >= 15 ? 15 : mc);
+                dp[1] = (uint8_t)mo;
+                dp[2] = (uint8_t)(mo >> 8);
+            }
+            op += 3;
+            if (mc >= 15) {
+                const int rem = mc - 15, nff = rem / 255;
+                for (int xx = lane; xx < nff; xx += 32) dst[op + xx] = 255;
+                if (lane == 0) dst[op + nff] = (uint8_t)(rem % 255);
+                op += nff + 1;
+            }
+            ip += mc + 4;
+        }
     }
 last_literals:
     {
@@ -825,7 +1063,7 @@ last_literals:
             if (lane == 0) dst[op] = (uint8_t)(last << 4);
             op += 1;
         }
-        for (int x = lane; x < last; x += 32) dst[op + x] = __ldg(src + anchor + x);
+        for (int x = lane; x < last; x += 32) dst[op + x] = (uint8_t)es_byte(s, anchor + x);
         op += last;
     }
 #undef TGET
@@ -841,13 +1079,14 @@ last_literals:
 // Streams are handed out dynamically (one atomic per stream): compressible streams cost
 // far more than incompressible ones, and in shuffled float data they recur at a fixed
 // stride, which a static round-robin assignment would pile onto the same warps.
-__global__ void __launch_bounds__(128) k_lz4_encode(const uint8_t *__restrict__ img, int64_t nstreams_total,
+__global__ void __launch_bounds__(96, 3) k_lz4_encode(const uint8_t *__restrict__ img, int64_t nstreams_total,
                                                     int neblock, uint8_t *slots, EncStream *es,
                                                     unsigned long long *next)
 {
-    extern __shared__ uint32_t sm_tab[];
+    extern __shared__ __align__(16) uint32_t sm_tab[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint32_t *tab = sm_tab + warp * 4096;
+    uint32_t *tab = sm_tab + warp * (4096 + (ERING + 16) / 4);
+    uint8_t *ring = reinterpret_cast<uint8_t *>(tab + 4096);
     for (;;) {
         unsigned long long got = 0;
         if (lane == 0) got = atomicAdd(next, 1ull);
@@ -870,7 +1109,9 @@ __global__ void __launch_bounds__(128) k_lz4_encode(const uint8_t *__restrict__ 
             e.kind = SK_RUN; e.csize = first; e.need = 0;
         } else {
             int need = 0;
-            const int cs = warp_lz4_compress(src, neblock, slots + sid * neblock, neblock, tab, &need);
+            const int cs = neblock < 65536 + 12 - 1
+                               ? warp_lz4_compress<true>(src, neblock, slots + sid * neblock, neblock, tab, ring, &need)
+                               : warp_lz4_compress<false>(src, neblock, slots + sid * neblock, neblock, tab, ring, &need);
             if (cs > 0 && cs < neblock) { e.kind = SK_LZ4; e.csize = cs; e.need = need; }
             else { e.kind = SK_RAW; e.csize = neblock; e.need = need; }
         }
@@ -928,9 +1169,45 @@ __global__ void k_layout(Geom g, int nstreams, int neblock, EncStream *es, EncCh
     }
 }
 
+// Copies len bytes with the whole CTA: 16-byte aligned stores to dst, each fed by five
+// aligned 32-bit loads of src funnel-shifted into place.  Source words are only read
+// inside [lo, hi); pieces whose words would leave it are copied bytewise.
+__device__ __forceinline__ void cta_copy(uint8_t *__restrict__ dst, const uint8_t *__restrict__ src, int len,
+                                         const uint8_t *lo, const uint8_t *hi)
+{
+    int head = (int)((16 - (reinterpret_cast<uintptr_t>(dst) & 15)) & 15);
+    if (head > len) head = len;
+    for (int x = threadIdx.x; x < head; x += blockDim.x) dst[x] = __ldg(src + x);
+    const int nvec = (len - head) >> 4;
+    for (int v = threadIdx.x; v < nvec; v += blockDim.x) {
+        const int s = head + (v << 4);
+        const uint8_t *sp = src + s;
+        const uint8_t *sa = reinterpret_cast<const uint8_t *>(reinterpret_cast<uintptr_t>(sp) & ~uintptr_t(3));
+        uint4 o;
+        if (sa >= lo && sa + 20 <= hi) {
+            const uint32_t *w = reinterpret_cast<const uint32_t *>(sa);
+            const uint32_t sh = (uint32_t)(reinterpret_cast<uintptr_t>(sp) & 3) * 8;
+            const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3), w4 = __ldg(w + 4);
+            o.x = __funnelshift_r(w0, w1, sh);
+            o.y = __funnelshift_r(w1, w2, sh);
+            o.z = __funnelshift_r(w2, w3, sh);
+            o.w = __funnelshift_r(w3, w4, sh);
+        } else {
+            uint32_t b[4];
+            for (int k = 0; k < 4; k++)
+                b[k] = (uint32_t)__ldg(sp + 4 * k) | ((uint32_t)__ldg(sp + 4 * k + 1) << 8) |
+                       ((uint32_t)__ldg(sp + 4 * k + 2) << 16) | ((uint32_t)__ldg(sp + 4 * k + 3) << 24);
+            o = make_uint4(b[0], b[1], b[2], b[3]);
+        }
+        *reinterpret_cast<uint4 *>(dst + s) = o;
+    }
+    for (int x = head + (nvec << 4) + threadIdx.x; x < len; x += blockDim.x) dst[x] = __ldg(src + x);
+}
+
 // E5: write headers, bstarts, csize words and payloads.  One CTA per (chunk, block).
 __global__ void __launch_bounds__(256) k_emit(Geom g, int nstreams, int neblock, bool shuffle, int splitflag,
                                               const uint8_t *__restrict__ img, const uint8_t *__restrict__ slots,
+                                              int64_t img_bytes,
                                               const EncStream *__restrict__ es, const EncChunk *__restrict__ ec,
                                               uint8_t *__restrict__ outbuf)
 {
@@ -982,7 +1259,10 @@ __global__ void __launch_bounds__(256) k_emit(Geom g, int nstreams, int neblock,
             else { word = neblock; payload = blk_img + (int64_t)j * neblock; plen = neblock; }
             if (threadIdx.x < 4) w[threadIdx.x] = (uint8_t)((uint32_t)word >> (8 * threadIdx.x));
             if (e.kind == SK_RUN && e.csize != 0 && threadIdx.x == 4) w[4] = 1;
-            for (int x = threadIdx.x; x < plen; x += blockDim.x) w[4 + x] = payload[x];
+            if (plen > 0) {
+                const uint8_t *base = e.kind == SK_LZ4 ? slots : img;
+                cta_copy(w + 4, payload, plen, base, base + img_bytes);
+            }
         }
     }
 }
@@ -1012,7 +1292,8 @@ int decode_container(const Geom &g, const uint8_t *d_chunks, int64_t chunks_byte
 int decode_finish(DecodeWork *w, cudaStream_t st)
 {
     int h_err = 0;
-    cudaMemcpyAsync(&h_err, w->counters.as<int>() + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    const int *cnt = w->ext_counters ? w->ext_counters : w->counters.as<int>();
+    cudaMemcpyAsync(&h_err, cnt + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return -101;
     return h_err;
 }
@@ -1026,10 +1307,11 @@ int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, 
     DevBuf &bd = w->bd, &sd = w->sd, &jobs = w->jobs, &scratch = w->scratch, &counters = w->counters;
     if (!bd.allocate(sizeof(BlockDesc) * nbl, dev) || !sd.allocate(sizeof(StreamDesc) * nbl * 8, dev) ||
         !jobs.allocate(sizeof(Lz4Job) * nbl * 8, dev) || !scratch.allocate((size_t)(nbl * g.blocksize), dev) ||
-        !counters.allocate(64, dev))
+        (!w->ext_counters && !counters.allocate(64, dev)))
         return -100;
-    int *njobs = counters.as<int>(), *err = counters.as<int>() + 1;
-    cudaMemsetAsync(counters.p, 0, 64, st);
+    int *cnt = w->ext_counters ? w->ext_counters : counters.as<int>();
+    int *njobs = cnt, *err = cnt + 1;
+    cudaMemsetAsync(cnt, 0, 64, st);
     const int sms = sm_count();
     {
         const int threads = 128;
@@ -1039,15 +1321,14 @@ int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, 
     }
     {
         static bool attr = false;
-        constexpr int RING = 4096, WIN = 1024, WARPS = 4;
-        const int smem = WARPS * (RING + WIN + 16 + 5 * WIN * 2);
+        const int smem = (int)sizeof(dcta::Smem);
         if (!attr) {
-            cudaFuncSetAttribute(k_lz4_decode_jump<RING, WIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            cudaFuncSetAttribute(k_lz4_decode_cta, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             attr = true;
         }
-        IAB_TIMED("k_lz4_decode_jump", st, k_lz4_decode_jump<RING, WIN><<<sms * 3, WARPS * 32, smem, st>>>(d_chunks, jobs.as<Lz4Job>(), njobs,
-                                                                      scratch.as<uint8_t>(), err,
-                                                                      reinterpret_cast<unsigned *>(counters.as<int>() + 2)));
+        IAB_TIMED("k_lz4_decode_cta", st, k_lz4_decode_cta<<<sms * 4, dcta::THREADS, smem, st>>>(
+            d_chunks, jobs.as<Lz4Job>(), njobs, scratch.as<uint8_t>(), err,
+            reinterpret_cast<unsigned *>(cnt + 2)));
     }
     {
         const int64_t tpb = (g.blockn + TILE - 1) / TILE;
@@ -1070,8 +1351,8 @@ int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, 
     return 0;
 }
 
-int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, DevBuf *d_out,
-                     std::vector<int64_t> *h_off, std::vector<int32_t> *h_len, cudaStream_t st)
+int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, DevBuf *d_out, EncodeWork *w,
+                  cudaStream_t st)
 {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -1086,11 +1367,14 @@ int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, in
     else split = shuffle && ts <= 16 && (g.blocksize / ts) >= 32;
     const int nstreams = split ? ts : 1;
     const int neblock = (int)(g.blocksize / nstreams);
-    DevBuf img, slots, es, ec, tot;
+    DevBuf &img = w->img, &slots = w->slots, &es = w->es, &tot = w->tot;
     if (!img.allocate(img_bytes, dev) || !slots.allocate(img_bytes, dev) ||
-        !es.allocate(sizeof(EncStream) * nbl * nstreams, dev) || !ec.allocate(sizeof(EncChunk) * g.nchunks, dev) ||
-        !tot.allocate(64, dev) || !d_out->allocate((size_t)(g.nchunks * (g.chunk_nbytes + 32)), dev))
+        !es.allocate(sizeof(EncStream) * nbl * nstreams, dev) ||
+        (!w->ext_chunks && !w->ec.allocate(sizeof(EncChunk) * g.nchunks, dev)) || !tot.allocate(64, dev) ||
+        !d_out->allocate((size_t)(g.nchunks * (g.chunk_nbytes + 32)), dev))
         return -100;
+    EncChunk *ec = w->ext_chunks ? w->ext_chunks : w->ec.as<EncChunk>();
+    w->nchunks = g.nchunks;
     cudaMemsetAsync(tot.p, 0, 64, st);
     const int sms = sm_count();
     {
@@ -1111,7 +1395,8 @@ int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, in
     }
     {
         static bool attr = false;
-        const int wpb = 4, smem = wpb * 4096 * 4;
+        // per warp: 16 KiB hash table + the source window; 3 warps per CTA, 3 CTAs per SM
+        const int wpb = 3, smem = wpb * (4096 * 4 + ERING + 16);
         if (!attr) {
             cudaFuncSetAttribute(k_lz4_encode, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             attr = true;
@@ -1122,20 +1407,36 @@ int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, in
             img.as<uint8_t>(), ns, neblock, slots.as<uint8_t>(), es.as<EncStream>(),
             reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1)));
     }
-    IAB_TIMED("k_layout", st, k_layout<<<1, 1024, 0, st>>>(g, nstreams, neblock, es.as<EncStream>(), ec.as<EncChunk>(), tot.as<int64_t>()));
+    IAB_TIMED("k_layout", st, k_layout<<<1, 1024, 0, st>>>(g, nstreams, neblock, es.as<EncStream>(), ec, tot.as<int64_t>()));
     {
         const int64_t blocks = std::min<int64_t>(nbl, (int64_t)sms * 8);
         IAB_TIMED("k_emit", st, k_emit<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, nstreams, neblock, shuffle, split ? 1 : 0,
-                                                                      img.as<uint8_t>(), slots.as<uint8_t>(),
-                                                                      es.as<EncStream>(), ec.as<EncChunk>(), d_out->as<uint8_t>()));
+                                                                      img.as<uint8_t>(), slots.as<uint8_t>(), img_bytes,
+                                                                      es.as<EncStream>(), ec, d_out->as<uint8_t>()));
     }
-    std::vector<EncChunk> hc((size_t)g.nchunks);
-    cudaMemcpyAsync(hc.data(), ec.p, sizeof(EncChunk) * g.nchunks, cudaMemcpyDeviceToHost, st);
-    if (cudaStreamSynchronize(st) != cudaSuccess) return -101;
-    h_off->resize((size_t)g.nchunks);
-    h_len->resize((size_t)g.nchunks);
-    for (int64_t c = 0; c < g.nchunks; c++) { (*h_off)[c] = hc[c].offset; (*h_len)[c] = hc[c].cbytes; }
     return 0;
+}
+
+int encode_finish(EncodeWork *w, std::vector<int64_t> *h_off, std::vector<int32_t> *h_len, cudaStream_t st)
+{
+    const int64_t n = w->nchunks;
+    std::vector<EncChunk> hc((size_t)n);
+    const EncChunk *ec = w->ext_chunks ? w->ext_chunks : w->ec.as<EncChunk>();
+    cudaMemcpyAsync(hc.data(), ec, sizeof(EncChunk) * n, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return -101;
+    h_off->resize((size_t)n);
+    h_len->resize((size_t)n);
+    for (int64_t c = 0; c < n; c++) { (*h_off)[c] = hc[c].offset; (*h_len)[c] = hc[c].cbytes; }
+    return 0;
+}
+
+int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, DevBuf *d_out,
+                     std::vector<int64_t> *h_off, std::vector<int32_t> *h_len, cudaStream_t st)
+{
+    EncodeWork w;
+    const int r = encode_launch(g, in, ld, shuffle, splitmode, d_out, &w, st);
+    if (r) return r;
+    return encode_finish(&w, h_off, h_len, st);
 }
 
 // ============================================================================ decode without allocation
@@ -1194,10 +1495,8 @@ static uint8_t *noalloc_scratch()
     if (!ptr[dev]) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) { cudaGetLastError(); return nullptr; }
-        constexpr int RING = 4096, WIN = 1024, WARPS = 4;
-        const int smem = WARPS * (RING + WIN + 16 + 5 * WIN * 2);
-        if (cudaFuncSetAttribute(k_lz4_decode_jump<RING, WIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-            cudaSuccess) { cudaGetLastError(); return nullptr; }
+        if (cudaFuncSetAttribute(k_lz4_decode_cta, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(dcta::Smem)) != cudaSuccess) { cudaGetLastError(); return nullptr; }
         ptr[dev] = static_cast<uint8_t *>(p);
     }
     return ptr[dev];
@@ -1229,10 +1528,8 @@ int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes,
         IAB_TIMED("k_parse", st, k_parse<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, st>>>(g, d_chunks, off, len, bd, sd, jobs, njobs, err));
     }
     {
-        constexpr int RING = 4096, WIN = 1024, WARPS = 4;
-        const int smem = WARPS * (RING + WIN + 16 + 5 * WIN * 2);
-        IAB_TIMED("k_lz4_decode_jump", st, k_lz4_decode_jump<RING, WIN><<<sms * 3, WARPS * 32, smem, st>>>(d_chunks, jobs, njobs, img, err,
-                                                                      reinterpret_cast<unsigned *>(counters + 2)));
+        IAB_TIMED("k_lz4_decode_cta", st, k_lz4_decode_cta<<<sms * 4, dcta::THREADS, (int)sizeof(dcta::Smem), st>>>(
+            d_chunks, jobs, njobs, img, err, reinterpret_cast<unsigned *>(counters + 2)));
     }
     {
         const int64_t tpb = (g.blockn + TILE - 1) / TILE;

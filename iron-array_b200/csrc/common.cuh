@@ -150,6 +150,7 @@ int decode_container(const Geom &g, const uint8_t *d_chunks, int64_t chunks_byte
 // *w until decode_finish, which synchronises `st` and returns the DevErr).
 struct DecodeWork {
     DevBuf bd, sd, jobs, scratch, counters;
+    int *ext_counters = nullptr;   // optional caller-owned 16-int status slot (device) instead of `counters`
 };
 int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, const int64_t *d_off, const int32_t *d_len,
                   void *out, int64_t ld, cudaStream_t st, DecodeWork *w);
@@ -168,6 +169,16 @@ int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes,
 int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode,
                      DevBuf *d_out, std::vector<int64_t> *h_off, std::vector<int32_t> *h_len,
                      cudaStream_t st);
+// Asynchronous form: encode_launch enqueues the kernels (no host synchronisation; work
+// buffers held in *w), encode_finish synchronises and reads the chunk table.
+struct EncodeWork {
+    DevBuf img, slots, es, ec, tot;
+    EncChunk *ext_chunks = nullptr;   // optional caller-owned chunk table (device) instead of `ec`
+    int64_t nchunks = 0;
+};
+int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, DevBuf *d_out,
+                  EncodeWork *w, cudaStream_t st);
+int encode_finish(EncodeWork *w, std::vector<int64_t> *h_off, std::vector<int32_t> *h_len, cudaStream_t st);
 
 // Dense products (row-major, leading dimensions in items).
 void gemm_f64_native(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda,
@@ -176,6 +187,19 @@ void gemm_f32_native(int64_t M, int64_t N, int64_t K, const float *A, int64_t ld
                      const float *B, int64_t ldb, float *C, int64_t ldc, cudaStream_t st);
 void gemv_native(int dtype, int64_t M, int64_t K, const void *A, int64_t lda, const void *x,
                  void *y, cudaStream_t st);
+// Grouped FP64 product: many independent C_p = A_p B_p in one persistent launch.
+// tile_start is the first global tile of problem p for the chosen tile configuration
+// (cfg 0: 128x128, 1: 64x128, 2: 128x64, 3: 64x64); problems are listed in tile order.
+struct GemmProblem {
+    int M, N, K, tile_start;
+    const double *A;
+    const double *B;
+    double *C;
+    int64_t lda, ldb, ldc;
+};
+int gemm_f64_grouped_tiles(int cfg, int M, int N);
+void gemm_f64_grouped(int cfg, const GemmProblem *d_probs, int nprob, int total_tiles, int ctas, cudaStream_t st);
+
 // Split-precision forms; return 0 on success, < 0 when unsupported on this device.
 int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda,
                    const double *B, int64_t ldb, double *C, int64_t ldc, int nterms, cudaStream_t st);

@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace iab {
@@ -35,11 +37,14 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 // ============================================================================ FP64 DMMA
 namespace f64k {
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3;
+constexpr int BK = 16, STAGES = 3;
 constexpr int SA = BK + 4;    // A tile row stride (doubles): 20 = 4 mod 16 -> conflict-free fragments
-constexpr int SB = BN + 4;    // B tile row stride: 132 = 4 mod 16
-constexpr int A_STAGE = BM * SA, B_STAGE = BK * SB;
-constexpr int SMEM = STAGES * (A_STAGE + B_STAGE) * 8;
+template <int BM, int BN> struct Cfg {
+    static constexpr int SB = BN + 4;                    // B tile row stride: 4 mod 16
+    static constexpr int A_STAGE = BM * SA, B_STAGE = BK * SB;
+    static constexpr int SMEM = STAGES * (A_STAGE + B_STAGE) * 8;
+    static constexpr int MI = BM / 32, NJ = BN / 32;     // 2 x 4 warps, warp tile (BM/2) x (BN/4)
+};
 }
 
 __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], const double (&a)[2], double b)
@@ -50,43 +55,44 @@ __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], const double (&a)[2]
         : "d"(a[0]), "d"(a[1]), "d"(b));
 }
 
-// Requires lda, ldb even and 16-byte aligned bases (true for the library's dense buffers).
-__global__ void __launch_bounds__(256) k_gemm_f64(int M, int N, int K, const double *__restrict__ A, int64_t lda,
-                                                  const double *__restrict__ B, int64_t ldb, double *__restrict__ C,
-                                                  int64_t ldc)
+// One BM x BN tile of C = A B at (m0, n0), 256 threads.  Requires lda, ldb even and
+// 16-byte aligned bases (true for the library's dense buffers).
+template <int BM, int BN>
+__device__ __forceinline__ void f64_tile(int M, int N, int K, const double *__restrict__ A, int64_t lda,
+                                         const double *__restrict__ B, int64_t ldb, double *__restrict__ C,
+                                         int64_t ldc, int m0, int n0, double *smf64)
 {
     using namespace f64k;
-    extern __shared__ __align__(16) double smf64[];
-    double *sA = smf64, *sB = smf64 + STAGES * A_STAGE;
+    using G = Cfg<BM, BN>;
+    double *sA = smf64, *sB = smf64 + STAGES * G::A_STAGE;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int wm = warp >> 2, wn = warp & 3;   // 2 x 4 warps, warp tile 64 x 32
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int wm = warp >> 2, wn = warp & 3;
     const int ktiles = (K + BK - 1) / BK;
 
     auto load_tile = [&](int kt, int s) {
         const int k0 = kt * BK;
-        double *a = sA + s * A_STAGE, *b = sB + s * B_STAGE;
+        double *a = sA + s * G::A_STAGE, *b = sB + s * G::B_STAGE;
 #pragma unroll
-        for (int i = 0; i < 4; i++) {           // A: 128 rows x 8 16-byte pieces
+        for (int i = 0; i < BM / 32; i++) {      // A: BM rows x 8 16-byte pieces
             const int idx = tid + i * 256, r = idx >> 3, cpc = (idx & 7) * 2;
             const int gr = m0 + r, gk = k0 + cpc;
             const bool ok = gr < M && gk < K;
             cp_async16(a + r * SA + cpc, ok ? (const void *)(A + (int64_t)gr * lda + gk) : (const void *)A, ok);
         }
 #pragma unroll
-        for (int i = 0; i < 4; i++) {           // B: 16 rows x 64 pieces
-            const int idx = tid + i * 256, r = idx >> 6, cpc = (idx & 63) * 2;
+        for (int i = 0; i < BN / 32; i++) {      // B: 16 rows x BN/2 pieces
+            const int idx = tid + i * 256, r = idx / (BN / 2), cpc = (idx % (BN / 2)) * 2;
             const int gk = k0 + r, gn = n0 + cpc;
             const bool ok = gk < K && gn < N;
-            cp_async16(b + r * SB + cpc, ok ? (const void *)(B + (int64_t)gk * ldb + gn) : (const void *)B, ok);
+            cp_async16(b + r * G::SB + cpc, ok ? (const void *)(B + (int64_t)gk * ldb + gn) : (const void *)B, ok);
         }
     };
 
-    double acc[4][4][4];
+    double acc[G::MI][G::NJ][4];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int i = 0; i < G::MI; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++)
+        for (int j = 0; j < G::NJ; j++)
 #pragma unroll
             for (int r = 0; r < 4; r++) acc[i][j][r] = 0.0;
 
@@ -102,31 +108,31 @@ __global__ void __launch_bounds__(256) k_gemm_f64(int M, int N, int K, const dou
         const int nk = kt + STAGES - 1;
         if (nk < ktiles) load_tile(nk, nk % STAGES);
         cp_async_commit();
-        const double *a = sA + (kt % STAGES) * A_STAGE + (wm * 64) * SA;
-        const double *b = sB + (kt % STAGES) * B_STAGE + wn * 32;
+        const double *a = sA + (kt % STAGES) * G::A_STAGE + (wm * (BM / 2)) * SA;
+        const double *b = sB + (kt % STAGES) * G::B_STAGE + wn * (BN / 4);
 #pragma unroll
         for (int kk = 0; kk < BK; kk += 4) {
-            double af[4][2], bf[4];
+            double af[G::MI][2], bf[G::NJ];
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
+            for (int i = 0; i < G::MI; i++) {
                 af[i][0] = a[(i * 16 + g) * SA + kk + q];
                 af[i][1] = a[(i * 16 + g + 8) * SA + kk + q];
             }
 #pragma unroll
-            for (int j = 0; j < 4; j++) bf[j] = b[(kk + q) * SB + j * 8 + g];
+            for (int j = 0; j < G::NJ; j++) bf[j] = b[(kk + q) * G::SB + j * 8 + g];
 #pragma unroll
-            for (int i = 0; i < 4; i++)
+            for (int i = 0; i < G::MI; i++)
 #pragma unroll
-                for (int j = 0; j < 4; j++) dmma_16x8x4(acc[i][j], af[i], bf[j]);
+                for (int j = 0; j < G::NJ; j++) dmma_16x8x4(acc[i][j], af[i], bf[j]);
         }
     }
     cp_async_wait<0>();
     // epilogue: fragment rows g, g+8; cols 2q, 2q+1
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int i = 0; i < G::MI; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int r0 = m0 + wm * 64 + i * 16 + g, c0 = n0 + wn * 32 + j * 8 + 2 * q;
+        for (int j = 0; j < G::NJ; j++) {
+            const int r0 = m0 + wm * (BM / 2) + i * 16 + g, c0 = n0 + wn * (BN / 4) + j * 8 + 2 * q;
 #pragma unroll
             for (int h = 0; h < 2; h++) {
                 const int r = r0 + h * 8;
@@ -141,17 +147,76 @@ __global__ void __launch_bounds__(256) k_gemm_f64(int M, int N, int K, const dou
         }
 }
 
+__global__ void __launch_bounds__(256) k_gemm_f64(int M, int N, int K, const double *__restrict__ A, int64_t lda,
+                                                  const double *__restrict__ B, int64_t ldb, double *__restrict__ C,
+                                                  int64_t ldc)
+{
+    extern __shared__ __align__(16) double smf64[];
+    f64_tile<128, 128>(M, N, K, A, lda, B, ldb, C, ldc, blockIdx.y * 128, blockIdx.x * 128, smf64);
+}
+
 void gemm_f64_native(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B, int64_t ldb,
                      double *C, int64_t ldc, cudaStream_t st)
 {
-    using namespace f64k;
+    using G = f64k::Cfg<128, 128>;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_gemm_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+        cudaFuncSetAttribute(k_gemm_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
         attr = true;
     }
-    dim3 grid((unsigned)((N + BN - 1) / BN), (unsigned)((M + BM - 1) / BM));
-    IAB_TIMED("k_gemm_f64", st, k_gemm_f64<<<grid, 256, SMEM, st>>>((int)M, (int)N, (int)K, A, lda, B, ldb, C, ldc));
+    dim3 grid((unsigned)((N + 127) / 128), (unsigned)((M + 127) / 128));
+    IAB_TIMED("k_gemm_f64", st, k_gemm_f64<<<grid, 256, G::SMEM, st>>>((int)M, (int)N, (int)K, A, lda, B, ldb, C, ldc));
+}
+
+// Grouped form: one persistent launch over the tiles of many independent products.
+// Problem p owns global tiles [tile_start, tile_start + tiles_m * tiles_n); CTAs take
+// tiles round-robin and find their problem by binary search.
+template <int BM, int BN>
+__global__ void __launch_bounds__(256) k_gemm_f64_grouped(const GemmProblem *__restrict__ probs, int nprob,
+                                                          int total_tiles)
+{
+    extern __shared__ __align__(16) double smf64[];
+    for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+        int lo = 0, hi = nprob - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (probs[mid].tile_start <= t) lo = mid; else hi = mid - 1;
+        }
+        const GemmProblem &p = probs[lo];
+        const int local = t - p.tile_start, tn_count = (p.N + BN - 1) / BN;
+        const int tm = local / tn_count, tn = local - tm * tn_count;
+        f64_tile<BM, BN>(p.M, p.N, p.K, p.A, p.lda, p.B, p.ldb, p.C, p.ldc, tm * BM, tn * BN, smf64);
+        __syncthreads();
+    }
+}
+
+int gemm_f64_grouped_tiles(int cfg, int M, int N)
+{
+    const int bm = (cfg == 0 || cfg == 2) ? 128 : 64, bn = (cfg == 0 || cfg == 1) ? 128 : 64;
+    return ((M + bm - 1) / bm) * ((N + bn - 1) / bn);
+}
+
+template <int BM, int BN>
+static void launch_grouped(const GemmProblem *d_probs, int nprob, int total, int ctas, cudaStream_t st)
+{
+    using G = f64k::Cfg<BM, BN>;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_gemm_f64_grouped<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+        attr = true;
+    }
+    IAB_TIMED("k_gemm_f64_grouped", st, k_gemm_f64_grouped<BM, BN><<<(unsigned)std::max(1, std::min(ctas, total)), 256, G::SMEM, st>>>(
+        d_probs, nprob, total));
+}
+
+void gemm_f64_grouped(int cfg, const GemmProblem *d_probs, int nprob, int total_tiles, int ctas, cudaStream_t st)
+{
+    switch (cfg) {
+    case 0: launch_grouped<128, 128>(d_probs, nprob, total_tiles, ctas, st); break;
+    case 1: launch_grouped<64, 128>(d_probs, nprob, total_tiles, ctas, st); break;
+    case 2: launch_grouped<128, 64>(d_probs, nprob, total_tiles, ctas, st); break;
+    default: launch_grouped<64, 64>(d_probs, nprob, total_tiles, ctas, st); break;
+    }
 }
 
 // ============================================================================ FP32 FFMA

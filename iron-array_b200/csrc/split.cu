@@ -16,6 +16,7 @@
 //      arithmetic), centred, converted to float64 and scaled back by 2^-(sA_i + sB_j).
 // FP64 is used only for the scaling, the residue arithmetic and the final conversion.
 #include <cuda.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -401,7 +402,9 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
                         o4[0] = make_uint4(w[0], w[1], w[2], w[3]);
                         o4[1] = make_uint4(w[4], w[5], w[6], w[7]);
                     } else {
-                        for (int b = 0; b < 32 && col + b < p.N; b++) out[c + b] = (uint8_t)(w[b >> 2] >> (8 * (b & 3)));
+#pragma unroll
+                        for (int b = 0; b < 32; b++)
+                            if (col + b < p.N) out[c + b] = (uint8_t)(w[b >> 2] >> (8 * (b & 3)));
                     }
                 }
             }
@@ -608,10 +611,247 @@ int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda
     return h_err ? -3 : 0;
 }
 
-int gemm_f32_bf16x3(int64_t, int64_t, int64_t, const float *, int64_t, const float *, int64_t, float *, int64_t,
-                    cudaStream_t)
+// ============================================================================ float32: 3xBF16
+// A float32 x is split as x = hi + lo + e, hi = bf16(x), lo = bf16(x - hi), |e| <= 2^-17 |x|.
+// C = A_hi B_hi + A_hi B_lo + A_lo B_hi (the lo*lo term, below float32 resolution, is
+// dropped) is one tcgen05.mma kind::f16 GEMM whose K loop runs three times over the
+// operand planes, all passes accumulating into the same FP32 TMEM tile.
+namespace b3 {
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;        // BK bf16 = 128 bytes per row
+constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int THREADS = 192;
+constexpr int SMEM = 1024 + STAGES * STAGE_BYTES + 256;
+constexpr uint32_t IDESC = tc::make_idesc(1 /*F32*/, 1 /*BF16*/, 1 /*BF16*/, BM, BN);
+__device__ __constant__ int kAPlane[3] = {0, 0, 1};
+__device__ __constant__ int kBPlane[3] = {0, 1, 0};
+}
+
+struct B3Params {
+    int M, N, Kp, tiles_m, tiles_n;
+    float *C;
+    int64_t ldc;
+    int *err;
+};
+
+// Row-major A (M x K) -> planes [2][M][Kp] of bf16 (hi, lo), K padded with zeros.
+__global__ void __launch_bounds__(256) k_split_rows(int M, int K, int Kp, const float *__restrict__ A, int64_t lda,
+                                                    __nv_bfloat16 *__restrict__ P)
 {
-    return -1;
+    const int groups = Kp / 4;
+    const int64_t total = (int64_t)M * groups, plane = (int64_t)M * Kp;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(t / groups), k0 = (int)(t - (int64_t)i * groups) * 4;
+        __nv_bfloat16 h[4], l[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const float x = k0 + u < K ? A[(int64_t)i * lda + k0 + u] : 0.f;
+            h[u] = __float2bfloat16_rn(x);
+            l[u] = __float2bfloat16_rn(x - __bfloat162float(h[u]));
+        }
+        __nv_bfloat16 *ph = P + (int64_t)i * Kp + k0;
+        *reinterpret_cast<uint2 *>(ph) = *reinterpret_cast<const uint2 *>(h);
+        *reinterpret_cast<uint2 *>(ph + plane) = *reinterpret_cast<const uint2 *>(l);
+    }
+}
+
+// Row-major B (K x N) -> planes [2][N][Kp] of bf16 (transposed, K-major).
+__global__ void __launch_bounds__(256) k_split_cols(int K, int N, int Kp, const float *__restrict__ B, int64_t ldb,
+                                                    __nv_bfloat16 *__restrict__ P)
+{
+    __shared__ float tile[64][65];
+    const int k0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
+    for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+        const int r = e >> 6, c = e & 63;
+        const int k = k0 + r, j = j0 + c;
+        tile[r][c] = (k < K && j < N) ? B[(int64_t)k * ldb + j] : 0.f;
+    }
+    __syncthreads();
+    const int64_t plane = (int64_t)N * Kp;
+    for (int e = threadIdx.x; e < 64 * 16; e += blockDim.x) {
+        const int c = e >> 4, kg = (e & 15) * 4;
+        const int j = j0 + c;
+        if (j >= N || k0 + kg >= Kp) continue;
+        __nv_bfloat16 h[4], l[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const float x = tile[kg + u][c];
+            h[u] = __float2bfloat16_rn(x);
+            l[u] = __float2bfloat16_rn(x - __bfloat162float(h[u]));
+        }
+        __nv_bfloat16 *ph = P + (int64_t)j * Kp + k0 + kg;
+        *reinterpret_cast<uint2 *>(ph) = *reinterpret_cast<const uint2 *>(h);
+        *reinterpret_cast<uint2 *>(ph + plane) = *reinterpret_cast<const uint2 *>(l);
+    }
+}
+
+// Persistent, warp-specialised like k_i8gemm_mod: warp 0 loads (TMA), warp 1 issues the
+// MMAs of the three passes into one of two 128 x 256 FP32 TMEM accumulators, warps 2-5
+// store the other accumulator as float32 rows of C.
+__global__ void __launch_bounds__(b3::THREADS, 1) k_bf16x3_gemm(const __grid_constant__ CUtensorMap tmA,
+                                                                 const __grid_constant__ CUtensorMap tmB, B3Params p)
+{
+    using namespace b3;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t *sA = smem, *sB = smem + STAGES * A_BYTES;
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+    uint64_t *tfull = empty + STAGES;
+    uint64_t *tempty = tfull + 2;
+    uint64_t *drain = tempty + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) { tc::mbar_init(&full[s], 1); tc::mbar_init(&empty[s], 1); }
+        for (int b = 0; b < 2; b++) { tc::mbar_init(&tfull[b], 1); tc::mbar_init(&tempty[b], 4); }
+        tc::mbar_init(drain, 1);
+        tc::fence_barrier_init();
+        tc::tma_prefetch_desc(&tmA);
+        tc::tma_prefetch_desc(&tmB);
+    }
+    if (warp == 1) {
+        tc::tmem_alloc(tmem_slot, 512);
+        tc::tmem_relinquish();
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const int total = p.tiles_m * p.tiles_n;
+    const int ktiles = p.Kp / BK;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int64_t issued = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+                const int tm = t / p.tiles_n, tn = t - tm * p.tiles_n;
+                for (int pass = 0; pass < 3 && ok; pass++) {
+                    const int pa = kAPlane[pass], pb = kBPlane[pass];
+                    for (int kt = 0; kt < ktiles; kt++) {
+                        if (!tc::mbar_wait(&empty[stage], phase ^ 1, p.err)) { ok = false; break; }
+                        tc::mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
+                        tc::tma_load_3d(sA + stage * A_BYTES, &tmA, kt * BK, tm * BM, pa, &full[stage]);
+                        tc::tma_load_3d(sB + stage * B_BYTES, &tmB, kt * BK, tn * BN, pb, &full[stage]);
+                        issued++;
+                        if (++stage == STAGES) { stage = 0; phase ^= 1; }
+                    }
+                }
+            }
+            for (int64_t it = issued > STAGES ? issued - STAGES : 0; it < issued; it++)
+                tc::mbar_wait(&full[it % STAGES], (uint32_t)((it / STAGES) & 1), p.err, 1u << 20);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int stage = 0, acc = 0;
+            uint32_t phase = 0, acc_phase = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+                if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, p.err)) { ok = false; break; }
+                tc::tc_fence_after();
+                const uint32_t dt = tmem_base + (uint32_t)(acc * BN);
+                for (int step = 0; step < 3 * ktiles; step++) {
+                    if (!tc::mbar_wait(&full[stage], phase, p.err)) { ok = false; break; }
+                    tc::tc_fence_after();
+                    const uint32_t a0 = tc::smem_addr(sA + stage * A_BYTES), b0 = tc::smem_addr(sB + stage * B_BYTES);
+#pragma unroll
+                    for (int kk = 0; kk < BK / 16; kk++) {
+                        tc::mma_f16(dt, tc::sw128_kmajor_desc(a0 + kk * 32), tc::sw128_kmajor_desc(b0 + kk * 32), IDESC,
+                                    (step | kk) != 0);
+                    }
+                    tc::tc_commit(&empty[stage]);
+                    if (++stage == STAGES) { stage = 0; phase ^= 1; }
+                }
+                if (!ok) break;
+                tc::tc_commit(&tfull[acc]);
+                if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+            }
+            tc::tc_commit(drain);
+            tc::mbar_wait(drain, 0, p.err, 1u << 20);
+        }
+    } else {
+        const int q = warp & 3;
+        int acc = 0;
+        uint32_t acc_phase = 0;
+        for (int t = blockIdx.x; t < total; t += gridDim.x) {
+            const int tm = t / p.tiles_n, tn = t - tm * p.tiles_n;
+            if (!tc::mbar_wait(&tfull[acc], acc_phase, p.err)) break;
+            tc::tc_fence_after();
+            const int row = tm * BM + q * 32 + lane;
+            float *out = p.C + (int64_t)row * p.ldc + (int64_t)tn * BN;
+            for (int c = 0; c < BN; c += 32) {
+                uint32_t v[32];
+                tc::tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + c), v);
+                const int col = tn * BN + c;
+                if (row < p.M) {
+                    if (col + 32 <= p.N && ((reinterpret_cast<uintptr_t>(out + c) & 15) == 0)) {
+                        float4 *o4 = reinterpret_cast<float4 *>(out + c);
+#pragma unroll
+                        for (int u = 0; u < 8; u++)
+                            o4[u] = make_float4(__uint_as_float(v[4 * u]), __uint_as_float(v[4 * u + 1]),
+                                                __uint_as_float(v[4 * u + 2]), __uint_as_float(v[4 * u + 3]));
+                    } else {
+#pragma unroll
+                        for (int b = 0; b < 32; b++)
+                            if (col + b < p.N) out[c + b] = __uint_as_float(v[b]);
+                    }
+                }
+            }
+            tc::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&tempty[acc]);
+            if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    if (warp == 1) tc::tmem_dealloc(tmem_base, 512);
+}
+
+int gemm_f32_bf16x3(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda, const float *B, int64_t ldb,
+                    float *C, int64_t ldc, cudaStream_t st)
+{
+    if (!device_is_sm100()) return -1;
+    if (M <= 0 || N <= 0 || K <= 0) return 0;
+    if (M > (1 << 30) || N > (1 << 30) || K > (1 << 30)) return -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int64_t Kp = round_up(K, b3::BK);
+    DevBuf pa, pb, err;
+    if (!pa.allocate((size_t)(2 * M * Kp * 2), dev) || !pb.allocate((size_t)(2 * N * Kp * 2), dev) ||
+        !err.allocate(16, dev))
+        return -100;
+    cudaMemsetAsync(err.p, 0, 16, st);
+    const int nsm = sms();
+    IAB_TIMED("k_split_rows", st, k_split_rows<<<(unsigned)(nsm * 16), 256, 0, st>>>(
+        (int)M, (int)K, (int)Kp, A, lda, pa.as<__nv_bfloat16>()));
+    IAB_TIMED("k_split_cols", st, k_split_cols<<<dim3((unsigned)((N + 63) / 64), (unsigned)((Kp + 63) / 64)), 256, 0, st>>>(
+        (int)K, (int)N, (int)Kp, B, ldb, pb.as<__nv_bfloat16>()));
+    CUtensorMap tmA, tmB;
+    if (!make_tmap_3d(&tmA, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, pa.p, (uint64_t)Kp, (uint64_t)M, 2, (uint64_t)Kp * 2,
+                      (uint64_t)(Kp * M * 2), b3::BK, b3::BM, CU_TENSOR_MAP_SWIZZLE_128B) ||
+        !make_tmap_3d(&tmB, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, pb.p, (uint64_t)Kp, (uint64_t)N, 2, (uint64_t)Kp * 2,
+                      (uint64_t)(Kp * N * 2), b3::BK, b3::BN, CU_TENSOR_MAP_SWIZZLE_128B))
+        return -1;
+    B3Params prm;
+    prm.M = (int)M; prm.N = (int)N; prm.Kp = (int)Kp;
+    prm.tiles_m = (int)ceil_div(M, b3::BM); prm.tiles_n = (int)ceil_div(N, b3::BN);
+    prm.C = C; prm.ldc = ldc; prm.err = err.as<int>();
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_bf16x3_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, b3::SMEM);
+        attr = true;
+    }
+    const int tiles = prm.tiles_m * prm.tiles_n;
+    IAB_TIMED("k_bf16x3_gemm", st, k_bf16x3_gemm<<<(unsigned)std::min(tiles, nsm), b3::THREADS, b3::SMEM, st>>>(tmA, tmB, prm));
+    int h_err = 0;
+    cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return -2;
+    return h_err ? -3 : 0;
 }
 
 }  // namespace iab

@@ -82,3 +82,48 @@ def test_split_f64_more_moduli_is_at_least_as_accurate(ia, nterms):
                   ia.Container.from_numpy(ctx, B, (256, 256), (64, 64)), (256, 256), (64, 64)).to_numpy()
     hi, lo = O.dd_rows(A, B, np.arange(256))
     assert O.normwise_error(C, hi, lo, np.arange(256)) <= 2e-15
+
+
+def _f32_inputs(rng, M, K, N):
+    i, j = np.meshgrid(np.arange(M), np.arange(K), indexing="ij")
+    A = rng.standard_normal((M, K)) + 0.1 * np.sin(0.003 * (i + j))
+    i, j = np.meshgrid(np.arange(K), np.arange(N), indexing="ij")
+    B = rng.standard_normal((K, N)) + 0.1 * np.sin(0.003 * (i + j))
+    return A.astype(np.float32), B.astype(np.float32)
+
+
+@pytest.mark.parametrize("M,K,N,cs,bs", [
+    (300, 257, 200, 128, 32),        # ragged tiles and a K that is not a multiple of 64
+    (256, 1024, 512, 256, 64),
+    (1000, 1000, 1000, 500, 100),
+    (64, 4096, 96, 64, 32),
+])
+def test_split_f32_bf16x3_error(ia, M, K, N, cs, bs):
+    """float32 split form (3xBF16 on tcgen05, FP32 accumulation): normwise error against
+    the float64 product of the same float32 operands stays at float32 level (the split
+    represents each operand to 2^-17 relative)."""
+    rng = np.random.default_rng(4 + M + K + N)
+    A, B = _f32_inputs(rng, M, K, N)
+    sctx, nctx = _split_ctx(ia), ia.Context()
+    Ac = ia.Container.from_numpy(nctx, A, (cs, cs), (bs, bs))
+    Bc = ia.Container.from_numpy(nctx, B, (cs, cs), (bs, bs))
+    cn = ia.opt_gemm(nctx, Ac, Bc, (cs, cs), (bs, bs)).to_numpy()
+    cs_ = ia.opt_gemm(sctx, Ac, Bc, (cs, cs), (bs, bs)).to_numpy()
+    exact = A.astype(np.float64) @ B.astype(np.float64)
+    nrm = np.linalg.norm(exact)
+    en = np.linalg.norm(cn - exact) / nrm
+    es = np.linalg.norm(cs_ - exact) / nrm
+    assert es < 5e-5, (es, en)
+    assert np.abs(cs_ - exact).max() <= 1e-4 * np.abs(exact).max() + 1e-6
+
+
+def test_split_f32_zero_and_single_tile(ia):
+    ctx = _split_ctx(ia)
+    A = np.zeros((5, 7), np.float32)
+    B = np.ones((7, 3), np.float32)
+    Ac = ia.Container.from_numpy(ctx, A, (5, 7), (5, 7))
+    Bc = ia.Container.from_numpy(ctx, B, (7, 3), (7, 3))
+    assert not ia.opt_gemm(ctx, Ac, Bc, (5, 3), (5, 3)).to_numpy().any()
+    A = np.full((5, 7), 0.5, np.float32)
+    Ac = ia.Container.from_numpy(ctx, A, (5, 7), (5, 7))
+    assert np.array_equal(ia.opt_gemm(ctx, Ac, Bc, (5, 3), (5, 3)).to_numpy(), np.full((5, 3), 3.5, np.float32))
