@@ -205,6 +205,151 @@ def roofline(kprof, pk, dgemm_tflops, c_cbytes, a_cb, b_cb):
             "traffic": traffic}
 
 
+# ============================================================================ secondary workloads
+def _timed(ctx, stream, fn, steps, warmup):
+    """Device time per call (CUDA events on the context stream) and wall time per call."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    ctx.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t = time.perf_counter()
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    ctx.synchronize()
+    wall = (time.perf_counter() - t) / steps
+    return e0.elapsed_time(e1) / steps, wall * 1e3
+
+
+def secondary_gemv(ia, ctx, stream, args, pk):
+    """Plain GEMV: float32 y = A x, A 20000 x 20000 with A[i, j] = sin(0.001 i) + cos(0.002 j)
+    (computed in float64, stored as float32), x uniform(-1, 1) (default_rng(2)), chunk 4000^2,
+    block 500^2; standalone decode of A and the full iarray_opt_gemv call."""
+    import torch
+    n, ch, bl = 20000, 4000, 500
+    A = np.empty((n, n), np.float32)
+    cj = np.cos(0.002 * np.arange(n))
+    for r0 in range(0, n, 2000):
+        A[r0:r0 + 2000] = (np.sin(0.001 * np.arange(r0, r0 + 2000))[:, None] + cj[None, :]).astype(np.float32)
+    x = np.random.default_rng(2).uniform(-1, 1, n).astype(np.float32)
+    Ac = ia.Container.from_numpy(ctx, A, (ch, ch), (bl, bl))
+    xc = ia.Container.from_numpy(ctx, x, (ch,), (bl,))
+    nb, cb = Ac.info()
+    ref = A.astype(np.float64) @ x.astype(np.float64)
+    del A
+    dense = torch.empty((n, n), dtype=torch.float32, device="cuda")
+    dec_ms, _ = _timed(ctx, stream, lambda: Ac.decode_to_device(dense.data_ptr(), n), args.steps, args.warmup)
+    del dense
+    torch.cuda.empty_cache()
+    out = []
+
+    def step():
+        out.append(ia.opt_gemv(ctx, Ac, xc, (ch,), (bl,)))
+        if len(out) > 1:
+            out.pop(0).free()
+    gemv_ms, gemv_wall = _timed(ctx, stream, step, args.steps, args.warmup)
+    y = out[-1].to_numpy().astype(np.float64)
+    err = float(np.linalg.norm(y - ref) / np.linalg.norm(ref))
+    for c in out + [Ac, xc]:
+        c.free()
+    gbs = (nb + cb) / (dec_ms * 1e-3) / 1e9
+    return {"workload": "gemv f32 20000x20000 smooth, chunk 4000^2, block 500^2",
+            "decode_gbs": gbs, "decode_frac_of_measured_hbm": gbs / pk["hbm_gbs"], "decode_ms": dec_ms,
+            "compression_ratio": nb / cb, "opt_gemv_ms": gemv_ms, "opt_gemv_wall_ms": gemv_wall,
+            "opt_gemv_gflops": 2.0 * n * n / (gemv_ms * 1e-3) / 1e9,
+            "opt_gemv_gbs": (cb + 8 * n) / (gemv_ms * 1e-3) / 1e9,
+            "normwise_err_vs_f64": err}
+
+
+def secondary_f32(ia, ctx, stream, args):
+    """Precision, float32: A 16384 x 4096, B 4096 x 16384, normal(0, 1) (default_rng(4)) plus
+    0.1 sin(0.003 (i + j)), chunk 4096^2, block 512^2; native FFMA and 3xBF16 split forms."""
+    M, K, N, ch, bl = 16384, 4096, 16384, 4096, 512
+    rng = np.random.default_rng(4)
+    A = rng.standard_normal((M, K))
+    A += 0.1 * np.sin(0.003 * (np.arange(M)[:, None] + np.arange(K)[None, :]))
+    A = A.astype(np.float32)
+    B = rng.standard_normal((K, N))
+    B += 0.1 * np.sin(0.003 * (np.arange(K)[:, None] + np.arange(N)[None, :]))
+    B = B.astype(np.float32)
+    Ac = ia.Container.from_numpy(ctx, A, (ch, ch), (bl, bl))
+    Bc = ia.Container.from_numpy(ctx, B, (ch, ch), (bl, bl))
+    rows = np.sort(np.random.default_rng(99).choice(M, args.err_rows, replace=False))
+    exact = A[rows].astype(np.float64) @ B.astype(np.float64)
+    del A, B
+    flop = 2.0 * M * N * K
+    res = {"workload": "precision_f32 16384x4096 @ 4096x16384, chunk 4096^2, block 512^2"}
+    for name, form in (("native", ia.FORM_NATIVE), ("split", ia.FORM_SPLIT)):
+        ctx.set_form(form)
+        out = []
+
+        def step():
+            out.append(ia.opt_gemm(ctx, Ac, Bc, (ch, ch), (bl, bl)))
+            if len(out) > 1:
+                out.pop(0).free()
+        steps = max(2, args.steps // 2)
+        ms, _ = _timed(ctx, stream, step, steps, max(1, args.warmup - 1))
+        ia.profile_kernels(True)
+        step()
+        ctx.synchronize()
+        ia.profile_kernels(False)
+        prof = ia.kernel_profile()
+        prod = sum(v[1] for k, v in prof.items() if k in ("k_gemm_f32", "k_bf16x3_gemm", "k_split_rows", "k_split_cols"))
+        c = out[-1].to_numpy()[rows].astype(np.float64)
+        err = float(np.linalg.norm(c - exact) / np.linalg.norm(exact))
+        for x in out:
+            x.free()
+        res[name] = {"ms_per_step": ms, "tflops": flop / (ms * 1e-3) / 1e12, "product_ms": prod,
+                     "product_tflops": flop / (prod * 1e-3) / 1e12 if prod else None,
+                     "normwise_err_vs_f64": err, "kernel_ms": {k: v[1] for k, v in sorted(prof.items())}}
+    ctx.set_form(ia.FORM_NATIVE)
+    Ac.free()
+    Bc.free()
+    return res
+
+
+def secondary_batch(ia, ctx, stream, args):
+    """Batching: 512 independent float64 products, m, n, k uniform integers in [64, 2048]
+    (default_rng(5)), entries uniform(-1, 1), chunk 512^2, block 128^2 (ragged edges); one
+    CUDA graph per form, grouped persistent product kernel in the native form."""
+    rng = np.random.default_rng(5)
+    dims = rng.integers(64, 2049, (512, 3))
+    As, Bs = [], []
+    for m, n, k in dims:
+        As.append(ia.Container.from_numpy(ctx, rng.uniform(-1, 1, (int(m), int(k))), (512, 512), (128, 128)))
+        Bs.append(ia.Container.from_numpy(ctx, rng.uniform(-1, 1, (int(k), int(n))), (512, 512), (128, 128)))
+    flop = float(sum(2.0 * int(m) * int(n) * int(k) for m, n, k in dims))
+    cs, bs = [(512, 512)] * len(dims), [(128, 128)] * len(dims)
+    res = {"workload": "batching 512 float64 products, m,n,k in [64,2048], chunk 512^2, block 128^2",
+           "flop": flop}
+    for name, form in (("native", ia.FORM_NATIVE), ("split", ia.FORM_SPLIT)):
+        ctx.set_form(form)
+        t = time.perf_counter()
+        batch = ia.Batch(ctx, As, Bs, cs, bs)
+        build_s = time.perf_counter() - t
+        info = batch.info()
+        dev, wall = [], []
+        for s in range(max(1, args.warmup - 1) + max(2, args.steps // 2)):
+            t = time.perf_counter()
+            outs = batch.run()
+            w = time.perf_counter() - t
+            d = ctx.timings()["total"]
+            for c in outs:
+                c.free()
+            if s >= max(1, args.warmup - 1):
+                dev.append(d)
+                wall.append(w * 1e3)
+        batch.free()
+        res[name] = {"graph_ms": float(np.mean(dev)), "tflops": flop / (np.mean(dev) * 1e-3) / 1e12,
+                     "run_wall_ms": float(np.mean(wall)), "build_s": build_s, **info}
+    ctx.set_form(ia.FORM_NATIVE)
+    for c in As + Bs:
+        c.free()
+    return res
+
+
 # ============================================================================ our arm
 def run_ours(args):
     world, rank, local, pg = dist_setup(args)
@@ -358,11 +503,26 @@ def run_ours(args):
                          "loop: per-pair LZ4 block decode, single-threaded OpenBLAS dgemm per worker thread, LZ4 "
                          "re-encode; rate scaled to the full product"}
 
+    pk = peaks()
+    secondary = None
+    if rank == 0 and world == 1 and not args.no_secondary:
+        for c in (Ac, Bc):
+            c.free()
+        torch.cuda.empty_cache()
+        secondary = {}
+        for key, fn in (("gemv_f32", lambda: secondary_gemv(ia, ctx, stream, args, pk)),
+                        ("precision_f32", lambda: secondary_f32(ia, ctx, stream, args)),
+                        ("batching_f64", lambda: secondary_batch(ia, ctx, stream, args))):
+            try:
+                secondary[key] = fn()
+            except Exception as e:          # reported, not fatal: the headline stands alone
+                secondary[key] = {"error": str(e)[:200]}
+            torch.cuda.empty_cache()
+
     if rank != 0:
         barrier(pg)
         return
     barrier(pg)
-    pk = peaks()
     hr = results[head]
     value = world * FLOP / (hr["ms"] * 1e-3) / 1e12
     roof = roofline(hr["kprof"], pk, dgemm_tflops, c_cbytes=hr.get("c_cbytes"), a_cb=a_cb, b_cb=b_cb)
@@ -396,6 +556,7 @@ def run_ours(args):
         "gpu_launches": int(hr["launches"]),
         "clocks": hr["clocks"],
         "peaks_used": {"hbm_gbs": pk.get("hbm_gbs"), "bf16_tflops": pk.get("bf16_tflops")},
+        "secondary": secondary,
     }
     if "split" in results and "native" in results:
         line["split_vs_native"] = {"speedup": results["native"]["ms"] / results["split"]["ms"],
@@ -412,6 +573,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--err-rows", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the GEMV, float32 and batching workloads")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -340,6 +340,30 @@ INA_API(ina_rc_t) iarray_b200_get_stream(iarray_context_t *ctx, void **stream);
 INA_API(ina_rc_t) iarray_b200_to_cframe_into(iarray_context_t *ctx, iarray_container_t *c, uint8_t *buf,
                                              int64_t cap, int64_t *len);
 
+/* Batched products (B200 addition; the reference has no counterpart: its callers loop over
+ * iarray_opt_gemm).  C_i = A_i * B_i for i < n, float64, each pair with its own shapes
+ * (A_i: M_i x K_i, B_i: K_i x N_i) and partitions, output i partitioned by storage[i].
+ * iarray_b200_batch_new decodes the operands, times the grouped product's tile
+ * configurations on them (autotuner; choice cached per set of shapes), runs the batch once
+ * and captures decode -> product -> encode of every problem in one CUDA graph: in the
+ * native form the products of all problems are one persistent grouped kernel launch, in
+ * the split form (context form IARRAY_B200_FORM_SPLIT) each problem's split-precision
+ * pipeline.  iarray_b200_batch_run replays the graph and returns n new containers in c
+ * (free each with iarray_container_free).  The operand containers are borrowed: they must
+ * stay alive and unchanged until iarray_b200_batch_free.  Operands must not be transposed
+ * views. */
+typedef struct iarray_b200_batch_s iarray_b200_batch_t;
+INA_API(ina_rc_t) iarray_b200_batch_new(iarray_context_t *ctx, int64_t n, iarray_container_t *const *a,
+                                        iarray_container_t *const *b, const iarray_storage_t *storage,
+                                        iarray_b200_batch_t **batch);
+INA_API(ina_rc_t) iarray_b200_batch_run(iarray_b200_batch_t *batch, iarray_container_t **c);
+/* Tile configuration chosen by the autotuner (0: 128x128, 1: 64x128, 2: 128x64, 3: 64x64;
+ * -1 in the split form), the tuning times of the four configurations in ms (-1: not
+ * measured, e.g. a cached choice), and the number of nodes of the captured graph. */
+INA_API(ina_rc_t) iarray_b200_batch_info(iarray_b200_batch_t *batch, int *tile_config, double *tune_ms,
+                                         int64_t *graph_nodes);
+INA_API(void) iarray_b200_batch_free(iarray_b200_batch_t **batch);
+
 /* Per-kernel device time (B200 addition; the reference has no counterpart).  While
  * enabled, every kernel launch of the library is bracketed by CUDA events on its stream;
  * iarray_b200_profile_kernels(1) clears the totals and starts, (0) stops.

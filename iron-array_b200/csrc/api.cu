@@ -15,6 +15,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -1210,4 +1211,350 @@ INA_API(ina_rc_t) iarray_opt_gemv(iarray_context_t *ctx, iarray_container_t *a, 
     rc = run_matmul(ctx, a, b, *c);
     if (INA_FAILED(rc)) iarray_container_free(ctx, c);
     return rc;
+}
+
+// ============================================================================ batched products
+// A batch of independent float64 products C_i = A_i * B_i with their own shapes and
+// partitions.  iarray_b200_batch_new allocates every buffer the batch needs, decodes the
+// operands once, runs the autotuner over the grouped product's tile configurations,
+// runs the whole batch once eagerly, and captures decode -> product -> encode of all
+// problems in one CUDA graph.  iarray_b200_batch_run replays the graph and turns the
+// encoded outputs into containers.  Native form: one persistent grouped DMMA launch over
+// the tiles of all problems (tiles ordered by descending K); split form: the Ozaki
+// pipeline of each problem, all inside the same graph.
+struct iarray_b200_batch_s {
+    iarray_context_t *ctx = nullptr;
+    int form = IARRAY_B200_FORM_NATIVE;
+    int64_t n = 0;
+    std::vector<iarray_container_t *> a, b;
+    std::vector<iarray_storage_t> storage;
+    std::vector<Geom> cgeom;
+    std::vector<int64_t> M, N, K, lda, ldb, ldc;
+    std::vector<DevBuf> dA, dB, dC, cbuf;
+    std::vector<iab::DecodeWork> decA, decB;
+    std::vector<iab::EncodeWork> enc;
+    std::vector<iab::OzakiWork> oz;
+    DevBuf status;                    // 16 ints per decode: [2i] operand A, [2i + 1] operand B
+    DevBuf chunks;                    // chunk tables of all outputs
+    std::vector<int64_t> chunk_base;  // first entry of output i in `chunks`
+    DevBuf probs;
+    std::vector<iab::GemmProblem> hprobs;
+    int cfg = 0, ctas = 0, total_tiles = 0;
+    double tune_ms[4] = {-1, -1, -1, -1};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t nodes = 0;
+};
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune_cache;   // problem-set signature -> tile configuration
+
+void batch_problems(iarray_b200_batch_t *bt, int cfg, std::vector<iab::GemmProblem> *out, int *total)
+{
+    std::vector<int64_t> order((size_t)bt->n);
+    for (int64_t i = 0; i < bt->n; i++) order[(size_t)i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return bt->K[(size_t)x] > bt->K[(size_t)y]; });
+    out->clear();
+    int t = 0;
+    for (int64_t i : order) {
+        iab::GemmProblem p;
+        p.M = (int)bt->M[(size_t)i]; p.N = (int)bt->N[(size_t)i]; p.K = (int)bt->K[(size_t)i];
+        p.tile_start = t;
+        p.A = bt->dA[(size_t)i].as<double>(); p.B = bt->dB[(size_t)i].as<double>(); p.C = bt->dC[(size_t)i].as<double>();
+        p.lda = bt->lda[(size_t)i]; p.ldb = bt->ldb[(size_t)i]; p.ldc = bt->ldc[(size_t)i];
+        if (p.M > 0 && p.N > 0) {
+            out->push_back(p);
+            t += iab::gemm_f64_grouped_tiles(cfg, p.M, p.N);
+        }
+    }
+    *total = t;
+}
+
+// Enqueues decode (parts & 1), product (parts & 2) and encode (parts & 4) of the whole
+// batch on the context stream.
+int batch_enqueue(iarray_b200_batch_t *bt, int parts)
+{
+    cudaStream_t st = bt->ctx->stream;
+    int *status = bt->status.as<int>();
+    for (int64_t i = 0; i < bt->n && (parts & 1); i++) {
+        const iarray_container_t *x[2] = {bt->a[(size_t)i], bt->b[(size_t)i]};
+        DevBuf *dst[2] = {&bt->dA[(size_t)i], &bt->dB[(size_t)i]};
+        iab::DecodeWork *w[2] = {&bt->decA[(size_t)i], &bt->decB[(size_t)i]};
+        const int64_t ld[2] = {bt->lda[(size_t)i], bt->ldb[(size_t)i]};
+        for (int k = 0; k < 2; k++) {
+            if (!x[k]->geom.nchunks) continue;
+            w[k]->ext_counters = status + (2 * i + k) * 16;
+            const int r = iab::decode_launch(x[k]->geom, x[k]->store->buf.as<uint8_t>(), (int64_t)x[k]->store->buf.n,
+                                             x[k]->store->d_off.as<int64_t>(), x[k]->store->d_len.as<int32_t>(), dst[k]->p,
+                                             ld[k], st, w[k]);
+            if (r) return r;
+        }
+    }
+    if (!(parts & 2)) {
+    } else if (bt->form == IARRAY_B200_FORM_SPLIT) {
+        for (int64_t i = 0; i < bt->n; i++) {
+            const int r = iab::gemm_f64_ozaki_launch(bt->M[(size_t)i], bt->N[(size_t)i], bt->K[(size_t)i],
+                                                     bt->dA[(size_t)i].as<double>(), bt->lda[(size_t)i],
+                                                     bt->dB[(size_t)i].as<double>(), bt->ldb[(size_t)i],
+                                                     bt->dC[(size_t)i].as<double>(), bt->ldc[(size_t)i],
+                                                     bt->ctx->split_terms, &bt->oz[(size_t)i], st);
+            if (r) return r;
+        }
+    } else if (bt->total_tiles > 0) {
+        iab::gemm_f64_grouped(bt->cfg, bt->probs.as<iab::GemmProblem>(), (int)bt->hprobs.size(), bt->total_tiles,
+                              bt->ctas, st);
+    }
+    for (int64_t i = 0; i < bt->n && (parts & 4); i++) {
+        const Geom &g = bt->cgeom[(size_t)i];
+        if (!g.nchunks) continue;
+        bt->enc[(size_t)i].ext_chunks = bt->chunks.as<iab::EncChunk>() + bt->chunk_base[(size_t)i];
+        const int r = iab::encode_launch(g, bt->dC[(size_t)i].p, bt->ldc[(size_t)i], true, IARRAY_AUTO_SPLIT,
+                                         &bt->cbuf[(size_t)i], &bt->enc[(size_t)i], st);
+        if (r) return r;
+    }
+    return 0;
+}
+
+ina_rc_t batch_rc(int r)
+{
+    if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    return rc_err(IARRAY_ERR_GPU_FAILED);
+}
+
+// Reads the decode status words: a failed decode is a codec failure.
+ina_rc_t batch_status(iarray_b200_batch_t *bt)
+{
+    std::vector<int> h((size_t)(bt->n * 32));
+    if (cudaMemcpy(h.data(), bt->status.p, h.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return rc_err(IARRAY_ERR_GPU_FAILED);
+    for (int64_t i = 0; i < 2 * bt->n; i++)
+        if (h[(size_t)(i * 16 + 1)]) return rc_err(IARRAY_ERR_BLOSC_FAILED);
+    if (bt->form == IARRAY_B200_FORM_SPLIT)
+        for (auto &w : bt->oz)
+            if (iab::gemm_f64_ozaki_finish(&w, bt->ctx->stream)) return rc_err(IARRAY_ERR_GPU_FAILED);
+    return INA_SUCCESS;
+}
+}  // namespace
+
+INA_API(ina_rc_t) iarray_b200_batch_new(iarray_context_t *ctx, int64_t n, iarray_container_t *const *a,
+                                        iarray_container_t *const *b, const iarray_storage_t *storage,
+                                        iarray_b200_batch_t **batch)
+{
+    CHECK_ARG(ctx && a && b && storage && batch && n > 0);
+    for (int64_t i = 0; i < n; i++) {
+        CHECK_ARG(a[i] && b[i]);
+        if (a[i]->dtshape.dtype != IARRAY_DATA_TYPE_DOUBLE || b[i]->dtshape.dtype != IARRAY_DATA_TYPE_DOUBLE)
+            return rc_err(IARRAY_ERR_INVALID_DTYPE);
+        if (a[i]->dtshape.ndim != 2 || b[i]->dtshape.ndim != 2) return rc_err(IARRAY_ERR_INVALID_NDIM);
+        if (a[i]->dtshape.shape[1] != b[i]->dtshape.shape[0]) return rc_err(IARRAY_ERR_INVALID_SHAPE);
+        if (a[i]->transposed || b[i]->transposed) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
+    }
+    std::unique_ptr<iarray_b200_batch_s> bt(new iarray_b200_batch_s());
+    bt->ctx = ctx;
+    bt->form = ctx->form;
+    bt->n = n;
+    const size_t un = (size_t)n;
+    bt->a.assign(a, a + n);
+    bt->b.assign(b, b + n);
+    bt->storage.assign(storage, storage + n);
+    bt->cgeom.resize(un);
+    bt->M.resize(un); bt->N.resize(un); bt->K.resize(un); bt->lda.resize(un); bt->ldb.resize(un); bt->ldc.resize(un);
+    bt->dA.resize(un); bt->dB.resize(un); bt->dC.resize(un); bt->cbuf.resize(un);
+    bt->decA.resize(un); bt->decB.resize(un); bt->enc.resize(un);
+    if (bt->form == IARRAY_B200_FORM_SPLIT) bt->oz.resize(un);
+    bt->chunk_base.resize(un);
+    int64_t nch = 0;
+    for (size_t i = 0; i < un; i++) {
+        const int64_t M = a[i]->dtshape.shape[0], K = a[i]->dtshape.shape[1], N = b[i]->dtshape.shape[1];
+        bt->M[i] = M; bt->N[i] = N; bt->K[i] = K;
+        bt->lda[i] = pad_ld(K); bt->ldb[i] = pad_ld(N); bt->ldc[i] = pad_ld(N);
+        const int64_t shape[2] = {M, N};
+        if (!iab::make_geom(2, shape, storage[i].chunkshape, storage[i].blockshape, 8, &bt->cgeom[i]))
+            return rc_err(IARRAY_ERR_INVALID_STORAGE);
+        if (!bt->dA[i].allocate((size_t)std::max<int64_t>(M * bt->lda[i] * 8, 16), ctx->device) ||
+            !bt->dB[i].allocate((size_t)std::max<int64_t>(K * bt->ldb[i] * 8, 16), ctx->device) ||
+            !bt->dC[i].allocate((size_t)std::max<int64_t>(M * bt->ldc[i] * 8, 16), ctx->device))
+            return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+        bt->chunk_base[i] = nch;
+        nch += bt->cgeom[i].nchunks;
+    }
+    if (!bt->status.allocate((size_t)(n * 32 * sizeof(int)), ctx->device) ||
+        !bt->chunks.allocate((size_t)std::max<int64_t>(nch, 1) * sizeof(iab::EncChunk), ctx->device))
+        return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    cudaMemsetAsync(bt->status.p, 0, bt->status.n, ctx->stream);
+    // autotuner (native form): time every tile configuration of the grouped kernel on the
+    // decoded operands of this batch; the choice is cached per problem-set signature
+    std::string sig;
+    for (size_t i = 0; i < un; i++)
+        sig += std::to_string(bt->M[i]) + "x" + std::to_string(bt->N[i]) + "x" + std::to_string(bt->K[i]) + ";";
+    bt->cfg = 0;
+    if (bt->form != IARRAY_B200_FORM_SPLIT) {
+        bool cached = false;
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            auto it = g_tune_cache.find(sig);
+            if (it != g_tune_cache.end()) { bt->cfg = it->second; cached = true; }
+        }
+        // first eager pass: decode every operand (also sets up the codec kernels)
+        {
+            const int r = batch_enqueue(bt.get(), 1);
+            if (r) return batch_rc(r);
+            if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return rc_err(IARRAY_ERR_GPU_FAILED);
+            ina_rc_t rc = batch_status(bt.get());
+            if (INA_FAILED(rc)) return rc;
+        }
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        for (int cfg = 0; cfg < 4 && !cached; cfg++) {
+            std::vector<iab::GemmProblem> hp;
+            int total = 0;
+            batch_problems(bt.get(), cfg, &hp, &total);
+            DevBuf dp;
+            if (!dp.allocate(std::max<size_t>(hp.size(), 1) * sizeof(iab::GemmProblem), ctx->device)) break;
+            cudaMemcpyAsync(dp.p, hp.data(), hp.size() * sizeof(iab::GemmProblem), cudaMemcpyHostToDevice, ctx->stream);
+            const int ctas = iab::gemm_f64_grouped_ctas(cfg);
+            iab::gemm_f64_grouped(cfg, dp.as<iab::GemmProblem>(), (int)hp.size(), total, ctas, ctx->stream);
+            cudaEventRecord(e0, ctx->stream);
+            for (int rep = 0; rep < 2; rep++)
+                iab::gemm_f64_grouped(cfg, dp.as<iab::GemmProblem>(), (int)hp.size(), total, ctas, ctx->stream);
+            cudaEventRecord(e1, ctx->stream);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            bt->tune_ms[cfg] = ms / 2;
+            if (bt->tune_ms[bt->cfg] < 0 || bt->tune_ms[cfg] < bt->tune_ms[bt->cfg]) bt->cfg = cfg;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (cudaGetLastError() != cudaSuccess) return rc_err(IARRAY_ERR_GPU_FAILED);
+        if (!cached) {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tune_cache[sig] = bt->cfg;
+        }
+        batch_problems(bt.get(), bt->cfg, &bt->hprobs, &bt->total_tiles);
+        bt->ctas = iab::gemm_f64_grouped_ctas(bt->cfg);
+        if (!bt->probs.allocate(std::max<size_t>(bt->hprobs.size(), 1) * sizeof(iab::GemmProblem), ctx->device))
+            return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+        cudaMemcpyAsync(bt->probs.p, bt->hprobs.data(), bt->hprobs.size() * sizeof(iab::GemmProblem),
+                        cudaMemcpyHostToDevice, ctx->stream);
+    }
+    // one complete eager pass, then the capture (every buffer above is owned by the batch,
+    // so the graph's pointers stay valid until iarray_b200_batch_free)
+    {
+        const int r = batch_enqueue(bt.get(), 7);
+        if (r) return batch_rc(r);
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return rc_err(IARRAY_ERR_GPU_FAILED);
+        ina_rc_t rc = batch_status(bt.get());
+        if (INA_FAILED(rc)) return rc;
+    }
+    // kernel profiling records events around launches: keep it out of the capture
+    const bool prof = iab::kprof_enable(false);
+    if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+        iab::kprof_enable(prof);
+        return rc_err(IARRAY_ERR_GPU_FAILED);
+    }
+    const int r = batch_enqueue(bt.get(), 7);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+    iab::kprof_enable(prof);
+    if (r || ce != cudaSuccess || !graph) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return r ? batch_rc(r) : rc_err(IARRAY_ERR_GPU_FAILED);
+    }
+    bt->graph = graph;
+    if (cudaGraphInstantiate(&bt->exec, graph, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return rc_err(IARRAY_ERR_GPU_FAILED);
+    }
+    size_t nodes = 0;
+    cudaGraphGetNodes(graph, nullptr, &nodes);
+    bt->nodes = (int64_t)nodes;
+    *batch = bt.release();
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_b200_batch_run(iarray_b200_batch_t *bt, iarray_container_t **c)
+{
+    CHECK_ARG(bt && c);
+    iarray_context_t *ctx = bt->ctx;
+    const size_t un = (size_t)bt->n;
+    for (size_t i = 0; i < un; i++) c[i] = nullptr;
+    cudaEventRecord(ctx->ev[0], ctx->stream);
+    if (cudaGraphLaunch(bt->exec, ctx->stream) != cudaSuccess) return rc_err(IARRAY_ERR_GPU_FAILED);
+    cudaEventRecord(ctx->ev[4], ctx->stream);
+    int64_t nch = bt->chunk_base.empty() ? 0 : bt->chunk_base.back() + bt->cgeom.back().nchunks;
+    std::vector<iab::EncChunk> hc((size_t)std::max<int64_t>(nch, 1));
+    cudaMemcpyAsync(hc.data(), bt->chunks.p, (size_t)nch * sizeof(iab::EncChunk), cudaMemcpyDeviceToHost, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return rc_err(IARRAY_ERR_GPU_FAILED);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[4]);
+    for (int k = 0; k < 4; k++) ctx->timings[k] = 0;
+    ctx->timings[2] = ms;
+    ctx->timings[4] = ms;
+    ina_rc_t rc = batch_status(bt);
+    if (INA_FAILED(rc)) return rc;
+    for (size_t i = 0; i < un && INA_SUCCEED(rc); i++) {
+        iarray_dtshape_t d;
+        memset(&d, 0, sizeof(d));
+        d.dtype = IARRAY_DATA_TYPE_DOUBLE;
+        d.ndim = 2;
+        d.shape[0] = bt->M[i];
+        d.shape[1] = bt->N[i];
+        iarray_storage_t st = bt->storage[i];
+        rc = new_container(ctx, &d, &st, &c[i]);
+        if (INA_FAILED(rc)) break;
+        iarray_container_t *ci = c[i];
+        if (!ci->geom.nchunks) { rc = fill_zero_chunks(ci); continue; }
+        ChunkStore &s = *ci->store;
+        const int64_t n = ci->geom.nchunks, base = bt->chunk_base[i];
+        s.off.resize((size_t)n);
+        s.len.resize((size_t)n);
+        int64_t total = 0;
+        for (int64_t k = 0; k < n; k++) {
+            s.off[(size_t)k] = hc[(size_t)(base + k)].offset;
+            s.len[(size_t)k] = hc[(size_t)(base + k)].cbytes;
+            total = std::max<int64_t>(total, s.off[(size_t)k] + s.len[(size_t)k]);
+        }
+        if (!s.buf.allocate((size_t)std::max<int64_t>(total, 1), ctx->device) ||
+            !s.d_off.allocate((size_t)n * 8, ctx->device) || !s.d_len.allocate((size_t)n * 4, ctx->device)) {
+            rc = rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+            break;
+        }
+        cudaMemcpyAsync(s.buf.p, bt->cbuf[i].p, (size_t)total, cudaMemcpyDeviceToDevice, ctx->stream);
+        cudaMemcpyAsync(s.d_off.p, s.off.data(), (size_t)n * 8, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync(s.d_len.p, s.len.data(), (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream);
+        s.cbytes = 0;
+        for (int32_t l : s.len) s.cbytes += l;
+    }
+    if (INA_SUCCEED(rc) && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = rc_err(IARRAY_ERR_GPU_FAILED);
+    if (INA_FAILED(rc))
+        for (size_t i = 0; i < un; i++)
+            if (c[i]) iarray_container_free(ctx, &c[i]);
+    return rc;
+}
+
+INA_API(ina_rc_t) iarray_b200_batch_info(iarray_b200_batch_t *bt, int *tile_config, double *tune_ms,
+                                         int64_t *graph_nodes)
+{
+    CHECK_ARG(bt);
+    if (tile_config) *tile_config = bt->form == IARRAY_B200_FORM_SPLIT ? -1 : bt->cfg;
+    if (tune_ms)
+        for (int k = 0; k < 4; k++) tune_ms[k] = bt->tune_ms[k];
+    if (graph_nodes) *graph_nodes = bt->nodes;
+    return INA_SUCCESS;
+}
+
+INA_API(void) iarray_b200_batch_free(iarray_b200_batch_t **batch)
+{
+    if (!batch || !*batch) return;
+    iarray_b200_batch_t *bt = *batch;
+    // the context may already be gone: wait on the device, not on the context's stream
+    cudaDeviceSynchronize();
+    if (bt->exec) cudaGraphExecDestroy(bt->exec);
+    if (bt->graph) cudaGraphDestroy(bt->graph);
+    delete bt;
+    *batch = nullptr;
 }

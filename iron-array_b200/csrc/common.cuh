@@ -139,6 +139,9 @@ private:
     cudaEvent_t e0_ = nullptr;
 };
 
+// Switches kernel profiling on or off without clearing it; returns the previous state.
+bool kprof_enable(bool on);
+
 struct CodecStats { int32_t err; };
 
 // Decode `g.nchunks` chunks (buffer d_chunks, offsets d_off) into a dense row-major
@@ -198,11 +201,19 @@ struct GemmProblem {
     int64_t lda, ldb, ldc;
 };
 int gemm_f64_grouped_tiles(int cfg, int M, int N);
+int gemm_f64_grouped_ctas(int cfg);          // resident CTAs of the persistent launch (SMs x occupancy)
 void gemm_f64_grouped(int cfg, const GemmProblem *d_probs, int nprob, int total_tiles, int ctas, cudaStream_t st);
 
 // Split-precision forms; return 0 on success, < 0 when unsupported on this device.
 int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda,
                    const double *B, int64_t ldb, double *C, int64_t ldc, int nterms, cudaStream_t st);
+// Asynchronous form with caller-owned work buffers (no host synchronisation until finish).
+struct OzakiWork {
+    DevBuf ra, rb, rr, sa, sb, pm, ps, err;
+};
+int gemm_f64_ozaki_launch(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B,
+                          int64_t ldb, double *C, int64_t ldc, int nterms, OzakiWork *w, cudaStream_t st);
+int gemm_f64_ozaki_finish(OzakiWork *w, cudaStream_t st);
 int gemm_f32_bf16x3(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda,
                     const float *B, int64_t ldb, float *C, int64_t ldc, cudaStream_t st);
 

@@ -209,6 +209,29 @@ static void launch_grouped(const GemmProblem *d_probs, int nprob, int total, int
         d_probs, nprob, total));
 }
 
+template <int BM, int BN>
+static int grouped_ctas()
+{
+    using G = f64k::Cfg<BM, BN>;
+    cudaFuncSetAttribute(k_gemm_f64_grouped<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+    int per_sm = 0, dev = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gemm_f64_grouped<BM, BN>, 256, G::SMEM) != cudaSuccess)
+        per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return std::max(1, per_sm) * std::max(1, sms);
+}
+
+int gemm_f64_grouped_ctas(int cfg)
+{
+    switch (cfg) {
+    case 0: return grouped_ctas<128, 128>();
+    case 1: return grouped_ctas<64, 128>();
+    case 2: return grouped_ctas<128, 64>();
+    default: return grouped_ctas<64, 64>();
+    }
+}
+
 void gemm_f64_grouped(int cfg, const GemmProblem *d_probs, int nprob, int total_tiles, int ctas, cudaStream_t st)
 {
     switch (cfg) {

@@ -69,6 +69,11 @@ KernelTimer::~KernelTimer()
     g_pending.push_back({name_, e0_, e1});
 }
 
+bool kprof_enable(bool on)
+{
+    return g_on.exchange(on);
+}
+
 }  // namespace iab
 
 INA_API(ina_rc_t) iarray_b200_profile_kernels(int on)

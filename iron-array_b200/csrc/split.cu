@@ -548,6 +548,24 @@ static bool device_is_sm100()
 int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B, int64_t ldb,
                    double *C, int64_t ldc, int nterms, cudaStream_t st)
 {
+    OzakiWork w;
+    const int r = gemm_f64_ozaki_launch(M, N, K, A, lda, B, ldb, C, ldc, nterms, &w, st);
+    if (r) return r;
+    return gemm_f64_ozaki_finish(&w, st);
+}
+
+int gemm_f64_ozaki_finish(OzakiWork *w, cudaStream_t st)
+{
+    if (!w->err.p) return 0;
+    int h_err = 0;
+    cudaMemcpyAsync(&h_err, w->err.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return -2;
+    return h_err ? -3 : 0;
+}
+
+int gemm_f64_ozaki_launch(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B, int64_t ldb,
+                          double *C, int64_t ldc, int nterms, OzakiWork *w, cudaStream_t st)
+{
     if (!device_is_sm100()) return -1;
     if (M <= 0 || N <= 0 || K <= 0) return 0;
     // |sum_k a*b| <= K * 2^14 must keep the epilogue's float quotient within one of the
@@ -571,7 +589,7 @@ int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda
     cudaGetDevice(&dev);
     const int64_t Kp = round_up(K, oz::BK);
     const int64_t ldr = round_up(N, 16);
-    DevBuf ra, rb, rr, sa, sb, pm, ps, err;
+    DevBuf &ra = w->ra, &rb = w->rb, &rr = w->rr, &sa = w->sa, &sb = w->sb, &pm = w->pm, &ps = w->ps, &err = w->err;
     if (!ra.allocate((size_t)(L * M * Kp), dev) || !rb.allocate((size_t)(L * N * Kp), dev) ||
         !rr.allocate((size_t)(L * M * ldr), dev) || !sa.allocate((size_t)M * 4, dev) ||
         !sb.allocate((size_t)N * 4, dev) || !pm.allocate((size_t)COL_SEGS * N * 8, dev) ||
@@ -605,10 +623,7 @@ int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda
     const int tiles = L * prm.tiles_m * prm.tiles_n;
     IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
     IAB_TIMED("k_crt", st, k_crt<<<(unsigned)(nsm * 8), 256, 0, st>>>((int)M, (int)N, rr.as<uint8_t>(), ldr, sa.as<int>(), sb.as<int>(), C, ldc));
-    int h_err = 0;
-    cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (cudaStreamSynchronize(st) != cudaSuccess) return -2;
-    return h_err ? -3 : 0;
+    return 0;
 }
 
 // ============================================================================ float32: 3xBF16

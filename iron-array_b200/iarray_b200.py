@@ -124,6 +124,10 @@ def _lib():
             "iarray_b200_get_stream": ([P, P], RC),
             "iarray_b200_to_cframe_into": ([P, P, P, I64, P], RC),
             "iarray_b200_profile_kernels": ([ctypes.c_int], RC),
+            "iarray_b200_batch_new": ([P, I64, P, P, P, P], RC),
+            "iarray_b200_batch_run": ([P, P], RC),
+            "iarray_b200_batch_info": ([P, P, P, P], RC),
+            "iarray_b200_batch_free": ([P], None),
             "iarray_b200_kernel_profile": ([P, I64, P], RC),
             "iarray_b200_decode_noalloc": ([ctypes.c_int8, P, P, P, ctypes.c_int32, P, I64, P, I64, P], RC),
         }
@@ -405,6 +409,46 @@ def opt_gemm_b(ctx, a, b, chunkshape, blockshape):
 
 def opt_gemv(ctx, a, b, chunkshape, blockshape):
     return _product(_lib().iarray_opt_gemv, "iarray_opt_gemv", ctx, a, b, chunkshape, blockshape)
+
+
+class Batch:
+    """Batched float64 products C_i = A_i * B_i (iarray_b200_batch_*): built once (autotuned
+    grouped product, captured CUDA graph), run any number of times."""
+
+    def __init__(self, ctx, As, Bs, chunkshapes, blockshapes):
+        n = len(As)
+        self.ctx, self.n = ctx, n
+        self._keep = (list(As), list(Bs))
+        a = (ctypes.c_void_p * n)(*[x.ptr for x in As])
+        b = (ctypes.c_void_p * n)(*[x.ptr for x in Bs])
+        st = (Storage * n)()
+        for i in range(n):
+            st[i] = storage(chunkshapes[i], blockshapes[i])
+        self.ptr = ctypes.c_void_p()
+        check(_lib().iarray_b200_batch_new(ctx.ptr, n, a, b, st, ctypes.byref(self.ptr)), "iarray_b200_batch_new")
+
+    def run(self):
+        out = (ctypes.c_void_p * self.n)()
+        check(_lib().iarray_b200_batch_run(self.ptr, out), "iarray_b200_batch_run")
+        return [Container(self.ctx, ctypes.c_void_p(out[i])) for i in range(self.n)]
+
+    def info(self):
+        cfg = ctypes.c_int()
+        ms = (ctypes.c_double * 4)()
+        nodes = ctypes.c_int64()
+        check(_lib().iarray_b200_batch_info(self.ptr, ctypes.byref(cfg), ms, ctypes.byref(nodes)))
+        return {"tile_config": cfg.value, "tune_ms": list(ms), "graph_nodes": nodes.value}
+
+    def free(self):
+        if self.ptr:
+            _lib().iarray_b200_batch_free(ctypes.byref(self.ptr))
+            self.ptr = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 def almost_equal(a, b, tol):
