@@ -1244,6 +1244,18 @@ struct iarray_b200_batch_s {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int64_t nodes = 0;
+    // independent containers are decoded / encoded on parallel branches
+    std::vector<cudaStream_t> br;
+    std::vector<cudaEvent_t> brev;
+    cudaEvent_t fork = nullptr;
+    ~iarray_b200_batch_s()
+    {
+        for (cudaStream_t x : br)
+            if (x) cudaStreamDestroy(x);
+        for (cudaEvent_t e : brev)
+            if (e) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
+    }
 };
 
 namespace {
@@ -1273,11 +1285,28 @@ void batch_problems(iarray_b200_batch_t *bt, int cfg, std::vector<iab::GemmProbl
 
 // Enqueues decode (parts & 1), product (parts & 2) and encode (parts & 4) of the whole
 // batch on the context stream.
+// Branch streams: fork from the context stream, join back into it.
+void batch_fork(iarray_b200_batch_t *bt)
+{
+    cudaEventRecord(bt->fork, bt->ctx->stream);
+    for (cudaStream_t x : bt->br) cudaStreamWaitEvent(x, bt->fork, 0);
+}
+void batch_join(iarray_b200_batch_t *bt)
+{
+    for (size_t k = 0; k < bt->br.size(); k++) {
+        cudaEventRecord(bt->brev[k], bt->br[k]);
+        cudaStreamWaitEvent(bt->ctx->stream, bt->brev[k], 0);
+    }
+}
+
 int batch_enqueue(iarray_b200_batch_t *bt, int parts)
 {
     cudaStream_t st = bt->ctx->stream;
     int *status = bt->status.as<int>();
+    const size_t nbr = bt->br.size();
+    if (parts & 1) batch_fork(bt);
     for (int64_t i = 0; i < bt->n && (parts & 1); i++) {
+        cudaStream_t bs = bt->br[(size_t)i % nbr];
         const iarray_container_t *x[2] = {bt->a[(size_t)i], bt->b[(size_t)i]};
         DevBuf *dst[2] = {&bt->dA[(size_t)i], &bt->dB[(size_t)i]};
         iab::DecodeWork *w[2] = {&bt->decA[(size_t)i], &bt->decB[(size_t)i]};
@@ -1287,32 +1316,37 @@ int batch_enqueue(iarray_b200_batch_t *bt, int parts)
             w[k]->ext_counters = status + (2 * i + k) * 16;
             const int r = iab::decode_launch(x[k]->geom, x[k]->store->buf.as<uint8_t>(), (int64_t)x[k]->store->buf.n,
                                              x[k]->store->d_off.as<int64_t>(), x[k]->store->d_len.as<int32_t>(), dst[k]->p,
-                                             ld[k], st, w[k]);
-            if (r) return r;
+                                             ld[k], bs, w[k]);
+            if (r) { batch_join(bt); return r; }
         }
     }
+    if (parts & 1) batch_join(bt);
     if (!(parts & 2)) {
     } else if (bt->form == IARRAY_B200_FORM_SPLIT) {
+        batch_fork(bt);
         for (int64_t i = 0; i < bt->n; i++) {
             const int r = iab::gemm_f64_ozaki_launch(bt->M[(size_t)i], bt->N[(size_t)i], bt->K[(size_t)i],
                                                      bt->dA[(size_t)i].as<double>(), bt->lda[(size_t)i],
                                                      bt->dB[(size_t)i].as<double>(), bt->ldb[(size_t)i],
                                                      bt->dC[(size_t)i].as<double>(), bt->ldc[(size_t)i],
-                                                     bt->ctx->split_terms, &bt->oz[(size_t)i], st);
-            if (r) return r;
+                                                     bt->ctx->split_terms, &bt->oz[(size_t)i], bt->br[(size_t)i % nbr]);
+            if (r) { batch_join(bt); return r; }
         }
+        batch_join(bt);
     } else if (bt->total_tiles > 0) {
         iab::gemm_f64_grouped(bt->cfg, bt->probs.as<iab::GemmProblem>(), (int)bt->hprobs.size(), bt->total_tiles,
                               bt->ctas, st);
     }
+    if (parts & 4) batch_fork(bt);
     for (int64_t i = 0; i < bt->n && (parts & 4); i++) {
         const Geom &g = bt->cgeom[(size_t)i];
         if (!g.nchunks) continue;
         bt->enc[(size_t)i].ext_chunks = bt->chunks.as<iab::EncChunk>() + bt->chunk_base[(size_t)i];
         const int r = iab::encode_launch(g, bt->dC[(size_t)i].p, bt->ldc[(size_t)i], true, IARRAY_AUTO_SPLIT,
-                                         &bt->cbuf[(size_t)i], &bt->enc[(size_t)i], st);
-        if (r) return r;
+                                         &bt->cbuf[(size_t)i], &bt->enc[(size_t)i], bt->br[(size_t)i % nbr]);
+        if (r) { batch_join(bt); return r; }
     }
+    if (parts & 4) batch_join(bt);
     return 0;
 }
 
@@ -1352,6 +1386,17 @@ INA_API(ina_rc_t) iarray_b200_batch_new(iarray_context_t *ctx, int64_t n, iarray
     }
     std::unique_ptr<iarray_b200_batch_s> bt(new iarray_b200_batch_s());
     bt->ctx = ctx;
+    {
+        const int nbr = (int)std::min<int64_t>(n, 16);
+        bt->br.resize((size_t)nbr);
+        bt->brev.resize((size_t)nbr);
+        for (int k = 0; k < nbr; k++) {
+            if (cudaStreamCreateWithFlags(&bt->br[(size_t)k], cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&bt->brev[(size_t)k], cudaEventDisableTiming) != cudaSuccess)
+                return rc_err(IARRAY_ERR_GPU_FAILED);
+        }
+        if (cudaEventCreateWithFlags(&bt->fork, cudaEventDisableTiming) != cudaSuccess) return rc_err(IARRAY_ERR_GPU_FAILED);
+    }
     bt->form = ctx->form;
     bt->n = n;
     const size_t un = (size_t)n;
