@@ -294,6 +294,16 @@ typedef enum iarray_b200_form_e {
 } iarray_b200_form_t;
 
 INA_API(ina_rc_t) iarray_b200_set_form(iarray_context_t *ctx, iarray_b200_form_t form);
+/* LZ4 encoder used when this context writes chunks.  Both write standard LZ4 blocks that
+ * the reference's Blosc2 decodes bit-exactly.  LIBLZ4 (default) reproduces liblz4 1.9.4
+ * LZ4_compress_fast(acceleration 1), c-blosc2's codec, byte for byte, so chunks equal the
+ * reference's own; PARALLEL parses each window of every stream in parallel (different
+ * bytes, compression ratio within a few percent on typical data). */
+typedef enum iarray_b200_encoder_e {
+    IARRAY_B200_ENCODER_PARALLEL = 0,
+    IARRAY_B200_ENCODER_LIBLZ4 = 1,
+} iarray_b200_encoder_t;
+INA_API(ina_rc_t) iarray_b200_set_encoder(iarray_context_t *ctx, iarray_b200_encoder_t encoder);
 /* Number of INT8 moduli/slices the float64 split form uses (0 = automatic). */
 INA_API(ina_rc_t) iarray_b200_set_split_terms(iarray_context_t *ctx, int nterms);
 

@@ -169,6 +169,7 @@ struct iarray_context_s {
     cudaStream_t stream = nullptr;
     int form = IARRAY_B200_FORM_NATIVE;
     int split_terms = 0;
+    int encoder = IARRAY_B200_ENCODER_LIBLZ4;
     double timings[5] = {0, 0, 0, 0, 0};
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     cudaStream_t stream2 = nullptr;          // second stream for concurrent operand decode
@@ -283,6 +284,13 @@ INA_API(void) iarray_context_free(iarray_context_t **ctx)
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
     delete c;
     *ctx = nullptr;
+}
+
+INA_API(ina_rc_t) iarray_b200_set_encoder(iarray_context_t *ctx, iarray_b200_encoder_t encoder)
+{
+    CHECK_ARG(ctx && (encoder == IARRAY_B200_ENCODER_PARALLEL || encoder == IARRAY_B200_ENCODER_LIBLZ4));
+    ctx->encoder = encoder;
+    return INA_SUCCESS;
 }
 
 INA_API(ina_rc_t) iarray_b200_set_form(iarray_context_t *ctx, iarray_b200_form_t form)
@@ -423,7 +431,8 @@ static ina_rc_t encode_into(iarray_context_t *ctx, iarray_container_t *c, const 
     DevBuf out;
     std::vector<int64_t> off;
     std::vector<int32_t> len;
-    int r = iab::encode_container(c->geom, dense, ld, c->shuffle, c->splitmode, &out, &off, &len, ctx->stream);
+    int r = iab::encode_container(c->geom, dense, ld, c->shuffle, c->splitmode, &out, &off, &len, ctx->stream,
+                                  ctx->encoder == IARRAY_B200_ENCODER_LIBLZ4);
     if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
     if (r != 0) return rc_err(IARRAY_ERR_GPU_FAILED);
     s.buf = std::move(out);
@@ -1342,6 +1351,7 @@ int batch_enqueue(iarray_b200_batch_t *bt, int parts)
         const Geom &g = bt->cgeom[(size_t)i];
         if (!g.nchunks) continue;
         bt->enc[(size_t)i].ext_chunks = bt->chunks.as<iab::EncChunk>() + bt->chunk_base[(size_t)i];
+        bt->enc[(size_t)i].exact_lz4 = bt->ctx->encoder == IARRAY_B200_ENCODER_LIBLZ4;
         const int r = iab::encode_launch(g, bt->dC[(size_t)i].p, bt->ldc[(size_t)i], true, IARRAY_AUTO_SPLIT,
                                          &bt->cbuf[(size_t)i], &bt->enc[(size_t)i], bt->br[(size_t)i % nbr]);
         if (r) { batch_join(bt); return r; }

@@ -1120,6 +1120,268 @@ __global__ void __launch_bounds__(96, 3) k_lz4_encode(const uint8_t *__restrict_
     }
 }
 
+// ---------------------------------------------------------------- LZ4 encoder, parallel parse
+// The second encoder mode.  It writes standard LZ4 blocks (any LZ4 decoder, liblz4 and the
+// reference's Blosc2 included, reads them back bit-exactly) but does not retrace liblz4's
+// serial search, so its bytes differ from liblz4's.  Per window of PW positions:
+//  A. every position is hashed (4 bytes, 13 bits); its candidate is the table entry of its
+//     bucket as of the previous round of 32 positions (the table keeps the low 16 bits of a
+//     recent position of each bucket; a reconstructed position is verified by its bytes),
+//     and the previous position is a second candidate (runs); the longer match is kept,
+//     measured up to PCAP bytes.  Every position enters the table.
+//  B. the greedy parse (from the parse position, take the first position with a match of
+//     at least 4 bytes, continue after it) is a chain over match positions: J[q] = the first
+//     match position at or after q + L(q).  The chain is located by pointer doubling (J,
+//     J^2, J^4, ... in two ping-pong tables, the chain doubled alongside), the sequences'
+//     output sizes are prefix-summed across the warp, and every lane writes its own
+//     sequences.  A chain ends at the window end, after the window's last match, or at a
+//     match of PCAP bytes or more, which is extended exactly before it is written.
+// Format rules kept: offsets 1..65535, matches start at least 12 bytes before the end and
+// end at least 5 bytes before it, so the block ends with >= 5 literals.
+constexpr int PW = 1024;
+constexpr int PCAP = 128;                 // match lengths measured in phase A (PCAP: at least PCAP)
+constexpr uint16_t PJ_NONE = 0xFFFF, PJ_OUT = 0xFFFE, PJ_LONG = 0xFFFD;
+
+struct ParSmem {              // per warp
+    uint16_t tab[8192];
+    uint8_t ring[ERING + 16];
+    uint16_t cw[PW];          // match distance of each window position
+    uint8_t lw[PW];           // match length (0: none, 4..PCAP; PCAP: at least PCAP)
+    uint16_t J[2][PW];        // chain tables
+    uint16_t path[PW / 4 * 2 + 2];
+    uint32_t bits[32];        // match flags, one word per 32 positions
+};
+
+// First match position at or after window offset rel (PJ_NONE: none left in the window).
+__device__ __forceinline__ uint32_t par_next_match(const uint32_t *bits, int rel)
+{
+    if (rel >= PW) return PJ_OUT;
+    int wi = rel >> 5;
+    uint32_t m = bits[wi] & (0xFFFFFFFFu << (rel & 31));
+    while (!m && ++wi < 32) m = bits[wi];
+    return m ? (uint32_t)(wi * 32 + __ffs((int)m) - 1) : PJ_NONE;
+}
+
+__device__ __forceinline__ int lz4_seq_bytes(int lit, int ml)
+{
+    return 1 + (lit >= 15 ? 1 + (lit - 15) / 255 : 0) + lit + 2 + (ml >= 15 ? 1 + (ml - 15) / 255 : 0);
+}
+
+// One sequence (literals src[anchor, q), match at q, distance d, length L) at dst + o.
+__device__ __forceinline__ void lz4_put_seq(const EncSrc &s, uint8_t *o, int anchor, int q, int d, int L)
+{
+    const int lit = q - anchor, ml = L - 4;
+    int k = 1;
+    if (lit >= 15) {
+        int rem = lit - 15;
+        for (; rem >= 255; rem -= 255) o[k++] = 255;
+        o[k++] = (uint8_t)rem;
+    }
+    for (int x = 0; x < lit; x++) o[k + x] = (uint8_t)es_byte(s, anchor + x);
+    k += lit;
+    o[0] = (uint8_t)(((lit >= 15 ? 15 : lit) << 4) | (ml >= 15 ? 15 : ml));
+    o[k] = (uint8_t)d;
+    o[k + 1] = (uint8_t)(d >> 8);
+    k += 2;
+    if (ml >= 15) {
+        int rem = ml - 15;
+        for (; rem >= 255; rem -= 255) o[k++] = 255;
+        o[k] = (uint8_t)rem;
+    }
+}
+
+__device__ __forceinline__ int warp_lz4_compress_par(const uint8_t *__restrict__ src, int n,
+                                                     uint8_t *__restrict__ dst, int cap, ParSmem &S)
+{
+    const int lane = threadIdx.x & 31;
+    for (int i = lane; i < 8192; i += 32) S.tab[i] = 0;
+    EncSrc s;
+    s.g = src; s.r = S.ring; s.lo = 0; s.hi = 0; s.n = n;
+    __syncwarp();
+    int op = 0, anchor = 0, pos = 0;
+    const int mfl1 = n - 11, mlimit = n - 5;
+    for (int w0 = 0; n >= 13 && w0 < mfl1; w0 += PW) {
+        const int wend = min(w0 + PW, mfl1), wn = wend - w0;
+        es_fill(s, wend + PCAP + 32);
+        // ---- A: candidates and lengths
+        for (int r = 0; r < PW / 32; r++) {
+            const int p = w0 + r * 32 + lane;
+            const bool valid = p < wend;
+            const uint32_t v = valid ? es_rd32(s, p) : 0u;
+            const uint32_t h = (v * 2654435761u) >> (32 - 13);
+            const uint32_t tv = valid ? (uint32_t)S.tab[h] : 0u;
+            const int cand = p - (int)(((uint32_t)p - tv) & 0xFFFFu);
+            __syncwarp();
+            if (valid) S.tab[h] = (uint16_t)p;          // same-bucket lanes race: any of them may win
+            // two candidates: the table's and the previous position (runs); keep the longer
+            int L = 0, best = cand;
+            const int lim = min(mlimit - p, PCAP);
+#pragma unroll
+            for (int t = 0; t < 2; t++) {
+                const int c = t ? p - 1 : cand;
+                if (!valid || c >= p || c < 0 || (t && c == cand) || es_rd32(s, c) != v) continue;
+                int l = 4;
+                while (l < lim) {
+                    const uint32_t x = es_rd32(s, p + l) ^ es_rd32(s, c + l);
+                    if (x) { l += (__ffs((int)x) - 1) >> 3; break; }
+                    l += 4;
+                }
+                l = min(l, lim);
+                if (l > L) { L = l; best = c; }
+            }
+            S.cw[r * 32 + lane] = (uint16_t)(p - best);
+            S.lw[r * 32 + lane] = (uint8_t)L;
+            const unsigned b = __ballot_sync(FULLMASK, L >= 4);
+            if (lane == r) S.bits[r] = b;
+        }
+        __syncwarp();
+        // ---- B: chains of matches from the parse position
+        while (pos < wend) {
+            const uint32_t s0 = par_next_match(S.bits, pos - w0);
+            if (s0 >= (uint32_t)wn) { pos = wend; break; }   // no match left: literals run on
+            // J[q]: the match after the one at q, or why the chain stops there
+            for (int q = lane; q < wn; q += 32) {
+                const int L = S.lw[q];
+                uint16_t j = PJ_NONE;
+                if (L >= PCAP) j = PJ_LONG;
+                else if (L >= 4) {
+                    const uint32_t nx = par_next_match(S.bits, q + L);
+                    j = nx >= (uint32_t)wn ? (q + L >= wn ? PJ_OUT : PJ_NONE) : (uint16_t)nx;
+                }
+                S.J[0][q] = j;
+            }
+            if (lane == 0) S.path[0] = (uint16_t)s0;
+            __syncwarp();
+            int len = 1, cur = 0, cnt = 0;
+            for (;;) {
+                int first = 0x7FFFFFFF;
+                for (int j = lane; j < len; j += 32) {
+                    const uint16_t pj = S.path[j];
+                    const uint16_t v = pj < wn ? S.J[cur][pj] : pj;
+                    S.path[len + j] = v;
+                    if (v >= wn) first = min(first, len + j);
+                }
+                first = (int)__reduce_min_sync(FULLMASK, (unsigned)first);
+                __syncwarp();
+                if (first < 2 * len) { cnt = first; break; }
+                for (int q = lane; q < wn; q += 32) {
+                    const uint16_t v = S.J[cur][q];
+                    S.J[cur ^ 1][q] = v < wn ? S.J[cur][v] : v;
+                }
+                cur ^= 1;
+                len *= 2;
+                __syncwarp();
+            }
+            const uint16_t term = S.path[cnt];                  // why the chain stopped
+            // a capped last match: extend it exactly (warp-wide) before writing it
+            int lastL = S.lw[S.path[cnt - 1]];
+            const int lastq = w0 + S.path[cnt - 1], lastd = S.cw[S.path[cnt - 1]];
+            if (term == PJ_LONG) {
+                for (;;) {
+                    const int a = lastq + lastL;
+                    es_fill(s, a + 32 + ELOOK);
+                    const bool eq = a + lane < mlimit && es_byte(s, a + lane) == es_byte(s, a - lastd + lane);
+                    const unsigned ne = __ballot_sync(FULLMASK, !eq);
+                    const int cnum = ne ? __ffs((int)ne) - 1 : 32;
+                    lastL += cnum;
+                    if (cnum < 32) break;
+                }
+            }
+            // output sizes, exclusive prefix across the warp (lane owns sequences lane + 32 k)
+            int mine = 0;
+            for (int i = lane; i < cnt; i += 32) {
+                const int q = w0 + S.path[i];
+                const int prev_end = i ? w0 + S.path[i - 1] + S.lw[S.path[i - 1]] : anchor;
+                const int L = (i == cnt - 1) ? lastL : S.lw[S.path[i]];
+                mine += lz4_seq_bytes(q - prev_end, L - 4);
+            }
+            // a lane's sequences are not contiguous in order: scan per round of 32 instead
+            int total = (int)__reduce_add_sync(FULLMASK, (unsigned)mine);
+            if (op + total + 1 + 6 > cap) return 0;
+            int base = op;
+            for (int i0 = 0; i0 < cnt; i0 += 32) {
+                const int i = i0 + lane;
+                int sz = 0, q = 0, prev_end = 0, L = 0, d = 0;
+                if (i < cnt) {
+                    q = w0 + S.path[i];
+                    prev_end = i ? w0 + S.path[i - 1] + S.lw[S.path[i - 1]] : anchor;
+                    L = (i == cnt - 1) ? lastL : S.lw[S.path[i]];
+                    d = S.cw[S.path[i]];
+                    sz = lz4_seq_bytes(q - prev_end, L - 4);
+                }
+                int incl = sz;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(FULLMASK, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                if (i < cnt) lz4_put_seq(s, dst + base + incl - sz, prev_end, q, d, L);
+                base += __shfl_sync(FULLMASK, incl, 31);
+            }
+            op = base;
+            anchor = lastq + lastL;
+            pos = anchor;
+            __syncwarp();
+            if (term == PJ_NONE) { pos = max(pos, wend); }
+        }
+    }
+    {
+        const int last = n - anchor;
+        if (op + 1 + last + (last + 240) / 255 > cap) return 0;
+        uint8_t *o = dst + op;
+        int k = 1;
+        if (last >= 15) {
+            const int rem = last - 15, nff = rem / 255;
+            for (int x = lane; x < nff; x += 32) o[1 + x] = 255;
+            if (lane == 0) o[1 + nff] = (uint8_t)(rem % 255);
+            k += nff + 1;
+        }
+        if (lane == 0) o[0] = (uint8_t)((last >= 15 ? 15 : last) << 4);
+        for (int x = lane; x < last; x += 32) o[k + x] = (uint8_t)es_byte(s, anchor + x);
+        op += k + last;
+    }
+    __syncwarp();
+    return op;
+}
+
+// E2 (parallel mode): one warp per stream, as k_lz4_encode.
+__global__ void __launch_bounds__(64, 3) k_lz4_encode_par(const uint8_t *__restrict__ img, int64_t nstreams_total,
+                                                       int neblock, uint8_t *slots, EncStream *es,
+                                                       unsigned long long *next)
+{
+    extern __shared__ __align__(16) uint8_t sm_par[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    ParSmem &S = reinterpret_cast<ParSmem *>(sm_par)[warp];
+    for (;;) {
+        unsigned long long got = 0;
+        if (lane == 0) got = atomicAdd(next, 1ull);
+        const int64_t sid = (int64_t)__shfl_sync(FULLMASK, got, 0);
+        if (sid >= nstreams_total) break;
+        const uint8_t *src = img + sid * neblock;
+        const uint8_t first = __ldg(src);
+        bool run = true;
+        for (int b = 0; b < neblock && run; b += 32 * 16) {
+            bool mine = true;
+            for (int k = 0; k < 16; k++) {
+                const int x = b + k * 32 + lane;
+                if (x < neblock && __ldg(src + x) != first) mine = false;
+            }
+            run = __all_sync(FULLMASK, mine);
+        }
+        EncStream e;
+        e.out = -1;
+        if (run) {
+            e.kind = SK_RUN; e.csize = first; e.need = 0;
+        } else {
+            const int cs = warp_lz4_compress_par(src, neblock, slots + sid * neblock, neblock, S);
+            if (cs > 0 && cs < neblock) { e.kind = SK_LZ4; e.csize = cs; e.need = cs; }
+            else { e.kind = SK_RAW; e.csize = neblock; e.need = neblock + 1; }
+        }
+        if (lane == 0) es[sid] = e;
+        __syncwarp();
+    }
+}
+
 // E3: per chunk, walk streams in order as blosc_c does, assigning offsets and deciding
 // the memcpy fallback (destination capacity nbytes + 32); then scan chunk sizes.
 __global__ void k_layout(Geom g, int nstreams, int neblock, EncStream *es, EncChunk *ec, int64_t *total)
@@ -1393,7 +1655,7 @@ int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int s
         IAB_TIMED("k_gather", st, k_gather<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
             g, fast, (const uint8_t *)in, ld, shuffle, img.as<uint8_t>()));
     }
-    {
+    if (w->exact_lz4) {
         static bool attr = false;
         // per warp: 16 KiB hash table + the source window; 3 warps per CTA, 3 CTAs per SM
         const int wpb = 3, smem = wpb * (4096 * 4 + ERING + 16);
@@ -1404,6 +1666,18 @@ int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int s
         const int64_t ns = nbl * nstreams;
         const int64_t blocks = std::min<int64_t>((ns + wpb - 1) / wpb, (int64_t)sms * 3);
         IAB_TIMED("k_lz4_encode", st, k_lz4_encode<<<(unsigned)std::max<int64_t>(blocks, 1), wpb * 32, smem, st>>>(
+            img.as<uint8_t>(), ns, neblock, slots.as<uint8_t>(), es.as<EncStream>(),
+            reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1)));
+    } else {
+        static bool attr = false;
+        const int wpb = 2, smem = wpb * (int)sizeof(ParSmem);   // 2 warps per CTA, 3 CTAs per SM
+        if (!attr) {
+            cudaFuncSetAttribute(k_lz4_encode_par, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            attr = true;
+        }
+        const int64_t ns = nbl * nstreams;
+        const int64_t blocks = std::min<int64_t>((ns + wpb - 1) / wpb, (int64_t)sms * 3);
+        IAB_TIMED("k_lz4_encode_par", st, k_lz4_encode_par<<<(unsigned)std::max<int64_t>(blocks, 1), wpb * 32, smem, st>>>(
             img.as<uint8_t>(), ns, neblock, slots.as<uint8_t>(), es.as<EncStream>(),
             reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1)));
     }
@@ -1431,9 +1705,10 @@ int encode_finish(EncodeWork *w, std::vector<int64_t> *h_off, std::vector<int32_
 }
 
 int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, DevBuf *d_out,
-                     std::vector<int64_t> *h_off, std::vector<int32_t> *h_len, cudaStream_t st)
+                     std::vector<int64_t> *h_off, std::vector<int32_t> *h_len, cudaStream_t st, bool exact_lz4)
 {
     EncodeWork w;
+    w.exact_lz4 = exact_lz4;
     const int r = encode_launch(g, in, ld, shuffle, splitmode, d_out, &w, st);
     if (r) return r;
     return encode_finish(&w, h_off, h_len, st);

@@ -169,13 +169,16 @@ int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes,
 
 // Encode a dense row-major array into Blosc2 chunks.  On return *d_out holds the
 // chunks back-to-back, h_off / h_len (host) their offsets and lengths.
+// exact_lz4: streams byte-identical to liblz4 1.9.4 LZ4_compress_fast(acceleration 1); else
+// the parallel-parse encoder (valid LZ4, different bytes).
 int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode,
                      DevBuf *d_out, std::vector<int64_t> *h_off, std::vector<int32_t> *h_len,
-                     cudaStream_t st);
+                     cudaStream_t st, bool exact_lz4);
 // Asynchronous form: encode_launch enqueues the kernels (no host synchronisation; work
 // buffers held in *w), encode_finish synchronises and reads the chunk table.
 struct EncodeWork {
     DevBuf img, slots, es, ec, tot;
+    bool exact_lz4 = true;            // liblz4-identical streams (see encode_container)
     EncChunk *ext_chunks = nullptr;   // optional caller-owned chunk table (device) instead of `ec`
     int64_t nchunks = 0;
 };

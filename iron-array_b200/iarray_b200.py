@@ -22,6 +22,7 @@ NP_DTYPE = {DTYPE_DOUBLE: np.float64, DTYPE_FLOAT: np.float32, 10: np.int64, 11:
             13: np.int8, 16: np.uint64, 17: np.uint32, 18: np.uint16, 19: np.uint8}
 IA_DTYPE = {np.dtype(v): k for k, v in NP_DTYPE.items()}
 FORM_NATIVE, FORM_SPLIT = 0, 1
+ENCODER_PARALLEL, ENCODER_LIBLZ4 = 0, 1
 ALWAYS_SPLIT, NEVER_SPLIT, AUTO_SPLIT = 1, 2, 3
 
 RC_ERROR_BIT = 1 << 63
@@ -112,7 +113,7 @@ def _lib():
             "iarray_gemm": ([P, P, P, P], RC), "iarray_gemv": ([P, P, P, P], RC),
             "iarray_opt_gemm": ([P, P, P, P, P], RC), "iarray_opt_gemm_a": ([P, P, P, P, P], RC),
             "iarray_opt_gemm_b": ([P, P, P, P, P], RC), "iarray_opt_gemv": ([P, P, P, P, P], RC),
-            "iarray_b200_set_form": ([P, ctypes.c_int], RC), "iarray_b200_set_split_terms": ([P, ctypes.c_int], RC),
+            "iarray_b200_set_form": ([P, ctypes.c_int], RC), "iarray_b200_set_encoder": ([P, ctypes.c_int], RC), "iarray_b200_set_split_terms": ([P, ctypes.c_int], RC),
             "iarray_b200_last_timings": ([P, P], RC),
             "iarray_b200_from_chunks": ([P, P, P, I64, P, P, P], RC),
             "iarray_b200_get_chunk": ([P, P, I64, P, P], RC), "iarray_b200_nchunks": ([P, P], RC),
@@ -197,12 +198,17 @@ def storage(chunkshape, blockshape, urlpath=None, contiguous=True):
 
 
 class Context:
-    def __init__(self, cfg: Config | None = None, form: int = FORM_NATIVE, split_terms: int = 0):
+    def __init__(self, cfg: Config | None = None, form: int = FORM_NATIVE, split_terms: int = 0,
+                 encoder: int = ENCODER_LIBLZ4):
         init()
         self.cfg = cfg or Config.defaults()
         self.ptr = ctypes.c_void_p()
         check(_lib().iarray_context_new(ctypes.byref(self.cfg), ctypes.byref(self.ptr)), "iarray_context_new")
         self.set_form(form, split_terms)
+        self.set_encoder(encoder)
+
+    def set_encoder(self, encoder):
+        check(_lib().iarray_b200_set_encoder(self.ptr, encoder), "set_encoder")
 
     def set_form(self, form, split_terms=0):
         check(_lib().iarray_b200_set_form(self.ptr, form), "set_form")
