@@ -749,7 +749,7 @@ __device__ __forceinline__ int64_t probe_offset(int64_t t)
 // never wrap.  The window follows the parse position; reads outside it (far search
 // probes, old match candidates) go to global memory.  Without it the candidate reads of
 // low-entropy streams, spread over the last few KiB, mostly miss L1.
-constexpr int ERING = 8192, ESEG = 1024, ELOOK = 512;
+constexpr int ERING = 4096, ESEG = 1024, ELOOK = 512;
 
 struct EncSrc {
     const uint8_t *g;   // the stream in global memory
@@ -1079,7 +1079,7 @@ last_literals:
 // Streams are handed out dynamically (one atomic per stream): compressible streams cost
 // far more than incompressible ones, and in shuffled float data they recur at a fixed
 // stride, which a static round-robin assignment would pile onto the same warps.
-__global__ void __launch_bounds__(96, 3) k_lz4_encode(const uint8_t *__restrict__ img, int64_t nstreams_total,
+__global__ void __launch_bounds__(32, 10) k_lz4_encode(const uint8_t *__restrict__ img, int64_t nstreams_total,
                                                     int neblock, uint8_t *slots, EncStream *es,
                                                     unsigned long long *next)
 {
@@ -1344,8 +1344,34 @@ __device__ __forceinline__ int warp_lz4_compress_par(const uint8_t *__restrict__
     return op;
 }
 
-// E2 (parallel mode): one warp per stream, as k_lz4_encode.
-__global__ void __launch_bounds__(64, 3) k_lz4_encode_par(const uint8_t *__restrict__ img, int64_t nstreams_total,
+// Fraction of the first 1024 positions of a stream that have a 4-byte match (a table of
+// recent positions plus the previous position), in matches per 1024.
+__device__ __forceinline__ int par_probe(const uint8_t *__restrict__ src, int n, uint16_t *tab)
+{
+    const int lane = threadIdx.x & 31;
+    for (int i = lane; i < 8192; i += 32) tab[i] = 0xFFFF;
+    __syncwarp();
+    const int lim = min(n - 11, 1024);
+    int hits = 0;
+    for (int r = 0; r < 32; r++) {
+        const int p = r * 32 + lane;
+        const bool valid = p < lim;
+        const uint32_t v = valid ? ld4u(src + p) : 0u;
+        const uint32_t h = (v * 2654435761u) >> (32 - 13);
+        const uint32_t c = valid ? tab[h] : 0xFFFFu;
+        __syncwarp();
+        if (valid) tab[h] = (uint16_t)p;
+        const bool m = valid && ((c < (uint32_t)p && ld4u(src + c) == v) || (p > 0 && ld4u(src + p - 1) == v));
+        hits += __popc(__ballot_sync(FULLMASK, m));
+    }
+    __syncwarp();
+    return hits;
+}
+
+// E2 (parallel mode): one warp per stream, as k_lz4_encode.  Streams whose first 1024
+// positions have few matches (incompressible byte planes) go through the liblz4 search,
+// whose accelerating skip makes them cheap; the rest take the parallel parse.
+__global__ void __launch_bounds__(32, 7) k_lz4_encode_par(const uint8_t *__restrict__ img, int64_t nstreams_total,
                                                        int neblock, uint8_t *slots, EncStream *es,
                                                        unsigned long long *next)
 {
@@ -1373,9 +1399,19 @@ __global__ void __launch_bounds__(64, 3) k_lz4_encode_par(const uint8_t *__restr
         if (run) {
             e.kind = SK_RUN; e.csize = first; e.need = 0;
         } else {
-            const int cs = warp_lz4_compress_par(src, neblock, slots + sid * neblock, neblock, S);
-            if (cs > 0 && cs < neblock) { e.kind = SK_LZ4; e.csize = cs; e.need = cs; }
-            else { e.kind = SK_RAW; e.csize = neblock; e.need = neblock + 1; }
+            if (par_probe(src, neblock, S.tab) < 64) {
+                int need = 0;
+                uint32_t *t32 = reinterpret_cast<uint32_t *>(S.tab);
+                const int cs = neblock < 65536 + 12 - 1
+                                   ? warp_lz4_compress<true>(src, neblock, slots + sid * neblock, neblock, t32, S.ring, &need)
+                                   : warp_lz4_compress<false>(src, neblock, slots + sid * neblock, neblock, t32, S.ring, &need);
+                if (cs > 0 && cs < neblock) { e.kind = SK_LZ4; e.csize = cs; e.need = need; }
+                else { e.kind = SK_RAW; e.csize = neblock; e.need = need; }
+            } else {
+                const int cs = warp_lz4_compress_par(src, neblock, slots + sid * neblock, neblock, S);
+                if (cs > 0 && cs < neblock) { e.kind = SK_LZ4; e.csize = cs; e.need = cs; }
+                else { e.kind = SK_RAW; e.csize = neblock; e.need = neblock + 1; }
+            }
         }
         if (lane == 0) es[sid] = e;
         __syncwarp();
@@ -1657,26 +1693,26 @@ int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int s
     }
     if (w->exact_lz4) {
         static bool attr = false;
-        // per warp: 16 KiB hash table + the source window; 3 warps per CTA, 3 CTAs per SM
-        const int wpb = 3, smem = wpb * (4096 * 4 + ERING + 16);
+        // per warp: 16 KiB hash table + the source window; 1 warp per CTA, 10 CTAs per SM
+        const int wpb = 1, smem = wpb * (4096 * 4 + ERING + 16);
         if (!attr) {
             cudaFuncSetAttribute(k_lz4_encode, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             attr = true;
         }
         const int64_t ns = nbl * nstreams;
-        const int64_t blocks = std::min<int64_t>((ns + wpb - 1) / wpb, (int64_t)sms * 3);
+        const int64_t blocks = std::min<int64_t>((ns + wpb - 1) / wpb, (int64_t)sms * 10);
         IAB_TIMED("k_lz4_encode", st, k_lz4_encode<<<(unsigned)std::max<int64_t>(blocks, 1), wpb * 32, smem, st>>>(
             img.as<uint8_t>(), ns, neblock, slots.as<uint8_t>(), es.as<EncStream>(),
             reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1)));
     } else {
         static bool attr = false;
-        const int wpb = 2, smem = wpb * (int)sizeof(ParSmem);   // 2 warps per CTA, 3 CTAs per SM
+        const int wpb = 1, smem = wpb * (int)sizeof(ParSmem);   // 1 warp per CTA, 7 CTAs per SM
         if (!attr) {
             cudaFuncSetAttribute(k_lz4_encode_par, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             attr = true;
         }
         const int64_t ns = nbl * nstreams;
-        const int64_t blocks = std::min<int64_t>((ns + wpb - 1) / wpb, (int64_t)sms * 3);
+        const int64_t blocks = std::min<int64_t>((ns + wpb - 1) / wpb, (int64_t)sms * 7);
         IAB_TIMED("k_lz4_encode_par", st, k_lz4_encode_par<<<(unsigned)std::max<int64_t>(blocks, 1), wpb * 32, smem, st>>>(
             img.as<uint8_t>(), ns, neblock, slots.as<uint8_t>(), es.as<EncStream>(),
             reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1)));
