@@ -1190,10 +1190,19 @@ __device__ __forceinline__ void lz4_put_seq(const EncSrc &s, uint8_t *o, int anc
     }
 }
 
+// 4 bytes at stream position x from the window (x must be inside it).
+__device__ __forceinline__ uint32_t par_rd32(uint32_t ring_s, int x)
+{
+    const uint32_t o = (uint32_t)x & (ERING - 1);
+    const uint32_t wa = ring_s + (o & ~3u);
+    return __funnelshift_r(lds32(wa), lds32(wa + 4), (o & 3) * 8);
+}
+
 __device__ __forceinline__ int warp_lz4_compress_par(const uint8_t *__restrict__ src, int n,
                                                      uint8_t *__restrict__ dst, int cap, ParSmem &S)
 {
     const int lane = threadIdx.x & 31;
+    const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(S.ring);
     for (int i = lane; i < 8192; i += 32) S.tab[i] = 0;
     EncSrc s;
     s.g = src; s.r = S.ring; s.lo = 0; s.hi = 0; s.n = n;
@@ -1203,11 +1212,12 @@ __device__ __forceinline__ int warp_lz4_compress_par(const uint8_t *__restrict__
     for (int w0 = 0; n >= 13 && w0 < mfl1; w0 += PW) {
         const int wend = min(w0 + PW, mfl1), wn = wend - w0;
         es_fill(s, wend + PCAP + 32);
-        // ---- A: candidates and lengths
+        // ---- A: candidates and lengths.  Positions p .. p + PCAP + 4 lie in the window;
+        // a candidate is read from the window when it is still there, else from global memory.
         for (int r = 0; r < PW / 32; r++) {
             const int p = w0 + r * 32 + lane;
             const bool valid = p < wend;
-            const uint32_t v = valid ? es_rd32(s, p) : 0u;
+            const uint32_t v = valid ? par_rd32(ring_s, p) : 0u;
             const uint32_t h = (v * 2654435761u) >> (32 - 13);
             const uint32_t tv = valid ? (uint32_t)S.tab[h] : 0u;
             const int cand = p - (int)(((uint32_t)p - tv) & 0xFFFFu);
@@ -1219,10 +1229,12 @@ __device__ __forceinline__ int warp_lz4_compress_par(const uint8_t *__restrict__
 #pragma unroll
             for (int t = 0; t < 2; t++) {
                 const int c = t ? p - 1 : cand;
-                if (!valid || c >= p || c < 0 || (t && c == cand) || es_rd32(s, c) != v) continue;
+                if (!valid || c >= p || c < 0 || (t && c == cand)) continue;
+                const bool inring = c >= s.lo;
+                if ((inring ? par_rd32(ring_s, c) : ld4u(src + c)) != v) continue;
                 int l = 4;
                 while (l < lim) {
-                    const uint32_t x = es_rd32(s, p + l) ^ es_rd32(s, c + l);
+                    const uint32_t x = par_rd32(ring_s, p + l) ^ (inring ? par_rd32(ring_s, c + l) : ld4u(src + c + l));
                     if (x) { l += (__ffs((int)x) - 1) >> 3; break; }
                     l += 4;
                 }
@@ -1344,17 +1356,20 @@ __device__ __forceinline__ int warp_lz4_compress_par(const uint8_t *__restrict__
     return op;
 }
 
-// Fraction of the first 1024 positions of a stream that have a 4-byte match (a table of
-// recent positions plus the previous position), in matches per 1024.
+// Matches found in four sampled windows of 1024 positions (at 0, 1/4, 1/2 and 3/4 of the
+// stream): positions with a 4-byte match against a table of recent positions or against
+// the previous position.
 __device__ __forceinline__ int par_probe(const uint8_t *__restrict__ src, int n, uint16_t *tab)
 {
     const int lane = threadIdx.x & 31;
     for (int i = lane; i < 8192; i += 32) tab[i] = 0xFFFF;
     __syncwarp();
-    const int lim = min(n - 11, 1024);
     int hits = 0;
-    for (int r = 0; r < 32; r++) {
-        const int p = r * 32 + lane;
+    for (int w = 0; w < 4; w++) {
+      const int base = (int)(((int64_t)(n - 11) * w / 4) & ~31);
+      const int lim = min(n - 11, base + 1024);
+      for (int r = 0; r < 32; r++) {
+        const int p = base + r * 32 + lane;
         const bool valid = p < lim;
         const uint32_t v = valid ? ld4u(src + p) : 0u;
         const uint32_t h = (v * 2654435761u) >> (32 - 13);
@@ -1363,14 +1378,16 @@ __device__ __forceinline__ int par_probe(const uint8_t *__restrict__ src, int n,
         if (valid) tab[h] = (uint16_t)p;
         const bool m = valid && ((c < (uint32_t)p && ld4u(src + c) == v) || (p > 0 && ld4u(src + p - 1) == v));
         hits += __popc(__ballot_sync(FULLMASK, m));
+      }
     }
     __syncwarp();
     return hits;
 }
 
-// E2 (parallel mode): one warp per stream, as k_lz4_encode.  Streams whose first 1024
-// positions have few matches (incompressible byte planes) go through the liblz4 search,
-// whose accelerating skip makes them cheap; the rest take the parallel parse.
+// E2 (parallel mode): one warp per stream, as k_lz4_encode.  A probe of four sampled
+// windows routes each stream: almost no matches (incompressible byte planes): stored raw;
+// few matches: the liblz4 search, whose accelerating skip makes them cheap; the rest: the
+// parallel parse.
 __global__ void __launch_bounds__(32, 7) k_lz4_encode_par(const uint8_t *__restrict__ img, int64_t nstreams_total,
                                                        int neblock, uint8_t *slots, EncStream *es,
                                                        unsigned long long *next)
@@ -1399,7 +1416,10 @@ __global__ void __launch_bounds__(32, 7) k_lz4_encode_par(const uint8_t *__restr
         if (run) {
             e.kind = SK_RUN; e.csize = first; e.need = 0;
         } else {
-            if (par_probe(src, neblock, S.tab) < 64) {
+            const int hits = par_probe(src, neblock, S.tab);
+            if (hits < 16) {                     // no matches to speak of: store the stream raw
+                e.kind = SK_RAW; e.csize = neblock; e.need = neblock + 1;
+            } else if (hits < 256) {
                 int need = 0;
                 uint32_t *t32 = reinterpret_cast<uint32_t *>(S.tab);
                 const int cs = neblock < 65536 + 12 - 1
