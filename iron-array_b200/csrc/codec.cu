@@ -508,20 +508,24 @@ __device__ __forceinline__ uint32_t ld4_any(const uint8_t *p, const uint8_t *lim
 
 // D2 fast path: one CTA per interior, shuffled, split block; each thread rebuilds 4
 // consecutive items from one 4-byte word per byte plane (read in place from raw streams
-// or the LZ4 scratch) and writes them to the dense row.
+// or the LZ4 scratch) and writes them to the dense row.  Every other block is appended to
+// the list `rest` for the general path.
 template <int TS>
 __global__ void __launch_bounds__(256) k_scatter_fast(Geom g, const uint8_t *__restrict__ ch, const uint8_t *ch_end,
                                                       const BlockDesc *__restrict__ bd,
                                                       const StreamDesc *__restrict__ sd,
                                                       const uint8_t *__restrict__ scratch, const uint8_t *scratch_end,
-                                                      uint8_t *__restrict__ out, int64_t ld)
+                                                      uint8_t *__restrict__ out, int64_t ld, int *rest, int *nrest)
 {
     const int64_t nbl = g.nchunks * g.nblocks;
     const int qpr = (int)(g.block[1] / 4), nq = (int)(g.blockn / 4);
     for (int64_t t = blockIdx.x; t < nbl; t += gridDim.x) {
         const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
         const BlockDesc d = bd[t];
-        if (d.mode != BM_SHUFFLED || d.nstreams != TS || !block_fast(g, c, b)) continue;
+        if (d.mode != BM_SHUFFLED || d.nstreams != TS || !block_fast(g, c, b)) {
+            if (threadIdx.x == 0) rest[atomicAdd(nrest, 1)] = (int)t;   // left to k_scatter
+            continue;
+        }
         const uint8_t *base[TS];
         const uint8_t *lim[TS];
         uint32_t fill[TS];
@@ -573,21 +577,21 @@ __global__ void __launch_bounds__(256) k_scatter_fast(Geom g, const uint8_t *__r
 
 // D2 general path: unshuffle one tile of TILE items of one block through shared memory
 // and scatter it to the dense array (padded edge blocks, other item sizes, plain and
-// special chunks).  With skip_fast, blocks the fast path handles are skipped.
-__global__ void __launch_bounds__(256) k_scatter(Geom g, bool skip_fast, const uint8_t *__restrict__ ch,
+// special chunks).  With a `rest` list, only the blocks listed there; else every block.
+__global__ void __launch_bounds__(256) k_scatter(Geom g, const int *__restrict__ rest, const int *__restrict__ nrest,
+                                                 const uint8_t *__restrict__ ch,
                                                  const BlockDesc *__restrict__ bd, const StreamDesc *__restrict__ sd,
                                                  const uint8_t *__restrict__ scratch, uint8_t *__restrict__ out, int64_t ld)
 {
     __shared__ __align__(16) uint8_t planes[8 * TILE];
     const int ts = g.itemsize;
     const int64_t tpb = (g.blockn + TILE - 1) / TILE;
-    const int64_t nwork = g.nchunks * g.nblocks * tpb;
+    const int64_t nwork = (rest ? (int64_t)*nrest : g.nchunks * g.nblocks) * tpb;
     for (int64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
-        const int64_t t = w / tpb, i0 = (w - t * tpb) * TILE;
+        const int64_t k = w / tpb, t = rest ? rest[k] : k, i0 = (w - k * tpb) * TILE;
         const int cnt = (int)min((int64_t)TILE, g.blockn - i0);
         const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
         const BlockDesc d = bd[t];
-        if (skip_fast && d.mode == BM_SHUFFLED && d.nstreams == ts && block_fast(g, c, b)) continue;
         const StreamDesc *s = sd + t * 8;
         const uint8_t *blk_scratch = scratch + t * g.blocksize;
         if (d.mode == BM_SHUFFLED) {
@@ -1653,18 +1657,23 @@ int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, 
         const int64_t nwork = nbl * tpb;
         const int64_t blocks = std::min<int64_t>(nwork, (int64_t)sms * 8);
         const bool fast = g.itemsize == 4 || g.itemsize == 8;
+        int *rest = nullptr, *nrest = cnt + 3;
         if (fast) {
+            if (!w->rest.allocate(sizeof(int) * (size_t)nbl, dev)) return -100;
+            rest = w->rest.as<int>();
             const int64_t fb = std::min<int64_t>(nbl, (int64_t)sms * 8);
             const uint8_t *cend = d_chunks + chunks_bytes, *send = scratch.as<uint8_t>() + nbl * g.blocksize;
             if (g.itemsize == 8)
                 IAB_TIMED("k_scatter_fast", st, k_scatter_fast<8><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
-                    g, d_chunks, cend, bd.as<BlockDesc>(), sd.as<StreamDesc>(), scratch.as<uint8_t>(), send, (uint8_t *)out, ld));
+                    g, d_chunks, cend, bd.as<BlockDesc>(), sd.as<StreamDesc>(), scratch.as<uint8_t>(), send, (uint8_t *)out, ld,
+                    rest, nrest));
             else
                 IAB_TIMED("k_scatter_fast", st, k_scatter_fast<4><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
-                    g, d_chunks, cend, bd.as<BlockDesc>(), sd.as<StreamDesc>(), scratch.as<uint8_t>(), send, (uint8_t *)out, ld));
+                    g, d_chunks, cend, bd.as<BlockDesc>(), sd.as<StreamDesc>(), scratch.as<uint8_t>(), send, (uint8_t *)out, ld,
+                    rest, nrest));
         }
-        IAB_TIMED("k_scatter", st, k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, fast, d_chunks, bd.as<BlockDesc>(), sd.as<StreamDesc>(),
-                                                                        scratch.as<uint8_t>(), (uint8_t *)out, ld));
+        IAB_TIMED("k_scatter", st, k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
+            g, rest, nrest, d_chunks, bd.as<BlockDesc>(), sd.as<StreamDesc>(), scratch.as<uint8_t>(), (uint8_t *)out, ld));
     }
     return 0;
 }
@@ -1788,7 +1797,8 @@ constexpr size_t NA_LEN = na_align(NA_OFF + sizeof(int64_t) * NA_MAX_BLOCKS);
 constexpr size_t NA_BD = na_align(NA_LEN + sizeof(int32_t) * NA_MAX_BLOCKS);
 constexpr size_t NA_SD = na_align(NA_BD + sizeof(BlockDesc) * NA_MAX_BLOCKS);
 constexpr size_t NA_JOBS = na_align(NA_SD + sizeof(StreamDesc) * 8 * NA_MAX_BLOCKS);
-constexpr size_t NA_IMG = na_align(NA_JOBS + sizeof(Lz4Job) * 8 * NA_MAX_BLOCKS);
+constexpr size_t NA_REST = na_align(NA_JOBS + sizeof(Lz4Job) * 8 * NA_MAX_BLOCKS);
+constexpr size_t NA_IMG = na_align(NA_REST + sizeof(int) * NA_MAX_BLOCKS);
 constexpr size_t NA_TOTAL = NA_IMG + (size_t)NOALLOC_MAX_BYTES;
 
 static __device__ __align__(256) uint8_t g_noalloc_scratch[NA_TOTAL];
@@ -1866,17 +1876,19 @@ int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes,
         const int64_t tpb = (g.blockn + TILE - 1) / TILE;
         const int64_t blocks = std::min<int64_t>(nbl * tpb, (int64_t)sms * 8);
         const bool fast = g.itemsize == 4 || g.itemsize == 8;
+        int *rest = fast ? reinterpret_cast<int *>(base + NA_REST) : nullptr, *nrest = counters + 3;
         if (fast) {
             const int64_t fb = std::min<int64_t>(nbl, (int64_t)sms * 8);
             const uint8_t *cend = d_chunks + chunks_bytes, *send = img + nbl * g.blocksize;
             if (g.itemsize == 8)
                 IAB_TIMED("k_scatter_fast", st, k_scatter_fast<8><<<(unsigned)fb, 256, 0, st>>>(
-                    g, d_chunks, cend, bd, sd, img, send, (uint8_t *)out, ld));
+                    g, d_chunks, cend, bd, sd, img, send, (uint8_t *)out, ld, rest, nrest));
             else
                 IAB_TIMED("k_scatter_fast", st, k_scatter_fast<4><<<(unsigned)fb, 256, 0, st>>>(
-                    g, d_chunks, cend, bd, sd, img, send, (uint8_t *)out, ld));
+                    g, d_chunks, cend, bd, sd, img, send, (uint8_t *)out, ld, rest, nrest));
         }
-        IAB_TIMED("k_scatter", st, k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, fast, d_chunks, bd, sd, img, (uint8_t *)out, ld));
+        IAB_TIMED("k_scatter", st, k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
+            g, rest, nrest, d_chunks, bd, sd, img, (uint8_t *)out, ld));
     }
     int h_err = 0;
     if (cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return -101;

@@ -152,7 +152,7 @@ int decode_container(const Geom &g, const uint8_t *d_chunks, int64_t chunks_byte
 // Asynchronous form: decode_launch enqueues the kernels on `st` (work buffers held in
 // *w until decode_finish, which synchronises `st` and returns the DevErr).
 struct DecodeWork {
-    DevBuf bd, sd, jobs, scratch, counters;
+    DevBuf bd, sd, jobs, scratch, counters, rest;
     int *ext_counters = nullptr;   // optional caller-owned 16-int status slot (device) instead of `counters`
 };
 int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, const int64_t *d_off, const int32_t *d_len,

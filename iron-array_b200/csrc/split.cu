@@ -268,6 +268,19 @@ constexpr int SMEM = 1024 + STAGES * STAGE_BYTES + 256;
 constexpr uint32_t IDESC = tc::make_idesc(2 /*S32*/, 1 /*s8*/, 1 /*s8*/, BM, BN);
 }
 
+// Tile order of the persistent tensor-core kernels: tile rows are taken in groups of
+// TILE_GROUP; inside a group the walk is column by column, so the CTAs of one wave share a
+// few B column panels and the group's A row panels stay in L2 across the whole group.
+constexpr int TILE_GROUP = 32;
+__device__ __forceinline__ void tile_of(int local, int tiles_m, int tiles_n, int &tm, int &tn)
+{
+    const int per_group = TILE_GROUP * tiles_n;
+    const int g = local / per_group, rem = local - g * per_group;
+    const int rows = min(TILE_GROUP, tiles_m - g * TILE_GROUP);
+    tn = rem / rows;
+    tm = g * TILE_GROUP + (rem - tn * rows);
+}
+
 struct I8Params {
     int M, N, Kp, L, tiles_m, tiles_n;
     uint8_t *R;        // [L][M][ldr] residues of the products
@@ -320,7 +333,8 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
             bool ok = true;
             for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
                 const int l = t / (p.tiles_m * p.tiles_n), rem = t - l * p.tiles_m * p.tiles_n;
-                const int tm = rem / p.tiles_n, tn = rem - tm * p.tiles_n;
+                int tm, tn;
+                tile_of(rem, p.tiles_m, p.tiles_n, tm, tn);
                 for (int kt = 0; kt < ktiles; kt++) {
                     if (!tc::mbar_wait(&empty[stage], phase ^ 1, p.err)) { ok = false; break; }
                     tc::mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
@@ -370,7 +384,8 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
         uint32_t acc_phase = 0;
         for (int t = blockIdx.x; t < total; t += gridDim.x) {
             const int l = t / (p.tiles_m * p.tiles_n), rem = t - l * p.tiles_m * p.tiles_n;
-            const int tm = rem / p.tiles_n, tn = rem - tm * p.tiles_n;
+            int tm, tn;
+            tile_of(rem, p.tiles_m, p.tiles_n, tm, tn);
             if (!tc::mbar_wait(&tfull[acc], acc_phase, p.err)) break;
             tc::tc_fence_after();
             const int m = c_crt.mod[l];
@@ -743,7 +758,8 @@ __global__ void __launch_bounds__(b3::THREADS, 1) k_bf16x3_gemm(const __grid_con
             int64_t issued = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-                const int tm = t / p.tiles_n, tn = t - tm * p.tiles_n;
+                int tm, tn;
+                tile_of(t, p.tiles_m, p.tiles_n, tm, tn);
                 for (int pass = 0; pass < 3 && ok; pass++) {
                     const int pa = kAPlane[pass], pb = kBPlane[pass];
                     for (int kt = 0; kt < ktiles; kt++) {
@@ -792,7 +808,8 @@ __global__ void __launch_bounds__(b3::THREADS, 1) k_bf16x3_gemm(const __grid_con
         int acc = 0;
         uint32_t acc_phase = 0;
         for (int t = blockIdx.x; t < total; t += gridDim.x) {
-            const int tm = t / p.tiles_n, tn = t - tm * p.tiles_n;
+            int tm, tn;
+            tile_of(t, p.tiles_m, p.tiles_n, tm, tn);
             if (!tc::mbar_wait(&tfull[acc], acc_phase, p.err)) break;
             tc::tc_fence_after();
             const int row = tm * BM + q * 32 + lane;
