@@ -145,7 +145,7 @@ constexpr int THREADS = 256;
 constexpr int DW = 2048;                   // compressed bytes per window
 constexpr int MAXS = DW / 3 + 2;           // sequences per window (a non-final one takes >= 3 bytes)
 constexpr int PATH = 1024;                 // >= 2 * the largest power of two below MAXS + 1
-constexpr int DCAP = 8192;                 // output bytes resolved in shared memory at once
+constexpr int DCAP = 4096;                 // output bytes resolved in shared memory at once
 constexpr uint16_t STOP = 0xFFFF, ENDS = 0xFFFE;
 constexpr uint32_t RES = 0x80000000u;      // resolved output byte (value in the low 8 bits)
 struct Smem {
@@ -193,7 +193,7 @@ __device__ __forceinline__ uint16_t dcta_next(const uint8_t *win, int q, int n, 
     return (uint16_t)r;                   // r <= n; r == n: the next token starts the next window
 }
 
-__global__ void __launch_bounds__(dcta::THREADS, 4) k_lz4_decode_cta(const uint8_t *__restrict__ ch,
+__global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const uint8_t *__restrict__ ch,
                                                                   const Lz4Job *__restrict__ jobs,
                                                                   const int *__restrict__ njobs_p, uint8_t *scratch,
                                                                   int *err, unsigned *next_job)
@@ -1648,7 +1648,7 @@ int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, 
             cudaFuncSetAttribute(k_lz4_decode_cta, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             attr = true;
         }
-        IAB_TIMED("k_lz4_decode_cta", st, k_lz4_decode_cta<<<sms * 4, dcta::THREADS, smem, st>>>(
+        IAB_TIMED("k_lz4_decode_cta", st, k_lz4_decode_cta<<<sms * 5, dcta::THREADS, smem, st>>>(
             d_chunks, jobs.as<Lz4Job>(), njobs, scratch.as<uint8_t>(), err,
             reinterpret_cast<unsigned *>(cnt + 2)));
     }
@@ -1869,7 +1869,7 @@ int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes,
         IAB_TIMED("k_parse", st, k_parse<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, st>>>(g, d_chunks, off, len, bd, sd, jobs, njobs, err));
     }
     {
-        IAB_TIMED("k_lz4_decode_cta", st, k_lz4_decode_cta<<<sms * 4, dcta::THREADS, (int)sizeof(dcta::Smem), st>>>(
+        IAB_TIMED("k_lz4_decode_cta", st, k_lz4_decode_cta<<<sms * 5, dcta::THREADS, (int)sizeof(dcta::Smem), st>>>(
             d_chunks, jobs, njobs, img, err, reinterpret_cast<unsigned *>(counters + 2)));
     }
     {
