@@ -12,9 +12,11 @@
 //      K-major, for the tensor-core operand layout).
 //   3. INT8 GEMM per modulus on tcgen05 (kind::i8, INT32 accumulate in TMEM, exact since
 //      K * 128 * 128 < 2^31), fused epilogue reducing every entry modulo m_l to a byte.
-//   4. Reconstruction.  C'_ij = sum_l r_l w_l mod P (w_l the CRT basis, 128-bit integer
-//      arithmetic), centred, converted to float64 and scaled back by 2^-(sA_i + sB_j).
-// FP64 is used only for the scaling, the residue arithmetic and the final conversion.
+//   4. Reconstruction.  C'_ij = sum_l r_l w_l mod P (w_l the CRT basis, held in 40-bit
+//      chunks so that the sums are exact in FP64), centred, rounded to float64 and scaled
+//      back by 2^-(sA_i + sB_j).
+// FP64 (non-tensor) arithmetic is used for the scaling, the residues and the
+// reconstruction; every step before the final rounding is exact.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -70,13 +72,13 @@ static const int kModuli[MAX_MODULI] = {256, 255, 253, 251, 247, 241, 239, 233, 
 
 struct CrtConst {
     int L;
+    int nc;                                        // 40-bit chunks needed for P (1..4)
     int mod[MAX_MODULI];
     double inv_mod[MAX_MODULI];
     float inv_modf[MAX_MODULI];
-    uint64_t w_lo[MAX_MODULI], w_hi[MAX_MODULI];   // CRT basis w_l = (P/m_l) * ((P/m_l)^-1 mod m_l) mod P
-    uint32_t w32[MAX_MODULI][4];                   // the same, as 32-bit limbs (least significant first)
-    uint32_t p32[4], h32[4];                       // P and floor(P/2) as 32-bit limbs
-    uint64_t p_lo, p_hi, h_lo, h_hi;               // P and floor(P/2)
+    double wf[MAX_MODULI][4];                      // CRT basis w_l = (P/m_l) * ((P/m_l)^-1 mod m_l) mod P,
+                                                   // 40-bit chunks (least significant first) as exact doubles
+    double pf[4];                                  // P in 40-bit chunks
     double inv_p;                                  // 1/P (rounded)
     double log2p;
 };
@@ -85,12 +87,16 @@ __constant__ CrtConst c_crt;
 
 static bool build_crt(int L, CrtConst *c)
 {
-    if (L < 2 || L > 16) return false;   // P < 2^126 keeps the reconstruction in two limbs + sign
+    if (L < 2 || L > 16) return false;   // P < 2^126: at most four 40-bit chunks
     typedef unsigned __int128 u128;
+    const u128 mask40 = ((u128)1 << 40) - 1;
     u128 P = 1;
     for (int l = 0; l < L; l++) P *= (u128)kModuli[l];
     memset(c, 0, sizeof(*c));
     c->L = L;
+    int bits = 0;
+    for (u128 t = P; t; t >>= 1) bits++;
+    c->nc = (bits + 39) / 40;
     double lp = 0;
     for (int l = 0; l < L; l++) {
         const int m = kModuli[l];
@@ -105,20 +111,10 @@ static bool build_crt(int L, CrtConst *c)
             if ((a * x) % m == 1) { inv = x; break; }
         if (!inv) return false;
         const u128 w = (Ml * (u128)inv) % P;
-        c->w_lo[l] = (uint64_t)w;
-        c->w_hi[l] = (uint64_t)(w >> 64);
-        for (int k = 0; k < 4; k++) c->w32[l][k] = (uint32_t)(w >> (32 * k));
+        for (int k = 0; k < 4; k++) c->wf[l][k] = (double)(uint64_t)((w >> (40 * k)) & mask40);
     }
-    c->p_lo = (uint64_t)P;
-    c->p_hi = (uint64_t)(P >> 64);
-    const u128 H = P / 2;
-    c->h_lo = (uint64_t)H;
-    c->h_hi = (uint64_t)(H >> 64);
-    for (int k = 0; k < 4; k++) {
-        c->p32[k] = (uint32_t)(P >> (32 * k));
-        c->h32[k] = (uint32_t)(H >> (32 * k));
-    }
-    c->inv_p = 1.0 / ((double)c->p_hi * 18446744073709551616.0 + (double)c->p_lo);
+    for (int k = 0; k < 4; k++) c->pf[k] = (double)(uint64_t)((P >> (40 * k)) & mask40);
+    c->inv_p = 1.0 / ((double)(uint64_t)(P >> 64) * 18446744073709551616.0 + (double)(uint64_t)P);
     c->log2p = lp;
     return true;
 }
@@ -188,11 +184,36 @@ __global__ void k_col_shift(int N, const double *__restrict__ pmax, const double
 }
 
 // ============================================================================ residues
+// Rounding by the 1.5 * 2^52 constant: for |y| < 2^51, (y + kRound) is the double of ulp 1
+// nearest to y + kRound, so (y + kRound) - kRound = rint(y), and the low 32 bits of
+// y + kRound hold rint(y) in two's complement.  This keeps the per-modulus work on the
+// FP64 pipe (no float/int conversions).
+constexpr double kRound = 6755399441055744.0;
+constexpr double kTwo52 = 4503599627370496.0;
+constexpr double kTwo40 = 1099511627776.0;
+
+// 2^s for -1022 <= s <= 1023.
+__device__ __forceinline__ double pow2i(int s) { return __hiloint2double((1023 + s) << 20, 0); }
+
+// rint(y) for |y| < 2^52 (ties to even, like rint).
+__device__ __forceinline__ double rint52(double y)
+{
+    const double c = copysign(kTwo52, y);
+    return (y + c) - c;
+}
+
+// rint(a * 2^s): the scaled, rounded entry of an operand row or column.
+__device__ __forceinline__ double scaled_int(double a, int s, bool pow2_ok, double f)
+{
+    return pow2_ok ? rint52(a * f) : rint(ldexp(a, s));
+}
+
+// Symmetric residue of the integer-valued x (|x| < 2^52) modulo m_l.
 __device__ __forceinline__ int sym_residue(double x, int l)
 {
     const int m = c_crt.mod[l];
-    const double q = rint(x * c_crt.inv_mod[l]);
-    int r = (int)fma(-q, (double)m, x);            // exact: small integer
+    const double q = fma(x, c_crt.inv_mod[l], kRound) - kRound;    // rint(x / m), or one off
+    int r = __double2loint(fma(-q, (double)m, x) + kRound);         // x - q m, exact, |.| < 1.5 m
     const int hi = (m == 256) ? 127 : (m - 1) / 2;
     const int lo = (m == 256) ? -128 : -(m - 1) / 2;
     if (r > hi) r -= m;
@@ -210,19 +231,24 @@ __global__ void __launch_bounds__(256) k_residues_rows(int M, int K, int Kp, con
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(t / groups), k0 = (int)(t - (int64_t)i * groups) * 8;
         const int s = shift[i];
+        const bool p2 = s >= -1022 && s <= 1023;
+        const double f = p2 ? pow2i(s) : 0.0;
         double x[8];
 #pragma unroll
         for (int u = 0; u < 8; u++) {
             const int k = k0 + u;
-            x[u] = k < K ? rint(ldexp(A[(int64_t)i * lda + k], s)) : 0.0;
+            x[u] = k < K ? scaled_int(A[(int64_t)i * lda + k], s, p2, f) : 0.0;
         }
-        for (int l = 0; l < L; l++) {
-            uint32_t w0 = 0, w1 = 0;
 #pragma unroll
-            for (int u = 0; u < 4; u++) w0 |= (uint32_t)(uint8_t)sym_residue(x[u], l) << (8 * u);
+        for (int l = 0; l < 16; l++) {
+            if (l < L) {
+                uint32_t w0 = 0, w1 = 0;
 #pragma unroll
-            for (int u = 0; u < 4; u++) w1 |= (uint32_t)(uint8_t)sym_residue(x[4 + u], l) << (8 * u);
-            *reinterpret_cast<uint2 *>(res + ((int64_t)l * M + i) * Kp + k0) = make_uint2(w0, w1);
+                for (int u = 0; u < 4; u++) w0 |= (uint32_t)(uint8_t)sym_residue(x[u], l) << (8 * u);
+#pragma unroll
+                for (int u = 0; u < 4; u++) w1 |= (uint32_t)(uint8_t)sym_residue(x[4 + u], l) << (8 * u);
+                *reinterpret_cast<uint2 *>(res + ((int64_t)l * M + i) * Kp + k0) = make_uint2(w0, w1);
+            }
         }
     }
 }
@@ -245,16 +271,21 @@ __global__ void __launch_bounds__(256) k_residues_cols(int K, int N, int Kp, con
         const int j = j0 + c;
         if (j >= N || k0 + kg >= Kp) continue;
         const int s = shift[j];
+        const bool p2 = s >= -1022 && s <= 1023;
+        const double f = p2 ? pow2i(s) : 0.0;
         double x[8];
 #pragma unroll
-        for (int u = 0; u < 8; u++) x[u] = rint(ldexp(tile[kg + u][c], s));
-        for (int l = 0; l < L; l++) {
-            uint32_t w0 = 0, w1 = 0;
+        for (int u = 0; u < 8; u++) x[u] = scaled_int(tile[kg + u][c], s, p2, f);
 #pragma unroll
-            for (int u = 0; u < 4; u++) w0 |= (uint32_t)(uint8_t)sym_residue(x[u], l) << (8 * u);
+        for (int l = 0; l < 16; l++) {
+            if (l < L) {
+                uint32_t w0 = 0, w1 = 0;
 #pragma unroll
-            for (int u = 0; u < 4; u++) w1 |= (uint32_t)(uint8_t)sym_residue(x[4 + u], l) << (8 * u);
-            *reinterpret_cast<uint2 *>(res + ((int64_t)l * N + j) * Kp + k0 + kg) = make_uint2(w0, w1);
+                for (int u = 0; u < 4; u++) w0 |= (uint32_t)(uint8_t)sym_residue(x[u], l) << (8 * u);
+#pragma unroll
+                for (int u = 0; u < 4; u++) w1 |= (uint32_t)(uint8_t)sym_residue(x[4 + u], l) << (8 * u);
+                *reinterpret_cast<uint2 *>(res + ((int64_t)l * N + j) * Kp + k0 + kg) = make_uint2(w0, w1);
+            }
         }
     }
 }
@@ -436,89 +467,36 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
 }
 
 // ============================================================================ reconstruction
-// X = sum_l r_l w_l mod P, centred into (-P/2, P/2], as a float64 (32-bit limbs: every
-// r_l * limb product is one 32x32->64 multiply-add; L * 2^8 * 2^32 < 2^45 per limb).
-__device__ __forceinline__ double crt_value(const uint32_t (&w)[16], int u, int L)
+// X = sum_l r_l w_l mod P, centred into (-P/2, P/2), in exact FP64 arithmetic.  Each w_l is
+// held as NC chunks of 40 bits, so with r_l < 2^8 and L <= 16 every partial sum
+// S_k = sum_l r_l w_lk stays below 2^52 and is exact.  The quotient q = rint(S / P) < 2^12
+// comes from a rounded estimate of S: the scaling keeps |X| below P / 8 (both norms are
+// held to 2^(gamma - 1)), so S / P stays far from a half-integer compared with the
+// estimate's error (about 2^-39 of one unit), and q is exact.  Then every
+// D_k = S_k - q P_k is exact (q P_k < 2^52) and X = sum_k D_k 2^(40 k) is formed by Horner
+// steps whose intermediates are exact or within a factor 1.5 of |X|: error at most about
+// 1.5 ulp of X.
+template <int NC>
+__device__ __forceinline__ double crt_value(const double (&S)[NC])
 {
-    uint64_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    double s = S[NC - 1];
 #pragma unroll
-    for (int l = 0; l < 16; l++) {
-        if (l < L) {
-            const uint64_t v = (w[l] >> (8 * u)) & 0xffu;
-            a0 += v * c_crt.w32[l][0];
-            a1 += v * c_crt.w32[l][1];
-            a2 += v * c_crt.w32[l][2];
-            a3 += v * c_crt.w32[l][3];
-        }
-    }
-    // S in five 32-bit limbs
-    uint32_t s0 = (uint32_t)a0;
-    a1 += a0 >> 32;
-    uint32_t s1 = (uint32_t)a1;
-    a2 += a1 >> 32;
-    uint32_t s2 = (uint32_t)a2;
-    a3 += a2 >> 32;
-    uint32_t s3 = (uint32_t)a3;
-    uint32_t s4 = (uint32_t)(a3 >> 32);
-    // quotient estimate (within one of floor(S / P)), then X = S - qP with a signed carry
-    const double sd = ((((double)s4 * 4294967296.0 + (double)s3) * 4294967296.0 + (double)s2) * 4294967296.0 +
-                       (double)s1) * 4294967296.0 + (double)s0;
-    const uint32_t q = (uint32_t)(sd * c_crt.inv_p);
-    int64_t x[5];
-    int64_t carry = 0;
-    const uint32_t sv[4] = {s0, s1, s2, s3};
+    for (int k = NC - 2; k >= 0; k--) s = fma(s, kTwo40, S[k]);
+    const double q = fma(s, c_crt.inv_p, kRound) - kRound;
+    double x = fma(-q, c_crt.pf[NC - 1], S[NC - 1]);
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const uint64_t m = (uint64_t)q * c_crt.p32[k];
-        const int64_t d = (int64_t)sv[k] + carry - (int64_t)(m & 0xffffffffu);
-        x[k] = d & 0xffffffff;
-        carry = (d >> 32) - (int64_t)(m >> 32);
-    }
-    x[4] = (int64_t)s4 + carry;                  // sign of X lives here
-    // one correction either way, then centre
-    auto add_p = [&](int sgn) {
-        int64_t c = 0;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const int64_t d = x[k] + sgn * (int64_t)c_crt.p32[k] + c;
-            x[k] = d & 0xffffffff;
-            c = d >> 32;
-        }
-        x[4] += c;
-    };
-    auto ge = [&](const uint32_t (&v)[4]) -> bool {   // X >= v (X non-negative, v < 2^128)
-        if (x[4] > 0) return true;
-        for (int k = 3; k >= 0; k--) {
-            if ((uint64_t)x[k] != v[k]) return (uint64_t)x[k] > v[k];
-        }
-        return true;
-    };
-    if (x[4] < 0) add_p(1);
-    else if (ge(c_crt.p32)) add_p(-1);
-    bool neg = false;
-    if (!ge(c_crt.h32)) {
-        // X <= P/2 - 1 ... keep
-    } else {
-        bool eq = x[4] == 0;
-        for (int k = 0; k < 4 && eq; k++) eq = (uint64_t)x[k] == c_crt.h32[k];
-        if (!eq) {       // X > floor(P/2): use X - P < 0, magnitude P - X
-            int64_t c = 0;
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const int64_t d = (int64_t)c_crt.p32[k] - x[k] + c;
-                x[k] = d & 0xffffffff;
-                c = d >> 32;
-            }
-            x[4] = 0;
-            neg = true;
-        }
-    }
-    const double v = (((double)x[3] * 4294967296.0 + (double)x[2]) * 4294967296.0 + (double)x[1]) * 4294967296.0 +
-                     (double)x[0];
-    return neg ? -v : v;
+    for (int k = NC - 2; k >= 0; k--) x = fma(x, kTwo40, fma(-q, c_crt.pf[k], S[k]));
+    return x;
+}
+
+// x * 2^-e, exact scaling (one rounding when the result is subnormal).
+__device__ __forceinline__ double unscale(double x, int e)
+{
+    return (e >= -1023 && e <= 1022) ? x * pow2i(-e) : ldexp(x, -e);
 }
 
 // C_ij = 2^-(sA_i + sB_j) * centred( sum_l r_l w_l mod P ); four entries per thread.
+template <int NC>
 __global__ void __launch_bounds__(256) k_crt(int M, int N, const uint8_t *__restrict__ R, int64_t ldr,
                                              const int *__restrict__ sA, const int *__restrict__ sB,
                                              double *__restrict__ C, int64_t ldc)
@@ -533,12 +511,47 @@ __global__ void __launch_bounds__(256) k_crt(int M, int N, const uint8_t *__rest
         uint32_t w[16];
 #pragma unroll
         for (int l = 0; l < 16; l++) w[l] = l < L ? *reinterpret_cast<const uint32_t *>(rp + l * plane) : 0u;  // ldr % 16 == 0
-        const int si = sA[i];
+        double S[4][NC];
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int j = j0 + u;
-            if (j < N) C[(int64_t)i * ldc + j] = ldexp(crt_value(w, u, L), -(si + sB[j]));
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int k = 0; k < NC; k++) S[u][k] = 0.0;
+#pragma unroll
+        for (int l = 0; l < 16; l++) {
+            if (l < L) {
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    // the residue byte as a double: 2^52 + r, less 2^52
+                    const double r = __hiloint2double(0x43300000, (int)((w[l] >> (8 * u)) & 0xffu)) - kTwo52;
+#pragma unroll
+                    for (int k = 0; k < NC; k++) S[u][k] = fma(r, c_crt.wf[l][k], S[u][k]);
+                }
+            }
         }
+        const int si = sA[i];
+        double v[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) v[u] = j0 + u < N ? unscale(crt_value<NC>(S[u]), si + sB[j0 + u]) : 0.0;
+        double *cp = C + (int64_t)i * ldc + j0;
+        if (j0 + 3 < N && (reinterpret_cast<uintptr_t>(cp) & 15) == 0) {
+            reinterpret_cast<double2 *>(cp)[0] = make_double2(v[0], v[1]);
+            reinterpret_cast<double2 *>(cp)[1] = make_double2(v[2], v[3]);
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (j0 + u < N) cp[u] = v[u];
+        }
+    }
+}
+
+static void launch_crt(int nc, unsigned grid, int M, int N, const uint8_t *R, int64_t ldr, const int *sA,
+                       const int *sB, double *C, int64_t ldc, cudaStream_t st)
+{
+    switch (nc) {
+    case 1: IAB_TIMED("k_crt", st, k_crt<1><<<grid, 256, 0, st>>>(M, N, R, ldr, sA, sB, C, ldc)); break;
+    case 2: IAB_TIMED("k_crt", st, k_crt<2><<<grid, 256, 0, st>>>(M, N, R, ldr, sA, sB, C, ldc)); break;
+    case 3: IAB_TIMED("k_crt", st, k_crt<3><<<grid, 256, 0, st>>>(M, N, R, ldr, sA, sB, C, ldc)); break;
+    default: IAB_TIMED("k_crt", st, k_crt<4><<<grid, 256, 0, st>>>(M, N, R, ldr, sA, sB, C, ldc)); break;
     }
 }
 
@@ -637,7 +650,7 @@ int gemm_f64_ozaki_launch(int64_t M, int64_t N, int64_t K, const double *A, int6
     }
     const int tiles = L * prm.tiles_m * prm.tiles_n;
     IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
-    IAB_TIMED("k_crt", st, k_crt<<<(unsigned)(nsm * 8), 256, 0, st>>>((int)M, (int)N, rr.as<uint8_t>(), ldr, sa.as<int>(), sb.as<int>(), C, ldc));
+    launch_crt(cached.nc, (unsigned)(nsm * 8), (int)M, (int)N, rr.as<uint8_t>(), ldr, sa.as<int>(), sb.as<int>(), C, ldc, st);
     return 0;
 }
 
