@@ -120,18 +120,26 @@ static bool build_crt(int L, CrtConst *c)
 }
 
 // ============================================================================ scaling
+// Shift value of a row / column that holds a NaN or an infinity: its residues are zero and
+// its outputs are recomputed by k_nonfinite_fix.
+constexpr int kNonFinite = -0x7fffffff - 1;
+
 // Shift for one row / column: the largest s with max|x| * 2^s < 2^52 and
-// ||x||_2 * 2^s <= 2^(gamma - 1).
-__device__ __forceinline__ int pick_shift(double amax, double sumsq, double gamma)
+// ||x||_2 * 2^s <= 2^(gamma - 1); lg2nrm = log2 ||x||_2.
+__device__ __forceinline__ int pick_shift(double amax, double lg2nrm, double gamma)
 {
     if (!(amax > 0.0)) return 0;
     int e;
     frexp(amax, &e);                      // amax < 2^e
     const int s1 = 52 - e;
-    const double nrm = sqrt(sumsq);
-    const int s2 = (int)floor(gamma - log2(nrm)) - 1;
+    const int s2 = (int)floor(gamma - lg2nrm) - 1;
     return min(s1, s2);
 }
+
+// Largest magnitude for which the plain sum of squares of up to 65536 entries neither
+// overflows nor loses the largest square to underflow (2^-480 .. 2^480); outside it the
+// norm is taken again from the entries scaled by 2^-e.
+__device__ __forceinline__ bool norm_needs_rescale(double amax) { return amax > 0x1p480 || amax < 0x1p-480; }
 
 __global__ void __launch_bounds__(256) k_row_shift(int M, int K, const double *__restrict__ A, int64_t lda, double gamma,
                                                    int *__restrict__ shift)
@@ -149,7 +157,24 @@ __global__ void __launch_bounds__(256) k_row_shift(int M, int K, const double *_
         mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
         ss += __shfl_xor_sync(0xffffffffu, ss, o);
     }
-    if (lane == 0) shift[warp] = pick_shift(mx, ss, gamma);
+    // a NaN reaches ss (fmax drops it), an infinity reaches mx
+    if (isnan(ss) || isinf(mx)) {
+        if (lane == 0) shift[warp] = kNonFinite;
+        return;
+    }
+    double lg = 0.5 * log2(ss);
+    if (mx > 0.0 && norm_needs_rescale(mx)) {
+        int e;
+        frexp(mx, &e);
+        double s2 = 0.0;
+        for (int k = lane; k < K; k += 32) {
+            const double v = ldexp(fabs(row[k]), -e);
+            s2 = fma(v, v, s2);
+        }
+        for (int o = 16; o; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        lg = 0.5 * log2(s2) + e;
+    }
+    if (lane == 0) shift[warp] = pick_shift(mx, lg, gamma);
 }
 
 constexpr int COL_SEGS = 64;
@@ -170,8 +195,8 @@ __global__ void __launch_bounds__(256) k_col_partial(int K, int N, const double 
     pss[(int64_t)seg * N + j] = ss;
 }
 
-__global__ void k_col_shift(int N, const double *__restrict__ pmax, const double *__restrict__ pss, double gamma,
-                            int *__restrict__ shift)
+__global__ void k_col_shift(int K, int N, const double *__restrict__ B, int64_t ldb, const double *__restrict__ pmax,
+                            const double *__restrict__ pss, double gamma, int *__restrict__ shift)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= N) return;
@@ -180,7 +205,62 @@ __global__ void k_col_shift(int N, const double *__restrict__ pmax, const double
         mx = fmax(mx, pmax[(int64_t)s * N + j]);
         ss += pss[(int64_t)s * N + j];
     }
-    shift[j] = pick_shift(mx, ss, gamma);
+    if (isnan(ss) || isinf(mx)) {
+        shift[j] = kNonFinite;
+        return;
+    }
+    double lg = 0.5 * log2(ss);
+    if (mx > 0.0 && norm_needs_rescale(mx)) {
+        int e;
+        frexp(mx, &e);
+        double s2 = 0.0;
+        for (int k = 0; k < K; k++) {
+            const double v = ldexp(fabs(B[(int64_t)k * ldb + j]), -e);
+            s2 = fma(v, v, s2);
+        }
+        lg = 0.5 * log2(s2) + e;
+    }
+    shift[j] = pick_shift(mx, lg, gamma);
+}
+
+// Outputs whose row of A or column of B holds a NaN or an infinity are recomputed as plain
+// dot products (one FMA per k, in order), so they carry the native product's IEEE
+// propagation.  One warp per row (warp index < M, flag rflag[i] == flagval) or column
+// (warp index - M); warps of rows and columns without such values return at once.
+template <typename T>
+__global__ void __launch_bounds__(256) k_nonfinite_fix(int M, int N, int K, const T *__restrict__ A, int64_t lda,
+                                                      const T *__restrict__ B, int64_t ldb, T *__restrict__ C,
+                                                      int64_t ldc, const int *__restrict__ rflag,
+                                                      const int *__restrict__ cflag, int flagval)
+{
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w < M) {
+        const int i = (int)w;
+        if (rflag[i] != flagval) return;
+        for (int j = lane; j < N; j += 32) {
+            T acc = 0;
+            for (int k = 0; k < K; k++) acc = fma(A[(int64_t)i * lda + k], B[(int64_t)k * ldb + j], acc);
+            C[(int64_t)i * ldc + j] = acc;
+        }
+    } else if (w < (int64_t)M + N) {
+        const int j = (int)(w - M);
+        if (cflag[j] != flagval) return;
+        for (int i = lane; i < M; i += 32) {
+            T acc = 0;
+            for (int k = 0; k < K; k++) acc = fma(A[(int64_t)i * lda + k], B[(int64_t)k * ldb + j], acc);
+            C[(int64_t)i * ldc + j] = acc;
+        }
+    }
+}
+
+template <typename T>
+static void launch_nonfinite_fix(int64_t M, int64_t N, int64_t K, const T *A, int64_t lda, const T *B, int64_t ldb,
+                                 T *C, int64_t ldc, const int *rflag, const int *cflag, int flagval, cudaStream_t st)
+{
+    const int64_t threads = (M + N) * 32;
+    IAB_TIMED("k_nonfinite_fix", st, k_nonfinite_fix<T><<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
+        (int)M, (int)N, (int)K, A, lda, B, ldb, C, ldc, rflag, cflag, flagval));
 }
 
 // ============================================================================ residues
@@ -231,13 +311,13 @@ __global__ void __launch_bounds__(256) k_residues_rows(int M, int K, int Kp, con
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(t / groups), k0 = (int)(t - (int64_t)i * groups) * 8;
         const int s = shift[i];
-        const bool p2 = s >= -1022 && s <= 1023;
+        const bool p2 = s >= -1022 && s <= 1023, fin = s != kNonFinite;
         const double f = p2 ? pow2i(s) : 0.0;
         double x[8];
 #pragma unroll
         for (int u = 0; u < 8; u++) {
             const int k = k0 + u;
-            x[u] = k < K ? scaled_int(A[(int64_t)i * lda + k], s, p2, f) : 0.0;
+            x[u] = k < K && fin ? scaled_int(A[(int64_t)i * lda + k], s, p2, f) : 0.0;
         }
 #pragma unroll
         for (int l = 0; l < 16; l++) {
@@ -271,11 +351,11 @@ __global__ void __launch_bounds__(256) k_residues_cols(int K, int N, int Kp, con
         const int j = j0 + c;
         if (j >= N || k0 + kg >= Kp) continue;
         const int s = shift[j];
-        const bool p2 = s >= -1022 && s <= 1023;
+        const bool p2 = s >= -1022 && s <= 1023, fin = s != kNonFinite;
         const double f = p2 ? pow2i(s) : 0.0;
         double x[8];
 #pragma unroll
-        for (int u = 0; u < 8; u++) x[u] = scaled_int(tile[kg + u][c], s, p2, f);
+        for (int u = 0; u < 8; u++) x[u] = fin ? scaled_int(tile[kg + u][c], s, p2, f) : 0.0;
 #pragma unroll
         for (int l = 0; l < 16; l++) {
             if (l < L) {
@@ -530,8 +610,17 @@ __global__ void __launch_bounds__(256) k_crt(int M, int N, const uint8_t *__rest
         }
         const int si = sA[i];
         double v[4];
+        bool ok[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++) v[u] = j0 + u < N ? unscale(crt_value<NC>(S[u]), si + sB[j0 + u]) : 0.0;
+        for (int u = 0; u < 4; u++) {
+            const int sj = j0 + u < N ? sB[j0 + u] : kNonFinite;
+            // rows / columns with NaN or infinity are recomputed by k_nonfinite_fix
+            ok[u] = si != kNonFinite && sj != kNonFinite;
+            v[u] = crt_value<NC>(S[u]);
+            v[u] = unscale(v[u], ok[u] ? si + sj : 0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) v[u] = ok[u] ? v[u] : 0.0;
         double *cp = C + (int64_t)i * ldc + j0;
         if (j0 + 3 < N && (reinterpret_cast<uintptr_t>(cp) & 15) == 0) {
             reinterpret_cast<double2 *>(cp)[0] = make_double2(v[0], v[1]);
@@ -628,7 +717,7 @@ int gemm_f64_ozaki_launch(int64_t M, int64_t N, int64_t K, const double *A, int6
     IAB_TIMED("k_row_shift", st, k_row_shift<<<(unsigned)((M * 32 + 255) / 256), 256, 0, st>>>((int)M, (int)K, A, lda, gamma, sa.as<int>()));
     IAB_TIMED("k_col_partial", st, k_col_partial<<<dim3((unsigned)((N + 255) / 256), COL_SEGS), 256, 0, st>>>((int)K, (int)N, B, ldb, pm.as<double>(),
                                                                                ps.as<double>()));
-    IAB_TIMED("k_col_shift", st, k_col_shift<<<(unsigned)((N + 255) / 256), 256, 0, st>>>((int)N, pm.as<double>(), ps.as<double>(), gamma, sb.as<int>()));
+    IAB_TIMED("k_col_shift", st, k_col_shift<<<(unsigned)((N + 255) / 256), 256, 0, st>>>((int)K, (int)N, B, ldb, pm.as<double>(), ps.as<double>(), gamma, sb.as<int>()));
     IAB_TIMED("k_residues_rows", st, k_residues_rows<<<(unsigned)(nsm * 16), 256, 0, st>>>((int)M, (int)K, (int)Kp, A, lda, sa.as<int>(), ra.as<int8_t>()));
     IAB_TIMED("k_residues_cols", st, k_residues_cols<<<dim3((unsigned)((N + 63) / 64), (unsigned)((Kp + 63) / 64)), 256, 0, st>>>(
         (int)K, (int)N, (int)Kp, B, ldb, sb.as<int>(), rb.as<int8_t>()));
@@ -651,6 +740,7 @@ int gemm_f64_ozaki_launch(int64_t M, int64_t N, int64_t K, const double *A, int6
     const int tiles = L * prm.tiles_m * prm.tiles_n;
     IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
     launch_crt(cached.nc, (unsigned)(nsm * 8), (int)M, (int)N, rr.as<uint8_t>(), ldr, sa.as<int>(), sb.as<int>(), C, ldc, st);
+    launch_nonfinite_fix<double>(M, N, K, A, lda, B, ldb, C, ldc, sa.as<int>(), sb.as<int>(), kNonFinite, st);
     return 0;
 }
 
@@ -677,8 +767,10 @@ struct B3Params {
 };
 
 // Row-major A (M x K) -> planes [2][M][Kp] of bf16 (hi, lo), K padded with zeros.
+// A row (column) holding a value whose bf16 part is not finite (NaN, infinity, or a float
+// beyond bf16's range) sets its flag; its outputs are recomputed by k_nonfinite_fix.
 __global__ void __launch_bounds__(256) k_split_rows(int M, int K, int Kp, const float *__restrict__ A, int64_t lda,
-                                                    __nv_bfloat16 *__restrict__ P)
+                                                    __nv_bfloat16 *__restrict__ P, int *__restrict__ rflag)
 {
     const int groups = Kp / 4;
     const int64_t total = (int64_t)M * groups, plane = (int64_t)M * Kp;
@@ -690,6 +782,7 @@ __global__ void __launch_bounds__(256) k_split_rows(int M, int K, int Kp, const 
             const float x = k0 + u < K ? A[(int64_t)i * lda + k0 + u] : 0.f;
             h[u] = __float2bfloat16_rn(x);
             l[u] = __float2bfloat16_rn(x - __bfloat162float(h[u]));
+            if (!isfinite(__bfloat162float(h[u]))) rflag[i] = 1;
         }
         __nv_bfloat16 *ph = P + (int64_t)i * Kp + k0;
         *reinterpret_cast<uint2 *>(ph) = *reinterpret_cast<const uint2 *>(h);
@@ -699,7 +792,7 @@ __global__ void __launch_bounds__(256) k_split_rows(int M, int K, int Kp, const 
 
 // Row-major B (K x N) -> planes [2][N][Kp] of bf16 (transposed, K-major).
 __global__ void __launch_bounds__(256) k_split_cols(int K, int N, int Kp, const float *__restrict__ B, int64_t ldb,
-                                                    __nv_bfloat16 *__restrict__ P)
+                                                    __nv_bfloat16 *__restrict__ P, int *__restrict__ cflag)
 {
     __shared__ float tile[64][65];
     const int k0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
@@ -720,6 +813,7 @@ __global__ void __launch_bounds__(256) k_split_cols(int K, int N, int Kp, const 
             const float x = tile[kg + u][c];
             h[u] = __float2bfloat16_rn(x);
             l[u] = __float2bfloat16_rn(x - __bfloat162float(h[u]));
+            if (!isfinite(__bfloat162float(h[u]))) cflag[j] = 1;
         }
         __nv_bfloat16 *ph = P + (int64_t)j * Kp + k0 + kg;
         *reinterpret_cast<uint2 *>(ph) = *reinterpret_cast<const uint2 *>(h);
@@ -866,16 +960,18 @@ int gemm_f32_bf16x3(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda
     int dev = 0;
     cudaGetDevice(&dev);
     const int64_t Kp = round_up(K, b3::BK);
-    DevBuf pa, pb, err;
+    DevBuf pa, pb, err, flg;
     if (!pa.allocate((size_t)(2 * M * Kp * 2), dev) || !pb.allocate((size_t)(2 * N * Kp * 2), dev) ||
-        !err.allocate(16, dev))
+        !err.allocate(16, dev) || !flg.allocate((size_t)(M + N) * 4, dev))
         return -100;
     cudaMemsetAsync(err.p, 0, 16, st);
+    cudaMemsetAsync(flg.p, 0, (size_t)(M + N) * 4, st);
+    int *rflag = flg.as<int>(), *cflag = rflag + M;
     const int nsm = sms();
     IAB_TIMED("k_split_rows", st, k_split_rows<<<(unsigned)(nsm * 16), 256, 0, st>>>(
-        (int)M, (int)K, (int)Kp, A, lda, pa.as<__nv_bfloat16>()));
+        (int)M, (int)K, (int)Kp, A, lda, pa.as<__nv_bfloat16>(), rflag));
     IAB_TIMED("k_split_cols", st, k_split_cols<<<dim3((unsigned)((N + 63) / 64), (unsigned)((Kp + 63) / 64)), 256, 0, st>>>(
-        (int)K, (int)N, (int)Kp, B, ldb, pb.as<__nv_bfloat16>()));
+        (int)K, (int)N, (int)Kp, B, ldb, pb.as<__nv_bfloat16>(), cflag));
     CUtensorMap tmA, tmB;
     if (!make_tmap_3d(&tmA, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, pa.p, (uint64_t)Kp, (uint64_t)M, 2, (uint64_t)Kp * 2,
                       (uint64_t)(Kp * M * 2), b3::BK, b3::BM, CU_TENSOR_MAP_SWIZZLE_128B) ||
@@ -893,6 +989,7 @@ int gemm_f32_bf16x3(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda
     }
     const int tiles = prm.tiles_m * prm.tiles_n;
     IAB_TIMED("k_bf16x3_gemm", st, k_bf16x3_gemm<<<(unsigned)std::min(tiles, nsm), b3::THREADS, b3::SMEM, st>>>(tmA, tmB, prm));
+    launch_nonfinite_fix<float>(M, N, K, A, lda, B, ldb, C, ldc, rflag, cflag, 1, st);
     int h_err = 0;
     cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return -2;

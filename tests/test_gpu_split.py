@@ -127,3 +127,84 @@ def test_split_f32_zero_and_single_tile(ia):
     A = np.full((5, 7), 0.5, np.float32)
     Ac = ia.Container.from_numpy(ctx, A, (5, 7), (5, 7))
     assert np.array_equal(ia.opt_gemm(ctx, Ac, Bc, (5, 3), (5, 3)).to_numpy(), np.full((5, 3), 3.5, np.float32))
+
+
+def _classes(c):
+    return np.isnan(c), np.isposinf(c), np.isneginf(c)
+
+
+def _nonfinite_inputs(rng, dtype):
+    A = _scaled(rng, (150, 230)).astype(dtype)
+    B = _scaled(rng, (230, 170)).astype(dtype)
+    A[3, 10] = np.nan
+    A[7, 2] = np.inf
+    A[9, 100] = -np.inf
+    B[4, 5] = -np.inf
+    B[50, 60] = np.nan
+    return A, B
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_split_nonfinite_propagates_like_native(ia, dtype):
+    """A NaN or an infinity in a row of A (column of B) reaches that row (column) of C with
+    the same IEEE classes as the native product; every other output stays accurate."""
+    rng = np.random.default_rng(11)
+    A, B = _nonfinite_inputs(rng, dtype)
+    ctx = _split_ctx(ia)
+    C = ia.matmul(ctx, ia.Container.from_numpy(ctx, A, (64, 64), (32, 32)),
+                  ia.Container.from_numpy(ctx, B, (64, 64), (32, 32)), (64, 64), (32, 32)).to_numpy()
+    with np.errstate(invalid="ignore", over="ignore"):
+        ref = A @ B
+    for got, want in zip(_classes(C), _classes(ref)):
+        assert np.array_equal(got, want)
+    rows = np.setdiff1d(np.arange(A.shape[0]), [3, 7, 9])
+    cols = np.setdiff1d(np.arange(B.shape[1]), [5, 60])
+    a, b = A[rows].astype(np.float64), B[:, cols].astype(np.float64)
+    exact = a @ b
+    err = np.linalg.norm(C[np.ix_(rows, cols)] - exact) / np.linalg.norm(exact)
+    assert err <= (1e-14 if dtype == np.float64 else 5e-5), err
+
+
+def test_split_f64_extreme_magnitudes(ia):
+    """Rows and columns near the ends of the float64 range: the scaling takes their norms
+    without overflow or underflow, so every block of C keeps the split form's accuracy."""
+    rng = np.random.default_rng(12)
+    A, B = _scaled(rng, (120, 300)), _scaled(rng, (300, 110))
+    A[:20] *= 2.0 ** -600
+    A[20:40] *= 2.0 ** 600
+    B[:, :20] *= 2.0 ** -300
+    B[:, 20:40] *= 2.0 ** 300
+    ctx = _split_ctx(ia)
+    C = ia.matmul(ctx, ia.Container.from_numpy(ctx, A, (64, 64), (32, 32)),
+                  ia.Container.from_numpy(ctx, B, (64, 64), (32, 32)), (64, 64), (32, 32)).to_numpy()
+    rows = np.arange(A.shape[0])
+    hi, lo = O.dd_rows(A, B, rows)
+    for rs in (slice(0, 20), slice(20, 40), slice(40, 120)):
+        for cs in (slice(0, 20), slice(20, 40), slice(40, 110)):
+            h, l, c = hi[rs, cs], lo[rs, cs], C[rs, cs]
+            scale = np.abs(h).max()
+            d = ((c - h) - l) / scale
+            assert np.all(np.isfinite(c))
+            assert np.linalg.norm(d) <= 1e-14 * np.linalg.norm(h / scale), (rs, cs)
+
+
+def test_split_f64_fewer_moduli(ia):
+    """8 and 10 moduli (two 40-bit reconstruction chunks) stay exact on small integers and
+    lose accuracy only as the smaller product of moduli dictates."""
+    rng = np.random.default_rng(13)
+    A, B = _scaled(rng, (96, 512)), _scaled(rng, (512, 80))
+    hi, lo = O.dd_rows(A, B, np.arange(96))
+    errs = []
+    for nterms in (8, 10, 12, 14):
+        ctx = ia.Context(form=ia.FORM_SPLIT, split_terms=nterms)
+        C = ia.matmul(ctx, ia.Container.from_numpy(ctx, A, (64, 64), (32, 32)),
+                      ia.Container.from_numpy(ctx, B, (64, 64), (32, 32)), (64, 64), (32, 32)).to_numpy()
+        errs.append(O.normwise_error(C, hi, lo, np.arange(96)))
+    assert errs[0] <= 1e-6 and errs[-1] <= 1e-14, errs
+    assert all(errs[i + 1] <= errs[i] for i in range(len(errs) - 1)), errs
+    X = np.arange(48 * 64, dtype=np.float64).reshape(48, 64) % 17
+    Y = np.arange(64 * 40, dtype=np.float64).reshape(64, 40) % 13
+    ctx = ia.Context(form=ia.FORM_SPLIT, split_terms=8)
+    Z = ia.matmul(ctx, ia.Container.from_numpy(ctx, X, (32, 32), (16, 16)),
+                  ia.Container.from_numpy(ctx, Y, (32, 32), (16, 16)), (32, 32), (16, 16)).to_numpy()
+    assert np.array_equal(Z, X @ Y)
