@@ -1127,33 +1127,46 @@ __global__ void __launch_bounds__(32, 10) k_lz4_encode(const uint8_t *__restrict
 // ---------------------------------------------------------------- LZ4 encoder, parallel parse
 // The second encoder mode.  It writes standard LZ4 blocks (any LZ4 decoder, liblz4 and the
 // reference's Blosc2 included, reads them back bit-exactly) but does not retrace liblz4's
-// serial search, so its bytes differ from liblz4's.  Per window of PW positions:
-//  A. every position is hashed (4 bytes, 13 bits); its candidate is the table entry of its
-//     bucket as of the previous round of 32 positions (the table keeps the low 16 bits of a
-//     recent position of each bucket; a reconstructed position is verified by its bytes),
-//     and the previous position is a second candidate (runs); the longer match is kept,
-//     measured up to PCAP bytes.  Every position enters the table.
+// serial search, so its bytes differ from liblz4's.  One CTA of PT threads encodes one
+// stream; per window of PW positions:
+//  A. every position is hashed (4 bytes, 12 bits); its candidate is the latest position of
+//     its bucket among the previous rounds of PT positions (the table keeps the largest
+//     position written, so it is the same whatever the order of the writes), and the
+//     previous position is a second candidate (runs); the longer match is kept, measured
+//     up to PCAP bytes.  Every position enters the table.
 //  B. the greedy parse (from the parse position, take the first position with a match of
 //     at least 4 bytes, continue after it) is a chain over match positions: J[q] = the first
 //     match position at or after q + L(q).  The chain is located by pointer doubling (J,
 //     J^2, J^4, ... in two ping-pong tables, the chain doubled alongside), the sequences'
-//     output sizes are prefix-summed across the warp, and every lane writes its own
+//     output sizes are prefix-summed across the CTA, and every thread writes its own
 //     sequences.  A chain ends at the window end, after the window's last match, or at a
 //     match of PCAP bytes or more, which is extended exactly before it is written.
 // Format rules kept: offsets 1..65535, matches start at least 12 bytes before the end and
 // end at least 5 bytes before it, so the block ends with >= 5 literals.
 constexpr int PW = 1024;
+constexpr int PT = 128;                   // threads per stream
 constexpr int PCAP = 128;                 // match lengths measured in phase A (PCAP: at least PCAP)
 constexpr uint16_t PJ_NONE = 0xFFFF, PJ_OUT = 0xFFFE, PJ_LONG = 0xFFFD;
+constexpr int PSTAGE = 1024 + 16;         // staged bytes per probe window (from 4 before it)
 
-struct ParSmem {              // per warp
-    uint16_t tab[8192];
+struct ParSmem {              // per CTA
+    union {
+        uint16_t tab16[8192]; // liblz4 search (byU16); probe: four tables of 2048
+        uint32_t tab32[4096]; // parallel parse: position + 1 of each bucket (0: empty); liblz4 byU32
+    };
     uint8_t ring[ERING + 16];
-    uint16_t cw[PW];          // match distance of each window position
-    uint8_t lw[PW];           // match length (0: none, 4..PCAP; PCAP: at least PCAP)
-    uint16_t J[2][PW];        // chain tables
-    uint16_t path[PW / 4 * 2 + 2];
+    union {
+        struct {
+            uint16_t cw[PW];  // match distance of each window position
+            uint8_t lw[PW];   // match length (0: none, 4..PCAP; PCAP: at least PCAP)
+            uint16_t J[2][PW];// chain tables
+            uint16_t path[PW / 4 * 2 + 2];
+        } w;
+        uint8_t stage[4][PSTAGE];
+    };
     uint32_t bits[32];        // match flags, one word per 32 positions
+    int32_t red[8];           // block reductions
+    long long sid;
 };
 
 // First match position at or after window offset rel (PJ_NONE: none left in the window).
@@ -1202,38 +1215,86 @@ __device__ __forceinline__ uint32_t par_rd32(uint32_t ring_s, int x)
     return __funnelshift_r(lds32(wa), lds32(wa + 4), (o & 3) * 8);
 }
 
-__device__ __forceinline__ int warp_lz4_compress_par(const uint8_t *__restrict__ src, int n,
-                                                     uint8_t *__restrict__ dst, int cap, ParSmem &S)
+// es_fill for a whole CTA (every thread calls it with the same `want`).
+__device__ __forceinline__ void cta_fill(EncSrc &s, int want)
 {
-    const int lane = threadIdx.x & 31;
+    while (s.hi < s.n && s.hi < want) {
+        const int base = s.hi, cnt = min(ESEG, s.n - base);
+        __syncthreads();                                 // reads of the slots being replaced are done
+        for (int x = threadIdx.x * 4; x < cnt; x += PT * 4) {
+            uint32_t v = 0;
+            if (base + x + 8 <= s.n) {
+                v = ld4u(s.g + base + x);
+            } else {
+                for (int k = 0; k < 4; k++)
+                    if (base + x + k < s.n) v |= (uint32_t)__ldg(s.g + base + x + k) << (8 * k);
+            }
+            const int o = (base + x) & (ERING - 1);
+            *reinterpret_cast<uint32_t *>(s.r + o) = v;
+            if (o < 16) *reinterpret_cast<uint32_t *>(s.r + ERING + o) = v;
+        }
+        s.hi = base + cnt;
+        s.lo = max(s.lo, base + ESEG - ERING);
+        __syncthreads();
+    }
+}
+
+// Block-wide sum / min of one int per thread (uses red[]; ends with every thread holding
+// the result and red[] free again).
+__device__ __forceinline__ int cta_sum(int v, int32_t *red)
+{
+    v = (int)__reduce_add_sync(FULLMASK, (unsigned)v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    const int t = red[0] + red[1] + red[2] + red[3];
+    __syncthreads();
+    return t;
+}
+
+__device__ __forceinline__ int cta_min(int v, int32_t *red)
+{
+    v = (int)__reduce_min_sync(FULLMASK, (unsigned)v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    const int t = min(min(red[0], red[1]), min(red[2], red[3]));
+    __syncthreads();
+    return t;
+}
+
+__device__ __forceinline__ int cta_lz4_compress_par(const uint8_t *__restrict__ src, int n,
+                                                    uint8_t *__restrict__ dst, int cap, ParSmem &S)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(S.ring);
-    for (int i = lane; i < 8192; i += 32) S.tab[i] = 0;
+    for (int i = tid; i < 4096 / 4; i += PT) reinterpret_cast<uint4 *>(S.tab32)[i] = make_uint4(0u, 0u, 0u, 0u);
     EncSrc s;
     s.g = src; s.r = S.ring; s.lo = 0; s.hi = 0; s.n = n;
-    __syncwarp();
+    __syncthreads();
     int op = 0, anchor = 0, pos = 0;
     const int mfl1 = n - 11, mlimit = n - 5;
     for (int w0 = 0; n >= 13 && w0 < mfl1; w0 += PW) {
         const int wend = min(w0 + PW, mfl1), wn = wend - w0;
-        es_fill(s, wend + PCAP + 32);
+        cta_fill(s, wend + PCAP + 32);
         // ---- A: candidates and lengths.  Positions p .. p + PCAP + 4 lie in the window;
         // a candidate is read from the window when it is still there, else from global memory.
-        for (int r = 0; r < PW / 32; r++) {
-            const int p = w0 + r * 32 + lane;
-            const bool valid = p < wend;
+        // The stream's first PT positions go in rounds of 32 (one warp), so that short streams
+        // keep table candidates for most of their positions; then rounds of PT.
+        for (int q0 = 0, rsz; q0 < PW; q0 += rsz) {
+            rsz = w0 + q0 < PT ? 32 : PT;
+            const int q = q0 + tid, p = w0 + q;
+            const bool valid = tid < rsz && p < wend;
             const uint32_t v = valid ? par_rd32(ring_s, p) : 0u;
-            const uint32_t h = (v * 2654435761u) >> (32 - 13);
-            const uint32_t tv = valid ? (uint32_t)S.tab[h] : 0u;
-            const int cand = p - (int)(((uint32_t)p - tv) & 0xFFFFu);
-            __syncwarp();
-            if (valid) S.tab[h] = (uint16_t)p;          // same-bucket lanes race: any of them may win
-            // two candidates: the table's and the previous position (runs); keep the longer
+            const uint32_t h = (v * 2654435761u) >> (32 - 12);
+            const uint32_t tv = valid ? S.tab32[h] : 0u;
+            __syncthreads();                             // every read of this round precedes its writes
+            if (valid) atomicMax(&S.tab32[h], (uint32_t)p + 1u);
+            const int cand = (int)tv - 1;
             int L = 0, best = cand;
             const int lim = min(mlimit - p, PCAP);
 #pragma unroll
             for (int t = 0; t < 2; t++) {
                 const int c = t ? p - 1 : cand;
-                if (!valid || c >= p || c < 0 || (t && c == cand)) continue;
+                if (!valid || c >= p || c < 0 || p - c > 65535 || (t && c == cand)) continue;
                 const bool inring = c >= s.lo;
                 if ((inring ? par_rd32(ring_s, c) : ld4u(src + c)) != v) continue;
                 int l = 4;
@@ -1245,84 +1306,85 @@ __device__ __forceinline__ int warp_lz4_compress_par(const uint8_t *__restrict__
                 l = min(l, lim);
                 if (l > L) { L = l; best = c; }
             }
-            S.cw[r * 32 + lane] = (uint16_t)(p - best);
-            S.lw[r * 32 + lane] = (uint8_t)L;
+            if (tid < rsz) {
+                S.w.cw[q] = (uint16_t)(p - best);
+                S.w.lw[q] = (uint8_t)L;
+            }
             const unsigned b = __ballot_sync(FULLMASK, L >= 4);
-            if (lane == r) S.bits[r] = b;
+            if (lane == 0 && warp < rsz / 32) S.bits[(q0 >> 5) + warp] = b;
+            __syncthreads();                             // this round's writes precede the next reads
         }
-        __syncwarp();
         // ---- B: chains of matches from the parse position
         while (pos < wend) {
             const uint32_t s0 = par_next_match(S.bits, pos - w0);
             if (s0 >= (uint32_t)wn) { pos = wend; break; }   // no match left: literals run on
             // J[q]: the match after the one at q, or why the chain stops there
-            for (int q = lane; q < wn; q += 32) {
-                const int L = S.lw[q];
+            for (int q = tid; q < wn; q += PT) {
+                const int L = S.w.lw[q];
                 uint16_t j = PJ_NONE;
                 if (L >= PCAP) j = PJ_LONG;
                 else if (L >= 4) {
                     const uint32_t nx = par_next_match(S.bits, q + L);
                     j = nx >= (uint32_t)wn ? (q + L >= wn ? PJ_OUT : PJ_NONE) : (uint16_t)nx;
                 }
-                S.J[0][q] = j;
+                S.w.J[0][q] = j;
             }
-            if (lane == 0) S.path[0] = (uint16_t)s0;
-            __syncwarp();
+            if (tid == 0) S.w.path[0] = (uint16_t)s0;
+            __syncthreads();
             int len = 1, cur = 0, cnt = 0;
             for (;;) {
                 int first = 0x7FFFFFFF;
-                for (int j = lane; j < len; j += 32) {
-                    const uint16_t pj = S.path[j];
-                    const uint16_t v = pj < wn ? S.J[cur][pj] : pj;
-                    S.path[len + j] = v;
+                for (int j = tid; j < len; j += PT) {
+                    const uint16_t pj = S.w.path[j];
+                    const uint16_t v = pj < wn ? S.w.J[cur][pj] : pj;
+                    S.w.path[len + j] = v;
                     if (v >= wn) first = min(first, len + j);
                 }
-                first = (int)__reduce_min_sync(FULLMASK, (unsigned)first);
-                __syncwarp();
+                first = cta_min(first, S.red);
                 if (first < 2 * len) { cnt = first; break; }
-                for (int q = lane; q < wn; q += 32) {
-                    const uint16_t v = S.J[cur][q];
-                    S.J[cur ^ 1][q] = v < wn ? S.J[cur][v] : v;
+                for (int q = tid; q < wn; q += PT) {
+                    const uint16_t v = S.w.J[cur][q];
+                    S.w.J[cur ^ 1][q] = v < wn ? S.w.J[cur][v] : v;
                 }
                 cur ^= 1;
                 len *= 2;
-                __syncwarp();
+                __syncthreads();
             }
-            const uint16_t term = S.path[cnt];                  // why the chain stopped
-            // a capped last match: extend it exactly (warp-wide) before writing it
-            int lastL = S.lw[S.path[cnt - 1]];
-            const int lastq = w0 + S.path[cnt - 1], lastd = S.cw[S.path[cnt - 1]];
+            const uint16_t term = S.w.path[cnt];                // why the chain stopped
+            // a capped last match: extend it exactly (CTA-wide) before writing it
+            int lastL = S.w.lw[S.w.path[cnt - 1]];
+            const int lastq = w0 + S.w.path[cnt - 1], lastd = S.w.cw[S.w.path[cnt - 1]];
             if (term == PJ_LONG) {
                 for (;;) {
                     const int a = lastq + lastL;
-                    es_fill(s, a + 32 + ELOOK);
-                    const bool eq = a + lane < mlimit && es_byte(s, a + lane) == es_byte(s, a - lastd + lane);
+                    cta_fill(s, a + PT + ELOOK);
+                    const bool eq = a + tid < mlimit && es_byte(s, a + tid) == es_byte(s, a - lastd + tid);
                     const unsigned ne = __ballot_sync(FULLMASK, !eq);
-                    const int cnum = ne ? __ffs((int)ne) - 1 : 32;
+                    const int cnum = cta_min(ne ? warp * 32 + __ffs((int)ne) - 1 : PT, S.red);
                     lastL += cnum;
-                    if (cnum < 32) break;
+                    if (cnum < PT) break;
                 }
             }
-            // output sizes, exclusive prefix across the warp (lane owns sequences lane + 32 k)
+            // output sizes
             int mine = 0;
-            for (int i = lane; i < cnt; i += 32) {
-                const int q = w0 + S.path[i];
-                const int prev_end = i ? w0 + S.path[i - 1] + S.lw[S.path[i - 1]] : anchor;
-                const int L = (i == cnt - 1) ? lastL : S.lw[S.path[i]];
+            for (int i = tid; i < cnt; i += PT) {
+                const int q = w0 + S.w.path[i];
+                const int prev_end = i ? w0 + S.w.path[i - 1] + S.w.lw[S.w.path[i - 1]] : anchor;
+                const int L = (i == cnt - 1) ? lastL : S.w.lw[S.w.path[i]];
                 mine += lz4_seq_bytes(q - prev_end, L - 4);
             }
-            // a lane's sequences are not contiguous in order: scan per round of 32 instead
-            int total = (int)__reduce_add_sync(FULLMASK, (unsigned)mine);
+            const int total = cta_sum(mine, S.red);
             if (op + total + 1 + 6 > cap) return 0;
+            // write: exclusive scan per round of PT sequences
             int base = op;
-            for (int i0 = 0; i0 < cnt; i0 += 32) {
-                const int i = i0 + lane;
+            for (int i0 = 0; i0 < cnt; i0 += PT) {
+                const int i = i0 + tid;
                 int sz = 0, q = 0, prev_end = 0, L = 0, d = 0;
                 if (i < cnt) {
-                    q = w0 + S.path[i];
-                    prev_end = i ? w0 + S.path[i - 1] + S.lw[S.path[i - 1]] : anchor;
-                    L = (i == cnt - 1) ? lastL : S.lw[S.path[i]];
-                    d = S.cw[S.path[i]];
+                    q = w0 + S.w.path[i];
+                    prev_end = i ? w0 + S.w.path[i - 1] + S.w.lw[S.w.path[i - 1]] : anchor;
+                    L = (i == cnt - 1) ? lastL : S.w.lw[S.w.path[i]];
+                    d = S.w.cw[S.w.path[i]];
                     sz = lz4_seq_bytes(q - prev_end, L - 4);
                 }
                 int incl = sz;
@@ -1331,13 +1393,22 @@ __device__ __forceinline__ int warp_lz4_compress_par(const uint8_t *__restrict__
                     const int t = __shfl_up_sync(FULLMASK, incl, o);
                     if (lane >= o) incl += t;
                 }
-                if (i < cnt) lz4_put_seq(s, dst + base + incl - sz, prev_end, q, d, L);
-                base += __shfl_sync(FULLMASK, incl, 31);
+                if (lane == 31) S.red[warp] = incl;
+                __syncthreads();
+                int before = 0, all = 0;
+#pragma unroll
+                for (int k = 0; k < PT / 32; k++) {
+                    const int t = S.red[k];
+                    before += k < warp ? t : 0;
+                    all += t;
+                }
+                if (i < cnt) lz4_put_seq(s, dst + base + before + incl - sz, prev_end, q, d, L);
+                base += all;
+                __syncthreads();
             }
             op = base;
             anchor = lastq + lastL;
             pos = anchor;
-            __syncwarp();
             if (term == PJ_NONE) { pos = max(pos, wend); }
         }
     }
@@ -1348,97 +1419,119 @@ __device__ __forceinline__ int warp_lz4_compress_par(const uint8_t *__restrict__
         int k = 1;
         if (last >= 15) {
             const int rem = last - 15, nff = rem / 255;
-            for (int x = lane; x < nff; x += 32) o[1 + x] = 255;
-            if (lane == 0) o[1 + nff] = (uint8_t)(rem % 255);
+            for (int x = tid; x < nff; x += PT) o[1 + x] = 255;
+            if (tid == 0) o[1 + nff] = (uint8_t)(rem % 255);
             k += nff + 1;
         }
-        if (lane == 0) o[0] = (uint8_t)((last >= 15 ? 15 : last) << 4);
-        for (int x = lane; x < last; x += 32) o[k + x] = (uint8_t)es_byte(s, anchor + x);
+        if (tid == 0) o[0] = (uint8_t)((last >= 15 ? 15 : last) << 4);
+        for (int x = tid; x < last; x += PT) o[k + x] = (uint8_t)es_byte(s, anchor + x);
         op += k + last;
     }
-    __syncwarp();
+    __syncthreads();
     return op;
 }
 
 // Matches found in four sampled windows of 1024 positions (at 0, 1/4, 1/2 and 3/4 of the
-// stream): positions with a 4-byte match against a table of recent positions or against
-// the previous position.
-__device__ __forceinline__ int par_probe(const uint8_t *__restrict__ src, int n, uint16_t *tab)
+// stream), one window per warp: positions with a 4-byte match against the warp's table of
+// recent positions of the window (11-bit hash) or against the previous position.  Each
+// window is staged in shared memory first by one round of coalesced word loads.  Returns
+// the CTA's total.
+__device__ __forceinline__ uint32_t stage_rd32(const uint8_t *stage, int o)
 {
-    const int lane = threadIdx.x & 31;
-    for (int i = lane; i < 8192; i += 32) tab[i] = 0xFFFF;
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(stage) + (o >> 2);
+    return __funnelshift_r(w[0], w[1], (uint32_t)(o & 3) * 8);
+}
+
+__device__ __forceinline__ int cta_probe(const uint8_t *__restrict__ src, int n, ParSmem &S)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint16_t *tab = S.tab16 + w * 2048;
+    uint8_t *stage = S.stage[w];
+    for (int i = lane; i < 2048 / 8; i += 32) reinterpret_cast<uint4 *>(tab)[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
+    const int base = (int)(((int64_t)(n - 11) * w / 4) & ~31);
+    const int lim = min(n - 11, base + 1024);
+    const int b0 = base >= 4 ? base - 4 : 0;                 // word aligned: base is a multiple of 32
+    const int cnt = min(PSTAGE, n - b0);
+    for (int x = lane * 4; x < cnt; x += 128) {
+        uint32_t v = 0;
+        if (b0 + x + 8 <= n) {                               // ld4u reads 8 bytes
+            v = ld4u(src + b0 + x);
+        } else {
+            for (int k = 0; k < 4; k++)
+                if (b0 + x + k < n) v |= (uint32_t)__ldg(src + b0 + x + k) << (8 * k);
+        }
+        *reinterpret_cast<uint32_t *>(stage + x) = v;
+    }
     __syncwarp();
     int hits = 0;
-    for (int w = 0; w < 4; w++) {
-      const int base = (int)(((int64_t)(n - 11) * w / 4) & ~31);
-      const int lim = min(n - 11, base + 1024);
-      for (int r = 0; r < 32; r++) {
+    for (int r = 0; r < 32; r++) {
         const int p = base + r * 32 + lane;
         const bool valid = p < lim;
-        const uint32_t v = valid ? ld4u(src + p) : 0u;
-        const uint32_t h = (v * 2654435761u) >> (32 - 13);
+        const uint32_t v = valid ? stage_rd32(stage, p - b0) : 0u;
+        const uint32_t h = (v * 2654435761u) >> (32 - 11);
         const uint32_t c = valid ? tab[h] : 0xFFFFu;
         __syncwarp();
         if (valid) tab[h] = (uint16_t)p;
-        const bool m = valid && ((c < (uint32_t)p && ld4u(src + c) == v) || (p > 0 && ld4u(src + p - 1) == v));
+        const bool m = valid && ((c < (uint32_t)p && c >= (uint32_t)b0 && stage_rd32(stage, (int)c - b0) == v) ||
+                                 (p > b0 && stage_rd32(stage, p - 1 - b0) == v));
         hits += __popc(__ballot_sync(FULLMASK, m));
-      }
     }
-    __syncwarp();
-    return hits;
+    return cta_sum(lane == 0 ? hits : 0, S.red);
 }
 
-// E2 (parallel mode): one warp per stream, as k_lz4_encode.  A probe of four sampled
-// windows routes each stream: almost no matches (incompressible byte planes): stored raw;
-// few matches: the liblz4 search, whose accelerating skip makes them cheap; the rest: the
-// parallel parse.
-__global__ void __launch_bounds__(32, 7) k_lz4_encode_par(const uint8_t *__restrict__ img, int64_t nstreams_total,
+// E2 (parallel mode): one CTA of PT threads per stream, streams handed out dynamically.  A
+// probe of four sampled windows routes each stream: almost no matches (incompressible
+// byte planes): stored raw; few matches: the liblz4 search (one warp), whose accelerating
+// skip makes them cheap; the rest: the parallel parse.
+__global__ void __launch_bounds__(PT, 7) k_lz4_encode_par(const uint8_t *__restrict__ img, int64_t nstreams_total,
                                                        int neblock, uint8_t *slots, EncStream *es,
                                                        unsigned long long *next)
 {
     extern __shared__ __align__(16) uint8_t sm_par[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    ParSmem &S = reinterpret_cast<ParSmem *>(sm_par)[warp];
+    ParSmem &S = *reinterpret_cast<ParSmem *>(sm_par);
+    const int tid = threadIdx.x, warp = tid >> 5;
     for (;;) {
-        unsigned long long got = 0;
-        if (lane == 0) got = atomicAdd(next, 1ull);
-        const int64_t sid = (int64_t)__shfl_sync(FULLMASK, got, 0);
+        if (tid == 0) S.sid = (long long)atomicAdd(next, 1ull);
+        __syncthreads();
+        const int64_t sid = S.sid;
+        __syncthreads();
         if (sid >= nstreams_total) break;
         const uint8_t *src = img + sid * neblock;
         const uint8_t first = __ldg(src);
         bool run = true;
-        for (int b = 0; b < neblock && run; b += 32 * 16) {
+        for (int b = 0; b < neblock && run; b += PT * 16) {
             bool mine = true;
             for (int k = 0; k < 16; k++) {
-                const int x = b + k * 32 + lane;
+                const int x = b + k * PT + tid;
                 if (x < neblock && __ldg(src + x) != first) mine = false;
             }
-            run = __all_sync(FULLMASK, mine);
+            run = __syncthreads_and(mine);
         }
         EncStream e;
         e.out = -1;
         if (run) {
             e.kind = SK_RUN; e.csize = first; e.need = 0;
         } else {
-            const int hits = par_probe(src, neblock, S.tab);
+            const int hits = cta_probe(src, neblock, S);
             if (hits < 16) {                     // no matches to speak of: store the stream raw
                 e.kind = SK_RAW; e.csize = neblock; e.need = neblock + 1;
             } else if (hits < 256) {
-                int need = 0;
-                uint32_t *t32 = reinterpret_cast<uint32_t *>(S.tab);
-                const int cs = neblock < 65536 + 12 - 1
-                                   ? warp_lz4_compress<true>(src, neblock, slots + sid * neblock, neblock, t32, S.ring, &need)
-                                   : warp_lz4_compress<false>(src, neblock, slots + sid * neblock, neblock, t32, S.ring, &need);
-                if (cs > 0 && cs < neblock) { e.kind = SK_LZ4; e.csize = cs; e.need = need; }
-                else { e.kind = SK_RAW; e.csize = neblock; e.need = need; }
+                if (warp == 0) {
+                    int need = 0;
+                    const int cs = neblock < 65536 + 12 - 1
+                                       ? warp_lz4_compress<true>(src, neblock, slots + sid * neblock, neblock, S.tab32, S.ring, &need)
+                                       : warp_lz4_compress<false>(src, neblock, slots + sid * neblock, neblock, S.tab32, S.ring, &need);
+                    if (cs > 0 && cs < neblock) { e.kind = SK_LZ4; e.csize = cs; e.need = need; }
+                    else { e.kind = SK_RAW; e.csize = neblock; e.need = need; }
+                }
             } else {
-                const int cs = warp_lz4_compress_par(src, neblock, slots + sid * neblock, neblock, S);
+                const int cs = cta_lz4_compress_par(src, neblock, slots + sid * neblock, neblock, S);
                 if (cs > 0 && cs < neblock) { e.kind = SK_LZ4; e.csize = cs; e.need = cs; }
                 else { e.kind = SK_RAW; e.csize = neblock; e.need = neblock + 1; }
             }
         }
-        if (lane == 0) es[sid] = e;
-        __syncwarp();
+        if (tid == 0) es[sid] = e;
+        __syncthreads();
     }
 }
 
@@ -1735,14 +1828,14 @@ int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int s
             reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1)));
     } else {
         static bool attr = false;
-        const int wpb = 1, smem = wpb * (int)sizeof(ParSmem);   // 1 warp per CTA, 7 CTAs per SM
+        const int smem = (int)sizeof(ParSmem);                 // one stream per CTA of PT threads, 7 CTAs per SM
         if (!attr) {
             cudaFuncSetAttribute(k_lz4_encode_par, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             attr = true;
         }
         const int64_t ns = nbl * nstreams;
-        const int64_t blocks = std::min<int64_t>((ns + wpb - 1) / wpb, (int64_t)sms * 7);
-        IAB_TIMED("k_lz4_encode_par", st, k_lz4_encode_par<<<(unsigned)std::max<int64_t>(blocks, 1), wpb * 32, smem, st>>>(
+        const int64_t blocks = std::min<int64_t>(ns, (int64_t)sms * 7);
+        IAB_TIMED("k_lz4_encode_par", st, k_lz4_encode_par<<<(unsigned)std::max<int64_t>(blocks, 1), PT, smem, st>>>(
             img.as<uint8_t>(), ns, neblock, slots.as<uint8_t>(), es.as<EncStream>(),
             reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1)));
     }

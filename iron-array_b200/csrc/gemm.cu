@@ -26,10 +26,11 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p)
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc, bool pred)
+// Copies `bytes` (0, 8 or 16) from global memory into a 16-byte shared slot; the rest of the
+// slot is zero-filled, so nothing past a matrix edge is read.
+__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc, int bytes)
 {
-    const int sz = pred ? 16 : 0;   // src-size 0 -> the 16 bytes are zero-filled
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(sdst)), "l"(gsrc), "r"(sz));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(sdst)), "l"(gsrc), "r"(bytes));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
@@ -76,15 +77,17 @@ __device__ __forceinline__ void f64_tile(int M, int N, int K, const double *__re
         for (int i = 0; i < BM / 32; i++) {      // A: BM rows x 8 16-byte pieces
             const int idx = tid + i * 256, r = idx >> 3, cpc = (idx & 7) * 2;
             const int gr = m0 + r, gk = k0 + cpc;
-            const bool ok = gr < M && gk < K;
-            cp_async16(a + r * SA + cpc, ok ? (const void *)(A + (int64_t)gr * lda + gk) : (const void *)A, ok);
+            // the two doubles at gk, gk + 1 that lie inside the row (K may be odd: the padding
+            // column after it is never read, it may hold anything)
+            const int nb = gr < M ? 8 * max(0, min(2, K - gk)) : 0;
+            cp_async16(a + r * SA + cpc, nb ? (const void *)(A + (int64_t)gr * lda + gk) : (const void *)A, nb);
         }
 #pragma unroll
         for (int i = 0; i < BN / 32; i++) {      // B: 16 rows x BN/2 pieces
             const int idx = tid + i * 256, r = idx / (BN / 2), cpc = (idx % (BN / 2)) * 2;
             const int gk = k0 + r, gn = n0 + cpc;
-            const bool ok = gk < K && gn < N;
-            cp_async16(b + r * G::SB + cpc, ok ? (const void *)(B + (int64_t)gk * ldb + gn) : (const void *)B, ok);
+            const int nb = gk < K ? 8 * max(0, min(2, N - gn)) : 0;
+            cp_async16(b + r * G::SB + cpc, nb ? (const void *)(B + (int64_t)gk * ldb + gn) : (const void *)B, nb);
         }
     };
 

@@ -189,3 +189,22 @@ def test_matmul_persists_output_when_urlpath_given(ctx, ia, tmp_path):
     C = ia.matmul(ctx, ia.Container.from_numpy(ctx, A, (50, 40), (25, 20)),
                   ia.Container.from_numpy(ctx, B, (40, 30), (20, 15)), (50, 30), (25, 15), urlpath=p)
     assert np.array_equal(ia.Container.open(ctx, p).to_numpy(), C.to_numpy())
+
+
+@pytest.mark.parametrize("K", [33, 1, 129])
+def test_native_f64_odd_k_reads_nothing_past_the_row(ctx, ia, K):
+    """Dense operands pad their rows to a multiple of 32 items and the padding is never
+    written: a product with odd K must not read it.  A first product of the same dense size
+    leaves NaN in recycled device buffers; the second must still be exact."""
+    M, N = 100, 50
+    ld = (K + 31) // 32 * 32
+    nan_a = np.full((M, ld), np.nan)
+    nan_b = np.full((ld, N), np.nan)
+    ia.opt_gemm(ctx, ia.Container.from_numpy(ctx, nan_a, (M, ld), (20, ld)),
+                ia.Container.from_numpy(ctx, nan_b, (ld, N), (ld, 10)), (M, N), (20, 10)).free()
+    rng = np.random.default_rng(K)
+    A = rng.integers(-8, 9, (M, K)).astype(np.float64)
+    B = rng.integers(-8, 9, (K, N)).astype(np.float64)
+    C = ia.opt_gemm(ctx, ia.Container.from_numpy(ctx, A, (M, K), (20, K)),
+                    ia.Container.from_numpy(ctx, B, (K, N), (K, 10)), (M, N), (20, 10)).to_numpy()
+    assert np.array_equal(C, A @ B)
