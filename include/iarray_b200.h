@@ -350,6 +350,22 @@ INA_API(ina_rc_t) iarray_b200_get_stream(iarray_context_t *ctx, void **stream);
 INA_API(ina_rc_t) iarray_b200_to_cframe_into(iarray_context_t *ctx, iarray_container_t *c, uint8_t *buf,
                                              int64_t cap, int64_t *len);
 
+/* B200 addition (no reference counterpart; it fuses the reference sequence
+ * iarray_from_cframe (iarray.h:611-615) for a and b + iarray_opt_gemm (iarray.h:866-870) +
+ * iarray_to_cframe (iarray.h:605-609) into one call).  C = A * B with A and B given as
+ * contiguous frames in host memory and C written as a contiguous frame into host memory
+ * `out` (capacity out_cap bytes; *out_len receives the frame's length, also when it does
+ * not fit, in which case IARRAY_ERR_TOO_SMALL_BUFFER is returned).  Partition rules,
+ * context form and encoder are those of iarray_opt_gemm; storage->urlpath must be NULL.
+ * The work runs in row bands of C (one chunk row each) so that the uploads of later bands,
+ * the kernels of the current one and the download of earlier ones overlap; with pinned
+ * host memory (cudaHostAlloc) the call approaches the time of the uploads.  A capacity of
+ * M * N * itemsize rounded up to whole chunks, plus 64 bytes per chunk, plus 4 KiB always
+ * suffices.  Implemented by iarray_b200_opt_gemm_cframes in api.cu. */
+INA_API(ina_rc_t) iarray_b200_opt_gemm_cframes(iarray_context_t *ctx, const uint8_t *a_frame, int64_t a_len,
+                                               const uint8_t *b_frame, int64_t b_len, iarray_storage_t *storage,
+                                               uint8_t *out, int64_t out_cap, int64_t *out_len);
+
 /* Batched products (B200 addition; the reference has no counterpart: its callers loop over
  * iarray_opt_gemm).  C_i = A_i * B_i for i < n, float64, each pair with its own shapes
  * (A_i: M_i x K_i, B_i: K_i x N_i) and partitions, output i partitioned by storage[i].

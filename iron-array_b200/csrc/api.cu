@@ -174,6 +174,10 @@ struct iarray_context_s {
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     cudaStream_t stream2 = nullptr;          // second stream for concurrent operand decode
     cudaEvent_t fork = nullptr, join = nullptr;
+    // iarray_b200_opt_gemm_cframes: copy streams and pinned staging for chunk tables
+    cudaStream_t up = nullptr, down = nullptr, enc = nullptr;
+    void *pin = nullptr;
+    size_t pin_n = 0;
 };
 
 struct iarray_container_s {
@@ -279,6 +283,10 @@ INA_API(void) iarray_context_free(iarray_context_t **ctx)
     iarray_context_t *c = *ctx;
     if (c->stream) { cudaStreamSynchronize(c->stream); cudaStreamDestroy(c->stream); }
     if (c->stream2) { cudaStreamSynchronize(c->stream2); cudaStreamDestroy(c->stream2); }
+    if (c->up) { cudaStreamSynchronize(c->up); cudaStreamDestroy(c->up); }
+    if (c->down) { cudaStreamSynchronize(c->down); cudaStreamDestroy(c->down); }
+    if (c->enc) { cudaStreamSynchronize(c->enc); cudaStreamDestroy(c->enc); }
+    if (c->pin) cudaFreeHost(c->pin);
     if (c->fork) cudaEventDestroy(c->fork);
     if (c->join) cudaEventDestroy(c->join);
     for (auto &e : c->ev) if (e) cudaEventDestroy(e);
@@ -448,7 +456,7 @@ static ina_rc_t decode_store(iarray_context_t *ctx, const iarray_container_t *c,
     const Geom &g = c->geom;
     if (g.nchunks == 0) return INA_SUCCESS;
     if (ld != g.shape[1] || g.nchunks * g.nblocks == 0) {
-        // padding columns must read as zero for the products
+        // callers of iarray_b200_decode_to_device get defined padding columns
         cudaMemsetAsync(dense, 0, (size_t)(g.shape[0] * ld * g.itemsize), ctx->stream);
     }
     const ChunkStore &s = *c->store;
@@ -473,9 +481,8 @@ static ina_rc_t decode_rc(int r)
 static ina_rc_t decode_pair(iarray_context_t *ctx, const iarray_container_t *a, void *da, int64_t lda,
                             const iarray_container_t *b, void *db, int64_t ldb)
 {
+    // the padding columns past each row are left as they are: no product reads them
     const Geom &ga = a->geom, &gb = b->geom;
-    if (lda != ga.shape[1]) cudaMemsetAsync(da, 0, (size_t)(ga.shape[0] * lda * ga.itemsize), ctx->stream);
-    if (ldb != gb.shape[1]) cudaMemsetAsync(db, 0, (size_t)(gb.shape[0] * ldb * gb.itemsize), ctx->stream);
     cudaEventRecord(ctx->fork, ctx->stream);
     cudaStreamWaitEvent(ctx->stream2, ctx->fork, 0);
     iab::DecodeWork wa, wb;
@@ -1220,6 +1227,308 @@ INA_API(ina_rc_t) iarray_opt_gemv(iarray_context_t *ctx, iarray_container_t *a, 
     rc = run_matmul(ctx, a, b, *c);
     if (INA_FAILED(rc)) iarray_container_free(ctx, c);
     return rc;
+}
+
+// ============================================================================ product of host frames, pipelined
+// iarray_b200_opt_gemm_cframes: iarray_opt_gemm for operands held as contiguous frames in
+// host memory, with the result written as a contiguous frame into host memory.  The work is
+// cut into row bands of C, one chunk row each.  All uploads are queued at once on the upload
+// stream (B's chunk rows, then A's); the context stream decodes each chunk row as soon as its
+// bytes are on the device, multiplies each band of A with the whole of B and encodes the
+// band; the download stream copies a band's chunks to their final place in the output frame
+// as soon as their sizes are known.  Uploads, kernels and downloads of different bands
+// overlap; with pinned host buffers the step approaches the time of the uploads.
+namespace {
+struct FrameView {
+    iab::FrameInfo fi;
+    std::vector<std::pair<int64_t, int32_t>> chunks;   // (offset in the frame, cbytes)
+    Geom g;
+};
+
+ina_rc_t view_frame(const uint8_t *f, int64_t n, FrameView *v)
+{
+    std::string why;
+    if (!iab::read_frame(f, (size_t)n, &v->fi, &v->chunks, &why)) return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+    const int isz = dtype_size(v->fi.dtype);
+    if (!isz) return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    if (v->fi.ndim != 2) return rc_err(IARRAY_ERR_INVALID_NDIM);
+    if (!iab::make_geom(2, v->fi.shape, v->fi.chunk, v->fi.block, isz, &v->g)) return rc_err(IARRAY_ERR_INVALID_CHUNKSHAPE);
+    if (v->fi.typesize != isz || v->fi.chunksize != v->g.chunk_nbytes || (int64_t)v->chunks.size() != v->g.nchunks)
+        return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+    for (auto &pr : v->chunks)
+        if (pr.first < 0 || pr.second <= 0 || pr.second > v->g.chunk_nbytes + 64 || pr.first + pr.second > n)
+            return rc_err(IARRAY_ERR_BLOSC_FAILED);
+    return INA_SUCCESS;
+}
+
+// One matrix's chunks on the device: the frame region [lo, hi) and the chunk index.
+struct DevChunks {
+    DevBuf buf, d_off, d_len;
+    int64_t lo = 0, hi = 0;
+};
+
+bool upload_index(const FrameView &v, DevChunks *d, int device)
+{
+    d->lo = INT64_MAX;
+    d->hi = 0;
+    for (auto &pr : v.chunks) {
+        d->lo = std::min(d->lo, pr.first);
+        d->hi = std::max(d->hi, pr.first + (int64_t)pr.second);
+    }
+    const size_t n = v.chunks.size();
+    std::vector<int64_t> off(n);
+    std::vector<int32_t> len(n);
+    for (size_t k = 0; k < n; k++) { off[k] = v.chunks[k].first - d->lo; len[k] = v.chunks[k].second; }
+    if (!d->buf.allocate((size_t)(d->hi - d->lo), device) || !d->d_off.allocate(n * 8, device) ||
+        !d->d_len.allocate(n * 4, device))
+        return false;
+    return cudaMemcpy(d->d_off.p, off.data(), n * 8, cudaMemcpyHostToDevice) == cudaSuccess &&
+           cudaMemcpy(d->d_len.p, len.data(), n * 4, cudaMemcpyHostToDevice) == cudaSuccess;
+}
+
+// Queues the upload of chunk row r of v (its byte range in the frame) and records ev.
+void upload_row(const FrameView &v, const uint8_t *frame, DevChunks &d, int64_t r, cudaStream_t up, cudaEvent_t ev)
+{
+    const int64_t per = v.g.cgrid[1];
+    int64_t lo = INT64_MAX, hi = 0;
+    for (int64_t k = r * per; k < (r + 1) * per; k++) {
+        lo = std::min(lo, v.chunks[(size_t)k].first);
+        hi = std::max(hi, v.chunks[(size_t)k].first + (int64_t)v.chunks[(size_t)k].second);
+    }
+    cudaMemcpyAsync(d.buf.as<uint8_t>() + (lo - d.lo), frame + lo, (size_t)(hi - lo), cudaMemcpyHostToDevice, up);
+    cudaEventRecord(ev, up);
+}
+
+// Geometry of rows [r * chunk0, ...) of g: one chunk row.
+Geom row_geom(const Geom &g, int64_t r)
+{
+    Geom b;
+    const int64_t rows = std::min(g.chunk[0], g.shape[0] - r * g.chunk[0]);
+    const int64_t shape[2] = {rows, g.shape[1]};
+    iab::make_geom(2, shape, g.chunk, g.block, g.itemsize, &b);
+    return b;
+}
+
+struct EventSet {
+    std::vector<cudaEvent_t> ev;
+    explicit EventSet(size_t n) : ev(n, nullptr)
+    {
+        for (auto &e : ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    }
+    ~EventSet()
+    {
+        for (auto &e : ev) if (e) cudaEventDestroy(e);
+    }
+};
+}  // namespace
+
+// The same product without the pipeline (degenerate sizes).
+static ina_rc_t opt_gemm_cframes_plain(iarray_context_t *ctx, const uint8_t *a_frame, int64_t a_len,
+                                       const uint8_t *b_frame, int64_t b_len, iarray_storage_t *storage, uint8_t *out,
+                                       int64_t out_cap, int64_t *out_len)
+{
+    iarray_container_t *a = nullptr, *b = nullptr, *c = nullptr;
+    ina_rc_t rc = iarray_from_cframe(ctx, const_cast<uint8_t *>(a_frame), a_len, true, &a);
+    if (INA_SUCCEED(rc)) rc = iarray_from_cframe(ctx, const_cast<uint8_t *>(b_frame), b_len, true, &b);
+    if (INA_SUCCEED(rc)) rc = iarray_opt_gemm(ctx, a, b, storage, &c);
+    if (INA_SUCCEED(rc)) rc = frame_into(ctx, c, out, out_cap, out_len);
+    iarray_container_free(ctx, &a);
+    iarray_container_free(ctx, &b);
+    iarray_container_free(ctx, &c);
+    return rc;
+}
+
+INA_API(ina_rc_t) iarray_b200_opt_gemm_cframes(iarray_context_t *ctx, const uint8_t *a_frame, int64_t a_len,
+                                               const uint8_t *b_frame, int64_t b_len, iarray_storage_t *storage,
+                                               uint8_t *out, int64_t out_cap, int64_t *out_len)
+{
+    CHECK_ARG(ctx && a_frame && b_frame && storage && out_len && a_len > 0 && b_len > 0 && out_cap >= 0);
+    CHECK_ARG(!storage->urlpath);
+    FrameView fa, fb;
+    ina_rc_t rc = view_frame(a_frame, a_len, &fa);
+    if (INA_FAILED(rc)) return rc;
+    rc = view_frame(b_frame, b_len, &fb);
+    if (INA_FAILED(rc)) return rc;
+    // iarray_opt_gemm's checks (src/linalg/iarray_gemm.c:327-364)
+    const int dtype = fa.fi.dtype;
+    if (dtype != fb.fi.dtype || (dtype != IARRAY_DATA_TYPE_DOUBLE && dtype != IARRAY_DATA_TYPE_FLOAT))
+        return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    if (fa.fi.shape[1] != fb.fi.shape[0]) return rc_err(IARRAY_ERR_INVALID_SHAPE);
+    const int64_t *ac = fa.fi.chunk, *bc = fb.fi.chunk, *ab = fa.fi.block, *bb = fb.fi.block;
+    if (ac[0] != storage->chunkshape[0] || ac[1] != bc[0] || bc[1] != storage->chunkshape[1])
+        return rc_err(IARRAY_ERR_INVALID_CHUNKSHAPE);
+    if (ab[0] != storage->blockshape[0] || ab[1] != bb[0] || bb[1] != storage->blockshape[1])
+        return rc_err(IARRAY_ERR_INVALID_BLOCKSHAPE);
+    const int64_t M = fa.fi.shape[0], K = fa.fi.shape[1], N = fb.fi.shape[1];
+    const bool split = ctx->form == IARRAY_B200_FORM_SPLIT;
+    if (M == 0 || N == 0 || K == 0 || (split && dtype == IARRAY_DATA_TYPE_FLOAT))
+        return opt_gemm_cframes_plain(ctx, a_frame, a_len, b_frame, b_len, storage, out, out_cap, out_len);
+
+    // output container (host object only: its geometry and frame fields)
+    iarray_dtshape_t d;
+    memset(&d, 0, sizeof(d));
+    d.dtype = (iarray_data_type_t)dtype;
+    d.ndim = 2;
+    d.shape[0] = M;
+    d.shape[1] = N;
+    iarray_container_t *cc = nullptr;
+    rc = new_container(ctx, &d, storage, &cc);
+    if (INA_FAILED(rc)) return rc;
+    std::unique_ptr<iarray_container_t, void (*)(iarray_container_t *)> cguard(cc, [](iarray_container_t *p) { delete p; });
+    cc->shuffle = true;
+    const Geom gc = cc->geom;
+    const iab::FrameInfo fic = frame_info(ctx, cc);
+    const int64_t hsize = (int64_t)iab::frame_header(fic, 0, gc.nchunks).size();
+    const int64_t tsize = (int64_t)iab::frame_tail(std::vector<int32_t>((size_t)gc.nchunks, 0)).size();
+
+    if (!ctx->up) cudaStreamCreateWithFlags(&ctx->up, cudaStreamNonBlocking);
+    if (!ctx->down) cudaStreamCreateWithFlags(&ctx->down, cudaStreamNonBlocking);
+    if (!ctx->enc) cudaStreamCreateWithFlags(&ctx->enc, cudaStreamNonBlocking);
+    if (!ctx->up || !ctx->down || !ctx->enc || !ctx->stream2) return rc_err(IARRAY_ERR_GPU_FAILED);
+    cudaStream_t st = ctx->stream;
+    const int isz = fa.g.itemsize;
+    const int64_t lda = pad_ld(K), ldb = pad_ld(N), ldc = pad_ld(N);
+    const int64_t rowsA = fa.g.cgrid[0], rowsB = fb.g.cgrid[0], bands = gc.cgrid[0];
+    DevChunks da, db;
+    DevBuf dA, dB, dC, status;
+    if (!upload_index(fa, &da, ctx->device) || !upload_index(fb, &db, ctx->device) ||
+        !dA.allocate((size_t)(M * lda * isz), ctx->device) || !dB.allocate((size_t)(K * ldb * isz), ctx->device) ||
+        !dC.allocate((size_t)(M * ldc * isz), ctx->device) ||
+        !status.allocate((size_t)(rowsA + rowsB) * 16 * 4, ctx->device))
+        return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    const size_t tab_bytes = (size_t)gc.nchunks * sizeof(iab::EncChunk);
+    if (ctx->pin_n < tab_bytes) {
+        if (ctx->pin) cudaFreeHost(ctx->pin);
+        ctx->pin = nullptr;
+        ctx->pin_n = 0;
+        if (cudaHostAlloc(&ctx->pin, tab_bytes, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+        }
+        ctx->pin_n = tab_bytes;
+    }
+    iab::EncChunk *htab = static_cast<iab::EncChunk *>(ctx->pin);
+    cudaMemsetAsync(status.p, 0, status.n, st);
+    // everything above is ordered before the uploads
+    cudaEventRecord(ctx->fork, st);
+    cudaStreamWaitEvent(ctx->up, ctx->fork, 0);
+    EventSet evB((size_t)rowsB), evA((size_t)rowsA), evE((size_t)bands);
+    for (int64_t r = 0; r < rowsB; r++) upload_row(fb, b_frame, db, r, ctx->up, evB.ev[(size_t)r]);
+    for (int64_t r = 0; r < rowsA; r++) upload_row(fa, a_frame, da, r, ctx->up, evA.ev[(size_t)r]);
+
+    // Three compute streams: the second stream decodes (B's chunk rows, then A's, each as
+    // soon as it is uploaded), the context stream prepares B and multiplies each band, the
+    // encode stream encodes each finished band.  A band's decode and the previous band's
+    // encode are both latency-bound and run side by side.
+    cudaStream_t sd = ctx->stream2, se = ctx->enc;
+    cudaStreamWaitEvent(sd, ctx->fork, 0);
+    cudaStreamWaitEvent(se, ctx->fork, 0);
+    Timer tm(ctx);                 // timings: [0] B decoded and prepared, [3] the bands, [4] total
+    tm.mark(1);
+    int err = 0;
+    EventSet evD((size_t)rowsA + 1), evP((size_t)bands);
+    std::vector<iab::DecodeWork> decB((size_t)rowsB), decA((size_t)rowsA);
+    for (int64_t r = 0; r < rowsB && !err; r++) {
+        cudaStreamWaitEvent(sd, evB.ev[(size_t)r], 0);
+        const Geom g = row_geom(fb.g, r);
+        decB[(size_t)r].ext_counters = status.as<int>() + r * 16;
+        err = iab::decode_launch(g, db.buf.as<uint8_t>(), (int64_t)db.buf.n, db.d_off.as<int64_t>() + r * fb.g.cgrid[1],
+                                 db.d_len.as<int32_t>() + r * fb.g.cgrid[1],
+                                 dB.as<uint8_t>() + r * fb.g.chunk[0] * ldb * isz, ldb, sd, &decB[(size_t)r]);
+    }
+    cudaEventRecord(evD.ev[(size_t)rowsA], sd);                 // all of B decoded
+    for (int64_t k = 0; k < rowsA && !err; k++) {
+        cudaStreamWaitEvent(sd, evA.ev[(size_t)k], 0);
+        const Geom ga = row_geom(fa.g, k);
+        decA[(size_t)k].ext_counters = status.as<int>() + (rowsB + k) * 16;
+        err = iab::decode_launch(ga, da.buf.as<uint8_t>(), (int64_t)da.buf.n, da.d_off.as<int64_t>() + k * fa.g.cgrid[1],
+                                 da.d_len.as<int32_t>() + k * fa.g.cgrid[1],
+                                 dA.as<uint8_t>() + k * fa.g.chunk[0] * lda * isz, lda, sd, &decA[(size_t)k]);
+        cudaEventRecord(evD.ev[(size_t)k], sd);
+    }
+    cudaStreamWaitEvent(st, evD.ev[(size_t)rowsA], 0);
+    iab::OzakiB ob;
+    if (!err && split) err = iab::gemm_f64_ozaki_prepare_b(K, N, dB.as<double>(), ldb, ctx->split_terms, &ob, st);
+    tm.mark(2);
+    tm.mark(3);
+    std::vector<iab::OzakiWork> oz((size_t)bands);
+    std::vector<iab::EncodeWork> enc((size_t)bands);
+    std::vector<DevBuf> cbuf((size_t)bands);
+    std::vector<int32_t> lens((size_t)gc.nchunks, 0);
+    int64_t acc = 0;
+    bool small = false;
+    // band k's chunks to the output frame (after its encode and chunk table are done)
+    auto drain = [&](int64_t k) {
+        cudaEventSynchronize(evE.ev[(size_t)k]);
+        const int64_t per = gc.cgrid[1], c0 = k * per;
+        int64_t bytes = 0, first = htab[c0].offset;
+        for (int64_t c = c0; c < c0 + per; c++) {
+            lens[(size_t)c] = htab[c].cbytes;
+            bytes += htab[c].cbytes;
+        }
+        if (hsize + acc + bytes + tsize > out_cap || !out) small = true;
+        if (!small) {
+            cudaStreamWaitEvent(ctx->down, evE.ev[(size_t)k], 0);
+            cudaMemcpyAsync(out + hsize + acc, cbuf[(size_t)k].as<uint8_t>() + first, (size_t)bytes,
+                            cudaMemcpyDeviceToHost, ctx->down);
+        }
+        acc += bytes;
+    };
+    int64_t queued = 0;            // bands whose encode is queued
+    for (int64_t k = 0; k < bands && !err; k++) {
+        cudaStreamWaitEvent(st, evD.ev[(size_t)k], 0);
+        const int64_t r0 = k * gc.chunk[0], mk = row_geom(fa.g, k).shape[0];
+        uint8_t *a_k = dA.as<uint8_t>() + r0 * lda * isz, *c_k = dC.as<uint8_t>() + r0 * ldc * isz;
+        if (split) {
+            err = iab::gemm_f64_ozaki_rows(mk, (const double *)a_k, lda, ob, (double *)c_k, ldc, &oz[(size_t)k], st);
+        } else if (dtype == IARRAY_DATA_TYPE_DOUBLE) {
+            iab::gemm_f64_native(mk, N, K, (const double *)a_k, lda, dB.as<double>(), ldb, (double *)c_k, ldc, st);
+        } else {
+            iab::gemm_f32_native(mk, N, K, (const float *)a_k, lda, dB.as<float>(), ldb, (float *)c_k, ldc, st);
+        }
+        if (err) break;
+        cudaEventRecord(evP.ev[(size_t)k], st);
+        cudaStreamWaitEvent(se, evP.ev[(size_t)k], 0);
+        const Geom gk = row_geom(gc, k);
+        iab::EncodeWork &w = enc[(size_t)k];
+        w.exact_lz4 = ctx->encoder == IARRAY_B200_ENCODER_LIBLZ4;
+        err = iab::encode_launch(gk, c_k, ldc, cc->shuffle, cc->splitmode, &cbuf[(size_t)k], &w, se);
+        if (err) break;
+        cudaMemcpyAsync(htab + k * gc.cgrid[1], w.ec.p, (size_t)gk.nchunks * sizeof(iab::EncChunk),
+                        cudaMemcpyDeviceToHost, se);
+        cudaEventRecord(evE.ev[(size_t)k], se);
+        queued = k + 1;
+        if (k > 0) drain(k - 1);
+    }
+    if (!err) drain(bands - 1);
+    // the context stream waits for the other compute streams before the final timestamp
+    cudaEventRecord(ctx->join, sd);
+    cudaStreamWaitEvent(st, ctx->join, 0);
+    if (queued) cudaStreamWaitEvent(st, evE.ev[(size_t)queued - 1], 0);
+    tm.mark(4);
+    const cudaError_t ce1 = cudaStreamSynchronize(st), ce2 = cudaStreamSynchronize(ctx->down),
+                      ce3 = cudaStreamSynchronize(ctx->up), ce4 = cudaStreamSynchronize(sd),
+                      ce5 = cudaStreamSynchronize(se);
+    tm.finish();
+    if (err == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    if (err || ce1 != cudaSuccess || ce2 != cudaSuccess || ce3 != cudaSuccess || ce4 != cudaSuccess ||
+        ce5 != cudaSuccess)
+        return rc_err(IARRAY_ERR_GPU_FAILED);
+    // decode status words, then the split product's error flags
+    std::vector<int> hs((size_t)(rowsA + rowsB) * 16);
+    if (cudaMemcpy(hs.data(), status.p, hs.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return rc_err(IARRAY_ERR_GPU_FAILED);
+    for (int64_t r = 0; r < rowsA + rowsB; r++)
+        if (hs[(size_t)(r * 16 + 1)]) return rc_err(IARRAY_ERR_BLOSC_FAILED);
+    for (auto &w : oz)
+        if (w.err.p && iab::gemm_f64_ozaki_finish(&w, st)) return rc_err(IARRAY_ERR_GPU_FAILED);
+    *out_len = hsize + acc + tsize;
+    if (small) return rc_err(IARRAY_ERR_TOO_SMALL_BUFFER);
+    const std::vector<uint8_t> head = iab::frame_header(fic, acc, gc.nchunks);
+    const std::vector<uint8_t> tail = iab::frame_tail(lens);
+    memcpy(out, head.data(), head.size());
+    memcpy(out + hsize + acc, tail.data(), tail.size());
+    return INA_SUCCESS;
 }
 
 // ============================================================================ batched products

@@ -211,11 +211,26 @@ void gemm_f64_grouped(int cfg, const GemmProblem *d_probs, int nprob, int total_
 int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda,
                    const double *B, int64_t ldb, double *C, int64_t ldc, int nterms, cudaStream_t st);
 // Asynchronous form with caller-owned work buffers (no host synchronisation until finish).
+// The B side (column scaling, residues, tensor map) is prepared once and can serve several
+// row bands of A (gemm_f64_ozaki_rows), each with its own OzakiWork.
+struct OzakiB {
+    DevBuf rb, sb, pm, ps;
+    int L = 0, nc = 0;
+    int64_t K = 0, N = 0, Kp = 0;
+    double gamma = 0;
+    const double *B = nullptr;
+    int64_t ldb = 0;
+    alignas(64) unsigned char tmB[128];   // CUtensorMap of the residues of B
+};
 struct OzakiWork {
-    DevBuf ra, rb, rr, sa, sb, pm, ps, err;
+    DevBuf ra, rr, sa, err;
+    OzakiB b;                              // used by gemm_f64_ozaki_launch
 };
 int gemm_f64_ozaki_launch(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B,
                           int64_t ldb, double *C, int64_t ldc, int nterms, OzakiWork *w, cudaStream_t st);
+int gemm_f64_ozaki_prepare_b(int64_t K, int64_t N, const double *B, int64_t ldb, int nterms, OzakiB *ob, cudaStream_t st);
+int gemm_f64_ozaki_rows(int64_t M, const double *A, int64_t lda, const OzakiB &ob, double *C, int64_t ldc,
+                        OzakiWork *w, cudaStream_t st);
 int gemm_f64_ozaki_finish(OzakiWork *w, cudaStream_t st);
 int gemm_f32_bf16x3(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda,
                     const float *B, int64_t ldb, float *C, int64_t ldc, cudaStream_t st);

@@ -4,9 +4,9 @@
 //
 //   1. Scaling.  Row i of A is scaled by 2^sA_i and rounded to an integer matrix A'
 //      (|A'_ik| < 2^52), column j of B by 2^sB_j -> B'.  The shifts are chosen from the
-//      row / column 2-norms so that ||A'_i||_2 * ||B'_j||_2 < P / 2, where P is the
+//      row / column 2-norms so that ||A'_i||_2 * ||B'_j||_2 < P / 8, where P is the
 //      product of the moduli; by Cauchy-Schwarz every entry of C' = A' B' then lies in
-//      (-P/2, P/2) and is recovered exactly from its residues.
+//      (-P/8, P/8) and is recovered exactly from its residues.
 //   2. Residues.  For each modulus m_l (pairwise coprime, <= 256) the symmetric residues
 //      A'_l = A' mod m_l and B'_l = B' mod m_l fit in int8 (B'_l is stored transposed,
 //      K-major, for the tensor-core operand layout).
@@ -282,23 +282,36 @@ __device__ __forceinline__ double rint52(double y)
     return (y + c) - c;
 }
 
-// rint(a * 2^s): the scaled, rounded entry of an operand row or column.
-__device__ __forceinline__ double scaled_int(double a, int s, bool pow2_ok, double f)
+// x = rint(a * 2^s), the scaled entry of an operand row or column (|x| < 2^52), and the low
+// 32 bits of x as an integer: y + copysign(2^52, y) holds |x| in its mantissa field.
+__device__ __forceinline__ double scaled_int(double a, int s, bool pow2_ok, double f, uint32_t &xlo)
 {
-    return pow2_ok ? rint52(a * f) : rint(ldexp(a, s));
+    const double y = pow2_ok ? a * f : ldexp(a, s);
+    if (!pow2_ok) {
+        const double x = rint(y);
+        xlo = (uint32_t)__double2ll_rn(x);
+        return x;
+    }
+    const double c = copysign(kTwo52, y);
+    const double t = y + c;
+    const uint32_t mag = (uint32_t)__double2loint(t);
+    xlo = y < 0.0 ? 0u - mag : mag;
+    return t - c;
 }
 
-// Symmetric residue of the integer-valued x (|x| < 2^52) modulo m_l.
-__device__ __forceinline__ int sym_residue(double x, int l)
+// Residue of the integer x (|x| < 2^52, low 32 bits xlo) modulo m_l, as the byte of an int8
+// in [-128, 127].  The INT8 products need only some representative of the class, not the
+// centred one.  l = 0 is m = 256: the low byte.  Otherwise q = rint(x / m) comes from one
+// FMA (its low 32 bits sit in the low word of x / m + 1.5 * 2^52); q may be one off near a
+// half-integer, so x - q m lies in [-m/2 - 1, m/2 + 1] and one correction brings it below 128.
+__device__ __forceinline__ uint32_t residue_byte(double x, uint32_t xlo, int l)
 {
-    const int m = c_crt.mod[l];
-    const double q = fma(x, c_crt.inv_mod[l], kRound) - kRound;    // rint(x / m), or one off
-    int r = __double2loint(fma(-q, (double)m, x) + kRound);         // x - q m, exact, |.| < 1.5 m
-    const int hi = (m == 256) ? 127 : (m - 1) / 2;
-    const int lo = (m == 256) ? -128 : -(m - 1) / 2;
-    if (r > hi) r -= m;
-    if (r < lo) r += m;
-    return r;
+    if (l == 0) return xlo & 0xffu;
+    const uint32_t m = (uint32_t)c_crt.mod[l];
+    const uint32_t q = (uint32_t)__double2loint(fma(x, c_crt.inv_mod[l], kRound));
+    int r = (int)(xlo - q * m);
+    if (r > 127) r -= (int)m;
+    return (uint32_t)r & 0xffu;
 }
 
 // A (M x K, row-major) -> res[l][i][k] (int8, row pitch Kp), 8 consecutive k per thread.
@@ -314,19 +327,21 @@ __global__ void __launch_bounds__(256) k_residues_rows(int M, int K, int Kp, con
         const bool p2 = s >= -1022 && s <= 1023, fin = s != kNonFinite;
         const double f = p2 ? pow2i(s) : 0.0;
         double x[8];
+        uint32_t xl[8];
 #pragma unroll
         for (int u = 0; u < 8; u++) {
             const int k = k0 + u;
-            x[u] = k < K && fin ? scaled_int(A[(int64_t)i * lda + k], s, p2, f) : 0.0;
+            xl[u] = 0u;
+            x[u] = k < K && fin ? scaled_int(A[(int64_t)i * lda + k], s, p2, f, xl[u]) : 0.0;
         }
 #pragma unroll
         for (int l = 0; l < 16; l++) {
             if (l < L) {
                 uint32_t w0 = 0, w1 = 0;
 #pragma unroll
-                for (int u = 0; u < 4; u++) w0 |= (uint32_t)(uint8_t)sym_residue(x[u], l) << (8 * u);
+                for (int u = 0; u < 4; u++) w0 |= residue_byte(x[u], xl[u], l) << (8 * u);
 #pragma unroll
-                for (int u = 0; u < 4; u++) w1 |= (uint32_t)(uint8_t)sym_residue(x[4 + u], l) << (8 * u);
+                for (int u = 0; u < 4; u++) w1 |= residue_byte(x[4 + u], xl[4 + u], l) << (8 * u);
                 *reinterpret_cast<uint2 *>(res + ((int64_t)l * M + i) * Kp + k0) = make_uint2(w0, w1);
             }
         }
@@ -354,16 +369,20 @@ __global__ void __launch_bounds__(256) k_residues_cols(int K, int N, int Kp, con
         const bool p2 = s >= -1022 && s <= 1023, fin = s != kNonFinite;
         const double f = p2 ? pow2i(s) : 0.0;
         double x[8];
+        uint32_t xl[8];
 #pragma unroll
-        for (int u = 0; u < 8; u++) x[u] = fin ? scaled_int(tile[kg + u][c], s, p2, f) : 0.0;
+        for (int u = 0; u < 8; u++) {
+            xl[u] = 0u;
+            x[u] = fin ? scaled_int(tile[kg + u][c], s, p2, f, xl[u]) : 0.0;
+        }
 #pragma unroll
         for (int l = 0; l < 16; l++) {
             if (l < L) {
                 uint32_t w0 = 0, w1 = 0;
 #pragma unroll
-                for (int u = 0; u < 4; u++) w0 |= (uint32_t)(uint8_t)sym_residue(x[u], l) << (8 * u);
+                for (int u = 0; u < 4; u++) w0 |= residue_byte(x[u], xl[u], l) << (8 * u);
 #pragma unroll
-                for (int u = 0; u < 4; u++) w1 |= (uint32_t)(uint8_t)sym_residue(x[4 + u], l) << (8 * u);
+                for (int u = 0; u < 4; u++) w1 |= residue_byte(x[4 + u], xl[4 + u], l) << (8 * u);
                 *reinterpret_cast<uint2 *>(res + ((int64_t)l * N + j) * Kp + k0 + kg) = make_uint2(w0, w1);
             }
         }
@@ -553,9 +572,10 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
 // comes from a rounded estimate of S: the scaling keeps |X| below P / 8 (both norms are
 // held to 2^(gamma - 1)), so S / P stays far from a half-integer compared with the
 // estimate's error (about 2^-39 of one unit), and q is exact.  Then every
-// D_k = S_k - q P_k is exact (q P_k < 2^52) and X = sum_k D_k 2^(40 k) is formed by Horner
-// steps whose intermediates are exact or within a factor 1.5 of |X|: error at most about
-// 1.5 ulp of X.
+// D_k = S_k - q P_k is exact (q P_k < 2^52); with the low chunks carried into [0, 2^40),
+// X = sum_k D_k 2^(40 k) is formed by Horner steps that are exact whenever X is
+// representable (every partial floor(X / 2^(40 j)) then is too) and round at most twice
+// otherwise.
 template <int NC>
 __device__ __forceinline__ double crt_value(const double (&S)[NC])
 {
@@ -563,9 +583,20 @@ __device__ __forceinline__ double crt_value(const double (&S)[NC])
 #pragma unroll
     for (int k = NC - 2; k >= 0; k--) s = fma(s, kTwo40, S[k]);
     const double q = fma(s, c_crt.inv_p, kRound) - kRound;
-    double x = fma(-q, c_crt.pf[NC - 1], S[NC - 1]);
+    double D[NC];
 #pragma unroll
-    for (int k = NC - 2; k >= 0; k--) x = fma(x, kTwo40, fma(-q, c_crt.pf[k], S[k]));
+    for (int k = 0; k < NC; k++) D[k] = fma(-q, c_crt.pf[k], S[k]);
+    // carry the low chunks into [0, 2^40) (every step exact: integers below 2^53); then the
+    // Horner sum is exact whenever X is representable, and within one rounding otherwise
+#pragma unroll
+    for (int k = 0; k < NC - 1; k++) {
+        const double c = floor(D[k] * 0x1p-40);
+        D[k] = fma(-c, kTwo40, D[k]);
+        D[k + 1] += c;
+    }
+    double x = D[NC - 1];
+#pragma unroll
+    for (int k = NC - 2; k >= 0; k--) x = fma(x, kTwo40, D[k]);
     return x;
 }
 
@@ -680,53 +711,79 @@ int gemm_f64_ozaki_finish(OzakiWork *w, cudaStream_t st)
     return h_err ? -3 : 0;
 }
 
-int gemm_f64_ozaki_launch(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B, int64_t ldb,
-                          double *C, int64_t ldc, int nterms, OzakiWork *w, cudaStream_t st)
+// CRT constants for L moduli, copied to the device constant bank on `st`.
+static bool set_crt(int L, CrtConst *out, cudaStream_t st)
 {
-    if (!device_is_sm100()) return -1;
-    if (M <= 0 || N <= 0 || K <= 0) return 0;
-    // |sum_k a*b| <= K * 2^14 must keep the epilogue's float quotient within one of the
-    // true quotient (K * 2^14 * 2^-24 / 173 < 0.5) and the int32 accumulator exact
-    if (K > 65536 || M > (1 << 30) || N > (1 << 30)) return -1;
-    const int L = nterms > 0 ? nterms : 14;
     static std::mutex mu;
     static CrtConst cached;
     static int cached_L = -1;
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        if (cached_L != L) {
-            if (!build_crt(L, &cached)) return -1;
-            cached_L = L;
-        }
-        if (cudaMemcpyToSymbolAsync(c_crt, &cached, sizeof(CrtConst), 0, cudaMemcpyHostToDevice, st) != cudaSuccess)
-            return -1;
+    std::lock_guard<std::mutex> lk(mu);
+    if (cached_L != L) {
+        if (!build_crt(L, &cached)) return false;
+        cached_L = L;
     }
-    const double gamma = (cached.log2p - 1.0) / 2.0 - 0.01;
+    *out = cached;
+    return cudaMemcpyToSymbolAsync(c_crt, &cached, sizeof(CrtConst), 0, cudaMemcpyHostToDevice, st) == cudaSuccess;
+}
+
+int gemm_f64_ozaki_prepare_b(int64_t K, int64_t N, const double *B, int64_t ldb, int nterms, OzakiB *ob, cudaStream_t st)
+{
+    if (!device_is_sm100()) return -1;
+    // |sum_k a*b| <= K * 2^14 must keep the epilogue's float quotient within one of the
+    // true quotient (K * 2^14 * 2^-24 / 173 < 0.5) and the int32 accumulator exact
+    if (K <= 0 || N <= 0 || K > 65536 || N > (1 << 30)) return -1;
+    const int L = nterms > 0 ? nterms : 14;
+    CrtConst cc;
+    if (!set_crt(L, &cc, st)) return -1;
     int dev = 0;
     cudaGetDevice(&dev);
-    const int64_t Kp = round_up(K, oz::BK);
+    ob->L = L;
+    ob->nc = cc.nc;
+    ob->K = K;
+    ob->N = N;
+    ob->Kp = round_up(K, oz::BK);
+    ob->gamma = (cc.log2p - 1.0) / 2.0 - 0.01;
+    ob->B = B;
+    ob->ldb = ldb;
+    const int64_t Kp = ob->Kp;
+    if (!ob->rb.allocate((size_t)(L * N * Kp), dev) || !ob->sb.allocate((size_t)N * 4, dev) ||
+        !ob->pm.allocate((size_t)COL_SEGS * N * 8, dev) || !ob->ps.allocate((size_t)COL_SEGS * N * 8, dev))
+        return -100;
+    IAB_TIMED("k_col_partial", st, k_col_partial<<<dim3((unsigned)((N + 255) / 256), COL_SEGS), 256, 0, st>>>(
+        (int)K, (int)N, B, ldb, ob->pm.as<double>(), ob->ps.as<double>()));
+    IAB_TIMED("k_col_shift", st, k_col_shift<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(
+        (int)K, (int)N, B, ldb, ob->pm.as<double>(), ob->ps.as<double>(), ob->gamma, ob->sb.as<int>()));
+    IAB_TIMED("k_residues_cols", st, k_residues_cols<<<dim3((unsigned)((N + 63) / 64), (unsigned)((Kp + 63) / 64)), 256, 0, st>>>(
+        (int)K, (int)N, (int)Kp, B, ldb, ob->sb.as<int>(), ob->rb.as<int8_t>()));
+    static_assert(sizeof(CUtensorMap) <= sizeof(ob->tmB), "tensor map storage");
+    if (!make_tmap_3d(reinterpret_cast<CUtensorMap *>(ob->tmB), CU_TENSOR_MAP_DATA_TYPE_UINT8, ob->rb.p, (uint64_t)Kp,
+                      (uint64_t)N, (uint64_t)L, (uint64_t)Kp, (uint64_t)(Kp * N), oz::BK, oz::BN,
+                      CU_TENSOR_MAP_SWIZZLE_128B))
+        return -1;
+    return 0;
+}
+
+int gemm_f64_ozaki_rows(int64_t M, const double *A, int64_t lda, const OzakiB &ob, double *C, int64_t ldc,
+                        OzakiWork *w, cudaStream_t st)
+{
+    if (M <= 0) return 0;
+    if (M > (1 << 30)) return -1;
+    const int L = ob.L;
+    const int64_t N = ob.N, K = ob.K, Kp = ob.Kp;
     const int64_t ldr = round_up(N, 16);
-    DevBuf &ra = w->ra, &rb = w->rb, &rr = w->rr, &sa = w->sa, &sb = w->sb, &pm = w->pm, &ps = w->ps, &err = w->err;
-    if (!ra.allocate((size_t)(L * M * Kp), dev) || !rb.allocate((size_t)(L * N * Kp), dev) ||
-        !rr.allocate((size_t)(L * M * ldr), dev) || !sa.allocate((size_t)M * 4, dev) ||
-        !sb.allocate((size_t)N * 4, dev) || !pm.allocate((size_t)COL_SEGS * N * 8, dev) ||
-        !ps.allocate((size_t)COL_SEGS * N * 8, dev) || !err.allocate(16, dev))
+    int dev = 0;
+    cudaGetDevice(&dev);
+    DevBuf &ra = w->ra, &rr = w->rr, &sa = w->sa, &err = w->err;
+    if (!ra.allocate((size_t)(L * M * Kp), dev) || !rr.allocate((size_t)(L * M * ldr), dev) ||
+        !sa.allocate((size_t)M * 4, dev) || !err.allocate(16, dev))
         return -100;
     cudaMemsetAsync(err.p, 0, 16, st);
     const int nsm = sms();
-    IAB_TIMED("k_row_shift", st, k_row_shift<<<(unsigned)((M * 32 + 255) / 256), 256, 0, st>>>((int)M, (int)K, A, lda, gamma, sa.as<int>()));
-    IAB_TIMED("k_col_partial", st, k_col_partial<<<dim3((unsigned)((N + 255) / 256), COL_SEGS), 256, 0, st>>>((int)K, (int)N, B, ldb, pm.as<double>(),
-                                                                               ps.as<double>()));
-    IAB_TIMED("k_col_shift", st, k_col_shift<<<(unsigned)((N + 255) / 256), 256, 0, st>>>((int)K, (int)N, B, ldb, pm.as<double>(), ps.as<double>(), gamma, sb.as<int>()));
+    IAB_TIMED("k_row_shift", st, k_row_shift<<<(unsigned)((M * 32 + 255) / 256), 256, 0, st>>>((int)M, (int)K, A, lda, ob.gamma, sa.as<int>()));
     IAB_TIMED("k_residues_rows", st, k_residues_rows<<<(unsigned)(nsm * 16), 256, 0, st>>>((int)M, (int)K, (int)Kp, A, lda, sa.as<int>(), ra.as<int8_t>()));
-    IAB_TIMED("k_residues_cols", st, k_residues_cols<<<dim3((unsigned)((N + 63) / 64), (unsigned)((Kp + 63) / 64)), 256, 0, st>>>(
-        (int)K, (int)N, (int)Kp, B, ldb, sb.as<int>(), rb.as<int8_t>()));
-
-    CUtensorMap tmA, tmB;
+    CUtensorMap tmA;
     if (!make_tmap_3d(&tmA, CU_TENSOR_MAP_DATA_TYPE_UINT8, ra.p, (uint64_t)Kp, (uint64_t)M, (uint64_t)L, (uint64_t)Kp,
-                      (uint64_t)(Kp * M), oz::BK, oz::BM, CU_TENSOR_MAP_SWIZZLE_128B) ||
-        !make_tmap_3d(&tmB, CU_TENSOR_MAP_DATA_TYPE_UINT8, rb.p, (uint64_t)Kp, (uint64_t)N, (uint64_t)L, (uint64_t)Kp,
-                      (uint64_t)(Kp * N), oz::BK, oz::BN, CU_TENSOR_MAP_SWIZZLE_128B))
+                      (uint64_t)(Kp * M), oz::BK, oz::BM, CU_TENSOR_MAP_SWIZZLE_128B))
         return -1;
     I8Params prm;
     prm.M = (int)M; prm.N = (int)N; prm.Kp = (int)Kp; prm.L = L;
@@ -738,10 +795,22 @@ int gemm_f64_ozaki_launch(int64_t M, int64_t N, int64_t K, const double *A, int6
         attr = true;
     }
     const int tiles = L * prm.tiles_m * prm.tiles_n;
+    const CUtensorMap &tmB = *reinterpret_cast<const CUtensorMap *>(ob.tmB);
     IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
-    launch_crt(cached.nc, (unsigned)(nsm * 8), (int)M, (int)N, rr.as<uint8_t>(), ldr, sa.as<int>(), sb.as<int>(), C, ldc, st);
-    launch_nonfinite_fix<double>(M, N, K, A, lda, B, ldb, C, ldc, sa.as<int>(), sb.as<int>(), kNonFinite, st);
+    launch_crt(ob.nc, (unsigned)(nsm * 8), (int)M, (int)N, rr.as<uint8_t>(), ldr, sa.as<int>(), ob.sb.as<int>(), C, ldc, st);
+    launch_nonfinite_fix<double>(M, N, K, A, lda, ob.B, ob.ldb, C, ldc, sa.as<int>(), ob.sb.as<int>(), kNonFinite, st);
     return 0;
+}
+
+int gemm_f64_ozaki_launch(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B, int64_t ldb,
+                          double *C, int64_t ldc, int nterms, OzakiWork *w, cudaStream_t st)
+{
+    if (!device_is_sm100()) return -1;
+    if (M <= 0 || N <= 0 || K <= 0) return 0;
+    if (K > 65536 || M > (1 << 30) || N > (1 << 30)) return -1;
+    const int r = gemm_f64_ozaki_prepare_b(K, N, B, ldb, nterms, &w->b, st);
+    if (r) return r;
+    return gemm_f64_ozaki_rows(M, A, lda, w->b, C, ldc, w, st);
 }
 
 // ============================================================================ float32: 3xBF16

@@ -120,6 +120,7 @@ def _lib():
             "iarray_b200_decode_to_device": ([P, P, P, I64], RC),
             "iarray_b200_encode_from_device": ([P, P, P, I64, P, P], RC),
             "iarray_b200_dense_gemm": ([P, ctypes.c_int, I64, I64, I64, P, I64, P, I64, P, I64], RC),
+            "iarray_b200_opt_gemm_cframes": ([P, P, I64, P, I64, P, P, I64, P], RC),
             "iarray_b200_synchronize": ([P], RC),
             "iarray_b200_kernel_launches": ([], ctypes.c_uint64),
             "iarray_b200_get_stream": ([P, P], RC),
@@ -403,6 +404,37 @@ def matmul(ctx, a, b, chunkshape, blockshape, urlpath=None):
 
 def opt_gemm(ctx, a, b, chunkshape, blockshape):
     return _product(_lib().iarray_opt_gemm, "iarray_opt_gemm", ctx, a, b, chunkshape, blockshape)
+
+
+def opt_gemm_cframes(ctx, a_frame, b_frame, chunkshape, blockshape, out=None):
+    """iarray_b200_opt_gemm_cframes: A and B as contiguous frames in host memory (bytes or
+    uint8 numpy arrays, ideally pinned), C's frame written into `out` (a uint8 numpy array;
+    allocated with the documented upper bound when None).  Returns (out, frame length)."""
+    def buf(x):
+        if isinstance(x, np.ndarray):
+            return x.ctypes.data_as(ctypes.c_void_p), x.nbytes
+        b = ctypes.create_string_buffer(bytes(x), len(x))
+        return ctypes.cast(b, ctypes.c_void_p), len(x), b
+    pa, pb = buf(a_frame), buf(b_frame)
+    s = storage(chunkshape, blockshape)
+    n = ctypes.c_int64()
+    if out is None:
+        hdr = read_frame_shapes(a_frame, b_frame)
+        out = np.empty(hdr, np.uint8)
+    check(_lib().iarray_b200_opt_gemm_cframes(ctx.ptr, pa[0], pa[1], pb[0], pb[1], ctypes.byref(s),
+                                              out.ctypes.data_as(ctypes.c_void_p), out.nbytes, ctypes.byref(n)),
+          "iarray_b200_opt_gemm_cframes")
+    return out, n.value
+
+
+def read_frame_shapes(a_frame, b_frame):
+    """Upper bound of the C frame size for two operand frames (their containers' shapes)."""
+    ctx = Context()
+    a = Container.from_cframe(ctx, bytes(a_frame))
+    b = Container.from_cframe(ctx, bytes(b_frame))
+    (m, _), (_, n) = a.shape, b.shape
+    isz = np.dtype(a.dtype).itemsize
+    return m * n * isz * 2 + 64 * 1024 + (1 << 20)
 
 
 def opt_gemm_a(ctx, a, b, chunkshape, blockshape):

@@ -191,20 +191,28 @@ def test_matmul_persists_output_when_urlpath_given(ctx, ia, tmp_path):
     assert np.array_equal(ia.Container.open(ctx, p).to_numpy(), C.to_numpy())
 
 
+@pytest.mark.parametrize("form", ["native", "split"])
 @pytest.mark.parametrize("K", [33, 1, 129])
-def test_native_f64_odd_k_reads_nothing_past_the_row(ctx, ia, K):
-    """Dense operands pad their rows to a multiple of 32 items and the padding is never
-    written: a product with odd K must not read it.  A first product of the same dense size
-    leaves NaN in recycled device buffers; the second must still be exact."""
+def test_dense_f64_reads_nothing_past_k(ctx, ia, K, form):
+    """Dense operands have rows padded past K (leading dimension a multiple of 32) and
+    nothing writes the padding.  NaN planted there must not reach C: every product reads
+    only the K columns of A (and the K rows of B)."""
+    import ctypes
+    import torch
     M, N = 100, 50
-    ld = (K + 31) // 32 * 32
-    nan_a = np.full((M, ld), np.nan)
-    nan_b = np.full((ld, N), np.nan)
-    ia.opt_gemm(ctx, ia.Container.from_numpy(ctx, nan_a, (M, ld), (20, ld)),
-                ia.Container.from_numpy(ctx, nan_b, (ld, N), (ld, 10)), (M, N), (20, 10)).free()
+    lda, ldb, ldc = (K + 31) // 32 * 32, 64, 64
     rng = np.random.default_rng(K)
-    A = rng.integers(-8, 9, (M, K)).astype(np.float64)
-    B = rng.integers(-8, 9, (K, N)).astype(np.float64)
-    C = ia.opt_gemm(ctx, ia.Container.from_numpy(ctx, A, (M, K), (20, K)),
-                    ia.Container.from_numpy(ctx, B, (K, N), (K, 10)), (M, N), (20, 10)).to_numpy()
-    assert np.array_equal(C, A @ B)
+    a = rng.integers(-8, 9, (M, K)).astype(np.float64)
+    b = rng.integers(-8, 9, (K, N)).astype(np.float64)
+    A = torch.full((M, lda), float("nan"), dtype=torch.float64, device="cuda")
+    B = torch.full((K + 3, ldb), float("nan"), dtype=torch.float64, device="cuda")
+    A[:, :K] = torch.from_numpy(a).cuda()
+    B[:K, :N] = torch.from_numpy(b).cuda()
+    C = torch.zeros((M, ldc), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()          # the library's stream does not wait for torch's
+    c = ia.Context(form=ia.FORM_SPLIT if form == "split" else ia.FORM_NATIVE)
+    ia.check(ia.lib().iarray_b200_dense_gemm(c.ptr, ia.DTYPE_DOUBLE, M, N, K, ctypes.c_void_p(A.data_ptr()), lda,
+                                              ctypes.c_void_p(B.data_ptr()), ldb, ctypes.c_void_p(C.data_ptr()), ldc),
+             "dense_gemm")
+    c.synchronize()
+    assert np.array_equal(C[:, :N].cpu().numpy(), a @ b)
