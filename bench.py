@@ -593,6 +593,47 @@ def run_ours(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_case(args):
+    """Small cases for ncu captures (--set full on one kernel family at a time).
+    codec: a 4096 x 4096 float64 container of the product's kind of values (gaussian) encoded
+    with the parallel encoder, then an A-like one (uniform(-1,1) x 2^U{-8..8}) decoded; three
+    rounds each.  split: the split-precision float64 product 4096 x 4096 x 4096 on device
+    operands (iarray_b200_dense_gemm), two rounds.  Inputs are larger than L2."""
+    import ctypes
+    import torch
+    import iarray_b200 as ia
+    ia.init()
+    rng = np.random.default_rng(5)
+    n = 4096
+    if args.profile_case == "codec":
+        ctx = ia.Context(encoder=ia.ENCODER_PARALLEL)
+        C = rng.standard_normal((n, n)) * 600.0
+        A = rng.uniform(-1, 1, (n, n)) * np.exp2(rng.integers(-8, 9, (n, n)))
+        for _ in range(3):
+            ia.Container.from_numpy(ctx, C, (2048, 2048), (256, 256)).free()
+        a = ia.Container.from_numpy(ctx, A, (2048, 2048), (256, 256))
+        out = torch.empty((n, n), dtype=torch.float64, device="cuda")
+        for _ in range(3):
+            a.decode_to_device(out.data_ptr(), n)
+        ctx.synchronize()
+        assert np.array_equal(out.cpu().numpy(), A)
+    else:
+        ctx = ia.Context(form=ia.FORM_SPLIT)
+        A = torch.from_numpy(rng.uniform(-1, 1, (n, n)) * np.exp2(rng.integers(-8, 9, (n, n)))).cuda()
+        B = torch.from_numpy(rng.uniform(-1, 1, (n, n)) * np.exp2(rng.integers(-8, 9, (n, n)))).cuda()
+        C = torch.empty((n, n), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        for _ in range(2):
+            ia.check(ia.lib().iarray_b200_dense_gemm(ctx.ptr, ia.DTYPE_DOUBLE, n, n, n, ctypes.c_void_p(A.data_ptr()), n,
+                                                      ctypes.c_void_p(B.data_ptr()), n, ctypes.c_void_p(C.data_ptr()), n),
+                     "dense_gemm")
+        ctx.synchronize()
+        ref = (A[:64] @ B).cpu().numpy()
+        err = np.linalg.norm(C[:64].cpu().numpy() - ref) / np.linalg.norm(ref)
+        assert err < 1e-13, err
+    print(json.dumps({"profile_case": args.profile_case, "ok": True}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -602,8 +643,12 @@ def main():
     ap.add_argument("--err-rows", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the GEMV, float32 and batching workloads")
+    ap.add_argument("--profile-case", choices=["codec", "split"], default=None,
+                    help="run one small case for an ncu capture instead of the benchmark")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile_case:
+        run_profile_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -1535,53 +1535,132 @@ __global__ void __launch_bounds__(PT, 7) k_lz4_encode_par(const uint8_t *__restr
     }
 }
 
-// E3: per chunk, walk streams in order as blosc_c does, assigning offsets and deciding
-// the memcpy fallback (destination capacity nbytes + 32); then scan chunk sizes.
-__global__ void k_layout(Geom g, int nstreams, int neblock, EncStream *es, EncChunk *ec, int64_t *total)
+// E3: per chunk (one CTA each), the stream layout blosc_c produces: streams in order, each a
+// 4-byte csize word and its payload (a run: one byte or none), an LZ4 stream only where its
+// output fits the space left (else raw); a chunk that does not fit nbytes + 32 is stored
+// memcpyed.  The space left only binds near the end of a chunk, so sizes are prefix-summed
+// as if it never binds, and thread 0 replays the stream-by-stream walk from the first stream
+// where it could.
+constexpr int LAYOUT_T = 256;
+
+// The blosc_c walk for one stream from running size ntb; false: the chunk does not fit.
+__device__ __forceinline__ bool layout_step(EncStream &e, int64_t &ntb, int64_t destsize, int neblock)
 {
-    const int64_t destsize = g.chunk_nbytes + 32;
-    for (int64_t c = threadIdx.x; c < g.nchunks; c += blockDim.x) {
-        int64_t ntb = 32 + 4 * g.nblocks;
-        bool ok = ntb <= destsize;
-        for (int64_t b = 0; ok && b < g.nblocks; b++) {
-            for (int j = 0; j < nstreams; j++) {
-                EncStream &e = es[(c * g.nblocks + b) * nstreams + j];
-                ntb += 4;
-                if (e.kind == SK_RUN) {
-                    if (ntb > destsize) { ok = false; break; }
-                    e.out = (int32_t)(ntb - 4);
-                    if (e.csize != 0) {
-                        if (ntb + 1 > destsize) { ok = false; break; }
-                        ntb += 1;
-                    }
-                    continue;
-                }
-                int64_t maxout = neblock;
-                if (ntb + maxout > destsize) {
-                    maxout = destsize - ntb;
-                    if (maxout <= 0) { ok = false; break; }
-                }
-                int64_t sz;
-                if (e.kind == SK_LZ4 && e.need <= maxout) {
-                    sz = e.csize;
-                } else {
-                    if (ntb + neblock > destsize) { ok = false; break; }
-                    e.kind = SK_RAW;
-                    sz = neblock;
-                }
-                e.out = (int32_t)(ntb - 4);
-                ntb += sz;
-            }
+    ntb += 4;
+    if (e.kind == SK_RUN) {
+        if (ntb > destsize) return false;
+        e.out = (int32_t)(ntb - 4);
+        if (e.csize != 0) {
+            if (ntb + 1 > destsize) return false;
+            ntb += 1;
+        }
+        return true;
+    }
+    int64_t maxout = neblock;
+    if (ntb + maxout > destsize) {
+        maxout = destsize - ntb;
+        if (maxout <= 0) return false;
+    }
+    int64_t sz;
+    if (e.kind == SK_LZ4 && e.need <= maxout) {
+        sz = e.csize;
+    } else {
+        if (ntb + neblock > destsize) return false;
+        e.kind = SK_RAW;
+        sz = neblock;
+    }
+    e.out = (int32_t)(ntb - 4);
+    ntb += sz;
+    return true;
+}
+
+__global__ void __launch_bounds__(LAYOUT_T) k_layout(Geom g, int nstreams, int neblock, EncStream *es, EncChunk *ec)
+{
+    __shared__ int64_t wsum[LAYOUT_T / 32];
+    __shared__ int64_t s_before;
+    __shared__ int s_first;
+    const int64_t c = blockIdx.x;
+    const int64_t destsize = g.chunk_nbytes + 32, ns = g.nblocks * nstreams;
+    const int64_t ntb0 = 32 + 4 * g.nblocks;
+    EncStream *e0 = es + c * ns;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_first = 0x7FFFFFFF;
+    __syncthreads();
+    int64_t base = ntb0;
+    for (int64_t r0 = 0; ntb0 <= destsize && r0 < ns; r0 += LAYOUT_T) {
+        const int64_t i = r0 + threadIdx.x;
+        EncStream e;
+        e.kind = SK_RAW; e.csize = 0; e.need = 0; e.out = -1;
+        int64_t sz = 0;
+        if (i < ns) {
+            e = e0[i];
+            sz = e.kind == SK_RUN ? 4 + (e.csize != 0) : e.kind == SK_LZ4 ? 4 + (int64_t)e.csize : 4 + (int64_t)neblock;
+        }
+        int64_t incl = sz;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t t = __shfl_up_sync(FULLMASK, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        int64_t before = base + incl - sz, all = 0;
+#pragma unroll
+        for (int w = 0; w < LAYOUT_T / 32; w++) {
+            before += w < warp ? wsum[w] : 0;
+            all += wsum[w];
+        }
+        // the unconstrained choice holds while the stream (raw, at worst) still fits
+        const bool safe = e.kind == SK_RUN ? before + sz <= destsize
+                                           : before + 4 + neblock <= destsize && (e.kind != SK_LZ4 || e.need <= neblock);
+        if (i < ns && !safe) atomicMin(&s_first, (int)i);
+        __syncthreads();
+        const int first = s_first;
+        if (i < ns && i < first) e0[i].out = (int32_t)before;
+        if (i == first) s_before = before;
+        base += all;
+        __syncthreads();
+        if (first != 0x7FFFFFFF) break;
+    }
+    if (threadIdx.x == 0) {
+        bool ok = ntb0 <= destsize;
+        int64_t ntb = base;
+        if (ok && s_first != 0x7FFFFFFF) {
+            ntb = s_before;
+            for (int64_t i = s_first; ok && i < ns; i++) ok = layout_step(e0[i], ntb, destsize, neblock);
         }
         ec[c].memcpyed = ok ? 0 : 1;
         ec[c].cbytes = (int32_t)(ok ? ntb : destsize);
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int64_t acc = 0;
-        for (int64_t c = 0; c < g.nchunks; c++) { ec[c].offset = acc; acc += ec[c].cbytes; }
-        *total = acc;
+}
+
+// Chunk offsets: exclusive scan of the chunk sizes (one CTA).
+__global__ void __launch_bounds__(1024) k_chunk_offsets(int64_t nchunks, EncChunk *ec, int64_t *total)
+{
+    __shared__ int64_t wsum[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int64_t base = 0;
+    for (int64_t r0 = 0; r0 < nchunks; r0 += 1024) {
+        const int64_t i = r0 + threadIdx.x;
+        const int64_t v = i < nchunks ? ec[i].cbytes : 0;
+        int64_t incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t t = __shfl_up_sync(FULLMASK, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        int64_t before = base + incl - v, all = 0;
+        for (int w = 0; w < 32; w++) {
+            before += w < warp ? wsum[w] : 0;
+            all += wsum[w];
+        }
+        if (i < nchunks) ec[i].offset = before;
+        base += all;
+        __syncthreads();
     }
+    if (threadIdx.x == 0) *total = base;
 }
 
 // Copies len bytes with the whole CTA: 16-byte aligned stores to dst, each fed by five
@@ -1810,8 +1889,12 @@ int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int s
                 IAB_TIMED("k_gather_fast", st, k_gather_fast<4><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
                     g, (const uint8_t *)in, ld, img.as<uint8_t>()));
         }
-        IAB_TIMED("k_gather", st, k_gather<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
-            g, fast, (const uint8_t *)in, ld, shuffle, img.as<uint8_t>()));
+        // the general gather covers the blocks the fast one leaves (padded or partial ones)
+        const bool all_fast = fast && g.chunk[0] % g.block[0] == 0 && g.chunk[1] % g.block[1] == 0 &&
+                              g.shape[0] % g.chunk[0] == 0 && g.shape[1] % g.chunk[1] == 0 && !(g.block[1] & 3);
+        if (!all_fast)
+            IAB_TIMED("k_gather", st, k_gather<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
+                g, fast, (const uint8_t *)in, ld, shuffle, img.as<uint8_t>()));
     }
     if (w->exact_lz4) {
         static bool attr = false;
@@ -1839,7 +1922,8 @@ int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int s
             img.as<uint8_t>(), ns, neblock, slots.as<uint8_t>(), es.as<EncStream>(),
             reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1)));
     }
-    IAB_TIMED("k_layout", st, k_layout<<<1, 1024, 0, st>>>(g, nstreams, neblock, es.as<EncStream>(), ec, tot.as<int64_t>()));
+    IAB_TIMED("k_layout", st, k_layout<<<(unsigned)std::max<int64_t>(g.nchunks, 1), LAYOUT_T, 0, st>>>(g, nstreams, neblock, es.as<EncStream>(), ec));
+    IAB_TIMED("k_chunk_offsets", st, k_chunk_offsets<<<1, 1024, 0, st>>>(g.nchunks, ec, tot.as<int64_t>()));
     {
         const int64_t blocks = std::min<int64_t>(nbl, (int64_t)sms * 8);
         IAB_TIMED("k_emit", st, k_emit<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, nstreams, neblock, shuffle, split ? 1 : 0,
