@@ -264,6 +264,37 @@ def secondary_gemv(ia, ctx, stream, args, pk):
             "normwise_err_vs_f64": err}
 
 
+def secondary_plain_f64(ia, ctx, stream, args):
+    """Plain drop-in: iarray_linalg_matmul, A, B 1000 x 1000 float64, A = uniform(-1, 1)
+    (default_rng(0)), B = uniform(-1, 1) (default_rng(1)), chunk 500^2, block 100^2 for A, B and
+    C; both forms, normwise error against double-double on every row."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    n, ch, bl = 1000, 500, 100
+    A = np.random.default_rng(0).uniform(-1, 1, (n, n))
+    B = np.random.default_rng(1).uniform(-1, 1, (n, n))
+    hi, lo = O.dd_rows(A, B, np.arange(n))
+    out = {"workload": "plain matmul f64 1000^3, chunk 500^2, block 100^2"}
+    for form_name, form in (("native", ia.FORM_NATIVE), ("split", ia.FORM_SPLIT)):
+        ctx.set_form(form)
+        Ac = ia.Container.from_numpy(ctx, A, (ch, ch), (bl, bl))
+        Bc = ia.Container.from_numpy(ctx, B, (ch, ch), (bl, bl))
+        res = []
+
+        def step():
+            res.append(ia.matmul(ctx, Ac, Bc, (ch, ch), (bl, bl)))
+            if len(res) > 1:
+                res.pop(0).free()
+        ms, wall = _timed(ctx, stream, step, args.steps, args.warmup)
+        err = O.normwise_error(res[-1].to_numpy(), hi, lo, np.arange(n))
+        for c in res + [Ac, Bc]:
+            c.free()
+        out[form_name] = {"ms": ms, "wall_ms": wall, "tflops": 2.0 * n ** 3 / (ms * 1e-3) / 1e12,
+                          "normwise_err_vs_dd": err}
+    ctx.set_form(ia.FORM_NATIVE)
+    return out
+
+
 def secondary_f32(ia, ctx, stream, args):
     """Precision, float32: A 16384 x 4096, B 4096 x 16384, normal(0, 1) (default_rng(4)) plus
     0.1 sin(0.003 (i + j)), chunk 4096^2, block 512^2; native FFMA and 3xBF16 split forms."""
@@ -525,6 +556,16 @@ def run_ours(args):
                "sample": "one 2048x2048 output chunk (1/16 of the 8192^3 opt_gemm) with the reference's block-pair "
                          "loop: per-pair LZ4 block decode, single-threaded OpenBLAS dgemm per worker thread, LZ4 "
                          "re-encode; rate scaled to the full product"}
+        # upper bound on the host: dense float64 product of the decoded operands with
+        # torch.mm on all cores (no codec work), one warm-up and one timed call
+        torch.set_num_threads(cores)
+        ta, tb = torch.from_numpy(A), torch.from_numpy(B)
+        torch.mm(ta[:1024], tb)
+        t = time.perf_counter()
+        torch.mm(ta, tb)
+        cpu["dense_upper_bound"] = {"value": FLOP / (time.perf_counter() - t) / 1e12, "unit": "TFLOP/s",
+                                    "cores": cores, "what": "torch.mm float64 8192^3 on decoded operands"}
+        del ta, tb
 
     pk = peaks()
     secondary = None
@@ -533,7 +574,8 @@ def run_ours(args):
             c.free()
         torch.cuda.empty_cache()
         secondary = {}
-        for key, fn in (("gemv_f32", lambda: secondary_gemv(ia, ctx, stream, args, pk)),
+        for key, fn in (("plain_f64_1000", lambda: secondary_plain_f64(ia, ctx, stream, args)),
+                        ("gemv_f32", lambda: secondary_gemv(ia, ctx, stream, args, pk)),
                         ("precision_f32", lambda: secondary_f32(ia, ctx, stream, args)),
                         ("batching_f64", lambda: secondary_batch(ia, ctx, stream, args))):
             try:
@@ -640,7 +682,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--err-rows", type=int, default=64)
+    ap.add_argument("--err-rows", type=int, default=256, help="rows (default_rng(99)) for the normwise error")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the GEMV, float32 and batching workloads")
     ap.add_argument("--profile-case", choices=["codec", "split"], default=None,

@@ -1065,8 +1065,9 @@ static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_
     }
     if (INA_FAILED(rc)) return rc;
     tm.mark(3);
-    dA.reset();
-    dB.reset();
+    // dA and dB stay allocated until the encode below has synchronised the stream: the pool is
+    // shared by every context, so memory released while the product may still read it could be
+    // handed to another stream
     rc = c->geom.nchunks ? encode_into(ctx, c, dC.p, vec ? M : ldc) : fill_zero_chunks(c);
     if (INA_FAILED(rc)) return rc;
     tm.mark(4);

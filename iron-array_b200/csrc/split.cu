@@ -70,15 +70,19 @@ constexpr int MAX_MODULI = 20;
 static const int kModuli[MAX_MODULI] = {256, 255, 253, 251, 247, 241, 239, 233, 229, 227,
                                         223, 217, 211, 199, 197, 193, 191, 181, 179, 173};
 
+constexpr int CRT_BITS = 34;                       // chunk width of the reconstruction
 struct CrtConst {
     int L;
-    int nc;                                        // 40-bit chunks needed for P (1..4)
+    int np;                                        // residue pairs (m_2p, m_2p+1); the last is single when L is odd
+    int nc;                                        // CRT_BITS-bit chunks needed for P (1..4)
     int mod[MAX_MODULI];
     double inv_mod[MAX_MODULI];
     float inv_modf[MAX_MODULI];
-    double wf[MAX_MODULI][4];                      // CRT basis w_l = (P/m_l) * ((P/m_l)^-1 mod m_l) mod P,
-                                                   // 40-bit chunks (least significant first) as exact doubles
-    double pf[4];                                  // P in 40-bit chunks
+    uint32_t pm0[8], pm1[8];                       // pair moduli (pm1 = 1: single)
+    uint32_t pinv[8], pmagic[8];                   // pm0^-1 mod pm1, ceil(2^32 / pm1)
+    double pw[8][4];                               // CRT basis of the pair moduli M_p = pm0 pm1:
+                                                   // (P/M_p) ((P/M_p)^-1 mod M_p) mod P, in chunks
+    double pp[4];                                  // P in chunks (least significant first)
     double inv_p;                                  // 1/P (rounded)
     double log2p;
 };
@@ -87,16 +91,16 @@ __constant__ CrtConst c_crt;
 
 static bool build_crt(int L, CrtConst *c)
 {
-    if (L < 2 || L > 16) return false;   // P < 2^126: at most four 40-bit chunks
+    if (L < 2 || L > 16) return false;   // P < 2^126: at most four chunks
     typedef unsigned __int128 u128;
-    const u128 mask40 = ((u128)1 << 40) - 1;
+    const u128 mask = ((u128)1 << CRT_BITS) - 1;
     u128 P = 1;
     for (int l = 0; l < L; l++) P *= (u128)kModuli[l];
     memset(c, 0, sizeof(*c));
     c->L = L;
     int bits = 0;
     for (u128 t = P; t; t >>= 1) bits++;
-    c->nc = (bits + 39) / 40;
+    c->nc = (bits + CRT_BITS - 1) / CRT_BITS;
     double lp = 0;
     for (int l = 0; l < L; l++) {
         const int m = kModuli[l];
@@ -104,16 +108,29 @@ static bool build_crt(int L, CrtConst *c)
         c->inv_mod[l] = 1.0 / m;
         c->inv_modf[l] = 1.0f / (float)m;
         lp += log2((double)m);
-        const u128 Ml = P / (u128)m;
-        const int a = (int)(Ml % (u128)m);
-        int inv = 0;
-        for (int x = 1; x < m; x++)
-            if ((a * x) % m == 1) { inv = x; break; }
-        if (!inv) return false;
-        const u128 w = (Ml * (u128)inv) % P;
-        for (int k = 0; k < 4; k++) c->wf[l][k] = (double)(uint64_t)((w >> (40 * k)) & mask40);
     }
-    for (int k = 0; k < 4; k++) c->pf[k] = (double)(uint64_t)((P >> (40 * k)) & mask40);
+    auto inverse = [](uint64_t a, uint64_t m) -> uint64_t {   // a^-1 mod m (m > 1, gcd 1)
+        for (uint64_t x = 1; x < m; x++)
+            if ((a * x) % m == 1) return x;
+        return 0;
+    };
+    c->np = (L + 1) / 2;
+    for (int p = 0; p < c->np; p++) {
+        const uint64_t m0 = (uint64_t)kModuli[2 * p], m1 = 2 * p + 1 < L ? (uint64_t)kModuli[2 * p + 1] : 1;
+        c->pm0[p] = (uint32_t)m0;
+        c->pm1[p] = (uint32_t)m1;
+        if (m1 > 1) {
+            c->pinv[p] = (uint32_t)inverse(m0 % m1, m1);
+            c->pmagic[p] = (uint32_t)(((uint64_t)1 << 32) / m1 + 1);   // ceil(2^32 / m1): m1 is odd
+            if (!c->pinv[p]) return false;
+        }
+        const u128 Mp = (u128)(m0 * m1), Q = P / Mp;
+        const uint64_t inv = inverse((uint64_t)(Q % Mp), (uint64_t)Mp);
+        if (!inv) return false;
+        const u128 w = (Q * (u128)inv) % P;
+        for (int k = 0; k < 4; k++) c->pw[p][k] = (double)(uint64_t)((w >> (CRT_BITS * k)) & mask);
+    }
+    for (int k = 0; k < 4; k++) c->pp[k] = (double)(uint64_t)((P >> (CRT_BITS * k)) & mask);
     c->inv_p = 1.0 / ((double)(uint64_t)(P >> 64) * 18446744073709551616.0 + (double)(uint64_t)P);
     c->log2p = lp;
     return true;
@@ -270,7 +287,6 @@ static void launch_nonfinite_fix(int64_t M, int64_t N, int64_t K, const T *A, in
 // FP64 pipe (no float/int conversions).
 constexpr double kRound = 6755399441055744.0;
 constexpr double kTwo52 = 4503599627370496.0;
-constexpr double kTwo40 = 1099511627776.0;
 
 // 2^s for -1022 <= s <= 1023.
 __device__ __forceinline__ double pow2i(int s) { return __hiloint2double((1023 + s) << 20, 0); }
@@ -566,37 +582,41 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
 }
 
 // ============================================================================ reconstruction
-// X = sum_l r_l w_l mod P, centred into (-P/2, P/2), in exact FP64 arithmetic.  Each w_l is
-// held as NC chunks of 40 bits, so with r_l < 2^8 and L <= 16 every partial sum
-// S_k = sum_l r_l w_lk stays below 2^52 and is exact.  The quotient q = rint(S / P) < 2^12
-// comes from a rounded estimate of S: the scaling keeps |X| below P / 8 (both norms are
-// held to 2^(gamma - 1)), so S / P stays far from a half-integer compared with the
-// estimate's error (about 2^-39 of one unit), and q is exact.  Then every
-// D_k = S_k - q P_k is exact (q P_k < 2^52); with the low chunks carried into [0, 2^40),
-// X = sum_k D_k 2^(40 k) is formed by Horner steps that are exact whenever X is
-// representable (every partial floor(X / 2^(40 j)) then is too) and round at most twice
-// otherwise.
+// X = sum_l r_l w_l mod P, centred into (-P/2, P/2), in exact arithmetic.  The residues of
+// each pair of moduli (m0, m1) are first combined in integers (Garner: y = r0 + m0 t with
+// t = (r1 - r0) m0^-1 mod m1, so y = X mod m0 m1 < 2^16), then X = sum_p y_p W_p mod P over
+// the pair moduli.  Each W_p is held as NC chunks of CRT_BITS = 34 bits, so with at most 8
+// pairs every partial sum S_k = sum_p y_p W_pk stays below 2^53 and is exact in FP64.  The
+// quotient q = rint(S / P) < 2^19 comes from a rounded estimate of S: the scaling keeps |X|
+// below P / 8 (both norms are held to 2^(gamma - 1)), so S / P stays far from a half-integer
+// compared with the estimate's error (about 2^-34 of one unit), and q is exact.  Then every
+// D_k = S_k - q P_k is exact (q P_k < 2^53); with the low chunks carried into [0, 2^34),
+// X = sum_k D_k 2^(34 k) is formed by Horner steps that are exact whenever X is
+// representable (every partial floor(X / 2^(34 j)) then is too) and otherwise stay within
+// about one ulp.
+constexpr double kTwoCB = 17179869184.0;           // 2^CRT_BITS
+constexpr double kInvTwoCB = 0x1p-34;
+
 template <int NC>
 __device__ __forceinline__ double crt_value(const double (&S)[NC])
 {
     double s = S[NC - 1];
 #pragma unroll
-    for (int k = NC - 2; k >= 0; k--) s = fma(s, kTwo40, S[k]);
+    for (int k = NC - 2; k >= 0; k--) s = fma(s, kTwoCB, S[k]);
     const double q = fma(s, c_crt.inv_p, kRound) - kRound;
     double D[NC];
 #pragma unroll
-    for (int k = 0; k < NC; k++) D[k] = fma(-q, c_crt.pf[k], S[k]);
-    // carry the low chunks into [0, 2^40) (every step exact: integers below 2^53); then the
-    // Horner sum is exact whenever X is representable, and within one rounding otherwise
+    for (int k = 0; k < NC; k++) D[k] = fma(-q, c_crt.pp[k], S[k]);
+    // carry the low chunks into [0, 2^34) (every step exact: integers below 2^53)
 #pragma unroll
     for (int k = 0; k < NC - 1; k++) {
-        const double c = floor(D[k] * 0x1p-40);
-        D[k] = fma(-c, kTwo40, D[k]);
+        const double c = floor(D[k] * kInvTwoCB);
+        D[k] = fma(-c, kTwoCB, D[k]);
         D[k + 1] += c;
     }
     double x = D[NC - 1];
 #pragma unroll
-    for (int k = NC - 2; k >= 0; k--) x = fma(x, kTwo40, D[k]);
+    for (int k = NC - 2; k >= 0; k--) x = fma(x, kTwoCB, D[k]);
     return x;
 }
 
@@ -627,15 +647,25 @@ __global__ void __launch_bounds__(256) k_crt(int M, int N, const uint8_t *__rest
         for (int u = 0; u < 4; u++)
 #pragma unroll
             for (int k = 0; k < NC; k++) S[u][k] = 0.0;
+        const int np = c_crt.np;
 #pragma unroll
-        for (int l = 0; l < 16; l++) {
-            if (l < L) {
+        for (int p = 0; p < 8; p++) {
+            if (p < np) {
+                const uint32_t m0 = c_crt.pm0[p], m1 = c_crt.pm1[p], inv = c_crt.pinv[p], mg = c_crt.pmagic[p];
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
-                    // the residue byte as a double: 2^52 + r, less 2^52
-                    const double r = __hiloint2double(0x43300000, (int)((w[l] >> (8 * u)) & 0xffu)) - kTwo52;
+                    const uint32_t r0 = (w[2 * p] >> (8 * u)) & 0xffu;
+                    uint32_t y = r0;
+                    if (m1 > 1) {
+                        const uint32_t r1 = (w[2 * p + 1] >> (8 * u)) & 0xffu;
+                        const uint32_t prod = (r1 + 2 * m1 - r0) * inv;           // < 2^18
+                        const uint32_t t = prod - __umulhi(prod, mg) * m1;         // prod mod m1, exact
+                        y = r0 + m0 * t;
+                    }
+                    // y as a double: 2^52 + y, less 2^52
+                    const double yd = __hiloint2double(0x43300000, (int)y) - kTwo52;
 #pragma unroll
-                    for (int k = 0; k < NC; k++) S[u][k] = fma(r, c_crt.wf[l][k], S[u][k]);
+                    for (int k = 0; k < NC; k++) S[u][k] = fma(yd, c_crt.pw[p][k], S[u][k]);
                 }
             }
         }
