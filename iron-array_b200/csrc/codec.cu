@@ -145,6 +145,7 @@ constexpr int THREADS = 256;
 constexpr int DW = 2048;                   // compressed bytes per window
 constexpr int MAXS = DW / 3 + 2;           // sequences per window (a non-final one takes >= 3 bytes)
 constexpr int PATH = 1024;                 // >= 2 * the largest power of two below MAXS + 1
+constexpr int HB = 4096;                   // output history kept in shared memory for match sources
 constexpr int DCAP = 4096;                 // output bytes resolved in shared memory at once
 constexpr uint16_t STOP = 0xFFFF, ENDS = 0xFFFE;
 constexpr uint32_t RES = 0x80000000u;      // resolved output byte (value in the low 8 bits)
@@ -158,6 +159,7 @@ struct Smem {
     uint16_t J[2][DW];
     uint16_t path[PATH];
     uint8_t win[DW + 16];
+    uint8_t hist[HB];                      // the last HB output bytes (ring, by absolute position)
     int32_t wsum[THREADS / 32];
     int32_t scal[8];
 };
@@ -215,11 +217,21 @@ __global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const uint8
         uint8_t *out = scratch + jb.dst;
         const int osz = jb.dlen;
         int p = 0, op = 0;                 // window start in the input, output written so far
+        int hist_from = 0;                 // S.hist holds output bytes [hist_from, written)
         bool bad = false, done = false;    // block-uniform
         while (!done && !bad) {
             const int rem = isz - p, n = min(DW, rem);
             __syncthreads();
-            for (int x = tid; x < n; x += THREADS) S.win[x] = __ldg(in + p + x);
+            {                                          // every load issued before any store
+                uint8_t v[DW / THREADS];
+#pragma unroll
+                for (int k = 0; k < DW / THREADS; k++) {
+                    const int x = tid + k * THREADS;
+                    v[k] = x < n ? __ldg(in + p + x) : (uint8_t)0;
+                }
+#pragma unroll
+                for (int k = 0; k < DW / THREADS; k++) S.win[tid + k * THREADS] = v[k];
+            }
             __syncthreads();
             for (int q = tid; q < n; q += THREADS) S.J[0][q] = dcta_next(S.win, q, n, rem);
             if (tid == 0) { S.path[0] = 0; S.scal[1] = PATH; }
@@ -339,7 +351,12 @@ __global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const uint8
                                 } else {
                                     const int m0 = s0 + lit, k = x - m0;
                                     const int src = d > k ? x - d : m0 - d + k % d;
-                                    v = src >= 0 ? (uint32_t)src : (RES | __ldcg(out + op + base + src));
+                                    if (src >= 0) {
+                                        v = (uint32_t)src;
+                                    } else {                        // earlier output: the ring, else global
+                                        const int abs = op + base + src;
+                                        v = RES | (abs >= hist_from ? (uint32_t)S.hist[abs & (HB - 1)] : (uint32_t)__ldcg(out + abs));
+                                    }
                                 }
                                 S.st[x] = v;
                             }
@@ -358,7 +375,12 @@ __global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const uint8
                             if (!__syncthreads_or(open)) break;
                         }
                         uint8_t *o = out + op + base;
-                        for (int x = tid; x < span; x += THREADS) o[x] = (uint8_t)S.st[x];
+                        for (int x = tid; x < span; x += THREADS) {
+                            const uint8_t byte = (uint8_t)S.st[x];
+                            o[x] = byte;
+                            S.hist[(op + base + x) & (HB - 1)] = byte;
+                        }
+                        hist_from = max(hist_from, op + base + span - HB);
                         a = b;
                     } else {
                         // one sequence larger than DCAP: literals, then the match from global memory
@@ -367,6 +389,7 @@ __global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const uint8
                         __syncthreads();
                         const int m0 = abs0 + lit;
                         for (int x = tid; x < ml; x += THREADS) out[m0 + x] = __ldcg(out + m0 - d + (d > x ? x : x % d));
+                        hist_from = m0 + ml;                        // the ring missed this sequence
                         a = a + 1;
                     }
                     __syncthreads();
@@ -425,6 +448,7 @@ __global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const uint8
                 for (int x = tid; x < ml; x += THREADS) out[m0 + x] = __ldcg(out + m0 - mo + (mo > x ? x : x % mo));
                 __syncthreads();
                 op += lit + ml;
+                hist_from = op;                            // the ring missed this sequence
                 if (nr < 0) done = true; else p = nr;
             }
         }
@@ -1159,12 +1183,13 @@ struct ParSmem {              // per CTA
         struct {
             uint16_t cw[PW];  // match distance of each window position
             uint8_t lw[PW];   // match length (0: none, 4..PCAP; PCAP: at least PCAP)
-            uint16_t J[2][PW];// chain tables
-            uint16_t path[PW / 4 * 2 + 2];
+            uint16_t J[PW];   // the match after the one at each position, or why the chain stops
+            uint16_t path[PW / 4 + 2];
         } w;
         uint8_t stage[4][PSTAGE];
     };
     uint32_t bits[32];        // match flags, one word per 32 positions
+    int32_t nchain;           // matches on the window's chain
     int32_t red[8];           // block reductions
     long long sid;
 };
@@ -1327,29 +1352,71 @@ __device__ __forceinline__ int cta_lz4_compress_par(const uint8_t *__restrict__ 
                     const uint32_t nx = par_next_match(S.bits, q + L);
                     j = nx >= (uint32_t)wn ? (q + L >= wn ? PJ_OUT : PJ_NONE) : (uint16_t)nx;
                 }
-                S.w.J[0][q] = j;
+                S.w.J[q] = j;
             }
-            if (tid == 0) S.w.path[0] = (uint16_t)s0;
             __syncthreads();
-            int len = 1, cur = 0, cnt = 0;
-            for (;;) {
-                int first = 0x7FFFFFFF;
-                for (int j = tid; j < len; j += PT) {
-                    const uint16_t pj = S.w.path[j];
-                    const uint16_t v = pj < wn ? S.w.J[cur][pj] : pj;
-                    S.w.path[len + j] = v;
-                    if (v >= wn) first = min(first, len + j);
+            // The chain from s0 by segment walks (warp 0): lane t walks J from the first match
+            // at or after 32 t, recording the matches it visits; then, in rounds, lane t takes
+            // the exit of lane t - 1 as its entry (lane 0: s0), follows its own walk once the
+            // chain meets it and publishes its exit, until no exit changes.
+            if (warp == 0) {
+                const int lo = lane * 32, hi = lo + 32;
+                const int nl = (wn + 31) / 32;              // lanes whose segment holds window positions
+                const bool act = lane < nl;
+                uint32_t mask = 0;
+                int ex = PJ_NONE;
+                if (act) {
+                    int q = (int)par_next_match(S.bits, lo);
+                    ex = q;
+                    if (q < hi && q < wn) {
+                        for (;;) {                          // positions grow: at most 32 steps
+                            mask |= 1u << (q - lo);
+                            const int v = S.w.J[q];
+                            if (v >= hi || v >= wn) { ex = v; break; }
+                            q = v;
+                        }
+                    }
                 }
-                first = cta_min(first, S.red);
-                if (first < 2 * len) { cnt = first; break; }
-                for (int q = tid; q < wn; q += PT) {
-                    const uint16_t v = S.w.J[cur][q];
-                    S.w.J[cur ^ 1][q] = v < wn ? S.w.J[cur][v] : v;
+                uint32_t fm = 0;
+                int cur = ex;
+                for (int round = 0; round < 32; round++) {  // one round settles at least one more lane
+                    int entry = __shfl_up_sync(FULLMASK, cur, 1);
+                    if (lane == 0) entry = (int)s0;
+                    uint32_t m = 0;
+                    int e2 = entry;
+                    if (act && entry < hi && entry < wn) {
+                        int q = entry;
+                        for (;;) {
+                            const int b = q - lo;
+                            if ((mask >> b) & 1u) { m |= mask & (~0u << b); e2 = ex; break; }
+                            m |= 1u << b;
+                            const int v = S.w.J[q];
+                            if (v >= hi || v >= wn) { e2 = v; break; }
+                            q = v;
+                        }
+                    }
+                    const bool changed = act && e2 != cur;
+                    fm = m;
+                    cur = e2;
+                    if (!__any_sync(FULLMASK, changed)) break;
                 }
-                cur ^= 1;
-                len *= 2;
-                __syncthreads();
+                const int chain_end = __shfl_sync(FULLMASK, cur, max(nl, 1) - 1);
+                const int c = __popc(fm);
+                int incl = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(FULLMASK, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                int o = incl - c;
+                for (uint32_t x = fm; x; x &= x - 1) S.w.path[o++] = (uint16_t)(lo + __ffs((int)x) - 1);
+                if (lane == 31) {
+                    S.w.path[incl] = (uint16_t)chain_end;   // PJ_NONE, PJ_OUT or PJ_LONG
+                    S.nchain = incl;
+                }
             }
+            __syncthreads();
+            const int cnt = S.nchain;
             const uint16_t term = S.w.path[cnt];                // why the chain stopped
             // a capped last match: extend it exactly (CTA-wide) before writing it
             int lastL = S.w.lw[S.w.path[cnt - 1]];
@@ -1483,7 +1550,7 @@ __device__ __forceinline__ int cta_probe(const uint8_t *__restrict__ src, int n,
 // probe of four sampled windows routes each stream: almost no matches (incompressible
 // byte planes): stored raw; few matches: the liblz4 search (one warp), whose accelerating
 // skip makes them cheap; the rest: the parallel parse.
-__global__ void __launch_bounds__(PT, 7) k_lz4_encode_par(const uint8_t *__restrict__ img, int64_t nstreams_total,
+__global__ void __launch_bounds__(PT, 8) k_lz4_encode_par(const uint8_t *__restrict__ img, int64_t nstreams_total,
                                                        int neblock, uint8_t *slots, EncStream *es,
                                                        unsigned long long *next)
 {
@@ -1911,13 +1978,13 @@ int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int s
             reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1)));
     } else {
         static bool attr = false;
-        const int smem = (int)sizeof(ParSmem);                 // one stream per CTA of PT threads, 7 CTAs per SM
+        const int smem = (int)sizeof(ParSmem);                 // one stream per CTA of PT threads, 8 CTAs per SM
         if (!attr) {
             cudaFuncSetAttribute(k_lz4_encode_par, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             attr = true;
         }
         const int64_t ns = nbl * nstreams;
-        const int64_t blocks = std::min<int64_t>(ns, (int64_t)sms * 7);
+        const int64_t blocks = std::min<int64_t>(ns, (int64_t)sms * 8);
         IAB_TIMED("k_lz4_encode_par", st, k_lz4_encode_par<<<(unsigned)std::max<int64_t>(blocks, 1), PT, smem, st>>>(
             img.as<uint8_t>(), ns, neblock, slots.as<uint8_t>(), es.as<EncStream>(),
             reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1)));
