@@ -1302,41 +1302,57 @@ __device__ __forceinline__ int cta_lz4_compress_par(const uint8_t *__restrict__ 
         cta_fill(s, wend + PCAP + 32);
         // ---- A: candidates and lengths.  Positions p .. p + PCAP + 4 lie in the window;
         // a candidate is read from the window when it is still there, else from global memory.
-        // The stream's first PT positions go in rounds of 32 (one warp), so that short streams
-        // keep table candidates for most of their positions; then rounds of PT.
+        // Rounds of 2 PT positions (two per thread; a round's positions see the table as it was
+        // before the round).  The stream's first PT positions go in rounds of 32 and the next PT
+        // in one round of PT, so that short streams keep table candidates for most positions.
         for (int q0 = 0, rsz; q0 < PW; q0 += rsz) {
-            rsz = w0 + q0 < PT ? 32 : PT;
-            const int q = q0 + tid, p = w0 + q;
-            const bool valid = tid < rsz && p < wend;
-            const uint32_t v = valid ? par_rd32(ring_s, p) : 0u;
-            const uint32_t h = (v * 2654435761u) >> (32 - 12);
-            const uint32_t tv = valid ? S.tab32[h] : 0u;
-            __syncthreads();                             // every read of this round precedes its writes
-            if (valid) atomicMax(&S.tab32[h], (uint32_t)p + 1u);
-            const int cand = (int)tv - 1;
-            int L = 0, best = cand;
-            const int lim = min(mlimit - p, PCAP);
+            rsz = w0 + q0 < PT ? 32 : w0 + q0 < 2 * PT ? PT : 2 * PT;
+            int p2[2];
+            bool valid[2];
+            uint32_t v2[2], h2[2], tv2[2];
 #pragma unroll
-            for (int t = 0; t < 2; t++) {
-                const int c = t ? p - 1 : cand;
-                if (!valid || c >= p || c < 0 || p - c > 65535 || (t && c == cand)) continue;
-                const bool inring = c >= s.lo;
-                if ((inring ? par_rd32(ring_s, c) : ld4u(src + c)) != v) continue;
-                int l = 4;
-                while (l < lim) {
-                    const uint32_t x = par_rd32(ring_s, p + l) ^ (inring ? par_rd32(ring_s, c + l) : ld4u(src + c + l));
-                    if (x) { l += (__ffs((int)x) - 1) >> 3; break; }
-                    l += 4;
+            for (int k = 0; k < 2; k++) {
+                const int q = q0 + tid + k * PT;
+                p2[k] = w0 + q;
+                valid[k] = tid + k * PT < rsz && p2[k] < wend;
+                v2[k] = valid[k] ? par_rd32(ring_s, p2[k]) : 0u;
+                h2[k] = (v2[k] * 2654435761u) >> (32 - 12);
+                tv2[k] = valid[k] ? S.tab32[h2[k]] : 0u;
+            }
+            __syncthreads();                             // every read of this round precedes its writes
+#pragma unroll
+            for (int k = 0; k < 2; k++)
+                if (valid[k]) atomicMax(&S.tab32[h2[k]], (uint32_t)p2[k] + 1u);
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+                const int p = p2[k];
+                const uint32_t v = v2[k];
+                const int cand = (int)tv2[k] - 1;
+                int L = 0, best = cand;
+                const int lim = min(mlimit - p, PCAP);
+#pragma unroll
+                for (int t = 0; t < 2; t++) {
+                    const int c = t ? p - 1 : cand;
+                    if (!valid[k] || c >= p || c < 0 || p - c > 65535 || (t && c == cand)) continue;
+                    const bool inring = c >= s.lo;
+                    if ((inring ? par_rd32(ring_s, c) : ld4u(src + c)) != v) continue;
+                    int l = 4;
+                    while (l < lim) {
+                        const uint32_t x = par_rd32(ring_s, p + l) ^ (inring ? par_rd32(ring_s, c + l) : ld4u(src + c + l));
+                        if (x) { l += (__ffs((int)x) - 1) >> 3; break; }
+                        l += 4;
+                    }
+                    l = min(l, lim);
+                    if (l > L) { L = l; best = c; }
                 }
-                l = min(l, lim);
-                if (l > L) { L = l; best = c; }
+                const int q = q0 + tid + k * PT;
+                if (tid + k * PT < rsz) {
+                    S.w.cw[q] = (uint16_t)(p - best);
+                    S.w.lw[q] = (uint8_t)L;
+                }
+                const unsigned bb = __ballot_sync(FULLMASK, L >= 4);
+                if (lane == 0 && k * PT + warp * 32 < rsz) S.bits[((q0 + k * PT) >> 5) + warp] = bb;
             }
-            if (tid < rsz) {
-                S.w.cw[q] = (uint16_t)(p - best);
-                S.w.lw[q] = (uint8_t)L;
-            }
-            const unsigned b = __ballot_sync(FULLMASK, L >= 4);
-            if (lane == 0 && warp < rsz / 32) S.bits[(q0 >> 5) + warp] = b;
             __syncthreads();                             // this round's writes precede the next reads
         }
         // ---- B: chains of matches from the parse position
