@@ -233,7 +233,11 @@ __global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const uint8
                 for (int k = 0; k < DW / THREADS; k++) S.win[tid + k * THREADS] = v[k];
             }
             __syncthreads();
-            for (int q = tid; q < n; q += THREADS) S.J[0][q] = dcta_next(S.win, q, n, rem);
+#pragma unroll
+            for (int k = 0; k < DW / THREADS; k++) {      // eight independent table entries per thread
+                const int q = tid + k * THREADS;
+                if (q < n) S.J[0][q] = dcta_next(S.win, q, n, rem);
+            }
             if (tid == 0) { S.path[0] = 0; S.scal[1] = PATH; }
             __syncthreads();
             // chain of token positions by doubling: after level k, path[0 .. 2^(k+1)) known
@@ -248,10 +252,21 @@ __global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const uint8
                 __syncthreads();
                 const int t = S.scal[1];
                 if (t < 2 * len) { cnt = t; break; }
-                // J_{k+1} = J_k o J_k
-                for (int q = tid; q < n; q += THREADS) {
-                    const uint16_t v = S.J[cur][q];
-                    S.J[cur ^ 1][q] = v < n ? S.J[cur][v] : v;
+                // J_{k+1} = J_k o J_k (a thread's loads issued together, then its stores)
+                {
+                    uint16_t v[DW / THREADS], w[DW / THREADS];
+#pragma unroll
+                    for (int k = 0; k < DW / THREADS; k++) {
+                        const int q = tid + k * THREADS;
+                        v[k] = q < n ? S.J[cur][q] : (uint16_t)0xFFFF;
+                    }
+#pragma unroll
+                    for (int k = 0; k < DW / THREADS; k++) w[k] = v[k] < n ? S.J[cur][v[k]] : v[k];
+#pragma unroll
+                    for (int k = 0; k < DW / THREADS; k++) {
+                        const int q = tid + k * THREADS;
+                        if (q < n) S.J[cur ^ 1][q] = w[k];
+                    }
                 }
                 cur ^= 1;
                 len *= 2;
@@ -327,7 +342,8 @@ __global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const uint8
                         const int span = S.ostart[b] - base;
                         // each thread fills a contiguous run of output bytes: one binary search
                         // for the sequence holding its first byte, then a forward walk
-                        const int per = (span + THREADS - 1) / THREADS;
+                        // odd run length: the lanes' stores st[t * per + i] fall in 32 different banks
+                        const int per = ((span + THREADS - 1) / THREADS) | 1;
                         const int x0 = tid * per, x1 = min(span, x0 + per);
                         if (x0 < x1) {
                             int l2 = a, h2 = b - 1;
