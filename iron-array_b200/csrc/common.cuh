@@ -224,11 +224,20 @@ struct OzakiB {
 };
 struct OzakiWork {
     DevBuf ra, rr, sa, err;
+    alignas(64) unsigned char tmA[128];   // CUtensorMap of the residues of A (rows_prep -> rows_product)
     OzakiB b;                              // used by gemm_f64_ozaki_launch
 };
 int gemm_f64_ozaki_launch(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B,
                           int64_t ldb, double *C, int64_t ldc, int nterms, OzakiWork *w, cudaStream_t st);
 int gemm_f64_ozaki_prepare_b(int64_t K, int64_t N, const double *B, int64_t ldb, int nterms, OzakiB *ob, cudaStream_t st);
+// The same in two parts: setup (CRT constants on `st`, the B side's sizes) and the B kernels;
+// and rows = rows_prep (scaling and residues of the A rows) + rows_product (INT8 GEMM, CRT).
+// The CRT constants are read by every kernel after setup: other streams must wait for `st`.
+int gemm_f64_ozaki_setup(int64_t K, int64_t N, int nterms, OzakiB *ob, cudaStream_t st);
+int gemm_f64_ozaki_b_kernels(const double *B, int64_t ldb, OzakiB *ob, cudaStream_t st);
+int gemm_f64_ozaki_rows_prep(int64_t M, const double *A, int64_t lda, const OzakiB &ob, OzakiWork *w, cudaStream_t st);
+int gemm_f64_ozaki_rows_product(int64_t M, const double *A, int64_t lda, const OzakiB &ob, double *C, int64_t ldc,
+                                OzakiWork *w, cudaStream_t st);
 int gemm_f64_ozaki_rows(int64_t M, const double *A, int64_t lda, const OzakiB &ob, double *C, int64_t ldc,
                         OzakiWork *w, cudaStream_t st);
 int gemm_f64_ozaki_finish(OzakiWork *w, cudaStream_t st);

@@ -756,7 +756,7 @@ static bool set_crt(int L, CrtConst *out, cudaStream_t st)
     return cudaMemcpyToSymbolAsync(c_crt, &cached, sizeof(CrtConst), 0, cudaMemcpyHostToDevice, st) == cudaSuccess;
 }
 
-int gemm_f64_ozaki_prepare_b(int64_t K, int64_t N, const double *B, int64_t ldb, int nterms, OzakiB *ob, cudaStream_t st)
+int gemm_f64_ozaki_setup(int64_t K, int64_t N, int nterms, OzakiB *ob, cudaStream_t st)
 {
     if (!device_is_sm100()) return -1;
     // |sum_k a*b| <= K * 2^14 must keep the epilogue's float quotient within one of the
@@ -765,17 +765,23 @@ int gemm_f64_ozaki_prepare_b(int64_t K, int64_t N, const double *B, int64_t ldb,
     const int L = nterms > 0 ? nterms : 14;
     CrtConst cc;
     if (!set_crt(L, &cc, st)) return -1;
-    int dev = 0;
-    cudaGetDevice(&dev);
     ob->L = L;
     ob->nc = cc.nc;
     ob->K = K;
     ob->N = N;
     ob->Kp = round_up(K, oz::BK);
     ob->gamma = (cc.log2p - 1.0) / 2.0 - 0.01;
+    return 0;
+}
+
+int gemm_f64_ozaki_b_kernels(const double *B, int64_t ldb, OzakiB *ob, cudaStream_t st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int L = ob->L;
+    const int64_t K = ob->K, N = ob->N, Kp = ob->Kp;
     ob->B = B;
     ob->ldb = ldb;
-    const int64_t Kp = ob->Kp;
     if (!ob->rb.allocate((size_t)(L * N * Kp), dev) || !ob->sb.allocate((size_t)N * 4, dev) ||
         !ob->pm.allocate((size_t)COL_SEGS * N * 8, dev) || !ob->ps.allocate((size_t)COL_SEGS * N * 8, dev))
         return -100;
@@ -793,8 +799,13 @@ int gemm_f64_ozaki_prepare_b(int64_t K, int64_t N, const double *B, int64_t ldb,
     return 0;
 }
 
-int gemm_f64_ozaki_rows(int64_t M, const double *A, int64_t lda, const OzakiB &ob, double *C, int64_t ldc,
-                        OzakiWork *w, cudaStream_t st)
+int gemm_f64_ozaki_prepare_b(int64_t K, int64_t N, const double *B, int64_t ldb, int nterms, OzakiB *ob, cudaStream_t st)
+{
+    const int r = gemm_f64_ozaki_setup(K, N, nterms, ob, st);
+    return r ? r : gemm_f64_ozaki_b_kernels(B, ldb, ob, st);
+}
+
+int gemm_f64_ozaki_rows_prep(int64_t M, const double *A, int64_t lda, const OzakiB &ob, OzakiWork *w, cudaStream_t st)
 {
     if (M <= 0) return 0;
     if (M > (1 << 30)) return -1;
@@ -811,25 +822,45 @@ int gemm_f64_ozaki_rows(int64_t M, const double *A, int64_t lda, const OzakiB &o
     const int nsm = sms();
     IAB_TIMED("k_row_shift", st, k_row_shift<<<(unsigned)((M * 32 + 255) / 256), 256, 0, st>>>((int)M, (int)K, A, lda, ob.gamma, sa.as<int>()));
     IAB_TIMED("k_residues_rows", st, k_residues_rows<<<(unsigned)(nsm * 16), 256, 0, st>>>((int)M, (int)K, (int)Kp, A, lda, sa.as<int>(), ra.as<int8_t>()));
-    CUtensorMap tmA;
-    if (!make_tmap_3d(&tmA, CU_TENSOR_MAP_DATA_TYPE_UINT8, ra.p, (uint64_t)Kp, (uint64_t)M, (uint64_t)L, (uint64_t)Kp,
-                      (uint64_t)(Kp * M), oz::BK, oz::BM, CU_TENSOR_MAP_SWIZZLE_128B))
+    static_assert(sizeof(CUtensorMap) <= sizeof(w->tmA), "tensor map storage");
+    if (!make_tmap_3d(reinterpret_cast<CUtensorMap *>(w->tmA), CU_TENSOR_MAP_DATA_TYPE_UINT8, ra.p, (uint64_t)Kp,
+                      (uint64_t)M, (uint64_t)L, (uint64_t)Kp, (uint64_t)(Kp * M), oz::BK, oz::BM,
+                      CU_TENSOR_MAP_SWIZZLE_128B))
         return -1;
+    return 0;
+}
+
+int gemm_f64_ozaki_rows_product(int64_t M, const double *A, int64_t lda, const OzakiB &ob, double *C, int64_t ldc,
+                                OzakiWork *w, cudaStream_t st)
+{
+    if (M <= 0) return 0;
+    const int L = ob.L;
+    const int64_t N = ob.N, K = ob.K, Kp = ob.Kp;
+    const int64_t ldr = round_up(N, 16);
+    const int nsm = sms();
     I8Params prm;
     prm.M = (int)M; prm.N = (int)N; prm.Kp = (int)Kp; prm.L = L;
     prm.tiles_m = (int)ceil_div(M, oz::BM); prm.tiles_n = (int)ceil_div(N, oz::BN);
-    prm.R = rr.as<uint8_t>(); prm.ldr = ldr; prm.err = err.as<int>();
+    prm.R = w->rr.as<uint8_t>(); prm.ldr = ldr; prm.err = w->err.as<int>();
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_i8gemm_mod, cudaFuncAttributeMaxDynamicSharedMemorySize, oz::SMEM);
         attr = true;
     }
     const int tiles = L * prm.tiles_m * prm.tiles_n;
+    const CUtensorMap &tmA = *reinterpret_cast<const CUtensorMap *>(w->tmA);
     const CUtensorMap &tmB = *reinterpret_cast<const CUtensorMap *>(ob.tmB);
     IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
-    launch_crt(ob.nc, (unsigned)(nsm * 8), (int)M, (int)N, rr.as<uint8_t>(), ldr, sa.as<int>(), ob.sb.as<int>(), C, ldc, st);
-    launch_nonfinite_fix<double>(M, N, K, A, lda, ob.B, ob.ldb, C, ldc, sa.as<int>(), ob.sb.as<int>(), kNonFinite, st);
+    launch_crt(ob.nc, (unsigned)(nsm * 8), (int)M, (int)N, w->rr.as<uint8_t>(), ldr, w->sa.as<int>(), ob.sb.as<int>(), C, ldc, st);
+    launch_nonfinite_fix<double>(M, N, K, A, lda, ob.B, ob.ldb, C, ldc, w->sa.as<int>(), ob.sb.as<int>(), kNonFinite, st);
     return 0;
+}
+
+int gemm_f64_ozaki_rows(int64_t M, const double *A, int64_t lda, const OzakiB &ob, double *C, int64_t ldc,
+                        OzakiWork *w, cudaStream_t st)
+{
+    const int r = gemm_f64_ozaki_rows_prep(M, A, lda, ob, w, st);
+    return r ? r : gemm_f64_ozaki_rows_product(M, A, lda, ob, C, ldc, w, st);
 }
 
 int gemm_f64_ozaki_launch(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B, int64_t ldb,
