@@ -146,6 +146,7 @@ constexpr int DW = 2048;                   // compressed bytes per window
 constexpr int MAXS = DW / 3 + 2;           // sequences per window (a non-final one takes >= 3 bytes)
 constexpr int PATH = 1024;                 // >= 2 * the largest power of two below MAXS + 1
 constexpr int HB = 4096;                   // output history kept in shared memory for match sources
+constexpr int LONGSEQ = 64;                // longer sequences are filled by the whole CTA
 constexpr int DCAP = 4096;                 // output bytes resolved in shared memory at once
 constexpr uint16_t STOP = 0xFFFF, ENDS = 0xFFFE;
 constexpr uint32_t RES = 0x80000000u;      // resolved output byte (value in the low 8 bits)
@@ -160,6 +161,8 @@ struct Smem {
     uint16_t path[PATH];
     uint8_t win[DW + 16];
     uint8_t hist[HB];                      // the last HB output bytes (ring, by absolute position)
+    int32_t longs[DCAP / (LONGSEQ + 1) + 1];  // sequences of a group longer than LONGSEQ bytes
+    int32_t nlong;
     int32_t wsum[THREADS / 32];
     int32_t scal[8];
 };
@@ -205,6 +208,7 @@ __global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const uint8
     Smem &S = *reinterpret_cast<Smem *>(sm_dcta);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int njobs = *njobs_p;
+    if (tid == 0) S.nlong = 0;                     // first use follows the barriers below
     for (;;) {
         __syncthreads();
         if (tid == 0) S.scal[0] = (int)atomicAdd(next_job, 1u);
@@ -340,44 +344,42 @@ __global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const uint8
                     const int b = lo;
                     if (S.ostart[b] - base <= DCAP) {
                         const int span = S.ostart[b] - base;
-                        // each thread fills a contiguous run of output bytes: one binary search
-                        // for the sequence holding its first byte, then a forward walk
-                        // odd run length: the lanes' stores st[t * per + i] fall in 32 different banks
-                        const int per = ((span + THREADS - 1) / THREADS) | 1;
-                        const int x0 = tid * per, x1 = min(span, x0 + per);
-                        if (x0 < x1) {
-                            int l2 = a, h2 = b - 1;
-                            while (l2 < h2) {
-                                const int mid = (l2 + h2 + 1) >> 1;
-                                if (S.ostart[mid] - base <= x0) l2 = mid; else h2 = mid - 1;
+                        // a match byte's source, relative to the group (>= 0: a pointer into st),
+                        // or its value when it precedes the group (the ring, else global memory)
+                        auto src_entry = [&](int src) -> uint32_t {
+                            if (src >= 0) return (uint32_t)src;
+                            const int abs = op + base + src;
+                            return RES | (abs >= hist_from ? (uint32_t)S.hist[abs & (HB - 1)] : (uint32_t)__ldcg(out + abs));
+                        };
+                        // Sequence-parallel fill: a thread writes whole sequences (match byte k at
+                        // m0 + k takes its source at m0 - d + (k mod d): below the match start even
+                        // when the match overlaps itself); sequences longer than LONGSEQ bytes are
+                        // listed and filled by the whole CTA after.
+                        for (int i = a + tid; i < b; i += THREADS) {
+                            const int s0 = S.ostart[i] - base, lit = S.llen[i], ml = S.mlen[i];
+                            if (lit + ml > LONGSEQ) {
+                                S.longs[atomicAdd(&S.nlong, 1)] = i;
+                                continue;
                             }
-                            int s0 = S.ostart[l2] - base, s1 = S.ostart[l2 + 1] - base;
-                            int lit = S.llen[l2], d = S.off[l2], lp = S.lpos[l2];
-                            for (int x = x0; x < x1; x++) {
-                                while (x >= s1) {                   // next non-empty sequence
-                                    l2++;
-                                    s0 = s1;
-                                    s1 = S.ostart[l2 + 1] - base;
-                                    lit = S.llen[l2]; d = S.off[l2]; lp = S.lpos[l2];
-                                }
-                                const int rel = x - s0;
-                                uint32_t v;
-                                if (rel < lit) {
-                                    v = RES | S.win[lp + rel];
-                                } else {
-                                    const int m0 = s0 + lit, k = x - m0;
-                                    const int src = d > k ? x - d : m0 - d + k % d;
-                                    if (src >= 0) {
-                                        v = (uint32_t)src;
-                                    } else {                        // earlier output: the ring, else global
-                                        const int abs = op + base + src;
-                                        v = RES | (abs >= hist_from ? (uint32_t)S.hist[abs & (HB - 1)] : (uint32_t)__ldcg(out + abs));
-                                    }
-                                }
-                                S.st[x] = v;
+                            const int lp = S.lpos[i], d = S.off[i], m0 = s0 + lit;
+                            for (int r = 0; r < lit; r++) S.st[s0 + r] = RES | S.win[lp + r];
+                            int km = 0;                                  // k mod d
+                            for (int k = 0; k < ml; k++) {
+                                S.st[m0 + k] = src_entry(m0 - d + km);
+                                if (++km == d) km = 0;
                             }
                         }
                         __syncthreads();
+                        const int nlong = S.nlong;
+                        for (int j = 0; j < nlong; j++) {
+                            const int i = S.longs[j];
+                            const int s0 = S.ostart[i] - base, lit = S.llen[i], ml = S.mlen[i];
+                            const int lp = S.lpos[i], d = S.off[i], m0 = s0 + lit;
+                            for (int x = tid; x < lit + ml; x += THREADS)
+                                S.st[s0 + x] = x < lit ? RES | S.win[lp + x] : src_entry(m0 - d + (x - lit) % d);
+                        }
+                        __syncthreads();
+                        if (tid == 0) S.nlong = 0;                     // read above, before the barrier
                         for (;;) {                                 // pointer jumping
                             int open = 0;
                             for (int x = tid; x < span; x += THREADS) {
