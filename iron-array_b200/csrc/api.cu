@@ -476,28 +476,31 @@ static ina_rc_t decode_rc(int r)
     return INA_SUCCESS;
 }
 
-// Decode two stored (non-view) containers concurrently: the first on the context's
-// stream, the second on its second stream; returns after both finished.
+// Decode two stored (non-view) containers on the context's stream with one LZ4 launch for
+// the streams of both (one job queue), then each container's scatter; returns after both
+// finished.
 static ina_rc_t decode_pair(iarray_context_t *ctx, const iarray_container_t *a, void *da, int64_t lda,
                             const iarray_container_t *b, void *db, int64_t ldb)
 {
     // the padding columns past each row are left as they are: no product reads them
-    const Geom &ga = a->geom, &gb = b->geom;
-    cudaEventRecord(ctx->fork, ctx->stream);
-    cudaStreamWaitEvent(ctx->stream2, ctx->fork, 0);
-    iab::DecodeWork wa, wb;
-    int ra = 0, rb = 0;
-    if (ga.nchunks) ra = iab::decode_launch(ga, a->store->buf.as<uint8_t>(), (int64_t)a->store->buf.n, a->store->d_off.as<int64_t>(),
-                                            a->store->d_len.as<int32_t>(), da, lda, ctx->stream, &wa);
-    if (gb.nchunks) rb = iab::decode_launch(gb, b->store->buf.as<uint8_t>(), (int64_t)b->store->buf.n, b->store->d_off.as<int64_t>(),
-                                            b->store->d_len.as<int32_t>(), db, ldb, ctx->stream2, &wb);
-    cudaEventRecord(ctx->join, ctx->stream2);
-    cudaStreamWaitEvent(ctx->stream, ctx->join, 0);
-    if (ga.nchunks && !ra) ra = iab::decode_finish(&wa, ctx->stream);
-    if (gb.nchunks && !rb) rb = iab::decode_finish(&wb, ctx->stream2);
-    cudaStreamSynchronize(ctx->stream);
-    ina_rc_t rc = decode_rc(ra);
-    return INA_FAILED(rc) ? rc : decode_rc(rb);
+    const iarray_container_t *x[2] = {a, b};
+    const iab::DecodeArgs args[2] = {
+        {a->geom, a->store->buf.as<uint8_t>(), (int64_t)a->store->buf.n, a->store->d_off.as<int64_t>(),
+         a->store->d_len.as<int32_t>(), da, lda},
+        {b->geom, b->store->buf.as<uint8_t>(), (int64_t)b->store->buf.n, b->store->d_off.as<int64_t>(),
+         b->store->d_len.as<int32_t>(), db, ldb}};
+    iab::DecodeQueue q;
+    iab::DecodeWork w[2];
+    int r = iab::decode_queue_init(&q, iab::decode_max_jobs(a->geom) + iab::decode_max_jobs(b->geom), ctx->stream);
+    for (int k = 0; k < 2 && !r; k++)
+        if (x[k]->geom.nchunks) r = iab::decode_parse(args[k], &q, &w[k], ctx->stream);
+    if (!r) r = iab::decode_lz4(&q, ctx->stream);
+    for (int k = 0; k < 2 && !r; k++)
+        if (x[k]->geom.nchunks) r = iab::decode_scatter(args[k], &w[k], ctx->stream);
+    for (int k = 0; k < 2 && !r; k++)
+        if (x[k]->geom.nchunks) r = iab::decode_finish(&w[k], ctx->stream);
+    if (r) cudaStreamSynchronize(ctx->stream);     // the work buffers go back to the pool idle
+    return decode_rc(r);
 }
 
 static int64_t rows_of(const iarray_dtshape_t &d) { return d.ndim == 2 ? d.shape[0] : 1; }
@@ -1551,6 +1554,7 @@ struct iarray_b200_batch_s {
     std::vector<int64_t> M, N, K, lda, ldb, ldc;
     std::vector<DevBuf> dA, dB, dC, cbuf;
     std::vector<iab::DecodeWork> decA, decB;
+    iab::DecodeQueue dq;              // the LZ4 streams of every operand
     std::vector<iab::EncodeWork> enc;
     std::vector<iab::OzakiWork> oz;
     DevBuf status;                    // 16 ints per decode: [2i] operand A, [2i + 1] operand B
@@ -1623,23 +1627,37 @@ int batch_enqueue(iarray_b200_batch_t *bt, int parts)
     cudaStream_t st = bt->ctx->stream;
     int *status = bt->status.as<int>();
     const size_t nbr = bt->br.size();
-    if (parts & 1) batch_fork(bt);
-    for (int64_t i = 0; i < bt->n && (parts & 1); i++) {
-        cudaStream_t bs = bt->br[(size_t)i % nbr];
-        const iarray_container_t *x[2] = {bt->a[(size_t)i], bt->b[(size_t)i]};
-        DevBuf *dst[2] = {&bt->dA[(size_t)i], &bt->dB[(size_t)i]};
-        iab::DecodeWork *w[2] = {&bt->decA[(size_t)i], &bt->decB[(size_t)i]};
-        const int64_t ld[2] = {bt->lda[(size_t)i], bt->ldb[(size_t)i]};
-        for (int k = 0; k < 2; k++) {
-            if (!x[k]->geom.nchunks) continue;
-            w[k]->ext_counters = status + (2 * i + k) * 16;
-            const int r = iab::decode_launch(x[k]->geom, x[k]->store->buf.as<uint8_t>(), (int64_t)x[k]->store->buf.n,
-                                             x[k]->store->d_off.as<int64_t>(), x[k]->store->d_len.as<int32_t>(), dst[k]->p,
-                                             ld[k], bs, w[k]);
-            if (r) { batch_join(bt); return r; }
+    if (parts & 1) {
+        // every operand's parse on the branches, one LZ4 launch for the streams of all of
+        // them, then every operand's scatter on the branches
+        auto operand = [&](int64_t i, int k) {
+            const iarray_container_t *x = k ? bt->b[(size_t)i] : bt->a[(size_t)i];
+            return iab::DecodeArgs{x->geom, x->store->buf.as<uint8_t>(), (int64_t)x->store->buf.n,
+                                   x->store->d_off.as<int64_t>(), x->store->d_len.as<int32_t>(),
+                                   (k ? bt->dB : bt->dA)[(size_t)i].p, k ? bt->ldb[(size_t)i] : bt->lda[(size_t)i]};
+        };
+        int64_t mj = 0;
+        for (int64_t i = 0; i < bt->n; i++)
+            for (int k = 0; k < 2; k++) mj += iab::decode_max_jobs(operand(i, k).g);
+        int r = iab::decode_queue_init(&bt->dq, mj, st);
+        if (r) return r;
+        for (int pass = 0; pass < 2; pass++) {
+            batch_fork(bt);
+            for (int64_t i = 0; i < bt->n && !r; i++) {
+                cudaStream_t bs = bt->br[(size_t)i % nbr];
+                for (int k = 0; k < 2 && !r; k++) {
+                    const iab::DecodeArgs a = operand(i, k);
+                    if (!a.g.nchunks) continue;
+                    iab::DecodeWork *w = k ? &bt->decB[(size_t)i] : &bt->decA[(size_t)i];
+                    w->ext_counters = status + (2 * i + k) * 16;
+                    r = pass ? iab::decode_scatter(a, w, bs) : iab::decode_parse(a, &bt->dq, w, bs);
+                }
+            }
+            batch_join(bt);
+            if (r) return r;
+            if (!pass) iab::decode_lz4(&bt->dq, st);
         }
     }
-    if (parts & 1) batch_join(bt);
     if (!(parts & 2)) {
     } else if (bt->form == IARRAY_B200_FORM_SPLIT) {
         batch_fork(bt);

@@ -25,6 +25,7 @@
 #include <stdint.h>
 
 #include "common.cuh"
+#include "tc_common.cuh"
 
 namespace iab {
 
@@ -41,7 +42,7 @@ __device__ __forceinline__ void dev_fail(int *err, int code) { atomicCAS(err, 0,
 // D0: parse one (chunk, block) per thread.
 __global__ void k_parse(Geom g, const uint8_t *__restrict__ ch, const int64_t *__restrict__ off,
                         const int32_t *__restrict__ len, BlockDesc *bd, StreamDesc *sd, Lz4Job *jobs,
-                        int *njobs, int *err)
+                        int *njobs, int64_t jcap, int *err, uint8_t *scratch)
 {
     const int64_t total = g.nchunks * g.nblocks;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
@@ -110,9 +111,14 @@ __global__ void k_parse(Geom g, const uint8_t *__restrict__ ch, const int64_t *_
             } else {
                 s[j].kind = SK_LZ4;
                 const int k = atomicAdd(njobs, 1);
-                Lz4Job jb;
-                jb.src = off[c] + q; jb.csize = cs; jb.dst = t * g.blocksize + (int64_t)j * neblock; jb.dlen = neblock;
-                jobs[k] = jb;
+                if (k < jcap) {
+                    Lz4Job jb;
+                    jb.src = ch + off[c] + q; jb.dst = scratch + t * g.blocksize + (int64_t)j * neblock; jb.err = err;
+                    jb.csize = cs; jb.dlen = neblock;
+                    jobs[k] = jb;
+                } else {
+                    dev_fail(err, DE_BOUNDS);                            // queue full: left undecoded
+                }
             }
             q += cs;
         }
@@ -122,7 +128,8 @@ __global__ void k_parse(Geom g, const uint8_t *__restrict__ ch, const int64_t *_
 }
 
 // D1: LZ4 stream decode, one CTA (256 threads) per stream, streams handed out
-// dynamically.  The stream is consumed in windows of up to DW compressed bytes staged in
+// dynamically from a job queue (which may hold the streams of several containers: each job
+// carries its source, destination and status word).  The stream is consumed in windows of up to DW compressed bytes staged in
 // shared memory, and each window is decoded without any serial walk:
 //  1. for every byte q of the window, next[q] = where the following token would start if
 //     a sequence began at q (STOP when that sequence does not end inside the window,
@@ -198,16 +205,15 @@ __device__ __forceinline__ uint16_t dcta_next(const uint8_t *win, int q, int n, 
     return (uint16_t)r;                   // r <= n; r == n: the next token starts the next window
 }
 
-__global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const uint8_t *__restrict__ ch,
-                                                                  const Lz4Job *__restrict__ jobs,
-                                                                  const int *__restrict__ njobs_p, uint8_t *scratch,
-                                                                  int *err, unsigned *next_job)
+__global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const Lz4Job *__restrict__ jobs,
+                                                                  const int *__restrict__ njobs_p, int64_t jcap,
+                                                                  unsigned *next_job)
 {
     using namespace dcta;
     extern __shared__ __align__(16) uint8_t sm_dcta[];
     Smem &S = *reinterpret_cast<Smem *>(sm_dcta);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int njobs = *njobs_p;
+    const int njobs = (int)min((int64_t)*njobs_p, jcap);
     if (tid == 0) S.nlong = 0;                     // first use follows the barriers below
     for (;;) {
         __syncthreads();
@@ -216,9 +222,9 @@ __global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const uint8
         const int jid = S.scal[0];
         if (jid >= njobs) break;
         const Lz4Job jb = jobs[jid];
-        const uint8_t *__restrict__ in = ch + jb.src;
+        const uint8_t *__restrict__ in = jb.src;
         const int isz = jb.csize;
-        uint8_t *out = scratch + jb.dst;
+        uint8_t *out = jb.dst;
         const int osz = jb.dlen;
         int p = 0, op = 0;                 // window start in the input, output written so far
         int hist_from = 0;                 // S.hist holds output bytes [hist_from, written)
@@ -471,7 +477,7 @@ __global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const uint8
             }
         }
         if (!bad && op != osz) bad = true;
-        if (bad && tid == 0) dev_fail(err, DE_LZ4);
+        if (bad && tid == 0) dev_fail(jb.err, DE_LZ4);
     }
 }
 
@@ -548,53 +554,140 @@ __device__ __forceinline__ uint32_t ld4_any(const uint8_t *p, const uint8_t *lim
            ((uint32_t)__ldg(p + 3) << 24);
 }
 
-// D2 fast path: one CTA per interior, shuffled, split block; each thread rebuilds 4
-// consecutive items from one 4-byte word per byte plane (read in place from raw streams
-// or the LZ4 scratch) and writes them to the dense row.  Every other block is appended to
-// the list `rest` for the general path.
+// D2 fast path: interior, shuffled, split blocks, in slices of SC_ITEMS items (one CTA per
+// slice at a time).  One thread stages the slice's bytes of every byte plane (read in place
+// from raw streams or the LZ4 scratch) into shared memory with bulk asynchronous copies
+// completing on an mbarrier; then each thread rebuilds 4 consecutive items from one 4-byte
+// word per plane and writes them to the dense row.  Every other block is appended to the
+// list `rest` for the general path.
+constexpr int SC_ITEMS = 4096;
+constexpr int SC_PLANE = SC_ITEMS + 32;            // a slice of a plane from its 16-byte boundary
+constexpr uint32_t SC_WAIT_POLLS = 1u << 22;
+
+__device__ __forceinline__ void bulk_g2s(void *sdst, const void *gsrc, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(tc::smem_addr(sdst)), "l"(gsrc), "r"(bytes), "r"(tc::smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool sc_wait(uint64_t *bar, uint32_t parity)
+{
+    for (uint32_t i = 0; i < SC_WAIT_POLLS; i++)
+        if (tc::mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
 template <int TS>
-__global__ void __launch_bounds__(256) k_scatter_fast(Geom g, const uint8_t *__restrict__ ch, const uint8_t *ch_end,
+__global__ void __launch_bounds__(256, 6) k_scatter_fast(Geom g, const uint8_t *__restrict__ ch, const uint8_t *ch_end,
                                                       const BlockDesc *__restrict__ bd,
                                                       const StreamDesc *__restrict__ sd,
                                                       const uint8_t *__restrict__ scratch, const uint8_t *scratch_end,
-                                                      uint8_t *__restrict__ out, int64_t ld, int *rest, int *nrest)
+                                                      uint8_t *__restrict__ out, int64_t ld, int *rest, int *nrest,
+                                                      int *err)
 {
+    __shared__ __align__(128) uint8_t stage[TS][SC_PLANE];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int abort_all;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        tc::mbar_init(&bar, 1);
+        tc::fence_barrier_init();
+        abort_all = 0;
+    }
+    __syncthreads();
     const int64_t nbl = g.nchunks * g.nblocks;
-    const int qpr = (int)(g.block[1] / 4), nq = (int)(g.blockn / 4);
-    for (int64_t t = blockIdx.x; t < nbl; t += gridDim.x) {
+    const int64_t nsl = (g.blockn + SC_ITEMS - 1) / SC_ITEMS;
+    const int qpr = (int)(g.block[1] / 4);
+    uint32_t parity = 0;
+    for (int64_t u = blockIdx.x; u < nbl * nsl; u += gridDim.x) {
+        const int64_t t = u / nsl;
+        const int sl = (int)(u - t * nsl);
         const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
         const BlockDesc d = bd[t];
         if (d.mode != BM_SHUFFLED || d.nstreams != TS || !block_fast(g, c, b)) {
-            if (threadIdx.x == 0) rest[atomicAdd(nrest, 1)] = (int)t;   // left to k_scatter
+            if (tid == 0 && sl == 0) rest[atomicAdd(nrest, 1)] = (int)t;   // left to k_scatter
             continue;
         }
-        const uint8_t *base[TS];
-        const uint8_t *lim[TS];
-        uint32_t fill[TS];
+        const int i0s = sl * SC_ITEMS, cnt = (int)min((int64_t)SC_ITEMS, g.blockn - i0s);
+        // per plane: its slice starts at src, 16-byte word a16 = src - shift; the bulk copy
+        // takes the whole words of [a16, a16 + want) before the buffer end lim, threads copy
+        // the bytes that the buffer end cuts off (zeros past it)
+        auto plane = [&](int j, const uint8_t *&src, const uint8_t *&lim, int &want, int &bulk) {
+            const StreamDesc q = sd[t * 8 + j];
+            src = nullptr; lim = nullptr;
+            if (q.kind == SK_RAW) { src = ch + q.src + i0s; lim = ch_end; }
+            else if (q.kind == SK_LZ4) { src = scratch + t * g.blocksize + (int64_t)j * d.neblock + i0s; lim = scratch_end; }
+            want = bulk = 0;
+            if (src) {
+                const uint8_t *a16 = src - (reinterpret_cast<uintptr_t>(src) & 15);
+                want = ((int)(src - a16) + cnt + 15) & ~15;
+                bulk = (int)min((int64_t)want, (lim - a16) & ~int64_t(15));
+            }
+            return q;
+        };
+        if (tid == 0) {
+            uint32_t tx = 0;
+#pragma unroll
+            for (int j = 0; j < TS; j++) {
+                const uint8_t *src, *lim;
+                int want, bulk;
+                plane(j, src, lim, want, bulk);
+                tx += (uint32_t)bulk;
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier reads of stage precede the copies
+            tc::mbar_arrive_expect_tx(&bar, tx);
+#pragma unroll
+            for (int j = 0; j < TS; j++) {
+                const uint8_t *src, *lim;
+                int want, bulk;
+                plane(j, src, lim, want, bulk);
+                if (bulk > 0) bulk_g2s(stage[j], src - (reinterpret_cast<uintptr_t>(src) & 15), (uint32_t)bulk, &bar);
+            }
+        }
+        int code[TS];                                  // 0..15: the plane's shift in stage; 256 + v: a run of byte v
 #pragma unroll
         for (int j = 0; j < TS; j++) {
-            const StreamDesc q = sd[t * 8 + j];
-            fill[j] = q.kind == SK_RUN ? (uint32_t)q.len * 0x01010101u : 0u;
-            if (q.kind == SK_RAW) { base[j] = ch + q.src; lim[j] = ch_end; }
-            else if (q.kind == SK_LZ4) { base[j] = scratch + t * g.blocksize + (int64_t)j * d.neblock; lim[j] = scratch_end; }
-            else { base[j] = nullptr; lim[j] = nullptr; }
+            const uint8_t *src, *lim;
+            int want, bulk;
+            const StreamDesc q = plane(j, src, lim, want, bulk);
+            code[j] = src ? (int)(reinterpret_cast<uintptr_t>(src) & 15) : 256 + (q.kind == SK_RUN ? (q.len & 255) : 0);
+            if (bulk < want) {
+                const uint8_t *a16 = src - code[j];
+                for (int x = bulk + tid; x < want; x += blockDim.x) stage[j][x] = a16 + x < lim ? __ldg(a16 + x) : (uint8_t)0;
+            }
+        }
+        const bool ok = sc_wait(&bar, parity);
+        parity ^= 1;
+        if (!ok) abort_all = 1;
+        __syncthreads();
+        if (abort_all) {                               // the copies did not complete: report, wait once more, leave
+            if (tid == 0) {
+                dev_fail(err, DE_WAIT);
+                sc_wait(&bar, parity ^ 1);
+            }
+            return;
         }
         const int64_t ci0 = c / g.cgrid[1], ci1 = c - ci0 * g.cgrid[1];
         const int64_t bi0 = b / g.bgrid[1], bi1 = b - bi0 * g.bgrid[1];
         const int64_t row0 = ci0 * g.chunk[0] + bi0 * g.block[0], col0 = ci1 * g.chunk[1] + bi1 * g.block[1];
-        for (int qd = threadIdx.x; qd < nq; qd += blockDim.x) {
-            const int i0 = qd * 4, r = qd / qpr, cc = (qd - r * qpr) * 4;
+        for (int qd = tid; qd < cnt / 4; qd += blockDim.x) {
             uint32_t w[TS];
 #pragma unroll
-            for (int j = 0; j < TS; j++) w[j] = base[j] ? ld4_any(base[j] + i0, lim[j]) : fill[j];
+            for (int j = 0; j < TS; j++) {
+                if (code[j] >= 256) { w[j] = (uint32_t)(code[j] - 256) * 0x01010101u; continue; }
+                const uint32_t *pw = reinterpret_cast<const uint32_t *>(stage[j]);
+                const int byte = code[j] + qd * 4, wi = byte >> 2, sh = (byte & 3) * 8;
+                w[j] = sh ? __funnelshift_r(pw[wi], pw[wi + 1], sh) : pw[wi];
+            }
+            const int it = i0s + qd * 4, r = it / (qpr * 4), cc = it - r * qpr * 4;
             uint8_t *o = out + ((row0 + r) * ld + col0 + cc) * TS;
             uint32_t v0, v1, v2, v3;
             transpose4x4(w[0], w[1], w[2], w[3], v0, v1, v2, v3);
-            const bool a16 = (reinterpret_cast<uintptr_t>(o) & 15) == 0;
+            const bool o16a = (reinterpret_cast<uintptr_t>(o) & 15) == 0;
             if constexpr (TS == 8) {
                 uint32_t h0, h1, h2, h3;
                 transpose4x4(w[4], w[5], w[6], w[7], h0, h1, h2, h3);
-                if (a16) {
+                if (o16a) {
                     uint4 *o16 = reinterpret_cast<uint4 *>(o);
                     o16[0] = make_uint4(v0, h0, v1, h1);
                     o16[1] = make_uint4(v2, h2, v3, h3);
@@ -606,7 +699,7 @@ __global__ void __launch_bounds__(256) k_scatter_fast(Geom g, const uint8_t *__r
                     o8[3] = ((uint64_t)h3 << 32) | v3;
                 }
             } else {
-                if (a16) {
+                if (o16a) {
                     *reinterpret_cast<uint4 *>(o) = make_uint4(v0, v1, v2, v3);
                 } else {
                     uint32_t *o4 = reinterpret_cast<uint32_t *>(o);
@@ -614,6 +707,7 @@ __global__ void __launch_bounds__(256) k_scatter_fast(Geom g, const uint8_t *__r
                 }
             }
         }
+        __syncthreads();                               // stage is read before the next slice's copies
     }
 }
 
@@ -1352,6 +1446,8 @@ __device__ __forceinline__ int cta_lz4_compress_par(const uint8_t *__restrict__ 
                 for (int t = 0; t < 2; t++) {
                     const int c = t ? p - 1 : cand;
                     if (!valid[k] || c >= p || c < 0 || p - c > 65535 || (t && c == cand)) continue;
+                    // the previous position matches only inside a run: the 4 bytes at p are equal
+                    if (t && v != (v & 0xFFu) * 0x01010101u) continue;
                     const bool inring = c >= s.lo;
                     if ((inring ? par_rd32(ring_s, c) : ld4u(src + c)) != v) continue;
                     int l = 4;
@@ -1893,62 +1989,109 @@ int decode_finish(DecodeWork *w, cudaStream_t st)
     return h_err;
 }
 
-int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, const int64_t *d_off, const int32_t *d_len, void *out,
-                  int64_t ld, cudaStream_t st, DecodeWork *w)
+// Grid of the fast scatter: the CTAs resident at once (one wave), at most one per slice.
+template <int TS>
+static int64_t scatter_fast_grid(const Geom &g, int64_t nbl)
+{
+    static int per_sm = 0;
+    if (!per_sm) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_scatter_fast<TS>, 256, 0) != cudaSuccess || n < 1) {
+            cudaGetLastError();
+            n = 4;
+        }
+        per_sm = n;
+    }
+    const int64_t units = nbl * ((g.blockn + SC_ITEMS - 1) / SC_ITEMS);
+    return std::max<int64_t>(std::min<int64_t>(units, (int64_t)sm_count() * per_sm), 1);
+}
+
+int64_t decode_max_jobs(const Geom &g) { return g.nchunks * g.nblocks * 8; }
+
+int decode_queue_init(DecodeQueue *q, int64_t max_jobs, cudaStream_t st)
 {
     int dev = 0;
     cudaGetDevice(&dev);
-    const int64_t nbl = g.nchunks * g.nblocks;
-    DevBuf &bd = w->bd, &sd = w->sd, &jobs = w->jobs, &scratch = w->scratch, &counters = w->counters;
-    if (!bd.allocate(sizeof(BlockDesc) * nbl, dev) || !sd.allocate(sizeof(StreamDesc) * nbl * 8, dev) ||
-        !jobs.allocate(sizeof(Lz4Job) * nbl * 8, dev) || !scratch.allocate((size_t)(nbl * g.blocksize), dev) ||
-        (!w->ext_counters && !counters.allocate(64, dev)))
+    if (!q->jobs.allocate(sizeof(Lz4Job) * (size_t)std::max<int64_t>(max_jobs, 1), dev) || !q->counters.allocate(64, dev))
         return -100;
-    int *cnt = w->ext_counters ? w->ext_counters : counters.as<int>();
-    int *njobs = cnt, *err = cnt + 1;
-    cudaMemsetAsync(cnt, 0, 64, st);
-    const int sms = sm_count();
-    {
-        const int threads = 128;
-        const int64_t blocks = std::min<int64_t>((nbl + threads - 1) / threads, (int64_t)sms * 16);
-        IAB_TIMED("k_parse", st, k_parse<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, st>>>(g, d_chunks, d_off, d_len, bd.as<BlockDesc>(),
-                                                                          sd.as<StreamDesc>(), jobs.as<Lz4Job>(), njobs, err));
-    }
-    {
-        static bool attr = false;
-        const int smem = (int)sizeof(dcta::Smem);
-        if (!attr) {
-            cudaFuncSetAttribute(k_lz4_decode_cta, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            attr = true;
-        }
-        IAB_TIMED("k_lz4_decode_cta", st, k_lz4_decode_cta<<<sms * 5, dcta::THREADS, smem, st>>>(
-            d_chunks, jobs.as<Lz4Job>(), njobs, scratch.as<uint8_t>(), err,
-            reinterpret_cast<unsigned *>(cnt + 2)));
-    }
-    {
-        const int64_t tpb = (g.blockn + TILE - 1) / TILE;
-        const int64_t nwork = nbl * tpb;
-        const int64_t blocks = std::min<int64_t>(nwork, (int64_t)sms * 8);
-        const bool fast = g.itemsize == 4 || g.itemsize == 8;
-        int *rest = nullptr, *nrest = cnt + 3;
-        if (fast) {
-            if (!w->rest.allocate(sizeof(int) * (size_t)nbl, dev)) return -100;
-            rest = w->rest.as<int>();
-            const int64_t fb = std::min<int64_t>(nbl, (int64_t)sms * 8);
-            const uint8_t *cend = d_chunks + chunks_bytes, *send = scratch.as<uint8_t>() + nbl * g.blocksize;
-            if (g.itemsize == 8)
-                IAB_TIMED("k_scatter_fast", st, k_scatter_fast<8><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
-                    g, d_chunks, cend, bd.as<BlockDesc>(), sd.as<StreamDesc>(), scratch.as<uint8_t>(), send, (uint8_t *)out, ld,
-                    rest, nrest));
-            else
-                IAB_TIMED("k_scatter_fast", st, k_scatter_fast<4><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
-                    g, d_chunks, cend, bd.as<BlockDesc>(), sd.as<StreamDesc>(), scratch.as<uint8_t>(), send, (uint8_t *)out, ld,
-                    rest, nrest));
-        }
-        IAB_TIMED("k_scatter", st, k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
-            g, rest, nrest, d_chunks, bd.as<BlockDesc>(), sd.as<StreamDesc>(), scratch.as<uint8_t>(), (uint8_t *)out, ld));
-    }
+    q->cap = max_jobs;
+    cudaMemsetAsync(q->counters.p, 0, 64, st);
     return 0;
+}
+
+int decode_parse(const DecodeArgs &a, DecodeQueue *q, DecodeWork *w, cudaStream_t st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const Geom &g = a.g;
+    const int64_t nbl = g.nchunks * g.nblocks;
+    if (!w->bd.allocate(sizeof(BlockDesc) * nbl, dev) || !w->sd.allocate(sizeof(StreamDesc) * nbl * 8, dev) ||
+        !w->scratch.allocate((size_t)(nbl * g.blocksize), dev) || (!w->ext_counters && !w->counters.allocate(64, dev)))
+        return -100;
+    int *cnt = w->ext_counters ? w->ext_counters : w->counters.as<int>();
+    cudaMemsetAsync(cnt, 0, 64, st);
+    const int threads = 128;
+    const int64_t blocks = std::min<int64_t>((nbl + threads - 1) / threads, (int64_t)sm_count() * 16);
+    IAB_TIMED("k_parse", st, k_parse<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, st>>>(
+        g, a.chunks, a.off, a.len, w->bd.as<BlockDesc>(), w->sd.as<StreamDesc>(), q->jobs.as<Lz4Job>(),
+        q->counters.as<int>(), q->cap, cnt + 1, w->scratch.as<uint8_t>()));
+    return 0;
+}
+
+int decode_lz4(DecodeQueue *q, cudaStream_t st)
+{
+    static bool attr = false;
+    const int smem = (int)sizeof(dcta::Smem);
+    if (!attr) {
+        cudaFuncSetAttribute(k_lz4_decode_cta, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr = true;
+    }
+    int *qc = q->counters.as<int>();
+    IAB_TIMED("k_lz4_decode_cta", st, k_lz4_decode_cta<<<sm_count() * 5, dcta::THREADS, smem, st>>>(
+        q->jobs.as<Lz4Job>(), qc, q->cap, reinterpret_cast<unsigned *>(qc + 1)));
+    return 0;
+}
+
+int decode_scatter(const DecodeArgs &a, DecodeWork *w, cudaStream_t st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const Geom &g = a.g;
+    const int64_t nbl = g.nchunks * g.nblocks;
+    int *cnt = w->ext_counters ? w->ext_counters : w->counters.as<int>();
+    const int sms = sm_count();
+    const uint8_t *scratch = w->scratch.as<uint8_t>();
+    const int64_t tpb = (g.blockn + TILE - 1) / TILE;
+    const int64_t blocks = std::min<int64_t>(nbl * tpb, (int64_t)sms * 8);
+    const bool fast = g.itemsize == 4 || g.itemsize == 8;
+    int *rest = nullptr, *nrest = cnt + 3;
+    if (fast) {
+        if (!w->rest.allocate(sizeof(int) * (size_t)nbl, dev)) return -100;
+        rest = w->rest.as<int>();
+        const uint8_t *cend = a.chunks + a.chunks_bytes, *send = scratch + nbl * g.blocksize;
+        if (g.itemsize == 8)
+            IAB_TIMED("k_scatter_fast", st, k_scatter_fast<8><<<(unsigned)scatter_fast_grid<8>(g, nbl), 256, 0, st>>>(
+                g, a.chunks, cend, w->bd.as<BlockDesc>(), w->sd.as<StreamDesc>(), scratch, send, (uint8_t *)a.out, a.ld,
+                rest, nrest, cnt + 1));
+        else
+            IAB_TIMED("k_scatter_fast", st, k_scatter_fast<4><<<(unsigned)scatter_fast_grid<4>(g, nbl), 256, 0, st>>>(
+                g, a.chunks, cend, w->bd.as<BlockDesc>(), w->sd.as<StreamDesc>(), scratch, send, (uint8_t *)a.out, a.ld,
+                rest, nrest, cnt + 1));
+    }
+    IAB_TIMED("k_scatter", st, k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
+        g, rest, nrest, a.chunks, w->bd.as<BlockDesc>(), w->sd.as<StreamDesc>(), scratch, (uint8_t *)a.out, a.ld));
+    return 0;
+}
+
+int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, const int64_t *d_off, const int32_t *d_len, void *out,
+                  int64_t ld, cudaStream_t st, DecodeWork *w)
+{
+    const DecodeArgs a{g, d_chunks, chunks_bytes, d_off, d_len, out, ld};
+    int r = decode_queue_init(&w->queue, decode_max_jobs(g), st);
+    if (!r) r = decode_parse(a, &w->queue, w, st);
+    if (!r) r = decode_lz4(&w->queue, st);
+    if (!r) r = decode_scatter(a, w, st);
+    return r;
 }
 
 int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, DevBuf *d_out, EncodeWork *w,
@@ -2144,11 +2287,12 @@ int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes,
     {
         const int threads = 128;
         const int64_t blocks = std::min<int64_t>((nbl + threads - 1) / threads, (int64_t)sms * 16);
-        IAB_TIMED("k_parse", st, k_parse<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, st>>>(g, d_chunks, off, len, bd, sd, jobs, njobs, err));
+        IAB_TIMED("k_parse", st, k_parse<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, st>>>(g, d_chunks, off, len, bd, sd, jobs, njobs,
+                                                                                      8 * NA_MAX_BLOCKS, err, img));
     }
     {
         IAB_TIMED("k_lz4_decode_cta", st, k_lz4_decode_cta<<<sms * 5, dcta::THREADS, (int)sizeof(dcta::Smem), st>>>(
-            d_chunks, jobs, njobs, img, err, reinterpret_cast<unsigned *>(counters + 2)));
+            jobs, njobs, 8 * NA_MAX_BLOCKS, reinterpret_cast<unsigned *>(counters + 2)));
     }
     {
         const int64_t tpb = (g.blockn + TILE - 1) / TILE;
@@ -2156,14 +2300,13 @@ int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes,
         const bool fast = g.itemsize == 4 || g.itemsize == 8;
         int *rest = fast ? reinterpret_cast<int *>(base + NA_REST) : nullptr, *nrest = counters + 3;
         if (fast) {
-            const int64_t fb = std::min<int64_t>(nbl, (int64_t)sms * 8);
             const uint8_t *cend = d_chunks + chunks_bytes, *send = img + nbl * g.blocksize;
             if (g.itemsize == 8)
-                IAB_TIMED("k_scatter_fast", st, k_scatter_fast<8><<<(unsigned)fb, 256, 0, st>>>(
-                    g, d_chunks, cend, bd, sd, img, send, (uint8_t *)out, ld, rest, nrest));
+                IAB_TIMED("k_scatter_fast", st, k_scatter_fast<8><<<(unsigned)scatter_fast_grid<8>(g, nbl), 256, 0, st>>>(
+                    g, d_chunks, cend, bd, sd, img, send, (uint8_t *)out, ld, rest, nrest, err));
             else
-                IAB_TIMED("k_scatter_fast", st, k_scatter_fast<4><<<(unsigned)fb, 256, 0, st>>>(
-                    g, d_chunks, cend, bd, sd, img, send, (uint8_t *)out, ld, rest, nrest));
+                IAB_TIMED("k_scatter_fast", st, k_scatter_fast<4><<<(unsigned)scatter_fast_grid<4>(g, nbl), 256, 0, st>>>(
+                    g, d_chunks, cend, bd, sd, img, send, (uint8_t *)out, ld, rest, nrest, err));
         }
         IAB_TIMED("k_scatter", st, k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
             g, rest, nrest, d_chunks, bd, sd, img, (uint8_t *)out, ld));

@@ -54,8 +54,9 @@ struct BlockDesc {
 };
 
 struct Lz4Job {       // decode job: one LZ4 stream
-    int64_t src;      // payload offset in chunk buffer
-    int64_t dst;      // offset in the scratch image
+    const uint8_t *src;  // payload in the container's chunk buffer
+    uint8_t *dst;        // its place in the container's decoded-stream image
+    int *err;            // the container's status word
     int32_t csize;
     int32_t dlen;
 };
@@ -80,6 +81,7 @@ enum DevErr : int32_t {
     DE_BOUNDS = 2,      // a bstart / csize points outside the chunk
     DE_LZ4 = 3,         // malformed LZ4 stream
     DE_RUN_TOKEN = 4,   // negative csize without a valid run token
+    DE_WAIT = 5,        // a bounded wait for an asynchronous copy gave up
 };
 
 // ------------------------------------------------------------------ device memory pool
@@ -149,15 +151,41 @@ struct CodecStats { int32_t err; };
 int decode_container(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, const int64_t *d_off,
                      const int32_t *d_len, void *out, int64_t ld, cudaStream_t st);
 
+struct DecodeArgs {
+    Geom g;
+    const uint8_t *chunks;  // the container's chunks, back to back
+    int64_t chunks_bytes;
+    const int64_t *off;     // chunk offsets and lengths (device)
+    const int32_t *len;
+    void *out;              // dense row-major destination
+    int64_t ld;             // its leading dimension in items
+};
+struct DecodeQueue {
+    DevBuf jobs, counters;  // counters: [0] jobs queued, [1] the next job to hand out
+    int64_t cap = 0;
+};
 // Asynchronous form: decode_launch enqueues the kernels on `st` (work buffers held in
 // *w until decode_finish, which synchronises `st` and returns the DevErr).
 struct DecodeWork {
-    DevBuf bd, sd, jobs, scratch, counters, rest;
+    DevBuf bd, sd, scratch, counters, rest;
+    DecodeQueue queue;             // the job queue of decode_launch (unused by decode_parse / _scatter)
     int *ext_counters = nullptr;   // optional caller-owned 16-int status slot (device) instead of `counters`
 };
 int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, const int64_t *d_off, const int32_t *d_len,
                   void *out, int64_t ld, cudaStream_t st, DecodeWork *w);
 int decode_finish(DecodeWork *w, cudaStream_t st);
+
+// Several containers decoded with one LZ4 launch: decode_queue_init (on the stream that
+// will run the LZ4 launch), then decode_parse of each container (any streams ordered after
+// the init), decode_lz4 once (ordered after every parse), then decode_scatter of each
+// container (after the LZ4 launch); decode_finish(w) per container as above.  The LZ4
+// streams of all containers are handed out from one queue, so the LZ4 kernel's CTAs stay
+// busy across container boundaries.
+int decode_queue_init(DecodeQueue *q, int64_t max_jobs, cudaStream_t st);
+int64_t decode_max_jobs(const Geom &g);
+int decode_parse(const DecodeArgs &a, DecodeQueue *q, DecodeWork *w, cudaStream_t st);
+int decode_lz4(DecodeQueue *q, cudaStream_t st);
+int decode_scatter(const DecodeArgs &a, DecodeWork *w, cudaStream_t st);
 
 // Decode without allocating: the work buffers live in a fixed device array of the library
 // (at most NOALLOC_MAX_BYTES decoded bytes and NOALLOC_MAX_BLOCKS blocks per call; larger
