@@ -637,16 +637,16 @@ def run_ours(args):
 
 def run_profile_case(args):
     """Small cases for ncu captures (--set full on one kernel family at a time).
-    codec: a 4096 x 4096 float64 container of the product's kind of values (gaussian) encoded
+    codec: an n x n float64 container (n = --profile-n, default 4096) of the product's kind of values (gaussian) encoded
     with the parallel encoder, then an A-like one (uniform(-1,1) x 2^U{-8..8}) decoded; three
-    rounds each.  split: the split-precision float64 product 4096 x 4096 x 4096 on device
+    rounds each.  split: the split-precision float64 product n x n x n on device
     operands (iarray_b200_dense_gemm), two rounds.  Inputs are larger than L2."""
     import ctypes
     import torch
     import iarray_b200 as ia
     ia.init()
     rng = np.random.default_rng(5)
-    n = 4096
+    n = args.profile_n
     if args.profile_case == "codec":
         ctx = ia.Context(encoder=ia.ENCODER_PARALLEL)
         C = rng.standard_normal((n, n)) * 600.0
@@ -687,6 +687,7 @@ def main():
     ap.add_argument("--no-secondary", action="store_true", help="skip the GEMV, float32 and batching workloads")
     ap.add_argument("--profile-case", choices=["codec", "split"], default=None,
                     help="run one small case for an ncu capture instead of the benchmark")
+    ap.add_argument("--profile-n", type=int, default=4096, help="matrix size of --profile-case")
     args = ap.parse_args()
     if args.profile_case:
         run_profile_case(args)
