@@ -172,10 +172,11 @@ struct iarray_context_s {
     int encoder = IARRAY_B200_ENCODER_LIBLZ4;
     double timings[5] = {0, 0, 0, 0, 0};
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-    cudaStream_t stream2 = nullptr;          // second stream for concurrent operand decode
+    cudaStream_t stream2 = nullptr;          // second stream (operand decode of the pipelined call)
     cudaEvent_t fork = nullptr, join = nullptr;
-    // iarray_b200_opt_gemm_cframes: copy streams and pinned staging for chunk tables
-    cudaStream_t up = nullptr, down = nullptr, enc = nullptr;
+    // iarray_b200_opt_gemm_cframes: copy streams, the encode stream, the chunk-table copy
+    // stream and pinned staging for chunk tables
+    cudaStream_t up = nullptr, down = nullptr, enc = nullptr, tabs = nullptr;
     void *pin = nullptr;
     size_t pin_n = 0;
 };
@@ -286,6 +287,7 @@ INA_API(void) iarray_context_free(iarray_context_t **ctx)
     if (c->up) { cudaStreamSynchronize(c->up); cudaStreamDestroy(c->up); }
     if (c->down) { cudaStreamSynchronize(c->down); cudaStreamDestroy(c->down); }
     if (c->enc) { cudaStreamSynchronize(c->enc); cudaStreamDestroy(c->enc); }
+    if (c->tabs) { cudaStreamSynchronize(c->tabs); cudaStreamDestroy(c->tabs); }
     if (c->pin) cudaFreeHost(c->pin);
     if (c->fork) cudaEventDestroy(c->fork);
     if (c->join) cudaEventDestroy(c->join);
@@ -1388,7 +1390,8 @@ INA_API(ina_rc_t) iarray_b200_opt_gemm_cframes(iarray_context_t *ctx, const uint
     if (!ctx->up) cudaStreamCreateWithFlags(&ctx->up, cudaStreamNonBlocking);
     if (!ctx->down) cudaStreamCreateWithFlags(&ctx->down, cudaStreamNonBlocking);
     if (!ctx->enc) cudaStreamCreateWithFlags(&ctx->enc, cudaStreamNonBlocking);
-    if (!ctx->up || !ctx->down || !ctx->enc || !ctx->stream2) return rc_err(IARRAY_ERR_GPU_FAILED);
+    if (!ctx->tabs) cudaStreamCreateWithFlags(&ctx->tabs, cudaStreamNonBlocking);
+    if (!ctx->up || !ctx->down || !ctx->enc || !ctx->tabs || !ctx->stream2) return rc_err(IARRAY_ERR_GPU_FAILED);
     cudaStream_t st = ctx->stream;
     const int isz = fa.g.itemsize;
     const int64_t lda = pad_ld(K), ldb = pad_ld(N), ldc = pad_ld(N);
@@ -1430,7 +1433,7 @@ INA_API(ina_rc_t) iarray_b200_opt_gemm_cframes(iarray_context_t *ctx, const uint
     Timer tm(ctx);                 // timings: [0] B decoded and prepared, [3] the bands, [4] total
     tm.mark(1);
     int err = 0;
-    EventSet evD((size_t)rowsA + 1), evP((size_t)bands);
+    EventSet evD((size_t)rowsA + 1), evP((size_t)bands), evK((size_t)bands);
     std::vector<iab::DecodeWork> decB((size_t)rowsB), decA((size_t)rowsA);
     for (int64_t r = 0; r < rowsB && !err; r++) {
         cudaStreamWaitEvent(sd, evB.ev[(size_t)r], 0);
@@ -1481,6 +1484,12 @@ INA_API(ina_rc_t) iarray_b200_opt_gemm_cframes(iarray_context_t *ctx, const uint
     int64_t queued = 0;            // bands whose encode is queued
     for (int64_t k = 0; k < bands && !err; k++) {
         cudaStreamWaitEvent(st, evD.ev[(size_t)k], 0);
+        // split form: a band's product (about 1.6 ms for 2048 x 8192 x 8192) is shorter than
+        // the download of an encoded band, so the downloads bound the call once the first
+        // band is out; each product waits for the previous band's encode kernels, which then
+        // run alone instead of sharing the SMs with the product (the native form's products
+        // are the longer part and keep overlapping the encodes)
+        if (split && k > 0) cudaStreamWaitEvent(st, evK.ev[(size_t)k - 1], 0);
         const int64_t r0 = k * gc.chunk[0], mk = row_geom(fa.g, k).shape[0];
         uint8_t *a_k = dA.as<uint8_t>() + r0 * lda * isz, *c_k = dC.as<uint8_t>() + r0 * ldc * isz;
         if (split) {
@@ -1498,9 +1507,14 @@ INA_API(ina_rc_t) iarray_b200_opt_gemm_cframes(iarray_context_t *ctx, const uint
         w.exact_lz4 = ctx->encoder == IARRAY_B200_ENCODER_LIBLZ4;
         err = iab::encode_launch(gk, c_k, ldc, cc->shuffle, cc->splitmode, &cbuf[(size_t)k], &w, se);
         if (err) break;
+        // the chunk table goes to the host on its own stream: a device-to-host copy queued on
+        // the encode stream would wait behind the previous band's download and hold up the
+        // next band's encode
+        cudaEventRecord(evK.ev[(size_t)k], se);
+        cudaStreamWaitEvent(ctx->tabs, evK.ev[(size_t)k], 0);
         cudaMemcpyAsync(htab + k * gc.cgrid[1], w.ec.p, (size_t)gk.nchunks * sizeof(iab::EncChunk),
-                        cudaMemcpyDeviceToHost, se);
-        cudaEventRecord(evE.ev[(size_t)k], se);
+                        cudaMemcpyDeviceToHost, ctx->tabs);
+        cudaEventRecord(evE.ev[(size_t)k], ctx->tabs);
         queued = k + 1;
         if (k > 0) drain(k - 1);
     }
@@ -1512,11 +1526,11 @@ INA_API(ina_rc_t) iarray_b200_opt_gemm_cframes(iarray_context_t *ctx, const uint
     tm.mark(4);
     const cudaError_t ce1 = cudaStreamSynchronize(st), ce2 = cudaStreamSynchronize(ctx->down),
                       ce3 = cudaStreamSynchronize(ctx->up), ce4 = cudaStreamSynchronize(sd),
-                      ce5 = cudaStreamSynchronize(se);
+                      ce5 = cudaStreamSynchronize(se), ce6 = cudaStreamSynchronize(ctx->tabs);
     tm.finish();
     if (err == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
     if (err || ce1 != cudaSuccess || ce2 != cudaSuccess || ce3 != cudaSuccess || ce4 != cudaSuccess ||
-        ce5 != cudaSuccess)
+        ce5 != cudaSuccess || ce6 != cudaSuccess)
         return rc_err(IARRAY_ERR_GPU_FAILED);
     // decode status words, then the split product's error flags
     std::vector<int> hs((size_t)(rowsA + rowsB) * 16);
