@@ -158,13 +158,15 @@ constexpr int DCAP = 4096;                 // output bytes resolved in shared me
 constexpr uint16_t STOP = 0xFFFF, ENDS = 0xFFFE;
 constexpr uint32_t RES = 0x80000000u;      // resolved output byte (value in the low 8 bits)
 struct Smem {
-    uint32_t st[DCAP];                     // per output byte: RES | value, or the source's index
+    union {
+        uint32_t st[DCAP];                 // per output byte: RES | value, or the source's index
+        uint16_t J[2][DW];                 // next-token tables (dead once the window's chain is known)
+    };
     int32_t ostart[MAXS + 1];              // output offset of each sequence in the window
     int32_t llen[MAXS];
     int32_t mlen[MAXS];
     uint16_t lpos[MAXS];
     uint16_t off[MAXS];
-    uint16_t J[2][DW];
     uint16_t path[PATH];
     uint8_t win[DW + 16];
     uint8_t hist[HB];                      // the last HB output bytes (ring, by absolute position)
@@ -205,7 +207,7 @@ __device__ __forceinline__ uint16_t dcta_next(const uint8_t *win, int q, int n, 
     return (uint16_t)r;                   // r <= n; r == n: the next token starts the next window
 }
 
-__global__ void __launch_bounds__(dcta::THREADS, 5) k_lz4_decode_cta(const Lz4Job *__restrict__ jobs,
+__global__ void __launch_bounds__(dcta::THREADS, 6) k_lz4_decode_cta(const Lz4Job *__restrict__ jobs,
                                                                   const int *__restrict__ njobs_p, int64_t jcap,
                                                                   unsigned *next_job)
 {
@@ -2047,7 +2049,7 @@ int decode_lz4(DecodeQueue *q, cudaStream_t st)
         attr = true;
     }
     int *qc = q->counters.as<int>();
-    IAB_TIMED("k_lz4_decode_cta", st, k_lz4_decode_cta<<<sm_count() * 5, dcta::THREADS, smem, st>>>(
+    IAB_TIMED("k_lz4_decode_cta", st, k_lz4_decode_cta<<<sm_count() * 6, dcta::THREADS, smem, st>>>(
         q->jobs.as<Lz4Job>(), qc, q->cap, reinterpret_cast<unsigned *>(qc + 1)));
     return 0;
 }
@@ -2291,7 +2293,7 @@ int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes,
                                                                                       8 * NA_MAX_BLOCKS, err, img));
     }
     {
-        IAB_TIMED("k_lz4_decode_cta", st, k_lz4_decode_cta<<<sms * 5, dcta::THREADS, (int)sizeof(dcta::Smem), st>>>(
+        IAB_TIMED("k_lz4_decode_cta", st, k_lz4_decode_cta<<<sms * 6, dcta::THREADS, (int)sizeof(dcta::Smem), st>>>(
             jobs, njobs, 8 * NA_MAX_BLOCKS, reinterpret_cast<unsigned *>(counters + 2)));
     }
     {
