@@ -8,19 +8,22 @@
 // plus Caterva's padded blocked layout (iarray_from_buffer / iarray_to_buffer,
 // src/iarray_constructor.c:218-305).
 //
-// Decode = parse (one thread per block walks its stream headers) -> LZ4 (one warp per
-// LZ4 stream, sequences located 32 at a time by pointer doubling) -> unshuffle/scatter (one CTA per
-// block tile, byte planes staged in shared memory, items written to the dense
-// row-major array).  Raw and run streams are never copied before the scatter.
+// Decode = parse (one thread per block walks its stream headers and queues its LZ4 streams)
+// -> LZ4 (one CTA per LZ4 stream from a job queue that may span several containers; each
+// window of the stream decoded in parallel: token chain by pointer doubling, output resolved
+// in shared memory by pointer jumping) -> unshuffle/scatter (slices of interior blocks staged
+// in shared memory by bulk asynchronous copies, items written to the dense row-major array;
+// a general path for the other blocks).  Raw and run streams are never copied before the
+// scatter.
 //
-// Encode = gather/shuffle (dense -> byte-plane image) -> LZ4 (one warp per stream,
-// 16 KiB hash table in shared memory, 32 match probes evaluated per step) -> layout
-// (per chunk: stream kinds, offsets, memcpy fallback; exclusive scan of chunk sizes)
-// -> emit (copy payloads into the final contiguous chunk buffer).
-// The LZ4 encoder reproduces liblz4 1.9.4 LZ4_compress_fast(acceleration 1) output
-// byte for byte (the codec c-blosc2 calls for BLOSC_LZ4); stream-kind selection
-// (zero/run, raw when LZ4 does not fit, memcpyed chunk when the output would exceed
-// nbytes + 32) follows c-blosc2's blosc_c rules.
+// Encode = gather/shuffle (dense -> byte-plane image) -> LZ4 -> layout (per chunk: stream
+// kinds, offsets, memcpy fallback; exclusive scan of chunk sizes) -> emit (copy payloads
+// into the final contiguous chunk buffer).  Two LZ4 encoders: one warp per stream
+// reproducing liblz4 1.9.4 LZ4_compress_fast(acceleration 1) output byte for byte (the codec
+// c-blosc2 calls for BLOSC_LZ4: 16 KiB hash table in shared memory, 32 match probes
+// evaluated per step), and a parallel-parse encoder (one CTA per stream, valid LZ4 with
+// different bytes).  Stream-kind selection (zero/run, raw when LZ4 does not fit, memcpyed
+// chunk when the output would exceed nbytes + 32) follows c-blosc2's blosc_c rules.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
