@@ -1570,6 +1570,7 @@ struct iarray_b200_batch_s {
     std::vector<iab::DecodeWork> decA, decB;
     iab::DecodeQueue dq;              // the LZ4 streams of every operand
     std::vector<iab::EncodeWork> enc;
+    DevBuf eimg, eslots, ees, ecursor;  // outputs' byte-plane images, LZ4 slots, stream results, cursor
     std::vector<iab::OzakiWork> oz;
     DevBuf status;                    // 16 ints per decode: [2i] operand A, [2i + 1] operand B
     DevBuf chunks;                    // chunk tables of all outputs
@@ -1688,17 +1689,69 @@ int batch_enqueue(iarray_b200_batch_t *bt, int parts)
         iab::gemm_f64_grouped(bt->cfg, bt->probs.as<iab::GemmProblem>(), (int)bt->hprobs.size(), bt->total_tiles,
                               bt->ctas, st);
     }
-    if (parts & 4) batch_fork(bt);
-    for (int64_t i = 0; i < bt->n && (parts & 4); i++) {
+    if (!(parts & 4)) return 0;
+    const bool exact = bt->ctx->encoder == IARRAY_B200_ENCODER_LIBLZ4;
+    // When every output has streams of one size, their byte-plane images, LZ4 slots and
+    // stream results lie back to back and one LZ4 launch encodes the streams of all of
+    // them (gathers and chunk layouts stay per output, on the branches).
+    int nsb = 0, neb = 0;
+    bool shared = true;
+    int64_t img_total = 0, es_total = 0;
+    for (int64_t i = 0; i < bt->n; i++) {
+        const Geom &g = bt->cgeom[(size_t)i];
+        if (!g.nchunks) continue;
+        const int ns = iab::encode_nstreams(g, true, IARRAY_AUTO_SPLIT), ne = (int)(g.blocksize / ns);
+        if (!nsb) { nsb = ns; neb = ne; }
+        shared = shared && ns == nsb && ne == neb;
+        img_total += g.nchunks * g.nblocks * g.blocksize;
+        es_total += g.nchunks * g.nblocks * ns;
+    }
+    if (shared && img_total > 0) {
+        const int dev = bt->ctx->device;
+        if (!bt->eimg.allocate((size_t)img_total, dev) || !bt->eslots.allocate((size_t)img_total, dev) ||
+            !bt->ees.allocate(sizeof(iab::EncStream) * (size_t)es_total, dev) || !bt->ecursor.allocate(64, dev))
+            return -100;
+        cudaMemsetAsync(bt->ecursor.p, 0, 64, st);
+        int r = 0;
+        for (int pass = 0; pass < 2 && !r; pass++) {
+            batch_fork(bt);
+            int64_t io = 0, so = 0;
+            for (int64_t i = 0; i < bt->n && !r; i++) {
+                const Geom &g = bt->cgeom[(size_t)i];
+                if (!g.nchunks) continue;
+                iab::EncodeWork &w = bt->enc[(size_t)i];
+                cudaStream_t bs = bt->br[(size_t)i % nbr];
+                if (!pass) {
+                    w.ext_chunks = bt->chunks.as<iab::EncChunk>() + bt->chunk_base[(size_t)i];
+                    w.exact_lz4 = exact;
+                    w.ext_img = bt->eimg.as<uint8_t>() + io;
+                    w.ext_slots = bt->eslots.as<uint8_t>() + io;
+                    w.ext_es = bt->ees.as<iab::EncStream>() + so;
+                    r = iab::encode_gather(g, bt->dC[(size_t)i].p, bt->ldc[(size_t)i], true, IARRAY_AUTO_SPLIT, &w, bs);
+                } else {
+                    r = iab::encode_emit(g, true, IARRAY_AUTO_SPLIT, &bt->cbuf[(size_t)i], &w, bs);
+                }
+                io += g.nchunks * g.nblocks * g.blocksize;
+                so += g.nchunks * g.nblocks * nsb;
+            }
+            batch_join(bt);
+            if (!pass && !r)
+                iab::encode_streams(bt->eimg.as<uint8_t>(), es_total, neb, bt->eslots.as<uint8_t>(),
+                                    bt->ees.as<iab::EncStream>(), bt->ecursor.as<unsigned long long>(), exact, st);
+        }
+        return r;
+    }
+    batch_fork(bt);
+    for (int64_t i = 0; i < bt->n; i++) {
         const Geom &g = bt->cgeom[(size_t)i];
         if (!g.nchunks) continue;
         bt->enc[(size_t)i].ext_chunks = bt->chunks.as<iab::EncChunk>() + bt->chunk_base[(size_t)i];
-        bt->enc[(size_t)i].exact_lz4 = bt->ctx->encoder == IARRAY_B200_ENCODER_LIBLZ4;
+        bt->enc[(size_t)i].exact_lz4 = exact;
         const int r = iab::encode_launch(g, bt->dC[(size_t)i].p, bt->ldc[(size_t)i], true, IARRAY_AUTO_SPLIT,
                                          &bt->cbuf[(size_t)i], &bt->enc[(size_t)i], bt->br[(size_t)i % nbr]);
         if (r) { batch_join(bt); return r; }
     }
-    if (parts & 4) batch_join(bt);
+    batch_join(bt);
     return 0;
 }
 

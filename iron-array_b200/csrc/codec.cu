@@ -2099,53 +2099,63 @@ int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, 
     return r;
 }
 
-int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, DevBuf *d_out, EncodeWork *w,
-                  cudaStream_t st)
+// c-blosc2's split rule for LZ4 (always / never / automatic: LZ4 + shuffle, typesize <= 16
+// and at least 32 items per block); a split block has one stream per item byte.
+static bool encode_split(const Geom &g, bool shuffle, int splitmode)
+{
+    if (splitmode == 1) return true;
+    if (splitmode == 2) return false;
+    return shuffle && g.itemsize <= 16 && (g.blocksize / g.itemsize) >= 32;
+}
+
+int encode_nstreams(const Geom &g, bool shuffle, int splitmode)
+{
+    return encode_split(g, shuffle, splitmode) ? g.itemsize : 1;
+}
+
+int encode_gather(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, EncodeWork *w, cudaStream_t st)
 {
     int dev = 0;
     cudaGetDevice(&dev);
     const int ts = g.itemsize;
     const int64_t nbl = g.nchunks * g.nblocks;
     const int64_t img_bytes = nbl * g.blocksize;
-    // c-blosc2's split rule for LZ4 (always / never / automatic: LZ4 + shuffle,
-    // typesize <= 16 and at least 32 items per block)
-    bool split;
-    if (splitmode == 1) split = true;
-    else if (splitmode == 2) split = false;
-    else split = shuffle && ts <= 16 && (g.blocksize / ts) >= 32;
-    const int nstreams = split ? ts : 1;
-    const int neblock = (int)(g.blocksize / nstreams);
-    DevBuf &img = w->img, &slots = w->slots, &es = w->es, &tot = w->tot;
-    if (!img.allocate(img_bytes, dev) || !slots.allocate(img_bytes, dev) ||
-        !es.allocate(sizeof(EncStream) * nbl * nstreams, dev) ||
-        (!w->ext_chunks && !w->ec.allocate(sizeof(EncChunk) * g.nchunks, dev)) || !tot.allocate(64, dev) ||
-        !d_out->allocate((size_t)(g.nchunks * (g.chunk_nbytes + 32)), dev))
+    const int nstreams = encode_nstreams(g, shuffle, splitmode);
+    const bool ext = w->ext_img != nullptr;
+    if ((!ext && (!w->img.allocate(img_bytes, dev) || !w->slots.allocate(img_bytes, dev) ||
+                  !w->es.allocate(sizeof(EncStream) * nbl * nstreams, dev))) ||
+        (!w->ext_chunks && !w->ec.allocate(sizeof(EncChunk) * g.nchunks, dev)) || !w->tot.allocate(64, dev))
         return -100;
-    EncChunk *ec = w->ext_chunks ? w->ext_chunks : w->ec.as<EncChunk>();
     w->nchunks = g.nchunks;
-    cudaMemsetAsync(tot.p, 0, 64, st);
+    uint8_t *img = ext ? w->ext_img : w->img.as<uint8_t>();
+    cudaMemsetAsync(w->tot.p, 0, 64, st);
     const int sms = sm_count();
-    {
-        const int64_t tpb = (g.blockn + TILE - 1) / TILE;
-        const int64_t blocks = std::min<int64_t>(nbl * tpb, (int64_t)sms * 8);
-        const bool fast = shuffle && (ts == 4 || ts == 8);
-        if (fast) {
-            const int64_t fb = std::min<int64_t>(nbl, (int64_t)sms * 8);
-            if (ts == 8)
-                IAB_TIMED("k_gather_fast", st, k_gather_fast<8><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
-                    g, (const uint8_t *)in, ld, img.as<uint8_t>()));
-            else
-                IAB_TIMED("k_gather_fast", st, k_gather_fast<4><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
-                    g, (const uint8_t *)in, ld, img.as<uint8_t>()));
-        }
-        // the general gather covers the blocks the fast one leaves (padded or partial ones)
-        const bool all_fast = fast && g.chunk[0] % g.block[0] == 0 && g.chunk[1] % g.block[1] == 0 &&
-                              g.shape[0] % g.chunk[0] == 0 && g.shape[1] % g.chunk[1] == 0 && !(g.block[1] & 3);
-        if (!all_fast)
-            IAB_TIMED("k_gather", st, k_gather<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
-                g, fast, (const uint8_t *)in, ld, shuffle, img.as<uint8_t>()));
+    const int64_t tpb = (g.blockn + TILE - 1) / TILE;
+    const int64_t blocks = std::min<int64_t>(nbl * tpb, (int64_t)sms * 8);
+    const bool fast = shuffle && (ts == 4 || ts == 8);
+    if (fast) {
+        const int64_t fb = std::min<int64_t>(nbl, (int64_t)sms * 8);
+        if (ts == 8)
+            IAB_TIMED("k_gather_fast", st, k_gather_fast<8><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
+                g, (const uint8_t *)in, ld, img));
+        else
+            IAB_TIMED("k_gather_fast", st, k_gather_fast<4><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
+                g, (const uint8_t *)in, ld, img));
     }
-    if (w->exact_lz4) {
+    // the general gather covers the blocks the fast one leaves (padded or partial ones)
+    const bool all_fast = fast && g.chunk[0] % g.block[0] == 0 && g.chunk[1] % g.block[1] == 0 &&
+                          g.shape[0] % g.chunk[0] == 0 && g.shape[1] % g.chunk[1] == 0 && !(g.block[1] & 3);
+    if (!all_fast)
+        IAB_TIMED("k_gather", st, k_gather<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
+            g, fast, (const uint8_t *)in, ld, shuffle, img));
+    return 0;
+}
+
+void encode_streams(const uint8_t *img, int64_t ns, int neblock, uint8_t *slots, EncStream *es,
+                    unsigned long long *cursor, bool exact_lz4, cudaStream_t st)
+{
+    const int sms = sm_count();
+    if (exact_lz4) {
         static bool attr = false;
         // per warp: 16 KiB hash table + the source window; 1 warp per CTA, 10 CTAs per SM
         const int wpb = 1, smem = wpb * (4096 * 4 + ERING + 16);
@@ -2153,11 +2163,9 @@ int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int s
             cudaFuncSetAttribute(k_lz4_encode, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             attr = true;
         }
-        const int64_t ns = nbl * nstreams;
         const int64_t blocks = std::min<int64_t>((ns + wpb - 1) / wpb, (int64_t)sms * 10);
         IAB_TIMED("k_lz4_encode", st, k_lz4_encode<<<(unsigned)std::max<int64_t>(blocks, 1), wpb * 32, smem, st>>>(
-            img.as<uint8_t>(), ns, neblock, slots.as<uint8_t>(), es.as<EncStream>(),
-            reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1)));
+            img, ns, neblock, slots, es, cursor));
     } else {
         static bool attr = false;
         const int smem = (int)sizeof(ParSmem);                 // one stream per CTA of PT threads, 8 CTAs per SM
@@ -2165,21 +2173,48 @@ int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int s
             cudaFuncSetAttribute(k_lz4_encode_par, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
             attr = true;
         }
-        const int64_t ns = nbl * nstreams;
         const int64_t blocks = std::min<int64_t>(ns, (int64_t)sms * 8);
         IAB_TIMED("k_lz4_encode_par", st, k_lz4_encode_par<<<(unsigned)std::max<int64_t>(blocks, 1), PT, smem, st>>>(
-            img.as<uint8_t>(), ns, neblock, slots.as<uint8_t>(), es.as<EncStream>(),
-            reinterpret_cast<unsigned long long *>(tot.as<int64_t>() + 1)));
+            img, ns, neblock, slots, es, cursor));
     }
-    IAB_TIMED("k_layout", st, k_layout<<<(unsigned)std::max<int64_t>(g.nchunks, 1), LAYOUT_T, 0, st>>>(g, nstreams, neblock, es.as<EncStream>(), ec));
-    IAB_TIMED("k_chunk_offsets", st, k_chunk_offsets<<<1, 1024, 0, st>>>(g.nchunks, ec, tot.as<int64_t>()));
-    {
-        const int64_t blocks = std::min<int64_t>(nbl, (int64_t)sms * 8);
-        IAB_TIMED("k_emit", st, k_emit<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(g, nstreams, neblock, shuffle, split ? 1 : 0,
-                                                                      img.as<uint8_t>(), slots.as<uint8_t>(), img_bytes,
-                                                                      es.as<EncStream>(), ec, d_out->as<uint8_t>()));
-    }
+}
+
+int encode_emit(const Geom &g, bool shuffle, int splitmode, DevBuf *d_out, EncodeWork *w, cudaStream_t st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int64_t nbl = g.nchunks * g.nblocks;
+    const int64_t img_bytes = nbl * g.blocksize;
+    const int nstreams = encode_nstreams(g, shuffle, splitmode);
+    const int neblock = (int)(g.blocksize / nstreams);
+    if (!d_out->allocate((size_t)(g.nchunks * (g.chunk_nbytes + 32)), dev)) return -100;
+    const bool ext = w->ext_img != nullptr;
+    const uint8_t *img = ext ? w->ext_img : w->img.as<uint8_t>();
+    const uint8_t *slots = ext ? w->ext_slots : w->slots.as<uint8_t>();
+    EncStream *es = ext ? w->ext_es : w->es.as<EncStream>();
+    EncChunk *ec = w->ext_chunks ? w->ext_chunks : w->ec.as<EncChunk>();
+    IAB_TIMED("k_layout", st, k_layout<<<(unsigned)std::max<int64_t>(g.nchunks, 1), LAYOUT_T, 0, st>>>(g, nstreams, neblock, es, ec));
+    IAB_TIMED("k_chunk_offsets", st, k_chunk_offsets<<<1, 1024, 0, st>>>(g.nchunks, ec, w->tot.as<int64_t>()));
+    const int64_t blocks = std::min<int64_t>(nbl, (int64_t)sm_count() * 8);
+    IAB_TIMED("k_emit", st, k_emit<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
+        g, nstreams, neblock, shuffle, encode_split(g, shuffle, splitmode) ? 1 : 0, img, slots, img_bytes, es, ec,
+        d_out->as<uint8_t>()));
     return 0;
+}
+
+int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, DevBuf *d_out, EncodeWork *w,
+                  cudaStream_t st)
+{
+    w->ext_img = nullptr;
+    w->ext_slots = nullptr;
+    w->ext_es = nullptr;
+    const int r = encode_gather(g, in, ld, shuffle, splitmode, w, st);
+    if (r) return r;
+    const int nstreams = encode_nstreams(g, shuffle, splitmode);
+    encode_streams(w->img.as<uint8_t>(), g.nchunks * g.nblocks * nstreams, (int)(g.blocksize / nstreams),
+                   w->slots.as<uint8_t>(), w->es.as<EncStream>(),
+                   reinterpret_cast<unsigned long long *>(w->tot.as<int64_t>() + 1), w->exact_lz4, st);
+    return encode_emit(g, shuffle, splitmode, d_out, w, st);
 }
 
 int encode_finish(EncodeWork *w, std::vector<int64_t> *h_off, std::vector<int32_t> *h_len, cudaStream_t st)

@@ -208,10 +208,25 @@ struct EncodeWork {
     DevBuf img, slots, es, ec, tot;
     bool exact_lz4 = true;            // liblz4-identical streams (see encode_container)
     EncChunk *ext_chunks = nullptr;   // optional caller-owned chunk table (device) instead of `ec`
+    // optional caller-owned byte-plane image, LZ4 output slots and stream results (device)
+    // instead of img / slots / es: slices of buffers shared by several containers
+    uint8_t *ext_img = nullptr, *ext_slots = nullptr;
+    EncStream *ext_es = nullptr;
     int64_t nchunks = 0;
 };
 int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, DevBuf *d_out,
                   EncodeWork *w, cudaStream_t st);
+
+// encode_launch in stages, so that several containers can share one LZ4 launch:
+// encode_gather (dense -> byte-plane image), encode_streams (LZ4 over ns streams of neblock
+// bytes each; the streams of several containers when their images, slots and results lie
+// back to back), encode_emit (chunk layout, offsets, payloads into *d_out).  The stream
+// cursor `cursor` must be zero before encode_streams.
+int encode_nstreams(const Geom &g, bool shuffle, int splitmode);
+int encode_gather(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, EncodeWork *w, cudaStream_t st);
+void encode_streams(const uint8_t *img, int64_t ns, int neblock, uint8_t *slots, EncStream *es,
+                    unsigned long long *cursor, bool exact_lz4, cudaStream_t st);
+int encode_emit(const Geom &g, bool shuffle, int splitmode, DevBuf *d_out, EncodeWork *w, cudaStream_t st);
 int encode_finish(EncodeWork *w, std::vector<int64_t> *h_off, std::vector<int32_t> *h_len, cudaStream_t st);
 
 // Dense products (row-major, leading dimensions in items).
