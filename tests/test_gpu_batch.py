@@ -71,6 +71,35 @@ def test_batch_uneven_sizes_with_empty_and_tiny_problems(ia):
     batch.free()
 
 
+@pytest.mark.parametrize("encoder", ["liblz4", "parallel"])
+@pytest.mark.parametrize("mixed", [False, True])
+def test_batch_encoders_and_mixed_partitions(ia, encoder, mixed):
+    """One LZ4 launch encodes the streams of every output when they share one stream size
+    (mixed=False); outputs of different block shapes are encoded one by one (mixed=True).
+    Either way each output is byte-identical to the single-product path with the same
+    encoder."""
+    ctx = ia.Context(encoder=ia.ENCODER_PARALLEL if encoder == "parallel" else ia.ENCODER_LIBLZ4)
+    rng = np.random.default_rng(11)
+    As, Bs, cs, bs = [], [], [], []
+    for i in range(6):
+        # output chunks (48, 80) fit every output, as iarray_linalg_matmul requires
+        m, n = (int(x) for x in rng.integers(80, 200, 2))
+        k = int(rng.integers(1, 200))
+        As.append(ia.Container.from_numpy(ctx, rng.uniform(-1, 1, (m, k)) * 50.0, (64, 64), (16, 16)))
+        Bs.append(ia.Container.from_numpy(ctx, rng.uniform(-1, 1, (k, n)), (64, 64), (16, 16)))
+        cs.append((48, 80))
+        bs.append((16, 40) if mixed and i % 2 else (16, 16))
+    batch = ia.Batch(ctx, As, Bs, cs, bs)
+    for rep in range(2):
+        outs = batch.run()
+        for i, c in enumerate(outs):
+            ref = ia.matmul(ctx, As[i], Bs[i], cs[i], bs[i])
+            assert c.chunks() == ref.chunks(), (rep, i)
+            c.free()
+            ref.free()
+    batch.free()
+
+
 def test_batch_rejects_bad_operands(ia):
     ctx = ia.Context()
     a = ia.Container.from_numpy(ctx, np.ones((4, 5)), (4, 5), (2, 5))
