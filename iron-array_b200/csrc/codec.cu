@@ -546,19 +546,6 @@ __device__ __forceinline__ void transpose4x4(uint32_t a, uint32_t b, uint32_t c,
     o3 = __byte_perm(ab_hi, cd_hi, 0x7632);
 }
 
-// 4 bytes at any address p < lim - 3: two aligned word loads and a funnel shift when the
-// second word still lies below lim, byte loads otherwise.
-__device__ __forceinline__ uint32_t ld4_any(const uint8_t *p, const uint8_t *lim)
-{
-    const uintptr_t a = reinterpret_cast<uintptr_t>(p) & ~uintptr_t(3);
-    if (a + 8 <= reinterpret_cast<uintptr_t>(lim)) {
-        const uint32_t *w = reinterpret_cast<const uint32_t *>(a);
-        return __funnelshift_r(__ldg(w), __ldg(w + 1), (uint32_t)(reinterpret_cast<uintptr_t>(p) & 3) * 8);
-    }
-    return (uint32_t)__ldg(p) | ((uint32_t)__ldg(p + 1) << 8) | ((uint32_t)__ldg(p + 2) << 16) |
-           ((uint32_t)__ldg(p + 3) << 24);
-}
-
 // D2 fast path: interior, shuffled, split blocks, in slices of SC_ITEMS items (one CTA per
 // slice at a time).  One thread stages the slice's bytes of every byte plane (read in place
 // from raw streams or the LZ4 scratch) into shared memory with bulk asynchronous copies
@@ -871,13 +858,6 @@ __device__ __forceinline__ uint32_t ld4u(const uint8_t *p)
     const uintptr_t a = reinterpret_cast<uintptr_t>(p);
     const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~uintptr_t(3));
     return __funnelshift_r(__ldg(w), __ldg(w + 1), (uint32_t)(a & 3) * 8);
-}
-
-__device__ __forceinline__ uint32_t lz_hash(const uint8_t *p, bool small)
-{
-    if (small) return (ld4u(p) * 2654435761u) >> (32 - 13);
-    const uint64_t v = (uint64_t)ld4u(p) | ((uint64_t)__ldg(p + 4) << 32);
-    return (uint32_t)(((v << 24) * 889523592379ull) >> (64 - 12));
 }
 
 // Position offset of the t-th probe of a search, relative to its start: the step is
