@@ -291,13 +291,6 @@ constexpr double kTwo52 = 4503599627370496.0;
 // 2^s for -1022 <= s <= 1023.
 __device__ __forceinline__ double pow2i(int s) { return __hiloint2double((1023 + s) << 20, 0); }
 
-// rint(y) for |y| < 2^52 (ties to even, like rint).
-__device__ __forceinline__ double rint52(double y)
-{
-    const double c = copysign(kTwo52, y);
-    return (y + c) - c;
-}
-
 // x = rint(a * 2^s), the scaled entry of an operand row or column (|x| < 2^52), and the low
 // 32 bits of x as an integer: y + copysign(2^52, y) holds |x| in its mantissa field.
 __device__ __forceinline__ double scaled_int(double a, int s, bool pow2_ok, double f, uint32_t &xlo)
