@@ -415,7 +415,7 @@ INA_API(ina_rc_t) iarray_b200_kernel_profile(char *buf, int64_t cap, int64_t *le
  * IARRAY_B200_NOALLOC_MAX_BYTES and nchunks x blocks per chunk <=
  * IARRAY_B200_NOALLOC_MAX_BLOCKS; larger geometries return IARRAY_ERR_NOALLOC_TOO_LARGE
  * (decode a large container chunk by chunk, passing chunkshape as the shape).
- * The fixed array (about 9.4 MiB) is held by every GPU that loads the library's kernels
+ * The fixed array (about 9.7 MiB) is held by every GPU that loads the library's kernels
  * until the process exits.  The first call on each device looks up the array's device
  * address and sets a kernel attribute; make that first call before any stream capture.
  * All calls share the array and it keeps the last call's contents: calls whose work
