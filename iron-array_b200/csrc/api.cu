@@ -1047,7 +1047,7 @@ static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_
     if (vec) cudaMemsetAsync(dB.p, 0, (size_t)(pad_ld(K) * isz), ctx->stream);
     ina_rc_t rc;
     if (!a->transposed && !b->transposed) {
-        // both operands at once: A on the context stream, B on the second stream
+        // both operands at once: one LZ4 launch over the streams of A and B
         rc = decode_pair(ctx, a, dA.p, lda, b, dB.p, vec ? K : ldb);
         if (INA_FAILED(rc)) return rc;
         tm.mark(1);
