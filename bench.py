@@ -21,6 +21,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -32,6 +33,13 @@ M = N = K = 8192
 CHUNK, BLOCK = (2048, 2048), (256, 256)
 FLOP = 2.0 * M * N * K
 METRIC = "GEMM TFLOP/s split-precision vs native FP64 at stated error; decode GB/s"
+
+
+def bench_config(world):
+    """The workload's config, the same dict in both arms."""
+    return {"workload": "precision_f64 opt_gemm 8192^3, chunk 2048^2, block 256^2, LZ4 clevel5 + SHUFFLE",
+            "M": M, "N": N, "K": K, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (compressed A + B about 1 GB), no flush needed"}
 
 
 def make_inputs():
@@ -53,8 +61,8 @@ class Clocks:
 
     def __init__(self, index):
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
-                                 f".clocks_{os.getpid()}.csv")
+        fd, self.path = tempfile.mkstemp(prefix="iarray_b200_clocks_", suffix=".csv")
+        os.close(fd)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -140,24 +148,27 @@ def run_reference(args):
     gc = O.Geom((M, N), CHUNK, BLOCK, 8)
     del A, B
     cores = os.cpu_count() or 1
-    times = []
-    for s in range(args.warmup + args.steps):
-        t = time.perf_counter()
+    # warm-up: one output chunk per step (page-ins, thread start-up, BLAS kernels); each
+    # timed step is the whole product, every one of the 16 output chunks
+    for s in range(args.warmup):
         O.cpu_opt_gemm_chunk(ga, ach, gb, bch, gc, s % gc.nchunks, cores)
-        if s >= args.warmup:
-            times.append(time.perf_counter() - t)
-    chunk_flop = 2.0 * CHUNK[0] * CHUNK[1] * K
-    sec_full = float(np.mean(times)) * gc.nchunks
-    v = FLOP / sec_full / 1e12
-    sample = (f"one 2048x2048 output chunk of the 8192^3 opt_gemm per step (1/{gc.nchunks} of the work, "
-              f"{chunk_flop / 1e9:.1f} GFLOP), block-pair loop with per-pair LZ4 block decode, "
-              f"single-threaded OpenBLAS dgemm per worker, LZ4 re-encode; scaled to the full product")
+    times = []
+    for s in range(args.steps):
+        t = time.perf_counter()
+        O.cpu_opt_gemm(ga, ach, gb, bch, gc, cores)
+        times.append(time.perf_counter() - t)
+    sec = float(np.mean(times))
+    v = FLOP / sec / 1e12
+    sample = (f"the whole 8192^3 opt_gemm per timed step ({gc.nchunks} output chunks, {FLOP / 1e12:.2f} TFLOP): "
+              f"the reference's block-pair loop with per-pair LZ4 block decode (liblz4), single-threaded OpenBLAS "
+              f"dgemm per worker thread ({cores} workers over each chunk's blocks), each block LZ4-compressed by its "
+              f"worker; warm-up steps compute one output chunk each")
     line = {"metric": METRIC, "value": v, "unit": "TFLOP/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_full * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "precision_f64 8192^3, chunk 2048^2, block 256^2, LZ4+SHUFFLE",
-                       "M": M, "N": N, "K": K},
-            "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": cores, "kind": "port", "sample": sample},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (numpy default_rng(3))",
+            "config": bench_config(world),
+            "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": cores, "kind": "port", "sample": sample,
+                             "samples": len(times), "step_s": [round(x, 3) for x in times]},
             "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     barrier(pg)
@@ -203,7 +214,10 @@ def roofline(kprof, pk, dgemm_tflops, c_cbytes, a_cb, b_cb):
         traffic = json.load(open(tf)).get(name)
     return {"bound": bound, "kernel": name, "launches": cnt, "avg_ms": tot / cnt, "achieved": achieved,
             "peak": peak, "peak_source": src, "unit": unit, "frac": achieved / peak if peak else None,
-            "traffic": traffic}
+            "traffic": traffic,
+            "traffic_source": "profiles/ncu_traffic.json: dram bytes read + written of one launch of this "
+                              "kernel at this workload, from a committed counter capture (not re-measured "
+                              "by this run)" if traffic is not None else None}
 
 
 # ============================================================================ secondary workloads
@@ -313,8 +327,10 @@ def secondary_f32(ia, ctx, stream, args):
     del A, B
     flop = 2.0 * M * N * K
     res = {"workload": "precision_f32 16384x4096 @ 4096x16384, chunk 4096^2, block 512^2"}
-    for name, form in (("native", ia.FORM_NATIVE), ("split", ia.FORM_SPLIT)):
+    for name, form, prods in (("native", ia.FORM_NATIVE, 0), ("split", ia.FORM_SPLIT, 6),
+                              ("split_3xbf16", ia.FORM_SPLIT, 3)):
         ctx.set_form(form)
+        ctx.set_split_products_f32(prods)
         out = []
 
         def step():
@@ -328,7 +344,8 @@ def secondary_f32(ia, ctx, stream, args):
         ctx.synchronize()
         ia.profile_kernels(False)
         prof = ia.kernel_profile()
-        prod = sum(v[1] for k, v in prof.items() if k in ("k_gemm_f32", "k_bf16x3_gemm", "k_split_rows", "k_split_cols"))
+        prod = sum(v[1] for k, v in prof.items() if k in ("k_gemm_f32", "k_bf16s_gemm", "k_split_rows", "k_split_cols"))
+        tc_ms = prof.get("k_bf16s_gemm", (0, 0.0))[1]
         c = out[-1].to_numpy()[rows].astype(np.float64)
         err = float(np.linalg.norm(c - exact) / np.linalg.norm(exact))
         for x in out:
@@ -336,6 +353,12 @@ def secondary_f32(ia, ctx, stream, args):
         res[name] = {"ms_per_step": ms, "tflops": flop / (ms * 1e-3) / 1e12, "product_ms": prod,
                      "product_tflops": flop / (prod * 1e-3) / 1e12 if prod else None,
                      "normwise_err_vs_f64": err, "kernel_ms": {k: v[1] for k, v in sorted(prof.items())}}
+        if prods and tc_ms:
+            # the tensor-core kernel's BF16 work: `prods` products of 2 M N K each
+            bf = prods * flop / (tc_ms * 1e-3) / 1e12
+            res[name]["bf16_products"] = prods
+            res[name]["tensor_tflops"] = bf
+            res[name]["tensor_frac_of_measured_bf16"] = bf / peaks()["bf16_tflops"]
     ctx.set_form(ia.FORM_NATIVE)
     Ac.free()
     Bc.free()
@@ -546,25 +569,31 @@ def run_ours(args):
         gb, bch = O.Geom((K, N), CHUNK, BLOCK, 8), Bc.chunks()
         gc = O.Geom((M, N), CHUNK, BLOCK, 8)
         cores = os.cpu_count() or 1
+        O.cpu_opt_gemm_chunk(ga, ach, gb, bch, gc, 0, cores)      # warm-up
         ts = []
-        for s in range(2):
+        for s in range(args.cpu_samples):
             t = time.perf_counter()
-            O.cpu_opt_gemm_chunk(ga, ach, gb, bch, gc, s, cores)
+            O.cpu_opt_gemm(ga, ach, gb, bch, gc, cores)
             ts.append(time.perf_counter() - t)
-        v = FLOP / (min(ts[1:] or ts) * gc.nchunks) / 1e12
-        cpu = {"value": v, "unit": "TFLOP/s", "cores": cores, "kind": "port",
-               "sample": "one 2048x2048 output chunk (1/16 of the 8192^3 opt_gemm) with the reference's block-pair "
-                         "loop: per-pair LZ4 block decode, single-threaded OpenBLAS dgemm per worker thread, LZ4 "
-                         "re-encode; rate scaled to the full product"}
+        v = FLOP / float(np.median(ts)) / 1e12
+        cpu = {"value": v, "unit": "TFLOP/s", "cores": cores, "kind": "port", "samples": len(ts),
+               "sample_s": [round(x, 3) for x in ts], "statistic": "median",
+               "sample": "the whole 8192^3 opt_gemm (16 output chunks) per sample with the reference's block-pair "
+                         "loop: per-pair LZ4 block decode, single-threaded OpenBLAS dgemm per worker thread, each "
+                         "block LZ4-compressed by its worker"}
         # upper bound on the host: dense float64 product of the decoded operands with
         # torch.mm on all cores (no codec work), one warm-up and one timed call
         torch.set_num_threads(cores)
         ta, tb = torch.from_numpy(A), torch.from_numpy(B)
         torch.mm(ta[:1024], tb)
-        t = time.perf_counter()
-        torch.mm(ta, tb)
-        cpu["dense_upper_bound"] = {"value": FLOP / (time.perf_counter() - t) / 1e12, "unit": "TFLOP/s",
-                                    "cores": cores, "what": "torch.mm float64 8192^3 on decoded operands"}
+        td = []
+        for _ in range(3):
+            t = time.perf_counter()
+            torch.mm(ta, tb)
+            td.append(time.perf_counter() - t)
+        cpu["dense_upper_bound"] = {"value": FLOP / float(np.median(td)) / 1e12, "unit": "TFLOP/s",
+                                    "cores": cores, "samples": len(td), "statistic": "median",
+                                    "what": "torch.mm float64 8192^3 on decoded operands"}
         del ta, tb
 
     pk = peaks()
@@ -595,9 +624,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": hr["ms"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (numpy default_rng(3))",
-        "config": {"workload": "precision_f64 opt_gemm 8192^3, chunk 2048^2, block 256^2, LZ4 clevel5 + SHUFFLE",
-                   "form": head, "M": M, "N": N, "K": K, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (compressed A+B %.0f MB)" % ((a_cb + b_cb) / 1e6)},
+        "config": bench_config(world), "form": head,
         "forms": {k: {"tflops": world * FLOP / (r["ms"] * 1e-3) / 1e12, "ms_per_step": r["ms"],
                       "encoder": "liblz4-identical" if r["encoder"] == ia.ENCODER_LIBLZ4 else "parallel-parse",
                       "ms_parts": {"decode_a": r["parts"][0], "decode_b": r["parts"][1], "product": r["parts"][2],
@@ -635,19 +662,20 @@ def run_ours(args):
     print(json.dumps(line), flush=True)
 
 
-def run_profile_case(args):
-    """Small cases for ncu captures (--set full on one kernel family at a time).
-    codec: an n x n float64 container (n = --profile-n, default 4096) of the product's kind of values (gaussian) encoded
-    with the parallel encoder, then an A-like one (uniform(-1,1) x 2^U{-8..8}) decoded; three
-    rounds each.  split: the split-precision float64 product n x n x n on device
-    operands (iarray_b200_dense_gemm), two rounds.  Inputs are larger than L2."""
+def run_kernel_case(args):
+    """One small case of one kernel family, for per-kernel counter captures.
+    codec: an n x n float64 container (n = --case-n, default 4096) of the product's kind of
+    values (gaussian) encoded with the parallel encoder, then an A-like one
+    (uniform(-1,1) x 2^U{-8..8}) decoded; three rounds each.  split: the split-precision
+    float64 product n x n x n on device operands (iarray_b200_dense_gemm), two rounds.
+    Inputs are larger than L2 and a few GB at most are held on the device."""
     import ctypes
     import torch
     import iarray_b200 as ia
     ia.init()
     rng = np.random.default_rng(5)
-    n = args.profile_n
-    if args.profile_case == "codec":
+    n = args.case_n
+    if args.kernel_case == "codec":
         ctx = ia.Context(encoder=ia.ENCODER_PARALLEL)
         C = rng.standard_normal((n, n)) * 600.0
         A = rng.uniform(-1, 1, (n, n)) * np.exp2(rng.integers(-8, 9, (n, n)))
@@ -673,7 +701,7 @@ def run_profile_case(args):
         ref = (A[:64] @ B).cpu().numpy()
         err = np.linalg.norm(C[:64].cpu().numpy() - ref) / np.linalg.norm(ref)
         assert err < 1e-13, err
-    print(json.dumps({"profile_case": args.profile_case, "ok": True}))
+    print(json.dumps({"kernel_case": args.kernel_case, "ok": True}))
 
 
 def main():
@@ -684,13 +712,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--err-rows", type=int, default=256, help="rows (default_rng(99)) for the normwise error")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-samples", type=int, default=3, help="whole-product samples of the CPU baseline")
     ap.add_argument("--no-secondary", action="store_true", help="skip the GEMV, float32 and batching workloads")
-    ap.add_argument("--profile-case", choices=["codec", "split"], default=None,
-                    help="run one small case for an ncu capture instead of the benchmark")
-    ap.add_argument("--profile-n", type=int, default=4096, help="matrix size of --profile-case")
+    ap.add_argument("--kernel-case", choices=["codec", "split"], default=None,
+                    help="run one small case of one kernel family instead of the benchmark")
+    ap.add_argument("--case-n", type=int, default=4096, help="matrix size of --kernel-case")
     args = ap.parse_args()
-    if args.profile_case:
-        run_profile_case(args)
+    if args.kernel_case:
+        run_kernel_case(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

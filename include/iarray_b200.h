@@ -14,7 +14,11 @@
  *
  * Return codes follow libinac's 64-bit RC layout (doc/inac/error.md in the
  * reference): bit 63 = error flag, bits 16..23 = adjective/verb code, bit 15 =
- * negate flag, bits 0..14 = subject.
+ * negate flag, bits 0..14 = subject.  The subject numbers (IARRAY_ES_*) are the
+ * reference's; the adjective/verb numbers behind INA_ERR_* are this library's own,
+ * because libinac, which defines them, is not part of the reference's sources.
+ * Compare return codes with the IARRAY_ERR_* / INA_ERR_* macros of this header, not
+ * with raw numbers taken from a libinac build.
  */
 #ifndef IARRAY_B200_H
 #define IARRAY_B200_H
@@ -290,7 +294,8 @@ INA_API(ina_rc_t) iarray_opt_gemv(iarray_context_t *ctx, iarray_container_t *a, 
 typedef enum iarray_b200_form_e {
     IARRAY_B200_FORM_NATIVE = 0,   /* FP64 DMMA / FP32 FFMA, the plain drop-in */
     IARRAY_B200_FORM_SPLIT = 1,    /* float64: Ozaki INT8 slices on tcgen05;
-                                      float32: 3xBF16 on tcgen05 with FP32 accumulation */
+                                      float32: BF16 word splits on tcgen05 (6 or 3
+                                      products) with FP32 accumulation */
 } iarray_b200_form_t;
 
 INA_API(ina_rc_t) iarray_b200_set_form(iarray_context_t *ctx, iarray_b200_form_t form);
@@ -306,6 +311,11 @@ typedef enum iarray_b200_encoder_e {
 INA_API(ina_rc_t) iarray_b200_set_encoder(iarray_context_t *ctx, iarray_b200_encoder_t encoder);
 /* Number of INT8 moduli/slices the float64 split form uses (0 = automatic). */
 INA_API(ina_rc_t) iarray_b200_set_split_terms(iarray_context_t *ctx, int nterms);
+/* Number of BF16 tensor-core products of the float32 split form: 6 (each operand split
+ * into three bf16 words; float32 accuracy) or 3 (two words, "3xBF16": each operand held
+ * to about 2^-17 relative, so the result carries about 4e-6 normwise error on random data
+ * whatever the accumulation); 0 = automatic (6).  Both sum their products in FP32. */
+INA_API(ina_rc_t) iarray_b200_set_split_products_f32(iarray_context_t *ctx, int nproducts);
 
 /* Per-call timing of the last product on this context, in milliseconds (CUDA events):
  * [0] decode A, [1] decode B, [2] product, [3] encode C, [4] total device time. */
@@ -418,9 +428,10 @@ INA_API(ina_rc_t) iarray_b200_kernel_profile(char *buf, int64_t cap, int64_t *le
  * The fixed array (about 9.7 MiB) is held by every GPU that loads the library's kernels
  * until the process exits.  The first call on each device looks up the array's device
  * address and sets a kernel attribute; make that first call before any stream capture.
- * All calls share the array and it keeps the last call's contents: calls whose work
- * overlaps on the GPU (other streams, other host threads) race on it and must be
- * serialised by the caller. */
+ * Every call waits for `stream` before it returns (it reads the decoders' status word
+ * back to the host).  All calls share the array and it keeps the last call's contents:
+ * calls whose work overlaps on the GPU (other streams, other host threads) race on it
+ * and must be serialised by the caller. */
 #define IARRAY_B200_NOALLOC_MAX_BYTES (8LL << 20)
 #define IARRAY_B200_NOALLOC_MAX_BLOCKS 4096LL
 #define IARRAY_ERR_NOALLOC_TOO_LARGE (INA_ERR_OUT_OF_RANGE | IARRAY_ES_BUFFER)

@@ -118,23 +118,31 @@ bool make_geom(int ndim, const int64_t *shape, const int64_t *chunk, const int64
     memset(g, 0, sizeof(*g));
     g->itemsize = itemsize;
     g->ndim = ndim;
+    // every extent is held below 2^48 and every product below is checked by division
+    // first, so no size computed here can wrap around
+    constexpr int64_t kMaxExtent = int64_t(1) << 48;
     for (int d = 0; d < 2; d++) {
         const int s = d - (2 - ndim);   // 1-D arrays are 1 x n
         g->shape[d] = s < 0 ? 1 : shape[s];
         g->chunk[d] = s < 0 ? 1 : chunk[s];
         g->block[d] = s < 0 ? 1 : block[s];
         if (g->shape[d] < 0 || g->chunk[d] <= 0 || g->block[d] <= 0) return false;
+        if (g->shape[d] > kMaxExtent || g->chunk[d] > kMaxExtent) return false;
         if (g->block[d] > g->chunk[d]) return false;
         g->extc[d] = round_up(g->chunk[d], g->block[d]);
         g->cgrid[d] = g->shape[d] == 0 ? 0 : ceil_div(g->shape[d], g->chunk[d]);
         g->bgrid[d] = g->extc[d] / g->block[d];
     }
+    // Blosc2 chunks are below 2 GiB: extc0 * extc1 * itemsize < 2^31 - 64
+    const int64_t kChunkMax = (int64_t)INT32_MAX - 64;
+    if (g->extc[0] > kChunkMax / g->extc[1] / itemsize) return false;
+    if (g->cgrid[1] && g->cgrid[0] > INT64_MAX / 2 / g->cgrid[1]) return false;
     g->nchunks = g->cgrid[0] * g->cgrid[1];
     g->nblocks = g->bgrid[0] * g->bgrid[1];
     g->blockn = g->block[0] * g->block[1];
     g->blocksize = g->blockn * itemsize;
     g->chunk_nbytes = g->extc[0] * g->extc[1] * itemsize;
-    if (g->chunk_nbytes > (int64_t)INT32_MAX - 64) return false;   // Blosc2 chunks are < 2 GiB
+    if (g->chunk_nbytes > kChunkMax) return false;
     return true;
 }
 
@@ -169,6 +177,7 @@ struct iarray_context_s {
     cudaStream_t stream = nullptr;
     int form = IARRAY_B200_FORM_NATIVE;
     int split_terms = 0;
+    int split_products_f32 = 0;              // float32 split form: 3 or 6 BF16 products (0: 6)
     int encoder = IARRAY_B200_ENCODER_LIBLZ4;
     double timings[5] = {0, 0, 0, 0, 0};
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -317,6 +326,13 @@ INA_API(ina_rc_t) iarray_b200_set_split_terms(iarray_context_t *ctx, int nterms)
     return INA_SUCCESS;
 }
 
+INA_API(ina_rc_t) iarray_b200_set_split_products_f32(iarray_context_t *ctx, int nproducts)
+{
+    CHECK_ARG(ctx && (nproducts == 0 || nproducts == 3 || nproducts == 6));
+    ctx->split_products_f32 = nproducts;
+    return INA_SUCCESS;
+}
+
 INA_API(ina_rc_t) iarray_b200_last_timings(iarray_context_t *ctx, double *ms5)
 {
     CHECK_ARG(ctx && ms5);
@@ -452,6 +468,21 @@ static ina_rc_t encode_into(iarray_context_t *ctx, iarray_container_t *c, const 
     return INA_SUCCESS;
 }
 
+// A decoder's status word: malformed chunk data is a codec failure; a bounded wait on an
+// asynchronous copy that gave up (DE_WAIT) is a GPU failure, not bad data.
+static ina_rc_t status_rc(int status)
+{
+    if (status == 0) return INA_SUCCESS;
+    return rc_err(status == iab::DE_WAIT ? IARRAY_ERR_GPU_FAILED : IARRAY_ERR_BLOSC_FAILED);
+}
+
+static ina_rc_t decode_rc(int r)
+{
+    if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    if (r < 0) return rc_err(IARRAY_ERR_GPU_FAILED);
+    return status_rc(r);
+}
+
 // Decode the stored chunks of c (its base geometry, not the view) into dense memory.
 static ina_rc_t decode_store(iarray_context_t *ctx, const iarray_container_t *c, void *dense, int64_t ld)
 {
@@ -464,18 +495,7 @@ static ina_rc_t decode_store(iarray_context_t *ctx, const iarray_container_t *c,
     const ChunkStore &s = *c->store;
     const int r = iab::decode_container(g, s.buf.as<uint8_t>(), (int64_t)s.buf.n, s.d_off.as<int64_t>(), s.d_len.as<int32_t>(), dense, ld,
                                         ctx->stream);
-    if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
-    if (r < 0) return rc_err(IARRAY_ERR_GPU_FAILED);
-    if (r > 0) return rc_err(IARRAY_ERR_BLOSC_FAILED);
-    return INA_SUCCESS;
-}
-
-static ina_rc_t decode_rc(int r)
-{
-    if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
-    if (r < 0) return rc_err(IARRAY_ERR_GPU_FAILED);
-    if (r > 0) return rc_err(IARRAY_ERR_BLOSC_FAILED);
-    return INA_SUCCESS;
+    return decode_rc(r);
 }
 
 // Decode two stored (non-view) containers on the context's stream with one LZ4 launch for
@@ -710,14 +730,12 @@ INA_API(ina_rc_t) iarray_b200_decode_noalloc(int8_t ndim, const int64_t *shape, 
     CHECK_ARG(ld >= g.shape[1]);
     static_assert(IARRAY_B200_NOALLOC_MAX_BYTES == iab::NOALLOC_MAX_BYTES &&
                   IARRAY_B200_NOALLOC_MAX_BLOCKS == iab::NOALLOC_MAX_BLOCKS, "no-allocation limits");
-    if (g.nchunks * g.chunk_nbytes > iab::NOALLOC_MAX_BYTES || g.nchunks * g.nblocks > iab::NOALLOC_MAX_BLOCKS)
-        return rc_err(IARRAY_ERR_NOALLOC_TOO_LARGE);
+    if (!iab::noalloc_fits(g)) return rc_err(IARRAY_ERR_NOALLOC_TOO_LARGE);
     const int r = iab::decode_noalloc(g, static_cast<const uint8_t *>(chunks), chunks_len, dptr, ld,
                                       static_cast<cudaStream_t>(stream));
     if (r == -102) return rc_err(IARRAY_ERR_NOALLOC_TOO_LARGE);
     if (r < 0) return rc_err(IARRAY_ERR_GPU_FAILED);
-    if (r > 0) return rc_err(IARRAY_ERR_BLOSC_FAILED);
-    return INA_SUCCESS;
+    return status_rc(r);
 }
 
 INA_API(ina_rc_t) iarray_b200_encode_from_device(iarray_context_t *ctx, iarray_dtshape_t *dtshape, const void *dptr,
@@ -1006,7 +1024,8 @@ static ina_rc_t dense_product(iarray_context_t *ctx, int dtype, int64_t M, int64
             r = iab::gemm_f64_ozaki(M, N, K, (const double *)A, lda, (const double *)B, ldb, (double *)C, ldc,
                                     ctx->split_terms, ctx->stream);
         else
-            r = iab::gemm_f32_bf16x3(M, N, K, (const float *)A, lda, (const float *)B, ldb, (float *)C, ldc, ctx->stream);
+            r = iab::gemm_f32_bf16_split(M, N, K, (const float *)A, lda, (const float *)B, ldb, (float *)C, ldc,
+                                         ctx->split_products_f32, ctx->stream);
         if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
         if (r != 0) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
     } else if (dtype == IARRAY_DATA_TYPE_DOUBLE) {
@@ -1537,7 +1556,7 @@ INA_API(ina_rc_t) iarray_b200_opt_gemm_cframes(iarray_context_t *ctx, const uint
     if (cudaMemcpy(hs.data(), status.p, hs.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
         return rc_err(IARRAY_ERR_GPU_FAILED);
     for (int64_t r = 0; r < rowsA + rowsB; r++)
-        if (hs[(size_t)(r * 16 + 1)]) return rc_err(IARRAY_ERR_BLOSC_FAILED);
+        if (hs[(size_t)(r * 16 + 1)]) return status_rc(hs[(size_t)(r * 16 + 1)]);
     for (auto &w : oz)
         if (w.err.p && iab::gemm_f64_ozaki_finish(&w, st)) return rc_err(IARRAY_ERR_GPU_FAILED);
     *out_len = hsize + acc + tsize;
@@ -1768,7 +1787,7 @@ ina_rc_t batch_status(iarray_b200_batch_t *bt)
     if (cudaMemcpy(h.data(), bt->status.p, h.size() * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
         return rc_err(IARRAY_ERR_GPU_FAILED);
     for (int64_t i = 0; i < 2 * bt->n; i++)
-        if (h[(size_t)(i * 16 + 1)]) return rc_err(IARRAY_ERR_BLOSC_FAILED);
+        if (h[(size_t)(i * 16 + 1)]) return status_rc(h[(size_t)(i * 16 + 1)]);
     if (bt->form == IARRAY_B200_FORM_SPLIT)
         for (auto &w : bt->oz)
             if (iab::gemm_f64_ozaki_finish(&w, bt->ctx->stream)) return rc_err(IARRAY_ERR_GPU_FAILED);

@@ -2286,8 +2286,8 @@ static uint8_t *noalloc_scratch()
 
 int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, void *out, int64_t ld, cudaStream_t st)
 {
+    if (!noalloc_fits(g)) return -102;
     const int64_t nbl = g.nchunks * g.nblocks;
-    if (g.nchunks * g.chunk_nbytes > NOALLOC_MAX_BYTES || nbl > NOALLOC_MAX_BLOCKS) return -102;
     if (nbl == 0) return 0;
     uint8_t *base = noalloc_scratch();
     if (!base) return -101;
@@ -2301,7 +2301,7 @@ int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes,
     int *njobs = counters, *err = counters + 1;
     // the job count, the status word and the job cursor must start at zero; descriptors,
     // the chunk index and the image are fully rewritten before they are read
-    cudaMemsetAsync(counters, 0, 64, st);
+    if (cudaMemsetAsync(counters, 0, 64, st) != cudaSuccess) return -101;
     const int sms = sm_count();
     IAB_TIMED("k_chunk_walk", st, k_chunk_walk<<<1, 32, 0, st>>>(d_chunks, chunks_bytes, g.nchunks, off, len));
     {
@@ -2331,6 +2331,9 @@ int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes,
         IAB_TIMED("k_scatter", st, k_scatter<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
             g, rest, nrest, d_chunks, bd, sd, img, (uint8_t *)out, ld));
     }
+    // a launch that failed (a bad configuration, or an error left by earlier work) never
+    // wrote the status word: report it instead of the zero it still holds
+    if (cudaPeekAtLastError() != cudaSuccess) return -101;
     int h_err = 0;
     if (cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return -101;
     if (cudaStreamSynchronize(st) != cudaSuccess) return -101;

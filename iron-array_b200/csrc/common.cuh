@@ -193,6 +193,13 @@ int decode_scatter(const DecodeArgs &a, DecodeWork *w, cudaStream_t st);
 // DevErr (synchronises `st`), -101 on a CUDA error.
 constexpr int64_t NOALLOC_MAX_BYTES = int64_t(8) << 20;
 constexpr int64_t NOALLOC_MAX_BLOCKS = 4096;
+// Whether g fits those limits; the products are checked by division, so a huge geometry
+// cannot wrap around and pass.
+inline bool noalloc_fits(const Geom &g)
+{
+    if (g.nchunks == 0) return true;
+    return g.chunk_nbytes <= NOALLOC_MAX_BYTES / g.nchunks && g.nblocks <= NOALLOC_MAX_BLOCKS / g.nchunks;
+}
 int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, void *out, int64_t ld, cudaStream_t st);
 
 // Encode a dense row-major array into Blosc2 chunks.  On return *d_out holds the
@@ -284,8 +291,10 @@ int gemm_f64_ozaki_rows_product(int64_t M, const double *A, int64_t lda, const O
 int gemm_f64_ozaki_rows(int64_t M, const double *A, int64_t lda, const OzakiB &ob, double *C, int64_t ldc,
                         OzakiWork *w, cudaStream_t st);
 int gemm_f64_ozaki_finish(OzakiWork *w, cudaStream_t st);
-int gemm_f32_bf16x3(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda,
-                    const float *B, int64_t ldb, float *C, int64_t ldc, cudaStream_t st);
+// float32 split form: each operand split into bf16 words, `products` BF16 tensor-core
+// products (3: two words; 6: three words; 0: 6) summed in FP32 segments.
+int gemm_f32_bf16_split(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda,
+                        const float *B, int64_t ldb, float *C, int64_t ldc, int products, cudaStream_t st);
 
 void fill_arange(int dtype, int64_t M, int64_t N, int64_t ld, double start, double step, void *out,
                  cudaStream_t st);

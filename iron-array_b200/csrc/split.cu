@@ -867,55 +867,84 @@ int gemm_f64_ozaki_launch(int64_t M, int64_t N, int64_t K, const double *A, int6
     return gemm_f64_ozaki_rows(M, A, lda, w->b, C, ldc, w, st);
 }
 
-// ============================================================================ float32: 3xBF16
-// A float32 x is split as x = hi + lo + e, hi = bf16(x), lo = bf16(x - hi), |e| <= 2^-17 |x|.
-// C = A_hi B_hi + A_hi B_lo + A_lo B_hi (the lo*lo term, below float32 resolution, is
-// dropped) is one tcgen05.mma kind::f16 GEMM whose K loop runs three times over the
-// operand planes, all passes accumulating into the same FP32 TMEM tile.
-namespace b3 {
+// ============================================================================ float32: BF16 splits
+// A float32 x is split into bfloat16 words.  Two words: hi = bf16(x), lo = bf16(x - hi)
+// hold x to about 2^-17 relative, and C = A_lo B_hi + A_hi B_lo + A_hi B_hi (three
+// products; lo x lo is below that precision).  Three words: x1 = bf16(x),
+// x2 = bf16(x - x1), x3 = bf16(x - x1 - x2) hold x to about 2^-25 (every difference is
+// exact in float32), and C = A3 B1 + A1 B3 + A2 B2 + A2 B1 + A1 B2 + A1 B1 (six products,
+// the dropped ones below float32 resolution).  Each product is a tcgen05.mma kind::f16
+// pass over K (bf16 x bf16 -> fp32 in TMEM).
+//
+// Accuracy of the sums.  The tensor core adds each K = 16 slice into its FP32 accumulator
+// with a truncating alignment, so one long accumulation loses precision in proportion to
+// its length (measured on a B200: normwise 4.4e-6 at K = 4096 with exact bf16 operands,
+// against 1.1e-6 for FFMA).  Two changes keep the error at float32 level:
+//   - passes run smallest first, so the small cross products are never added to an
+//     accumulator that already holds the large A1 B1 sums;
+//   - the pass sequence is cut into segments of SEG_KT k-tiles (512 K).  Each segment
+//     starts a fresh TMEM accumulator (two alternate, so the tensor core never waits for
+//     the drain), and the epilogue warps add every segment into FP32 registers with
+//     round-to-nearest.  The truncation error is then bounded by one segment's length
+//     instead of the whole K.
+namespace bfs {
 constexpr int BM = 128, BN = 256, BK = 64, STAGES = 4;        // BK bf16 = 128 bytes per row
 constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTES + B_BYTES;
-constexpr int THREADS = 192;
+constexpr int EPI_WARPS = 8;                                  // two per TMEM lane quarter, 128 columns each
+constexpr int THREADS = 64 + 32 * EPI_WARPS;
 constexpr int SMEM = 1024 + STAGES * STAGE_BYTES + 256;
+constexpr int SEG_KT = 8;                                     // k-tiles per accumulation segment (512 K)
+constexpr int MAX_PASS = 6;
 constexpr uint32_t IDESC = tc::make_idesc(1 /*F32*/, 1 /*BF16*/, 1 /*BF16*/, BM, BN);
-__device__ __constant__ int kAPlane[3] = {0, 0, 1};
-__device__ __constant__ int kBPlane[3] = {0, 1, 0};
 }
 
-struct B3Params {
+struct BfsParams {
     int M, N, Kp, tiles_m, tiles_n;
+    int npass;                         // 3 or 6 products
+    int pa[bfs::MAX_PASS], pb[bfs::MAX_PASS];   // word plane of A and of B in each pass
     float *C;
     int64_t ldc;
     int *err;
 };
 
-// Row-major A (M x K) -> planes [2][M][Kp] of bf16 (hi, lo), K padded with zeros.
-// A row (column) holding a value whose bf16 part is not finite (NaN, infinity, or a float
-// beyond bf16's range) sets its flag; its outputs are recomputed by k_nonfinite_fix.
-__global__ void __launch_bounds__(256) k_split_rows(int M, int K, int Kp, const float *__restrict__ A, int64_t lda,
-                                                    __nv_bfloat16 *__restrict__ P, int *__restrict__ rflag)
+__device__ __forceinline__ void split_words(float x, int words, __nv_bfloat16 (&w)[3])
+{
+    w[0] = __float2bfloat16_rn(x);
+    const float r1 = x - __bfloat162float(w[0]);                  // exact
+    w[1] = __float2bfloat16_rn(r1);
+    const float r2 = r1 - __bfloat162float(w[1]);                 // exact
+    w[2] = words == 3 ? __float2bfloat16_rn(r2) : __float2bfloat16_rn(0.f);
+}
+
+// Row-major A (M x K) -> `words` planes [words][M][Kp] of bf16, K padded with zeros.
+// A row (column) holding a value whose leading bf16 word is not finite (NaN, infinity, or
+// a float beyond bf16's range) sets its flag; its outputs are recomputed by
+// k_nonfinite_fix.
+__global__ void __launch_bounds__(256) k_split_rows(int M, int K, int Kp, int words, const float *__restrict__ A,
+                                                    int64_t lda, __nv_bfloat16 *__restrict__ P, int *__restrict__ rflag)
 {
     const int groups = Kp / 4;
     const int64_t total = (int64_t)M * groups, plane = (int64_t)M * Kp;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
         const int i = (int)(t / groups), k0 = (int)(t - (int64_t)i * groups) * 4;
-        __nv_bfloat16 h[4], l[4];
+        __nv_bfloat16 h[3][4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             const float x = k0 + u < K ? A[(int64_t)i * lda + k0 + u] : 0.f;
-            h[u] = __float2bfloat16_rn(x);
-            l[u] = __float2bfloat16_rn(x - __bfloat162float(h[u]));
-            if (!isfinite(__bfloat162float(h[u]))) rflag[i] = 1;
+            __nv_bfloat16 w[3];
+            split_words(x, words, w);
+            h[0][u] = w[0]; h[1][u] = w[1]; h[2][u] = w[2];
+            if (!isfinite(__bfloat162float(w[0]))) rflag[i] = 1;
         }
         __nv_bfloat16 *ph = P + (int64_t)i * Kp + k0;
-        *reinterpret_cast<uint2 *>(ph) = *reinterpret_cast<const uint2 *>(h);
-        *reinterpret_cast<uint2 *>(ph + plane) = *reinterpret_cast<const uint2 *>(l);
+        for (int wd = 0; wd < words; wd++)
+            *reinterpret_cast<uint2 *>(ph + wd * plane) = *reinterpret_cast<const uint2 *>(h[wd]);
     }
 }
 
-// Row-major B (K x N) -> planes [2][N][Kp] of bf16 (transposed, K-major).
-__global__ void __launch_bounds__(256) k_split_cols(int K, int N, int Kp, const float *__restrict__ B, int64_t ldb,
-                                                    __nv_bfloat16 *__restrict__ P, int *__restrict__ cflag)
+// Row-major B (K x N) -> `words` planes [words][N][Kp] of bf16 (transposed, K-major).
+__global__ void __launch_bounds__(256) k_split_cols(int K, int N, int Kp, int words, const float *__restrict__ B,
+                                                    int64_t ldb, __nv_bfloat16 *__restrict__ P, int *__restrict__ cflag)
 {
     __shared__ float tile[64][65];
     const int k0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
@@ -930,27 +959,30 @@ __global__ void __launch_bounds__(256) k_split_cols(int K, int N, int Kp, const 
         const int c = e >> 4, kg = (e & 15) * 4;
         const int j = j0 + c;
         if (j >= N || k0 + kg >= Kp) continue;
-        __nv_bfloat16 h[4], l[4];
+        __nv_bfloat16 h[3][4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-            const float x = tile[kg + u][c];
-            h[u] = __float2bfloat16_rn(x);
-            l[u] = __float2bfloat16_rn(x - __bfloat162float(h[u]));
-            if (!isfinite(__bfloat162float(h[u]))) cflag[j] = 1;
+            __nv_bfloat16 w[3];
+            split_words(tile[kg + u][c], words, w);
+            h[0][u] = w[0]; h[1][u] = w[1]; h[2][u] = w[2];
+            if (!isfinite(__bfloat162float(w[0]))) cflag[j] = 1;
         }
         __nv_bfloat16 *ph = P + (int64_t)j * Kp + k0 + kg;
-        *reinterpret_cast<uint2 *>(ph) = *reinterpret_cast<const uint2 *>(h);
-        *reinterpret_cast<uint2 *>(ph + plane) = *reinterpret_cast<const uint2 *>(l);
+        for (int wd = 0; wd < words; wd++)
+            *reinterpret_cast<uint2 *>(ph + wd * plane) = *reinterpret_cast<const uint2 *>(h[wd]);
     }
 }
 
-// Persistent, warp-specialised like k_i8gemm_mod: warp 0 loads (TMA), warp 1 issues the
-// MMAs of the three passes into one of two 128 x 256 FP32 TMEM accumulators, warps 2-5
-// store the other accumulator as float32 rows of C.
-__global__ void __launch_bounds__(b3::THREADS, 1) k_bf16x3_gemm(const __grid_constant__ CUtensorMap tmA,
-                                                                 const __grid_constant__ CUtensorMap tmB, B3Params p)
+// Persistent, warp-specialised: warp 0 loads (TMA), warp 1 issues the MMAs, warps 2-9
+// drain.  Per output tile the k-tile sequence of all passes (pass-major) is cut into
+// segments of SEG_KT k-tiles; each segment accumulates into one of two 128 x 256 FP32
+// TMEM accumulators from zero, and the epilogue adds it into FP32 registers (warp w reads
+// TMEM lane quarter w % 4, columns 128 (w - 2) / 4 .. + 127), storing the tile as float32
+// rows of C after its last segment.
+__global__ void __launch_bounds__(bfs::THREADS, 1) k_bf16s_gemm(const __grid_constant__ CUtensorMap tmA,
+                                                                 const __grid_constant__ CUtensorMap tmB, BfsParams p)
 {
-    using namespace b3;
+    using namespace bfs;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t *sA = smem, *sB = smem + STAGES * A_BYTES;
@@ -964,7 +996,7 @@ __global__ void __launch_bounds__(b3::THREADS, 1) k_bf16x3_gemm(const __grid_con
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) { tc::mbar_init(&full[s], 1); tc::mbar_init(&empty[s], 1); }
-        for (int b = 0; b < 2; b++) { tc::mbar_init(&tfull[b], 1); tc::mbar_init(&tempty[b], 4); }
+        for (int b = 0; b < 2; b++) { tc::mbar_init(&tfull[b], 1); tc::mbar_init(&tempty[b], EPI_WARPS); }
         tc::mbar_init(drain, 1);
         tc::fence_barrier_init();
         tc::tma_prefetch_desc(&tmA);
@@ -980,6 +1012,8 @@ __global__ void __launch_bounds__(b3::THREADS, 1) k_bf16x3_gemm(const __grid_con
     const uint32_t tmem_base = *tmem_slot;
     const int total = p.tiles_m * p.tiles_n;
     const int ktiles = p.Kp / BK;
+    const int steps = p.npass * ktiles;                  // k-tiles per output tile
+    const int nseg = (steps + SEG_KT - 1) / SEG_KT;
 
     if (warp == 0) {
         if (lane == 0) {
@@ -990,16 +1024,14 @@ __global__ void __launch_bounds__(b3::THREADS, 1) k_bf16x3_gemm(const __grid_con
             for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
                 int tm, tn;
                 tile_of(t, p.tiles_m, p.tiles_n, tm, tn);
-                for (int pass = 0; pass < 3 && ok; pass++) {
-                    const int pa = kAPlane[pass], pb = kBPlane[pass];
-                    for (int kt = 0; kt < ktiles; kt++) {
-                        if (!tc::mbar_wait(&empty[stage], phase ^ 1, p.err)) { ok = false; break; }
-                        tc::mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
-                        tc::tma_load_3d(sA + stage * A_BYTES, &tmA, kt * BK, tm * BM, pa, &full[stage]);
-                        tc::tma_load_3d(sB + stage * B_BYTES, &tmB, kt * BK, tn * BN, pb, &full[stage]);
-                        issued++;
-                        if (++stage == STAGES) { stage = 0; phase ^= 1; }
-                    }
+                for (int st = 0; st < steps; st++) {
+                    const int pass = st / ktiles, kt = st - pass * ktiles;
+                    if (!tc::mbar_wait(&empty[stage], phase ^ 1, p.err)) { ok = false; break; }
+                    tc::mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
+                    tc::tma_load_3d(sA + stage * A_BYTES, &tmA, kt * BK, tm * BM, p.pa[pass], &full[stage]);
+                    tc::tma_load_3d(sB + stage * B_BYTES, &tmB, kt * BK, tn * BN, p.pb[pass], &full[stage]);
+                    issued++;
+                    if (++stage == STAGES) { stage = 0; phase ^= 1; }
                 }
             }
             for (int64_t it = issued > STAGES ? issued - STAGES : 0; it < issued; it++)
@@ -1011,61 +1043,75 @@ __global__ void __launch_bounds__(b3::THREADS, 1) k_bf16x3_gemm(const __grid_con
             uint32_t phase = 0, acc_phase = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-                if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, p.err)) { ok = false; break; }
-                tc::tc_fence_after();
-                const uint32_t dt = tmem_base + (uint32_t)(acc * BN);
-                for (int step = 0; step < 3 * ktiles; step++) {
-                    if (!tc::mbar_wait(&full[stage], phase, p.err)) { ok = false; break; }
+                for (int sg = 0; sg < nseg && ok; sg++) {
+                    if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, p.err)) { ok = false; break; }
                     tc::tc_fence_after();
-                    const uint32_t a0 = tc::smem_addr(sA + stage * A_BYTES), b0 = tc::smem_addr(sB + stage * B_BYTES);
+                    const uint32_t dt = tmem_base + (uint32_t)(acc * BN);
+                    const int s0 = sg * SEG_KT, s1 = min(steps, s0 + SEG_KT);
+                    for (int st = s0; st < s1; st++) {
+                        if (!tc::mbar_wait(&full[stage], phase, p.err)) { ok = false; break; }
+                        tc::tc_fence_after();
+                        const uint32_t a0 = tc::smem_addr(sA + stage * A_BYTES), b0 = tc::smem_addr(sB + stage * B_BYTES);
 #pragma unroll
-                    for (int kk = 0; kk < BK / 16; kk++) {
-                        tc::mma_f16(dt, tc::sw128_kmajor_desc(a0 + kk * 32), tc::sw128_kmajor_desc(b0 + kk * 32), IDESC,
-                                    (step | kk) != 0);
+                        for (int kk = 0; kk < BK / 16; kk++) {
+                            tc::mma_f16(dt, tc::sw128_kmajor_desc(a0 + kk * 32), tc::sw128_kmajor_desc(b0 + kk * 32),
+                                        IDESC, (st != s0 || kk != 0) ? 1u : 0u);
+                        }
+                        tc::tc_commit(&empty[stage]);
+                        if (++stage == STAGES) { stage = 0; phase ^= 1; }
                     }
-                    tc::tc_commit(&empty[stage]);
-                    if (++stage == STAGES) { stage = 0; phase ^= 1; }
+                    if (!ok) break;
+                    tc::tc_commit(&tfull[acc]);
+                    if (++acc == 2) { acc = 0; acc_phase ^= 1; }
                 }
-                if (!ok) break;
-                tc::tc_commit(&tfull[acc]);
-                if (++acc == 2) { acc = 0; acc_phase ^= 1; }
             }
             tc::tc_commit(drain);
             tc::mbar_wait(drain, 0, p.err, 1u << 20);
         }
     } else {
-        const int q = warp & 3;
+        const int q = warp & 3;                          // TMEM lane quarter this warp may access
+        const int half = (warp - 2) >> 2;                // columns 128 * half .. + 127
         int acc = 0;
         uint32_t acc_phase = 0;
-        for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        bool ok = true;
+        float sum[128];
+        for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
             int tm, tn;
             tile_of(t, p.tiles_m, p.tiles_n, tm, tn);
-            if (!tc::mbar_wait(&tfull[acc], acc_phase, p.err)) break;
-            tc::tc_fence_after();
+#pragma unroll
+            for (int u = 0; u < 128; u++) sum[u] = 0.f;
+            for (int sg = 0; sg < nseg; sg++) {
+                if (!tc::mbar_wait(&tfull[acc], acc_phase, p.err)) { ok = false; break; }
+                tc::tc_fence_after();
+                const uint32_t ta = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + half * 128);
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    uint32_t v[32];
+                    tc::tmem_ld32(ta + (uint32_t)(c * 32), v);
+#pragma unroll
+                    for (int u = 0; u < 32; u++) sum[c * 32 + u] = __fadd_rn(sum[c * 32 + u], __uint_as_float(v[u]));
+                }
+                tc::tc_fence_before();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&tempty[acc]);
+                if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+            }
+            if (!ok) break;
             const int row = tm * BM + q * 32 + lane;
-            float *out = p.C + (int64_t)row * p.ldc + (int64_t)tn * BN;
-            for (int c = 0; c < BN; c += 32) {
-                uint32_t v[32];
-                tc::tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + c), v);
-                const int col = tn * BN + c;
-                if (row < p.M) {
-                    if (col + 32 <= p.N && ((reinterpret_cast<uintptr_t>(out + c) & 15) == 0)) {
-                        float4 *o4 = reinterpret_cast<float4 *>(out + c);
+            const int col0 = tn * BN + half * 128;
+            if (row < p.M) {
+                float *out = p.C + (int64_t)row * p.ldc + col0;
+                if (col0 + 128 <= p.N && ((reinterpret_cast<uintptr_t>(out) & 15) == 0)) {
+                    float4 *o4 = reinterpret_cast<float4 *>(out);
 #pragma unroll
-                        for (int u = 0; u < 8; u++)
-                            o4[u] = make_float4(__uint_as_float(v[4 * u]), __uint_as_float(v[4 * u + 1]),
-                                                __uint_as_float(v[4 * u + 2]), __uint_as_float(v[4 * u + 3]));
-                    } else {
+                    for (int u = 0; u < 32; u++)
+                        o4[u] = make_float4(sum[4 * u], sum[4 * u + 1], sum[4 * u + 2], sum[4 * u + 3]);
+                } else {
 #pragma unroll
-                        for (int b = 0; b < 32; b++)
-                            if (col + b < p.N) out[c + b] = __uint_as_float(v[b]);
-                    }
+                    for (int b = 0; b < 128; b++)
+                        if (col0 + b < p.N) out[b] = sum[b];
                 }
             }
-            tc::tc_fence_before();
-            __syncwarp();
-            if (lane == 0) tc::mbar_arrive(&tempty[acc]);
-            if (++acc == 2) { acc = 0; acc_phase ^= 1; }
         }
     }
     tc::tc_fence_before();
@@ -1074,17 +1120,20 @@ __global__ void __launch_bounds__(b3::THREADS, 1) k_bf16x3_gemm(const __grid_con
     if (warp == 1) tc::tmem_dealloc(tmem_base, 512);
 }
 
-int gemm_f32_bf16x3(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda, const float *B, int64_t ldb,
-                    float *C, int64_t ldc, cudaStream_t st)
+int gemm_f32_bf16_split(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda, const float *B, int64_t ldb,
+                        float *C, int64_t ldc, int products, cudaStream_t st)
 {
     if (!device_is_sm100()) return -1;
+    if (products == 0) products = 6;
+    if (products != 3 && products != 6) return -4;
     if (M <= 0 || N <= 0 || K <= 0) return 0;
     if (M > (1 << 30) || N > (1 << 30) || K > (1 << 30)) return -1;
     int dev = 0;
     cudaGetDevice(&dev);
-    const int64_t Kp = round_up(K, b3::BK);
+    const int words = products == 6 ? 3 : 2;
+    const int64_t Kp = round_up(K, bfs::BK);
     DevBuf pa, pb, err, flg;
-    if (!pa.allocate((size_t)(2 * M * Kp * 2), dev) || !pb.allocate((size_t)(2 * N * Kp * 2), dev) ||
+    if (!pa.allocate((size_t)(words * M * Kp * 2), dev) || !pb.allocate((size_t)(words * N * Kp * 2), dev) ||
         !err.allocate(16, dev) || !flg.allocate((size_t)(M + N) * 4, dev))
         return -100;
     cudaMemsetAsync(err.p, 0, 16, st);
@@ -1092,26 +1141,35 @@ int gemm_f32_bf16x3(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda
     int *rflag = flg.as<int>(), *cflag = rflag + M;
     const int nsm = sms();
     IAB_TIMED("k_split_rows", st, k_split_rows<<<(unsigned)(nsm * 16), 256, 0, st>>>(
-        (int)M, (int)K, (int)Kp, A, lda, pa.as<__nv_bfloat16>(), rflag));
+        (int)M, (int)K, (int)Kp, words, A, lda, pa.as<__nv_bfloat16>(), rflag));
     IAB_TIMED("k_split_cols", st, k_split_cols<<<dim3((unsigned)((N + 63) / 64), (unsigned)((Kp + 63) / 64)), 256, 0, st>>>(
-        (int)K, (int)N, (int)Kp, B, ldb, pb.as<__nv_bfloat16>(), cflag));
+        (int)K, (int)N, (int)Kp, words, B, ldb, pb.as<__nv_bfloat16>(), cflag));
     CUtensorMap tmA, tmB;
-    if (!make_tmap_3d(&tmA, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, pa.p, (uint64_t)Kp, (uint64_t)M, 2, (uint64_t)Kp * 2,
-                      (uint64_t)(Kp * M * 2), b3::BK, b3::BM, CU_TENSOR_MAP_SWIZZLE_128B) ||
-        !make_tmap_3d(&tmB, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, pb.p, (uint64_t)Kp, (uint64_t)N, 2, (uint64_t)Kp * 2,
-                      (uint64_t)(Kp * N * 2), b3::BK, b3::BN, CU_TENSOR_MAP_SWIZZLE_128B))
+    if (!make_tmap_3d(&tmA, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, pa.p, (uint64_t)Kp, (uint64_t)M, (uint64_t)words,
+                      (uint64_t)Kp * 2, (uint64_t)(Kp * M * 2), bfs::BK, bfs::BM, CU_TENSOR_MAP_SWIZZLE_128B) ||
+        !make_tmap_3d(&tmB, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, pb.p, (uint64_t)Kp, (uint64_t)N, (uint64_t)words,
+                      (uint64_t)Kp * 2, (uint64_t)(Kp * N * 2), bfs::BK, bfs::BN, CU_TENSOR_MAP_SWIZZLE_128B))
         return -1;
-    B3Params prm;
+    BfsParams prm;
+    memset(&prm, 0, sizeof(prm));
     prm.M = (int)M; prm.N = (int)N; prm.Kp = (int)Kp;
-    prm.tiles_m = (int)ceil_div(M, b3::BM); prm.tiles_n = (int)ceil_div(N, b3::BN);
+    prm.tiles_m = (int)ceil_div(M, bfs::BM); prm.tiles_n = (int)ceil_div(N, bfs::BN);
+    // word planes of each pass, smallest products first (A word, B word; 0 = leading)
+    static const int kPa3[3] = {1, 0, 0}, kPb3[3] = {0, 1, 0};
+    static const int kPa6[6] = {2, 0, 1, 1, 0, 0}, kPb6[6] = {0, 2, 1, 0, 1, 0};
+    prm.npass = products;
+    for (int i = 0; i < products; i++) {
+        prm.pa[i] = products == 6 ? kPa6[i] : kPa3[i];
+        prm.pb[i] = products == 6 ? kPb6[i] : kPb3[i];
+    }
     prm.C = C; prm.ldc = ldc; prm.err = err.as<int>();
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_bf16x3_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, b3::SMEM);
+        cudaFuncSetAttribute(k_bf16s_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, bfs::SMEM);
         attr = true;
     }
     const int tiles = prm.tiles_m * prm.tiles_n;
-    IAB_TIMED("k_bf16x3_gemm", st, k_bf16x3_gemm<<<(unsigned)std::min(tiles, nsm), b3::THREADS, b3::SMEM, st>>>(tmA, tmB, prm));
+    IAB_TIMED("k_bf16s_gemm", st, k_bf16s_gemm<<<(unsigned)std::min(tiles, nsm), bfs::THREADS, bfs::SMEM, st>>>(tmA, tmB, prm));
     launch_nonfinite_fix<float>(M, N, K, A, lda, B, ldb, C, ldc, rflag, cflag, 1, st);
     int h_err = 0;
     cudaMemcpyAsync(&h_err, err.p, sizeof(int), cudaMemcpyDeviceToHost, st);

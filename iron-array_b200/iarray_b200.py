@@ -114,6 +114,7 @@ def _lib():
             "iarray_opt_gemm": ([P, P, P, P, P], RC), "iarray_opt_gemm_a": ([P, P, P, P, P], RC),
             "iarray_opt_gemm_b": ([P, P, P, P, P], RC), "iarray_opt_gemv": ([P, P, P, P, P], RC),
             "iarray_b200_set_form": ([P, ctypes.c_int], RC), "iarray_b200_set_encoder": ([P, ctypes.c_int], RC), "iarray_b200_set_split_terms": ([P, ctypes.c_int], RC),
+            "iarray_b200_set_split_products_f32": ([P, ctypes.c_int], RC),
             "iarray_b200_last_timings": ([P, P], RC),
             "iarray_b200_from_chunks": ([P, P, P, I64, P, P, P], RC),
             "iarray_b200_get_chunk": ([P, P, I64, P, P], RC), "iarray_b200_nchunks": ([P, P], RC),
@@ -214,6 +215,11 @@ class Context:
     def set_form(self, form, split_terms=0):
         check(_lib().iarray_b200_set_form(self.ptr, form), "set_form")
         check(_lib().iarray_b200_set_split_terms(self.ptr, split_terms), "set_split_terms")
+
+    def set_split_products_f32(self, nproducts):
+        """BF16 products of the float32 split form: 6 (three-word split), 3 (two-word
+        split, "3xBF16"), 0 (automatic: 6)."""
+        check(_lib().iarray_b200_set_split_products_f32(self.ptr, nproducts), "set_split_products_f32")
 
     def timings(self):
         t = (ctypes.c_double * 5)()

@@ -774,6 +774,12 @@ typedef struct {
     cblas_dgemm_fn dgemm;
     lz4_dec_fn dec;
     uint8_t *cchunk;
+    /* per-block compression (whole-product form): block b's Blosc2 payload (its streams,
+     * csize words included) goes to bout + b * bcap, its length to blen[b]; -1 when the
+     * block does not compress into its own size (the chunk is then compressed whole) */
+    uint8_t *bout;
+    int64_t bcap;
+    int32_t *blen;
     int64_t next;
     pthread_mutex_t mu;
     int err;
@@ -839,6 +845,21 @@ static void *bl_worker(void *arg)
                           (const double *)bblk, (int)bn, 1.0, out, (int)bn);
             }
         }
+        if (jb->bout) {
+            /* Blosc2 compresses each block in the thread that filled it: shuffle + split
+             * streams of this block alone (a one-block chunk holds exactly those bytes
+             * after its header and its single bstart) */
+            const int bsz = (int)(bm * bn * 8);
+            uint8_t *cb1 = malloc((size_t)bsz + HDR + 64);
+            int r = ora_chunk_compress((const uint8_t *)out, bsz, 8, bsz, 1, SPLIT_AUTO, cb1, bsz + HDR);
+            int32_t plen = -1;
+            if (r > 0 && !(cb1[2] & 0x02) && r - HDR - 4 <= jb->bcap) {
+                plen = r - HDR - 4;
+                memcpy(jb->bout + cb * jb->bcap, cb1 + HDR + 4, (size_t)plen);
+            }
+            jb->blen[cb] = plen;
+            free(cb1);
+        }
     }
     free(ablk); free(bblk); free(tmp);
     return NULL;
@@ -846,6 +867,62 @@ static void *bl_worker(void *arg)
 
 
 
+
+/* The whole product: every output chunk of iarray_opt_gemm in the reference's order
+ * (src/linalg/iarray_gemm.c:399-425: one blosc2_compress_ctx per output chunk, its
+ * prefilter run by `nthreads` workers over the chunk's blocks).  Each worker computes
+ * an output block and compresses it at once, as Blosc2's workers do; the chunk is then
+ * assembled from the block payloads (header, bstarts, payloads in block order).  Output
+ * chunk c goes to outs[c] (capacity chunk_nbytes + 32), its size to out_len[c].
+ * Returns 0, or < 0 on error. */
+EXPORT int ora_cpu_opt_gemm(const ora_schunk_t *A, const ora_schunk_t *B, const ora_geom_t *Cg, int nthreads,
+                            void *dgemm, void *lz4_dec, uint8_t **outs, int32_t *out_len)
+{
+    const int64_t ext0 = extc_of(Cg, 0), ext1 = extc_of(Cg, 1);
+    const int64_t cnb = ext0 * ext1 * 8;
+    const int64_t nch = (ext_of(Cg, 0) / Cg->chunk[0]) * (ext_of(Cg, 1) / Cg->chunk[1]);
+    const int64_t nbl = (ext0 / Cg->block[0]) * (ext1 / Cg->block[1]);
+    const int64_t bsz = Cg->block[0] * Cg->block[1] * 8;
+    const int64_t bcap = bsz + 8 * 4 + 8;          /* streams no larger than the block, csize words */
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    uint8_t *cchunk = malloc((size_t)cnb), *bout = malloc((size_t)(nbl * bcap));
+    int32_t *blen = malloc((size_t)nbl * 4);
+    int rc = 0;
+    for (int64_t cn = 0; cn < nch && rc == 0; cn++) {
+        bl_job_t jb;
+        memset(&jb, 0, sizeof(jb));
+        jb.A = A; jb.B = B; jb.Cg = Cg; jb.cn = cn;
+        jb.dgemm = (cblas_dgemm_fn)dgemm; jb.dec = (lz4_dec_fn)lz4_dec;
+        jb.cchunk = cchunk; jb.bout = bout; jb.bcap = bcap; jb.blen = blen;
+        pthread_mutex_init(&jb.mu, NULL);
+        pthread_t th[256];
+        for (int i = 0; i < nthreads; i++) pthread_create(&th[i], NULL, bl_worker, &jb);
+        for (int i = 0; i < nthreads; i++) pthread_join(th[i], NULL);
+        pthread_mutex_destroy(&jb.mu);
+        if (jb.err) { rc = -1; break; }
+        int64_t pos = HDR + 4 * nbl;
+        int whole = 0;
+        for (int64_t b = 0; b < nbl; b++) {
+            if (blen[b] < 0 || pos + blen[b] > cnb) { whole = 1; break; }
+            wr32(outs[cn] + HDR + 4 * b, (int32_t)pos);
+            memcpy(outs[cn] + pos, bout + b * bcap, (size_t)blen[b]);
+            pos += blen[b];
+        }
+        if (whole) {
+            int r = ora_chunk_compress(cchunk, (int)cnb, 8, (int)bsz, 1, SPLIT_AUTO, outs[cn], (int)cnb + 32);
+            if (r < 0) { rc = -2; break; }
+            out_len[cn] = r;
+        } else {
+            const int split = ora_split_decision(SPLIT_AUTO, CODEC_LZ4, 1, 8, (int)bsz);
+            write_header(outs[cn], 0x05 | (CODEC_LZ4 << 5) | (split ? 0 : 0x10), 8, (int)cnb, (int)bsz, (int)pos, 1,
+                         CODEC_LZ4);
+            out_len[cn] = (int32_t)pos;
+        }
+    }
+    free(cchunk); free(bout); free(blen);
+    return rc;
+}
 
 /* Returns the compressed size of the output chunk written to `out` (capacity
  * chunk_nbytes + 32), or < 0 on error. */

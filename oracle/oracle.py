@@ -435,3 +435,28 @@ def cpu_opt_gemm_chunk(ga: Geom, a_chunks, gb: Geom, b_chunks, gc: Geom, cn: int
     if r < 0:
         raise RuntimeError(f"cpu baseline failed ({r})")
     return out.raw[:r]
+
+
+LIB.ora_cpu_opt_gemm.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+
+
+def cpu_opt_gemm(ga: Geom, a_chunks, gb: Geom, b_chunks, gc: Geom, nthreads: int):
+    """The whole iarray_opt_gemm product by the reference's loop on host cores
+    (src/linalg/iarray_gemm.c:399-425: output chunk after output chunk, each one's blocks
+    computed by `nthreads` workers with per-pair block decode and single-threaded OpenBLAS
+    dgemm, each block compressed by its worker).  Returns the compressed output chunks."""
+    bl = openblas_dgemm()
+    if bl is None:
+        raise RuntimeError("no cblas_dgemm available for the CPU baseline")
+    dec = liblz4_decompress()
+    sa, sb = _schunk(ga, a_chunks), _schunk(gb, b_chunks)
+    cg = gc.cstruct()
+    outs = [ctypes.create_string_buffer(gc.chunk_nbytes + 64) for _ in range(gc.nchunks)]
+    ptrs = (ctypes.c_void_p * gc.nchunks)(*[ctypes.cast(o, ctypes.c_void_p) for o in outs])
+    lens = (ctypes.c_int32 * gc.nchunks)()
+    r = LIB.ora_cpu_opt_gemm(ctypes.byref(sa), ctypes.byref(sb), ctypes.byref(cg), nthreads, bl[0],
+                             dec[0] if dec else None, ptrs, lens)
+    if r < 0:
+        raise RuntimeError(f"cpu baseline failed ({r})")
+    return [outs[i].raw[:lens[i]] for i in range(gc.nchunks)]

@@ -98,23 +98,29 @@ def _f32_inputs(rng, M, K, N):
     (1000, 1000, 1000, 500, 100),
     (64, 4096, 96, 64, 32),
 ])
-def test_split_f32_bf16x3_error(ia, M, K, N, cs, bs):
-    """float32 split form (3xBF16 on tcgen05, FP32 accumulation): normwise error against
-    the float64 product of the same float32 operands stays at float32 level (the split
-    represents each operand to 2^-17 relative)."""
+def test_split_f32_bf16_error(ia, M, K, N, cs, bs):
+    """float32 split forms on tcgen05 with FP32 accumulation in segments, against the
+    float64 product of the same float32 operands.  Six products (three bf16 words per
+    operand, the default): float32 accuracy, within 2x the FFMA path's error.  Three
+    products (two words, 3xBF16): the split holds each operand to about 2^-17 relative,
+    so the error sits near 4e-6 whatever the accumulation."""
     rng = np.random.default_rng(4 + M + K + N)
     A, B = _f32_inputs(rng, M, K, N)
     sctx, nctx = _split_ctx(ia), ia.Context()
     Ac = ia.Container.from_numpy(nctx, A, (cs, cs), (bs, bs))
     Bc = ia.Container.from_numpy(nctx, B, (cs, cs), (bs, bs))
     cn = ia.opt_gemm(nctx, Ac, Bc, (cs, cs), (bs, bs)).to_numpy()
-    cs_ = ia.opt_gemm(sctx, Ac, Bc, (cs, cs), (bs, bs)).to_numpy()
+    cs6 = ia.opt_gemm(sctx, Ac, Bc, (cs, cs), (bs, bs)).to_numpy()
+    sctx.set_split_products_f32(3)
+    cs3 = ia.opt_gemm(sctx, Ac, Bc, (cs, cs), (bs, bs)).to_numpy()
     exact = A.astype(np.float64) @ B.astype(np.float64)
     nrm = np.linalg.norm(exact)
     en = np.linalg.norm(cn - exact) / nrm
-    es = np.linalg.norm(cs_ - exact) / nrm
-    assert es < 5e-5, (es, en)
-    assert np.abs(cs_ - exact).max() <= 1e-4 * np.abs(exact).max() + 1e-6
+    e6 = np.linalg.norm(cs6 - exact) / nrm
+    e3 = np.linalg.norm(cs3 - exact) / nrm
+    assert e6 <= max(2 * en, 5e-7), (e6, en)
+    assert e3 <= 8e-6, (e3, en)
+    assert np.abs(cs6 - exact).max() <= 1e-5 * np.abs(exact).max()
 
 
 def test_split_f32_zero_and_single_tile(ia):
