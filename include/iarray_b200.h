@@ -252,6 +252,12 @@ INA_API(ina_rc_t) iarray_container_save(iarray_context_t *ctx, iarray_container_
 INA_API(ina_rc_t) iarray_container_open(iarray_context_t *ctx, char *urlpath, iarray_container_t **container);
 /* iarray.h:593-595. */
 INA_API(ina_rc_t) iarray_container_load(iarray_context_t *ctx, char *urlpath, iarray_container_t **container);
+/* iarray.h:617 (src/iarray_container.c:219-225): removes a frame file, or a sparse frame's
+ * directory.  A container created with storage->urlpath set and storage->contiguous false
+ * is written as a sparse (directory) frame, c-blosc2's layout: <urlpath>/chunks.b2frame
+ * (header, metalayers and the offsets index, whose entries are chunk file numbers) and one
+ * file <urlpath>/%08X.chunk per chunk; iarray_container_open / _load read either kind. */
+INA_API(ina_rc_t) iarray_container_remove(char *urlpath);
 /* iarray.h:605-609 (src/iarray_container.c:228-260): serialise to a contiguous frame in
  * host memory; *needs_free tells the caller to free(*frame). */
 INA_API(ina_rc_t) iarray_to_cframe(iarray_context_t *ctx, iarray_container_t *src, uint8_t **frame,

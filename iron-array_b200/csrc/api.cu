@@ -9,10 +9,13 @@
 // kernel over the whole matrices, and re-encodes the result into `storage`'s
 // partition.  Calls are synchronous on one internal CUDA stream per context.
 #include <cuda_runtime.h>
+#include <dirent.h>
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <map>
@@ -23,6 +26,7 @@
 #include "../../include/iarray_b200.h"
 #include "common.cuh"
 #include "frame.h"
+#include "zskip.cuh"
 
 using iab::DevBuf;
 using iab::Geom;
@@ -269,7 +273,8 @@ INA_API(ina_rc_t) iarray_context_new(iarray_config_t *cfg, iarray_context_t **ct
     if (!g_initialized) return rc_err(INA_ERR_NOT_INITIALIZED);
     if (cfg->compression_codec != IARRAY_COMPRESSION_LZ4) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
     if (cfg->filter_flags & ~IARRAY_COMP_SHUFFLE) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
-    if (cfg->compression_level <= 0 || cfg->compression_level > 9) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
+    // level 0 stores chunks memcpyed, as c-blosc2 does (src/iarray.c:391-439 passes it on)
+    if (cfg->compression_level < 0 || cfg->compression_level > 9) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
     iarray_context_t *c = new iarray_context_t();
     c->cfg = *cfg;
     c->device = g_device;
@@ -458,7 +463,7 @@ static ina_rc_t encode_into(iarray_context_t *ctx, iarray_container_t *c, const 
     std::vector<int64_t> off;
     std::vector<int32_t> len;
     int r = iab::encode_container(c->geom, dense, ld, c->shuffle, c->splitmode, &out, &off, &len, ctx->stream,
-                                  ctx->encoder == IARRAY_B200_ENCODER_LIBLZ4);
+                                  ctx->encoder == IARRAY_B200_ENCODER_LIBLZ4, c->clevel == 0);
     if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
     if (r != 0) return rc_err(IARRAY_ERR_GPU_FAILED);
     s.buf = std::move(out);
@@ -501,8 +506,10 @@ static ina_rc_t decode_store(iarray_context_t *ctx, const iarray_container_t *c,
 // Decode two stored (non-view) containers on the context's stream with one LZ4 launch for
 // the streams of both (one job queue), then each container's scatter; returns after both
 // finished.
+// zf / nzero (optional): each container's per (chunk, block) zero flags and their count.
 static ina_rc_t decode_pair(iarray_context_t *ctx, const iarray_container_t *a, void *da, int64_t lda,
-                            const iarray_container_t *b, void *db, int64_t ldb)
+                            const iarray_container_t *b, void *db, int64_t ldb, DevBuf *zf = nullptr,
+                            int *nzero = nullptr)
 {
     // the padding columns past each row are left as they are: no product reads them
     const iarray_container_t *x[2] = {a, b};
@@ -522,6 +529,10 @@ static ina_rc_t decode_pair(iarray_context_t *ctx, const iarray_container_t *a, 
     for (int k = 0; k < 2 && !r; k++)
         if (x[k]->geom.nchunks) r = iab::decode_finish(&w[k], ctx->stream);
     if (r) cudaStreamSynchronize(ctx->stream);     // the work buffers go back to the pool idle
+    for (int k = 0; k < 2 && !r; k++) {
+        if (zf) zf[k] = std::move(w[k].zf);
+        if (nzero) nzero[k] = x[k]->geom.nchunks ? w[k].nzero : 0;
+    }
     return decode_rc(r);
 }
 
@@ -933,9 +944,46 @@ static ina_rc_t write_file(const char *path, const std::vector<uint8_t> &f)
     return w == f.size() ? INA_SUCCESS : rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
 }
 
+// Sparse (directory) frame, c-blosc2's layout for storage.contiguous == false: the
+// directory `dir` holds the index frame chunks.b2frame (header and metalayers, no chunk
+// bytes, offsets holding chunk file numbers) and chunk n in the file %08X.chunk (n in
+// upper-case hexadecimal, eight digits).
+static std::string chunk_file(const std::string &dir, int64_t n)
+{
+    char name[32];
+    snprintf(name, sizeof(name), "/%08X.chunk", (unsigned)n);
+    return dir + name;
+}
+
+static ina_rc_t write_sparse(iarray_context_t *ctx, iarray_container_t *c, const std::string &dir)
+{
+    struct stat sb;
+    if (stat(dir.c_str(), &sb) == 0) {
+        if (!S_ISDIR(sb.st_mode)) return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+    } else if (mkdir(dir.c_str(), 0755) != 0) {
+        return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+    }
+    const ChunkStore &s = *c->store;
+    iab::FrameInfo fi = frame_info(ctx, c);
+    fi.sparse = true;
+    std::vector<uint8_t> f = iab::frame_header(fi, s.cbytes, c->geom.nchunks);
+    const std::vector<uint8_t> tail = iab::frame_tail(s.len, true);
+    f.insert(f.end(), tail.begin(), tail.end());
+    ina_rc_t rc = write_file((dir + "/chunks.b2frame").c_str(), f);
+    std::vector<uint8_t> chunk;
+    for (int64_t k = 0; k < c->geom.nchunks && INA_SUCCEED(rc); k++) {
+        chunk.resize((size_t)s.len[k]);
+        if (cudaMemcpy(chunk.data(), s.buf.as<uint8_t>() + s.off[k], chunk.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return rc_err(IARRAY_ERR_GPU_FAILED);
+        rc = write_file(chunk_file(dir, k).c_str(), chunk);
+    }
+    return rc;
+}
+
 static ina_rc_t save_if_urlpath(iarray_context_t *ctx, iarray_container_t *c)
 {
     if (c->urlpath.empty()) return INA_SUCCESS;
+    if (!c->storage.contiguous) return write_sparse(ctx, c, c->urlpath);
     std::vector<uint8_t> f;
     ina_rc_t rc = to_frame(ctx, c, &f);
     if (INA_FAILED(rc)) return rc;
@@ -953,21 +1001,98 @@ INA_API(ina_rc_t) iarray_container_save(iarray_context_t *ctx, iarray_container_
     return write_file(urlpath, f);
 }
 
-static ina_rc_t load_file(iarray_context_t *ctx, char *urlpath, iarray_container_t **container, bool keep_path)
+static bool read_file(const std::string &path, std::vector<uint8_t> *f)
 {
-    CHECK_ARG(ctx && urlpath && container);
-    FILE *fp = fopen(urlpath, "rb");
-    if (!fp) return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+    FILE *fp = fopen(path.c_str(), "rb");
+    if (!fp) return false;
     fseek(fp, 0, SEEK_END);
     const long n = ftell(fp);
     fseek(fp, 0, SEEK_SET);
-    std::vector<uint8_t> f((size_t)std::max(n, 0L));
-    const size_t r = n > 0 ? fread(f.data(), 1, (size_t)n, fp) : 0;
+    f->resize((size_t)std::max(n, 0L));
+    const size_t r = n > 0 ? fread(f->data(), 1, (size_t)n, fp) : 0;
     fclose(fp);
-    if (n <= 0 || r != (size_t)n) return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
-    ina_rc_t rc = iarray_from_cframe(ctx, f.data(), (int64_t)f.size(), true, container);
+    return n > 0 && r == (size_t)n;
+}
+
+// Open a sparse (directory) frame: its index frame, then every chunk file it names.
+static ina_rc_t load_sparse(iarray_context_t *ctx, const std::string &dir, iarray_container_t **container)
+{
+    std::vector<uint8_t> f;
+    if (!read_file(dir + "/chunks.b2frame", &f)) return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+    iab::FrameInfo fi;
+    std::vector<std::pair<int64_t, int32_t>> index;
+    std::string why;
+    if (!iab::read_frame(f.data(), f.size(), &fi, &index, &why) || !fi.sparse)
+        return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+    std::vector<std::vector<uint8_t>> chunks(index.size());
+    std::vector<const uint8_t *> ptrs;
+    std::vector<int64_t> lens;
+    for (size_t k = 0; k < index.size(); k++) {
+        if (!read_file(chunk_file(dir, index[k].first), &chunks[k]) || chunks[k].size() < 32)
+            return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+        ptrs.push_back(chunks[k].data());
+        lens.push_back((int64_t)chunks[k].size());
+    }
+    iarray_dtshape_t d;
+    memset(&d, 0, sizeof(d));
+    d.dtype = (iarray_data_type_t)fi.dtype;
+    d.ndim = (int8_t)fi.ndim;
+    iarray_storage_t st;
+    memset(&st, 0, sizeof(st));
+    st.contiguous = false;
+    for (int i = 0; i < fi.ndim; i++) { d.shape[i] = fi.shape[i]; st.chunkshape[i] = fi.chunk[i]; st.blockshape[i] = fi.block[i]; }
+    ina_rc_t rc = new_container(ctx, &d, &st, container);
+    if (INA_FAILED(rc)) return rc;
+    iarray_container_t *c = *container;
+    if (fi.typesize != c->geom.itemsize || fi.chunksize != c->geom.chunk_nbytes ||
+        (int64_t)index.size() != c->geom.nchunks) {
+        iarray_container_free(ctx, container);
+        return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+    }
+    c->shuffle = fi.shuffle;
+    c->clevel = fi.clevel;
+    rc = upload_chunks(ctx, c, ptrs.data(), lens.data());
+    if (INA_FAILED(rc)) iarray_container_free(ctx, container);
+    return rc;
+}
+
+static ina_rc_t load_file(iarray_context_t *ctx, char *urlpath, iarray_container_t **container, bool keep_path)
+{
+    CHECK_ARG(ctx && urlpath && container);
+    struct stat sb;
+    if (stat(urlpath, &sb) != 0) return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+    ina_rc_t rc;
+    if (S_ISDIR(sb.st_mode)) {
+        rc = load_sparse(ctx, urlpath, container);
+    } else {
+        std::vector<uint8_t> f;
+        if (!read_file(urlpath, &f)) return rc_err(IARRAY_ERR_PERSISTENCY_FAILED);
+        rc = iarray_from_cframe(ctx, f.data(), (int64_t)f.size(), true, container);
+        if (INA_SUCCEED(rc)) (*container)->storage.contiguous = true;
+    }
     if (INA_SUCCEED(rc) && keep_path) (*container)->urlpath = urlpath;
     return rc;
+}
+
+// iarray.h:617 (src/iarray_container.c:219-225, blosc2_remove_urlpath): removes a
+// contiguous frame file, or a sparse frame's directory with its index and chunk files.
+INA_API(ina_rc_t) iarray_container_remove(char *urlpath)
+{
+    CHECK_ARG(urlpath);
+    struct stat sb;
+    if (stat(urlpath, &sb) != 0) return rc_err(IARRAY_ERR_BLOSC_FAILED);
+    if (!S_ISDIR(sb.st_mode)) return unlink(urlpath) == 0 ? INA_SUCCESS : rc_err(IARRAY_ERR_BLOSC_FAILED);
+    DIR *dp = opendir(urlpath);
+    if (!dp) return rc_err(IARRAY_ERR_BLOSC_FAILED);
+    bool ok = true;
+    for (struct dirent *e = readdir(dp); e; e = readdir(dp)) {
+        const std::string n = e->d_name;
+        const bool chunk = n.size() == 14 && n.compare(8, 6, ".chunk") == 0;
+        if (chunk || n == "chunks.b2frame") ok &= unlink((std::string(urlpath) + "/" + n).c_str()) == 0;
+    }
+    closedir(dp);
+    ok &= rmdir(urlpath) == 0;
+    return ok ? INA_SUCCESS : rc_err(IARRAY_ERR_BLOSC_FAILED);
 }
 
 INA_API(ina_rc_t) iarray_container_open(iarray_context_t *ctx, char *urlpath, iarray_container_t **container)
@@ -1015,21 +1140,23 @@ struct Timer {
 };
 
 // Run the product on dense device operands with the context's form.
+// zs (optional): leave out the K ranges of zero-block pairs in the float64 products.
 static ina_rc_t dense_product(iarray_context_t *ctx, int dtype, int64_t M, int64_t N, int64_t K, const void *A,
-                              int64_t lda, const void *B, int64_t ldb, void *C, int64_t ldc)
+                              int64_t lda, const void *B, int64_t ldb, void *C, int64_t ldc,
+                              const iab::ZeroSkip *zs = nullptr)
 {
     if (ctx->form == IARRAY_B200_FORM_SPLIT) {
         int r;
         if (dtype == IARRAY_DATA_TYPE_DOUBLE)
             r = iab::gemm_f64_ozaki(M, N, K, (const double *)A, lda, (const double *)B, ldb, (double *)C, ldc,
-                                    ctx->split_terms, ctx->stream);
+                                    ctx->split_terms, ctx->stream, zs);
         else
             r = iab::gemm_f32_bf16_split(M, N, K, (const float *)A, lda, (const float *)B, ldb, (float *)C, ldc,
                                          ctx->split_products_f32, ctx->stream);
         if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
         if (r != 0) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
     } else if (dtype == IARRAY_DATA_TYPE_DOUBLE) {
-        iab::gemm_f64_native(M, N, K, (const double *)A, lda, (const double *)B, ldb, (double *)C, ldc, ctx->stream);
+        iab::gemm_f64_native(M, N, K, (const double *)A, lda, (const double *)B, ldb, (double *)C, ldc, ctx->stream, zs);
     } else {
         iab::gemm_f32_native(M, N, K, (const float *)A, lda, (const float *)B, ldb, (float *)C, ldc, ctx->stream);
     }
@@ -1049,7 +1176,55 @@ INA_API(ina_rc_t) iarray_b200_dense_gemm(iarray_context_t *ctx, int dtype, int64
 }
 
 // Decode -> product -> encode into the already-created container c.
-static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b, iarray_container_t *c)
+// Zero-block rule of the entry point (which operands' special-zero chunks are skipped
+// besides zero blocks): none for the panel products (src/linalg/matmul/gemm.c, gemv.c
+// multiply whole panels), both for iarray_opt_gemm and iarray_opt_gemv
+// (src/linalg/iarray_gemm.c:146-168, iarray_gemv.c:131-150), B's only for
+// iarray_opt_gemm_a (iarray_gemm_a.c:127-146: A's blocks come from block_is_zeros alone),
+// A's only for iarray_opt_gemm_b (iarray_gemm_b.c:127-146).
+enum SkipRule { SKIP_NONE = 0, SKIP_BOTH, SKIP_B_CHUNKS, SKIP_A_CHUNKS };
+
+// The zero-block rule around a product of decoded operands: flag grids from the decoders'
+// per-block flags, and (after the product) the recomputation of output blocks whose
+// skipped pairs face a NaN or an infinity.
+struct ZeroRule {
+    DevBuf za, zb, nfa, nfb;
+    iab::ZeroSkip zs;
+    bool on = false;
+    bool build(iarray_context_t *ctx, const Geom &ga, const Geom &gb, bool vec, const DevBuf *zf, int rule)
+    {
+        const int64_t RB = ga.cgrid[0] * ga.bgrid[0], KB = ga.cgrid[1] * ga.bgrid[1];
+        const int64_t JB = vec ? 1 : gb.cgrid[1] * gb.bgrid[1];
+        if (RB * KB == 0 || KB * JB == 0) return true;
+        if (!za.allocate((size_t)(RB * KB), ctx->device) || !zb.allocate((size_t)(KB * JB), ctx->device) ||
+            !nfa.allocate((size_t)(RB * KB), ctx->device) || !nfb.allocate((size_t)(KB * JB), ctx->device))
+            return false;
+        iab::zero_grid(ga, zf[0].as<uint8_t>(), rule == SKIP_BOTH || rule == SKIP_A_CHUNKS, za.as<uint8_t>(), ctx->stream);
+        iab::zero_grid(gb, zf[1].as<uint8_t>(), rule == SKIP_BOTH || rule == SKIP_B_CHUNKS, zb.as<uint8_t>(), ctx->stream);
+        zs = iab::ZeroSkip{za.as<uint8_t>(), zb.as<uint8_t>(),
+                           ga.chunk[0], ga.block[0], ga.bgrid[0],
+                           ga.chunk[1], ga.block[1], ga.bgrid[1],
+                           vec ? 1 : gb.chunk[1], vec ? 1 : gb.block[1], vec ? 1 : gb.bgrid[1],
+                           RB, KB, JB};
+        on = true;
+        return true;
+    }
+    void fix(iarray_context_t *ctx, int isz, int64_t M, int64_t N, int64_t K, const void *A, int64_t lda, const void *B,
+             int64_t ldb, void *C, int64_t ldc)
+    {
+        if (!on) return;
+        cudaMemsetAsync(nfa.p, 0, nfa.n, ctx->stream);
+        cudaMemsetAsync(nfb.p, 0, nfb.n, ctx->stream);
+        iab::block_nonfinite(isz, M, K, A, lda, zs.r_chunk, zs.r_block, zs.r_bg, zs.k_chunk, zs.k_block, zs.k_bg, zs.KB,
+                             nfa.as<uint8_t>(), ctx->stream);
+        iab::block_nonfinite(isz, K, N, B, ldb, zs.k_chunk, zs.k_block, zs.k_bg, zs.c_chunk, zs.c_block, zs.c_bg, zs.JB,
+                             nfb.as<uint8_t>(), ctx->stream);
+        iab::zero_fix(isz, M, N, K, A, lda, B, ldb, C, ldc, zs, nfa.as<uint8_t>(), nfb.as<uint8_t>(), ctx->stream);
+    }
+};
+
+static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b, iarray_container_t *c,
+                           int skip = SKIP_NONE)
 {
     const int dtype = a->dtshape.dtype;
     const int isz = a->geom.itemsize;
@@ -1065,10 +1240,16 @@ static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_
         return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
     if (vec) cudaMemsetAsync(dB.p, 0, (size_t)(pad_ld(K) * isz), ctx->stream);
     ina_rc_t rc;
+    ZeroRule zr;
     if (!a->transposed && !b->transposed) {
         // both operands at once: one LZ4 launch over the streams of A and B
-        rc = decode_pair(ctx, a, dA.p, lda, b, dB.p, vec ? K : ldb);
+        DevBuf zf[2];
+        int nz[2] = {0, 0};
+        rc = decode_pair(ctx, a, dA.p, lda, b, dB.p, vec ? K : ldb, zf, nz);
         if (INA_FAILED(rc)) return rc;
+        if (skip != SKIP_NONE && nz[0] + nz[1] > 0 && K > 0 &&
+            !zr.build(ctx, a->geom, b->geom, vec, zf, skip))
+            return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
         tm.mark(1);
         tm.mark(2);
     } else {
@@ -1085,9 +1266,14 @@ static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_
         iab::gemv_native(dtype == IARRAY_DATA_TYPE_DOUBLE ? 0 : 1, M, K, dA.p, lda, dB.p, dC.p, ctx->stream);
         rc = cuda_rc(cudaGetLastError());
     } else {
-        rc = dense_product(ctx, dtype, M, N, K, dA.p, lda, dB.p, ldb, dC.p, ldc);
+        rc = dense_product(ctx, dtype, M, N, K, dA.p, lda, dB.p, ldb, dC.p, ldc, zr.on ? &zr.zs : nullptr);
     }
     if (INA_FAILED(rc)) return rc;
+    if (zr.on) {
+        zr.fix(ctx, isz, M, N, K, dA.p, lda, dB.p, vec ? 1 : ldb, dC.p, vec ? 1 : ldc);
+        rc = cuda_rc(cudaGetLastError());
+        if (INA_FAILED(rc)) return rc;
+    }
     tm.mark(3);
     // dA and dB stay allocated until the encode below has synchronised the stream: the pool is
     // shared by every context, so memory released while the product may still read it could be
@@ -1184,7 +1370,7 @@ INA_API(ina_rc_t) iarray_opt_gemm(iarray_context_t *ctx, iarray_container_t *a, 
         return rc_err(IARRAY_ERR_INVALID_BLOCKSHAPE);
     rc = output_container(ctx, a, b, storage, c);
     if (INA_FAILED(rc)) return rc;
-    rc = run_matmul(ctx, a, b, *c);
+    rc = run_matmul(ctx, a, b, *c, SKIP_BOTH);
     if (INA_FAILED(rc)) iarray_container_free(ctx, c);
     return rc;
 }
@@ -1216,7 +1402,7 @@ static ina_rc_t opt_gemm_ab(iarray_context_t *ctx, iarray_container_t *a, iarray
     }
     rc = output_container(ctx, a, b, storage, c);
     if (INA_FAILED(rc)) return rc;
-    rc = run_matmul(ctx, a, b, *c);
+    rc = run_matmul(ctx, a, b, *c, swap ? SKIP_A_CHUNKS : SKIP_B_CHUNKS);
     if (INA_FAILED(rc)) iarray_container_free(ctx, c);
     return rc;
 }
@@ -1249,7 +1435,7 @@ INA_API(ina_rc_t) iarray_opt_gemv(iarray_context_t *ctx, iarray_container_t *a, 
     if (ab[0] != storage->blockshape[0] || ab[1] != bb[0]) return rc_err(IARRAY_ERR_INVALID_BLOCKSHAPE);
     rc = output_container(ctx, a, b, storage, c);
     if (INA_FAILED(rc)) return rc;
-    rc = run_matmul(ctx, a, b, *c);
+    rc = run_matmul(ctx, a, b, *c, SKIP_BOTH);
     if (INA_FAILED(rc)) iarray_container_free(ctx, c);
     return rc;
 }
@@ -1524,6 +1710,7 @@ INA_API(ina_rc_t) iarray_b200_opt_gemm_cframes(iarray_context_t *ctx, const uint
         const Geom gk = row_geom(gc, k);
         iab::EncodeWork &w = enc[(size_t)k];
         w.exact_lz4 = ctx->encoder == IARRAY_B200_ENCODER_LIBLZ4;
+        w.memcpy_only = cc->clevel == 0;
         err = iab::encode_launch(gk, c_k, ldc, cc->shuffle, cc->splitmode, &cbuf[(size_t)k], &w, se);
         if (err) break;
         // the chunk table goes to the host on its own stream: a device-to-host copy queued on
@@ -1743,6 +1930,7 @@ int batch_enqueue(iarray_b200_batch_t *bt, int parts)
                 if (!pass) {
                     w.ext_chunks = bt->chunks.as<iab::EncChunk>() + bt->chunk_base[(size_t)i];
                     w.exact_lz4 = exact;
+                    w.memcpy_only = bt->ctx->cfg.compression_level == 0;
                     w.ext_img = bt->eimg.as<uint8_t>() + io;
                     w.ext_slots = bt->eslots.as<uint8_t>() + io;
                     w.ext_es = bt->ees.as<iab::EncStream>() + so;
@@ -1766,6 +1954,7 @@ int batch_enqueue(iarray_b200_batch_t *bt, int parts)
         if (!g.nchunks) continue;
         bt->enc[(size_t)i].ext_chunks = bt->chunks.as<iab::EncChunk>() + bt->chunk_base[(size_t)i];
         bt->enc[(size_t)i].exact_lz4 = exact;
+        bt->enc[(size_t)i].memcpy_only = bt->ctx->cfg.compression_level == 0;
         const int r = iab::encode_launch(g, bt->dC[(size_t)i].p, bt->ldc[(size_t)i], true, IARRAY_AUTO_SPLIT,
                                          &bt->cbuf[(size_t)i], &bt->enc[(size_t)i], bt->br[(size_t)i % nbr]);
         if (r) { batch_join(bt); return r; }

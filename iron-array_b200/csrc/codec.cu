@@ -43,9 +43,14 @@ __device__ __forceinline__ void dev_fail(int *err, int code) { atomicCAS(err, 0,
 
 // ============================================================================ decode
 // D0: parse one (chunk, block) per thread.
+// zf (optional): per (chunk, block) zero flags of the reference's block-pair products:
+// bit 0 = block_is_zeros (src/linalg/iarray_gemm.c:28-77: no memcpyed or special chunk, and
+// the first typesize csize words from the block's bstart are all 0: Blosc2 v5 chunks always
+// carry the flag bit the reference reads as "split"), bit 1 = chunk_is_zeros (:17-26:
+// special value ZERO); nzero counts the flagged blocks.
 __global__ void k_parse(Geom g, const uint8_t *__restrict__ ch, const int64_t *__restrict__ off,
                         const int32_t *__restrict__ len, BlockDesc *bd, StreamDesc *sd, Lz4Job *jobs,
-                        int *njobs, int64_t jcap, int *err, uint8_t *scratch)
+                        int *njobs, int64_t jcap, int *err, uint8_t *scratch, uint8_t *zf, int *nzero)
 {
     const int64_t total = g.nchunks * g.nblocks;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
@@ -65,8 +70,19 @@ __global__ void k_parse(Geom g, const uint8_t *__restrict__ ch, const int64_t *_
             nbytes = ld_s32(p + 4); bsz = ld_s32(p + 8); cbytes = ld_s32(p + 12);
             ok = (flags & 0x05) == 0x05 && nbytes == g.chunk_nbytes && cbytes >= 32 && cbytes <= clen;
         }
-        if (!ok) { dev_fail(err, DE_HEADER); bd[t] = d; continue; }
+        if (!ok) { dev_fail(err, DE_HEADER); bd[t] = d; if (zf) zf[t] = 0; continue; }
         const int special = (bflags >> 4) & 7;
+        if (zf) {
+            uint8_t zflag = special == 1 ? 2 : 0;
+            if (!special && !(flags & 0x02) && 32 + 4 * (b + 1) <= cbytes) {
+                const int64_t q0 = ld_s32(p + 32 + 4 * b);
+                bool z = q0 >= 32 && q0 + 4 * (int64_t)ts <= cbytes;
+                for (int j = 0; z && j < ts; j++) z = ld_s32(p + q0 + 4 * j) == 0;
+                if (z) zflag |= 1;
+            }
+            zf[t] = zflag;
+            if (zflag && nzero) atomicAdd(nzero, 1);
+        }
         if (special) {
             if (special == 2) d.mode = BM_NAN;
             else if (special == 3) {
@@ -1756,13 +1772,19 @@ __device__ __forceinline__ bool layout_step(EncStream &e, int64_t &ntb, int64_t 
     return true;
 }
 
-__global__ void __launch_bounds__(LAYOUT_T) k_layout(Geom g, int nstreams, int neblock, EncStream *es, EncChunk *ec)
+// memcpy_only (compression level 0): c-blosc2 stores every chunk memcpyed.
+__global__ void __launch_bounds__(LAYOUT_T) k_layout(Geom g, int nstreams, int neblock, EncStream *es, EncChunk *ec,
+                                                    int memcpy_only)
 {
     __shared__ int64_t wsum[LAYOUT_T / 32];
     __shared__ int64_t s_before;
     __shared__ int s_first;
     const int64_t c = blockIdx.x;
     const int64_t destsize = g.chunk_nbytes + 32, ns = g.nblocks * nstreams;
+    if (memcpy_only) {
+        if (threadIdx.x == 0) { ec[c].memcpyed = 1; ec[c].cbytes = (int32_t)destsize; }
+        return;
+    }
     const int64_t ntb0 = 32 + 4 * g.nblocks;
     EncStream *e0 = es + c * ns;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1967,11 +1989,12 @@ int decode_container(const Geom &g, const uint8_t *d_chunks, int64_t chunks_byte
 
 int decode_finish(DecodeWork *w, cudaStream_t st)
 {
-    int h_err = 0;
+    int h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     const int *cnt = w->ext_counters ? w->ext_counters : w->counters.as<int>();
-    cudaMemcpyAsync(&h_err, cnt + 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return -101;
-    return h_err;
+    w->nzero = h[4];
+    return h[1];
 }
 
 // Grid of the fast scatter: the CTAs resident at once (one wave), at most one per slice.
@@ -2017,9 +2040,10 @@ int decode_parse(const DecodeArgs &a, DecodeQueue *q, DecodeWork *w, cudaStream_
     cudaMemsetAsync(cnt, 0, 64, st);
     const int threads = 128;
     const int64_t blocks = std::min<int64_t>((nbl + threads - 1) / threads, (int64_t)sm_count() * 16);
+    if (!w->zf.allocate((size_t)std::max<int64_t>(nbl, 1), dev)) return -100;
     IAB_TIMED("k_parse", st, k_parse<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, st>>>(
         g, a.chunks, a.off, a.len, w->bd.as<BlockDesc>(), w->sd.as<StreamDesc>(), q->jobs.as<Lz4Job>(),
-        q->counters.as<int>(), q->cap, cnt + 1, w->scratch.as<uint8_t>()));
+        q->counters.as<int>(), q->cap, cnt + 1, w->scratch.as<uint8_t>(), w->zf.as<uint8_t>(), cnt + 4));
     return 0;
 }
 
@@ -2173,7 +2197,8 @@ int encode_emit(const Geom &g, bool shuffle, int splitmode, DevBuf *d_out, Encod
     const uint8_t *slots = ext ? w->ext_slots : w->slots.as<uint8_t>();
     EncStream *es = ext ? w->ext_es : w->es.as<EncStream>();
     EncChunk *ec = w->ext_chunks ? w->ext_chunks : w->ec.as<EncChunk>();
-    IAB_TIMED("k_layout", st, k_layout<<<(unsigned)std::max<int64_t>(g.nchunks, 1), LAYOUT_T, 0, st>>>(g, nstreams, neblock, es, ec));
+    IAB_TIMED("k_layout", st, k_layout<<<(unsigned)std::max<int64_t>(g.nchunks, 1), LAYOUT_T, 0, st>>>(
+        g, nstreams, neblock, es, ec, w->memcpy_only ? 1 : 0));
     IAB_TIMED("k_chunk_offsets", st, k_chunk_offsets<<<1, 1024, 0, st>>>(g.nchunks, ec, w->tot.as<int64_t>()));
     const int64_t blocks = std::min<int64_t>(nbl, (int64_t)sm_count() * 8);
     IAB_TIMED("k_emit", st, k_emit<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
@@ -2191,9 +2216,10 @@ int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int s
     const int r = encode_gather(g, in, ld, shuffle, splitmode, w, st);
     if (r) return r;
     const int nstreams = encode_nstreams(g, shuffle, splitmode);
-    encode_streams(w->img.as<uint8_t>(), g.nchunks * g.nblocks * nstreams, (int)(g.blocksize / nstreams),
-                   w->slots.as<uint8_t>(), w->es.as<EncStream>(),
-                   reinterpret_cast<unsigned long long *>(w->tot.as<int64_t>() + 1), w->exact_lz4, st);
+    if (!w->memcpy_only)
+        encode_streams(w->img.as<uint8_t>(), g.nchunks * g.nblocks * nstreams, (int)(g.blocksize / nstreams),
+                       w->slots.as<uint8_t>(), w->es.as<EncStream>(),
+                       reinterpret_cast<unsigned long long *>(w->tot.as<int64_t>() + 1), w->exact_lz4, st);
     return encode_emit(g, shuffle, splitmode, d_out, w, st);
 }
 
@@ -2211,10 +2237,12 @@ int encode_finish(EncodeWork *w, std::vector<int64_t> *h_off, std::vector<int32_
 }
 
 int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, DevBuf *d_out,
-                     std::vector<int64_t> *h_off, std::vector<int32_t> *h_len, cudaStream_t st, bool exact_lz4)
+                     std::vector<int64_t> *h_off, std::vector<int32_t> *h_len, cudaStream_t st, bool exact_lz4,
+                     bool memcpy_only)
 {
     EncodeWork w;
     w.exact_lz4 = exact_lz4;
+    w.memcpy_only = memcpy_only;
     const int r = encode_launch(g, in, ld, shuffle, splitmode, d_out, &w, st);
     if (r) return r;
     return encode_finish(&w, h_off, h_len, st);
@@ -2308,7 +2336,8 @@ int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes,
         const int threads = 128;
         const int64_t blocks = std::min<int64_t>((nbl + threads - 1) / threads, (int64_t)sms * 16);
         IAB_TIMED("k_parse", st, k_parse<<<(unsigned)std::max<int64_t>(blocks, 1), threads, 0, st>>>(g, d_chunks, off, len, bd, sd, jobs, njobs,
-                                                                                      8 * NA_MAX_BLOCKS, err, img));
+                                                                                      8 * NA_MAX_BLOCKS, err, img,
+                                                                                      nullptr, nullptr));
     }
     {
         IAB_TIMED("k_lz4_decode_cta", st, k_lz4_decode_cta<<<sms * 6, dcta::THREADS, (int)sizeof(dcta::Smem), st>>>(

@@ -31,6 +31,8 @@ struct Geom {
 static inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 static inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
 
+struct ZeroSkip;   // zskip.cuh
+
 // Builds the geometry; returns false when the partition is invalid.
 bool make_geom(int ndim, const int64_t *shape, const int64_t *chunk, const int64_t *block,
                int itemsize, Geom *g);
@@ -168,8 +170,10 @@ struct DecodeQueue {
 // *w until decode_finish, which synchronises `st` and returns the DevErr).
 struct DecodeWork {
     DevBuf bd, sd, scratch, counters, rest;
+    DevBuf zf;                     // per (chunk, block) zero flags of the block-pair products (k_parse)
     DecodeQueue queue;             // the job queue of decode_launch (unused by decode_parse / _scatter)
     int *ext_counters = nullptr;   // optional caller-owned 16-int status slot (device) instead of `counters`
+    int nzero = 0;                 // flagged blocks, read back by decode_finish
 };
 int decode_launch(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes, const int64_t *d_off, const int32_t *d_len,
                   void *out, int64_t ld, cudaStream_t st, DecodeWork *w);
@@ -206,14 +210,16 @@ int decode_noalloc(const Geom &g, const uint8_t *d_chunks, int64_t chunks_bytes,
 // chunks back-to-back, h_off / h_len (host) their offsets and lengths.
 // exact_lz4: streams byte-identical to liblz4 1.9.4 LZ4_compress_fast(acceleration 1); else
 // the parallel-parse encoder (valid LZ4, different bytes).
+// memcpy_only: compression level 0, every chunk stored memcpyed.
 int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode,
                      DevBuf *d_out, std::vector<int64_t> *h_off, std::vector<int32_t> *h_len,
-                     cudaStream_t st, bool exact_lz4);
+                     cudaStream_t st, bool exact_lz4, bool memcpy_only = false);
 // Asynchronous form: encode_launch enqueues the kernels (no host synchronisation; work
 // buffers held in *w), encode_finish synchronises and reads the chunk table.
 struct EncodeWork {
     DevBuf img, slots, es, ec, tot;
     bool exact_lz4 = true;            // liblz4-identical streams (see encode_container)
+    bool memcpy_only = false;         // compression level 0: every chunk stored memcpyed (c-blosc2's clevel 0)
     EncChunk *ext_chunks = nullptr;   // optional caller-owned chunk table (device) instead of `ec`
     // optional caller-owned byte-plane image, LZ4 output slots and stream results (device)
     // instead of img / slots / es: slices of buffers shared by several containers
@@ -237,8 +243,10 @@ int encode_emit(const Geom &g, bool shuffle, int splitmode, DevBuf *d_out, Encod
 int encode_finish(EncodeWork *w, std::vector<int64_t> *h_off, std::vector<int32_t> *h_len, cudaStream_t st);
 
 // Dense products (row-major, leading dimensions in items).
+// zs (optional): leave out the K ranges of zero-block pairs (zskip.cuh)
 void gemm_f64_native(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda,
-                     const double *B, int64_t ldb, double *C, int64_t ldc, cudaStream_t st);
+                     const double *B, int64_t ldb, double *C, int64_t ldc, cudaStream_t st,
+                     const ZeroSkip *zs = nullptr);
 void gemm_f32_native(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda,
                      const float *B, int64_t ldb, float *C, int64_t ldc, cudaStream_t st);
 void gemv_native(int dtype, int64_t M, int64_t K, const void *A, int64_t lda, const void *x,
@@ -259,7 +267,8 @@ void gemm_f64_grouped(int cfg, const GemmProblem *d_probs, int nprob, int total_
 
 // Split-precision forms; return 0 on success, < 0 when unsupported on this device.
 int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda,
-                   const double *B, int64_t ldb, double *C, int64_t ldc, int nterms, cudaStream_t st);
+                   const double *B, int64_t ldb, double *C, int64_t ldc, int nterms, cudaStream_t st,
+                   const ZeroSkip *zs = nullptr);
 // Asynchronous form with caller-owned work buffers (no host synchronisation until finish).
 // The B side (column scaling, residues, tensor map) is prepared once and can serve several
 // row bands of A (gemm_f64_ozaki_rows), each with its own OzakiWork.
@@ -274,6 +283,7 @@ struct OzakiB {
 };
 struct OzakiWork {
     DevBuf ra, rr, sa, err;
+    const ZeroSkip *zs = nullptr;          // optional: leave out zero-block pairs (zskip.cuh)
     alignas(64) unsigned char tmA[128];   // CUtensorMap of the residues of A (rows_prep -> rows_product)
     OzakiB b;                              // used by gemm_f64_ozaki_launch
 };
@@ -295,6 +305,14 @@ int gemm_f64_ozaki_finish(OzakiWork *w, cudaStream_t st);
 // products (3: two words; 6: three words; 0: 6) summed in FP32 segments.
 int gemm_f32_bf16_split(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda,
                         const float *B, int64_t ldb, float *C, int64_t ldc, int products, cudaStream_t st);
+
+// Zero-block rule of the block-pair products (zero.cu, zskip.cuh).
+void zero_grid(const Geom &g, const uint8_t *zf, bool use_chunk, uint8_t *grid, cudaStream_t st);
+void block_nonfinite(int itemsize, int64_t rows, int64_t cols, const void *x, int64_t ld, int64_t r_chunk,
+                     int64_t r_block, int64_t r_bg, int64_t c_chunk, int64_t c_block, int64_t c_bg, int64_t CB,
+                     uint8_t *flags, cudaStream_t st);
+void zero_fix(int itemsize, int64_t M, int64_t N, int64_t K, const void *A, int64_t lda, const void *B, int64_t ldb,
+              void *C, int64_t ldc, const ZeroSkip &z, const uint8_t *nfa, const uint8_t *nfb, cudaStream_t st);
 
 void fill_arange(int dtype, int64_t M, int64_t N, int64_t ld, double start, double step, void *out,
                  cudaStream_t st);

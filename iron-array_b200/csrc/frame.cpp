@@ -61,11 +61,11 @@ std::vector<uint8_t> memcpyed_chunk(const uint8_t *data, int32_t nbytes, int typ
 static const uint8_t kTrailer[35] = {0x94, 0x01, 0x93, 0xcd, 0x00, 0x06, 0xde, 0x00, 0x00, 0xdc, 0x00, 0x00,
                                      0xce, 0x00, 0x00, 0x00, 0x23, 0xd8, 0x00};
 
-std::vector<uint8_t> frame_tail(const std::vector<int32_t> &lens)
+std::vector<uint8_t> frame_tail(const std::vector<int32_t> &lens, bool sparse)
 {
     std::vector<int64_t> offsets;
     int64_t acc = 0;
-    for (int32_t l : lens) { offsets.push_back(acc); acc += l; }
+    for (int32_t l : lens) { offsets.push_back(sparse ? (int64_t)offsets.size() : acc); acc += l; }
     std::vector<uint8_t> t = memcpyed_chunk(reinterpret_cast<const uint8_t *>(offsets.data()),
                                             (int32_t)(offsets.size() * 8), 8);
     // trailer: [version, [vlmeta index size, {}, []], trailer length, fingerprint]
@@ -86,7 +86,7 @@ std::vector<uint8_t> frame_header(const FrameInfo &fi, int64_t data_cbytes, int6
     h.push_back(0xcf); put_be(h, 0, 8);                 // frame size, patched below
     h.push_back(0xa4);
     h.push_back(0x12);                                  // frame format 2, 64-bit offsets
-    h.push_back(0x00);
+    h.push_back(fi.sparse ? 0x01 : 0x00);               // frame type: contiguous / directory
     h.push_back((uint8_t)((fi.clevel << 4) | (fi.codec & 0x0f)));
     h.push_back(0x00);
     h.push_back(0xd3); put_be(h, (uint64_t)fi.nbytes, 8);
@@ -130,7 +130,8 @@ std::vector<uint8_t> frame_header(const FrameInfo &fi, int64_t data_cbytes, int6
     }
     const uint32_t header_size = (uint32_t)h.size();
     for (int k = 0; k < 4; k++) h[11 + k] = (uint8_t)(header_size >> (8 * (3 - k)));
-    const uint64_t fs = (uint64_t)h.size() + (uint64_t)data_cbytes + 32 + 8 * (uint64_t)nchunks + 35;
+    // a sparse frame's index file holds no chunk bytes
+    const uint64_t fs = (uint64_t)h.size() + (fi.sparse ? 0 : (uint64_t)data_cbytes) + 32 + 8 * (uint64_t)nchunks + 35;
     for (int k = 0; k < 8; k++) h[16 + k] = (uint8_t)(fs >> (8 * (7 - k)));
     return h;
 }
@@ -185,6 +186,8 @@ bool read_frame(const uint8_t *b, size_t n, FrameInfo *fi, std::vector<std::pair
     if (!mp_int(b, n, p, &frame_size)) return fail("frame size");
     if (frame_size > (int64_t)n || header_size > frame_size) return fail("truncated frame");
     if (b[p] != 0xa4) return fail("flags");
+    if (b[p + 2] > 1) return fail("frame type");
+    fi->sparse = b[p + 2] == 1;
     fi->codec = b[p + 3] & 0x0f;
     fi->clevel = b[p + 3] >> 4;
     p += 5;
@@ -253,7 +256,7 @@ bool read_frame(const uint8_t *b, size_t n, FrameInfo *fi, std::vector<std::pair
     if (!have_ia) fi->dtype = fi->typesize == 8 ? 0 : 1;
     const int64_t nchunks = fi->chunksize > 0 ? (fi->nbytes + fi->chunksize - 1) / fi->chunksize : 0;
     size_t pos = (size_t)header_size;
-    for (int64_t c = 0; c < nchunks; c++) {
+    for (int64_t c = 0; c < nchunks && !fi->sparse; c++) {
         if (pos + 32 > n) return fail("chunk past end");
         pos += (size_t)rd_le32(b + pos + 12);
     }
@@ -265,6 +268,11 @@ bool read_frame(const uint8_t *b, size_t n, FrameInfo *fi, std::vector<std::pair
     for (int64_t c = 0; c < nchunks; c++) {
         int64_t off;
         memcpy(&off, oc + 32 + 8 * c, 8);
+        if (fi->sparse) {
+            if (off < 0 || off > 0xFFFFFFFFll) return fail("chunk file number out of range");
+            chunks->emplace_back(off, 0);
+            continue;
+        }
         const size_t s = (size_t)header_size + (size_t)off;
         if (s + 32 > n) return fail("chunk offset out of range");
         const int32_t cb = rd_le32(b + s + 12);

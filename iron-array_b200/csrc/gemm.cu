@@ -18,6 +18,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "zskip.cuh"
 
 namespace iab {
 
@@ -57,18 +58,22 @@ __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], const double (&a)[2]
 }
 
 // One BM x BN tile of C = A B at (m0, n0), 256 threads.  Requires lda, ldb even and
-// 16-byte aligned bases (true for the library's dense buffers).
+// 16-byte aligned bases (true for the library's dense buffers).  With `klist`, only the
+// nk k-tiles it lists (ascending) are multiplied: the others are pairs of zero blocks the
+// block-pair product skips; without it, all k-tiles.
 template <int BM, int BN>
 __device__ __forceinline__ void f64_tile(int M, int N, int K, const double *__restrict__ A, int64_t lda,
                                          const double *__restrict__ B, int64_t ldb, double *__restrict__ C,
-                                         int64_t ldc, int m0, int n0, double *smf64)
+                                         int64_t ldc, int m0, int n0, double *smf64, const uint16_t *klist = nullptr,
+                                         int nk = -1)
 {
     using namespace f64k;
     using G = Cfg<BM, BN>;
     double *sA = smf64, *sB = smf64 + STAGES * G::A_STAGE;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int wm = warp >> 2, wn = warp & 3;
-    const int ktiles = (K + BK - 1) / BK;
+    const int ktiles = klist ? nk : (K + BK - 1) / BK;
+    auto kt_of = [&](int li) { return klist ? (int)klist[li] : li; };
 
     auto load_tile = [&](int kt, int s) {
         const int k0 = kt * BK;
@@ -101,15 +106,15 @@ __device__ __forceinline__ void f64_tile(int M, int N, int K, const double *__re
 
 #pragma unroll
     for (int s = 0; s < STAGES - 1; s++) {
-        if (s < ktiles) load_tile(s, s);
+        if (s < ktiles) load_tile(kt_of(s), s);
         cp_async_commit();
     }
     const int g = lane >> 2, q = lane & 3;
     for (int kt = 0; kt < ktiles; kt++) {
         cp_async_wait<STAGES - 2>();
         __syncthreads();
-        const int nk = kt + STAGES - 1;
-        if (nk < ktiles) load_tile(nk, nk % STAGES);
+        const int nxt = kt + STAGES - 1;
+        if (nxt < ktiles) load_tile(kt_of(nxt), nxt % STAGES);
         cp_async_commit();
         const double *a = sA + (kt % STAGES) * G::A_STAGE + (wm * (BM / 2)) * SA;
         const double *b = sB + (kt % STAGES) * G::B_STAGE + wn * (BN / 4);
@@ -158,16 +163,60 @@ __global__ void __launch_bounds__(256) k_gemm_f64(int M, int N, int K, const dou
     f64_tile<128, 128>(M, N, K, A, lda, B, ldb, C, ldc, blockIdx.y * 128, blockIdx.x * 128, smf64);
 }
 
+// The same product where the K ranges of zero-block pairs are left out: each CTA lists the
+// k-tiles its tile needs (zs_tile_active) in shared memory, compacted by warp ballots, and
+// multiplies only those.  K <= ZS_MAX_K.
+constexpr int ZS_MAX_K = 65536;
+constexpr int ZS_LIST_BYTES = (ZS_MAX_K / f64k::BK) * 3 + 64;    // flags + uint16 list + count
+__global__ void __launch_bounds__(256) k_gemm_f64_skip(int M, int N, int K, const double *__restrict__ A, int64_t lda,
+                                                       const double *__restrict__ B, int64_t ldb, double *__restrict__ C,
+                                                       int64_t ldc, ZeroSkip z)
+{
+    using G = f64k::Cfg<128, 128>;
+    extern __shared__ __align__(16) double smf64[];
+    uint8_t *extra = reinterpret_cast<uint8_t *>(smf64 + f64k::STAGES * (G::A_STAGE + G::B_STAGE));
+    const int ktiles = (K + f64k::BK - 1) / f64k::BK;
+    int *count = reinterpret_cast<int *>(extra);
+    uint16_t *list = reinterpret_cast<uint16_t *>(extra + 16);
+    uint8_t *flag = extra + 16 + 2 * ktiles;
+    const int m0 = blockIdx.y * 128, n0 = blockIdx.x * 128;
+    const int64_t r1 = min(m0 + 128, M), c1 = min(n0 + 128, N);
+    for (int kt = threadIdx.x; kt < ktiles; kt += blockDim.x)
+        flag[kt] = zs_tile_active(z, m0, r1, n0, c1, (int64_t)kt * f64k::BK, min((kt + 1) * f64k::BK, K)) ? 1 : 0;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        int c = 0;
+        for (int base = 0; base < ktiles; base += 32) {
+            const bool f = base + lane < ktiles && flag[base + lane];
+            const unsigned m = __ballot_sync(0xffffffffu, f);
+            if (f) list[c + __popc(m & ((1u << lane) - 1))] = (uint16_t)(base + lane);
+            c += __popc(m);
+        }
+        if (lane == 0) *count = c;
+    }
+    __syncthreads();
+    f64_tile<128, 128>(M, N, K, A, lda, B, ldb, C, ldc, m0, n0, smf64, list, *count);
+}
+
 void gemm_f64_native(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B, int64_t ldb,
-                     double *C, int64_t ldc, cudaStream_t st)
+                     double *C, int64_t ldc, cudaStream_t st, const ZeroSkip *zs)
 {
     using G = f64k::Cfg<128, 128>;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_gemm_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+        cudaFuncSetAttribute(k_gemm_f64_skip, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM + ZS_LIST_BYTES);
         attr = true;
     }
     dim3 grid((unsigned)((N + 127) / 128), (unsigned)((M + 127) / 128));
+    if (zs && K <= ZS_MAX_K) {
+        const int ktiles = (int)((K + f64k::BK - 1) / f64k::BK);
+        const int smem = G::SMEM + 3 * ktiles + 64;
+        IAB_TIMED("k_gemm_f64", st, k_gemm_f64_skip<<<grid, 256, smem, st>>>((int)M, (int)N, (int)K, A, lda, B, ldb, C,
+                                                                           ldc, *zs));
+        return;
+    }
     IAB_TIMED("k_gemm_f64", st, k_gemm_f64<<<grid, 256, G::SMEM, st>>>((int)M, (int)N, (int)K, A, lda, B, ldb, C, ldc));
 }
 

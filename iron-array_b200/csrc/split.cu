@@ -30,6 +30,7 @@
 
 #include "common.cuh"
 #include "tc_common.cuh"
+#include "zskip.cuh"
 
 namespace iab {
 
@@ -421,15 +422,52 @@ __device__ __forceinline__ void tile_of(int local, int tiles_m, int tiles_n, int
 }
 
 struct I8Params {
-    int M, N, Kp, L, tiles_m, tiles_n;
+    int M, N, K, Kp, L, tiles_m, tiles_n;
     uint8_t *R;        // [L][M][ldr] residues of the products
     int64_t ldr;
     int *err;
+    int use_skip;      // leave out the k-tiles of zero-block pairs (zskip.cuh)
+    ZeroSkip zs;
 };
+
+// Bit kt of mask[kt / 32] = k-tile kt of output tile (tm, tn) is needed (some K block in it
+// pairs a non-zero A block under the tile's rows with a non-zero B block under its
+// columns).  Called by a whole warp; K <= 65536 keeps the mask within 16 words.
+__device__ __forceinline__ void i8_kmask(const I8Params &p, int tm, int tn, int ktiles, uint32_t *mask)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t r0 = (int64_t)tm * oz::BM, r1 = min(r0 + oz::BM, (int64_t)p.M);
+    const int64_t c0 = (int64_t)tn * oz::BN, c1 = min(c0 + oz::BN, (int64_t)p.N);
+    for (int w = 0; w < (ktiles + 31) / 32; w++) {
+        const int kt = w * 32 + lane;
+        const bool f = kt < ktiles && zs_tile_active(p.zs, r0, r1, c0, c1, (int64_t)kt * oz::BK,
+                                                      min((int64_t)(kt + 1) * oz::BK, (int64_t)p.K));
+        const uint32_t b = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) mask[w] = b;
+    }
+    __syncwarp();
+}
+
+// Whether output tile (tm, tn) needs any k-tile (whole warp).
+__device__ __forceinline__ bool i8_tile_any(const I8Params &p, int tm, int tn, int ktiles)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t r0 = (int64_t)tm * oz::BM, r1 = min(r0 + oz::BM, (int64_t)p.M);
+    const int64_t c0 = (int64_t)tn * oz::BN, c1 = min(c0 + oz::BN, (int64_t)p.N);
+    for (int w = 0; w < (ktiles + 31) / 32; w++) {
+        const int kt = w * 32 + lane;
+        const bool f = kt < ktiles && zs_tile_active(p.zs, r0, r1, c0, c1, (int64_t)kt * oz::BK,
+                                                      min((int64_t)(kt + 1) * oz::BK, (int64_t)p.K));
+        if (__ballot_sync(0xffffffffu, f)) return true;
+    }
+    return false;
+}
 
 // Persistent, warp-specialised: warp 0 issues TMA loads, warp 1 issues tcgen05.mma into
 // one of two TMEM accumulators (128 x 256 int32 each), warps 2-5 drain the other
-// accumulator: r = C mod m_l in [0, m_l), stored as one byte per entry.
+// accumulator: r = C mod m_l in [0, m_l), stored as one byte per entry.  With use_skip,
+// the k-tiles of zero-block pairs are neither loaded nor multiplied (every role derives the
+// same mask); a tile that needs none is written as zero residues.
 __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_constant__ CUtensorMap tmA,
                                                                 const __grid_constant__ CUtensorMap tmB, I8Params p)
 {
@@ -443,6 +481,8 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
     uint64_t *tempty = tfull + 2;
     uint64_t *drain = tempty + 2;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    uint32_t *pmask = reinterpret_cast<uint32_t *>(smem + STAGES * STAGE_BYTES + 112);   // producer's k-tile mask
+    uint32_t *mmask = pmask + 16;                                                        // MMA issuer's
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
@@ -463,18 +503,21 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
     const uint32_t tmem_base = *tmem_slot;
     const int total = p.L * p.tiles_m * p.tiles_n;
     const int ktiles = p.Kp / BK;
+    auto needed = [&](const uint32_t *mask, int kt) { return !p.use_skip || ((mask[kt >> 5] >> (kt & 31)) & 1u); };
 
     if (warp == 0) {
-        if (lane == 0) {
-            int stage = 0;
-            uint32_t phase = 0;
-            int64_t issued = 0;
-            bool ok = true;
-            for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-                const int l = t / (p.tiles_m * p.tiles_n), rem = t - l * p.tiles_m * p.tiles_n;
-                int tm, tn;
-                tile_of(rem, p.tiles_m, p.tiles_n, tm, tn);
+        int stage = 0;
+        uint32_t phase = 0;
+        int64_t issued = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < total; t += gridDim.x) {      // the whole warp walks the tiles
+            const int l = t / (p.tiles_m * p.tiles_n), rem = t - l * p.tiles_m * p.tiles_n;
+            int tm, tn;
+            tile_of(rem, p.tiles_m, p.tiles_n, tm, tn);
+            if (p.use_skip) i8_kmask(p, tm, tn, ktiles, pmask);
+            if (lane == 0) {
                 for (int kt = 0; kt < ktiles; kt++) {
+                    if (!needed(pmask, kt)) continue;
                     if (!tc::mbar_wait(&empty[stage], phase ^ 1, p.err)) { ok = false; break; }
                     tc::mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
                     tc::tma_load_3d(sA + stage * A_BYTES, &tmA, kt * BK, tm * BM, l, &full[stage]);
@@ -483,37 +526,55 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
                     if (++stage == STAGES) { stage = 0; phase ^= 1; }
                 }
             }
-            // every load issued has landed before the CTA may exit (bounded waits on the
-            // full barriers of the last STAGES loads)
+            if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) break;
+        }
+        // every load issued has landed before the CTA may exit (bounded waits on the
+        // full barriers of the last STAGES loads)
+        if (lane == 0)
             for (int64_t it = issued > STAGES ? issued - STAGES : 0; it < issued; it++)
                 tc::mbar_wait(&full[it % STAGES], (uint32_t)((it / STAGES) & 1), p.err, 1u << 20);
-        }
     } else if (warp == 1) {
-        if (lane == 0) {
-            int stage = 0, acc = 0;
-            uint32_t phase = 0, acc_phase = 0;
-            bool ok = true;
-            for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
-                if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, p.err)) { ok = false; break; }
-                tc::tc_fence_after();
-                const uint32_t dt = tmem_base + (uint32_t)(acc * BN);
-                for (int kt = 0; kt < ktiles; kt++) {
-                    if (!tc::mbar_wait(&full[stage], phase, p.err)) { ok = false; break; }
+        int stage = 0, acc = 0;
+        uint32_t phase = 0, acc_phase = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < total; t += gridDim.x) {
+            const int l = t / (p.tiles_m * p.tiles_n), rem = t - l * p.tiles_m * p.tiles_n;
+            int tm, tn;
+            tile_of(rem, p.tiles_m, p.tiles_n, tm, tn);
+            if (p.use_skip) i8_kmask(p, tm, tn, ktiles, mmask);
+            if (lane == 0) {
+                if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, p.err)) {
+                    ok = false;
+                } else {
                     tc::tc_fence_after();
-                    const uint32_t a0 = tc::smem_addr(sA + stage * A_BYTES), b0 = tc::smem_addr(sB + stage * B_BYTES);
+                    const uint32_t dt = tmem_base + (uint32_t)(acc * BN);
+                    bool any = false;
+                    for (int kt = 0; kt < ktiles; kt++) {
+                        if (!needed(mmask, kt)) continue;
+                        if (!tc::mbar_wait(&full[stage], phase, p.err)) { ok = false; break; }
+                        tc::tc_fence_after();
+                        const uint32_t a0 = tc::smem_addr(sA + stage * A_BYTES), b0 = tc::smem_addr(sB + stage * B_BYTES);
 #pragma unroll
-                    for (int kk = 0; kk < BK / 32; kk++) {
-                        tc::mma_i8(dt, tc::sw128_kmajor_desc(a0 + kk * 32), tc::sw128_kmajor_desc(b0 + kk * 32), IDESC,
-                                   (kt | kk) != 0);
+                        for (int kk = 0; kk < BK / 32; kk++) {
+                            tc::mma_i8(dt, tc::sw128_kmajor_desc(a0 + kk * 32), tc::sw128_kmajor_desc(b0 + kk * 32),
+                                       IDESC, (any || kk != 0) ? 1u : 0u);
+                        }
+                        any = true;
+                        tc::tc_commit(&empty[stage]);
+                        if (++stage == STAGES) { stage = 0; phase ^= 1; }
                     }
-                    tc::tc_commit(&empty[stage]);
-                    if (++stage == STAGES) { stage = 0; phase ^= 1; }
+                    if (ok) {
+                        // an empty tile touches no TMEM: the epilogue writes zeros for it
+                        if (any) tc::tc_commit(&tfull[acc]);
+                        else tc::mbar_arrive(&tfull[acc]);
+                        if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+                    }
                 }
-                if (!ok) break;
-                tc::tc_commit(&tfull[acc]);
-                if (++acc == 2) { acc = 0; acc_phase ^= 1; }
             }
-            // all issued MMAs complete before TMEM is released
+            if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) break;
+        }
+        // all issued MMAs complete before TMEM is released
+        if (lane == 0) {
             tc::tc_commit(drain);
             tc::mbar_wait(drain, 0, p.err, 1u << 20);
         }
@@ -525,6 +586,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
             const int l = t / (p.tiles_m * p.tiles_n), rem = t - l * p.tiles_m * p.tiles_n;
             int tm, tn;
             tile_of(rem, p.tiles_m, p.tiles_n, tm, tn);
+            const bool active = !p.use_skip || i8_tile_any(p, tm, tn, ktiles);
             if (!tc::mbar_wait(&tfull[acc], acc_phase, p.err)) break;
             tc::tc_fence_after();
             const int m = c_crt.mod[l];
@@ -532,22 +594,24 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
             const int row = tm * BM + q * 32 + lane;
             uint8_t *out = p.R + ((int64_t)l * p.M + row) * p.ldr + (int64_t)tn * BN;
             for (int c = 0; c < BN; c += 32) {
-                uint32_t v[32];
-                tc::tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + c), v);
-                uint32_t w[8];
+                uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                if (active) {
+                    uint32_t v[32];
+                    tc::tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * BN + c), v);
 #pragma unroll
-                for (int u = 0; u < 8; u++) {
-                    uint32_t packed = 0;
+                    for (int u = 0; u < 8; u++) {
+                        uint32_t packed = 0;
 #pragma unroll
-                    for (int b = 0; b < 4; b++) {
-                        const int x = (int)v[u * 4 + b];
-                        const int qq = __float2int_rn((float)x * invm);
-                        int r = x - qq * m;
-                        r += (r < 0) ? m : 0;
-                        r -= (r >= m) ? m : 0;
-                        packed |= (uint32_t)r << (8 * b);
+                        for (int b = 0; b < 4; b++) {
+                            const int x = (int)v[u * 4 + b];
+                            const int qq = __float2int_rn((float)x * invm);
+                            int r = x - qq * m;
+                            r += (r < 0) ? m : 0;
+                            r -= (r >= m) ? m : 0;
+                            packed |= (uint32_t)r << (8 * b);
+                        }
+                        w[u] = packed;
                     }
-                    w[u] = packed;
                 }
                 const int col = tn * BN + c;
                 if (row < p.M) {
@@ -717,9 +781,10 @@ static bool device_is_sm100()
 }
 
 int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B, int64_t ldb,
-                   double *C, int64_t ldc, int nterms, cudaStream_t st)
+                   double *C, int64_t ldc, int nterms, cudaStream_t st, const ZeroSkip *zs)
 {
     OzakiWork w;
+    w.zs = zs;
     const int r = gemm_f64_ozaki_launch(M, N, K, A, lda, B, ldb, C, ldc, nterms, &w, st);
     if (r) return r;
     return gemm_f64_ozaki_finish(&w, st);
@@ -832,7 +897,12 @@ int gemm_f64_ozaki_rows_product(int64_t M, const double *A, int64_t lda, const O
     const int64_t ldr = round_up(N, 16);
     const int nsm = sms();
     I8Params prm;
-    prm.M = (int)M; prm.N = (int)N; prm.Kp = (int)Kp; prm.L = L;
+    memset(&prm, 0, sizeof(prm));
+    prm.M = (int)M; prm.N = (int)N; prm.K = (int)K; prm.Kp = (int)Kp; prm.L = L;
+    if (w->zs) {
+        prm.use_skip = 1;
+        prm.zs = *w->zs;
+    }
     prm.tiles_m = (int)ceil_div(M, oz::BM); prm.tiles_n = (int)ceil_div(N, oz::BN);
     prm.R = w->rr.as<uint8_t>(); prm.ldr = ldr; prm.err = w->err.as<int>();
     static bool attr = false;

@@ -108,6 +108,7 @@ def _lib():
             "iarray_container_save": ([P, P, ctypes.c_char_p], RC),
             "iarray_container_open": ([P, ctypes.c_char_p, P], RC),
             "iarray_container_load": ([P, ctypes.c_char_p, P], RC),
+            "iarray_container_remove": ([ctypes.c_char_p], RC),
             "iarray_to_cframe": ([P, P, P, P, P], RC), "iarray_from_cframe": ([P, P, I64, ctypes.c_bool, P], RC),
             "iarray_linalg_matmul": ([P, P, P, P, P], RC), "iarray_linalg_transpose": ([P, P, P], RC),
             "iarray_gemm": ([P, P, P, P], RC), "iarray_gemv": ([P, P, P, P], RC),
@@ -254,10 +255,12 @@ class Container:
 
     # ------------------------------------------------------------------ constructors
     @classmethod
-    def from_numpy(cls, ctx, arr, chunkshape, blockshape, urlpath=None):
+    def from_numpy(cls, ctx, arr, chunkshape, blockshape, urlpath=None, contiguous=True):
+        """With `urlpath` the container is also written to disk: a contiguous frame file, or
+        (contiguous=False) a sparse frame directory."""
         arr = np.ascontiguousarray(arr)
         d = dtshape(arr.shape, arr.dtype)
-        s = storage(chunkshape, blockshape, urlpath)
+        s = storage(chunkshape, blockshape, urlpath, contiguous)
         p = ctypes.c_void_p()
         check(_lib().iarray_from_buffer(ctx.ptr, ctypes.byref(d), arr.ctypes.data, arr.nbytes, ctypes.byref(s),
                                         ctypes.byref(p)), "iarray_from_buffer")
@@ -310,6 +313,11 @@ class Container:
         fn = _lib().iarray_container_load if load else _lib().iarray_container_open
         check(fn(ctx.ptr, path.encode(), ctypes.byref(p)), "iarray_container_open")
         return cls(ctx, p)
+
+    @staticmethod
+    def remove(path):
+        """iarray_container_remove: a frame file, or a sparse frame directory."""
+        check(_lib().iarray_container_remove(path.encode()), "iarray_container_remove")
 
     # ------------------------------------------------------------------ accessors
     def decode_to_device(self, dptr, ld):
@@ -397,15 +405,16 @@ class Container:
             pass
 
 
-def _product(fn, name, ctx, a, b, chunkshape, blockshape, urlpath=None):
-    s = storage(chunkshape, blockshape, urlpath)
+def _product(fn, name, ctx, a, b, chunkshape, blockshape, urlpath=None, contiguous=True):
+    s = storage(chunkshape, blockshape, urlpath, contiguous)
     p = ctypes.c_void_p()
     check(fn(ctx.ptr, a.ptr, b.ptr, ctypes.byref(s), ctypes.byref(p)), name)
     return Container(ctx, p)
 
 
-def matmul(ctx, a, b, chunkshape, blockshape, urlpath=None):
-    return _product(_lib().iarray_linalg_matmul, "iarray_linalg_matmul", ctx, a, b, chunkshape, blockshape, urlpath)
+def matmul(ctx, a, b, chunkshape, blockshape, urlpath=None, contiguous=True):
+    return _product(_lib().iarray_linalg_matmul, "iarray_linalg_matmul", ctx, a, b, chunkshape, blockshape, urlpath,
+                    contiguous)
 
 
 def opt_gemm(ctx, a, b, chunkshape, blockshape):

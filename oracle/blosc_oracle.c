@@ -566,8 +566,21 @@ DEF_BLOCK_GEMM(float, bgemm_f)
  * trim M/K/N at the container edge and accumulate A_blk * B_blk with the full
  * block leading dimensions.  Writes C's padded chunk data (c_chunks[n] holds
  * extchunk items of chunk n).  dtype 0 = double, 1 = float. */
+EXPORT int ora_opt_gemm_rule(const ora_schunk_t *A, const ora_schunk_t *B, const ora_geom_t *Cg,
+                             int dtype, uint8_t *const *c_chunks, int chunk_rule);
+
 EXPORT int ora_opt_gemm(const ora_schunk_t *A, const ora_schunk_t *B, const ora_geom_t *Cg,
                         int dtype, uint8_t *const *c_chunks)
+{
+    return ora_opt_gemm_rule(A, B, Cg, dtype, c_chunks, 3);
+}
+
+/* The same loop with the chunk-level skip of each operand switchable: chunk_rule bit 0 =
+ * skip A's special-zero chunks, bit 1 = B's.  iarray_opt_gemm uses both (3);
+ * iarray_opt_gemm_a only B's (2: src/linalg/iarray_gemm_a.c:127-146, where A's blocks are
+ * judged by block_is_zeros alone, :313); iarray_opt_gemm_b only A's (1: iarray_gemm_b.c). */
+EXPORT int ora_opt_gemm_rule(const ora_schunk_t *A, const ora_schunk_t *B, const ora_geom_t *Cg,
+                             int dtype, uint8_t *const *c_chunks, int chunk_rule)
 {
     const ora_geom_t *ag = &A->g, *bg = &B->g;
     int is = ag->itemsize;
@@ -587,8 +600,8 @@ EXPORT int ora_opt_gemm(const ora_schunk_t *A, const ora_schunk_t *B, const ora_
             uint8_t *out = cchunk + cb * cbn * is;
             for (int64_t kc = 0; kc < Kch; kc++) {
                 int64_t an = ci0 * Kch + kc, bn = kc * Nch + ci1;
-                if (ora_chunk_is_zeros(B->chunks[bn])) continue;
-                if (ora_chunk_is_zeros(A->chunks[an])) continue;
+                if ((chunk_rule & 2) && ora_chunk_is_zeros(B->chunks[bn])) continue;
+                if ((chunk_rule & 1) && ora_chunk_is_zeros(A->chunks[an])) continue;
                 if (ora_chunk_decompress(A->chunks[an], A->chunk_len[an], adec, (int)(a_extcn * is)) < 0) goto fail;
                 if (ora_chunk_decompress(B->chunks[bn], B->chunk_len[bn], bdec, (int)(b_extcn * is)) < 0) goto fail;
                 int pad_m = ag->shape[0] != ext_of(ag, 0) && ci0 == Mch - 1;

@@ -249,13 +249,15 @@ def _schunk(g: Geom, chunks):
     return s
 
 
-def opt_gemm(ga: Geom, a_chunks, gb: Geom, b_chunks, gc: Geom, dtype: int) -> np.ndarray:
-    """iarray_opt_gemm restated; returns C as a logical numpy array."""
+def opt_gemm(ga: Geom, a_chunks, gb: Geom, b_chunks, gc: Geom, dtype: int, chunk_rule: int = 3) -> np.ndarray:
+    """iarray_opt_gemm restated; returns C as a logical numpy array.  chunk_rule: which
+    operands' special-zero chunks are skipped (bit 0 A, bit 1 B): 3 for iarray_opt_gemm, 2 for
+    iarray_opt_gemm_a, 1 for iarray_opt_gemm_b."""
     sa, sb = _schunk(ga, a_chunks), _schunk(gb, b_chunks)
     cg = gc.cstruct()
     outs = [ctypes.create_string_buffer(gc.chunk_nbytes) for _ in range(gc.nchunks)]
     ptrs = (ctypes.c_void_p * gc.nchunks)(*[ctypes.cast(o, ctypes.c_void_p) for o in outs])
-    if LIB.ora_opt_gemm(ctypes.byref(sa), ctypes.byref(sb), ctypes.byref(cg), dtype, ptrs) != 0:
+    if LIB.ora_opt_gemm_rule(ctypes.byref(sa), ctypes.byref(sb), ctypes.byref(cg), dtype, ptrs, chunk_rule) != 0:
         raise ValueError("oracle opt_gemm failed")
     npdt = NP_OF[dtype]
     out = np.zeros(gc.shape, npdt)

@@ -8,6 +8,7 @@ tests/generator.py:24-76 with LZ4 clevel 5, SHUFFLE, btune off):
 
 Outputs (committed):
   chunk_<name>_0.bin       first data chunk of three frames, byte-for-byte
+  <name>.iarray            one whole frame (the smallest), byte-for-byte
   golden_digests.json      for all 10 frames: frame header / trailer bytes, and per chunk
                            the SHA-256 of the compressed chunk and of its decoded bytes,
                            its cbytes and stream-kind counts.
@@ -26,6 +27,8 @@ sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
 import oracle as O  # noqa: E402
 
 KEEP = ["test_binomial_int32_n1_p0.7", "test_poisson_int32_lam3", "test_rand_float32"]
+# whole frames copied byte for byte: opened by the library itself in the GPU tests
+KEEP_FRAMES = ["test_binomial_int32_n1_p0.7"]
 
 
 def main(ref):
@@ -61,6 +64,9 @@ def main(ref):
         if name in KEEP:
             with open(os.path.join(HERE, f"chunk_{name}_0.bin"), "wb") as fh:
                 fh.write(fr["chunks"][0])
+        if name in KEEP_FRAMES:
+            with open(os.path.join(HERE, f"{name}.iarray"), "wb") as fh:
+                fh.write(buf)
     with open(os.path.join(HERE, "golden_digests.json"), "w") as fh:
         json.dump(out, fh, indent=1, sort_keys=True)
     print(f"wrote {len(out)} frame digests, {len(KEEP)} chunks")

@@ -230,3 +230,17 @@ def test_cpu_baseline_whole_product_matches_oracle():
     assert np.allclose(C, ref, rtol=1e-13, atol=1e-13)
     for c in chunks:                                     # every chunk is valid Blosc2 for the oracle
         assert len(O.chunk_decompress(c)) == gc.chunk_nbytes
+
+
+def test_committed_reference_frame_matches_digests():
+    """The whole reference-written frame committed as a fixture: the oracle's frame reader
+    finds every chunk, and each chunk and its decoding match the recorded digests."""
+    import hashlib
+    name = "test_binomial_int32_n1_p0.7"
+    buf = open(os.path.join(GOLD, f"{name}.iarray"), "rb").read()
+    fr = O.read_frame(buf)
+    want = DIGESTS[name]["chunks"]
+    assert len(fr["chunks"]) == len(want)
+    for c, w in zip(fr["chunks"], want):
+        assert hashlib.sha256(c).hexdigest() == w["sha_chunk"]
+        assert hashlib.sha256(O.chunk_decompress(c)).hexdigest() == w["sha_decoded"]
