@@ -365,6 +365,44 @@ def secondary_f32(ia, ctx, stream, args):
     return res
 
 
+def secondary_sparse(ia, ctx, stream, args, dense_ms):
+    """Block-sparse precision_f64: the benchmark's A with 90% of its 256 x 256 blocks zero
+    (default_rng(7) picks them), B unchanged.  The reference skips every block pair with a
+    zero block (src/linalg/iarray_gemm.c:206-211); the GPU kernels leave out the k-tiles of
+    such pairs, so the step shrinks with the work."""
+    A, B = make_inputs()
+    rng = np.random.default_rng(7)
+    zero = rng.random((M // BLOCK[0], K // BLOCK[1])) < 0.9
+    for i, j in zip(*np.nonzero(zero)):
+        A[i * BLOCK[0]:(i + 1) * BLOCK[0], j * BLOCK[1]:(j + 1) * BLOCK[1]] = 0.0
+    Ac = ia.Container.from_numpy(ctx, A, CHUNK, BLOCK)
+    Bc = ia.Container.from_numpy(ctx, B, CHUNK, BLOCK)
+    rows = np.sort(np.random.default_rng(99).choice(M, 64, replace=False))
+    ref = A[rows] @ B
+    res = {"workload": "precision_f64 8192^3 with 90% of A's 256^2 blocks zero",
+           "zero_block_fraction": float(zero.mean())}
+    for name, form in (("native", ia.FORM_NATIVE), ("split", ia.FORM_SPLIT)):
+        ctx.set_form(form)
+        out = []
+
+        def step():
+            out.append(ia.opt_gemm(ctx, Ac, Bc, CHUNK, BLOCK))
+            if len(out) > 1:
+                out.pop(0).free()
+        ms, _ = _timed(ctx, stream, step, max(2, args.steps // 2), max(1, args.warmup - 1))
+        c = out[-1].to_numpy()[rows]
+        err = float(np.linalg.norm(c - ref) / np.linalg.norm(ref))
+        for x in out:
+            x.free()
+        res[name] = {"ms_per_step": ms, "dense_ms_per_step": dense_ms.get(name),
+                     "speedup_vs_dense": dense_ms[name] / ms if dense_ms.get(name) else None,
+                     "normwise_err_vs_f64": err}
+    ctx.set_form(ia.FORM_NATIVE)
+    Ac.free()
+    Bc.free()
+    return res
+
+
 def secondary_batch(ia, ctx, stream, args):
     """Batching: 512 independent float64 products, m, n, k uniform integers in [64, 2048]
     (default_rng(5)), entries uniform(-1, 1), chunk 512^2, block 128^2 (ragged edges); one
@@ -603,7 +641,9 @@ def run_ours(args):
             c.free()
         torch.cuda.empty_cache()
         secondary = {}
-        for key, fn in (("plain_f64_1000", lambda: secondary_plain_f64(ia, ctx, stream, args)),
+        dense_ms = {k: r["ms"] for k, r in results.items() if k in ("native", "split")}
+        for key, fn in (("sparse_blocks_f64", lambda: secondary_sparse(ia, ctx, stream, args, dense_ms)),
+                        ("plain_f64_1000", lambda: secondary_plain_f64(ia, ctx, stream, args)),
                         ("gemv_f32", lambda: secondary_gemv(ia, ctx, stream, args, pk)),
                         ("precision_f32", lambda: secondary_f32(ia, ctx, stream, args)),
                         ("batching_f64", lambda: secondary_batch(ia, ctx, stream, args))):

@@ -292,6 +292,42 @@ INA_API(ina_rc_t) iarray_opt_gemm_b(iarray_context_t *ctx, iarray_container_t *a
 INA_API(ina_rc_t) iarray_opt_gemv(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b,
                                   iarray_storage_t *storage, iarray_container_t **c);
 
+/* ---------------------------------------------------------------- expressions */
+/* include/libiarray/iarray.h:317-332 (opaque here) and :308-314. */
+typedef struct iarray_expression_s iarray_expression_t;
+typedef union {
+    float f32;
+    double f64;
+    int32_t i32;
+    int64_t i64;
+    bool b;
+} iarray_user_param_t;
+
+/* iarray.h:830-846 (src/iarray_expression.c:59-120, :780).  Element-wise expressions over
+ * containers of the output's shape, float64 or float32, evaluated on the GPU: operands are
+ * decoded in device memory and one kernel runs the compiled program for every element.
+ * Grammar: numbers, bound variables and scalars, pi, e, + - * / ** (right-associative),
+ * unary minus, parentheses, and the functions abs, sqrt, exp, expm1, log, log10, log1p, sin,
+ * cos, tan, asin, acos, atan, sinh, cosh, tanh, ceil, floor, negative (one argument), atan2,
+ * pow, min, max, fmod (two), with numpy's aliases absolute, arcsin, arccos, arctan, arctan2,
+ * power, minimum, maximum.  At most 16 operands.  iarray_expr_compile returns
+ * INA_ERR_INVALID_ARGUMENT for a malformed expression or an unbound name; iarray_eval returns
+ * INA_ERR_NOT_COMPLETE before compile / bind_out_properties and IARRAY_ERR_INVALID_SHAPE when
+ * an operand's shape differs from the output's.  User-defined functions (LLVM bitcode:
+ * iarray_expr_compile_udf, iarray_expr_bind_param) return IARRAY_ERR_NOT_SUPPORTED. */
+INA_API(ina_rc_t) iarray_expr_new(iarray_context_t *ctx, iarray_data_type_t dtype, iarray_expression_t **e);
+INA_API(void) iarray_expr_free(iarray_context_t *ctx, iarray_expression_t **e);
+INA_API(ina_rc_t) iarray_expr_bind(iarray_expression_t *e, const char *var, iarray_container_t *val);
+INA_API(ina_rc_t) iarray_expr_bind_out_properties(iarray_expression_t *e, iarray_dtshape_t *dtshape,
+                                                  iarray_storage_t *store);
+INA_API(ina_rc_t) iarray_expr_bind_param(iarray_expression_t *e, iarray_user_param_t val);
+INA_API(ina_rc_t) iarray_expr_bind_scalar_float(iarray_expression_t *e, const char *var, float val);
+INA_API(ina_rc_t) iarray_expr_bind_scalar_double(iarray_expression_t *e, const char *var, double val);
+INA_API(ina_rc_t) iarray_expr_compile(iarray_expression_t *e, const char *expr);
+INA_API(ina_rc_t) iarray_expr_compile_udf(iarray_expression_t *e, int llvm_bc_len, const char *llvm_bc,
+                                          const char *name);
+INA_API(ina_rc_t) iarray_eval(iarray_expression_t *e, iarray_container_t **container);
+
 /* ================================================================ B200 additions
  * No counterpart in the reference: the split-precision and batching forms named in
  * the project goal, plus chunk-level access used by the parity tests. */
@@ -315,6 +351,13 @@ typedef enum iarray_b200_encoder_e {
     IARRAY_B200_ENCODER_LIBLZ4 = 1,
 } iarray_b200_encoder_t;
 INA_API(ina_rc_t) iarray_b200_set_encoder(iarray_context_t *ctx, iarray_b200_encoder_t encoder);
+/* Binds expression variable `var` to the matrix product a * b (B200 addition; the
+ * reference's expressions take containers only, so a product is first written to a
+ * container by iarray_linalg_matmul).  The product is computed on the GPU in the context's
+ * form when iarray_eval runs and is consumed by the expression in device memory without
+ * being encoded: the expression is the product's epilogue, e.g. "max(ab, 0) + bias". */
+INA_API(ina_rc_t) iarray_b200_expr_bind_matmul(iarray_expression_t *e, const char *var, iarray_container_t *a,
+                                               iarray_container_t *b);
 /* Number of INT8 moduli/slices the float64 split form uses (0 = automatic). */
 INA_API(ina_rc_t) iarray_b200_set_split_terms(iarray_context_t *ctx, int nterms);
 /* Number of BF16 tensor-core products of the float32 split form: 6 (each operand split

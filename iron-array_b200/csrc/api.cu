@@ -25,6 +25,7 @@
 
 #include "../../include/iarray_b200.h"
 #include "common.cuh"
+#include "expr.h"
 #include "frame.h"
 #include "zskip.cuh"
 
@@ -2215,4 +2216,202 @@ INA_API(void) iarray_b200_batch_free(iarray_b200_batch_t **batch)
     if (bt->graph) cudaGraphDestroy(bt->graph);
     delete bt;
     *batch = nullptr;
+}
+
+// ============================================================================ expressions
+// iarray_expr_* / iarray_eval (include/libiarray/iarray.h:830-846, src/iarray_expression.c):
+// element-wise expressions over containers of one shape, evaluated on the GPU (expr.cu).  The
+// operands are decoded into dense device arrays, one kernel runs the compiled program for
+// every element, and the result is encoded into the output partition.  B200 addition:
+// iarray_b200_expr_bind_matmul binds a variable to the product A * B, computed on the GPU in
+// the context's form and consumed by the expression in device memory (the product is never
+// encoded): the expression acts as the product's epilogue.
+struct iarray_expression_s {
+    iarray_context_t *ctx = nullptr;
+    int dtype = IARRAY_DATA_TYPE_DOUBLE;
+    std::vector<std::string> names;
+    std::vector<iarray_container_t *> conts;                                  // nullptr for a product
+    std::vector<std::pair<iarray_container_t *, iarray_container_t *>> prods;  // {a, b} of a product operand
+    std::vector<std::pair<std::string, double>> scalars;
+    bool out_set = false, compiled = false;
+    iarray_dtshape_t out_dtshape;
+    iarray_storage_t out_storage;
+    std::string out_urlpath;
+    std::vector<iab::ExprOp> prog;
+};
+
+INA_API(ina_rc_t) iarray_expr_new(iarray_context_t *ctx, iarray_data_type_t dtype, iarray_expression_t **e)
+{
+    CHECK_ARG(ctx && e);
+    if (dtype != IARRAY_DATA_TYPE_DOUBLE && dtype != IARRAY_DATA_TYPE_FLOAT) return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    *e = new iarray_expression_t();
+    (*e)->ctx = ctx;
+    (*e)->dtype = dtype;
+    return INA_SUCCESS;
+}
+
+INA_API(void) iarray_expr_free(iarray_context_t *ctx, iarray_expression_t **e)
+{
+    (void)ctx;
+    if (!e || !*e) return;
+    delete *e;
+    *e = nullptr;
+}
+
+static ina_rc_t expr_add_operand(iarray_expression_t *e, const char *var, iarray_container_t *c, iarray_container_t *a,
+                                 iarray_container_t *b)
+{
+    CHECK_ARG(e && var && var[0]);
+    if ((int)e->names.size() >= iab::EXPR_MAX_OPERANDS) return rc_err(INA_ERR_FULL);
+    for (const std::string &n : e->names)
+        if (n == var) return rc_err(INA_ERR_INVALID_ARGUMENT);
+    e->names.push_back(var);
+    e->conts.push_back(c);
+    e->prods.emplace_back(a, b);
+    e->compiled = false;
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_expr_bind(iarray_expression_t *e, const char *var, iarray_container_t *val)
+{
+    CHECK_ARG(e && val);
+    if (val->dtshape.dtype != e->dtype) return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    return expr_add_operand(e, var, val, nullptr, nullptr);
+}
+
+INA_API(ina_rc_t) iarray_b200_expr_bind_matmul(iarray_expression_t *e, const char *var, iarray_container_t *a,
+                                               iarray_container_t *b)
+{
+    CHECK_ARG(e && a && b);
+    if (a->dtshape.dtype != e->dtype || b->dtshape.dtype != e->dtype) return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    if (a->dtshape.ndim != 2 || b->dtshape.ndim != 2) return rc_err(IARRAY_ERR_INVALID_NDIM);
+    if (a->dtshape.shape[1] != b->dtshape.shape[0]) return rc_err(IARRAY_ERR_INVALID_SHAPE);
+    return expr_add_operand(e, var, nullptr, a, b);
+}
+
+INA_API(ina_rc_t) iarray_expr_bind_out_properties(iarray_expression_t *e, iarray_dtshape_t *dtshape,
+                                                  iarray_storage_t *store)
+{
+    CHECK_ARG(e && dtshape && store);
+    e->out_dtshape = *dtshape;
+    e->out_storage = *store;
+    e->out_urlpath = store->urlpath ? store->urlpath : "";
+    e->out_storage.urlpath = nullptr;
+    e->out_set = true;
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_expr_bind_param(iarray_expression_t *e, iarray_user_param_t val)
+{
+    (void)e;
+    (void)val;
+    return rc_err(IARRAY_ERR_NOT_SUPPORTED);        // parameters of user-defined functions (LLVM bitcode)
+}
+
+static ina_rc_t expr_add_scalar(iarray_expression_t *e, const char *var, double val)
+{
+    CHECK_ARG(e && var && var[0]);
+    for (auto &sc : e->scalars)
+        if (sc.first == var) { sc.second = val; e->compiled = false; return INA_SUCCESS; }
+    e->scalars.emplace_back(var, val);
+    e->compiled = false;
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_expr_bind_scalar_float(iarray_expression_t *e, const char *var, float val)
+{
+    return expr_add_scalar(e, var, (double)val);
+}
+
+INA_API(ina_rc_t) iarray_expr_bind_scalar_double(iarray_expression_t *e, const char *var, double val)
+{
+    return expr_add_scalar(e, var, val);
+}
+
+INA_API(ina_rc_t) iarray_expr_compile(iarray_expression_t *e, const char *expr)
+{
+    CHECK_ARG(e && expr);
+    std::string why;
+    if (!iab::expr_compile(expr, e->names, e->scalars, &e->prog, &why)) {
+        e->compiled = false;
+        return rc_err(INA_ERR_INVALID_ARGUMENT);
+    }
+    e->compiled = true;
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_expr_compile_udf(iarray_expression_t *e, int llvm_bc_len, const char *llvm_bc,
+                                          const char *name)
+{
+    (void)e; (void)llvm_bc_len; (void)llvm_bc; (void)name;
+    return rc_err(IARRAY_ERR_NOT_SUPPORTED);        // user-defined functions come as LLVM bitcode
+}
+
+INA_API(ina_rc_t) iarray_eval(iarray_expression_t *e, iarray_container_t **container)
+{
+    CHECK_ARG(e && container);
+    if (!e->compiled || !e->out_set) return rc_err(INA_ERR_NOT_COMPLETE);
+    iarray_context_t *ctx = e->ctx;
+    iarray_dtshape_t od = e->out_dtshape;
+    if (od.dtype != e->dtype) return rc_err(IARRAY_ERR_INVALID_DTYPE);
+    iarray_storage_t os = e->out_storage;
+    os.urlpath = e->out_urlpath.empty() ? nullptr : (char *)e->out_urlpath.c_str();
+    iarray_container_t *out = nullptr;
+    ina_rc_t rc = new_container(ctx, &od, &os, &out);
+    if (INA_FAILED(rc)) return rc;
+    const int64_t rows = rows_of(out->dtshape), cols = cols_of(out->dtshape), ld = pad_ld(cols);
+    const int isz = out->geom.itemsize;
+    auto fail = [&](ina_rc_t r) { iarray_container_free(ctx, &out); return r; };
+    // operands: shapes, then dense device copies
+    for (size_t k = 0; k < e->names.size(); k++) {
+        if (e->conts[k]) {
+            const iarray_dtshape_t &d = e->conts[k]->dtshape;
+            if (d.ndim != od.ndim) return fail(rc_err(IARRAY_ERR_INVALID_NDIM));
+            for (int i = 0; i < od.ndim; i++)
+                if (d.shape[i] != od.shape[i]) return fail(rc_err(IARRAY_ERR_INVALID_SHAPE));
+        } else if (od.ndim != 2 || e->prods[k].first->dtshape.shape[0] != od.shape[0] ||
+                   e->prods[k].second->dtshape.shape[1] != od.shape[1]) {
+            return fail(rc_err(IARRAY_ERR_INVALID_SHAPE));
+        }
+    }
+    std::vector<DevBuf> dense(e->names.size());
+    iab::ExprArgs args;
+    memset(&args, 0, sizeof(args));
+    for (size_t k = 0; k < e->names.size(); k++) {
+        if (!dense[k].allocate((size_t)std::max<int64_t>(rows * ld * isz, 16), ctx->device))
+            return fail(rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY));
+        if (e->conts[k]) {
+            rc = decode_logical(ctx, e->conts[k], dense[k].p, ld);
+        } else {
+            iarray_container_t *a = e->prods[k].first, *b = e->prods[k].second;
+            const int64_t K = a->dtshape.shape[1], lda = pad_ld(K);
+            DevBuf dA, dB;
+            if (!dA.allocate((size_t)std::max<int64_t>(rows * lda * isz, 16), ctx->device) ||
+                !dB.allocate((size_t)std::max<int64_t>(K * ld * isz, 16), ctx->device))
+                return fail(rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY));
+            rc = decode_logical(ctx, a, dA.p, lda);
+            if (INA_SUCCEED(rc)) rc = decode_logical(ctx, b, dB.p, ld);
+            if (INA_SUCCEED(rc)) {
+                if (K == 0) cudaMemsetAsync(dense[k].p, 0, (size_t)(rows * ld * isz), ctx->stream);
+                else rc = dense_product(ctx, e->dtype, rows, cols, K, dA.p, lda, dB.p, ld, dense[k].p, ld);
+            }
+            if (INA_SUCCEED(rc)) rc = cuda_rc(cudaStreamSynchronize(ctx->stream));   // dA, dB go back to the pool idle
+        }
+        if (INA_FAILED(rc)) return fail(rc);
+        args.in[k] = dense[k].p;
+        args.ld[k] = ld;
+    }
+    args.nops = (int)e->prog.size();
+    for (int i = 0; i < args.nops; i++) args.ops[i] = e->prog[(size_t)i];
+    DevBuf res;
+    if (!res.allocate((size_t)std::max<int64_t>(rows * ld * isz, 16), ctx->device))
+        return fail(rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY));
+    iab::expr_eval(isz, rows, cols, args, res.p, ld, ctx->stream);
+    rc = cuda_rc(cudaGetLastError());
+    if (INA_FAILED(rc)) return fail(rc);
+    rc = out->geom.nchunks ? encode_into(ctx, out, res.p, ld) : fill_zero_chunks(out);
+    if (INA_SUCCEED(rc)) rc = save_if_urlpath(ctx, out);
+    if (INA_FAILED(rc)) return fail(rc);
+    *container = out;
+    return INA_SUCCESS;
 }

@@ -468,6 +468,7 @@ __device__ __forceinline__ bool i8_tile_any(const I8Params &p, int tm, int tn, i
 // accumulator: r = C mod m_l in [0, m_l), stored as one byte per entry.  With use_skip,
 // the k-tiles of zero-block pairs are neither loaded nor multiplied (every role derives the
 // same mask); a tile that needs none is written as zero residues.
+template <bool SKIP>
 __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_constant__ CUtensorMap tmA,
                                                                 const __grid_constant__ CUtensorMap tmB, I8Params p)
 {
@@ -503,7 +504,10 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
     const uint32_t tmem_base = *tmem_slot;
     const int total = p.L * p.tiles_m * p.tiles_n;
     const int ktiles = p.Kp / BK;
-    auto needed = [&](const uint32_t *mask, int kt) { return !p.use_skip || ((mask[kt >> 5] >> (kt & 31)) & 1u); };
+    auto needed = [&](const uint32_t *mask, int kt) {
+        if constexpr (SKIP) return ((mask[kt >> 5] >> (kt & 31)) & 1u) != 0;
+        else return true;
+    };
 
     if (warp == 0) {
         int stage = 0;
@@ -514,7 +518,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
             const int l = t / (p.tiles_m * p.tiles_n), rem = t - l * p.tiles_m * p.tiles_n;
             int tm, tn;
             tile_of(rem, p.tiles_m, p.tiles_n, tm, tn);
-            if (p.use_skip) i8_kmask(p, tm, tn, ktiles, pmask);
+            if constexpr (SKIP) i8_kmask(p, tm, tn, ktiles, pmask);
             if (lane == 0) {
                 for (int kt = 0; kt < ktiles; kt++) {
                     if (!needed(pmask, kt)) continue;
@@ -541,7 +545,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
             const int l = t / (p.tiles_m * p.tiles_n), rem = t - l * p.tiles_m * p.tiles_n;
             int tm, tn;
             tile_of(rem, p.tiles_m, p.tiles_n, tm, tn);
-            if (p.use_skip) i8_kmask(p, tm, tn, ktiles, mmask);
+            if constexpr (SKIP) i8_kmask(p, tm, tn, ktiles, mmask);
             if (lane == 0) {
                 if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, p.err)) {
                     ok = false;
@@ -586,7 +590,8 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
             const int l = t / (p.tiles_m * p.tiles_n), rem = t - l * p.tiles_m * p.tiles_n;
             int tm, tn;
             tile_of(rem, p.tiles_m, p.tiles_n, tm, tn);
-            const bool active = !p.use_skip || i8_tile_any(p, tm, tn, ktiles);
+            bool active = true;
+            if constexpr (SKIP) active = i8_tile_any(p, tm, tn, ktiles);
             if (!tc::mbar_wait(&tfull[acc], acc_phase, p.err)) break;
             tc::tc_fence_after();
             const int m = c_crt.mod[l];
@@ -907,13 +912,17 @@ int gemm_f64_ozaki_rows_product(int64_t M, const double *A, int64_t lda, const O
     prm.R = w->rr.as<uint8_t>(); prm.ldr = ldr; prm.err = w->err.as<int>();
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_i8gemm_mod, cudaFuncAttributeMaxDynamicSharedMemorySize, oz::SMEM);
+        cudaFuncSetAttribute(k_i8gemm_mod<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, oz::SMEM);
+        cudaFuncSetAttribute(k_i8gemm_mod<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, oz::SMEM);
         attr = true;
     }
     const int tiles = L * prm.tiles_m * prm.tiles_n;
     const CUtensorMap &tmA = *reinterpret_cast<const CUtensorMap *>(w->tmA);
     const CUtensorMap &tmB = *reinterpret_cast<const CUtensorMap *>(ob.tmB);
-    IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
+    if (prm.use_skip)
+        IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<true><<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
+    else
+        IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<false><<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
     launch_crt(ob.nc, (unsigned)(nsm * 8), (int)M, (int)N, w->rr.as<uint8_t>(), ldr, w->sa.as<int>(), ob.sb.as<int>(), C, ldc, st);
     launch_nonfinite_fix<double>(M, N, K, A, lda, ob.B, ob.ldb, C, ldc, w->sa.as<int>(), ob.sb.as<int>(), kNonFinite, st);
     return 0;

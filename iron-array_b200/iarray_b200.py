@@ -109,6 +109,14 @@ def _lib():
             "iarray_container_open": ([P, ctypes.c_char_p, P], RC),
             "iarray_container_load": ([P, ctypes.c_char_p, P], RC),
             "iarray_container_remove": ([ctypes.c_char_p], RC),
+            "iarray_expr_new": ([P, ctypes.c_int, P], RC), "iarray_expr_free": ([P, P], None),
+            "iarray_expr_bind": ([P, ctypes.c_char_p, P], RC),
+            "iarray_b200_expr_bind_matmul": ([P, ctypes.c_char_p, P, P], RC),
+            "iarray_expr_bind_out_properties": ([P, P, P], RC),
+            "iarray_expr_bind_scalar_double": ([P, ctypes.c_char_p, ctypes.c_double], RC),
+            "iarray_expr_bind_scalar_float": ([P, ctypes.c_char_p, ctypes.c_float], RC),
+            "iarray_expr_compile": ([P, ctypes.c_char_p], RC), "iarray_eval": ([P, P], RC),
+            "iarray_expr_compile_udf": ([P, ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p], RC),
             "iarray_to_cframe": ([P, P, P, P, P], RC), "iarray_from_cframe": ([P, P, I64, ctypes.c_bool, P], RC),
             "iarray_linalg_matmul": ([P, P, P, P, P], RC), "iarray_linalg_transpose": ([P, P, P], RC),
             "iarray_gemm": ([P, P, P, P], RC), "iarray_gemv": ([P, P, P, P], RC),
@@ -506,3 +514,42 @@ class Batch:
 
 def almost_equal(a, b, tol):
     return _lib().iarray_container_almost_equal(a.ptr, b.ptr, tol)
+
+
+class Expression:
+    """iarray_expr_* / iarray_eval: an element-wise expression over containers of the output's
+    shape, evaluated on the GPU; bind_matmul feeds a matrix product in as an operand."""
+
+    def __init__(self, ctx, dtype=np.float64):
+        self.ctx = ctx
+        self.ptr = ctypes.c_void_p()
+        check(_lib().iarray_expr_new(ctx.ptr, IA_DTYPE[np.dtype(dtype)], ctypes.byref(self.ptr)), "iarray_expr_new")
+
+    def bind(self, var, container):
+        check(_lib().iarray_expr_bind(self.ptr, var.encode(), container.ptr), "iarray_expr_bind")
+
+    def bind_matmul(self, var, a, b):
+        check(_lib().iarray_b200_expr_bind_matmul(self.ptr, var.encode(), a.ptr, b.ptr), "iarray_b200_expr_bind_matmul")
+
+    def bind_scalar(self, var, value, single=False):
+        fn = _lib().iarray_expr_bind_scalar_float if single else _lib().iarray_expr_bind_scalar_double
+        check(fn(self.ptr, var.encode(), value), "iarray_expr_bind_scalar")
+
+    def bind_out(self, shape, dtype, chunkshape, blockshape, urlpath=None, contiguous=True):
+        d = dtshape(shape, dtype)
+        s = storage(chunkshape, blockshape, urlpath, contiguous)
+        check(_lib().iarray_expr_bind_out_properties(self.ptr, ctypes.byref(d), ctypes.byref(s)),
+              "iarray_expr_bind_out_properties")
+
+    def compile(self, text):
+        check(_lib().iarray_expr_compile(self.ptr, text.encode()), "iarray_expr_compile")
+
+    def eval(self):
+        p = ctypes.c_void_p()
+        check(_lib().iarray_eval(self.ptr, ctypes.byref(p)), "iarray_eval")
+        return Container(self.ctx, p)
+
+    def free(self):
+        if self.ptr:
+            _lib().iarray_expr_free(self.ctx.ptr, ctypes.byref(self.ptr))
+            self.ptr = ctypes.c_void_p()

@@ -265,3 +265,52 @@ def test_gpu_parallel_encoder_stress(ia, n):
         (chunk,) = c.chunks()
         assert O.chunk_decompress(chunk) == a.tobytes()
         _check_streams_with_liblz4(chunk)
+
+
+def _mixed_stream_bytes(rng, n):
+    """Bytes whose LZ4 encoding has long literal runs, runs with offsets 1-7, matches within
+    2 KiB and beyond it, and stretches of dense short sequences."""
+    out = bytearray()
+    while len(out) < n:
+        kind = rng.integers(0, 5)
+        if kind == 0:                                          # literals
+            out += rng.integers(0, 256, int(rng.integers(100, 3000)), dtype=np.uint8).tobytes()
+        elif kind == 1 and len(out) > 8:                       # short-offset run
+            d = int(rng.integers(1, 8))
+            pat = bytes(out[-d:])
+            out += (pat * (int(rng.integers(50, 6000)) // d + 1))
+        elif kind == 2 and len(out) > 3000:                    # far match (beyond the ring)
+            s = len(out) - int(rng.integers(2100, 3000))
+            out += bytes(out[s:s + int(rng.integers(20, 500))])
+        elif kind == 3 and len(out) > 2000:                    # match within 2 KiB
+            s = len(out) - int(rng.integers(130, 1900))
+            out += bytes(out[s:s + int(rng.integers(5, 300))])
+        else:                                                  # dense short sequences
+            base = rng.integers(0, 4, 4000, dtype=np.uint8) + 60
+            out += base.tobytes()
+    return np.frombuffer(bytes(out[:n]), np.uint8).copy()
+
+
+def test_gpu_decodes_mixed_lz4_streams(ctx, ia):
+    """Streams of every shape in one launch (long literal runs, runs with offsets 1-7,
+    matches within and beyond 2 KiB, dense short sequences): bit-exact."""
+    rng = np.random.default_rng(41)
+    n = 1 << 20
+    a = _mixed_stream_bytes(rng, n)
+    g, chunks = O.encode_array(a, (262144,), (65536,))
+    kinds = [cs for ch in chunks for blk in O.chunk_streams(ch) for cs, _ in blk]
+    assert any(0 < cs < 65536 for cs in kinds)                 # LZ4 streams present
+    c = ia.Container.from_chunks(ctx, a.shape, np.uint8, (262144,), (65536,), chunks)
+    assert c.to_numpy().tobytes() == a.tobytes()
+    # float32 data of the plain GEMV workload: literal-heavy low planes, run-like high planes
+    i = np.arange(512)
+    f = (np.sin(0.001 * (i[:, None] + 3000)) + np.cos(0.002 * i[None, :])).astype(np.float32)
+    g2, ch2 = O.encode_array(f, (512, 512), (256, 256))
+    c2 = ia.Container.from_chunks(ctx, f.shape, np.float32, (512, 512), (256, 256), ch2)
+    assert c2.to_numpy().tobytes() == f.tobytes()
+    # corrupted: a truncated LZ4 stream is reported, not decoded
+    bad = bytearray(chunks[0])
+    bad[12:16] = (len(bad) - 7).to_bytes(4, "little")
+    c3 = ia.Container.from_chunks(ctx, (262144,), np.uint8, (262144,), (65536,), [bytes(bad[:-7])])
+    with pytest.raises(ia.IArrayError):
+        c3.to_numpy()
