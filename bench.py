@@ -708,6 +708,7 @@ def run_kernel_case(args):
     values (gaussian) encoded with the parallel encoder, then an A-like one
     (uniform(-1,1) x 2^U{-8..8}) decoded; three rounds each.  split: the split-precision
     float64 product n x n x n on device operands (iarray_b200_dense_gemm), two rounds.
+    f32split: the float32 split form (six BF16 products) n x n x n, two rounds.
     Inputs are larger than L2 and a few GB at most are held on the device."""
     import ctypes
     import torch
@@ -727,6 +728,20 @@ def run_kernel_case(args):
             a.decode_to_device(out.data_ptr(), n)
         ctx.synchronize()
         assert np.array_equal(out.cpu().numpy(), A)
+    elif args.kernel_case == "f32split":
+        ctx = ia.Context(form=ia.FORM_SPLIT)
+        A = torch.from_numpy(rng.standard_normal((n, n)).astype(np.float32)).cuda()
+        B = torch.from_numpy(rng.standard_normal((n, n)).astype(np.float32)).cuda()
+        C = torch.empty((n, n), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        for _ in range(2):
+            ia.check(ia.lib().iarray_b200_dense_gemm(ctx.ptr, ia.DTYPE_FLOAT, n, n, n, ctypes.c_void_p(A.data_ptr()), n,
+                                                      ctypes.c_void_p(B.data_ptr()), n, ctypes.c_void_p(C.data_ptr()), n),
+                     "dense_gemm")
+        ctx.synchronize()
+        ref = (A[:64].double() @ B.double()).cpu().numpy()
+        err = np.linalg.norm(C[:64].cpu().numpy() - ref) / np.linalg.norm(ref)
+        assert err < 2e-6, err
     else:
         ctx = ia.Context(form=ia.FORM_SPLIT)
         A = torch.from_numpy(rng.uniform(-1, 1, (n, n)) * np.exp2(rng.integers(-8, 9, (n, n)))).cuda()
@@ -754,7 +769,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-samples", type=int, default=3, help="whole-product samples of the CPU baseline")
     ap.add_argument("--no-secondary", action="store_true", help="skip the GEMV, float32 and batching workloads")
-    ap.add_argument("--kernel-case", choices=["codec", "split"], default=None,
+    ap.add_argument("--kernel-case", choices=["codec", "split", "f32split"], default=None,
                     help="run one small case of one kernel family instead of the benchmark")
     ap.add_argument("--case-n", type=int, default=4096, help="matrix size of --kernel-case")
     args = ap.parse_args()

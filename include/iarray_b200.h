@@ -432,8 +432,9 @@ INA_API(ina_rc_t) iarray_b200_opt_gemm_cframes(iarray_context_t *ctx, const uint
  * configurations on them (autotuner; choice cached per set of shapes), runs the batch once
  * and captures decode -> product -> encode of every problem in one CUDA graph: in the
  * native form the products of all problems are one persistent grouped kernel launch, in
- * the split form (context form IARRAY_B200_FORM_SPLIT) each problem's split-precision
- * pipeline.  iarray_b200_batch_run replays the graph and returns n new containers in c
+ * the split form (context form IARRAY_B200_FORM_SPLIT) one grouped split-precision
+ * pipeline (seven launches over all problems: scaling, residues, one persistent INT8
+ * tensor-core launch over every problem's tiles and moduli, reconstruction).  iarray_b200_batch_run replays the graph and returns n new containers in c
  * (free each with iarray_container_free).  The operand containers are borrowed: they must
  * stay alive and unchanged until iarray_b200_batch_free.  Operands must not be transposed
  * views. */
@@ -447,6 +448,16 @@ INA_API(ina_rc_t) iarray_b200_batch_run(iarray_b200_batch_t *batch, iarray_conta
  * measured, e.g. a cached choice), and the number of nodes of the captured graph. */
 INA_API(ina_rc_t) iarray_b200_batch_info(iarray_b200_batch_t *batch, int *tile_config, double *tune_ms,
                                          int64_t *graph_nodes);
+/* Split form: the number of moduli the batch uses.  When the context's count is automatic
+ * (iarray_b200_set_split_terms(ctx, 0)), iarray_b200_batch_new tunes it on the batch's own
+ * operands: 16 moduli serve as the reference, the native FP64 product's normwise error
+ * against it sets the bar, and of 16..12 moduli the fastest whose error stays within 4x that
+ * bar is kept (cached per set of shapes).  *err_native receives the bar's base error,
+ * tune_ms[5] / tune_err[5] the time and error of 16, 15, 14, 13, 12 moduli (-1: not measured,
+ * e.g. a cached choice or a count fixed by the context).  IARRAY_ERR invalid argument for a
+ * batch in the native form. */
+INA_API(ina_rc_t) iarray_b200_batch_split_tuning(iarray_b200_batch_t *batch, int *nterms, double *err_native,
+                                                 double *tune_ms, double *tune_err);
 INA_API(void) iarray_b200_batch_free(iarray_b200_batch_t **batch);
 
 /* Per-kernel device time (B200 addition; the reference has no counterpart).  While

@@ -1778,7 +1778,11 @@ struct iarray_b200_batch_s {
     iab::DecodeQueue dq;              // the LZ4 streams of every operand
     std::vector<iab::EncodeWork> enc;
     DevBuf eimg, eslots, ees, ecursor;  // outputs' byte-plane images, LZ4 slots, stream results, cursor
-    std::vector<iab::OzakiWork> oz;
+    iab::OzGroupWork ozg;             // split form: every product in one grouped pipeline
+    int split_terms = 0;              // split form: moduli in use (context's choice or the autotuner's)
+    double split_err_native = -1;     // autotuner: normwise error of the native product vs 16 moduli
+    double split_tune_ms[5] = {-1, -1, -1, -1, -1};    // autotuner: 16, 15, 14, 13, 12 moduli
+    double split_tune_err[5] = {-1, -1, -1, -1, -1};
     DevBuf status;                    // 16 ints per decode: [2i] operand A, [2i + 1] operand B
     DevBuf chunks;                    // chunk tables of all outputs
     std::vector<int64_t> chunk_base;  // first entry of output i in `chunks`
@@ -1882,16 +1886,8 @@ int batch_enqueue(iarray_b200_batch_t *bt, int parts)
     }
     if (!(parts & 2)) {
     } else if (bt->form == IARRAY_B200_FORM_SPLIT) {
-        batch_fork(bt);
-        for (int64_t i = 0; i < bt->n; i++) {
-            const int r = iab::gemm_f64_ozaki_launch(bt->M[(size_t)i], bt->N[(size_t)i], bt->K[(size_t)i],
-                                                     bt->dA[(size_t)i].as<double>(), bt->lda[(size_t)i],
-                                                     bt->dB[(size_t)i].as<double>(), bt->ldb[(size_t)i],
-                                                     bt->dC[(size_t)i].as<double>(), bt->ldc[(size_t)i],
-                                                     bt->ctx->split_terms, &bt->oz[(size_t)i], bt->br[(size_t)i % nbr]);
-            if (r) { batch_join(bt); return r; }
-        }
-        batch_join(bt);
+        const int r = iab::gemm_f64_ozaki_grouped_launch(&bt->ozg, st);
+        if (r) return r;
     } else if (bt->total_tiles > 0) {
         iab::gemm_f64_grouped(bt->cfg, bt->probs.as<iab::GemmProblem>(), (int)bt->hprobs.size(), bt->total_tiles,
                               bt->ctas, st);
@@ -1978,12 +1974,116 @@ ina_rc_t batch_status(iarray_b200_batch_t *bt)
         return rc_err(IARRAY_ERR_GPU_FAILED);
     for (int64_t i = 0; i < 2 * bt->n; i++)
         if (h[(size_t)(i * 16 + 1)]) return status_rc(h[(size_t)(i * 16 + 1)]);
-    if (bt->form == IARRAY_B200_FORM_SPLIT)
-        for (auto &w : bt->oz)
-            if (iab::gemm_f64_ozaki_finish(&w, bt->ctx->stream)) return rc_err(IARRAY_ERR_GPU_FAILED);
+    if (bt->form == IARRAY_B200_FORM_SPLIT && iab::gemm_f64_ozaki_grouped_finish(&bt->ozg, bt->ctx->stream))
+        return rc_err(IARRAY_ERR_GPU_FAILED);
     return INA_SUCCESS;
 }
 }  // namespace
+
+// Split form: the number of moduli.  With the context's count fixed
+// (iarray_b200_set_split_terms), that count; else an error-checked autotuner on the batch's
+// own decoded operands: the products with 16 moduli (about 2^-59 relative per scaled operand:
+// exact against float64 rounding) serve as the reference, the native grouped FP64 product's
+// normwise error against it sets the bar, and of 15, 14, 13 and 12 moduli the fastest whose
+// error stays within 4x the native error is kept (16 when none is).  The choice is cached per
+// set of shapes.  The grouped pipeline's buffers and tables are then written for the chosen
+// count, before any capture.
+static ina_rc_t batch_tune_split(iarray_b200_batch_t *bt)
+{
+    iarray_context_t *ctx = bt->ctx;
+    const size_t un = (size_t)bt->n;
+    auto items_into = [&](std::vector<DevBuf> *out) {
+        std::vector<iab::OzGroupItem> items(un);
+        for (size_t i = 0; i < un; i++)
+            items[i] = iab::OzGroupItem{bt->M[i], bt->N[i], bt->K[i], bt->dA[i].as<double>(), bt->dB[i].as<double>(),
+                                        out ? (*out)[i].as<double>() : bt->dC[i].as<double>(), bt->lda[i], bt->ldb[i],
+                                        bt->ldc[i]};
+        return items;
+    };
+    int L = ctx->split_terms;
+    std::string sig = "split";
+    for (size_t i = 0; i < un; i++)
+        sig += ";" + std::to_string(bt->M[i]) + "x" + std::to_string(bt->N[i]) + "x" + std::to_string(bt->K[i]);
+    if (L <= 0) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(sig);
+        if (it != g_tune_cache.end()) L = it->second;
+    }
+    if (L <= 0) {
+        // decode every operand once (also sets up the codec kernels)
+        int r = batch_enqueue(bt, 1);
+        if (r) return batch_rc(r);
+        if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return rc_err(IARRAY_ERR_GPU_FAILED);
+        ina_rc_t rc = batch_status(bt);
+        if (INA_FAILED(rc)) return rc;
+        std::vector<DevBuf> cref(un), cnat(un);
+        for (size_t i = 0; i < un; i++)
+            if (!cref[i].allocate(bt->dC[i].n, ctx->device) || !cnat[i].allocate(bt->dC[i].n, ctx->device))
+                return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+        auto diff_vs_ref = [&](const std::vector<DevBuf> &x) {
+            std::vector<iab::DiffItem> d(un);
+            for (size_t i = 0; i < un; i++)
+                d[i] = iab::DiffItem{x[i].as<double>(), cref[i].as<double>(), bt->M[i], bt->N[i], bt->ldc[i]};
+            return iab::normwise_diff_grouped(d, ctx->stream);
+        };
+        {   // reference: 16 moduli
+            iab::OzGroupWork w;
+            r = iab::gemm_f64_ozaki_grouped_setup(items_into(&cref), 16, &w, ctx->stream);
+            if (!r) r = iab::gemm_f64_ozaki_grouped_launch(&w, ctx->stream);
+            if (!r) r = iab::gemm_f64_ozaki_grouped_finish(&w, ctx->stream);
+            if (r) return rc_err(r == -100 ? IARRAY_ERR_GPU_OUT_OF_MEMORY : IARRAY_ERR_GPU_FAILED);
+        }
+        {   // the native grouped FP64 product sets the bar
+            std::vector<iab::GemmProblem> hp;
+            int total = 0;
+            batch_problems(bt, 0, &hp, &total);
+            std::vector<iab::GemmProblem> hn = hp;
+            for (auto &q : hn)
+                for (size_t i = 0; i < un; i++)
+                    if (q.C == bt->dC[i].as<double>()) q.C = cnat[i].as<double>();
+            DevBuf dp;
+            if (!dp.allocate(std::max<size_t>(hn.size(), 1) * sizeof(iab::GemmProblem), ctx->device))
+                return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+            cudaMemcpyAsync(dp.p, hn.data(), hn.size() * sizeof(iab::GemmProblem), cudaMemcpyHostToDevice, ctx->stream);
+            if (total > 0)
+                iab::gemm_f64_grouped(0, dp.as<iab::GemmProblem>(), (int)hn.size(), total, iab::gemm_f64_grouped_ctas(0),
+                                      ctx->stream);
+            bt->split_err_native = diff_vs_ref(cnat);
+        }
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        double best = -1.0;
+        L = 16;
+        for (int cand = 16; cand >= 12; cand--) {
+            iab::OzGroupWork w;
+            r = iab::gemm_f64_ozaki_grouped_setup(items_into(nullptr), cand, &w, ctx->stream);
+            if (r) break;
+            iab::gemm_f64_ozaki_grouped_launch(&w, ctx->stream);               // warm-up
+            cudaEventRecord(e0, ctx->stream);
+            for (int rep = 0; rep < 2; rep++) iab::gemm_f64_ozaki_grouped_launch(&w, ctx->stream);
+            cudaEventRecord(e1, ctx->stream);
+            if (iab::gemm_f64_ozaki_grouped_finish(&w, ctx->stream)) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            const double err = diff_vs_ref(bt->dC);
+            bt->split_tune_ms[16 - cand] = ms / 2;
+            bt->split_tune_err[16 - cand] = err;
+            const bool within = err >= 0.0 && err <= 4.0 * bt->split_err_native;
+            if (within && (best < 0.0 || ms / 2 < best)) { best = ms / 2; L = cand; }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (cudaGetLastError() != cudaSuccess) return rc_err(IARRAY_ERR_GPU_FAILED);
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[sig] = L;
+    }
+    bt->split_terms = L;
+    const int r = iab::gemm_f64_ozaki_grouped_setup(items_into(nullptr), L, &bt->ozg, ctx->stream);
+    if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    if (r) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
+    return INA_SUCCESS;
+}
 
 INA_API(ina_rc_t) iarray_b200_batch_new(iarray_context_t *ctx, int64_t n, iarray_container_t *const *a,
                                         iarray_container_t *const *b, const iarray_storage_t *storage,
@@ -2021,7 +2121,6 @@ INA_API(ina_rc_t) iarray_b200_batch_new(iarray_context_t *ctx, int64_t n, iarray
     bt->M.resize(un); bt->N.resize(un); bt->K.resize(un); bt->lda.resize(un); bt->ldb.resize(un); bt->ldc.resize(un);
     bt->dA.resize(un); bt->dB.resize(un); bt->dC.resize(un); bt->cbuf.resize(un);
     bt->decA.resize(un); bt->decB.resize(un); bt->enc.resize(un);
-    if (bt->form == IARRAY_B200_FORM_SPLIT) bt->oz.resize(un);
     bt->chunk_base.resize(un);
     int64_t nch = 0;
     for (size_t i = 0; i < un; i++) {
@@ -2041,6 +2140,10 @@ INA_API(ina_rc_t) iarray_b200_batch_new(iarray_context_t *ctx, int64_t n, iarray
     if (!bt->status.allocate((size_t)(n * 32 * sizeof(int)), ctx->device) ||
         !bt->chunks.allocate((size_t)std::max<int64_t>(nch, 1) * sizeof(iab::EncChunk), ctx->device))
         return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    if (bt->form == IARRAY_B200_FORM_SPLIT) {
+        ina_rc_t rc = batch_tune_split(bt.get());
+        if (INA_FAILED(rc)) return rc;
+    }
     cudaMemsetAsync(bt->status.p, 0, bt->status.n, ctx->stream);
     // autotuner (native form): time every tile configuration of the grouped kernel on the
     // decoded operands of this batch; the choice is cached per problem-set signature
@@ -2203,6 +2306,20 @@ INA_API(ina_rc_t) iarray_b200_batch_info(iarray_b200_batch_t *bt, int *tile_conf
     if (tune_ms)
         for (int k = 0; k < 4; k++) tune_ms[k] = bt->tune_ms[k];
     if (graph_nodes) *graph_nodes = bt->nodes;
+    return INA_SUCCESS;
+}
+
+INA_API(ina_rc_t) iarray_b200_batch_split_tuning(iarray_b200_batch_t *bt, int *nterms, double *err_native,
+                                                 double *tune_ms, double *tune_err)
+{
+    CHECK_ARG(bt);
+    if (bt->form != IARRAY_B200_FORM_SPLIT) return rc_err(INA_ERR_INVALID_ARGUMENT);
+    if (nterms) *nterms = bt->split_terms;
+    if (err_native) *err_native = bt->split_err_native;
+    for (int i = 0; i < 5; i++) {
+        if (tune_ms) tune_ms[i] = bt->split_tune_ms[i];
+        if (tune_err) tune_err[i] = bt->split_tune_err[i];
+    }
     return INA_SUCCESS;
 }
 

@@ -301,6 +301,35 @@ int gemm_f64_ozaki_rows_product(int64_t M, const double *A, int64_t lda, const O
 int gemm_f64_ozaki_rows(int64_t M, const double *A, int64_t lda, const OzakiB &ob, double *C, int64_t ldc,
                         OzakiWork *w, cudaStream_t st);
 int gemm_f64_ozaki_finish(OzakiWork *w, cudaStream_t st);
+// Grouped split-precision form: many independent products in one pipeline of seven kernel
+// launches over a table of products (split.cu).  setup allocates every buffer and writes the
+// tables (synchronously; call it outside stream capture); launch enqueues the kernels on `st`
+// (capturable); finish reads the status word.
+struct OzGroupItem {
+    int64_t M, N, K;
+    const double *A;
+    const double *B;
+    double *C;
+    int64_t lda, ldb, ldc;
+};
+struct OzGroupWork {
+    DevBuf ra, rb, rr, sa, sb, pm, ps, probs, maps, err;
+    int L = 0, nc = 0, np = 0;
+    double gamma = 0;
+    int64_t rows = 0, cols = 0, tasks_r = 0, tiles_c = 0, items = 0, crt = 0;
+};
+int gemm_f64_ozaki_grouped_setup(const std::vector<OzGroupItem> &items, int nterms, OzGroupWork *w, cudaStream_t st);
+int gemm_f64_ozaki_grouped_launch(OzGroupWork *w, cudaStream_t st);
+int gemm_f64_ozaki_grouped_finish(OzGroupWork *w, cudaStream_t st);
+// sqrt(sum_i ||X_i - Y_i||_F^2 / sum_i ||Y_i||_F^2) over M_i x N_i float64 matrices (row pitch
+// ld_i); synchronises st; < 0 on a CUDA error.
+struct DiffItem {
+    const double *X;
+    const double *Y;
+    int64_t M, N, ld;
+};
+double normwise_diff_grouped(const std::vector<DiffItem> &items, cudaStream_t st);
+
 // float32 split form: each operand split into bf16 words, `products` BF16 tensor-core
 // products (3: two words; 6: three words; 0: 6) summed in FP32 segments.
 int gemm_f32_bf16_split(int64_t M, int64_t N, int64_t K, const float *A, int64_t lda,

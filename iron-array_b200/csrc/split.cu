@@ -421,6 +421,36 @@ __device__ __forceinline__ void tile_of(int local, int tiles_m, int tiles_n, int
     tm = g * TILE_GROUP + (rem - tn * rows);
 }
 
+// One product of a grouped split-precision launch (device table, one entry per product).
+struct OzGProb {
+    int M, N, K, Kp;
+    int tiles_m, tiles_n;
+    int64_t row0, col0;          // first row / column of this product in the concatenated row / column index
+    int64_t task_r0;             // first task of the grouped row-residue kernel (8 k per task)
+    int64_t tile_c0;             // first 64 x 64 tile of the grouped column-residue kernel
+    int64_t item0;               // first item (modulus, tile) of the grouped INT8 GEMM
+    int64_t crt0;                // first task (row, 4 columns) of the grouped reconstruction
+    const double *A, *B;
+    double *C;
+    int64_t lda, ldb, ldc;
+    int8_t *ra, *rb;             // residues [L][M][Kp], [L][N][Kp]
+    uint8_t *R;                  // residues of the product [L][M][ldr]
+    int64_t ldr;
+};
+
+// Index of the product whose range [key(q), key(q + 1)) holds v: the last q with key(q) <= v
+// (products with empty ranges share their start with the next one).
+template <typename F>
+__device__ __forceinline__ int oz_find(const OzGProb *__restrict__ pr, int np, int64_t v, F key)
+{
+    int lo = 0, hi = np - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (key(pr[mid]) <= v) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 struct I8Params {
     int M, N, K, Kp, L, tiles_m, tiles_n;
     uint8_t *R;        // [L][M][ldr] residues of the products
@@ -428,7 +458,45 @@ struct I8Params {
     int *err;
     int use_skip;      // leave out the k-tiles of zero-block pairs (zskip.cuh)
     ZeroSkip zs;
+    // grouped launch: items of every product of the table, tensor maps 2q (A) and 2q + 1 (B)
+    const OzGProb *probs;
+    int nprob;
+    int64_t total;
+    const CUtensorMap *maps;
 };
+
+// The work of item t: product tile (tm, tn) for modulus l.
+struct I8Tile {
+    const CUtensorMap *ma, *mb;
+    int l, tm, tn, M, N, ktiles;
+    uint8_t *R;
+    int64_t ldr;
+};
+
+template <bool GROUPED>
+__device__ __forceinline__ I8Tile i8_tile(const I8Params &p, const CUtensorMap *tmA, const CUtensorMap *tmB, int64_t t)
+{
+    I8Tile r;
+    if constexpr (!GROUPED) {
+        r.l = (int)(t / (p.tiles_m * p.tiles_n));
+        const int rem = (int)(t - (int64_t)r.l * p.tiles_m * p.tiles_n);
+        tile_of(rem, p.tiles_m, p.tiles_n, r.tm, r.tn);
+        r.ma = tmA; r.mb = tmB;
+        r.M = p.M; r.N = p.N; r.ktiles = p.Kp / oz::BK;
+        r.R = p.R; r.ldr = p.ldr;
+    } else {
+        const int q = oz_find(p.probs, p.nprob, t, [](const OzGProb &x) { return x.item0; });
+        const OzGProb &pr = p.probs[q];
+        const int per = pr.tiles_m * pr.tiles_n;
+        const int64_t local = t - pr.item0;
+        r.l = (int)(local / per);
+        tile_of((int)(local - (int64_t)r.l * per), pr.tiles_m, pr.tiles_n, r.tm, r.tn);
+        r.ma = p.maps + 2 * q; r.mb = p.maps + 2 * q + 1;
+        r.M = pr.M; r.N = pr.N; r.ktiles = pr.Kp / oz::BK;
+        r.R = pr.R; r.ldr = pr.ldr;
+    }
+    return r;
+}
 
 // Bit kt of mask[kt / 32] = k-tile kt of output tile (tm, tn) is needed (some K block in it
 // pairs a non-zero A block under the tile's rows with a non-zero B block under its
@@ -468,10 +536,11 @@ __device__ __forceinline__ bool i8_tile_any(const I8Params &p, int tm, int tn, i
 // accumulator: r = C mod m_l in [0, m_l), stored as one byte per entry.  With use_skip,
 // the k-tiles of zero-block pairs are neither loaded nor multiplied (every role derives the
 // same mask); a tile that needs none is written as zero residues.
-template <bool SKIP>
+template <bool SKIP, bool GROUPED>
 __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_constant__ CUtensorMap tmA,
                                                                 const __grid_constant__ CUtensorMap tmB, I8Params p)
 {
+    static_assert(!(SKIP && GROUPED), "the grouped form does not skip zero blocks");
     using namespace oz;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -491,8 +560,10 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
         for (int b = 0; b < 2; b++) { tc::mbar_init(&tfull[b], 1); tc::mbar_init(&tempty[b], 4); }
         tc::mbar_init(drain, 1);
         tc::fence_barrier_init();
-        tc::tma_prefetch_desc(&tmA);
-        tc::tma_prefetch_desc(&tmB);
+        if constexpr (!GROUPED) {
+            tc::tma_prefetch_desc(&tmA);
+            tc::tma_prefetch_desc(&tmB);
+        }
     }
     if (warp == 1) {
         tc::tmem_alloc(tmem_slot, 512);
@@ -502,8 +573,8 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
-    const int total = p.L * p.tiles_m * p.tiles_n;
-    const int ktiles = p.Kp / BK;
+    const int64_t total = GROUPED ? p.total : (int64_t)p.L * p.tiles_m * p.tiles_n;
+    const int ktiles = p.Kp / BK;            // (SKIP only: the single product's k-tiles)
     auto needed = [&](const uint32_t *mask, int kt) {
         if constexpr (SKIP) return ((mask[kt >> 5] >> (kt & 31)) & 1u) != 0;
         else return true;
@@ -514,18 +585,17 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
         uint32_t phase = 0;
         int64_t issued = 0;
         bool ok = true;
-        for (int t = blockIdx.x; t < total; t += gridDim.x) {      // the whole warp walks the tiles
-            const int l = t / (p.tiles_m * p.tiles_n), rem = t - l * p.tiles_m * p.tiles_n;
-            int tm, tn;
-            tile_of(rem, p.tiles_m, p.tiles_n, tm, tn);
+        for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {  // the whole warp walks the tiles
+            const I8Tile tl = i8_tile<GROUPED>(p, &tmA, &tmB, t);
+            const int l = tl.l, tm = tl.tm, tn = tl.tn;
             if constexpr (SKIP) i8_kmask(p, tm, tn, ktiles, pmask);
             if (lane == 0) {
-                for (int kt = 0; kt < ktiles; kt++) {
+                for (int kt = 0; kt < tl.ktiles; kt++) {
                     if (!needed(pmask, kt)) continue;
                     if (!tc::mbar_wait(&empty[stage], phase ^ 1, p.err)) { ok = false; break; }
                     tc::mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
-                    tc::tma_load_3d(sA + stage * A_BYTES, &tmA, kt * BK, tm * BM, l, &full[stage]);
-                    tc::tma_load_3d(sB + stage * B_BYTES, &tmB, kt * BK, tn * BN, l, &full[stage]);
+                    tc::tma_load_3d(sA + stage * A_BYTES, tl.ma, kt * BK, tm * BM, l, &full[stage]);
+                    tc::tma_load_3d(sB + stage * B_BYTES, tl.mb, kt * BK, tn * BN, l, &full[stage]);
                     issued++;
                     if (++stage == STAGES) { stage = 0; phase ^= 1; }
                 }
@@ -541,11 +611,9 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
         int stage = 0, acc = 0;
         uint32_t phase = 0, acc_phase = 0;
         bool ok = true;
-        for (int t = blockIdx.x; t < total; t += gridDim.x) {
-            const int l = t / (p.tiles_m * p.tiles_n), rem = t - l * p.tiles_m * p.tiles_n;
-            int tm, tn;
-            tile_of(rem, p.tiles_m, p.tiles_n, tm, tn);
-            if constexpr (SKIP) i8_kmask(p, tm, tn, ktiles, mmask);
+        for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+            const I8Tile tl = i8_tile<GROUPED>(p, &tmA, &tmB, t);
+            if constexpr (SKIP) i8_kmask(p, tl.tm, tl.tn, ktiles, mmask);
             if (lane == 0) {
                 if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, p.err)) {
                     ok = false;
@@ -553,7 +621,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
                     tc::tc_fence_after();
                     const uint32_t dt = tmem_base + (uint32_t)(acc * BN);
                     bool any = false;
-                    for (int kt = 0; kt < ktiles; kt++) {
+                    for (int kt = 0; kt < tl.ktiles; kt++) {
                         if (!needed(mmask, kt)) continue;
                         if (!tc::mbar_wait(&full[stage], phase, p.err)) { ok = false; break; }
                         tc::tc_fence_after();
@@ -586,10 +654,9 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
         const int q = warp & 3;   // TMEM lane quarter this warp may access
         int acc = 0;
         uint32_t acc_phase = 0;
-        for (int t = blockIdx.x; t < total; t += gridDim.x) {
-            const int l = t / (p.tiles_m * p.tiles_n), rem = t - l * p.tiles_m * p.tiles_n;
-            int tm, tn;
-            tile_of(rem, p.tiles_m, p.tiles_n, tm, tn);
+        for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+            const I8Tile tl = i8_tile<GROUPED>(p, &tmA, &tmB, t);
+            const int l = tl.l, tm = tl.tm, tn = tl.tn;
             bool active = true;
             if constexpr (SKIP) active = i8_tile_any(p, tm, tn, ktiles);
             if (!tc::mbar_wait(&tfull[acc], acc_phase, p.err)) break;
@@ -597,7 +664,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
             const int m = c_crt.mod[l];
             const float invm = c_crt.inv_modf[l];
             const int row = tm * BM + q * 32 + lane;
-            uint8_t *out = p.R + ((int64_t)l * p.M + row) * p.ldr + (int64_t)tn * BN;
+            uint8_t *out = tl.R + ((int64_t)l * tl.M + row) * tl.ldr + (int64_t)tn * BN;
             for (int c = 0; c < BN; c += 32) {
                 uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                 if (active) {
@@ -619,15 +686,15 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
                     }
                 }
                 const int col = tn * BN + c;
-                if (row < p.M) {
-                    if (col + 32 <= p.N) {
+                if (row < tl.M) {
+                    if (col + 32 <= tl.N) {
                         uint4 *o4 = reinterpret_cast<uint4 *>(out + c);
                         o4[0] = make_uint4(w[0], w[1], w[2], w[3]);
                         o4[1] = make_uint4(w[4], w[5], w[6], w[7]);
                     } else {
 #pragma unroll
                         for (int b = 0; b < 32; b++)
-                            if (col + b < p.N) out[c + b] = (uint8_t)(w[b >> 2] >> (8 * (b & 3)));
+                            if (col + b < tl.N) out[c + b] = (uint8_t)(w[b >> 2] >> (8 * (b & 3)));
                     }
                 }
             }
@@ -689,17 +756,14 @@ __device__ __forceinline__ double unscale(double x, int e)
 }
 
 // C_ij = 2^-(sA_i + sB_j) * centred( sum_l r_l w_l mod P ); four entries per thread.
+// Outputs j0 .. j0 + 3 of row i of one product: reconstruction from the L residue planes
+// R[l][i][j] (plane = M ldr bytes), unscaled by the row and column shifts.
 template <int NC>
-__global__ void __launch_bounds__(256) k_crt(int M, int N, const uint8_t *__restrict__ R, int64_t ldr,
-                                             const int *__restrict__ sA, const int *__restrict__ sB,
-                                             double *__restrict__ C, int64_t ldc)
+__device__ __forceinline__ void crt_quad(int N, const uint8_t *__restrict__ R, int64_t ldr, int64_t plane, int si,
+                                         const int *__restrict__ sB, double *__restrict__ C, int64_t ldc, int i, int j0)
 {
     const int L = c_crt.L;
-    const int64_t plane = (int64_t)M * ldr;
-    const int nq = (N + 3) / 4;
-    const int64_t total = (int64_t)M * nq;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-        const int i = (int)(e / nq), j0 = (int)(e - (int64_t)i * nq) * 4;
+    {
         const uint8_t *rp = R + (int64_t)i * ldr + j0;
         uint32_t w[16];
 #pragma unroll
@@ -731,7 +795,6 @@ __global__ void __launch_bounds__(256) k_crt(int M, int N, const uint8_t *__rest
                 }
             }
         }
-        const int si = sA[i];
         double v[4];
         bool ok[4];
 #pragma unroll
@@ -753,6 +816,21 @@ __global__ void __launch_bounds__(256) k_crt(int M, int N, const uint8_t *__rest
             for (int u = 0; u < 4; u++)
                 if (j0 + u < N) cp[u] = v[u];
         }
+    }
+}
+
+
+template <int NC>
+__global__ void __launch_bounds__(256) k_crt(int M, int N, const uint8_t *__restrict__ R, int64_t ldr,
+                                             const int *__restrict__ sA, const int *__restrict__ sB,
+                                             double *__restrict__ C, int64_t ldc)
+{
+    const int64_t plane = (int64_t)M * ldr;
+    const int nq = (N + 3) / 4;
+    const int64_t total = (int64_t)M * nq;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e / nq), j0 = (int)(e - (int64_t)i * nq) * 4;
+        crt_quad<NC>(N, R, ldr, plane, sA[i], sB, C, ldc, i, j0);
     }
 }
 
@@ -912,17 +990,17 @@ int gemm_f64_ozaki_rows_product(int64_t M, const double *A, int64_t lda, const O
     prm.R = w->rr.as<uint8_t>(); prm.ldr = ldr; prm.err = w->err.as<int>();
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_i8gemm_mod<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, oz::SMEM);
-        cudaFuncSetAttribute(k_i8gemm_mod<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, oz::SMEM);
+        cudaFuncSetAttribute(k_i8gemm_mod<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, oz::SMEM);
+        cudaFuncSetAttribute(k_i8gemm_mod<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, oz::SMEM);
         attr = true;
     }
     const int tiles = L * prm.tiles_m * prm.tiles_n;
     const CUtensorMap &tmA = *reinterpret_cast<const CUtensorMap *>(w->tmA);
     const CUtensorMap &tmB = *reinterpret_cast<const CUtensorMap *>(ob.tmB);
     if (prm.use_skip)
-        IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<true><<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
+        IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<true, false><<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
     else
-        IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<false><<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
+        IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<false, false><<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
     launch_crt(ob.nc, (unsigned)(nsm * 8), (int)M, (int)N, w->rr.as<uint8_t>(), ldr, w->sa.as<int>(), ob.sb.as<int>(), C, ldc, st);
     launch_nonfinite_fix<double>(M, N, K, A, lda, ob.B, ob.ldb, C, ldc, w->sa.as<int>(), ob.sb.as<int>(), kNonFinite, st);
     return 0;
@@ -944,6 +1022,385 @@ int gemm_f64_ozaki_launch(int64_t M, int64_t N, int64_t K, const double *A, int6
     const int r = gemm_f64_ozaki_prepare_b(K, N, B, ldb, nterms, &w->b, st);
     if (r) return r;
     return gemm_f64_ozaki_rows(M, A, lda, w->b, C, ldc, w, st);
+}
+
+// ============================================================================ grouped form
+// Many independent products C_q = A_q B_q in one pipeline: every kernel of the split
+// product runs once over a table of products (OzGProb), with the products' rows, columns,
+// residue tasks and GEMM items numbered consecutively, so a batch costs seven launches
+// however many products it holds.  The INT8 GEMM reads each product's residues through
+// that product's tensor maps, kept in a device array.
+__global__ void __launch_bounds__(256) k_row_shift_g(const OzGProb *__restrict__ pr, int np, int64_t rows,
+                                                     double gamma, int *__restrict__ shift)
+{
+    const int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (g >= rows) return;
+    const OzGProb &q = pr[oz_find(pr, np, g, [](const OzGProb &x) { return x.row0; })];
+    const double *row = q.A + (g - q.row0) * q.lda;
+    const int K = q.K;
+    double mx = 0.0, ss = 0.0;
+    for (int k = lane; k < K; k += 32) {
+        const double v = fabs(row[k]);
+        mx = fmax(mx, v);
+        ss = fma(v, v, ss);
+    }
+    for (int o = 16; o; o >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    }
+    if (isnan(ss) || isinf(mx)) {
+        if (lane == 0) shift[g] = kNonFinite;
+        return;
+    }
+    double lg = 0.5 * log2(ss);
+    if (mx > 0.0 && norm_needs_rescale(mx)) {
+        int e;
+        frexp(mx, &e);
+        double s2 = 0.0;
+        for (int k = lane; k < K; k += 32) {
+            const double v = ldexp(fabs(row[k]), -e);
+            s2 = fma(v, v, s2);
+        }
+        for (int o = 16; o; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        lg = 0.5 * log2(s2) + e;
+    }
+    if (lane == 0) shift[g] = pick_shift(mx, lg, gamma);
+}
+
+__global__ void __launch_bounds__(256) k_residues_rows_g(const OzGProb *__restrict__ pr, int np, int64_t tasks,
+                                                         const int *__restrict__ shift)
+{
+    const int L = c_crt.L;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tasks; t += (int64_t)gridDim.x * blockDim.x) {
+        const OzGProb &q = pr[oz_find(pr, np, t, [](const OzGProb &x) { return x.task_r0; })];
+        const int groups = q.Kp / 8;
+        const int64_t lt = t - q.task_r0;
+        const int i = (int)(lt / groups), k0 = (int)(lt - (int64_t)i * groups) * 8;
+        const int s = shift[q.row0 + i];
+        const bool p2 = s >= -1022 && s <= 1023, fin = s != kNonFinite;
+        const double f = p2 ? pow2i(s) : 0.0;
+        double x[8];
+        uint32_t xl[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int k = k0 + u;
+            xl[u] = 0u;
+            x[u] = k < q.K && fin ? scaled_int(q.A[(int64_t)i * q.lda + k], s, p2, f, xl[u]) : 0.0;
+        }
+#pragma unroll
+        for (int l = 0; l < 16; l++) {
+            if (l < L) {
+                uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+                for (int u = 0; u < 4; u++) w0 |= residue_byte(x[u], xl[u], l) << (8 * u);
+#pragma unroll
+                for (int u = 0; u < 4; u++) w1 |= residue_byte(x[4 + u], xl[4 + u], l) << (8 * u);
+                *reinterpret_cast<uint2 *>(q.ra + ((int64_t)l * q.M + i) * q.Kp + k0) = make_uint2(w0, w1);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_col_partial_g(const OzGProb *__restrict__ pr, int np, int64_t cols,
+                                                       double *__restrict__ pmax, double *__restrict__ pss)
+{
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int seg = blockIdx.y;
+    if (g >= cols) return;
+    const OzGProb &q = pr[oz_find(pr, np, g, [](const OzGProb &x) { return x.col0; })];
+    const int64_t j = g - q.col0;
+    const int K = q.K, per = (K + COL_SEGS - 1) / COL_SEGS, k0 = seg * per, k1 = min(K, k0 + per);
+    double mx = 0.0, ss = 0.0;
+    for (int k = k0; k < k1; k++) {
+        const double v = fabs(q.B[(int64_t)k * q.ldb + j]);
+        mx = fmax(mx, v);
+        ss = fma(v, v, ss);
+    }
+    pmax[(int64_t)seg * cols + g] = mx;
+    pss[(int64_t)seg * cols + g] = ss;
+}
+
+__global__ void k_col_shift_g(const OzGProb *__restrict__ pr, int np, int64_t cols, const double *__restrict__ pmax,
+                              const double *__restrict__ pss, double gamma, int *__restrict__ shift)
+{
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= cols) return;
+    const OzGProb &q = pr[oz_find(pr, np, g, [](const OzGProb &x) { return x.col0; })];
+    const int64_t j = g - q.col0;
+    double mx = 0.0, ss = 0.0;
+    for (int sg = 0; sg < COL_SEGS; sg++) {
+        mx = fmax(mx, pmax[(int64_t)sg * cols + g]);
+        ss += pss[(int64_t)sg * cols + g];
+    }
+    if (isnan(ss) || isinf(mx)) {
+        shift[g] = kNonFinite;
+        return;
+    }
+    double lg = 0.5 * log2(ss);
+    if (mx > 0.0 && norm_needs_rescale(mx)) {
+        int e;
+        frexp(mx, &e);
+        double s2 = 0.0;
+        for (int k = 0; k < q.K; k++) {
+            const double v = ldexp(fabs(q.B[(int64_t)k * q.ldb + j]), -e);
+            s2 = fma(v, v, s2);
+        }
+        lg = 0.5 * log2(s2) + e;
+    }
+    shift[g] = pick_shift(mx, lg, gamma);
+}
+
+// One 64 x 64 tile of one product's B per CTA step (as k_residues_cols).
+__global__ void __launch_bounds__(256) k_residues_cols_g(const OzGProb *__restrict__ pr, int np, int64_t tiles,
+                                                         const int *__restrict__ shift)
+{
+    __shared__ double tile[64][65];
+    const int L = c_crt.L;
+    for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {                 // block-uniform loop
+        const OzGProb &q = pr[oz_find(pr, np, t, [](const OzGProb &x) { return x.tile_c0; })];
+        const int tx_n = (q.N + 63) / 64;
+        const int64_t lt = t - q.tile_c0;
+        const int ty = (int)(lt / tx_n), tx = (int)(lt - (int64_t)ty * tx_n);
+        const int k0 = ty * 64, j0 = tx * 64;
+        __syncthreads();                                                       // the previous tile is read
+        for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
+            const int r = e >> 6, c = e & 63;
+            const int k = k0 + r, j = j0 + c;
+            tile[r][c] = (k < q.K && j < q.N) ? q.B[(int64_t)k * q.ldb + j] : 0.0;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < 64 * 8; e += blockDim.x) {
+            const int c = e >> 3, kg = (e & 7) * 8;
+            const int j = j0 + c;
+            if (j >= q.N || k0 + kg >= q.Kp) continue;
+            const int s = shift[q.col0 + j];
+            const bool p2 = s >= -1022 && s <= 1023, fin = s != kNonFinite;
+            const double f = p2 ? pow2i(s) : 0.0;
+            double x[8];
+            uint32_t xl[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                xl[u] = 0u;
+                x[u] = fin ? scaled_int(tile[kg + u][c], s, p2, f, xl[u]) : 0.0;
+            }
+#pragma unroll
+            for (int l = 0; l < 16; l++) {
+                if (l < L) {
+                    uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+                    for (int u = 0; u < 4; u++) w0 |= residue_byte(x[u], xl[u], l) << (8 * u);
+#pragma unroll
+                    for (int u = 0; u < 4; u++) w1 |= residue_byte(x[4 + u], xl[4 + u], l) << (8 * u);
+                    *reinterpret_cast<uint2 *>(q.rb + ((int64_t)l * q.N + j) * q.Kp + k0 + kg) = make_uint2(w0, w1);
+                }
+            }
+        }
+    }
+}
+
+template <int NC>
+__global__ void __launch_bounds__(256) k_crt_g(const OzGProb *__restrict__ pr, int np, int64_t tasks,
+                                               const int *__restrict__ sA, const int *__restrict__ sB)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tasks; e += (int64_t)gridDim.x * blockDim.x) {
+        const OzGProb &q = pr[oz_find(pr, np, e, [](const OzGProb &x) { return x.crt0; })];
+        const int nq = (q.N + 3) / 4;
+        const int64_t lt = e - q.crt0;
+        const int i = (int)(lt / nq), j0 = (int)(lt - (int64_t)i * nq) * 4;
+        crt_quad<NC>(q.N, q.R, q.ldr, (int64_t)q.M * q.ldr, sA[q.row0 + i], sB + q.col0, q.C, q.ldc, i, j0);
+    }
+}
+
+// Rows and columns holding NaN or infinity, of every product: one warp per row (global row
+// index < rows) or column (the rest), recomputing its outputs as plain dot products.
+__global__ void __launch_bounds__(256) k_nonfinite_fix_g(const OzGProb *__restrict__ pr, int np, int64_t rows,
+                                                         int64_t cols, const int *__restrict__ sA,
+                                                         const int *__restrict__ sB)
+{
+    const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w < rows) {
+        if (sA[w] != kNonFinite) return;
+        const OzGProb &q = pr[oz_find(pr, np, w, [](const OzGProb &x) { return x.row0; })];
+        const int64_t i = w - q.row0;
+        for (int j = lane; j < q.N; j += 32) {
+            double acc = 0;
+            for (int k = 0; k < q.K; k++) acc = fma(q.A[i * q.lda + k], q.B[(int64_t)k * q.ldb + j], acc);
+            q.C[i * q.ldc + j] = acc;
+        }
+    } else if (w < rows + cols) {
+        const int64_t g = w - rows;
+        if (sB[g] != kNonFinite) return;
+        const OzGProb &q = pr[oz_find(pr, np, g, [](const OzGProb &x) { return x.col0; })];
+        const int64_t j = g - q.col0;
+        for (int i = lane; i < q.M; i += 32) {
+            double acc = 0;
+            for (int k = 0; k < q.K; k++) acc = fma(q.A[(int64_t)i * q.lda + k], q.B[(int64_t)k * q.ldb + j], acc);
+            q.C[(int64_t)i * q.ldc + j] = acc;
+        }
+    }
+}
+
+int gemm_f64_ozaki_grouped_setup(const std::vector<OzGroupItem> &items, int nterms, OzGroupWork *w, cudaStream_t st)
+{
+    if (!device_is_sm100()) return -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int L = nterms > 0 ? nterms : 14;
+    CrtConst cc;
+    if (!set_crt(L, &cc, st)) return -1;
+    w->L = L;
+    w->nc = cc.nc;
+    w->gamma = (cc.log2p - 1.0) / 2.0 - 0.01;
+    std::vector<OzGProb> hp;
+    int64_t rows = 0, cols = 0, tr = 0, tc = 0, items_total = 0, crt = 0;
+    size_t ra_bytes = 0, rb_bytes = 0, r_bytes = 0;
+    for (const OzGroupItem &it : items) {
+        if (it.M <= 0 || it.N <= 0 || it.K <= 0) continue;
+        if (it.K > 65536 || it.M > (1 << 30) || it.N > (1 << 30)) return -1;
+        OzGProb q;
+        memset(&q, 0, sizeof(q));
+        q.M = (int)it.M; q.N = (int)it.N; q.K = (int)it.K; q.Kp = (int)round_up(it.K, oz::BK);
+        q.tiles_m = (int)ceil_div(it.M, oz::BM); q.tiles_n = (int)ceil_div(it.N, oz::BN);
+        q.row0 = rows; q.col0 = cols; q.task_r0 = tr; q.tile_c0 = tc; q.item0 = items_total; q.crt0 = crt;
+        q.A = it.A; q.B = it.B; q.C = it.C; q.lda = it.lda; q.ldb = it.ldb; q.ldc = it.ldc;
+        q.ldr = round_up(it.N, 16);
+        rows += it.M; cols += it.N;
+        tr += it.M * (q.Kp / 8);
+        tc += ceil_div(it.N, 64) * ceil_div(q.Kp, 64);
+        items_total += (int64_t)L * q.tiles_m * q.tiles_n;
+        crt += it.M * ceil_div(it.N, 4);
+        ra_bytes += round_up((int64_t)L * it.M * q.Kp, 256);
+        rb_bytes += round_up((int64_t)L * it.N * q.Kp, 256);
+        r_bytes += round_up((int64_t)L * it.M * q.ldr, 256);
+        hp.push_back(q);
+    }
+    w->np = (int)hp.size();
+    w->rows = rows; w->cols = cols; w->tasks_r = tr; w->tiles_c = tc; w->items = items_total; w->crt = crt;
+    if (hp.empty()) return 0;
+    if (!w->ra.allocate(ra_bytes, dev) || !w->rb.allocate(rb_bytes, dev) || !w->rr.allocate(r_bytes, dev) ||
+        !w->sa.allocate((size_t)rows * 4, dev) || !w->sb.allocate((size_t)cols * 4, dev) ||
+        !w->pm.allocate((size_t)COL_SEGS * cols * 8, dev) || !w->ps.allocate((size_t)COL_SEGS * cols * 8, dev) ||
+        !w->probs.allocate(sizeof(OzGProb) * hp.size(), dev) ||
+        !w->maps.allocate(sizeof(CUtensorMap) * 2 * hp.size(), dev) || !w->err.allocate(16, dev))
+        return -100;
+    std::vector<CUtensorMap> hm(2 * hp.size());
+    size_t oa = 0, ob = 0, orr = 0;
+    for (size_t k = 0; k < hp.size(); k++) {
+        OzGProb &q = hp[k];
+        q.ra = w->ra.as<int8_t>() + oa;
+        q.rb = w->rb.as<int8_t>() + ob;
+        q.R = w->rr.as<uint8_t>() + orr;
+        oa += round_up((int64_t)L * q.M * q.Kp, 256);
+        ob += round_up((int64_t)L * q.N * q.Kp, 256);
+        orr += round_up((int64_t)L * q.M * q.ldr, 256);
+        if (!make_tmap_3d(&hm[2 * k], CU_TENSOR_MAP_DATA_TYPE_UINT8, q.ra, (uint64_t)q.Kp, (uint64_t)q.M, (uint64_t)L,
+                          (uint64_t)q.Kp, (uint64_t)q.Kp * q.M, oz::BK, oz::BM, CU_TENSOR_MAP_SWIZZLE_128B) ||
+            !make_tmap_3d(&hm[2 * k + 1], CU_TENSOR_MAP_DATA_TYPE_UINT8, q.rb, (uint64_t)q.Kp, (uint64_t)q.N,
+                          (uint64_t)L, (uint64_t)q.Kp, (uint64_t)q.Kp * q.N, oz::BK, oz::BN, CU_TENSOR_MAP_SWIZZLE_128B))
+            return -1;
+    }
+    // the tables are written once here, outside any captured work, and only read after
+    if (cudaMemcpy(w->probs.p, hp.data(), sizeof(OzGProb) * hp.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(w->maps.p, hm.data(), sizeof(CUtensorMap) * hm.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return -2;
+    return 0;
+}
+
+int gemm_f64_ozaki_grouped_launch(OzGroupWork *w, cudaStream_t st)
+{
+    if (w->np == 0) return 0;
+    const int nsm = sms();
+    const OzGProb *pr = w->probs.as<OzGProb>();
+    cudaMemsetAsync(w->err.p, 0, 16, st);
+    IAB_TIMED("k_row_shift", st, k_row_shift_g<<<(unsigned)((w->rows * 32 + 255) / 256), 256, 0, st>>>(
+        pr, w->np, w->rows, w->gamma, w->sa.as<int>()));
+    IAB_TIMED("k_residues_rows", st, k_residues_rows_g<<<(unsigned)(nsm * 16), 256, 0, st>>>(pr, w->np, w->tasks_r,
+                                                                                       w->sa.as<int>()));
+    IAB_TIMED("k_col_partial", st, k_col_partial_g<<<dim3((unsigned)((w->cols + 255) / 256), COL_SEGS), 256, 0, st>>>(
+        pr, w->np, w->cols, w->pm.as<double>(), w->ps.as<double>()));
+    IAB_TIMED("k_col_shift", st, k_col_shift_g<<<(unsigned)((w->cols + 255) / 256), 256, 0, st>>>(
+        pr, w->np, w->cols, w->pm.as<double>(), w->ps.as<double>(), w->gamma, w->sb.as<int>()));
+    IAB_TIMED("k_residues_cols", st, k_residues_cols_g<<<(unsigned)std::min<int64_t>(w->tiles_c, (int64_t)nsm * 8), 256, 0, st>>>(
+        pr, w->np, w->tiles_c, w->sb.as<int>()));
+    I8Params prm;
+    memset(&prm, 0, sizeof(prm));
+    prm.L = w->L;
+    prm.err = w->err.as<int>();
+    prm.probs = pr;
+    prm.nprob = w->np;
+    prm.total = w->items;
+    prm.maps = w->maps.as<CUtensorMap>();
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_i8gemm_mod<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, oz::SMEM);
+        attr = true;
+    }
+    // the tensor maps of the kernel parameters are unused in the grouped form
+    CUtensorMap unused;
+    memset(&unused, 0, sizeof(unused));
+    IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<false, true><<<(unsigned)std::min<int64_t>(w->items, nsm), oz::THREADS,
+                                                               oz::SMEM, st>>>(unused, unused, prm));
+    const unsigned cg = (unsigned)std::min<int64_t>((w->crt + 255) / 256, (int64_t)nsm * 8);
+    switch (w->nc) {
+    case 1: IAB_TIMED("k_crt", st, k_crt_g<1><<<cg, 256, 0, st>>>(pr, w->np, w->crt, w->sa.as<int>(), w->sb.as<int>())); break;
+    case 2: IAB_TIMED("k_crt", st, k_crt_g<2><<<cg, 256, 0, st>>>(pr, w->np, w->crt, w->sa.as<int>(), w->sb.as<int>())); break;
+    case 3: IAB_TIMED("k_crt", st, k_crt_g<3><<<cg, 256, 0, st>>>(pr, w->np, w->crt, w->sa.as<int>(), w->sb.as<int>())); break;
+    default: IAB_TIMED("k_crt", st, k_crt_g<4><<<cg, 256, 0, st>>>(pr, w->np, w->crt, w->sa.as<int>(), w->sb.as<int>())); break;
+    }
+    IAB_TIMED("k_nonfinite_fix", st, k_nonfinite_fix_g<<<(unsigned)(((w->rows + w->cols) * 32 + 255) / 256), 256, 0, st>>>(
+        pr, w->np, w->rows, w->cols, w->sa.as<int>(), w->sb.as<int>()));
+    return 0;
+}
+
+int gemm_f64_ozaki_grouped_finish(OzGroupWork *w, cudaStream_t st)
+{
+    if (!w->err.p) return 0;
+    int h_err = 0;
+    cudaMemcpyAsync(&h_err, w->err.p, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return -2;
+    return h_err ? -3 : 0;
+}
+
+// Normwise difference over many products (the split form's autotuner): per product, one CTA
+// sums (x - y)^2 and y^2 over its M x N outputs.
+__global__ void __launch_bounds__(256) k_normdiff(const DiffItem *__restrict__ it, double *__restrict__ out)
+{
+    __shared__ double s1[256], s2[256];
+    const DiffItem d = it[blockIdx.x];
+    double a = 0.0, b = 0.0;
+    for (int64_t e = threadIdx.x; e < d.M * d.N; e += blockDim.x) {
+        const int64_t i = e / d.N, j = e - i * d.N;
+        const double x = d.X[i * d.ld + j], y = d.Y[i * d.ld + j];
+        a = fma(x - y, x - y, a);
+        b = fma(y, y, b);
+    }
+    s1[threadIdx.x] = a;
+    s2[threadIdx.x] = b;
+    __syncthreads();
+    for (int o = 128; o; o >>= 1) {
+        if (threadIdx.x < o) { s1[threadIdx.x] += s1[threadIdx.x + o]; s2[threadIdx.x] += s2[threadIdx.x + o]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { out[2 * blockIdx.x] = s1[0]; out[2 * blockIdx.x + 1] = s2[0]; }
+}
+
+double normwise_diff_grouped(const std::vector<DiffItem> &items, cudaStream_t st)
+{
+    if (items.empty()) return 0.0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    DevBuf di, dout;
+    if (!di.allocate(sizeof(DiffItem) * items.size(), dev) || !dout.allocate(16 * items.size(), dev)) return -1.0;
+    cudaMemcpyAsync(di.p, items.data(), sizeof(DiffItem) * items.size(), cudaMemcpyHostToDevice, st);
+    IAB_TIMED("k_normdiff", st, k_normdiff<<<(unsigned)items.size(), 256, 0, st>>>(di.as<DiffItem>(), dout.as<double>()));
+    std::vector<double> h(2 * items.size());
+    cudaMemcpyAsync(h.data(), dout.p, 16 * items.size(), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return -1.0;
+    double a = 0.0, b = 0.0;
+    for (size_t i = 0; i < items.size(); i++) { a += h[2 * i]; b += h[2 * i + 1]; }
+    return b > 0.0 ? sqrt(a / b) : sqrt(a);
 }
 
 // ============================================================================ float32: BF16 splits

@@ -139,6 +139,7 @@ def _lib():
             "iarray_b200_batch_new": ([P, I64, P, P, P, P], RC),
             "iarray_b200_batch_run": ([P, P], RC),
             "iarray_b200_batch_info": ([P, P, P, P], RC),
+            "iarray_b200_batch_split_tuning": ([P, P, P, P, P], RC),
             "iarray_b200_batch_free": ([P], None),
             "iarray_b200_kernel_profile": ([P, I64, P], RC),
             "iarray_b200_decode_noalloc": ([ctypes.c_int8, P, P, P, ctypes.c_int32, P, I64, P, I64, P], RC),
@@ -499,6 +500,15 @@ class Batch:
         nodes = ctypes.c_int64()
         check(_lib().iarray_b200_batch_info(self.ptr, ctypes.byref(cfg), ms, ctypes.byref(nodes)))
         return {"tile_config": cfg.value, "tune_ms": list(ms), "graph_nodes": nodes.value}
+
+    def split_tuning(self):
+        """Moduli count of a split-form batch, the native product's error (the bar's base) and
+        the tuner's time and error for 16, 15, 14, 13, 12 moduli."""
+        n, en = ctypes.c_int(), ctypes.c_double()
+        ms, err = (ctypes.c_double * 5)(), (ctypes.c_double * 5)()
+        check(_lib().iarray_b200_batch_split_tuning(self.ptr, ctypes.byref(n), ctypes.byref(en), ms, err),
+              "batch_split_tuning")
+        return {"nterms": n.value, "err_native": en.value, "tune_ms": list(ms), "tune_err": list(err)}
 
     def free(self):
         if self.ptr:

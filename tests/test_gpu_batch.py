@@ -30,7 +30,7 @@ def _problems(ia, ctx, rng, count, lo=80, hi=300):
 def test_batch_matches_single_products(ia, form):
     ctx = ia.Context()
     if form == "split":
-        ctx.set_form(ia.FORM_SPLIT)
+        ctx.set_form(ia.FORM_SPLIT, 14)      # the single products' moduli count: byte-identical results
     rng = np.random.default_rng(5)
     As, Bs, cs, bs = _problems(ia, ctx, rng, 12)
     batch = ia.Batch(ctx, As, Bs, cs, bs)
@@ -112,3 +112,33 @@ def test_batch_rejects_bad_operands(ia):
     with pytest.raises(ia.IArrayError) as e:
         ia.Batch(ctx, [a32], [f], [(4, 3)], [(2, 3)])
     assert e.value.name == "INVALID_DTYPE"
+
+
+def test_batch_split_autotunes_moduli_within_the_error_bar(ia):
+    """With the context's moduli count automatic, the split batch picks the fastest count whose
+    normwise error (against 16 moduli) stays within 4x the native FP64 product's."""
+    ctx = ia.Context()
+    ctx.set_form(ia.FORM_SPLIT)
+    rng = np.random.default_rng(9)
+    As, Bs, cs, bs = _problems(ia, ctx, rng, 10, lo=200, hi=600)
+    batch = ia.Batch(ctx, As, Bs, cs, bs)
+    t = batch.split_tuning()
+    assert 12 <= t["nterms"] <= 16
+    k = 16 - t["nterms"]
+    assert t["tune_err"][k] <= 4 * t["err_native"]
+    assert all(e >= 0 for e in t["tune_err"]) and t["err_native"] > 0
+    outs = batch.run()
+    num = den = 0.0
+    for i, c in enumerate(outs):
+        x, y = As[i].to_numpy(), Bs[i].to_numpy()
+        ref = x @ y
+        num += float(np.sum((c.to_numpy() - ref) ** 2))
+        den += float(np.sum(ref ** 2))
+        c.free()
+    assert (num / den) ** 0.5 <= 1e-14
+    # a second batch of the same shapes takes the cached choice without tuning
+    batch2 = ia.Batch(ctx, As, Bs, cs, bs)
+    t2 = batch2.split_tuning()
+    assert t2["nterms"] == t["nterms"] and t2["tune_ms"] == [-1.0] * 5
+    batch.free()
+    batch2.free()

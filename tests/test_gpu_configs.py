@@ -132,7 +132,7 @@ def _batch_config5(ia, ctx, count):
 def test_batching_config_slice_matches_single_products(ia, form):
     ctx = ia.Context(encoder=ia.ENCODER_PARALLEL)
     if form == "split":
-        ctx.set_form(ia.FORM_SPLIT)
+        ctx.set_form(ia.FORM_SPLIT, 14)      # the single products' moduli count: byte-identical results
     As, Bs = _batch_config5(ia, ctx, 64)
     cs, bs = [(512, 512)] * len(As), [(128, 128)] * len(As)
     batch = ia.Batch(ctx, As, Bs, cs, bs)
