@@ -423,6 +423,8 @@ def secondary_batch(ia, ctx, stream, args):
         batch = ia.Batch(ctx, As, Bs, cs, bs)
         build_s = time.perf_counter() - t
         info = batch.info()
+        if form == ia.FORM_SPLIT:
+            info["split_tuning"] = batch.split_tuning()
         dev, wall = [], []
         for s in range(max(1, args.warmup - 1) + max(2, args.steps // 2)):
             t = time.perf_counter()
@@ -518,6 +520,28 @@ def run_ours(args):
             r["c_cbytes"] = c_cb
             C.free()
             del c
+
+    # split form at each moduli count (rank 0, outside the timed region): device time of the
+    # step and of its product, and the normwise error on the same sampled rows
+    moduli = None
+    if rank == 0 and world == 1 and not args.no_secondary and "split" in results:
+        moduli = {"native_err": results.get("native", {}).get("err")}
+        ctx.set_encoder(ia.ENCODER_PARALLEL)
+        for L in (12, 13, 14, 15, 16):
+            ctx.set_form(ia.FORM_SPLIT, L)
+            out, prod = [], []
+
+            def step():
+                out.append(ia.opt_gemm(ctx, Ac, Bc, CHUNK, BLOCK))
+                prod.append(ctx.timings()["product"])
+                if len(out) > 1:
+                    out.pop(0).free()
+            ms, _ = _timed(ctx, stream, step, 3, 1)
+            err = O.normwise_error(out[-1].to_numpy(), hi, lo, rows)
+            out[-1].free()
+            moduli[str(L)] = {"ms_per_step": ms, "product_ms": float(np.mean(prod[1:])), "normwise_err_vs_dd": err,
+                              "err_vs_native": err / moduli["native_err"] if moduli["native_err"] else None}
+        ctx.set_form(ia.FORM_NATIVE)
 
     # end-to-end through the C ABI with host frames in pinned memory: every step uploads
     # the A and B frames (iarray_from_cframe), runs the product and writes C's frame back
@@ -693,6 +717,7 @@ def run_ours(args):
         "gpu_launches": int(hr["launches"]),
         "clocks": hr["clocks"],
         "peaks_used": {"hbm_gbs": pk.get("hbm_gbs"), "bf16_tflops": pk.get("bf16_tflops")},
+        "split_moduli": moduli,
         "secondary": secondary,
     }
     if "split" in results and "native" in results:

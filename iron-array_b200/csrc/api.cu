@@ -1774,10 +1774,10 @@ struct iarray_b200_batch_s {
     std::vector<Geom> cgeom;
     std::vector<int64_t> M, N, K, lda, ldb, ldc;
     std::vector<DevBuf> dA, dB, dC, cbuf;
-    std::vector<iab::DecodeWork> decA, decB;
-    iab::DecodeQueue dq;              // the LZ4 streams of every operand
-    std::vector<iab::EncodeWork> enc;
-    DevBuf eimg, eslots, ees, ecursor;  // outputs' byte-plane images, LZ4 slots, stream results, cursor
+    iab::CodecGroup dgrp;             // every operand's decode: one launch per stage
+    iab::CodecGroup egrp;             // every output's encode, when they share one stream shape
+    bool egroup = false;
+    std::vector<iab::EncodeWork> enc; // else each output's encode on the branches
     iab::OzGroupWork ozg;             // split form: every product in one grouped pipeline
     int split_terms = 0;              // split form: moduli in use (context's choice or the autotuner's)
     double split_err_native = -1;     // autotuner: normwise error of the native product vs 16 moduli
@@ -1851,38 +1851,10 @@ void batch_join(iarray_b200_batch_t *bt)
 int batch_enqueue(iarray_b200_batch_t *bt, int parts)
 {
     cudaStream_t st = bt->ctx->stream;
-    int *status = bt->status.as<int>();
     const size_t nbr = bt->br.size();
     if (parts & 1) {
-        // every operand's parse on the branches, one LZ4 launch for the streams of all of
-        // them, then every operand's scatter on the branches
-        auto operand = [&](int64_t i, int k) {
-            const iarray_container_t *x = k ? bt->b[(size_t)i] : bt->a[(size_t)i];
-            return iab::DecodeArgs{x->geom, x->store->buf.as<uint8_t>(), (int64_t)x->store->buf.n,
-                                   x->store->d_off.as<int64_t>(), x->store->d_len.as<int32_t>(),
-                                   (k ? bt->dB : bt->dA)[(size_t)i].p, k ? bt->ldb[(size_t)i] : bt->lda[(size_t)i]};
-        };
-        int64_t mj = 0;
-        for (int64_t i = 0; i < bt->n; i++)
-            for (int k = 0; k < 2; k++) mj += iab::decode_max_jobs(operand(i, k).g);
-        int r = iab::decode_queue_init(&bt->dq, mj, st);
+        const int r = iab::decode_group_launch(&bt->dgrp, st);
         if (r) return r;
-        for (int pass = 0; pass < 2; pass++) {
-            batch_fork(bt);
-            for (int64_t i = 0; i < bt->n && !r; i++) {
-                cudaStream_t bs = bt->br[(size_t)i % nbr];
-                for (int k = 0; k < 2 && !r; k++) {
-                    const iab::DecodeArgs a = operand(i, k);
-                    if (!a.g.nchunks) continue;
-                    iab::DecodeWork *w = k ? &bt->decB[(size_t)i] : &bt->decA[(size_t)i];
-                    w->ext_counters = status + (2 * i + k) * 16;
-                    r = pass ? iab::decode_scatter(a, w, bs) : iab::decode_parse(a, &bt->dq, w, bs);
-                }
-            }
-            batch_join(bt);
-            if (r) return r;
-            if (!pass) iab::decode_lz4(&bt->dq, st);
-        }
     }
     if (!(parts & 2)) {
     } else if (bt->form == IARRAY_B200_FORM_SPLIT) {
@@ -1894,57 +1866,7 @@ int batch_enqueue(iarray_b200_batch_t *bt, int parts)
     }
     if (!(parts & 4)) return 0;
     const bool exact = bt->ctx->encoder == IARRAY_B200_ENCODER_LIBLZ4;
-    // When every output has streams of one size, their byte-plane images, LZ4 slots and
-    // stream results lie back to back and one LZ4 launch encodes the streams of all of
-    // them (gathers and chunk layouts stay per output, on the branches).
-    int nsb = 0, neb = 0;
-    bool shared = true;
-    int64_t img_total = 0, es_total = 0;
-    for (int64_t i = 0; i < bt->n; i++) {
-        const Geom &g = bt->cgeom[(size_t)i];
-        if (!g.nchunks) continue;
-        const int ns = iab::encode_nstreams(g, true, IARRAY_AUTO_SPLIT), ne = (int)(g.blocksize / ns);
-        if (!nsb) { nsb = ns; neb = ne; }
-        shared = shared && ns == nsb && ne == neb;
-        img_total += g.nchunks * g.nblocks * g.blocksize;
-        es_total += g.nchunks * g.nblocks * ns;
-    }
-    if (shared && img_total > 0) {
-        const int dev = bt->ctx->device;
-        if (!bt->eimg.allocate((size_t)img_total, dev) || !bt->eslots.allocate((size_t)img_total, dev) ||
-            !bt->ees.allocate(sizeof(iab::EncStream) * (size_t)es_total, dev) || !bt->ecursor.allocate(64, dev))
-            return -100;
-        cudaMemsetAsync(bt->ecursor.p, 0, 64, st);
-        int r = 0;
-        for (int pass = 0; pass < 2 && !r; pass++) {
-            batch_fork(bt);
-            int64_t io = 0, so = 0;
-            for (int64_t i = 0; i < bt->n && !r; i++) {
-                const Geom &g = bt->cgeom[(size_t)i];
-                if (!g.nchunks) continue;
-                iab::EncodeWork &w = bt->enc[(size_t)i];
-                cudaStream_t bs = bt->br[(size_t)i % nbr];
-                if (!pass) {
-                    w.ext_chunks = bt->chunks.as<iab::EncChunk>() + bt->chunk_base[(size_t)i];
-                    w.exact_lz4 = exact;
-                    w.memcpy_only = bt->ctx->cfg.compression_level == 0;
-                    w.ext_img = bt->eimg.as<uint8_t>() + io;
-                    w.ext_slots = bt->eslots.as<uint8_t>() + io;
-                    w.ext_es = bt->ees.as<iab::EncStream>() + so;
-                    r = iab::encode_gather(g, bt->dC[(size_t)i].p, bt->ldc[(size_t)i], true, IARRAY_AUTO_SPLIT, &w, bs);
-                } else {
-                    r = iab::encode_emit(g, true, IARRAY_AUTO_SPLIT, &bt->cbuf[(size_t)i], &w, bs);
-                }
-                io += g.nchunks * g.nblocks * g.blocksize;
-                so += g.nchunks * g.nblocks * nsb;
-            }
-            batch_join(bt);
-            if (!pass && !r)
-                iab::encode_streams(bt->eimg.as<uint8_t>(), es_total, neb, bt->eslots.as<uint8_t>(),
-                                    bt->ees.as<iab::EncStream>(), bt->ecursor.as<unsigned long long>(), exact, st);
-        }
-        return r;
-    }
+    if (bt->egroup) return iab::encode_group_launch(&bt->egrp, exact, bt->ctx->cfg.compression_level == 0, st);
     batch_fork(bt);
     for (int64_t i = 0; i < bt->n; i++) {
         const Geom &g = bt->cgeom[(size_t)i];
@@ -2120,7 +2042,7 @@ INA_API(ina_rc_t) iarray_b200_batch_new(iarray_context_t *ctx, int64_t n, iarray
     bt->cgeom.resize(un);
     bt->M.resize(un); bt->N.resize(un); bt->K.resize(un); bt->lda.resize(un); bt->ldb.resize(un); bt->ldc.resize(un);
     bt->dA.resize(un); bt->dB.resize(un); bt->dC.resize(un); bt->cbuf.resize(un);
-    bt->decA.resize(un); bt->decB.resize(un); bt->enc.resize(un);
+    bt->enc.resize(un);
     bt->chunk_base.resize(un);
     int64_t nch = 0;
     for (size_t i = 0; i < un; i++) {
@@ -2140,6 +2062,29 @@ INA_API(ina_rc_t) iarray_b200_batch_new(iarray_context_t *ctx, int64_t n, iarray
     if (!bt->status.allocate((size_t)(n * 32 * sizeof(int)), ctx->device) ||
         !bt->chunks.allocate((size_t)std::max<int64_t>(nch, 1) * sizeof(iab::EncChunk), ctx->device))
         return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    {   // the grouped decode of every operand and, when the outputs share a stream shape, encode
+        std::vector<iab::DecodeArgs> da;
+        std::vector<int *> dc;
+        for (size_t i = 0; i < un; i++)
+            for (int k = 0; k < 2; k++) {
+                const iarray_container_t *x = k ? b[i] : a[i];
+                da.push_back(iab::DecodeArgs{x->geom, x->store->buf.as<uint8_t>(), (int64_t)x->store->buf.n,
+                                             x->store->d_off.as<int64_t>(), x->store->d_len.as<int32_t>(),
+                                             (k ? bt->dB : bt->dA)[i].p, k ? bt->ldb[i] : bt->lda[i]});
+                dc.push_back(bt->status.as<int>() + (2 * i + k) * 16);
+            }
+        int r = iab::decode_group_setup(da, dc, &bt->dgrp, ctx->stream);
+        if (r) return r == -100 ? rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY) : rc_err(IARRAY_ERR_GPU_FAILED);
+        std::vector<const void *> dense(un);
+        std::vector<iab::EncChunk *> ec(un);
+        for (size_t i = 0; i < un; i++) {
+            dense[i] = bt->dC[i].p;
+            ec[i] = bt->chunks.as<iab::EncChunk>() + bt->chunk_base[i];
+        }
+        r = iab::encode_group_setup(bt->cgeom, dense, bt->ldc, ec, &bt->cbuf, &bt->egrp, ctx->stream);
+        if (r < 0) return r == -100 ? rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY) : rc_err(IARRAY_ERR_GPU_FAILED);
+        bt->egroup = r == 0;
+    }
     if (bt->form == IARRAY_B200_FORM_SPLIT) {
         ina_rc_t rc = batch_tune_split(bt.get());
         if (INA_FAILED(rc)) return rc;

@@ -48,13 +48,12 @@ __device__ __forceinline__ void dev_fail(int *err, int code) { atomicCAS(err, 0,
 // the first typesize csize words from the block's bstart are all 0: Blosc2 v5 chunks always
 // carry the flag bit the reference reads as "split"), bit 1 = chunk_is_zeros (:17-26:
 // special value ZERO); nzero counts the flagged blocks.
-__global__ void k_parse(Geom g, const uint8_t *__restrict__ ch, const int64_t *__restrict__ off,
-                        const int32_t *__restrict__ len, BlockDesc *bd, StreamDesc *sd, Lz4Job *jobs,
-                        int *njobs, int64_t jcap, int *err, uint8_t *scratch, uint8_t *zf, int *nzero)
+__device__ __forceinline__ void parse_block(const Geom &g, const uint8_t *__restrict__ ch, const int64_t *__restrict__ off,
+                                            const int32_t *__restrict__ len, BlockDesc *bd, StreamDesc *sd,
+                                            Lz4Job *jobs, int *njobs, int64_t jcap, int *err, uint8_t *scratch,
+                                            uint8_t *zf, int *nzero, int64_t t)
 {
-    const int64_t total = g.nchunks * g.nblocks;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
-         t += (int64_t)gridDim.x * blockDim.x) {
+    do {
         const int64_t c = t / g.nblocks, b = t % g.nblocks;
         const uint8_t *p = ch + off[c];
         const int32_t clen = len[c];
@@ -143,7 +142,17 @@ __global__ void k_parse(Geom g, const uint8_t *__restrict__ ch, const int64_t *_
         }
         if (!ok) { for (int j = 0; j < nstreams; j++) { s[j].kind = SK_RUN; s[j].len = 0; } }
         bd[t] = d;
-    }
+    } while (false);
+}
+
+__global__ void k_parse(Geom g, const uint8_t *__restrict__ ch, const int64_t *__restrict__ off,
+                        const int32_t *__restrict__ len, BlockDesc *bd, StreamDesc *sd, Lz4Job *jobs,
+                        int *njobs, int64_t jcap, int *err, uint8_t *scratch, uint8_t *zf, int *nzero)
+{
+    const int64_t total = g.nchunks * g.nblocks;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x)
+        parse_block(g, ch, off, len, bd, sd, jobs, njobs, jcap, err, scratch, zf, nzero, t);
 }
 
 // D1: LZ4 stream decode, one CTA (256 threads) per stream, streams handed out
@@ -537,17 +546,29 @@ __device__ __forceinline__ bool item_pos(const Geom &g, int64_t c, int64_t b, in
     return row < g.shape[0] && col < g.shape[1];
 }
 
-// True when every item of block b of chunk c is a logical item (no chunk or array
-// padding inside the block), block rows hold whole groups of 4 items and items are 4 or
-// 8 bytes: such blocks take the word-level fast paths below.
-__device__ __forceinline__ bool block_fast(const Geom &g, int64_t c, int64_t b)
+// Partitions whose block rows hold whole groups of 4 items of 4 or 8 bytes take the
+// word-level fast paths below, edge blocks included.
+__device__ __forceinline__ bool geom_fast(const Geom &g)
 {
-    if ((g.block[1] & 3) || (g.itemsize != 4 && g.itemsize != 8)) return false;
+    return !(g.block[1] & 3) && (g.itemsize == 4 || g.itemsize == 8);
+}
+
+// Block b of chunk c: its first logical row and column, and how many of its rows (nr) and
+// columns (nc) hold logical items (the rest is chunk or array padding; 0 when none do).
+struct BlockSpan {
+    int64_t row0, col0;
+    int nr, nc;
+};
+__device__ __forceinline__ BlockSpan block_span(const Geom &g, int64_t c, int64_t b)
+{
+    BlockSpan s;
     const int64_t ci0 = c / g.cgrid[1], ci1 = c - ci0 * g.cgrid[1];
     const int64_t bi0 = b / g.bgrid[1], bi1 = b - bi0 * g.bgrid[1];
-    const int64_t r1 = (bi0 + 1) * g.block[0], c1 = (bi1 + 1) * g.block[1];
-    return r1 <= g.chunk[0] && c1 <= g.chunk[1] && ci0 * g.chunk[0] + r1 <= g.shape[0] &&
-           ci1 * g.chunk[1] + c1 <= g.shape[1];
+    s.row0 = ci0 * g.chunk[0] + bi0 * g.block[0];
+    s.col0 = ci1 * g.chunk[1] + bi1 * g.block[1];
+    s.nr = (int)max((int64_t)0, min(min(g.block[0], g.chunk[0] - bi0 * g.block[0]), g.shape[0] - s.row0));
+    s.nc = (int)max((int64_t)0, min(min(g.block[1], g.chunk[1] - bi1 * g.block[1]), g.shape[1] - s.col0));
+    return s;
 }
 
 // 4x4 byte transpose: o_i holds byte i of a, b, c, d (in that order).
@@ -562,12 +583,14 @@ __device__ __forceinline__ void transpose4x4(uint32_t a, uint32_t b, uint32_t c,
     o3 = __byte_perm(ab_hi, cd_hi, 0x7632);
 }
 
-// D2 fast path: interior, shuffled, split blocks, in slices of SC_ITEMS items (one CTA per
-// slice at a time).  One thread stages the slice's bytes of every byte plane (read in place
-// from raw streams or the LZ4 scratch) into shared memory with bulk asynchronous copies
-// completing on an mbarrier; then each thread rebuilds 4 consecutive items from one 4-byte
-// word per plane and writes them to the dense row.  Every other block is appended to the
-// list `rest` for the general path.
+// D2 fast path: shuffled, split blocks of partitions whose block rows hold whole groups of 4
+// items, in slices of SC_ITEMS items (one CTA per slice at a time).  One thread stages the
+// slice's bytes of every byte plane (read in place from raw streams or the LZ4 scratch) into
+// shared memory with bulk asynchronous copies completing on an mbarrier; then each thread
+// rebuilds 4 consecutive items from one 4-byte word per plane and writes the logical ones to
+// the dense row (edge blocks: the items in chunk or array padding are not written; slices of
+// padding only are skipped).  Every other block is appended to the list `rest` for the
+// general path.
 constexpr int SC_ITEMS = 4096;
 constexpr int SC_PLANE = SC_ITEMS + 32;            // a slice of a plane from its 16-byte boundary
 constexpr uint32_t SC_WAIT_POLLS = 1u << 22;
@@ -583,6 +606,131 @@ __device__ __forceinline__ bool sc_wait(uint64_t *bar, uint32_t parity)
     for (uint32_t i = 0; i < SC_WAIT_POLLS; i++)
         if (tc::mbar_try_wait(bar, parity)) return true;
     return false;
+}
+
+// One slice (t, sl) of the fast scatter; false when a bounded wait gave up (the CTA must
+// leave).  rest_id: the block's entry for the general path's list.
+template <int TS>
+__device__ __forceinline__ bool scatter_fast_unit(const Geom &g, const uint8_t *__restrict__ ch, const uint8_t *ch_end,
+                                                  const BlockDesc *__restrict__ bd, const StreamDesc *__restrict__ sd,
+                                                  const uint8_t *__restrict__ scratch, const uint8_t *scratch_end,
+                                                  uint8_t *__restrict__ out, int64_t ld, int *rest, int *nrest,
+                                                  int rest_id, int *err, int64_t t, int sl, uint8_t (*stage)[SC_PLANE],
+                                                  uint64_t *bar, uint32_t &parity, int *abort_all)
+{
+    const int tid = threadIdx.x;
+    const int qpr = (int)(g.block[1] / 4);
+    const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
+    const BlockDesc d = bd[t];
+    if (d.mode != BM_SHUFFLED || d.nstreams != TS || !geom_fast(g)) {
+        if (tid == 0 && sl == 0) rest[atomicAdd(nrest, 1)] = rest_id;   // left to k_scatter
+        return true;
+    }
+    const BlockSpan sp = block_span(g, c, b);
+    const int i0s = sl * SC_ITEMS, cnt = (int)min((int64_t)SC_ITEMS, g.blockn - i0s);
+    if (sp.nc == 0 || i0s / (qpr * 4) >= sp.nr) return true;          // the slice holds only padding
+    // per plane: its slice starts at src, 16-byte word a16 = src - shift; the bulk copy
+    // takes the whole words of [a16, a16 + want) before the buffer end lim, threads copy
+    // the bytes that the buffer end cuts off (zeros past it)
+    auto plane = [&](int j, const uint8_t *&src, const uint8_t *&lim, int &want, int &bulk) {
+        const StreamDesc q = sd[t * 8 + j];
+        src = nullptr; lim = nullptr;
+        if (q.kind == SK_RAW) { src = ch + q.src + i0s; lim = ch_end; }
+        else if (q.kind == SK_LZ4) { src = scratch + t * g.blocksize + (int64_t)j * d.neblock + i0s; lim = scratch_end; }
+        want = bulk = 0;
+        if (src) {
+            const uint8_t *a16 = src - (reinterpret_cast<uintptr_t>(src) & 15);
+            want = ((int)(src - a16) + cnt + 15) & ~15;
+            bulk = (int)min((int64_t)want, (lim - a16) & ~int64_t(15));
+        }
+        return q;
+    };
+    if (tid == 0) {
+        uint32_t tx = 0;
+#pragma unroll
+        for (int j = 0; j < TS; j++) {
+            const uint8_t *src, *lim;
+            int want, bulk;
+            plane(j, src, lim, want, bulk);
+            tx += (uint32_t)bulk;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier reads of stage precede the copies
+        tc::mbar_arrive_expect_tx(bar, tx);
+#pragma unroll
+        for (int j = 0; j < TS; j++) {
+            const uint8_t *src, *lim;
+            int want, bulk;
+            plane(j, src, lim, want, bulk);
+            if (bulk > 0) bulk_g2s(stage[j], src - (reinterpret_cast<uintptr_t>(src) & 15), (uint32_t)bulk, bar);
+        }
+    }
+    int code[TS];                                  // 0..15: the plane's shift in stage; 256 + v: a run of byte v
+#pragma unroll
+    for (int j = 0; j < TS; j++) {
+        const uint8_t *src, *lim;
+        int want, bulk;
+        const StreamDesc q = plane(j, src, lim, want, bulk);
+        code[j] = src ? (int)(reinterpret_cast<uintptr_t>(src) & 15) : 256 + (q.kind == SK_RUN ? (q.len & 255) : 0);
+        if (bulk < want) {
+            const uint8_t *a16 = src - code[j];
+            for (int x = bulk + tid; x < want; x += blockDim.x) stage[j][x] = a16 + x < lim ? __ldg(a16 + x) : (uint8_t)0;
+        }
+    }
+    const bool ok = sc_wait(bar, parity);
+    parity ^= 1;
+    if (!ok) *abort_all = 1;
+    __syncthreads();
+    if (*abort_all) {                              // the copies did not complete: report, wait once more, leave
+        if (tid == 0) {
+            dev_fail(err, DE_WAIT);
+            sc_wait(bar, parity ^ 1);
+        }
+        return false;
+    }
+    uint8_t *const obase = out + (sp.row0 * ld + sp.col0) * TS;
+    const int nr = sp.nr, nc = sp.nc;
+    for (int qd = tid; qd < cnt / 4; qd += blockDim.x) {
+        const int it = i0s + qd * 4, r = it / (qpr * 4), cc = it - r * qpr * 4;
+        if (r >= nr || cc >= nc) continue;                                // padding items
+        uint32_t w[TS];
+#pragma unroll
+        for (int j = 0; j < TS; j++) {
+            if (code[j] >= 256) { w[j] = (uint32_t)(code[j] - 256) * 0x01010101u; continue; }
+            const uint32_t *pw = reinterpret_cast<const uint32_t *>(stage[j]);
+            const int byte = code[j] + qd * 4, wi = byte >> 2, sh = (byte & 3) * 8;
+            w[j] = sh ? __funnelshift_r(pw[wi], pw[wi + 1], sh) : pw[wi];
+        }
+        uint8_t *o = obase + ((int64_t)r * ld + cc) * TS;
+        uint32_t v[4];
+        transpose4x4(w[0], w[1], w[2], w[3], v[0], v[1], v[2], v[3]);
+        const bool whole = cc + 4 <= nc;
+        const bool o16a = (reinterpret_cast<uintptr_t>(o) & 15) == 0;
+        if constexpr (TS == 8) {
+            uint32_t h[4];
+            transpose4x4(w[4], w[5], w[6], w[7], h[0], h[1], h[2], h[3]);
+            if (whole && o16a) {
+                uint4 *o16 = reinterpret_cast<uint4 *>(o);
+                o16[0] = make_uint4(v[0], h[0], v[1], h[1]);
+                o16[1] = make_uint4(v[2], h[2], v[3], h[3]);
+            } else {
+                uint64_t *o8 = reinterpret_cast<uint64_t *>(o);
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (cc + u < nc) o8[u] = ((uint64_t)h[u] << 32) | v[u];
+            }
+        } else {
+            if (whole && o16a) {
+                *reinterpret_cast<uint4 *>(o) = make_uint4(v[0], v[1], v[2], v[3]);
+            } else {
+                uint32_t *o4 = reinterpret_cast<uint32_t *>(o);
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (cc + u < nc) o4[u] = v[u];
+            }
+        }
+    }
+    __syncthreads();                               // stage is read before the next slice's copies
+    return true;
 }
 
 template <int TS>
@@ -605,263 +753,188 @@ __global__ void __launch_bounds__(256, 6) k_scatter_fast(Geom g, const uint8_t *
     __syncthreads();
     const int64_t nbl = g.nchunks * g.nblocks;
     const int64_t nsl = (g.blockn + SC_ITEMS - 1) / SC_ITEMS;
-    const int qpr = (int)(g.block[1] / 4);
     uint32_t parity = 0;
     for (int64_t u = blockIdx.x; u < nbl * nsl; u += gridDim.x) {
         const int64_t t = u / nsl;
         const int sl = (int)(u - t * nsl);
-        const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
-        const BlockDesc d = bd[t];
-        if (d.mode != BM_SHUFFLED || d.nstreams != TS || !block_fast(g, c, b)) {
-            if (tid == 0 && sl == 0) rest[atomicAdd(nrest, 1)] = (int)t;   // left to k_scatter
-            continue;
-        }
-        const int i0s = sl * SC_ITEMS, cnt = (int)min((int64_t)SC_ITEMS, g.blockn - i0s);
-        // per plane: its slice starts at src, 16-byte word a16 = src - shift; the bulk copy
-        // takes the whole words of [a16, a16 + want) before the buffer end lim, threads copy
-        // the bytes that the buffer end cuts off (zeros past it)
-        auto plane = [&](int j, const uint8_t *&src, const uint8_t *&lim, int &want, int &bulk) {
-            const StreamDesc q = sd[t * 8 + j];
-            src = nullptr; lim = nullptr;
-            if (q.kind == SK_RAW) { src = ch + q.src + i0s; lim = ch_end; }
-            else if (q.kind == SK_LZ4) { src = scratch + t * g.blocksize + (int64_t)j * d.neblock + i0s; lim = scratch_end; }
-            want = bulk = 0;
-            if (src) {
-                const uint8_t *a16 = src - (reinterpret_cast<uintptr_t>(src) & 15);
-                want = ((int)(src - a16) + cnt + 15) & ~15;
-                bulk = (int)min((int64_t)want, (lim - a16) & ~int64_t(15));
-            }
-            return q;
-        };
-        if (tid == 0) {
-            uint32_t tx = 0;
-#pragma unroll
-            for (int j = 0; j < TS; j++) {
-                const uint8_t *src, *lim;
-                int want, bulk;
-                plane(j, src, lim, want, bulk);
-                tx += (uint32_t)bulk;
-            }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier reads of stage precede the copies
-            tc::mbar_arrive_expect_tx(&bar, tx);
-#pragma unroll
-            for (int j = 0; j < TS; j++) {
-                const uint8_t *src, *lim;
-                int want, bulk;
-                plane(j, src, lim, want, bulk);
-                if (bulk > 0) bulk_g2s(stage[j], src - (reinterpret_cast<uintptr_t>(src) & 15), (uint32_t)bulk, &bar);
-            }
-        }
-        int code[TS];                                  // 0..15: the plane's shift in stage; 256 + v: a run of byte v
-#pragma unroll
-        for (int j = 0; j < TS; j++) {
-            const uint8_t *src, *lim;
-            int want, bulk;
-            const StreamDesc q = plane(j, src, lim, want, bulk);
-            code[j] = src ? (int)(reinterpret_cast<uintptr_t>(src) & 15) : 256 + (q.kind == SK_RUN ? (q.len & 255) : 0);
-            if (bulk < want) {
-                const uint8_t *a16 = src - code[j];
-                for (int x = bulk + tid; x < want; x += blockDim.x) stage[j][x] = a16 + x < lim ? __ldg(a16 + x) : (uint8_t)0;
-            }
-        }
-        const bool ok = sc_wait(&bar, parity);
-        parity ^= 1;
-        if (!ok) abort_all = 1;
-        __syncthreads();
-        if (abort_all) {                               // the copies did not complete: report, wait once more, leave
-            if (tid == 0) {
-                dev_fail(err, DE_WAIT);
-                sc_wait(&bar, parity ^ 1);
-            }
+        if (!scatter_fast_unit<TS>(g, ch, ch_end, bd, sd, scratch, scratch_end, out, ld, rest, nrest, (int)t, err, t, sl,
+                                   stage, &bar, parity, &abort_all))
             return;
-        }
-        const int64_t ci0 = c / g.cgrid[1], ci1 = c - ci0 * g.cgrid[1];
-        const int64_t bi0 = b / g.bgrid[1], bi1 = b - bi0 * g.bgrid[1];
-        const int64_t row0 = ci0 * g.chunk[0] + bi0 * g.block[0], col0 = ci1 * g.chunk[1] + bi1 * g.block[1];
-        for (int qd = tid; qd < cnt / 4; qd += blockDim.x) {
-            uint32_t w[TS];
-#pragma unroll
-            for (int j = 0; j < TS; j++) {
-                if (code[j] >= 256) { w[j] = (uint32_t)(code[j] - 256) * 0x01010101u; continue; }
-                const uint32_t *pw = reinterpret_cast<const uint32_t *>(stage[j]);
-                const int byte = code[j] + qd * 4, wi = byte >> 2, sh = (byte & 3) * 8;
-                w[j] = sh ? __funnelshift_r(pw[wi], pw[wi + 1], sh) : pw[wi];
-            }
-            const int it = i0s + qd * 4, r = it / (qpr * 4), cc = it - r * qpr * 4;
-            uint8_t *o = out + ((row0 + r) * ld + col0 + cc) * TS;
-            uint32_t v0, v1, v2, v3;
-            transpose4x4(w[0], w[1], w[2], w[3], v0, v1, v2, v3);
-            const bool o16a = (reinterpret_cast<uintptr_t>(o) & 15) == 0;
-            if constexpr (TS == 8) {
-                uint32_t h0, h1, h2, h3;
-                transpose4x4(w[4], w[5], w[6], w[7], h0, h1, h2, h3);
-                if (o16a) {
-                    uint4 *o16 = reinterpret_cast<uint4 *>(o);
-                    o16[0] = make_uint4(v0, h0, v1, h1);
-                    o16[1] = make_uint4(v2, h2, v3, h3);
-                } else {
-                    uint64_t *o8 = reinterpret_cast<uint64_t *>(o);
-                    o8[0] = ((uint64_t)h0 << 32) | v0;
-                    o8[1] = ((uint64_t)h1 << 32) | v1;
-                    o8[2] = ((uint64_t)h2 << 32) | v2;
-                    o8[3] = ((uint64_t)h3 << 32) | v3;
-                }
-            } else {
-                if (o16a) {
-                    *reinterpret_cast<uint4 *>(o) = make_uint4(v0, v1, v2, v3);
-                } else {
-                    uint32_t *o4 = reinterpret_cast<uint32_t *>(o);
-                    o4[0] = v0; o4[1] = v1; o4[2] = v2; o4[3] = v3;
-                }
-            }
-        }
-        __syncthreads();                               // stage is read before the next slice's copies
     }
 }
 
 // D2 general path: unshuffle one tile of TILE items of one block through shared memory
 // and scatter it to the dense array (padded edge blocks, other item sizes, plain and
 // special chunks).  With a `rest` list, only the blocks listed there; else every block.
+__device__ __forceinline__ void scatter_tile(const Geom &g, const uint8_t *__restrict__ ch,
+                                             const BlockDesc *__restrict__ bd, const StreamDesc *__restrict__ sd,
+                                             const uint8_t *__restrict__ scratch, uint8_t *__restrict__ out, int64_t ld,
+                                             int64_t t, int64_t i0, uint8_t *planes)
+{
+    const int ts = g.itemsize;
+    const int cnt = (int)min((int64_t)TILE, g.blockn - i0);
+    const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
+    const BlockDesc d = bd[t];
+    const StreamDesc *s = sd + t * 8;
+    const uint8_t *blk_scratch = scratch + t * g.blocksize;
+    if (d.mode == BM_SHUFFLED) {
+        for (int j = 0; j < ts; j++) {
+            const int64_t pos = (int64_t)j * g.blockn + i0;
+            const int sidx = (int)(pos / d.neblock);
+            const int64_t so = pos - (int64_t)sidx * d.neblock;
+            const StreamDesc q = s[sidx];
+            uint8_t *pl = planes + j * TILE;
+            if (q.kind == SK_RUN) {
+                for (int x = threadIdx.x; x < cnt; x += blockDim.x) pl[x] = (uint8_t)q.len;
+            } else if (q.kind == SK_RAW) {
+                const uint8_t *src = ch + q.src + so;
+                for (int x = threadIdx.x; x < cnt; x += blockDim.x) pl[x] = __ldg(src + x);
+            } else {
+                const uint8_t *src = blk_scratch + (int64_t)sidx * d.neblock + so;
+                for (int x = threadIdx.x; x < cnt; x += blockDim.x) pl[x] = __ldcg(src + x);
+            }
+        }
+    } else if (d.mode == BM_PLAIN) {
+        for (int x = threadIdx.x; x < cnt * ts; x += blockDim.x) {
+            const int64_t pos = i0 * ts + x;
+            const int sidx = (int)(pos / d.neblock);
+            const int64_t so = pos - (int64_t)sidx * d.neblock;
+            const StreamDesc q = s[sidx];
+            uint8_t v;
+            if (q.kind == SK_RUN) v = (uint8_t)q.len;
+            else if (q.kind == SK_RAW) v = __ldg(ch + q.src + so);
+            else v = __ldcg(blk_scratch + (int64_t)sidx * d.neblock + so);
+            planes[x] = v;
+        }
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
+        int64_t row, col;
+        if (!item_pos(g, c, b, i0 + x, row, col)) continue;
+        uint8_t *o = out + (row * ld + col) * ts;
+        uint64_t v = 0;
+        if (d.mode == BM_SHUFFLED) {
+            for (int j = 0; j < ts; j++) v |= (uint64_t)planes[j * TILE + x] << (8 * j);
+        } else if (d.mode == BM_PLAIN) {
+            for (int j = 0; j < ts; j++) v |= (uint64_t)planes[x * ts + j] << (8 * j);
+        } else if (d.mode == BM_NAN) {
+            v = ts == 8 ? 0x7FF8000000000000ull : 0x7FC00000ull;
+        } else {
+            v = load_item(ch + d.value_src, ts);
+        }
+        store_item(o, ts, v);
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(256) k_scatter(Geom g, const int *__restrict__ rest, const int *__restrict__ nrest,
                                                  const uint8_t *__restrict__ ch,
                                                  const BlockDesc *__restrict__ bd, const StreamDesc *__restrict__ sd,
                                                  const uint8_t *__restrict__ scratch, uint8_t *__restrict__ out, int64_t ld)
 {
     __shared__ __align__(16) uint8_t planes[8 * TILE];
-    const int ts = g.itemsize;
     const int64_t tpb = (g.blockn + TILE - 1) / TILE;
     const int64_t nwork = (rest ? (int64_t)*nrest : g.nchunks * g.nblocks) * tpb;
     for (int64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
         const int64_t k = w / tpb, t = rest ? rest[k] : k, i0 = (w - k * tpb) * TILE;
-        const int cnt = (int)min((int64_t)TILE, g.blockn - i0);
-        const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
-        const BlockDesc d = bd[t];
-        const StreamDesc *s = sd + t * 8;
-        const uint8_t *blk_scratch = scratch + t * g.blocksize;
-        if (d.mode == BM_SHUFFLED) {
-            for (int j = 0; j < ts; j++) {
-                const int64_t pos = (int64_t)j * g.blockn + i0;
-                const int sidx = (int)(pos / d.neblock);
-                const int64_t so = pos - (int64_t)sidx * d.neblock;
-                const StreamDesc q = s[sidx];
-                uint8_t *pl = planes + j * TILE;
-                if (q.kind == SK_RUN) {
-                    for (int x = threadIdx.x; x < cnt; x += blockDim.x) pl[x] = (uint8_t)q.len;
-                } else if (q.kind == SK_RAW) {
-                    const uint8_t *src = ch + q.src + so;
-                    for (int x = threadIdx.x; x < cnt; x += blockDim.x) pl[x] = __ldg(src + x);
-                } else {
-                    const uint8_t *src = blk_scratch + (int64_t)sidx * d.neblock + so;
-                    for (int x = threadIdx.x; x < cnt; x += blockDim.x) pl[x] = __ldcg(src + x);
-                }
-            }
-        } else if (d.mode == BM_PLAIN) {
-            for (int x = threadIdx.x; x < cnt * ts; x += blockDim.x) {
-                const int64_t pos = i0 * ts + x;
-                const int sidx = (int)(pos / d.neblock);
-                const int64_t so = pos - (int64_t)sidx * d.neblock;
-                const StreamDesc q = s[sidx];
-                uint8_t v;
-                if (q.kind == SK_RUN) v = (uint8_t)q.len;
-                else if (q.kind == SK_RAW) v = __ldg(ch + q.src + so);
-                else v = __ldcg(blk_scratch + (int64_t)sidx * d.neblock + so);
-                planes[x] = v;
-            }
-        }
-        __syncthreads();
-        for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
-            int64_t row, col;
-            if (!item_pos(g, c, b, i0 + x, row, col)) continue;
-            uint8_t *o = out + (row * ld + col) * ts;
-            uint64_t v = 0;
-            if (d.mode == BM_SHUFFLED) {
-                for (int j = 0; j < ts; j++) v |= (uint64_t)planes[j * TILE + x] << (8 * j);
-            } else if (d.mode == BM_PLAIN) {
-                for (int j = 0; j < ts; j++) v |= (uint64_t)planes[x * ts + j] << (8 * j);
-            } else if (d.mode == BM_NAN) {
-                v = ts == 8 ? 0x7FF8000000000000ull : 0x7FC00000ull;
-            } else {
-                v = load_item(ch + d.value_src, ts);
-            }
-            store_item(o, ts, v);
-        }
-        __syncthreads();
+        scatter_tile(g, ch, bd, sd, scratch, out, ld, t, i0, planes);
     }
 }
 
 // ============================================================================ encode
-// E1 fast path: interior blocks, shuffle on; each thread reads 4 consecutive items of a
-// block row and writes one 4-byte word into each byte plane of the image.
+// E1 fast path: shuffle on, block rows of whole groups of 4 items; each thread reads 4
+// consecutive items of a block row (zero for the items in chunk or array padding) and
+// writes one 4-byte word into each byte plane of the image.
+template <int TS>
+__device__ __forceinline__ void gather_fast_block(const Geom &g, const uint8_t *__restrict__ in, int64_t ld,
+                                                  uint8_t *__restrict__ img, int64_t t)
+{
+    if (!geom_fast(g)) return;
+    const int qpr = (int)(g.block[1] / 4), nq = (int)(g.blockn / 4);
+    const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
+    const BlockSpan sp = block_span(g, c, b);
+    uint8_t *blk = img + t * g.blocksize;
+    for (int qd = threadIdx.x; qd < nq; qd += blockDim.x) {
+        const int i0 = qd * 4, r = qd / qpr, cc = (qd - r * qpr) * 4;
+        const uint8_t *src = in + ((sp.row0 + r) * ld + sp.col0 + cc) * TS;
+        uint64_t x[4] = {0, 0, 0, 0};                 // padding items are zero, as in Caterva
+        if (r < sp.nr && cc + 4 <= sp.nc) {
+            if constexpr (TS == 8) {
+                const uint64_t *s8 = reinterpret_cast<const uint64_t *>(src);
+#pragma unroll
+                for (int u = 0; u < 4; u++) x[u] = __ldg(s8 + u);
+            } else {
+                const uint32_t *s4 = reinterpret_cast<const uint32_t *>(src);
+#pragma unroll
+                for (int u = 0; u < 4; u++) x[u] = __ldg(s4 + u);
+            }
+        } else if (r < sp.nr) {
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (cc + u < sp.nc) x[u] = TS == 8 ? __ldg(reinterpret_cast<const uint64_t *>(src) + u)
+                                                   : __ldg(reinterpret_cast<const uint32_t *>(src) + u);
+        }
+        uint32_t o[TS];
+        transpose4x4((uint32_t)x[0], (uint32_t)x[1], (uint32_t)x[2], (uint32_t)x[3], o[0], o[1], o[2], o[3]);
+        if constexpr (TS == 8)
+            transpose4x4((uint32_t)(x[0] >> 32), (uint32_t)(x[1] >> 32), (uint32_t)(x[2] >> 32), (uint32_t)(x[3] >> 32),
+                         o[4], o[5], o[6], o[7]);
+#pragma unroll
+        for (int j = 0; j < TS; j++) *reinterpret_cast<uint32_t *>(blk + (int64_t)j * g.blockn + i0) = o[j];
+    }
+}
+
 template <int TS>
 __global__ void __launch_bounds__(256) k_gather_fast(Geom g, const uint8_t *__restrict__ in, int64_t ld,
                                                      uint8_t *__restrict__ img)
 {
     const int64_t nbl = g.nchunks * g.nblocks;
-    const int qpr = (int)(g.block[1] / 4), nq = (int)(g.blockn / 4);
-    for (int64_t t = blockIdx.x; t < nbl; t += gridDim.x) {
-        const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
-        if (!block_fast(g, c, b)) continue;
-        const int64_t ci0 = c / g.cgrid[1], ci1 = c - ci0 * g.cgrid[1];
-        const int64_t bi0 = b / g.bgrid[1], bi1 = b - bi0 * g.bgrid[1];
-        const int64_t row0 = ci0 * g.chunk[0] + bi0 * g.block[0], col0 = ci1 * g.chunk[1] + bi1 * g.block[1];
-        uint8_t *blk = img + t * g.blocksize;
-        for (int qd = threadIdx.x; qd < nq; qd += blockDim.x) {
-            const int i0 = qd * 4, r = qd / qpr, cc = (qd - r * qpr) * 4;
-            const uint8_t *src = in + ((row0 + r) * ld + col0 + cc) * TS;
-            uint32_t o[TS];
-            if constexpr (TS == 8) {
-                const uint64_t *s8 = reinterpret_cast<const uint64_t *>(src);
-                const uint64_t x0 = __ldg(s8), x1 = __ldg(s8 + 1), x2 = __ldg(s8 + 2), x3 = __ldg(s8 + 3);
-                transpose4x4((uint32_t)x0, (uint32_t)x1, (uint32_t)x2, (uint32_t)x3, o[0], o[1], o[2], o[3]);
-                transpose4x4((uint32_t)(x0 >> 32), (uint32_t)(x1 >> 32), (uint32_t)(x2 >> 32), (uint32_t)(x3 >> 32),
-                             o[4], o[5], o[6], o[7]);
-            } else {
-                const uint32_t *s4 = reinterpret_cast<const uint32_t *>(src);
-                transpose4x4(__ldg(s4), __ldg(s4 + 1), __ldg(s4 + 2), __ldg(s4 + 3), o[0], o[1], o[2], o[3]);
-            }
-#pragma unroll
-            for (int j = 0; j < TS; j++) *reinterpret_cast<uint32_t *>(blk + (int64_t)j * g.blockn + i0) = o[j];
-        }
-    }
+    for (int64_t t = blockIdx.x; t < nbl; t += gridDim.x) gather_fast_block<TS>(g, in, ld, img, t);
 }
 
 // E1 general path: dense -> byte-plane image (shuffled: plane j holds byte j of every
 // item; plain: items back to back).  Padding items are zero, as in Caterva.  With
-// skip_fast, blocks the fast path handles are skipped.
+// skip_fast, nothing is done for partitions the fast path handles.
+__device__ __forceinline__ void gather_tile(const Geom &g, const uint8_t *__restrict__ in, int64_t ld, bool shuffle,
+                                            uint8_t *__restrict__ img, int64_t t, int64_t i0, uint8_t *planes)
+{
+    const int ts = g.itemsize;
+    const int cnt = (int)min((int64_t)TILE, g.blockn - i0);
+    const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
+    for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
+        int64_t row, col;
+        uint64_t v = 0;
+        if (item_pos(g, c, b, i0 + x, row, col)) v = load_item(in + (row * ld + col) * ts, ts);
+        if (shuffle) {
+            for (int j = 0; j < ts; j++) planes[j * TILE + x] = (uint8_t)(v >> (8 * j));
+        } else {
+            for (int j = 0; j < ts; j++) planes[x * ts + j] = (uint8_t)(v >> (8 * j));
+        }
+    }
+    __syncthreads();
+    uint8_t *blk = img + t * g.blocksize;
+    if (shuffle) {
+        for (int j = 0; j < ts; j++) {
+            uint8_t *dst = blk + (int64_t)j * g.blockn + i0;
+            for (int x = threadIdx.x; x < cnt; x += blockDim.x) dst[x] = planes[j * TILE + x];
+        }
+    } else {
+        uint8_t *dst = blk + i0 * ts;
+        for (int x = threadIdx.x; x < cnt * ts; x += blockDim.x) dst[x] = planes[x];
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(256) k_gather(Geom g, bool skip_fast, const uint8_t *__restrict__ in, int64_t ld,
                                                 bool shuffle, uint8_t *__restrict__ img)
 {
     __shared__ __align__(16) uint8_t planes[8 * TILE];
-    const int ts = g.itemsize;
     const int64_t tpb = (g.blockn + TILE - 1) / TILE;
     const int64_t nwork = g.nchunks * g.nblocks * tpb;
     for (int64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
         const int64_t t = w / tpb, i0 = (w - t * tpb) * TILE;
-        const int cnt = (int)min((int64_t)TILE, g.blockn - i0);
-        const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
-        if (skip_fast && block_fast(g, c, b)) continue;
-        for (int x = threadIdx.x; x < cnt; x += blockDim.x) {
-            int64_t row, col;
-            uint64_t v = 0;
-            if (item_pos(g, c, b, i0 + x, row, col)) v = load_item(in + (row * ld + col) * ts, ts);
-            if (shuffle) {
-                for (int j = 0; j < ts; j++) planes[j * TILE + x] = (uint8_t)(v >> (8 * j));
-            } else {
-                for (int j = 0; j < ts; j++) planes[x * ts + j] = (uint8_t)(v >> (8 * j));
-            }
-        }
-        __syncthreads();
-        uint8_t *blk = img + t * g.blocksize;
-        if (shuffle) {
-            for (int j = 0; j < ts; j++) {
-                uint8_t *dst = blk + (int64_t)j * g.blockn + i0;
-                for (int x = threadIdx.x; x < cnt; x += blockDim.x) dst[x] = planes[j * TILE + x];
-            }
-        } else {
-            uint8_t *dst = blk + i0 * ts;
-            for (int x = threadIdx.x; x < cnt * ts; x += blockDim.x) dst[x] = planes[x];
-        }
-        __syncthreads();
+        if (skip_fast && geom_fast(g)) continue;
+        gather_tile(g, in, ld, shuffle, img, t, i0, planes);
     }
 }
 
@@ -1773,13 +1846,9 @@ __device__ __forceinline__ bool layout_step(EncStream &e, int64_t &ntb, int64_t 
 }
 
 // memcpy_only (compression level 0): c-blosc2 stores every chunk memcpyed.
-__global__ void __launch_bounds__(LAYOUT_T) k_layout(Geom g, int nstreams, int neblock, EncStream *es, EncChunk *ec,
-                                                    int memcpy_only)
+__device__ __forceinline__ void layout_chunk(const Geom &g, int nstreams, int neblock, EncStream *es, EncChunk *ec,
+                                             int memcpy_only, int64_t c, int64_t *wsum, int64_t &s_before, int &s_first)
 {
-    __shared__ int64_t wsum[LAYOUT_T / 32];
-    __shared__ int64_t s_before;
-    __shared__ int s_first;
-    const int64_t c = blockIdx.x;
     const int64_t destsize = g.chunk_nbytes + 32, ns = g.nblocks * nstreams;
     if (memcpy_only) {
         if (threadIdx.x == 0) { ec[c].memcpyed = 1; ec[c].cbytes = (int32_t)destsize; }
@@ -1838,10 +1907,18 @@ __global__ void __launch_bounds__(LAYOUT_T) k_layout(Geom g, int nstreams, int n
     }
 }
 
-// Chunk offsets: exclusive scan of the chunk sizes (one CTA).
-__global__ void __launch_bounds__(1024) k_chunk_offsets(int64_t nchunks, EncChunk *ec, int64_t *total)
+__global__ void __launch_bounds__(LAYOUT_T) k_layout(Geom g, int nstreams, int neblock, EncStream *es, EncChunk *ec,
+                                                    int memcpy_only)
 {
-    __shared__ int64_t wsum[32];
+    __shared__ int64_t wsum[LAYOUT_T / 32];
+    __shared__ int64_t s_before;
+    __shared__ int s_first;
+    layout_chunk(g, nstreams, neblock, es, ec, memcpy_only, blockIdx.x, wsum, s_before, s_first);
+}
+
+// Chunk offsets: exclusive scan of the chunk sizes (one CTA).
+__device__ __forceinline__ void chunk_offsets(int64_t nchunks, EncChunk *ec, int64_t *total, int64_t *wsum)
+{
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int64_t base = 0;
     for (int64_t r0 = 0; r0 < nchunks; r0 += 1024) {
@@ -1865,6 +1942,12 @@ __global__ void __launch_bounds__(1024) k_chunk_offsets(int64_t nchunks, EncChun
         __syncthreads();
     }
     if (threadIdx.x == 0) *total = base;
+}
+
+__global__ void __launch_bounds__(1024) k_chunk_offsets(int64_t nchunks, EncChunk *ec, int64_t *total)
+{
+    __shared__ int64_t wsum[32];
+    chunk_offsets(nchunks, ec, total, wsum);
 }
 
 // Copies len bytes with the whole CTA: 16-byte aligned stores to dst, each fed by five
@@ -1903,14 +1986,13 @@ __device__ __forceinline__ void cta_copy(uint8_t *__restrict__ dst, const uint8_
 }
 
 // E5: write headers, bstarts, csize words and payloads.  One CTA per (chunk, block).
-__global__ void __launch_bounds__(256) k_emit(Geom g, int nstreams, int neblock, bool shuffle, int splitflag,
-                                              const uint8_t *__restrict__ img, const uint8_t *__restrict__ slots,
-                                              int64_t img_bytes,
-                                              const EncStream *__restrict__ es, const EncChunk *__restrict__ ec,
-                                              uint8_t *__restrict__ outbuf)
+__device__ __forceinline__ void emit_block(const Geom &g, int nstreams, int neblock, bool shuffle, int splitflag,
+                                           const uint8_t *__restrict__ img, const uint8_t *__restrict__ slots,
+                                           int64_t img_bytes, const EncStream *__restrict__ es,
+                                           const EncChunk *__restrict__ ec, uint8_t *__restrict__ outbuf, int64_t t)
 {
     const int ts = g.itemsize;
-    for (int64_t t = blockIdx.x; t < g.nchunks * g.nblocks; t += gridDim.x) {
+    do {
         const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
         const EncChunk cc = ec[c];
         uint8_t *chunk = outbuf + cc.offset;
@@ -1962,7 +2044,17 @@ __global__ void __launch_bounds__(256) k_emit(Geom g, int nstreams, int neblock,
                 cta_copy(w + 4, payload, plen, base, base + img_bytes);
             }
         }
-    }
+    } while (false);
+}
+
+__global__ void __launch_bounds__(256) k_emit(Geom g, int nstreams, int neblock, bool shuffle, int splitflag,
+                                              const uint8_t *__restrict__ img, const uint8_t *__restrict__ slots,
+                                              int64_t img_bytes,
+                                              const EncStream *__restrict__ es, const EncChunk *__restrict__ ec,
+                                              uint8_t *__restrict__ outbuf)
+{
+    for (int64_t t = blockIdx.x; t < g.nchunks * g.nblocks; t += gridDim.x)
+        emit_block(g, nstreams, neblock, shuffle, splitflag, img, slots, img_bytes, es, ec, outbuf, t);
 }
 
 // ============================================================================ host launchers
@@ -2146,9 +2238,8 @@ int encode_gather(const Geom &g, const void *in, int64_t ld, bool shuffle, int s
             IAB_TIMED("k_gather_fast", st, k_gather_fast<4><<<(unsigned)std::max<int64_t>(fb, 1), 256, 0, st>>>(
                 g, (const uint8_t *)in, ld, img));
     }
-    // the general gather covers the blocks the fast one leaves (padded or partial ones)
-    const bool all_fast = fast && g.chunk[0] % g.block[0] == 0 && g.chunk[1] % g.block[1] == 0 &&
-                          g.shape[0] % g.chunk[0] == 0 && g.shape[1] % g.chunk[1] == 0 && !(g.block[1] & 3);
+    // the general gather covers the partitions the fast one does not take
+    const bool all_fast = fast && !(g.block[1] & 3);
     if (!all_fast)
         IAB_TIMED("k_gather", st, k_gather<<<(unsigned)std::max<int64_t>(blocks, 1), 256, 0, st>>>(
             g, fast, (const uint8_t *)in, ld, shuffle, img));
@@ -2246,6 +2337,333 @@ int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, in
     const int r = encode_launch(g, in, ld, shuffle, splitmode, d_out, &w, st);
     if (r) return r;
     return encode_finish(&w, h_off, h_len, st);
+}
+
+// ============================================================================ grouped codec
+// Largest k with start[k] <= u (containers with no units share their start with the next).
+__device__ __forceinline__ int group_find(const int64_t *__restrict__ start, int n, int64_t u)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(start + mid) <= u) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void k_group_reset(const CodecItem *__restrict__ items, int n)
+{
+    const int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (x < (int64_t)n * 16) items[x >> 4].cnt[x & 15] = 0;
+}
+
+__global__ void k_parse_g(const CodecItem *__restrict__ items, const int64_t *__restrict__ bstart, int n, int64_t nbl,
+                          Lz4Job *jobs, int *njobs, int64_t jcap)
+{
+    for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < nbl; u += (int64_t)gridDim.x * blockDim.x) {
+        const int k = group_find(bstart, n, u);
+        const CodecItem &it = items[k];
+        parse_block(it.g, it.ch, it.off, it.len, it.bd, it.sd, jobs, njobs, jcap, it.cnt + 1, it.scratch, nullptr,
+                    nullptr, u - bstart[k]);
+    }
+}
+
+template <int TS>
+__global__ void __launch_bounds__(256, 4) k_scatter_fast_g(const CodecItem *__restrict__ items,
+                                                        const int64_t *__restrict__ bstart,
+                                                        const int64_t *__restrict__ sstart, int n, int64_t nsf,
+                                                        int *rest, int *nrest)
+{
+    __shared__ __align__(128) uint8_t stage[TS][SC_PLANE];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int abort_all;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        tc::mbar_init(&bar, 1);
+        tc::fence_barrier_init();
+        abort_all = 0;
+    }
+    __syncthreads();
+    uint32_t parity = 0;
+    for (int64_t u = blockIdx.x; u < nsf; u += gridDim.x) {
+        const int k = group_find(sstart, n, u);
+        const CodecItem &it = items[k];
+        const int64_t nsl = (it.g.blockn + SC_ITEMS - 1) / SC_ITEMS;
+        const int64_t lu = u - sstart[k], t = lu / nsl;
+        const int sl = (int)(lu - t * nsl);
+        const int64_t nbk = it.g.nchunks * it.g.nblocks;
+        if (!scatter_fast_unit<TS>(it.g, it.ch, it.ch + it.ch_bytes, it.bd, it.sd, it.scratch,
+                                   it.scratch + nbk * it.g.blocksize, it.dense, it.ld, rest, nrest,
+                                   (int)(bstart[k] + t), it.cnt + 1, t, sl, stage, &bar, parity, &abort_all))
+            return;
+    }
+}
+
+// General scatter over the listed blocks (global block numbers), or every block without a list.
+__global__ void __launch_bounds__(256) k_scatter_g(const CodecItem *__restrict__ items, const int64_t *__restrict__ bstart,
+                                                   int n, const int *__restrict__ rest, const int *__restrict__ nrest,
+                                                   int64_t nbl, int64_t tpb)
+{
+    __shared__ __align__(16) uint8_t planes[8 * TILE];
+    const int64_t nwork = (rest ? (int64_t)*nrest : nbl) * tpb;
+    for (int64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int64_t kk = w / tpb, gb = rest ? rest[kk] : kk, i0 = (w - kk * tpb) * TILE;
+        const int k = group_find(bstart, n, gb);
+        const CodecItem &it = items[k];
+        if (i0 >= it.g.blockn) continue;
+        scatter_tile(it.g, it.ch, it.bd, it.sd, it.scratch, it.dense, it.ld, gb - bstart[k], i0, planes);
+    }
+}
+
+template <int TS>
+__global__ void __launch_bounds__(256) k_gather_fast_g(const CodecItem *__restrict__ items,
+                                                       const int64_t *__restrict__ bstart, int n, int64_t nbl)
+{
+    for (int64_t u = blockIdx.x; u < nbl; u += gridDim.x) {
+        const int k = group_find(bstart, n, u);
+        const CodecItem &it = items[k];
+        gather_fast_block<TS>(it.g, it.dense, it.ld, it.img, u - bstart[k]);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_gather_g(const CodecItem *__restrict__ items, const int64_t *__restrict__ bstart,
+                                                  int n, int64_t nbl, int64_t tpb, bool skip_fast, bool shuffle)
+{
+    __shared__ __align__(16) uint8_t planes[8 * TILE];
+    for (int64_t w = blockIdx.x; w < nbl * tpb; w += gridDim.x) {
+        const int64_t gb = w / tpb, i0 = (w - gb * tpb) * TILE;
+        const int k = group_find(bstart, n, gb);
+        const CodecItem &it = items[k];
+        if (i0 >= it.g.blockn) continue;
+        if (skip_fast && geom_fast(it.g)) continue;
+        gather_tile(it.g, it.dense, it.ld, shuffle, it.img, gb - bstart[k], i0, planes);
+    }
+}
+
+__global__ void __launch_bounds__(LAYOUT_T) k_layout_g(const CodecItem *__restrict__ items,
+                                                      const int64_t *__restrict__ cstart, int n, int nstreams,
+                                                      int neblock, int memcpy_only)
+{
+    __shared__ int64_t wsum[LAYOUT_T / 32];
+    __shared__ int64_t s_before;
+    __shared__ int s_first;
+    const int64_t u = blockIdx.x;
+    const int k = group_find(cstart, n, u);
+    const CodecItem &it = items[k];
+    layout_chunk(it.g, nstreams, neblock, it.es, it.ec, memcpy_only, u - cstart[k], wsum, s_before, s_first);
+}
+
+__global__ void __launch_bounds__(1024) k_chunk_offsets_g(CodecItem *items)
+{
+    __shared__ int64_t wsum[32];
+    CodecItem &it = items[blockIdx.x];
+    chunk_offsets(it.g.nchunks, it.ec, &it.out_bytes, wsum);
+}
+
+__global__ void __launch_bounds__(256) k_emit_g(const CodecItem *__restrict__ items, const int64_t *__restrict__ bstart,
+                                                int n, int64_t nbl, int nstreams, int neblock, bool shuffle, int splitflag)
+{
+    for (int64_t u = blockIdx.x; u < nbl; u += gridDim.x) {
+        const int k = group_find(bstart, n, u);
+        const CodecItem &it = items[k];
+        const int64_t img_bytes = it.g.nchunks * it.g.nblocks * it.g.blocksize;
+        emit_block(it.g, nstreams, neblock, shuffle, splitflag, it.img, it.slots, img_bytes, it.es, it.ec, it.outbuf,
+                   u - bstart[k]);
+    }
+}
+
+// Start tables (blocks, fast-scatter slices, chunks; n + 1 entries each) and the item table
+// on the device.  Synchronises `st` (setup only, before any capture).
+static int group_upload(CodecGroup *grp, cudaStream_t st)
+{
+    const int n = grp->n;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::vector<int64_t> s(3 * (size_t)(n + 1), 0);
+    for (int k = 0; k < n; k++) {
+        const Geom &g = grp->h[(size_t)k].g;
+        const int64_t nbl = g.nchunks * g.nblocks;
+        s[(size_t)k + 1] = s[(size_t)k] + nbl;
+        s[(size_t)(n + 1) + k + 1] = s[(size_t)(n + 1) + k] + nbl * ((g.blockn + SC_ITEMS - 1) / SC_ITEMS);
+        s[(size_t)(2 * (n + 1)) + k + 1] = s[(size_t)(2 * (n + 1)) + k] + g.nchunks;
+    }
+    grp->nbl = s[(size_t)n];
+    grp->nsf = s[(size_t)(2 * n + 1)];
+    grp->nch = s[(size_t)(3 * n + 2)];
+    if (grp->nbl > INT32_MAX) return -102;
+    if (!grp->items.allocate(sizeof(CodecItem) * (size_t)n, dev) || !grp->starts.allocate(sizeof(int64_t) * s.size(), dev))
+        return -100;
+    cudaMemcpyAsync(grp->items.p, grp->h.data(), sizeof(CodecItem) * (size_t)n, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(grp->starts.p, s.data(), sizeof(int64_t) * s.size(), cudaMemcpyHostToDevice, st);
+    return cudaStreamSynchronize(st) == cudaSuccess ? 0 : -101;
+}
+
+int decode_group_setup(const std::vector<DecodeArgs> &a, const std::vector<int *> &cnt, CodecGroup *grp, cudaStream_t st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int n = (int)a.size();
+    if (n <= 0 || cnt.size() != a.size()) return -102;
+    grp->n = n;
+    grp->ts = a[0].g.itemsize;
+    int64_t nbl = 0, img = 0, jobs = 0;
+    grp->max_tpb = 1;
+    for (const DecodeArgs &x : a) {
+        if (x.g.itemsize != grp->ts) return 1;
+        nbl += x.g.nchunks * x.g.nblocks;
+        img += x.g.nchunks * x.g.nblocks * x.g.blocksize;
+        jobs += decode_max_jobs(x.g);
+        grp->max_tpb = std::max<int64_t>(grp->max_tpb, (x.g.blockn + TILE - 1) / TILE);
+    }
+    if (!grp->bd.allocate(sizeof(BlockDesc) * (size_t)std::max<int64_t>(nbl, 1), dev) ||
+        !grp->sd.allocate(sizeof(StreamDesc) * 8 * (size_t)std::max<int64_t>(nbl, 1), dev) ||
+        !grp->scratch.allocate((size_t)std::max<int64_t>(img, 16), dev) ||
+        !grp->rest.allocate(sizeof(int) * (size_t)std::max<int64_t>(nbl, 1), dev) || !grp->counters.allocate(128, dev))
+        return -100;
+    int r = decode_queue_init(&grp->q, jobs, st);
+    if (r) return r;
+    grp->h.assign((size_t)n, CodecItem{});
+    int64_t bo = 0, io = 0;
+    for (int k = 0; k < n; k++) {
+        const DecodeArgs &x = a[(size_t)k];
+        CodecItem &it = grp->h[(size_t)k];
+        it.g = x.g;
+        it.ch = x.chunks; it.ch_bytes = x.chunks_bytes; it.off = x.off; it.len = x.len;
+        it.bd = grp->bd.as<BlockDesc>() + bo;
+        it.sd = grp->sd.as<StreamDesc>() + bo * 8;
+        it.scratch = grp->scratch.as<uint8_t>() + io;
+        it.dense = static_cast<uint8_t *>(x.out);
+        it.ld = x.ld;
+        it.cnt = cnt[(size_t)k];
+        bo += x.g.nchunks * x.g.nblocks;
+        io += x.g.nchunks * x.g.nblocks * x.g.blocksize;
+    }
+    return group_upload(grp, st);
+}
+
+int decode_group_launch(CodecGroup *grp, cudaStream_t st)
+{
+    const int n = grp->n, sms = sm_count();
+    const CodecItem *items = grp->items.as<CodecItem>();
+    const int64_t *bstart = grp->starts.as<int64_t>(), *sstart = bstart + (n + 1);
+    int *gc = grp->counters.as<int>();
+    cudaMemsetAsync(grp->q.counters.p, 0, 64, st);
+    cudaMemsetAsync(gc, 0, 128, st);
+    IAB_TIMED("k_group_reset", st, k_group_reset<<<(unsigned)((n * 16 + 255) / 256), 256, 0, st>>>(items, n));
+    if (grp->nbl == 0) return 0;
+    const int64_t pb = std::min<int64_t>((grp->nbl + 127) / 128, (int64_t)sms * 16);
+    IAB_TIMED("k_parse", st, k_parse_g<<<(unsigned)pb, 128, 0, st>>>(items, bstart, n, grp->nbl, grp->q.jobs.as<Lz4Job>(),
+                                                                     grp->q.counters.as<int>(), grp->q.cap));
+    int r = decode_lz4(&grp->q, st);
+    if (r) return r;
+    const bool fast = grp->ts == 4 || grp->ts == 8;
+    if (fast) {
+        static int per_sm[2] = {0, 0};
+        const int slot = grp->ts == 8;
+        if (!per_sm[slot]) {
+            int m = 0;
+            const cudaError_t e = slot ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_scatter_fast_g<8>, 256, 0)
+                                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_scatter_fast_g<4>, 256, 0);
+            if (e != cudaSuccess || m < 1) { cudaGetLastError(); m = 4; }
+            per_sm[slot] = m;
+        }
+        const int64_t grid = std::max<int64_t>(std::min<int64_t>(grp->nsf, (int64_t)sms * per_sm[slot]), 1);
+        if (slot)
+            IAB_TIMED("k_scatter_fast", st, k_scatter_fast_g<8><<<(unsigned)grid, 256, 0, st>>>(
+                items, bstart, sstart, n, grp->nsf, grp->rest.as<int>(), gc));
+        else
+            IAB_TIMED("k_scatter_fast", st, k_scatter_fast_g<4><<<(unsigned)grid, 256, 0, st>>>(
+                items, bstart, sstart, n, grp->nsf, grp->rest.as<int>(), gc));
+    }
+    const int64_t sb = std::min<int64_t>(grp->nbl * grp->max_tpb, (int64_t)sms * 8);
+    IAB_TIMED("k_scatter", st, k_scatter_g<<<(unsigned)std::max<int64_t>(sb, 1), 256, 0, st>>>(
+        items, bstart, n, fast ? grp->rest.as<int>() : nullptr, fast ? gc : nullptr, grp->nbl, grp->max_tpb));
+    return 0;
+}
+
+int encode_group_setup(const std::vector<Geom> &g, const std::vector<const void *> &dense, const std::vector<int64_t> &ld,
+                       const std::vector<EncChunk *> &ec, std::vector<DevBuf> *out, CodecGroup *grp, cudaStream_t st)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int n = (int)g.size();
+    if (n <= 0 || dense.size() != g.size() || ld.size() != g.size() || ec.size() != g.size() || out->size() != g.size())
+        return -102;
+    grp->n = n;
+    grp->ts = g[0].itemsize;
+    grp->shuffle = true;
+    grp->nstreams = encode_nstreams(g[0], true, 3 /* automatic split */);
+    grp->split = encode_split(g[0], true, 3);
+    grp->neblock = (int)(g[0].blocksize / grp->nstreams);
+    grp->max_tpb = 1;
+    int64_t img = 0, ns = 0;
+    for (const Geom &x : g) {
+        const int nsx = encode_nstreams(x, true, 3);
+        if (x.itemsize != grp->ts || nsx != grp->nstreams || x.blocksize / nsx != grp->neblock ||
+            encode_split(x, true, 3) != grp->split)
+            return 1;
+        img += x.nchunks * x.nblocks * x.blocksize;
+        ns += x.nchunks * x.nblocks * nsx;
+        grp->max_tpb = std::max<int64_t>(grp->max_tpb, (x.blockn + TILE - 1) / TILE);
+    }
+    if (!grp->img.allocate((size_t)std::max<int64_t>(img, 16), dev) || !grp->slots.allocate((size_t)std::max<int64_t>(img, 16), dev) ||
+        !grp->es.allocate(sizeof(EncStream) * (size_t)std::max<int64_t>(ns, 1), dev) || !grp->counters.allocate(128, dev))
+        return -100;
+    grp->h.assign((size_t)n, CodecItem{});
+    int64_t io = 0, so = 0;
+    for (int k = 0; k < n; k++) {
+        const Geom &x = g[(size_t)k];
+        if (!(*out)[(size_t)k].allocate((size_t)std::max<int64_t>(x.nchunks * (x.chunk_nbytes + 32), 16), dev)) return -100;
+        CodecItem &it = grp->h[(size_t)k];
+        it.g = x;
+        it.dense = const_cast<uint8_t *>(static_cast<const uint8_t *>(dense[(size_t)k]));
+        it.ld = ld[(size_t)k];
+        it.img = grp->img.as<uint8_t>() + io;
+        it.slots = grp->slots.as<uint8_t>() + io;
+        it.es = grp->es.as<EncStream>() + so;
+        it.ec = ec[(size_t)k];
+        it.outbuf = (*out)[(size_t)k].as<uint8_t>();
+        io += x.nchunks * x.nblocks * x.blocksize;
+        so += x.nchunks * x.nblocks * grp->nstreams;
+    }
+    return group_upload(grp, st);
+}
+
+int encode_group_launch(CodecGroup *grp, bool exact_lz4, bool memcpy_only, cudaStream_t st)
+{
+    const int n = grp->n, sms = sm_count(), ts = grp->ts;
+    CodecItem *items = grp->items.as<CodecItem>();
+    const int64_t *bstart = grp->starts.as<int64_t>(), *cstart = bstart + 2 * (n + 1);
+    if (grp->nbl == 0) return 0;
+    cudaMemsetAsync(grp->counters.p, 0, 128, st);
+    const bool fast = grp->shuffle && (ts == 4 || ts == 8);
+    bool all_fast = fast;
+    for (const CodecItem &it : grp->h) {
+        const Geom &g = it.g;
+        all_fast = all_fast && !(g.block[1] & 3);
+    }
+    const int64_t gb = std::max<int64_t>(std::min<int64_t>(grp->nbl, (int64_t)sms * 8), 1);
+    if (fast) {
+        if (ts == 8)
+            IAB_TIMED("k_gather_fast", st, k_gather_fast_g<8><<<(unsigned)gb, 256, 0, st>>>(items, bstart, n, grp->nbl));
+        else
+            IAB_TIMED("k_gather_fast", st, k_gather_fast_g<4><<<(unsigned)gb, 256, 0, st>>>(items, bstart, n, grp->nbl));
+    }
+    if (!all_fast) {
+        const int64_t tb = std::max<int64_t>(std::min<int64_t>(grp->nbl * grp->max_tpb, (int64_t)sms * 8), 1);
+        IAB_TIMED("k_gather", st, k_gather_g<<<(unsigned)tb, 256, 0, st>>>(items, bstart, n, grp->nbl, grp->max_tpb, fast,
+                                                                           grp->shuffle));
+    }
+    if (!memcpy_only)
+        encode_streams(grp->img.as<uint8_t>(), grp->nbl * grp->nstreams, grp->neblock, grp->slots.as<uint8_t>(),
+                       grp->es.as<EncStream>(), reinterpret_cast<unsigned long long *>(grp->counters.as<uint8_t>() + 64),
+                       exact_lz4, st);
+    IAB_TIMED("k_layout", st, k_layout_g<<<(unsigned)std::max<int64_t>(grp->nch, 1), LAYOUT_T, 0, st>>>(
+        items, cstart, n, grp->nstreams, grp->neblock, memcpy_only ? 1 : 0));
+    IAB_TIMED("k_chunk_offsets", st, k_chunk_offsets_g<<<(unsigned)n, 1024, 0, st>>>(items));
+    IAB_TIMED("k_emit", st, k_emit_g<<<(unsigned)gb, 256, 0, st>>>(items, bstart, n, grp->nbl, grp->nstreams, grp->neblock,
+                                                                   grp->shuffle, grp->split ? 1 : 0));
+    return 0;
 }
 
 // ============================================================================ decode without allocation

@@ -242,6 +242,51 @@ void encode_streams(const uint8_t *img, int64_t ns, int neblock, uint8_t *slots,
 int encode_emit(const Geom &g, bool shuffle, int splitmode, DevBuf *d_out, EncodeWork *w, cudaStream_t st);
 int encode_finish(EncodeWork *w, std::vector<int64_t> *h_off, std::vector<int32_t> *h_len, cudaStream_t st);
 
+// Grouped codec (batches): every stage of the decode (parse, LZ4, scatter) or of the encode
+// (gather, LZ4, layout, chunk offsets, emit) is one launch over the blocks or chunks of all
+// containers of the group; a unit finds its container by binary search of the group's start
+// tables.  The containers share one item size (and, for the encode, one stream size).
+struct CodecItem {                // one container of a group (device table entry)
+    Geom g;
+    const uint8_t *ch;            // decode: the container's chunks back to back
+    int64_t ch_bytes;
+    const int64_t *off;           // decode: chunk offsets and lengths
+    const int32_t *len;
+    BlockDesc *bd;                // decode work: descriptors, decoded-stream image
+    StreamDesc *sd;
+    uint8_t *scratch;
+    uint8_t *dense;               // decode destination / encode source (row-major)
+    int64_t ld;                   // its leading dimension in items
+    int *cnt;                     // the container's status words ([1] decode error)
+    uint8_t *img, *slots;         // encode: byte-plane image, LZ4 slots, stream results,
+    EncStream *es;                // chunk table and output chunks (slices of shared buffers)
+    EncChunk *ec;
+    uint8_t *outbuf;
+    int64_t out_bytes;            // total size of the output chunks (written by the encode)
+};
+struct CodecGroup {
+    int n = 0, ts = 0;
+    int nstreams = 0, neblock = 0;         // encode: the shared stream shape
+    int64_t nbl = 0, nch = 0, nsf = 0;     // blocks, chunks, fast-scatter slices of all containers
+    int64_t max_tpb = 0;                   // general-path tiles per block (largest over containers)
+    bool shuffle = true, split = true;     // encode: byte shuffle, one stream per item byte
+    std::vector<CodecItem> h;              // host copy of the table
+    DevBuf items, starts;                  // device table; starts: blocks, slices, chunks ([n + 1] each)
+    DevBuf bd, sd, scratch, rest, counters;   // decode work shared by the group; counters: [0] rest length, [2..] LZ4 cursor
+    DevBuf img, slots, es, outsz;          // encode work shared by the group
+    DecodeQueue q;
+};
+// Decode group: a[i] is container i (all of item size ts), cnt[i] its 16-int status slot.
+int decode_group_setup(const std::vector<DecodeArgs> &a, const std::vector<int *> &cnt, CodecGroup *grp, cudaStream_t st);
+// Enqueues the decode of every container of the group (three kernel launches and the resets).
+int decode_group_launch(CodecGroup *grp, cudaStream_t st);
+// Encode group: container i from dense[i] (leading dimension ld[i]) into out[i] (allocated
+// here), chunk table ec[i] (device, g[i].nchunks entries).  Returns 1 when the containers do
+// not share one item size and one stream shape (the caller encodes them one by one).
+int encode_group_setup(const std::vector<Geom> &g, const std::vector<const void *> &dense, const std::vector<int64_t> &ld,
+                       const std::vector<EncChunk *> &ec, std::vector<DevBuf> *out, CodecGroup *grp, cudaStream_t st);
+int encode_group_launch(CodecGroup *grp, bool exact_lz4, bool memcpy_only, cudaStream_t st);
+
 // Dense products (row-major, leading dimensions in items).
 // zs (optional): leave out the K ranges of zero-block pairs (zskip.cuh)
 void gemm_f64_native(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda,

@@ -35,7 +35,8 @@ def test_batch_matches_single_products(ia, form):
     As, Bs, cs, bs = _problems(ia, ctx, rng, 12)
     batch = ia.Batch(ctx, As, Bs, cs, bs)
     info = batch.info()
-    assert info["graph_nodes"] > 0
+    # grouped decode, product and encode: a few launches per stage for all problems
+    assert 0 < info["graph_nodes"] <= 32, info
     if form == "native":
         assert info["tile_config"] in (0, 1, 2, 3)
     else:
