@@ -443,9 +443,12 @@ INA_API(ina_rc_t) iarray_b200_batch_new(iarray_context_t *ctx, int64_t n, iarray
                                         iarray_container_t *const *b, const iarray_storage_t *storage,
                                         iarray_b200_batch_t **batch);
 INA_API(ina_rc_t) iarray_b200_batch_run(iarray_b200_batch_t *batch, iarray_container_t **c);
-/* Tile configuration chosen by the autotuner (0: 128x128, 1: 64x128, 2: 128x64, 3: 64x64;
- * -1 in the split form), the tuning times of the four configurations in ms (-1: not
- * measured, e.g. a cached choice), and the number of nodes of the captured graph. */
+/* Tile configuration chosen by the autotuner (-1 in the split form): cfg & 3 is the tile
+ * shape (0: 128x128, 1: 64x128, 2: 128x64, 3: 64x64), cfg < 4 pipeline stages 16 deep in
+ * k, cfg >= 4 32 deep; the tuning times of the IARRAY_B200_BATCH_TILE_CONFIGS
+ * configurations in ms (-1: not measured, e.g. a cached choice); and the number of nodes
+ * of the captured graph. */
+#define IARRAY_B200_BATCH_TILE_CONFIGS 8
 INA_API(ina_rc_t) iarray_b200_batch_info(iarray_b200_batch_t *batch, int *tile_config, double *tune_ms,
                                          int64_t *graph_nodes);
 /* Split form: the number of moduli the batch uses.  When the context's count is automatic

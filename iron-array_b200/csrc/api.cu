@@ -1789,7 +1789,7 @@ struct iarray_b200_batch_s {
     DevBuf probs;
     std::vector<iab::GemmProblem> hprobs;
     int cfg = 0, ctas = 0, total_tiles = 0;
-    double tune_ms[4] = {-1, -1, -1, -1};
+    double tune_ms[iab::GEMM_F64_GROUPED_CONFIGS] = {-1, -1, -1, -1, -1, -1, -1, -1};
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int64_t nodes = 0;
@@ -2114,7 +2114,7 @@ INA_API(ina_rc_t) iarray_b200_batch_new(iarray_context_t *ctx, int64_t n, iarray
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
-        for (int cfg = 0; cfg < 4 && !cached; cfg++) {
+        for (int cfg = 0; cfg < iab::GEMM_F64_GROUPED_CONFIGS && !cached; cfg++) {
             std::vector<iab::GemmProblem> hp;
             int total = 0;
             batch_problems(bt.get(), cfg, &hp, &total);
@@ -2249,7 +2249,7 @@ INA_API(ina_rc_t) iarray_b200_batch_info(iarray_b200_batch_t *bt, int *tile_conf
     CHECK_ARG(bt);
     if (tile_config) *tile_config = bt->form == IARRAY_B200_FORM_SPLIT ? -1 : bt->cfg;
     if (tune_ms)
-        for (int k = 0; k < 4; k++) tune_ms[k] = bt->tune_ms[k];
+        for (int k = 0; k < iab::GEMM_F64_GROUPED_CONFIGS; k++) tune_ms[k] = bt->tune_ms[k];
     if (graph_nodes) *graph_nodes = bt->nodes;
     return INA_SUCCESS;
 }

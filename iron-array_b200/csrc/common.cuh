@@ -298,7 +298,9 @@ void gemv_native(int dtype, int64_t M, int64_t K, const void *A, int64_t lda, co
                  void *y, cudaStream_t st);
 // Grouped FP64 product: many independent C_p = A_p B_p in one persistent launch.
 // tile_start is the first global tile of problem p for the chosen tile configuration
-// (cfg 0: 128x128, 1: 64x128, 2: 128x64, 3: 64x64); problems are listed in tile order.
+// (cfg & 3 the tile shape, 0: 128x128, 1: 64x128, 2: 128x64, 3: 64x64; cfg < 4: 16 k per
+// pipeline stage, else 32); problems are listed in tile order.
+constexpr int GEMM_F64_GROUPED_CONFIGS = 8;
 struct GemmProblem {
     int M, N, K, tile_start;
     const double *A;

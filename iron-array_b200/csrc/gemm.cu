@@ -8,7 +8,7 @@
 // (sum over K blocks of A_blk * B_blk == the dense product over the padded extents,
 // because Caterva's padding is zero).
 //
-// FP64: DMMA tensor-core tiles (mma.sync m16n8k4 .f64), 128x128x16 CTA tile,
+// FP64: DMMA tensor-core tiles (mma.sync m16n8k16 .f64), 128x128x32 CTA tile,
 //       8 warps (64x32 each), 3-stage cp.async pipeline with zero-filled edges.
 // FP32: FFMA SIMT tiles, 128x128x8, 8x8 outer product per thread, double buffer.
 // GEMV: one warp per row, 16-byte loads.
@@ -39,36 +39,43 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 // ============================================================================ FP64 DMMA
 namespace f64k {
-constexpr int BK = 16, STAGES = 3;
-constexpr int SA = BK + 4;    // A tile row stride (doubles): 20 = 4 mod 16 -> conflict-free fragments
-template <int BM, int BN> struct Cfg {
-    static constexpr int SB = BN + 4;                    // B tile row stride: 4 mod 16
+constexpr int STAGES = 3;
+// BK: k-depth of a pipeline stage (16 or 32; the single product uses 32, the grouped
+// autotuner tries both).  Row strides are 4 mod 16 doubles: conflict-free fragments.
+template <int BM, int BN, int BK> struct Cfg {
+    static constexpr int SA = BK + 4, SB = BN + 4;
     static constexpr int A_STAGE = BM * SA, B_STAGE = BK * SB;
     static constexpr int SMEM = STAGES * (A_STAGE + B_STAGE) * 8;
     static constexpr int MI = BM / 32, NJ = BN / 32;     // 2 x 4 warps, warp tile (BM/2) x (BN/4)
 };
+constexpr int BK_SINGLE = 32;
 }
 
-__device__ __forceinline__ void dmma_16x8x4(double (&d)[4], const double (&a)[2], double b)
+// D += A B for one 16x8 tile over k = 16 (a: rows g, g + 8 at columns q + 4u; b: rows q + 4u
+// at column g).  The products are summed in k order, as sixteen m16n8k1 steps would.
+__device__ __forceinline__ void dmma_16x8x16(double (&d)[4], const double (&a)[8], const double (&b)[4])
 {
     asm volatile(
-        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+        "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+        "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
         : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-        : "d"(a[0]), "d"(a[1]), "d"(b));
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+          "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
 // One BM x BN tile of C = A B at (m0, n0), 256 threads.  Requires lda, ldb even and
 // 16-byte aligned bases (true for the library's dense buffers).  With `klist`, only the
 // nk k-tiles it lists (ascending) are multiplied: the others are pairs of zero blocks the
 // block-pair product skips; without it, all k-tiles.
-template <int BM, int BN>
+template <int BM, int BN, int BK>
 __device__ __forceinline__ void f64_tile(int M, int N, int K, const double *__restrict__ A, int64_t lda,
                                          const double *__restrict__ B, int64_t ldb, double *__restrict__ C,
                                          int64_t ldc, int m0, int n0, double *smf64, const uint16_t *klist = nullptr,
                                          int nk = -1)
 {
     using namespace f64k;
-    using G = Cfg<BM, BN>;
+    using G = Cfg<BM, BN, BK>;
+    constexpr int SA = G::SA;
     double *sA = smf64, *sB = smf64 + STAGES * G::A_STAGE;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int wm = warp >> 2, wn = warp & 3;
@@ -79,8 +86,8 @@ __device__ __forceinline__ void f64_tile(int M, int N, int K, const double *__re
         const int k0 = kt * BK;
         double *a = sA + s * G::A_STAGE, *b = sB + s * G::B_STAGE;
 #pragma unroll
-        for (int i = 0; i < BM / 32; i++) {      // A: BM rows x 8 16-byte pieces
-            const int idx = tid + i * 256, r = idx >> 3, cpc = (idx & 7) * 2;
+        for (int i = 0; i < BM * BK / 512; i++) {      // A: BM rows x BK/2 16-byte pieces
+            const int idx = tid + i * 256, r = idx / (BK / 2), cpc = (idx % (BK / 2)) * 2;
             const int gr = m0 + r, gk = k0 + cpc;
             // the two doubles at gk, gk + 1 that lie inside the row (K may be odd: the padding
             // column after it is never read, it may hold anything)
@@ -88,7 +95,7 @@ __device__ __forceinline__ void f64_tile(int M, int N, int K, const double *__re
             cp_async16(a + r * SA + cpc, nb ? (const void *)(A + (int64_t)gr * lda + gk) : (const void *)A, nb);
         }
 #pragma unroll
-        for (int i = 0; i < BN / 32; i++) {      // B: 16 rows x BN/2 pieces
+        for (int i = 0; i < BN * BK / 512; i++) {      // B: BK rows x BN/2 pieces
             const int idx = tid + i * 256, r = idx / (BN / 2), cpc = (idx % (BN / 2)) * 2;
             const int gk = k0 + r, gn = n0 + cpc;
             const int nb = gk < K ? 8 * max(0, min(2, N - gn)) : 0;
@@ -119,19 +126,23 @@ __device__ __forceinline__ void f64_tile(int M, int N, int K, const double *__re
         const double *a = sA + (kt % STAGES) * G::A_STAGE + (wm * (BM / 2)) * SA;
         const double *b = sB + (kt % STAGES) * G::B_STAGE + wn * (BN / 4);
 #pragma unroll
-        for (int kk = 0; kk < BK; kk += 4) {
-            double af[G::MI][2], bf[G::NJ];
+        for (int kk = 0; kk < BK; kk += 16) {
+            double bf[G::NJ][4];
+#pragma unroll
+            for (int j = 0; j < G::NJ; j++)
+#pragma unroll
+                for (int u = 0; u < 4; u++) bf[j][u] = b[(kk + q + 4 * u) * G::SB + j * 8 + g];
 #pragma unroll
             for (int i = 0; i < G::MI; i++) {
-                af[i][0] = a[(i * 16 + g) * SA + kk + q];
-                af[i][1] = a[(i * 16 + g + 8) * SA + kk + q];
+                double af[8];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    af[2 * u] = a[(i * 16 + g) * SA + kk + q + 4 * u];
+                    af[2 * u + 1] = a[(i * 16 + g + 8) * SA + kk + q + 4 * u];
+                }
+#pragma unroll
+                for (int j = 0; j < G::NJ; j++) dmma_16x8x16(acc[i][j], af, bf[j]);
             }
-#pragma unroll
-            for (int j = 0; j < G::NJ; j++) bf[j] = b[(kk + q) * G::SB + j * 8 + g];
-#pragma unroll
-            for (int i = 0; i < G::MI; i++)
-#pragma unroll
-                for (int j = 0; j < G::NJ; j++) dmma_16x8x4(acc[i][j], af[i], bf[j]);
         }
     }
     cp_async_wait<0>();
@@ -160,29 +171,30 @@ __global__ void __launch_bounds__(256) k_gemm_f64(int M, int N, int K, const dou
                                                   int64_t ldc)
 {
     extern __shared__ __align__(16) double smf64[];
-    f64_tile<128, 128>(M, N, K, A, lda, B, ldb, C, ldc, blockIdx.y * 128, blockIdx.x * 128, smf64);
+    f64_tile<128, 128, f64k::BK_SINGLE>(M, N, K, A, lda, B, ldb, C, ldc, blockIdx.y * 128, blockIdx.x * 128, smf64);
 }
 
 // The same product where the K ranges of zero-block pairs are left out: each CTA lists the
 // k-tiles its tile needs (zs_tile_active) in shared memory, compacted by warp ballots, and
 // multiplies only those.  K <= ZS_MAX_K.
 constexpr int ZS_MAX_K = 65536;
-constexpr int ZS_LIST_BYTES = (ZS_MAX_K / f64k::BK) * 3 + 64;    // flags + uint16 list + count
+constexpr int ZS_LIST_BYTES = (ZS_MAX_K / f64k::BK_SINGLE) * 3 + 64;    // flags + uint16 list + count
 __global__ void __launch_bounds__(256) k_gemm_f64_skip(int M, int N, int K, const double *__restrict__ A, int64_t lda,
                                                        const double *__restrict__ B, int64_t ldb, double *__restrict__ C,
                                                        int64_t ldc, ZeroSkip z)
 {
-    using G = f64k::Cfg<128, 128>;
+    constexpr int BK = f64k::BK_SINGLE;
+    using G = f64k::Cfg<128, 128, BK>;
     extern __shared__ __align__(16) double smf64[];
     uint8_t *extra = reinterpret_cast<uint8_t *>(smf64 + f64k::STAGES * (G::A_STAGE + G::B_STAGE));
-    const int ktiles = (K + f64k::BK - 1) / f64k::BK;
+    const int ktiles = (K + BK - 1) / BK;
     int *count = reinterpret_cast<int *>(extra);
     uint16_t *list = reinterpret_cast<uint16_t *>(extra + 16);
     uint8_t *flag = extra + 16 + 2 * ktiles;
     const int m0 = blockIdx.y * 128, n0 = blockIdx.x * 128;
     const int64_t r1 = min(m0 + 128, M), c1 = min(n0 + 128, N);
     for (int kt = threadIdx.x; kt < ktiles; kt += blockDim.x)
-        flag[kt] = zs_tile_active(z, m0, r1, n0, c1, (int64_t)kt * f64k::BK, min((kt + 1) * f64k::BK, K)) ? 1 : 0;
+        flag[kt] = zs_tile_active(z, m0, r1, n0, c1, (int64_t)kt * BK, min((kt + 1) * BK, K)) ? 1 : 0;
     __syncthreads();
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
@@ -196,13 +208,13 @@ __global__ void __launch_bounds__(256) k_gemm_f64_skip(int M, int N, int K, cons
         if (lane == 0) *count = c;
     }
     __syncthreads();
-    f64_tile<128, 128>(M, N, K, A, lda, B, ldb, C, ldc, m0, n0, smf64, list, *count);
+    f64_tile<128, 128, BK>(M, N, K, A, lda, B, ldb, C, ldc, m0, n0, smf64, list, *count);
 }
 
 void gemm_f64_native(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B, int64_t ldb,
                      double *C, int64_t ldc, cudaStream_t st, const ZeroSkip *zs)
 {
-    using G = f64k::Cfg<128, 128>;
+    using G = f64k::Cfg<128, 128, f64k::BK_SINGLE>;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_gemm_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
@@ -211,7 +223,7 @@ void gemm_f64_native(int64_t M, int64_t N, int64_t K, const double *A, int64_t l
     }
     dim3 grid((unsigned)((N + 127) / 128), (unsigned)((M + 127) / 128));
     if (zs && K <= ZS_MAX_K) {
-        const int ktiles = (int)((K + f64k::BK - 1) / f64k::BK);
+        const int ktiles = (int)((K + f64k::BK_SINGLE - 1) / f64k::BK_SINGLE);
         const int smem = G::SMEM + 3 * ktiles + 64;
         IAB_TIMED("k_gemm_f64", st, k_gemm_f64_skip<<<grid, 256, smem, st>>>((int)M, (int)N, (int)K, A, lda, B, ldb, C,
                                                                            ldc, *zs));
@@ -223,7 +235,7 @@ void gemm_f64_native(int64_t M, int64_t N, int64_t K, const double *A, int64_t l
 // Grouped form: one persistent launch over the tiles of many independent products.
 // Problem p owns global tiles [tile_start, tile_start + tiles_m * tiles_n); CTAs take
 // tiles round-robin and find their problem by binary search.
-template <int BM, int BN>
+template <int BM, int BN, int BK>
 __global__ void __launch_bounds__(256) k_gemm_f64_grouped(const GemmProblem *__restrict__ probs, int nprob,
                                                           int total_tiles)
 {
@@ -237,37 +249,40 @@ __global__ void __launch_bounds__(256) k_gemm_f64_grouped(const GemmProblem *__r
         const GemmProblem &p = probs[lo];
         const int local = t - p.tile_start, tn_count = (p.N + BN - 1) / BN;
         const int tm = local / tn_count, tn = local - tm * tn_count;
-        f64_tile<BM, BN>(p.M, p.N, p.K, p.A, p.lda, p.B, p.ldb, p.C, p.ldc, tm * BM, tn * BN, smf64);
+        f64_tile<BM, BN, BK>(p.M, p.N, p.K, p.A, p.lda, p.B, p.ldb, p.C, p.ldc, tm * BM, tn * BN, smf64);
         __syncthreads();
     }
 }
 
+// Tile configuration cfg: shape (cfg & 3: 128x128, 64x128, 128x64, 64x64), stage depth
+// (cfg < 4: 16, else 32 k per stage).
 int gemm_f64_grouped_tiles(int cfg, int M, int N)
 {
-    const int bm = (cfg == 0 || cfg == 2) ? 128 : 64, bn = (cfg == 0 || cfg == 1) ? 128 : 64;
+    const int s = cfg & 3;
+    const int bm = (s == 0 || s == 2) ? 128 : 64, bn = (s == 0 || s == 1) ? 128 : 64;
     return ((M + bm - 1) / bm) * ((N + bn - 1) / bn);
 }
 
-template <int BM, int BN>
+template <int BM, int BN, int BK>
 static void launch_grouped(const GemmProblem *d_probs, int nprob, int total, int ctas, cudaStream_t st)
 {
-    using G = f64k::Cfg<BM, BN>;
+    using G = f64k::Cfg<BM, BN, BK>;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_gemm_f64_grouped<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+        cudaFuncSetAttribute(k_gemm_f64_grouped<BM, BN, BK>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
         attr = true;
     }
-    IAB_TIMED("k_gemm_f64_grouped", st, k_gemm_f64_grouped<BM, BN><<<(unsigned)std::max(1, std::min(ctas, total)), 256, G::SMEM, st>>>(
+    IAB_TIMED("k_gemm_f64_grouped", st, k_gemm_f64_grouped<BM, BN, BK><<<(unsigned)std::max(1, std::min(ctas, total)), 256, G::SMEM, st>>>(
         d_probs, nprob, total));
 }
 
-template <int BM, int BN>
+template <int BM, int BN, int BK>
 static int grouped_ctas()
 {
-    using G = f64k::Cfg<BM, BN>;
-    cudaFuncSetAttribute(k_gemm_f64_grouped<BM, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+    using G = f64k::Cfg<BM, BN, BK>;
+    cudaFuncSetAttribute(k_gemm_f64_grouped<BM, BN, BK>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
     int per_sm = 0, dev = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gemm_f64_grouped<BM, BN>, 256, G::SMEM) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gemm_f64_grouped<BM, BN, BK>, 256, G::SMEM) != cudaSuccess)
         per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -277,20 +292,28 @@ static int grouped_ctas()
 int gemm_f64_grouped_ctas(int cfg)
 {
     switch (cfg) {
-    case 0: return grouped_ctas<128, 128>();
-    case 1: return grouped_ctas<64, 128>();
-    case 2: return grouped_ctas<128, 64>();
-    default: return grouped_ctas<64, 64>();
+    case 0: return grouped_ctas<128, 128, 16>();
+    case 1: return grouped_ctas<64, 128, 16>();
+    case 2: return grouped_ctas<128, 64, 16>();
+    case 3: return grouped_ctas<64, 64, 16>();
+    case 4: return grouped_ctas<128, 128, 32>();
+    case 5: return grouped_ctas<64, 128, 32>();
+    case 6: return grouped_ctas<128, 64, 32>();
+    default: return grouped_ctas<64, 64, 32>();
     }
 }
 
 void gemm_f64_grouped(int cfg, const GemmProblem *d_probs, int nprob, int total_tiles, int ctas, cudaStream_t st)
 {
     switch (cfg) {
-    case 0: launch_grouped<128, 128>(d_probs, nprob, total_tiles, ctas, st); break;
-    case 1: launch_grouped<64, 128>(d_probs, nprob, total_tiles, ctas, st); break;
-    case 2: launch_grouped<128, 64>(d_probs, nprob, total_tiles, ctas, st); break;
-    default: launch_grouped<64, 64>(d_probs, nprob, total_tiles, ctas, st); break;
+    case 0: launch_grouped<128, 128, 16>(d_probs, nprob, total_tiles, ctas, st); break;
+    case 1: launch_grouped<64, 128, 16>(d_probs, nprob, total_tiles, ctas, st); break;
+    case 2: launch_grouped<128, 64, 16>(d_probs, nprob, total_tiles, ctas, st); break;
+    case 3: launch_grouped<64, 64, 16>(d_probs, nprob, total_tiles, ctas, st); break;
+    case 4: launch_grouped<128, 128, 32>(d_probs, nprob, total_tiles, ctas, st); break;
+    case 5: launch_grouped<64, 128, 32>(d_probs, nprob, total_tiles, ctas, st); break;
+    case 6: launch_grouped<128, 64, 32>(d_probs, nprob, total_tiles, ctas, st); break;
+    default: launch_grouped<64, 64, 32>(d_probs, nprob, total_tiles, ctas, st); break;
     }
 }
 

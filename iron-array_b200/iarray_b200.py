@@ -496,7 +496,7 @@ class Batch:
 
     def info(self):
         cfg = ctypes.c_int()
-        ms = (ctypes.c_double * 4)()
+        ms = (ctypes.c_double * 8)()             # IARRAY_B200_BATCH_TILE_CONFIGS
         nodes = ctypes.c_int64()
         check(_lib().iarray_b200_batch_info(self.ptr, ctypes.byref(cfg), ms, ctypes.byref(nodes)))
         return {"tile_config": cfg.value, "tune_ms": list(ms), "graph_nodes": nodes.value}

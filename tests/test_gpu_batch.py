@@ -38,7 +38,8 @@ def test_batch_matches_single_products(ia, form):
     # grouped decode, product and encode: a few launches per stage for all problems
     assert 0 < info["graph_nodes"] <= 32, info
     if form == "native":
-        assert info["tile_config"] in (0, 1, 2, 3)
+        assert info["tile_config"] in range(8)
+        assert len(info["tune_ms"]) == 8
     else:
         assert info["tile_config"] == -1
     for rep in range(2):                                    # graph replays
