@@ -733,7 +733,10 @@ def run_kernel_case(args):
     values (gaussian) encoded with the parallel encoder, then an A-like one
     (uniform(-1,1) x 2^U{-8..8}) decoded; three rounds each.  split: the split-precision
     float64 product n x n x n on device operands (iarray_b200_dense_gemm), two rounds.
-    f32split: the float32 split form (six BF16 products) n x n x n, two rounds.
+    f32split: the float32 split form (six BF16 products) n x n x n, two rounds.  gemv: the
+    plain GEMV workload's smooth float32 matrix at n x n (chunk 4000^2, block 500^2) decoded three
+    times, then one iarray_opt_gemv.  f64native: the native FP64 product n x n x n on device
+    operands, two rounds.
     Inputs are larger than L2 and a few GB at most are held on the device."""
     import ctypes
     import torch
@@ -753,6 +756,34 @@ def run_kernel_case(args):
             a.decode_to_device(out.data_ptr(), n)
         ctx.synchronize()
         assert np.array_equal(out.cpu().numpy(), A)
+    elif args.kernel_case == "gemv":
+        ctx = ia.Context(encoder=ia.ENCODER_PARALLEL)
+        A = (np.sin(0.001 * np.arange(n))[:, None] + np.cos(0.002 * np.arange(n))[None, :]).astype(np.float32)
+        a = ia.Container.from_numpy(ctx, A, (4000, 4000), (500, 500))
+        out = torch.empty((n, n), dtype=torch.float32, device="cuda")
+        for _ in range(3):
+            a.decode_to_device(out.data_ptr(), n)
+        ctx.synchronize()
+        assert np.array_equal(out.cpu().numpy(), A)
+        x = np.random.default_rng(2).uniform(-1, 1, n).astype(np.float32)
+        xc = ia.Container.from_numpy(ctx, x, (4000,), (500,))
+        y = ia.opt_gemv(ctx, a, xc, (4000,), (500,)).to_numpy().astype(np.float64)
+        ref = A.astype(np.float64) @ x.astype(np.float64)
+        assert np.linalg.norm(y - ref) / np.linalg.norm(ref) < 1e-5
+    elif args.kernel_case == "f64native":
+        ctx = ia.Context(form=ia.FORM_NATIVE)
+        A = torch.from_numpy(rng.uniform(-1, 1, (n, n))).cuda()
+        B = torch.from_numpy(rng.uniform(-1, 1, (n, n))).cuda()
+        C = torch.empty((n, n), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        for _ in range(2):
+            ia.check(ia.lib().iarray_b200_dense_gemm(ctx.ptr, ia.DTYPE_DOUBLE, n, n, n, ctypes.c_void_p(A.data_ptr()), n,
+                                                      ctypes.c_void_p(B.data_ptr()), n, ctypes.c_void_p(C.data_ptr()), n),
+                     "dense_gemm")
+        ctx.synchronize()
+        ref = (A[:64] @ B).cpu().numpy()
+        err = np.linalg.norm(C[:64].cpu().numpy() - ref) / np.linalg.norm(ref)
+        assert err < 1e-14, err
     elif args.kernel_case == "f32split":
         ctx = ia.Context(form=ia.FORM_SPLIT)
         A = torch.from_numpy(rng.standard_normal((n, n)).astype(np.float32)).cuda()
@@ -794,7 +825,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-samples", type=int, default=3, help="whole-product samples of the CPU baseline")
     ap.add_argument("--no-secondary", action="store_true", help="skip the GEMV, float32 and batching workloads")
-    ap.add_argument("--kernel-case", choices=["codec", "split", "f32split"], default=None,
+    ap.add_argument("--kernel-case", choices=["codec", "split", "f32split", "gemv", "f64native"], default=None,
                     help="run one small case of one kernel family instead of the benchmark")
     ap.add_argument("--case-n", type=int, default=4096, help="matrix size of --kernel-case")
     args = ap.parse_args()

@@ -1224,6 +1224,55 @@ struct ZeroRule {
     }
 };
 
+// y = A x with the GEMV fused into A's decode (iab::decode_gemv): x is decoded into dx, A's
+// streams through the parse and the LZ4 launch, then its items straight into the row sums.  When
+// the entry point's zero-block rule applies and the parse found zero blocks, A is also scattered
+// densely into *dA (leading dimension lda) from the same decoded streams and *zr is built, for
+// the caller's recomputation of the outputs the rule changes.
+static ina_rc_t gemv_fused(iarray_context_t *ctx, const iarray_container_t *a, const iarray_container_t *b, void *dx,
+                           void *dy, int skip, DevBuf *dA, int64_t lda, ZeroRule *zr)
+{
+    const Geom &g = a->geom;
+    DevBuf part;
+    if (!part.allocate((size_t)std::max<int64_t>(iab::decode_gemv_part_items(g) * g.itemsize, 16), ctx->device))
+        return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    const iab::DecodeArgs args[2] = {
+        {g, a->store->buf.as<uint8_t>(), (int64_t)a->store->buf.n, a->store->d_off.as<int64_t>(),
+         a->store->d_len.as<int32_t>(), nullptr, lda},
+        {b->geom, b->store->buf.as<uint8_t>(), (int64_t)b->store->buf.n, b->store->d_off.as<int64_t>(),
+         b->store->d_len.as<int32_t>(), dx, b->geom.shape[1]}};
+    iab::DecodeQueue q;
+    iab::DecodeWork w[2];
+    const bool xc = b->geom.nchunks > 0;
+    int r = iab::decode_queue_init(&q, iab::decode_max_jobs(g) + iab::decode_max_jobs(b->geom), ctx->stream);
+    if (!r) r = iab::decode_parse(args[0], &q, &w[0], ctx->stream);
+    if (!r && xc) r = iab::decode_parse(args[1], &q, &w[1], ctx->stream);
+    if (!r) r = iab::decode_lz4(&q, ctx->stream);
+    if (!r && xc) r = iab::decode_scatter(args[1], &w[1], ctx->stream);
+    if (!r) r = iab::decode_gemv(args[0], &w[0], dx, part.p, dy, ctx->stream);
+    if (!r) r = iab::decode_finish(&w[0], ctx->stream);
+    if (!r && xc) r = iab::decode_finish(&w[1], ctx->stream);
+    if (!r && skip != SKIP_NONE && w[0].nzero + (xc ? w[1].nzero : 0) > 0) {
+        if (!dA->allocate((size_t)std::max<int64_t>(g.shape[0] * lda * g.itemsize, 16), ctx->device)) {
+            cudaStreamSynchronize(ctx->stream);
+            return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+        }
+        iab::DecodeArgs da = args[0];
+        da.out = dA->p;
+        r = iab::decode_scatter(da, &w[0], ctx->stream);
+        if (!r) r = iab::decode_finish(&w[0], ctx->stream);
+        DevBuf zf[2];
+        zf[0] = std::move(w[0].zf);
+        if (xc) zf[1] = std::move(w[1].zf);
+        if (!r && !zr->build(ctx, g, b->geom, true, zf, skip)) {
+            cudaStreamSynchronize(ctx->stream);
+            return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+        }
+    }
+    if (r) cudaStreamSynchronize(ctx->stream);     // the work buffers go back to the pool idle
+    return decode_rc(r);
+}
+
 static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_container_t *b, iarray_container_t *c,
                            int skip = SKIP_NONE)
 {
@@ -1235,14 +1284,27 @@ static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_
     const int64_t lda = pad_ld(K), ldb = vec ? 1 : pad_ld(N), ldc = vec ? 1 : pad_ld(N);
     Timer tm(ctx);
     DevBuf dA, dB, dC;
-    if (!dA.allocate((size_t)std::max<int64_t>(M * lda * isz, 16), ctx->device) ||
+    // decode-fused GEMV: A's items go from its chunks straight into the row sums
+    const bool fused = vec && !a->transposed && !b->transposed && K > 0 && M > 0 && a->geom.nchunks &&
+                       b->geom.nchunks && iab::decode_gemv_fits(a->geom);
+    if ((!fused && !dA.allocate((size_t)std::max<int64_t>(M * lda * isz, 16), ctx->device)) ||
         !dB.allocate((size_t)std::max<int64_t>((vec ? pad_ld(K) : K * ldb) * isz, 16), ctx->device) ||
         !dC.allocate((size_t)std::max<int64_t>((vec ? pad_ld(M) : M * ldc) * isz, 16), ctx->device))
         return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
     if (vec) cudaMemsetAsync(dB.p, 0, (size_t)(pad_ld(K) * isz), ctx->stream);
     ina_rc_t rc;
     ZeroRule zr;
-    if (!a->transposed && !b->transposed) {
+    if (fused) {
+        rc = gemv_fused(ctx, a, b, dB.p, dC.p, skip, &dA, lda, &zr);
+        if (INA_FAILED(rc)) return rc;
+        tm.mark(1);
+        tm.mark(2);
+        if (zr.on) {
+            zr.fix(ctx, isz, M, N, K, dA.p, lda, dB.p, 1, dC.p, 1);
+            rc = cuda_rc(cudaGetLastError());
+            if (INA_FAILED(rc)) return rc;
+        }
+    } else if (!a->transposed && !b->transposed) {
         // both operands at once: one LZ4 launch over the streams of A and B
         DevBuf zf[2];
         int nz[2] = {0, 0};
@@ -1261,7 +1323,8 @@ static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_
         if (INA_FAILED(rc)) return rc;
         tm.mark(2);
     }
-    if (K == 0) {
+    if (fused) {
+    } else if (K == 0) {
         cudaMemsetAsync(dC.p, 0, (size_t)((vec ? M : M * ldc) * isz), ctx->stream);
     } else if (vec) {
         iab::gemv_native(dtype == IARRAY_DATA_TYPE_DOUBLE ? 0 : 1, M, K, dA.p, lda, dB.p, dC.p, ctx->stream);
@@ -1270,7 +1333,7 @@ static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_
         rc = dense_product(ctx, dtype, M, N, K, dA.p, lda, dB.p, ldb, dC.p, ldc, zr.on ? &zr.zs : nullptr);
     }
     if (INA_FAILED(rc)) return rc;
-    if (zr.on) {
+    if (zr.on && !fused) {
         zr.fix(ctx, isz, M, N, K, dA.p, lda, dB.p, vec ? 1 : ldb, dC.p, vec ? 1 : ldc);
         rc = cuda_rc(cudaGetLastError());
         if (INA_FAILED(rc)) return rc;

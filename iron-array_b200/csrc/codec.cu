@@ -183,6 +183,7 @@ constexpr int PATH = 1024;                 // >= 2 * the largest power of two be
 constexpr int HB = 4096;                   // output history kept in shared memory for match sources
 constexpr int LONGSEQ = 64;                // longer sequences are filled by the whole CTA
 constexpr int DCAP = 4096;                 // output bytes resolved in shared memory at once
+constexpr int WALK_MAX = 24;               // chains of at most this many sequences are walked
 constexpr uint16_t STOP = 0xFFFF, ENDS = 0xFFFE;
 constexpr uint32_t RES = 0x80000000u;      // resolved output byte (value in the low 8 bits)
 struct Smem {
@@ -201,7 +202,7 @@ struct Smem {
     int32_t longs[DCAP / (LONGSEQ + 1) + 1];  // sequences of a group longer than LONGSEQ bytes
     int32_t nlong;
     int32_t wsum[THREADS / 32];
-    int32_t scal[8];
+    int32_t scal[9];
 };
 }  // namespace dcta
 
@@ -259,6 +260,7 @@ __global__ void __launch_bounds__(dcta::THREADS, 6) k_lz4_decode_cta(const Lz4Jo
         int p = 0, op = 0;                 // window start in the input, output written so far
         int hist_from = 0;                 // S.hist holds output bytes [hist_from, written)
         bool bad = false, done = false;    // block-uniform
+        bool walk = true;                  // block-uniform: walk this window's chain (sparse windows)
         while (!done && !bad) {
             const int rem = isz - p, n = min(DW, rem);
             __syncthreads();
@@ -273,6 +275,28 @@ __global__ void __launch_bounds__(dcta::THREADS, 6) k_lz4_decode_cta(const Lz4Jo
                 for (int k = 0; k < DW / THREADS; k++) S.win[tid + k * THREADS] = v[k];
             }
             __syncthreads();
+            // Windows of few sequences (long literal runs, long matches): one thread walks the
+            // chain of token positions, at most WALK_MAX steps; when the chain does not leave the
+            // window by then, and for the windows that follow a dense one, the chain is built by
+            // doubling.  Both leave path[0 .. cnt) = token positions, path[cnt] >= n.
+            int cnt = -1;
+            if (walk) {
+                if (tid == 0) {
+                    int q = 0, k = 0, res = -1;
+                    S.path[0] = 0;
+                    for (;;) {
+                        const uint16_t v = dcta_next(S.win, q, n, rem);
+                        S.path[++k] = v;
+                        if (v >= n) { res = k; break; }
+                        if (k >= WALK_MAX) break;
+                        q = v;
+                    }
+                    S.scal[8] = res;
+                }
+                __syncthreads();
+                cnt = S.scal[8];
+            }
+            if (cnt < 0) {
 #pragma unroll
             for (int k = 0; k < DW / THREADS; k++) {      // eight independent table entries per thread
                 const int q = tid + k * THREADS;
@@ -281,7 +305,7 @@ __global__ void __launch_bounds__(dcta::THREADS, 6) k_lz4_decode_cta(const Lz4Jo
             if (tid == 0) { S.path[0] = 0; S.scal[1] = PATH; }
             __syncthreads();
             // chain of token positions by doubling: after level k, path[0 .. 2^(k+1)) known
-            int len = 1, cur = 0, cnt = 0;
+            int len = 1, cur = 0;
             for (;;) {
                 for (int j = tid; j < len; j += THREADS) {
                     const uint16_t pj = S.path[j];
@@ -312,6 +336,8 @@ __global__ void __launch_bounds__(dcta::THREADS, 6) k_lz4_decode_cta(const Lz4Jo
                 len *= 2;
                 __syncthreads();
             }
+            }
+            walk = cnt <= WALK_MAX;
             const uint16_t term = S.path[cnt];          // n, ENDS or STOP
             const int nseq = term == STOP ? cnt - 1 : cnt;
             if (nseq > 0) {
@@ -533,6 +559,15 @@ __device__ __forceinline__ uint64_t load_item(const uint8_t *o, int ts)
     }
 }
 
+// An item at any byte offset (a special-value chunk's value sits right after the chunk's
+// 32-byte header, and chunks lie back to back at arbitrary offsets).
+__device__ __forceinline__ uint64_t load_item_bytes(const uint8_t *o, int ts)
+{
+    uint64_t v = 0;
+    for (int j = 0; j < ts; j++) v |= (uint64_t)__ldg(o + j) << (8 * j);
+    return v;
+}
+
 // Map item i of block b of chunk c to its logical (row, col); false if it is padding.
 __device__ __forceinline__ bool item_pos(const Geom &g, int64_t c, int64_t b, int64_t i, int64_t &row, int64_t &col)
 {
@@ -555,6 +590,20 @@ __device__ __forceinline__ bool geom_fast(const Geom &g)
 
 // Block b of chunk c: its first logical row and column, and how many of its rows (nr) and
 // columns (nc) hold logical items (the rest is chunk or array padding; 0 when none do).
+// q = a / b, r = a - q b for a >= 0, b > 0: 32-bit division when both fit (the usual case),
+// 64-bit otherwise.
+__device__ __forceinline__ void divmod(int64_t a, int64_t b, int64_t &q, int64_t &r)
+{
+    if (((a | b) >> 31) == 0) {
+        const uint32_t q32 = (uint32_t)a / (uint32_t)b;
+        q = q32;
+        r = a - (int64_t)q32 * b;
+    } else {
+        q = a / b;
+        r = a - q * b;
+    }
+}
+
 struct BlockSpan {
     int64_t row0, col0;
     int nr, nc;
@@ -562,8 +611,9 @@ struct BlockSpan {
 __device__ __forceinline__ BlockSpan block_span(const Geom &g, int64_t c, int64_t b)
 {
     BlockSpan s;
-    const int64_t ci0 = c / g.cgrid[1], ci1 = c - ci0 * g.cgrid[1];
-    const int64_t bi0 = b / g.bgrid[1], bi1 = b - bi0 * g.bgrid[1];
+    int64_t ci0, ci1, bi0, bi1;
+    divmod(c, g.cgrid[1], ci0, ci1);
+    divmod(b, g.bgrid[1], bi0, bi1);
     s.row0 = ci0 * g.chunk[0] + bi0 * g.block[0];
     s.col0 = ci1 * g.chunk[1] + bi1 * g.block[1];
     s.nr = (int)max((int64_t)0, min(min(g.block[0], g.chunk[0] - bi0 * g.block[0]), g.shape[0] - s.row0));
@@ -620,7 +670,8 @@ __device__ __forceinline__ bool scatter_fast_unit(const Geom &g, const uint8_t *
 {
     const int tid = threadIdx.x;
     const int qpr = (int)(g.block[1] / 4);
-    const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
+    int64_t c, b;
+    divmod(t, g.nblocks, c, b);
     const BlockDesc d = bd[t];
     if (d.mode != BM_SHUFFLED || d.nstreams != TS || !geom_fast(g)) {
         if (tid == 0 && sl == 0) rest[atomicAdd(nrest, 1)] = rest_id;   // left to k_scatter
@@ -689,8 +740,13 @@ __device__ __forceinline__ bool scatter_fast_unit(const Geom &g, const uint8_t *
     }
     uint8_t *const obase = out + (sp.row0 * ld + sp.col0) * TS;
     const int nr = sp.nr, nc = sp.nc;
-    for (int qd = tid; qd < cnt / 4; qd += blockDim.x) {
-        const int it = i0s + qd * 4, r = it / (qpr * 4), cc = it - r * qpr * 4;
+    // (row, column) of each thread's quad, advanced by a fixed step per iteration (one
+    // division per slice instead of one per quad)
+    const int rowlen = qpr * 4, step = (int)blockDim.x * 4;
+    const int step_r = step / rowlen, step_c = step - step_r * rowlen;
+    int r = (i0s + tid * 4) / rowlen, cc = i0s + tid * 4 - r * rowlen;
+    for (int qd = tid; qd < cnt / 4; qd += blockDim.x, r += step_r, cc += step_c) {
+        if (cc >= rowlen) { cc -= rowlen; r++; }
         if (r >= nr || cc >= nc) continue;                                // padding items
         uint32_t w[TS];
 #pragma unroll
@@ -755,8 +811,9 @@ __global__ void __launch_bounds__(256, 6) k_scatter_fast(Geom g, const uint8_t *
     const int64_t nsl = (g.blockn + SC_ITEMS - 1) / SC_ITEMS;
     uint32_t parity = 0;
     for (int64_t u = blockIdx.x; u < nbl * nsl; u += gridDim.x) {
-        const int64_t t = u / nsl;
-        const int sl = (int)(u - t * nsl);
+        int64_t t, s64;
+        divmod(u, nsl, t, s64);
+        const int sl = (int)s64;
         if (!scatter_fast_unit<TS>(g, ch, ch_end, bd, sd, scratch, scratch_end, out, ld, rest, nrest, (int)t, err, t, sl,
                                    stage, &bar, parity, &abort_all))
             return;
@@ -820,7 +877,7 @@ __device__ __forceinline__ void scatter_tile(const Geom &g, const uint8_t *__res
         } else if (d.mode == BM_NAN) {
             v = ts == 8 ? 0x7FF8000000000000ull : 0x7FC00000ull;
         } else {
-            v = load_item(ch + d.value_src, ts);
+            v = load_item_bytes(ch + d.value_src, ts);
         }
         store_item(o, ts, v);
     }
@@ -851,11 +908,16 @@ __device__ __forceinline__ void gather_fast_block(const Geom &g, const uint8_t *
 {
     if (!geom_fast(g)) return;
     const int qpr = (int)(g.block[1] / 4), nq = (int)(g.blockn / 4);
-    const int64_t c = t / g.nblocks, b = t - c * g.nblocks;
+    int64_t c, b;
+    divmod(t, g.nblocks, c, b);
     const BlockSpan sp = block_span(g, c, b);
     uint8_t *blk = img + t * g.blocksize;
-    for (int qd = threadIdx.x; qd < nq; qd += blockDim.x) {
-        const int i0 = qd * 4, r = qd / qpr, cc = (qd - r * qpr) * 4;
+    // (row, quad column) of each thread's quad, advanced by a fixed step per iteration
+    const int step_r = (int)blockDim.x / qpr, step_q = (int)blockDim.x - step_r * qpr;
+    int r = (int)threadIdx.x / qpr, q = (int)threadIdx.x - r * qpr;
+    for (int qd = threadIdx.x; qd < nq; qd += blockDim.x, r += step_r, q += step_q) {
+        if (q >= qpr) { q -= qpr; r++; }
+        const int i0 = qd * 4, cc = q * 4;
         const uint8_t *src = in + ((sp.row0 + r) * ld + sp.col0 + cc) * TS;
         uint64_t x[4] = {0, 0, 0, 0};                 // padding items are zero, as in Caterva
         if (r < sp.nr && cc + 4 <= sp.nc) {
@@ -2337,6 +2399,292 @@ int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, in
     const int r = encode_launch(g, in, ld, shuffle, splitmode, d_out, &w, st);
     if (r) return r;
     return encode_finish(&w, h_off, h_len, st);
+}
+
+// ============================================================================ decode-fused GEMV
+// y = A x straight from A's chunks, after the parse and the LZ4 launch: the dense A is never
+// written.  A unit is one slice of whole rows of one block (SC_ITEMS / block[1] rows): its items
+// are rebuilt as the scatter rebuilds them (word-level from the staged byte planes for shuffled
+// split blocks, item by item from the stream descriptors otherwise), multiplied by x over the
+// block's columns, and each row's sum is stored in part[jb * M + row] (jb: the block's column in
+// the global block grid); k_gemv_rows then sums part over jb in order.  Every sum runs in a fixed
+// order, so the result does not vary from run to run.
+
+// Item i of a block from its stream descriptors (any block mode).
+__device__ __forceinline__ uint64_t item_bits(const Geom &g, const uint8_t *__restrict__ ch, const BlockDesc &d,
+                                              const StreamDesc *__restrict__ s, const uint8_t *__restrict__ blk_scratch,
+                                              int64_t i)
+{
+    const int ts = g.itemsize;
+    if (d.mode == BM_NAN) return ts == 8 ? 0x7FF8000000000000ull : 0x7FC00000ull;
+    if (d.mode == BM_VALUE) return load_item_bytes(ch + d.value_src, ts);
+    uint64_t v = 0;
+    for (int j = 0; j < ts; j++) {
+        const int64_t pos = d.mode == BM_SHUFFLED ? (int64_t)j * g.blockn + i : i * ts + j;
+        const int sidx = (int)(pos / d.neblock);
+        const int64_t so = pos - (int64_t)sidx * d.neblock;
+        const StreamDesc q = s[sidx];
+        uint8_t b;
+        if (q.kind == SK_RUN) b = (uint8_t)q.len;
+        else if (q.kind == SK_RAW) b = __ldg(ch + q.src + so);
+        else b = __ldcg(blk_scratch + (int64_t)sidx * d.neblock + so);
+        v |= (uint64_t)b << (8 * j);
+    }
+    return v;
+}
+
+template <typename T> __device__ __forceinline__ T bits_as(uint64_t v);
+template <> __device__ __forceinline__ float bits_as<float>(uint64_t v) { return __uint_as_float((uint32_t)v); }
+template <> __device__ __forceinline__ double bits_as<double>(uint64_t v) { return __longlong_as_double((long long)v); }
+
+// One unit of the fused GEMV: one slice of whole rows of one block (block-uniform values).
+struct GvUnit {
+    int64_t t, jb;
+    BlockSpan sp;
+    BlockDesc d;
+    int r0, nrow, i0s, cnt;
+    bool active, fast;         // active: the slice holds logical items; fast: word-level path
+};
+
+__device__ __forceinline__ GvUnit gv_unit(const Geom &g, const BlockDesc *__restrict__ bd, int64_t u, int64_t nsl,
+                                          int rps, int ts)
+{
+    GvUnit w;
+    int64_t s64, c, b, cq, cr, bq, br;
+    divmod(u, nsl, w.t, s64);
+    divmod(w.t, g.nblocks, c, b);
+    w.sp = block_span(g, c, b);
+    w.r0 = (int)s64 * rps;
+    w.active = w.sp.nc > 0 && w.r0 < w.sp.nr;
+    w.nrow = w.active ? min(rps, w.sp.nr - w.r0) : 0;
+    w.i0s = w.r0 * (int)g.block[1];
+    w.cnt = w.nrow * (int)g.block[1];
+    w.d = bd[w.t];
+    w.fast = w.d.mode == BM_SHUFFLED && w.d.nstreams == ts;
+    divmod(c, g.cgrid[1], cq, cr);
+    divmod(b, g.bgrid[1], bq, br);
+    w.jb = cr * g.bgrid[1] + br;
+    return w;
+}
+
+// Plane j of a fast unit: its slice starts at src (nullptr for a run), 16-byte word a16 =
+// src - shift; the bulk copy takes the whole words of [a16, a16 + want) before the buffer end
+// lim, threads copy the bytes that the buffer end cuts off (zeros past it).
+__device__ __forceinline__ StreamDesc gv_plane(const Geom &g, const uint8_t *ch, const uint8_t *ch_end,
+                                               const StreamDesc *__restrict__ sd, const uint8_t *scratch,
+                                               const uint8_t *scratch_end, const GvUnit &w, int j,
+                                               const uint8_t *&src, const uint8_t *&lim, int &want, int &bulk)
+{
+    const StreamDesc q = sd[w.t * 8 + j];
+    src = nullptr; lim = nullptr;
+    if (q.kind == SK_RAW) { src = ch + q.src + w.i0s; lim = ch_end; }
+    else if (q.kind == SK_LZ4) { src = scratch + w.t * g.blocksize + (int64_t)j * w.d.neblock + w.i0s; lim = scratch_end; }
+    want = bulk = 0;
+    if (src) {
+        const uint8_t *a16 = src - (reinterpret_cast<uintptr_t>(src) & 15);
+        want = ((int)(src - a16) + w.cnt + 15) & ~15;
+        bulk = (int)min((int64_t)want, (lim - a16) & ~int64_t(15));
+    }
+    return q;
+}
+
+template <int TS, typename T>
+__global__ void __launch_bounds__(256, 4) k_scatter_gemv(Geom g, const uint8_t *__restrict__ ch, const uint8_t *ch_end,
+                                                      const BlockDesc *__restrict__ bd,
+                                                      const StreamDesc *__restrict__ sd,
+                                                      const uint8_t *__restrict__ scratch, const uint8_t *scratch_end,
+                                                      const T *__restrict__ x, T *__restrict__ part, int64_t M,
+                                                      int *err)
+{
+    __shared__ __align__(128) uint8_t stage[TS][SC_PLANE];
+    __shared__ T qsum[SC_ITEMS / 4];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int abort_all;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        tc::mbar_init(&bar, 1);
+        tc::fence_barrier_init();
+        abort_all = 0;
+    }
+    __syncthreads();
+    const int qpr = (int)(g.block[1] / 4);
+    const int rps = (int)(SC_ITEMS / g.block[1]);            // whole rows per slice (>= 1: checked by the host)
+    const int64_t nsl = (g.block[0] + rps - 1) / rps;
+    const int64_t total = g.nchunks * g.nblocks * nsl;
+    uint32_t parity = 0;
+    for (int64_t u = blockIdx.x; u < total; u += gridDim.x) {          // block-uniform loop
+        const GvUnit w = gv_unit(g, bd, u, nsl, rps, TS);
+        if (!w.active) continue;                              // padding only
+        const T *__restrict__ xb = x + w.sp.col0;
+        if (w.fast) {
+            if (tid == 0) {
+                uint32_t tx = 0;
+#pragma unroll
+                for (int j = 0; j < TS; j++) {
+                    const uint8_t *src, *lim;
+                    int want, bulk;
+                    gv_plane(g, ch, ch_end, sd, scratch, scratch_end, w, j, src, lim, want, bulk);
+                    tx += (uint32_t)bulk;
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier reads of stage precede the copies
+                tc::mbar_arrive_expect_tx(&bar, tx);
+#pragma unroll
+                for (int j = 0; j < TS; j++) {
+                    const uint8_t *src, *lim;
+                    int want, bulk;
+                    gv_plane(g, ch, ch_end, sd, scratch, scratch_end, w, j, src, lim, want, bulk);
+                    if (bulk > 0) bulk_g2s(stage[j], src - (reinterpret_cast<uintptr_t>(src) & 15), (uint32_t)bulk, &bar);
+                }
+            }
+            int code[TS];
+#pragma unroll
+            for (int j = 0; j < TS; j++) {
+                const uint8_t *src, *lim;
+                int want, bulk;
+                const StreamDesc q = gv_plane(g, ch, ch_end, sd, scratch, scratch_end, w, j, src, lim, want, bulk);
+                code[j] = src ? (int)(reinterpret_cast<uintptr_t>(src) & 15) : 256 + (q.kind == SK_RUN ? (q.len & 255) : 0);
+                if (bulk < want) {
+                    const uint8_t *a16 = src - code[j];
+                    for (int xx = bulk + tid; xx < want; xx += blockDim.x)
+                        stage[j][xx] = a16 + xx < lim ? __ldg(a16 + xx) : (uint8_t)0;
+                }
+            }
+            const bool ok = sc_wait(&bar, parity);
+            parity ^= 1;
+            if (!ok) abort_all = 1;
+            __syncthreads();
+            if (abort_all) {                                  // the copies did not complete: report, wait once more, leave
+                if (tid == 0) {
+                    dev_fail(err, DE_WAIT);
+                    sc_wait(&bar, parity ^ 1);
+                }
+                return;
+            }
+            const int step_r = (int)blockDim.x / qpr, step_q = (int)blockDim.x - step_r * qpr;
+            int q = tid - (tid / qpr) * qpr;
+            for (int qd = tid; qd < w.cnt / 4; qd += blockDim.x, q += step_q) {
+                if (q >= qpr) q -= qpr;
+                const int cc = q * 4;
+                T sum = 0;
+                if (cc < w.sp.nc) {
+                    uint32_t wd[TS];
+#pragma unroll
+                    for (int j = 0; j < TS; j++) {
+                        if (code[j] >= 256) { wd[j] = (uint32_t)(code[j] - 256) * 0x01010101u; continue; }
+                        const uint32_t *pw = reinterpret_cast<const uint32_t *>(stage[j]);
+                        const int byte = code[j] + qd * 4, wi = byte >> 2, sh = (byte & 3) * 8;
+                        wd[j] = sh ? __funnelshift_r(pw[wi], pw[wi + 1], sh) : pw[wi];
+                    }
+                    uint32_t v[4];
+                    transpose4x4(wd[0], wd[1], wd[2], wd[3], v[0], v[1], v[2], v[3]);
+                    uint64_t item[4];
+                    if constexpr (TS == 8) {
+                        uint32_t h[4];
+                        transpose4x4(wd[4], wd[5], wd[6], wd[7], h[0], h[1], h[2], h[3]);
+#pragma unroll
+                        for (int k = 0; k < 4; k++) item[k] = ((uint64_t)h[k] << 32) | v[k];
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 4; k++) item[k] = v[k];
+                    }
+                    const T *xq = xb + cc;
+                    if (cc + 4 <= w.sp.nc && (reinterpret_cast<uintptr_t>(xq) & 15) == 0) {
+                        T xv[4];
+                        if constexpr (TS == 8) {
+                            const double2 x0 = __ldg(reinterpret_cast<const double2 *>(xq));
+                            const double2 x1 = __ldg(reinterpret_cast<const double2 *>(xq) + 1);
+                            xv[0] = x0.x; xv[1] = x0.y; xv[2] = x1.x; xv[3] = x1.y;
+                        } else {
+                            const float4 x0 = __ldg(reinterpret_cast<const float4 *>(xq));
+                            xv[0] = x0.x; xv[1] = x0.y; xv[2] = x0.z; xv[3] = x0.w;
+                        }
+#pragma unroll
+                        for (int k = 0; k < 4; k++) sum = fma(bits_as<T>(item[k]), xv[k], sum);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
+                            if (cc + k < w.sp.nc) sum = fma(bits_as<T>(item[k]), xq[k], sum);
+                    }
+                }
+                qsum[qd] = sum;
+            }
+        } else {
+            const StreamDesc *s = sd + w.t * 8;
+            const uint8_t *bs = scratch + w.t * g.blocksize;
+            for (int qd = tid; qd < w.cnt / 4; qd += blockDim.x) {
+                const int cc = (qd % qpr) * 4;
+                T sum = 0;
+                for (int k = 0; k < 4; k++)
+                    if (cc + k < w.sp.nc)
+                        sum = fma(bits_as<T>(item_bits(g, ch, w.d, s, bs, w.i0s + qd * 4 + k)), xb[cc + k], sum);
+                qsum[qd] = sum;
+            }
+        }
+        __syncthreads();
+        // row sums: warp w takes rows w, w + 8, ...; lanes stride the row's quads, then a shuffle tree
+        for (int rr = warp; rr < w.nrow; rr += blockDim.x / 32) {
+            T acc = 0;
+            for (int q = lane; q < qpr; q += 32) acc += qsum[rr * qpr + q];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULLMASK, acc, o);
+            if (lane == 0) part[w.jb * M + w.sp.row0 + w.r0 + rr] = acc;
+        }
+        __syncthreads();                                  // stage and qsum are read before the next slice
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_gemv_rows(const T *__restrict__ part, int64_t JB, int64_t M, T *__restrict__ y)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M; i += (int64_t)gridDim.x * blockDim.x) {
+        T acc = 0;
+        for (int64_t jb = 0; jb < JB; jb++) acc += part[jb * M + i];
+        y[i] = acc;
+    }
+}
+
+bool decode_gemv_fits(const Geom &g)
+{
+    return g.ndim == 2 && (g.itemsize == 4 || g.itemsize == 8) && !(g.block[1] & 3) && g.block[1] <= SC_ITEMS &&
+           g.block[1] > 0;
+}
+
+int64_t decode_gemv_part_items(const Geom &g) { return g.cgrid[1] * g.bgrid[1] * g.shape[0]; }
+
+int decode_gemv(const DecodeArgs &a, DecodeWork *w, const void *x, void *part, void *y, cudaStream_t st)
+{
+    const Geom &g = a.g;
+    if (!decode_gemv_fits(g)) return -102;
+    const int64_t M = g.shape[0], JB = g.cgrid[1] * g.bgrid[1], nbl = g.nchunks * g.nblocks;
+    cudaMemsetAsync(part, 0, (size_t)(JB * M * g.itemsize), st);
+    int *cnt = w->ext_counters ? w->ext_counters : w->counters.as<int>();
+    const uint8_t *scratch = w->scratch.as<uint8_t>();
+    const uint8_t *cend = a.chunks + a.chunks_bytes, *send = scratch + nbl * g.blocksize;
+    const int rps = (int)(SC_ITEMS / g.block[1]);
+    const int64_t units = nbl * ((g.block[0] + rps - 1) / rps);
+    static int per_sm[2] = {0, 0};
+    const int slot = g.itemsize == 8;
+    if (!per_sm[slot]) {
+        int m = 0;
+        const cudaError_t e = slot ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_scatter_gemv<8, double>, 256, 0)
+                                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_scatter_gemv<4, float>, 256, 0);
+        if (e != cudaSuccess || m < 1) { cudaGetLastError(); m = 4; }
+        per_sm[slot] = m;
+    }
+    const int64_t grid = std::max<int64_t>(std::min<int64_t>(units, (int64_t)sm_count() * per_sm[slot]), 1);
+    const unsigned rb = (unsigned)std::max<int64_t>(std::min<int64_t>((M + 255) / 256, (int64_t)sm_count() * 8), 1);
+    if (slot) {
+        IAB_TIMED("k_scatter_gemv", st, k_scatter_gemv<8, double><<<(unsigned)grid, 256, 0, st>>>(
+            g, a.chunks, cend, w->bd.as<BlockDesc>(), w->sd.as<StreamDesc>(), scratch, send, (const double *)x,
+            (double *)part, M, cnt + 1));
+        IAB_TIMED("k_gemv_rows", st, k_gemv_rows<double><<<rb, 256, 0, st>>>((const double *)part, JB, M, (double *)y));
+    } else {
+        IAB_TIMED("k_scatter_gemv", st, k_scatter_gemv<4, float><<<(unsigned)grid, 256, 0, st>>>(
+            g, a.chunks, cend, w->bd.as<BlockDesc>(), w->sd.as<StreamDesc>(), scratch, send, (const float *)x,
+            (float *)part, M, cnt + 1));
+        IAB_TIMED("k_gemv_rows", st, k_gemv_rows<float><<<rb, 256, 0, st>>>((const float *)part, JB, M, (float *)y));
+    }
+    return 0;
 }
 
 // ============================================================================ grouped codec

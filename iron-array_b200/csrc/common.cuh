@@ -190,6 +190,14 @@ int64_t decode_max_jobs(const Geom &g);
 int decode_parse(const DecodeArgs &a, DecodeQueue *q, DecodeWork *w, cudaStream_t st);
 int decode_lz4(DecodeQueue *q, cudaStream_t st);
 int decode_scatter(const DecodeArgs &a, DecodeWork *w, cudaStream_t st);
+// Decode-fused GEMV y = A x in place of decode_scatter(A) (after decode_parse and decode_lz4
+// of A; x dense on the device): part holds decode_gemv_part_items(g) items of A's type (row
+// sums per block column), y gets the M sums.  The dense A is never written.  Partitions of
+// 2-D float32 / float64 containers whose block rows hold whole groups of 4 items and at most
+// 4096 items (decode_gemv_fits).
+bool decode_gemv_fits(const Geom &g);
+int64_t decode_gemv_part_items(const Geom &g);
+int decode_gemv(const DecodeArgs &a, DecodeWork *w, const void *x, void *part, void *y, cudaStream_t st);
 
 // Decode without allocating: the work buffers live in a fixed device array of the library
 // (at most NOALLOC_MAX_BYTES decoded bytes and NOALLOC_MAX_BLOCKS blocks per call; larger

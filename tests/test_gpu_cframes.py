@@ -26,6 +26,7 @@ def _sequential(ia, ctx, fa, fb, cc, bc):
     (300, 257, 200, 64, 128, 96, 32),      # ragged last band, ragged chunks in every dimension
     (512, 512, 512, 128, 128, 128, 64),    # four full bands
     (70, 33, 50, 70, 33, 50, 11),          # one band
+    (200, 100, 150, 50, 100, 75, 25),      # column chunks off 16-byte boundaries
 ])
 def test_cframes_matches_sequential_calls(ia, form, dtype, M, K, N, c0, c1, c2, b):
     ctx = ia.Context(form=ia.FORM_SPLIT if form == "split" else ia.FORM_NATIVE, encoder=ia.ENCODER_PARALLEL)
