@@ -404,6 +404,11 @@ namespace oz {
 constexpr int BM = 128, BN = 256, BK = 128, STAGES = 4;
 constexpr int A_BYTES = BM * BK, B_BYTES = BN * BK, STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int THREADS = 192;
+// The grouped form's many small-K tiles leave the epilogue little MMA time to hide behind:
+// it drains each accumulator with eight warps (two per TMEM lane quarter, one column half
+// each) instead of four.
+template <bool GROUPED> constexpr int threads_of() { return GROUPED ? 320 : THREADS; }
+template <bool GROUPED> constexpr int epi_warps() { return GROUPED ? 8 : 4; }
 constexpr int SMEM = 1024 + STAGES * STAGE_BYTES + 256;
 constexpr uint32_t IDESC = tc::make_idesc(2 /*S32*/, 1 /*s8*/, 1 /*s8*/, BM, BN);
 }
@@ -451,6 +456,19 @@ __device__ __forceinline__ int oz_find(const OzGProb *__restrict__ pr, int np, i
     return lo;
 }
 
+// oz_find for a loop whose values only increase: from the previous product qh (-1: none yet)
+// a few steps forward, a binary search when the value has moved further.
+template <typename F>
+__device__ __forceinline__ int oz_walk(const OzGProb *__restrict__ pr, int np, int64_t v, F key, int &qh)
+{
+    int q = qh;
+    if (q >= 0)
+        for (int k = 0; k < 8 && q + 1 < np && key(pr[q + 1]) <= v; k++) q++;
+    if (q < 0 || (q + 1 < np && key(pr[q + 1]) <= v)) q = oz_find(pr, np, v, key);
+    qh = q;
+    return q;
+}
+
 struct I8Params {
     int M, N, K, Kp, L, tiles_m, tiles_n;
     uint8_t *R;        // [L][M][ldr] residues of the products
@@ -473,8 +491,20 @@ struct I8Tile {
     int64_t ldr;
 };
 
+// The product of grouped item t, walking forward from the product *qh of the caller's previous
+// item (a CTA's items only increase, by the grid size, so the walk is usually one compare).
+__device__ __forceinline__ int oz_item_prob(const I8Params &p, int64_t t, int &qh)
+{
+    int q = qh;
+    if (q < 0) q = oz_find(p.probs, p.nprob, t, [](const OzGProb &x) { return x.item0; });
+    while (q + 1 < p.nprob && p.probs[q + 1].item0 <= t) q++;
+    qh = q;
+    return q;
+}
+
 template <bool GROUPED>
-__device__ __forceinline__ I8Tile i8_tile(const I8Params &p, const CUtensorMap *tmA, const CUtensorMap *tmB, int64_t t)
+__device__ __forceinline__ I8Tile i8_tile(const I8Params &p, const CUtensorMap *tmA, const CUtensorMap *tmB, int64_t t,
+                                          int &qh)
 {
     I8Tile r;
     if constexpr (!GROUPED) {
@@ -485,7 +515,7 @@ __device__ __forceinline__ I8Tile i8_tile(const I8Params &p, const CUtensorMap *
         r.M = p.M; r.N = p.N; r.ktiles = p.Kp / oz::BK;
         r.R = p.R; r.ldr = p.ldr;
     } else {
-        const int q = oz_find(p.probs, p.nprob, t, [](const OzGProb &x) { return x.item0; });
+        const int q = oz_item_prob(p, t, qh);
         const OzGProb &pr = p.probs[q];
         const int per = pr.tiles_m * pr.tiles_n;
         const int64_t local = t - pr.item0;
@@ -537,7 +567,7 @@ __device__ __forceinline__ bool i8_tile_any(const I8Params &p, int tm, int tn, i
 // the k-tiles of zero-block pairs are neither loaded nor multiplied (every role derives the
 // same mask); a tile that needs none is written as zero residues.
 template <bool SKIP, bool GROUPED>
-__global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_constant__ CUtensorMap tmA,
+__global__ void __launch_bounds__(oz::threads_of<GROUPED>(), 1) k_i8gemm_mod(const __grid_constant__ CUtensorMap tmA,
                                                                 const __grid_constant__ CUtensorMap tmB, I8Params p)
 {
     static_assert(!(SKIP && GROUPED), "the grouped form does not skip zero blocks");
@@ -557,7 +587,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) { tc::mbar_init(&full[s], 1); tc::mbar_init(&empty[s], 1); }
-        for (int b = 0; b < 2; b++) { tc::mbar_init(&tfull[b], 1); tc::mbar_init(&tempty[b], 4); }
+        for (int b = 0; b < 2; b++) { tc::mbar_init(&tfull[b], 1); tc::mbar_init(&tempty[b], epi_warps<GROUPED>()); }
         tc::mbar_init(drain, 1);
         tc::fence_barrier_init();
         if constexpr (!GROUPED) {
@@ -580,14 +610,26 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
         else return true;
     };
 
+    int qh = -1;                             // grouped form: product of this warp's previous item
     if (warp == 0) {
         int stage = 0;
         uint32_t phase = 0;
         int64_t issued = 0;
         bool ok = true;
         for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {  // the whole warp walks the tiles
-            const I8Tile tl = i8_tile<GROUPED>(p, &tmA, &tmB, t);
+            const I8Tile tl = i8_tile<GROUPED>(p, &tmA, &tmB, t, qh);
             const int l = tl.l, tm = tl.tm, tn = tl.tn;
+            if constexpr (GROUPED) {
+                // the tensor maps of this CTA's next item (often another product's) are fetched
+                // while this item's loads run
+                const int64_t tn2 = t + gridDim.x;
+                if (lane == 0 && tn2 < total) {
+                    int q2 = qh;
+                    while (q2 + 1 < p.nprob && p.probs[q2 + 1].item0 <= tn2) q2++;
+                    tc::tma_prefetch_desc(p.maps + 2 * q2);
+                    tc::tma_prefetch_desc(p.maps + 2 * q2 + 1);
+                }
+            }
             if constexpr (SKIP) i8_kmask(p, tm, tn, ktiles, pmask);
             if (lane == 0) {
                 for (int kt = 0; kt < tl.ktiles; kt++) {
@@ -612,7 +654,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
         uint32_t phase = 0, acc_phase = 0;
         bool ok = true;
         for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
-            const I8Tile tl = i8_tile<GROUPED>(p, &tmA, &tmB, t);
+            const I8Tile tl = i8_tile<GROUPED>(p, &tmA, &tmB, t, qh);
             if constexpr (SKIP) i8_kmask(p, tl.tm, tl.tn, ktiles, mmask);
             if (lane == 0) {
                 if (!tc::mbar_wait(&tempty[acc], acc_phase ^ 1, p.err)) {
@@ -652,10 +694,12 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
         }
     } else {
         const int q = warp & 3;   // TMEM lane quarter this warp may access
+        constexpr int HALVES = epi_warps<GROUPED>() / 4;
+        const int c_lo = ((warp - 2) / 4) * (BN / HALVES), c_hi = c_lo + BN / HALVES;   // this warp's columns
         int acc = 0;
         uint32_t acc_phase = 0;
         for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
-            const I8Tile tl = i8_tile<GROUPED>(p, &tmA, &tmB, t);
+            const I8Tile tl = i8_tile<GROUPED>(p, &tmA, &tmB, t, qh);
             const int l = tl.l, tm = tl.tm, tn = tl.tn;
             bool active = true;
             if constexpr (SKIP) active = i8_tile_any(p, tm, tn, ktiles);
@@ -665,7 +709,7 @@ __global__ void __launch_bounds__(oz::THREADS, 1) k_i8gemm_mod(const __grid_cons
             const float invm = c_crt.inv_modf[l];
             const int row = tm * BM + q * 32 + lane;
             uint8_t *out = tl.R + ((int64_t)l * tl.M + row) * tl.ldr + (int64_t)tn * BN;
-            for (int c = 0; c < BN; c += 32) {
+            for (int c = c_lo; c < c_hi; c += 32) {
                 uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                 if (active) {
                     uint32_t v[32];
@@ -1072,8 +1116,9 @@ __global__ void __launch_bounds__(256) k_residues_rows_g(const OzGProb *__restri
                                                          const int *__restrict__ shift)
 {
     const int L = c_crt.L;
+    int qh = -1;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tasks; t += (int64_t)gridDim.x * blockDim.x) {
-        const OzGProb &q = pr[oz_find(pr, np, t, [](const OzGProb &x) { return x.task_r0; })];
+        const OzGProb &q = pr[oz_walk(pr, np, t, [](const OzGProb &x) { return x.task_r0; }, qh)];
         const int groups = q.Kp / 8;
         const int64_t lt = t - q.task_r0;
         const int i = (int)(lt / groups), k0 = (int)(lt - (int64_t)i * groups) * 8;
@@ -1157,8 +1202,9 @@ __global__ void __launch_bounds__(256) k_residues_cols_g(const OzGProb *__restri
 {
     __shared__ double tile[64][65];
     const int L = c_crt.L;
+    int qh = -1;
     for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {                 // block-uniform loop
-        const OzGProb &q = pr[oz_find(pr, np, t, [](const OzGProb &x) { return x.tile_c0; })];
+        const OzGProb &q = pr[oz_walk(pr, np, t, [](const OzGProb &x) { return x.tile_c0; }, qh)];
         const int tx_n = (q.N + 63) / 64;
         const int64_t lt = t - q.tile_c0;
         const int ty = (int)(lt / tx_n), tx = (int)(lt - (int64_t)ty * tx_n);
@@ -1203,8 +1249,9 @@ template <int NC>
 __global__ void __launch_bounds__(256) k_crt_g(const OzGProb *__restrict__ pr, int np, int64_t tasks,
                                                const int *__restrict__ sA, const int *__restrict__ sB)
 {
+    int qh = -1;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tasks; e += (int64_t)gridDim.x * blockDim.x) {
-        const OzGProb &q = pr[oz_find(pr, np, e, [](const OzGProb &x) { return x.crt0; })];
+        const OzGProb &q = pr[oz_walk(pr, np, e, [](const OzGProb &x) { return x.crt0; }, qh)];
         const int nq = (q.N + 3) / 4;
         const int64_t lt = e - q.crt0;
         const int i = (int)(lt / nq), j0 = (int)(lt - (int64_t)i * nq) * 4;
@@ -1340,7 +1387,7 @@ int gemm_f64_ozaki_grouped_launch(OzGroupWork *w, cudaStream_t st)
     // the tensor maps of the kernel parameters are unused in the grouped form
     CUtensorMap unused;
     memset(&unused, 0, sizeof(unused));
-    IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<false, true><<<(unsigned)std::min<int64_t>(w->items, nsm), oz::THREADS,
+    IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<false, true><<<(unsigned)std::min<int64_t>(w->items, nsm), oz::threads_of<true>(),
                                                                oz::SMEM, st>>>(unused, unused, prm));
     const unsigned cg = (unsigned)std::min<int64_t>((w->crt + 255) / 256, (int64_t)nsm * 8);
     switch (w->nc) {
