@@ -736,7 +736,8 @@ def run_kernel_case(args):
     f32split: the float32 split form (six BF16 products) n x n x n, two rounds.  gemv: the
     plain GEMV workload's smooth float32 matrix at n x n (chunk 4000^2, block 500^2) decoded three
     times, then one iarray_opt_gemv.  f64native: the native FP64 product n x n x n on device
-    operands, two rounds.
+    operands, two rounds.  batch: the first n / 64 problems of the batching workload in the
+    split form (creation and two graph replays).
     Inputs are larger than L2 and a few GB at most are held on the device."""
     import ctypes
     import torch
@@ -770,6 +771,21 @@ def run_kernel_case(args):
         y = ia.opt_gemv(ctx, a, xc, (4000,), (500,)).to_numpy().astype(np.float64)
         ref = A.astype(np.float64) @ x.astype(np.float64)
         assert np.linalg.norm(y - ref) / np.linalg.norm(ref) < 1e-5
+    elif args.kernel_case == "batch":
+        # the first n // 64 problems of the batching workload (n = --case-n, default 4096: 64
+        # problems), split form at 14 moduli: creation (one eager pass) and two graph replays
+        ctx = ia.Context(form=ia.FORM_SPLIT, split_terms=14, encoder=ia.ENCODER_PARALLEL)
+        count = max(1, min(512, n // 64))
+        dims = rng.integers(64, 2049, (512, 3))[:count]
+        As = [ia.Container.from_numpy(ctx, rng.uniform(-1, 1, (int(m), int(k))), (512, 512), (128, 128))
+              for m, _, k in dims]
+        Bs = [ia.Container.from_numpy(ctx, rng.uniform(-1, 1, (int(k), int(nn))), (512, 512), (128, 128))
+              for _, nn, k in dims]
+        batch = ia.Batch(ctx, As, Bs, [(512, 512)] * count, [(128, 128)] * count)
+        for _ in range(2):
+            for c in batch.run():
+                c.free()
+        batch.free()
     elif args.kernel_case == "f64native":
         ctx = ia.Context(form=ia.FORM_NATIVE)
         A = torch.from_numpy(rng.uniform(-1, 1, (n, n))).cuda()
@@ -825,7 +841,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-samples", type=int, default=3, help="whole-product samples of the CPU baseline")
     ap.add_argument("--no-secondary", action="store_true", help="skip the GEMV, float32 and batching workloads")
-    ap.add_argument("--kernel-case", choices=["codec", "split", "f32split", "gemv", "f64native"], default=None,
+    ap.add_argument("--kernel-case", choices=["codec", "split", "f32split", "gemv", "f64native", "batch"], default=None,
                     help="run one small case of one kernel family instead of the benchmark")
     ap.add_argument("--case-n", type=int, default=4096, help="matrix size of --kernel-case")
     args = ap.parse_args()
