@@ -694,8 +694,11 @@ __global__ void __launch_bounds__(oz::threads_of<GROUPED>(), 1) k_i8gemm_mod(con
         }
     } else {
         const int q = warp & 3;   // TMEM lane quarter this warp may access
-        constexpr int HALVES = epi_warps<GROUPED>() / 4;
-        const int c_lo = ((warp - 2) / 4) * (BN / HALVES), c_hi = c_lo + BN / HALVES;   // this warp's columns
+        int c_lo = 0, c_hi = BN;                                  // this warp's columns
+        if constexpr (GROUPED) {
+            c_lo = ((warp - 2) / 4) * (BN / 2);
+            c_hi = c_lo + BN / 2;
+        }
         int acc = 0;
         uint32_t acc_phase = 0;
         for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
