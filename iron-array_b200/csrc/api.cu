@@ -1822,12 +1822,14 @@ INA_API(ina_rc_t) iarray_b200_opt_gemm_cframes(iarray_context_t *ctx, const uint
 // ============================================================================ batched products
 // A batch of independent float64 products C_i = A_i * B_i with their own shapes and
 // partitions.  iarray_b200_batch_new allocates every buffer the batch needs, decodes the
-// operands once, runs the autotuner over the grouped product's tile configurations,
-// runs the whole batch once eagerly, and captures decode -> product -> encode of all
-// problems in one CUDA graph.  iarray_b200_batch_run replays the graph and turns the
-// encoded outputs into containers.  Native form: one persistent grouped DMMA launch over
-// the tiles of all problems (tiles ordered by descending K); split form: the Ozaki
-// pipeline of each problem, all inside the same graph.
+// operands once, runs the autotuner (native form: the grouped product's tile and stage
+// configurations; split form: the moduli count), runs the whole batch once eagerly, and
+// captures decode -> product -> encode of all problems in one CUDA graph.
+// iarray_b200_batch_run replays the graph and turns the encoded outputs into containers.
+// Every stage is one launch over all problems: the grouped codec (decode of every operand,
+// encode of every output when they share a stream shape), and the product: native form, one
+// persistent grouped DMMA launch over the tiles of all problems (tiles ordered by descending
+// K); split form, one grouped Ozaki pipeline over all problems.
 struct iarray_b200_batch_s {
     iarray_context_t *ctx = nullptr;
     int form = IARRAY_B200_FORM_NATIVE;
