@@ -42,6 +42,15 @@ def test_only_declared_symbols_are_exported():
     assert ours == set(declared_functions())
 
 
+def test_header_constants_match_the_binding():
+    """The binding's fixed-size buffers follow the header's constants."""
+    text = open(HEADER).read()
+    configs = int(re.search(r"#define IARRAY_B200_BATCH_TILE_CONFIGS (\d+)", text).group(1))
+    src = open(os.path.join(ROOT, "iron-array_b200", "iarray_b200.py")).read()
+    assert f"ms = (ctypes.c_double * {configs})()" in src
+    assert configs == 8
+
+
 def test_error_strings(ia=None):
     import iarray_b200 as m
     lib = m.lib()
