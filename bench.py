@@ -178,41 +178,45 @@ def run_reference(args):
 L_MODULI = 14          # moduli of the split-precision product (library default)
 
 
-def roofline(kprof, pk, dgemm_tflops, c_cbytes, a_cb, b_cb):
+def roofline(kprof, steps, pk, dgemm_tflops, c_cbytes, a_cb, b_cb):
     """Roofline of the kernel with the largest device time in the timed steps.
-    achieved = algorithmic work of one launch / its mean CUDA-event duration."""
+    achieved = algorithmic work of one launch / its mean CUDA-event duration, where the work of
+    one launch is the kernel's algorithmic work per step x steps / its launches (a kernel that
+    runs once per row band of the product launches several times a step)."""
     name, (cnt, tot) = max(kprof.items(), key=lambda kv: kv[1][1])
     avg_s = tot / cnt * 1e-3
+    share = steps / cnt                          # steps per launch
     img = M * N * 8                              # bytes of one dense 8192^2 float64 matrix
     if name == "k_i8gemm_mod":
-        work, unit, bound = 2.0 * M * N * K * L_MODULI / 1e12, "TOP/s", "tensor"
+        work, unit, bound = 2.0 * M * N * K * L_MODULI * share / 1e12, "TOP/s", "tensor"
         peak, src = 2 * pk["bf16_tflops"], "2 x measured dense BF16 (sm_100 dense INT8 rate is twice BF16)"
     elif name == "k_gemm_f64":
-        work, unit, bound = FLOP / 1e12, "TFLOP/s", "tensor"
+        work, unit, bound = FLOP * share / 1e12, "TFLOP/s", "tensor"
         peak, src = dgemm_tflops, "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor roof)"
     else:
-        bytes_per_launch = {
+        bytes_per_step = {
             "k_lz4_encode": img + (c_cbytes or img),            # read the byte-plane image, write LZ4 streams
             "k_lz4_encode_par": img + (c_cbytes or img),
-            "k_lz4_decode_cta": (a_cb + b_cb) / 2 + img,        # upper bound: all streams LZ4
+            "k_lz4_decode_cta": a_cb + b_cb + 2 * img,          # upper bound: all streams LZ4
             "k_crt": L_MODULI * M * N + img,                    # residue planes in, float64 out
             "k_residues_rows": img + L_MODULI * M * K,
             "k_residues_cols": img + L_MODULI * K * N,
-            "k_scatter_fast": 2 * img, "k_scatter": 2 * img,
+            "k_scatter_fast": 4 * img, "k_scatter": 4 * img,   # both operands, read + write
             "k_gather_fast": 2 * img, "k_gather": 2 * img,
             "k_emit": 2 * (c_cbytes or img),
         }.get(name)
-        if bytes_per_launch is None:
+        if bytes_per_step is None:
             return {"bound": None, "kernel": name, "achieved": None, "peak": None, "unit": None, "frac": None,
                     "traffic": None}
-        work, unit, bound = bytes_per_launch / 1e9, "GB/s", "hbm"
+        work, unit, bound = bytes_per_step * share / 1e9, "GB/s", "hbm"
         peak, src = pk["hbm_gbs"], "measured HBM copy bandwidth"
     achieved = work / avg_s
     traffic = None
     tf = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tf):
         traffic = json.load(open(tf)).get(name)
-    return {"bound": bound, "kernel": name, "launches": cnt, "avg_ms": tot / cnt, "achieved": achieved,
+    return {"bound": bound, "kernel": name, "launches": cnt, "launches_per_step": cnt / steps, "avg_ms": tot / cnt,
+            "achieved": achieved,
             "peak": peak, "peak_source": src, "unit": unit, "frac": achieved / peak if peak else None,
             "traffic": traffic,
             "traffic_source": "profiles/ncu_traffic.json: dram bytes read + written of one launch of this "
@@ -683,7 +687,7 @@ def run_ours(args):
     barrier(pg)
     hr = results[head]
     value = world * FLOP / (hr["ms"] * 1e-3) / 1e12
-    roof = roofline(hr["kprof"], pk, dgemm_tflops, c_cbytes=hr.get("c_cbytes"), a_cb=a_cb, b_cb=b_cb)
+    roof = roofline(hr["kprof"], args.steps, pk, dgemm_tflops, c_cbytes=hr.get("c_cbytes"), a_cb=a_cb, b_cb=b_cb)
     line = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": hr["ms"], "higher_is_better": True, "scaling": "weak",

@@ -214,3 +214,40 @@ def test_split_f64_fewer_moduli(ia):
     Z = ia.matmul(ctx, ia.Container.from_numpy(ctx, X, (32, 32), (16, 16)),
                   ia.Container.from_numpy(ctx, Y, (32, 32), (16, 16)), (32, 32), (16, 16)).to_numpy()
     assert np.array_equal(Z, X @ Y)
+
+
+@pytest.mark.parametrize("M,K,N", [(3000, 900, 700), (5000, 520, 1100), (8192, 256, 384)])
+def test_split_f64_row_slices_equal_whole(ia, M, K, N):
+    """Each row of C depends only on its row of A and on B: the row scaling, the residues, the
+    INT8 sums and the reconstruction do not see the other rows.  So the product computed in
+    slices of at most 1000 rows (as the pipelined call computes its bands of C) is bitwise the
+    whole product, NaN and infinity rows included."""
+    import ctypes
+    import torch
+    rng = np.random.default_rng(M + K)
+    a, b = _scaled(rng, (M, K)), _scaled(rng, (K, N))
+    a[M // 3, 5] = np.nan
+    a[M - 1, K - 1] = np.inf
+    A = torch.from_numpy(a).cuda()
+    B = torch.from_numpy(b).cuda()
+    C1 = torch.empty((M, N), dtype=torch.float64, device="cuda")
+    C2 = torch.empty((M, N), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    ctx = _split_ctx(ia)
+
+    def gemm(m, r0, C):
+        ia.check(ia.lib().iarray_b200_dense_gemm(
+            ctx.ptr, ia.DTYPE_DOUBLE, m, N, K, ctypes.c_void_p(A.data_ptr() + r0 * K * 8), K,
+            ctypes.c_void_p(B.data_ptr()), N, ctypes.c_void_p(C.data_ptr() + r0 * N * 8), N), "dense_gemm")
+
+    gemm(M, 0, C1)
+    for r0 in range(0, M, 1000):
+        gemm(min(1000, M - r0), r0, C2)
+    ctx.synchronize()
+    c1, c2 = C1.cpu().numpy(), C2.cpu().numpy()
+    assert c1.tobytes() == c2.tobytes()
+    assert np.isnan(c1[M // 3]).all() and not np.isfinite(c1[M - 1]).any()
+    rows = np.array([0, 1, M // 2, M - 2])
+    hi, lo = O.dd_rows(a, b, rows)
+    d = (c1[rows] - hi) - lo
+    assert np.linalg.norm(d) <= 1e-14 * np.linalg.norm(hi)
