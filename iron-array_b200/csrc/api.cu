@@ -474,6 +474,24 @@ static ina_rc_t encode_into(iarray_context_t *ctx, iarray_container_t *c, const 
     return INA_SUCCESS;
 }
 
+// encode_into for an image the product wrote (iab::encode_image_prepare).
+static ina_rc_t encode_into_image(iarray_context_t *ctx, iarray_container_t *c, iab::EncodeWork *w)
+{
+    ChunkStore &s = *c->store;
+    DevBuf out;
+    std::vector<int64_t> off;
+    std::vector<int32_t> len;
+    int r = iab::encode_image_finish(c->geom, c->shuffle, c->splitmode, &out, &off, &len, ctx->stream,
+                                     ctx->encoder == IARRAY_B200_ENCODER_LIBLZ4, w);
+    if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    if (r != 0) return rc_err(IARRAY_ERR_GPU_FAILED);
+    s.buf = std::move(out);
+    s.off = std::move(off);
+    s.len = std::move(len);
+    if (!s.upload_index()) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+    return INA_SUCCESS;
+}
+
 // A decoder's status word: malformed chunk data is a codec failure; a bounded wait on an
 // asynchronous copy that gave up (DE_WAIT) is a GPU failure, not bad data.
 static ina_rc_t status_rc(int status)
@@ -1142,15 +1160,17 @@ struct Timer {
 
 // Run the product on dense device operands with the context's form.
 // zs (optional): leave out the K ranges of zero-block pairs in the float64 products.
+// cimg (optional, split form, float64): the product goes into the output container's encoder
+// image instead of C.
 static ina_rc_t dense_product(iarray_context_t *ctx, int dtype, int64_t M, int64_t N, int64_t K, const void *A,
                               int64_t lda, const void *B, int64_t ldb, void *C, int64_t ldc,
-                              const iab::ZeroSkip *zs = nullptr)
+                              const iab::ZeroSkip *zs = nullptr, const iab::CImage *cimg = nullptr)
 {
     if (ctx->form == IARRAY_B200_FORM_SPLIT) {
         int r;
         if (dtype == IARRAY_DATA_TYPE_DOUBLE)
             r = iab::gemm_f64_ozaki(M, N, K, (const double *)A, lda, (const double *)B, ldb, (double *)C, ldc,
-                                    ctx->split_terms, ctx->stream, zs);
+                                    ctx->split_terms, ctx->stream, zs, cimg);
         else
             r = iab::gemm_f32_bf16_split(M, N, K, (const float *)A, lda, (const float *)B, ldb, (float *)C, ldc,
                                          ctx->split_products_f32, ctx->stream);
@@ -1287,9 +1307,12 @@ static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_
     // decode-fused GEMV: A's items go from its chunks straight into the row sums
     const bool fused = vec && !a->transposed && !b->transposed && K > 0 && M > 0 && a->geom.nchunks &&
                        b->geom.nchunks && iab::decode_gemv_fits(a->geom);
+    // split float64 product straight into C's encoder image (no dense C, no gather)
+    bool direct = !vec && K > 0 && ctx->form == IARRAY_B200_FORM_SPLIT && dtype == IARRAY_DATA_TYPE_DOUBLE &&
+                  iab::encode_image_ok(c->geom, c->shuffle, c->clevel == 0);
     if ((!fused && !dA.allocate((size_t)std::max<int64_t>(M * lda * isz, 16), ctx->device)) ||
         !dB.allocate((size_t)std::max<int64_t>((vec ? pad_ld(K) : K * ldb) * isz, 16), ctx->device) ||
-        !dC.allocate((size_t)std::max<int64_t>((vec ? pad_ld(M) : M * ldc) * isz, 16), ctx->device))
+        (!direct && !dC.allocate((size_t)std::max<int64_t>((vec ? pad_ld(M) : M * ldc) * isz, 16), ctx->device)))
         return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
     if (vec) cudaMemsetAsync(dB.p, 0, (size_t)(pad_ld(K) * isz), ctx->stream);
     ina_rc_t rc;
@@ -1323,6 +1346,24 @@ static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_
         if (INA_FAILED(rc)) return rc;
         tm.mark(2);
     }
+    // the zero-block rule's fix works on a dense C
+    if (direct && zr.on) {
+        direct = false;
+        if (!dC.allocate((size_t)std::max<int64_t>(M * ldc * isz, 16), ctx->device)) {
+            cudaStreamSynchronize(ctx->stream);
+            return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+        }
+    }
+    iab::EncodeWork ew;
+    iab::CImage cimg;
+    if (direct) {
+        if (iab::encode_image_prepare(c->geom, &ew) != 0) {
+            cudaStreamSynchronize(ctx->stream);
+            return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
+        }
+        cimg.g = c->geom;
+        cimg.img = ew.img.as<uint8_t>();
+    }
     if (fused) {
     } else if (K == 0) {
         cudaMemsetAsync(dC.p, 0, (size_t)((vec ? M : M * ldc) * isz), ctx->stream);
@@ -1330,7 +1371,8 @@ static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_
         iab::gemv_native(dtype == IARRAY_DATA_TYPE_DOUBLE ? 0 : 1, M, K, dA.p, lda, dB.p, dC.p, ctx->stream);
         rc = cuda_rc(cudaGetLastError());
     } else {
-        rc = dense_product(ctx, dtype, M, N, K, dA.p, lda, dB.p, ldb, dC.p, ldc, zr.on ? &zr.zs : nullptr);
+        rc = dense_product(ctx, dtype, M, N, K, dA.p, lda, dB.p, ldb, dC.p, ldc, zr.on ? &zr.zs : nullptr,
+                           direct ? &cimg : nullptr);
     }
     if (INA_FAILED(rc)) return rc;
     if (zr.on && !fused) {
@@ -1342,7 +1384,8 @@ static ina_rc_t run_matmul(iarray_context_t *ctx, iarray_container_t *a, iarray_
     // dA and dB stay allocated until the encode below has synchronised the stream: the pool is
     // shared by every context, so memory released while the product may still read it could be
     // handed to another stream
-    rc = c->geom.nchunks ? encode_into(ctx, c, dC.p, vec ? M : ldc) : fill_zero_chunks(c);
+    if (direct) rc = encode_into_image(ctx, c, &ew);
+    else rc = c->geom.nchunks ? encode_into(ctx, c, dC.p, vec ? M : ldc) : fill_zero_chunks(c);
     if (INA_FAILED(rc)) return rc;
     tm.mark(4);
     tm.finish();

@@ -27,6 +27,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "bytes.cuh"
 #include "common.cuh"
 #include "tc_common.cuh"
 
@@ -619,18 +620,6 @@ __device__ __forceinline__ BlockSpan block_span(const Geom &g, int64_t c, int64_
     s.nr = (int)max((int64_t)0, min(min(g.block[0], g.chunk[0] - bi0 * g.block[0]), g.shape[0] - s.row0));
     s.nc = (int)max((int64_t)0, min(min(g.block[1], g.chunk[1] - bi1 * g.block[1]), g.shape[1] - s.col0));
     return s;
-}
-
-// 4x4 byte transpose: o_i holds byte i of a, b, c, d (in that order).
-__device__ __forceinline__ void transpose4x4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t &o0, uint32_t &o1,
-                                             uint32_t &o2, uint32_t &o3)
-{
-    const uint32_t ab_lo = __byte_perm(a, b, 0x5140), ab_hi = __byte_perm(a, b, 0x7362);
-    const uint32_t cd_lo = __byte_perm(c, d, 0x5140), cd_hi = __byte_perm(c, d, 0x7362);
-    o0 = __byte_perm(ab_lo, cd_lo, 0x5410);
-    o1 = __byte_perm(ab_lo, cd_lo, 0x7632);
-    o2 = __byte_perm(ab_hi, cd_hi, 0x5410);
-    o3 = __byte_perm(ab_hi, cd_hi, 0x7632);
 }
 
 // D2 fast path: shuffled, split blocks of partitions whose block rows hold whole groups of 4
@@ -2280,13 +2269,15 @@ int encode_gather(const Geom &g, const void *in, int64_t ld, bool shuffle, int s
     const int64_t img_bytes = nbl * g.blocksize;
     const int nstreams = encode_nstreams(g, shuffle, splitmode);
     const bool ext = w->ext_img != nullptr;
-    if ((!ext && (!w->img.allocate(img_bytes, dev) || !w->slots.allocate(img_bytes, dev) ||
+    const bool ready = w->img_ready && !ext && w->img.n >= (size_t)img_bytes;
+    if ((!ext && ((!ready && !w->img.allocate(img_bytes, dev)) || !w->slots.allocate(img_bytes, dev) ||
                   !w->es.allocate(sizeof(EncStream) * nbl * nstreams, dev))) ||
         (!w->ext_chunks && !w->ec.allocate(sizeof(EncChunk) * g.nchunks, dev)) || !w->tot.allocate(64, dev))
         return -100;
     w->nchunks = g.nchunks;
     uint8_t *img = ext ? w->ext_img : w->img.as<uint8_t>();
     cudaMemsetAsync(w->tot.p, 0, 64, st);
+    if (ready) return 0;                   // the product wrote the image
     const int sms = sm_count();
     const int64_t tpb = (g.blockn + TILE - 1) / TILE;
     const int64_t blocks = std::min<int64_t>(nbl * tpb, (int64_t)sms * 8);
@@ -2387,6 +2378,32 @@ int encode_finish(EncodeWork *w, std::vector<int64_t> *h_off, std::vector<int32_
     h_len->resize((size_t)n);
     for (int64_t c = 0; c < n; c++) { (*h_off)[c] = hc[c].offset; (*h_len)[c] = hc[c].cbytes; }
     return 0;
+}
+
+bool encode_image_ok(const Geom &g, bool shuffle, bool memcpy_only)
+{
+    return g.ndim == 2 && g.itemsize == 8 && shuffle && !memcpy_only && g.nchunks > 0 && !(g.block[1] & 3) &&
+           !(g.chunk[1] & 3) && g.blocksize > 0;
+}
+
+int encode_image_prepare(const Geom &g, EncodeWork *w)
+{
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!w->img.allocate((size_t)(g.nchunks * g.nblocks * g.blocksize), dev)) return -100;
+    w->img_ready = true;
+    return 0;
+}
+
+int encode_image_finish(const Geom &g, bool shuffle, int splitmode, DevBuf *d_out, std::vector<int64_t> *h_off,
+                        std::vector<int32_t> *h_len, cudaStream_t st, bool exact_lz4, EncodeWork *w)
+{
+    if (!w->img_ready) return -1;
+    w->exact_lz4 = exact_lz4;
+    w->memcpy_only = false;
+    const int r = encode_launch(g, nullptr, 0, shuffle, splitmode, d_out, w, st);
+    if (r) return r;
+    return encode_finish(w, h_off, h_len, st);
 }
 
 int encode_container(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, DevBuf *d_out,

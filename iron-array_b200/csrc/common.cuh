@@ -228,6 +228,7 @@ struct EncodeWork {
     DevBuf img, slots, es, ec, tot;
     bool exact_lz4 = true;            // liblz4-identical streams (see encode_container)
     bool memcpy_only = false;         // compression level 0: every chunk stored memcpyed (c-blosc2's clevel 0)
+    bool img_ready = false;           // img already holds the byte-plane image (written by the product)
     EncChunk *ext_chunks = nullptr;   // optional caller-owned chunk table (device) instead of `ec`
     // optional caller-owned byte-plane image, LZ4 output slots and stream results (device)
     // instead of img / slots / es: slices of buffers shared by several containers
@@ -237,6 +238,14 @@ struct EncodeWork {
 };
 int encode_launch(const Geom &g, const void *in, int64_t ld, bool shuffle, int splitmode, DevBuf *d_out,
                   EncodeWork *w, cudaStream_t st);
+// Encoding from an image the caller writes: encode_image_ok says whether a container of
+// geometry g can take it (float64, shuffled, LZ4, block[1] and chunk[1] multiples of 4);
+// encode_image_prepare allocates w->img for the caller to fill; encode_image_finish encodes it
+// (no gather) and returns the chunk table as encode_container does.
+bool encode_image_ok(const Geom &g, bool shuffle, bool memcpy_only);
+int encode_image_prepare(const Geom &g, EncodeWork *w);
+int encode_image_finish(const Geom &g, bool shuffle, int splitmode, DevBuf *d_out, std::vector<int64_t> *h_off,
+                        std::vector<int32_t> *h_len, cudaStream_t st, bool exact_lz4, EncodeWork *w);
 
 // encode_launch in stages, so that several containers can share one LZ4 launch:
 // encode_gather (dense -> byte-plane image), encode_streams (LZ4 over ns streams of neblock
@@ -320,10 +329,20 @@ int gemm_f64_grouped_tiles(int cfg, int M, int N);
 int gemm_f64_grouped_ctas(int cfg);          // resident CTAs of the persistent launch (SMs x occupancy)
 void gemm_f64_grouped(int cfg, const GemmProblem *d_probs, int nprob, int total_tiles, int ctas, cudaStream_t st);
 
+// The output of a float64 split product written straight into the byte-plane image of the
+// output container's encoder (shuffled blocks, the layout the encoder's gather would write:
+// block t = chunk * nblocks + block at t * blocksize, byte j of every item in plane j, padding
+// items zero) instead of a dense matrix.  Needs itemsize 8, block[1] and chunk[1] multiples of 4.
+struct CImage {
+    Geom g;          // the output container's geometry (shape M x N)
+    uint8_t *img;    // nchunks x nblocks x blocksize bytes
+};
+
 // Split-precision forms; return 0 on success, < 0 when unsupported on this device.
+// With cimg, C and ldc are not used: the product goes into cimg->img.
 int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda,
                    const double *B, int64_t ldb, double *C, int64_t ldc, int nterms, cudaStream_t st,
-                   const ZeroSkip *zs = nullptr);
+                   const ZeroSkip *zs = nullptr, const CImage *cimg = nullptr);
 // Asynchronous form with caller-owned work buffers (no host synchronisation until finish).
 // The B side (column scaling, residues, tensor map) is prepared once and can serve several
 // row bands of A (gemm_f64_ozaki_rows), each with its own OzakiWork.
@@ -339,6 +358,7 @@ struct OzakiB {
 struct OzakiWork {
     DevBuf ra, rr, sa, err;
     const ZeroSkip *zs = nullptr;          // optional: leave out zero-block pairs (zskip.cuh)
+    const CImage *cimg = nullptr;          // optional: write the product into an encoder image, not C
     alignas(64) unsigned char tmA[128];   // CUtensorMap of the residues of A (rows_prep -> rows_product)
     OzakiB b;                              // used by gemm_f64_ozaki_launch
 };

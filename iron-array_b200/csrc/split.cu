@@ -28,6 +28,7 @@
 #include <mutex>
 #include <vector>
 
+#include "bytes.cuh"
 #include "common.cuh"
 #include "tc_common.cuh"
 #include "zskip.cuh"
@@ -245,11 +246,36 @@ __global__ void k_col_shift(int K, int N, const double *__restrict__ B, int64_t 
 // dot products (one FMA per k, in order), so they carry the native product's IEEE
 // propagation.  One warp per row (warp index < M, flag rflag[i] == flagval) or column
 // (warp index - M); warps of rows and columns without such values return at once.
-template <typename T>
+// Offset of item (i, j) of a container in its encoder's shuffled block image (plane 0; plane
+// p is p * blockn further).
+__device__ __forceinline__ int64_t img_item_offset(const Geom &g, int64_t i, int64_t j)
+{
+    const int64_t ci = i / g.chunk[0], ii = i - ci * g.chunk[0], bi = ii / g.block[0];
+    const int64_t cj = j / g.chunk[1], jj = j - cj * g.chunk[1], bj = jj / g.block[1];
+    const int64_t t = (ci * g.cgrid[1] + cj) * g.nblocks + bi * g.bgrid[1] + bj;
+    return t * g.blocksize + (ii - bi * g.block[0]) * g.block[1] + (jj - bj * g.block[1]);
+}
+
+// Store of one output of the non-finite fix: dense C, or (IMG, float64 only) the eight bytes of
+// the item in the output container's shuffled block image.
+template <typename T, bool IMG>
+__device__ __forceinline__ void fix_store(T *C, int64_t ldc, const Geom &g, uint8_t *img, int64_t i, int64_t j, T v)
+{
+    if constexpr (IMG) {
+        const uint64_t x = (uint64_t)__double_as_longlong((double)v);
+        uint8_t *o = img + img_item_offset(g, i, j);
+#pragma unroll
+        for (int p = 0; p < 8; p++) o[(int64_t)p * g.blockn] = (uint8_t)(x >> (8 * p));
+    } else {
+        C[i * ldc + j] = v;
+    }
+}
+
+template <typename T, bool IMG>
 __global__ void __launch_bounds__(256) k_nonfinite_fix(int M, int N, int K, const T *__restrict__ A, int64_t lda,
                                                       const T *__restrict__ B, int64_t ldb, T *__restrict__ C,
                                                       int64_t ldc, const int *__restrict__ rflag,
-                                                      const int *__restrict__ cflag, int flagval)
+                                                      const int *__restrict__ cflag, int flagval, Geom g, uint8_t *img)
 {
     const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -259,7 +285,7 @@ __global__ void __launch_bounds__(256) k_nonfinite_fix(int M, int N, int K, cons
         for (int j = lane; j < N; j += 32) {
             T acc = 0;
             for (int k = 0; k < K; k++) acc = fma(A[(int64_t)i * lda + k], B[(int64_t)k * ldb + j], acc);
-            C[(int64_t)i * ldc + j] = acc;
+            fix_store<T, IMG>(C, ldc, g, img, i, j, acc);
         }
     } else if (w < (int64_t)M + N) {
         const int j = (int)(w - M);
@@ -267,18 +293,27 @@ __global__ void __launch_bounds__(256) k_nonfinite_fix(int M, int N, int K, cons
         for (int i = lane; i < M; i += 32) {
             T acc = 0;
             for (int k = 0; k < K; k++) acc = fma(A[(int64_t)i * lda + k], B[(int64_t)k * ldb + j], acc);
-            C[(int64_t)i * ldc + j] = acc;
+            fix_store<T, IMG>(C, ldc, g, img, i, j, acc);
         }
     }
 }
 
 template <typename T>
 static void launch_nonfinite_fix(int64_t M, int64_t N, int64_t K, const T *A, int64_t lda, const T *B, int64_t ldb,
-                                 T *C, int64_t ldc, const int *rflag, const int *cflag, int flagval, cudaStream_t st)
+                                 T *C, int64_t ldc, const int *rflag, const int *cflag, int flagval, cudaStream_t st,
+                                 const CImage *cimg = nullptr)
 {
     const int64_t threads = (M + N) * 32;
-    IAB_TIMED("k_nonfinite_fix", st, k_nonfinite_fix<T><<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(
-        (int)M, (int)N, (int)K, A, lda, B, ldb, C, ldc, rflag, cflag, flagval));
+    const unsigned grid = (unsigned)((threads + 255) / 256);
+    if (cimg) {
+        IAB_TIMED("k_nonfinite_fix", st, k_nonfinite_fix<T, true><<<grid, 256, 0, st>>>(
+            (int)M, (int)N, (int)K, A, lda, B, ldb, C, ldc, rflag, cflag, flagval, cimg->g, cimg->img));
+    } else {
+        Geom g0;
+        memset(&g0, 0, sizeof(g0));
+        IAB_TIMED("k_nonfinite_fix", st, k_nonfinite_fix<T, false><<<grid, 256, 0, st>>>(
+            (int)M, (int)N, (int)K, A, lda, B, ldb, C, ldc, rflag, cflag, flagval, g0, nullptr));
+    }
 }
 
 // ============================================================================ residues
@@ -804,68 +839,143 @@ __device__ __forceinline__ double unscale(double x, int e)
 
 // C_ij = 2^-(sA_i + sB_j) * centred( sum_l r_l w_l mod P ); four entries per thread.
 // Outputs j0 .. j0 + 3 of row i of one product: reconstruction from the L residue planes
-// R[l][i][j] (plane = M ldr bytes), unscaled by the row and column shifts.
+// R[l][i][j] (plane = M ldr bytes), unscaled by the row and column shifts (j0 % 4 == 0; the
+// four residue bytes are read as one word, inside the row's ldr bytes).
+template <int NC>
+__device__ __forceinline__ void crt_quad_values(int N, const uint8_t *__restrict__ R, int64_t ldr, int64_t plane, int si,
+                                                const int *__restrict__ sB, int i, int j0, double (&v)[4])
+{
+    const int L = c_crt.L;
+    const uint8_t *rp = R + (int64_t)i * ldr + j0;
+    uint32_t w[16];
+#pragma unroll
+    for (int l = 0; l < 16; l++) w[l] = l < L ? *reinterpret_cast<const uint32_t *>(rp + l * plane) : 0u;  // ldr % 16 == 0
+    double S[4][NC];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int k = 0; k < NC; k++) S[u][k] = 0.0;
+    const int np = c_crt.np;
+#pragma unroll
+    for (int p = 0; p < 8; p++) {
+        if (p < np) {
+            const uint32_t m0 = c_crt.pm0[p], m1 = c_crt.pm1[p], inv = c_crt.pinv[p], mg = c_crt.pmagic[p];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const uint32_t r0 = (w[2 * p] >> (8 * u)) & 0xffu;
+                uint32_t y = r0;
+                if (m1 > 1) {
+                    const uint32_t r1 = (w[2 * p + 1] >> (8 * u)) & 0xffu;
+                    const uint32_t prod = (r1 + 2 * m1 - r0) * inv;           // < 2^18
+                    const uint32_t t = prod - __umulhi(prod, mg) * m1;         // prod mod m1, exact
+                    y = r0 + m0 * t;
+                }
+                // y as a double: 2^52 + y, less 2^52
+                const double yd = __hiloint2double(0x43300000, (int)y) - kTwo52;
+#pragma unroll
+                for (int k = 0; k < NC; k++) S[u][k] = fma(yd, c_crt.pw[p][k], S[u][k]);
+            }
+        }
+    }
+    bool ok[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        const int sj = j0 + u < N ? sB[j0 + u] : kNonFinite;
+        // rows / columns with NaN or infinity are recomputed by k_nonfinite_fix
+        ok[u] = si != kNonFinite && sj != kNonFinite;
+        v[u] = crt_value<NC>(S[u]);
+        v[u] = unscale(v[u], ok[u] ? si + sj : 0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) v[u] = ok[u] ? v[u] : 0.0;
+}
+
 template <int NC>
 __device__ __forceinline__ void crt_quad(int N, const uint8_t *__restrict__ R, int64_t ldr, int64_t plane, int si,
                                          const int *__restrict__ sB, double *__restrict__ C, int64_t ldc, int i, int j0)
 {
-    const int L = c_crt.L;
-    {
-        const uint8_t *rp = R + (int64_t)i * ldr + j0;
-        uint32_t w[16];
-#pragma unroll
-        for (int l = 0; l < 16; l++) w[l] = l < L ? *reinterpret_cast<const uint32_t *>(rp + l * plane) : 0u;  // ldr % 16 == 0
-        double S[4][NC];
+    double v[4];
+    crt_quad_values<NC>(N, R, ldr, plane, si, sB, i, j0, v);
+    double *cp = C + (int64_t)i * ldc + j0;
+    if (j0 + 3 < N && (reinterpret_cast<uintptr_t>(cp) & 15) == 0) {
+        reinterpret_cast<double2 *>(cp)[0] = make_double2(v[0], v[1]);
+        reinterpret_cast<double2 *>(cp)[1] = make_double2(v[2], v[3]);
+    } else {
 #pragma unroll
         for (int u = 0; u < 4; u++)
-#pragma unroll
-            for (int k = 0; k < NC; k++) S[u][k] = 0.0;
-        const int np = c_crt.np;
-#pragma unroll
-        for (int p = 0; p < 8; p++) {
-            if (p < np) {
-                const uint32_t m0 = c_crt.pm0[p], m1 = c_crt.pm1[p], inv = c_crt.pinv[p], mg = c_crt.pmagic[p];
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const uint32_t r0 = (w[2 * p] >> (8 * u)) & 0xffu;
-                    uint32_t y = r0;
-                    if (m1 > 1) {
-                        const uint32_t r1 = (w[2 * p + 1] >> (8 * u)) & 0xffu;
-                        const uint32_t prod = (r1 + 2 * m1 - r0) * inv;           // < 2^18
-                        const uint32_t t = prod - __umulhi(prod, mg) * m1;         // prod mod m1, exact
-                        y = r0 + m0 * t;
-                    }
-                    // y as a double: 2^52 + y, less 2^52
-                    const double yd = __hiloint2double(0x43300000, (int)y) - kTwo52;
-#pragma unroll
-                    for (int k = 0; k < NC; k++) S[u][k] = fma(yd, c_crt.pw[p][k], S[u][k]);
-                }
-            }
-        }
-        double v[4];
-        bool ok[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int sj = j0 + u < N ? sB[j0 + u] : kNonFinite;
-            // rows / columns with NaN or infinity are recomputed by k_nonfinite_fix
-            ok[u] = si != kNonFinite && sj != kNonFinite;
-            v[u] = crt_value<NC>(S[u]);
-            v[u] = unscale(v[u], ok[u] ? si + sj : 0);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++) v[u] = ok[u] ? v[u] : 0.0;
-        double *cp = C + (int64_t)i * ldc + j0;
-        if (j0 + 3 < N && (reinterpret_cast<uintptr_t>(cp) & 15) == 0) {
-            reinterpret_cast<double2 *>(cp)[0] = make_double2(v[0], v[1]);
-            reinterpret_cast<double2 *>(cp)[1] = make_double2(v[2], v[3]);
-        } else {
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-                if (j0 + u < N) cp[u] = v[u];
-        }
+            if (j0 + u < N) cp[u] = v[u];
     }
 }
 
+// Rows of a block per work unit of the image reconstruction.
+constexpr int CRT_SLICE = 128;
+
+// The reconstruction written into the output container's shuffled block image (CImage): work
+// units are slices of CRT_SLICE rows of one block; each thread takes 4 consecutive items of a
+// block row (one 4-byte word per byte plane), the logical ones reconstructed, chunk and array
+// padding zero, exactly the image the encoder's gather would write from the dense product.
+// Needs block[1] % 4 == 0 and chunk[1] % 4 == 0 (every quad starts at a column j0 % 4 == 0).
+template <int NC>
+__global__ void __launch_bounds__(256) k_crt_img(Geom g, const uint8_t *__restrict__ R, int64_t ldr,
+                                                 const int *__restrict__ sA, const int *__restrict__ sB,
+                                                 uint8_t *__restrict__ img)
+{
+    const int M = (int)g.shape[0], N = (int)g.shape[1];
+    const int64_t plane = (int64_t)M * ldr;
+    const int qpr = (int)(g.block[1] / 4);
+    const int step_r = (int)blockDim.x / qpr, step_q = (int)blockDim.x - step_r * qpr;
+    const int spb = (int)((g.block[0] + CRT_SLICE - 1) / CRT_SLICE);
+    const int64_t units = g.nchunks * g.nblocks * spb;
+    const bool small = units < (int64_t(1) << 31) && g.cgrid[1] < (int64_t(1) << 31);
+    for (int64_t un = blockIdx.x; un < units; un += gridDim.x) {
+        int64_t t, c, b, ci0, ci1, bi0, bi1;
+        int sl;
+        if (small) {                         // 32-bit divisions (the usual case)
+            const uint32_t t32 = (uint32_t)un / (uint32_t)spb, c32 = t32 / (uint32_t)g.nblocks;
+            const uint32_t b32 = t32 - c32 * (uint32_t)g.nblocks;
+            sl = (int)((uint32_t)un - t32 * (uint32_t)spb);
+            t = t32; c = c32; b = b32;
+            ci0 = c32 / (uint32_t)g.cgrid[1]; ci1 = c32 - (uint32_t)ci0 * (uint32_t)g.cgrid[1];
+            bi0 = b32 / (uint32_t)g.bgrid[1]; bi1 = b32 - (uint32_t)bi0 * (uint32_t)g.bgrid[1];
+        } else {
+            t = un / spb;
+            sl = (int)(un - t * spb);
+            c = t / g.nblocks; b = t - c * g.nblocks;
+            ci0 = c / g.cgrid[1]; ci1 = c - ci0 * g.cgrid[1];
+            bi0 = b / g.bgrid[1]; bi1 = b - bi0 * g.bgrid[1];
+        }
+        const int64_t row0 = ci0 * g.chunk[0] + bi0 * g.block[0], col0 = ci1 * g.chunk[1] + bi1 * g.block[1];
+        const int nr = (int)max((int64_t)0, min(min(g.block[0], g.chunk[0] - bi0 * g.block[0]), g.shape[0] - row0));
+        const int nc = (int)max((int64_t)0, min(min(g.block[1], g.chunk[1] - bi1 * g.block[1]), g.shape[1] - col0));
+        uint8_t *blk = img + t * g.blocksize;
+        const int r_lo = sl * CRT_SLICE, r_hi = (int)min((int64_t)r_lo + CRT_SLICE, g.block[0]);
+        const int nq = (r_hi - r_lo) * qpr;
+        // (row, quad column) of each thread's quad, advanced by a fixed step per iteration
+        int r = r_lo + (int)threadIdx.x / qpr, q = (int)threadIdx.x % qpr;
+        for (int k = threadIdx.x; k < nq; k += blockDim.x, r += step_r, q += step_q) {
+            if (q >= qpr) { q -= qpr; r++; }
+            const int cc = q * 4;
+            double v[4] = {0.0, 0.0, 0.0, 0.0};
+            if (r < nr && cc < nc) {
+                const int i = (int)row0 + r;
+                crt_quad_values<NC>(N, R, ldr, plane, sA[i], sB, i, (int)col0 + cc, v);
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (cc + u >= nc) v[u] = 0.0;                  // chunk or array padding
+            }
+            uint64_t x[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) x[u] = (uint64_t)__double_as_longlong(v[u]);
+            uint32_t o[8];
+            transpose4x4((uint32_t)x[0], (uint32_t)x[1], (uint32_t)x[2], (uint32_t)x[3], o[0], o[1], o[2], o[3]);
+            transpose4x4((uint32_t)(x[0] >> 32), (uint32_t)(x[1] >> 32), (uint32_t)(x[2] >> 32), (uint32_t)(x[3] >> 32),
+                         o[4], o[5], o[6], o[7]);
+            const int64_t i0 = (int64_t)r * g.block[1] + cc;
+#pragma unroll
+            for (int p = 0; p < 8; p++) *reinterpret_cast<uint32_t *>(blk + (int64_t)p * g.blockn + i0) = o[p];
+        }
+    }
+}
 
 template <int NC>
 __global__ void __launch_bounds__(256) k_crt(int M, int N, const uint8_t *__restrict__ R, int64_t ldr,
@@ -892,6 +1002,17 @@ static void launch_crt(int nc, unsigned grid, int M, int N, const uint8_t *R, in
     }
 }
 
+static void launch_crt_img(int nc, unsigned grid, const Geom &g, const uint8_t *R, int64_t ldr, const int *sA,
+                           const int *sB, uint8_t *img, cudaStream_t st)
+{
+    switch (nc) {
+    case 1: IAB_TIMED("k_crt_img", st, k_crt_img<1><<<grid, 256, 0, st>>>(g, R, ldr, sA, sB, img)); break;
+    case 2: IAB_TIMED("k_crt_img", st, k_crt_img<2><<<grid, 256, 0, st>>>(g, R, ldr, sA, sB, img)); break;
+    case 3: IAB_TIMED("k_crt_img", st, k_crt_img<3><<<grid, 256, 0, st>>>(g, R, ldr, sA, sB, img)); break;
+    default: IAB_TIMED("k_crt_img", st, k_crt_img<4><<<grid, 256, 0, st>>>(g, R, ldr, sA, sB, img)); break;
+    }
+}
+
 // ============================================================================ host driver
 static int sms()
 {
@@ -911,10 +1032,14 @@ static bool device_is_sm100()
 }
 
 int gemm_f64_ozaki(int64_t M, int64_t N, int64_t K, const double *A, int64_t lda, const double *B, int64_t ldb,
-                   double *C, int64_t ldc, int nterms, cudaStream_t st, const ZeroSkip *zs)
+                   double *C, int64_t ldc, int nterms, cudaStream_t st, const ZeroSkip *zs, const CImage *cimg)
 {
+    if (cimg && (cimg->g.shape[0] != M || cimg->g.shape[1] != N || cimg->g.itemsize != 8 || (cimg->g.block[1] & 3) ||
+                 (cimg->g.chunk[1] & 3) || M > (1 << 30) || N > (1 << 30)))
+        return -1;
     OzakiWork w;
     w.zs = zs;
+    w.cimg = cimg;
     const int r = gemm_f64_ozaki_launch(M, N, K, A, lda, B, ldb, C, ldc, nterms, &w, st);
     if (r) return r;
     return gemm_f64_ozaki_finish(&w, st);
@@ -1048,8 +1173,15 @@ int gemm_f64_ozaki_rows_product(int64_t M, const double *A, int64_t lda, const O
         IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<true, false><<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
     else
         IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<false, false><<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
-    launch_crt(ob.nc, (unsigned)(nsm * 8), (int)M, (int)N, w->rr.as<uint8_t>(), ldr, w->sa.as<int>(), ob.sb.as<int>(), C, ldc, st);
-    launch_nonfinite_fix<double>(M, N, K, A, lda, ob.B, ob.ldb, C, ldc, w->sa.as<int>(), ob.sb.as<int>(), kNonFinite, st);
+    if (w->cimg) {
+        launch_crt_img(ob.nc, (unsigned)(nsm * 8), w->cimg->g, w->rr.as<uint8_t>(), ldr, w->sa.as<int>(), ob.sb.as<int>(),
+                       w->cimg->img, st);
+    } else {
+        launch_crt(ob.nc, (unsigned)(nsm * 8), (int)M, (int)N, w->rr.as<uint8_t>(), ldr, w->sa.as<int>(), ob.sb.as<int>(), C,
+                   ldc, st);
+    }
+    launch_nonfinite_fix<double>(M, N, K, A, lda, ob.B, ob.ldb, C, ldc, w->sa.as<int>(), ob.sb.as<int>(), kNonFinite, st,
+                                 w->cimg);
     return 0;
 }
 

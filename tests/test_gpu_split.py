@@ -251,3 +251,43 @@ def test_split_f64_row_slices_equal_whole(ia, M, K, N):
     hi, lo = O.dd_rows(a, b, rows)
     d = (c1[rows] - hi) - lo
     assert np.linalg.norm(d) <= 1e-14 * np.linalg.norm(hi)
+
+
+@pytest.mark.parametrize("M,K,N,ch,bl", [
+    (300, 200, 260, (100, 120), (40, 40)),     # array and chunk padding (chunk 120 = 3 blocks of 40)
+    (512, 300, 512, (256, 256), (64, 64)),     # no padding
+    (130, 70, 100, (64, 52), (32, 20)),        # blocks wider than the chunk's last columns
+    (100, 50, 90, (50, 30), (25, 10)),         # chunk columns not a multiple of 4: dense C, then gather
+])
+@pytest.mark.parametrize("encoder", ["parallel", "liblz4"])
+def test_split_f64_output_written_into_encoder_image(ia, M, K, N, ch, bl, encoder):
+    """The split form writes C's reconstruction straight into the encoder's shuffled block image
+    (no dense C, no gather).  C's chunks must be byte for byte those of the same values encoded
+    from a dense array, its values those of the dense split product; rows and columns with NaN or
+    infinity go through the non-finite fix into the same image."""
+    import ctypes
+    import torch
+    rng = np.random.default_rng(M * N + K)
+    a, b = _scaled(rng, (M, K)), _scaled(rng, (K, N))
+    a[M // 2, 3] = np.nan
+    b[K - 1, N // 3] = np.inf
+    enc = ia.ENCODER_LIBLZ4 if encoder == "liblz4" else ia.ENCODER_PARALLEL
+    ctx = ia.Context(form=ia.FORM_SPLIT, encoder=enc)
+    Ac = ia.Container.from_numpy(ctx, a, ch, bl)
+    Bc = ia.Container.from_numpy(ctx, b, (ch[1], ch[1]), (bl[1], bl[1]))
+    C = ia.matmul(ctx, Ac, Bc, ch, bl)
+    got = C.to_numpy()
+    A = torch.from_numpy(a).cuda()
+    B = torch.from_numpy(b).cuda()
+    D = torch.empty((M, N), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    ia.check(ia.lib().iarray_b200_dense_gemm(ctx.ptr, ia.DTYPE_DOUBLE, M, N, K, ctypes.c_void_p(A.data_ptr()), K,
+                                              ctypes.c_void_p(B.data_ptr()), N, ctypes.c_void_p(D.data_ptr()), N),
+             "dense_gemm")
+    ctx.synchronize()
+    dense = D.cpu().numpy()
+    assert got.tobytes() == dense.tobytes()
+    assert np.isnan(got[M // 2]).all() and not np.isfinite(got[:, N // 3]).any()
+    ref = ia.Container.from_numpy(ctx, dense, ch, bl)
+    assert C.chunks() == ref.chunks()
+    ctx.close()
