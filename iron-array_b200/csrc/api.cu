@@ -2109,9 +2109,21 @@ static ina_rc_t batch_tune_split(iarray_b200_batch_t *bt)
         g_tune_cache[sig] = L;
     }
     bt->split_terms = L;
-    const int r = iab::gemm_f64_ozaki_grouped_setup(items_into(nullptr), L, &bt->ozg, ctx->stream);
+    // the graph's reconstruction writes the outputs' encoder images straight away (no dense C,
+    // no gather) when the outputs are encoded as one group and every one can take it
+    std::vector<iab::OzGroupItem> items = items_into(nullptr);
+    bool img = bt->egroup && ctx->cfg.compression_level != 0;
+    for (size_t i = 0; i < un && img; i++)
+        img = bt->M[i] > 0 && bt->N[i] > 0 && bt->K[i] > 0 && iab::encode_image_ok(bt->cgeom[i], true, false);
+    if (img)
+        for (size_t i = 0; i < un; i++) {
+            items[i].cimg = bt->egrp.h[i].img;
+            items[i].gc = bt->cgeom[i];
+        }
+    const int r = iab::gemm_f64_ozaki_grouped_setup(items, L, &bt->ozg, ctx->stream);
     if (r == -100) return rc_err(IARRAY_ERR_GPU_OUT_OF_MEMORY);
     if (r) return rc_err(IARRAY_ERR_NOT_SUPPORTED);
+    bt->egrp.img_ready = img;
     return INA_SUCCESS;
 }
 

@@ -3008,13 +3008,13 @@ int encode_group_launch(CodecGroup *grp, bool exact_lz4, bool memcpy_only, cudaS
         all_fast = all_fast && !(g.block[1] & 3);
     }
     const int64_t gb = std::max<int64_t>(std::min<int64_t>(grp->nbl, (int64_t)sms * 8), 1);
-    if (fast) {
+    if (fast && !grp->img_ready) {
         if (ts == 8)
             IAB_TIMED("k_gather_fast", st, k_gather_fast_g<8><<<(unsigned)gb, 256, 0, st>>>(items, bstart, n, grp->nbl));
         else
             IAB_TIMED("k_gather_fast", st, k_gather_fast_g<4><<<(unsigned)gb, 256, 0, st>>>(items, bstart, n, grp->nbl));
     }
-    if (!all_fast) {
+    if (!all_fast && !grp->img_ready) {
         const int64_t tb = std::max<int64_t>(std::min<int64_t>(grp->nbl * grp->max_tpb, (int64_t)sms * 8), 1);
         IAB_TIMED("k_gather", st, k_gather_g<<<(unsigned)tb, 256, 0, st>>>(items, bstart, n, grp->nbl, grp->max_tpb, fast,
                                                                            grp->shuffle));

@@ -291,6 +291,7 @@ struct CodecGroup {
     DevBuf items, starts;                  // device table; starts: blocks, slices, chunks ([n + 1] each)
     DevBuf bd, sd, scratch, rest, counters;   // decode work shared by the group; counters: [0] rest length, [2..] LZ4 cursor
     DevBuf img, slots, es, outsz;          // encode work shared by the group
+    bool img_ready = false;                // encode: the producer writes img itself (no gather)
     DecodeQueue q;
 };
 // Decode group: a[i] is container i (all of item size ts), cnt[i] its 16-int status slot.
@@ -386,12 +387,18 @@ struct OzGroupItem {
     const double *B;
     double *C;
     int64_t lda, ldb, ldc;
+    // optional (every item or none): C's encoder image and geometry, written instead of C
+    // (the CImage layout)
+    uint8_t *cimg = nullptr;
+    Geom gc = {};
 };
 struct OzGroupWork {
     DevBuf ra, rb, rr, sa, sb, pm, ps, probs, maps, err;
     int L = 0, nc = 0, np = 0;
     double gamma = 0;
     int64_t rows = 0, cols = 0, tasks_r = 0, tiles_c = 0, items = 0, crt = 0;
+    bool img = false;                // the reconstruction writes the items' encoder images
+    int64_t units = 0;               // its work units (block slices of every image)
 };
 int gemm_f64_ozaki_grouped_setup(const std::vector<OzGroupItem> &items, int nterms, OzGroupWork *w, cudaStream_t st);
 int gemm_f64_ozaki_grouped_launch(OzGroupWork *w, cudaStream_t st);

@@ -476,6 +476,9 @@ struct OzGProb {
     int8_t *ra, *rb;             // residues [L][M][Kp], [L][N][Kp]
     uint8_t *R;                  // residues of the product [L][M][ldr]
     int64_t ldr;
+    Geom gc;                     // image output (OzGroupWork::img): C's geometry, its encoder image,
+    uint8_t *cimg;               // and the first work unit of the grouped image reconstruction
+    int64_t unit0;
 };
 
 // Index of the product whose range [key(q), key(q + 1)) holds v: the last q with key(q) <= v
@@ -915,11 +918,13 @@ constexpr int CRT_SLICE = 128;
 // block row (one 4-byte word per byte plane), the logical ones reconstructed, chunk and array
 // padding zero, exactly the image the encoder's gather would write from the dense product.
 // Needs block[1] % 4 == 0 and chunk[1] % 4 == 0 (every quad starts at a column j0 % 4 == 0).
-// Held to 80 registers (three CTAs per SM): 0.70 ms instead of 0.79 ms at 8192^2 with 102.
+//
+// One work unit of it: rows [CRT_SLICE sl, CRT_SLICE (sl + 1)) of block t of the output's image
+// (unit un = t x slices-per-block + sl); sA / sB are the product's row and column shifts.
 template <int NC>
-__global__ void __launch_bounds__(256, 3) k_crt_img(Geom g, const uint8_t *__restrict__ R, int64_t ldr,
-                                                 const int *__restrict__ sA, const int *__restrict__ sB,
-                                                 uint8_t *__restrict__ img)
+__device__ __forceinline__ void crt_img_unit(const Geom &g, const uint8_t *__restrict__ R, int64_t ldr,
+                                             const int *__restrict__ sA, const int *__restrict__ sB,
+                                             uint8_t *__restrict__ img, int64_t un)
 {
     const int M = (int)g.shape[0], N = (int)g.shape[1];
     const int64_t plane = (int64_t)M * ldr;
@@ -928,54 +933,63 @@ __global__ void __launch_bounds__(256, 3) k_crt_img(Geom g, const uint8_t *__res
     const int spb = (int)((g.block[0] + CRT_SLICE - 1) / CRT_SLICE);
     const int64_t units = g.nchunks * g.nblocks * spb;
     const bool small = units < (int64_t(1) << 31) && g.cgrid[1] < (int64_t(1) << 31);
-    for (int64_t un = blockIdx.x; un < units; un += gridDim.x) {
-        int64_t t, c, b, ci0, ci1, bi0, bi1;
-        int sl;
-        if (small) {                         // 32-bit divisions (the usual case)
-            const uint32_t t32 = (uint32_t)un / (uint32_t)spb, c32 = t32 / (uint32_t)g.nblocks;
-            const uint32_t b32 = t32 - c32 * (uint32_t)g.nblocks;
-            sl = (int)((uint32_t)un - t32 * (uint32_t)spb);
-            t = t32; c = c32; b = b32;
-            ci0 = c32 / (uint32_t)g.cgrid[1]; ci1 = c32 - (uint32_t)ci0 * (uint32_t)g.cgrid[1];
-            bi0 = b32 / (uint32_t)g.bgrid[1]; bi1 = b32 - (uint32_t)bi0 * (uint32_t)g.bgrid[1];
-        } else {
-            t = un / spb;
-            sl = (int)(un - t * spb);
-            c = t / g.nblocks; b = t - c * g.nblocks;
-            ci0 = c / g.cgrid[1]; ci1 = c - ci0 * g.cgrid[1];
-            bi0 = b / g.bgrid[1]; bi1 = b - bi0 * g.bgrid[1];
-        }
-        const int64_t row0 = ci0 * g.chunk[0] + bi0 * g.block[0], col0 = ci1 * g.chunk[1] + bi1 * g.block[1];
-        const int nr = (int)max((int64_t)0, min(min(g.block[0], g.chunk[0] - bi0 * g.block[0]), g.shape[0] - row0));
-        const int nc = (int)max((int64_t)0, min(min(g.block[1], g.chunk[1] - bi1 * g.block[1]), g.shape[1] - col0));
-        uint8_t *blk = img + t * g.blocksize;
-        const int r_lo = sl * CRT_SLICE, r_hi = (int)min((int64_t)r_lo + CRT_SLICE, g.block[0]);
-        const int nq = (r_hi - r_lo) * qpr;
-        // (row, quad column) of each thread's quad, advanced by a fixed step per iteration
-        int r = r_lo + (int)threadIdx.x / qpr, q = (int)threadIdx.x % qpr;
-        for (int k = threadIdx.x; k < nq; k += blockDim.x, r += step_r, q += step_q) {
-            if (q >= qpr) { q -= qpr; r++; }
-            const int cc = q * 4;
-            double v[4] = {0.0, 0.0, 0.0, 0.0};
-            if (r < nr && cc < nc) {
-                const int i = (int)row0 + r;
-                crt_quad_values<NC>(N, R, ldr, plane, sA[i], sB, i, (int)col0 + cc, v);
-#pragma unroll
-                for (int u = 0; u < 4; u++)
-                    if (cc + u >= nc) v[u] = 0.0;                  // chunk or array padding
-            }
-            uint64_t x[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) x[u] = (uint64_t)__double_as_longlong(v[u]);
-            uint32_t o[8];
-            transpose4x4((uint32_t)x[0], (uint32_t)x[1], (uint32_t)x[2], (uint32_t)x[3], o[0], o[1], o[2], o[3]);
-            transpose4x4((uint32_t)(x[0] >> 32), (uint32_t)(x[1] >> 32), (uint32_t)(x[2] >> 32), (uint32_t)(x[3] >> 32),
-                         o[4], o[5], o[6], o[7]);
-            const int64_t i0 = (int64_t)r * g.block[1] + cc;
-#pragma unroll
-            for (int p = 0; p < 8; p++) *reinterpret_cast<uint32_t *>(blk + (int64_t)p * g.blockn + i0) = o[p];
-        }
+    int64_t t, c, b, ci0, ci1, bi0, bi1;
+    int sl;
+    if (small) {                         // 32-bit divisions (the usual case)
+        const uint32_t t32 = (uint32_t)un / (uint32_t)spb, c32 = t32 / (uint32_t)g.nblocks;
+        const uint32_t b32 = t32 - c32 * (uint32_t)g.nblocks;
+        sl = (int)((uint32_t)un - t32 * (uint32_t)spb);
+        t = t32; c = c32; b = b32;
+        ci0 = c32 / (uint32_t)g.cgrid[1]; ci1 = c32 - (uint32_t)ci0 * (uint32_t)g.cgrid[1];
+        bi0 = b32 / (uint32_t)g.bgrid[1]; bi1 = b32 - (uint32_t)bi0 * (uint32_t)g.bgrid[1];
+    } else {
+        t = un / spb;
+        sl = (int)(un - t * spb);
+        c = t / g.nblocks; b = t - c * g.nblocks;
+        ci0 = c / g.cgrid[1]; ci1 = c - ci0 * g.cgrid[1];
+        bi0 = b / g.bgrid[1]; bi1 = b - bi0 * g.bgrid[1];
     }
+    const int64_t row0 = ci0 * g.chunk[0] + bi0 * g.block[0], col0 = ci1 * g.chunk[1] + bi1 * g.block[1];
+    const int nr = (int)max((int64_t)0, min(min(g.block[0], g.chunk[0] - bi0 * g.block[0]), g.shape[0] - row0));
+    const int nc = (int)max((int64_t)0, min(min(g.block[1], g.chunk[1] - bi1 * g.block[1]), g.shape[1] - col0));
+    uint8_t *blk = img + t * g.blocksize;
+    const int r_lo = sl * CRT_SLICE, r_hi = (int)min((int64_t)r_lo + CRT_SLICE, g.block[0]);
+    const int nq = (r_hi - r_lo) * qpr;
+    // (row, quad column) of each thread's quad, advanced by a fixed step per iteration
+    int r = r_lo + (int)threadIdx.x / qpr, q = (int)threadIdx.x % qpr;
+    for (int k = threadIdx.x; k < nq; k += blockDim.x, r += step_r, q += step_q) {
+        if (q >= qpr) { q -= qpr; r++; }
+        const int cc = q * 4;
+        double v[4] = {0.0, 0.0, 0.0, 0.0};
+        if (r < nr && cc < nc) {
+            const int i = (int)row0 + r;
+            crt_quad_values<NC>(N, R, ldr, plane, sA[i], sB, i, (int)col0 + cc, v);
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (cc + u >= nc) v[u] = 0.0;                  // chunk or array padding
+        }
+        uint64_t x[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) x[u] = (uint64_t)__double_as_longlong(v[u]);
+        uint32_t o[8];
+        transpose4x4((uint32_t)x[0], (uint32_t)x[1], (uint32_t)x[2], (uint32_t)x[3], o[0], o[1], o[2], o[3]);
+        transpose4x4((uint32_t)(x[0] >> 32), (uint32_t)(x[1] >> 32), (uint32_t)(x[2] >> 32), (uint32_t)(x[3] >> 32),
+                     o[4], o[5], o[6], o[7]);
+        const int64_t i0 = (int64_t)r * g.block[1] + cc;
+#pragma unroll
+        for (int p = 0; p < 8; p++) *reinterpret_cast<uint32_t *>(blk + (int64_t)p * g.blockn + i0) = o[p];
+    }
+}
+
+// Work units: slices of CRT_SLICE rows of one block of the image.  Held to 80 registers (three
+// CTAs per SM): 0.70 ms instead of 0.79 ms at 8192^2 with 102.
+template <int NC>
+__global__ void __launch_bounds__(256, 3) k_crt_img(Geom g, const uint8_t *__restrict__ R, int64_t ldr,
+                                                    const int *__restrict__ sA, const int *__restrict__ sB,
+                                                    uint8_t *__restrict__ img)
+{
+    const int64_t units = g.nchunks * g.nblocks * ((g.block[0] + CRT_SLICE - 1) / CRT_SLICE);
+    for (int64_t un = blockIdx.x; un < units; un += gridDim.x) crt_img_unit<NC>(g, R, ldr, sA, sB, img, un);
 }
 
 template <int NC>
@@ -1395,6 +1409,38 @@ __global__ void __launch_bounds__(256) k_crt_g(const OzGProb *__restrict__ pr, i
     }
 }
 
+// The grouped reconstruction into the products' encoder images: the work units of every image
+// numbered consecutively (unit0), each unit as in k_crt_img.
+template <int NC>
+__global__ void __launch_bounds__(256, 3) k_crt_img_g(const OzGProb *__restrict__ pr, int np, int64_t units,
+                                                      const int *__restrict__ sA, const int *__restrict__ sB)
+{
+    int qh = -1;
+    for (int64_t un = blockIdx.x; un < units; un += gridDim.x) {
+        const OzGProb &q = pr[oz_walk(pr, np, un, [](const OzGProb &x) { return x.unit0; }, qh)];
+        // the product's fields read once (the image stores could alias the table as far as the
+        // compiler can tell, which would reload every field after each store)
+        const Geom g = q.gc;
+        const uint8_t *R = q.R;
+        uint8_t *img = q.cimg;
+        const int64_t ldr = q.ldr, row0 = q.row0, col0 = q.col0, unit0 = q.unit0;
+        crt_img_unit<NC>(g, R, ldr, sA + row0, sB + col0, img, un - unit0);
+    }
+}
+
+// Output (i, j) of product q: its dense C, or its encoder image's eight bytes.
+__device__ __forceinline__ void oz_store(const OzGProb &q, int64_t i, int64_t j, double v)
+{
+    if (q.cimg) {
+        const uint64_t x = (uint64_t)__double_as_longlong(v);
+        uint8_t *o = q.cimg + img_item_offset(q.gc, i, j);
+#pragma unroll
+        for (int p = 0; p < 8; p++) o[(int64_t)p * q.gc.blockn] = (uint8_t)(x >> (8 * p));
+    } else {
+        q.C[i * q.ldc + j] = v;
+    }
+}
+
 // Rows and columns holding NaN or infinity, of every product: one warp per row (global row
 // index < rows) or column (the rest), recomputing its outputs as plain dot products.
 __global__ void __launch_bounds__(256) k_nonfinite_fix_g(const OzGProb *__restrict__ pr, int np, int64_t rows,
@@ -1410,7 +1456,7 @@ __global__ void __launch_bounds__(256) k_nonfinite_fix_g(const OzGProb *__restri
         for (int j = lane; j < q.N; j += 32) {
             double acc = 0;
             for (int k = 0; k < q.K; k++) acc = fma(q.A[i * q.lda + k], q.B[(int64_t)k * q.ldb + j], acc);
-            q.C[i * q.ldc + j] = acc;
+            oz_store(q, i, j, acc);
         }
     } else if (w < rows + cols) {
         const int64_t g = w - rows;
@@ -1420,7 +1466,7 @@ __global__ void __launch_bounds__(256) k_nonfinite_fix_g(const OzGProb *__restri
         for (int i = lane; i < q.M; i += 32) {
             double acc = 0;
             for (int k = 0; k < q.K; k++) acc = fma(q.A[(int64_t)i * q.lda + k], q.B[(int64_t)k * q.ldb + j], acc);
-            q.C[(int64_t)i * q.ldc + j] = acc;
+            oz_store(q, i, j, acc);
         }
     }
 }
@@ -1437,9 +1483,15 @@ int gemm_f64_ozaki_grouped_setup(const std::vector<OzGroupItem> &items, int nter
     w->nc = cc.nc;
     w->gamma = (cc.log2p - 1.0) / 2.0 - 0.01;
     std::vector<OzGProb> hp;
-    int64_t rows = 0, cols = 0, tr = 0, tc = 0, items_total = 0, crt = 0;
+    int64_t rows = 0, cols = 0, tr = 0, tc = 0, items_total = 0, crt = 0, units = 0;
     size_t ra_bytes = 0, rb_bytes = 0, r_bytes = 0;
+    // image output: every item has one (then no item may be skipped: its image must be written)
+    const bool img = !items.empty() && items[0].cimg;
     for (const OzGroupItem &it : items) {
+        if ((it.cimg != nullptr) != img) return -1;
+        if (img && (it.M <= 0 || it.N <= 0 || it.K <= 0 || it.gc.shape[0] != it.M || it.gc.shape[1] != it.N ||
+                    it.gc.itemsize != 8 || (it.gc.block[1] & 3) || (it.gc.chunk[1] & 3)))
+            return -1;
         if (it.M <= 0 || it.N <= 0 || it.K <= 0) continue;
         if (it.K > 65536 || it.M > (1 << 30) || it.N > (1 << 30)) return -1;
         OzGProb q;
@@ -1449,6 +1501,12 @@ int gemm_f64_ozaki_grouped_setup(const std::vector<OzGroupItem> &items, int nter
         q.row0 = rows; q.col0 = cols; q.task_r0 = tr; q.tile_c0 = tc; q.item0 = items_total; q.crt0 = crt;
         q.A = it.A; q.B = it.B; q.C = it.C; q.lda = it.lda; q.ldb = it.ldb; q.ldc = it.ldc;
         q.ldr = round_up(it.N, 16);
+        if (img) {
+            q.gc = it.gc;
+            q.cimg = it.cimg;
+            q.unit0 = units;
+            units += it.gc.nchunks * it.gc.nblocks * ceil_div(it.gc.block[0], (int64_t)CRT_SLICE);
+        }
         rows += it.M; cols += it.N;
         tr += it.M * (q.Kp / 8);
         tc += ceil_div(it.N, 64) * ceil_div(q.Kp, 64);
@@ -1461,6 +1519,8 @@ int gemm_f64_ozaki_grouped_setup(const std::vector<OzGroupItem> &items, int nter
     }
     w->np = (int)hp.size();
     w->rows = rows; w->cols = cols; w->tasks_r = tr; w->tiles_c = tc; w->items = items_total; w->crt = crt;
+    w->img = img;
+    w->units = units;
     if (hp.empty()) return 0;
     if (!w->ra.allocate(ra_bytes, dev) || !w->rb.allocate(rb_bytes, dev) || !w->rr.allocate(r_bytes, dev) ||
         !w->sa.allocate((size_t)rows * 4, dev) || !w->sb.allocate((size_t)cols * 4, dev) ||
@@ -1526,11 +1586,21 @@ int gemm_f64_ozaki_grouped_launch(OzGroupWork *w, cudaStream_t st)
     IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<false, true><<<(unsigned)std::min<int64_t>(w->items, nsm), oz::threads_of<true>(),
                                                                oz::SMEM, st>>>(unused, unused, prm));
     const unsigned cg = (unsigned)std::min<int64_t>((w->crt + 255) / 256, (int64_t)nsm * 8);
-    switch (w->nc) {
-    case 1: IAB_TIMED("k_crt", st, k_crt_g<1><<<cg, 256, 0, st>>>(pr, w->np, w->crt, w->sa.as<int>(), w->sb.as<int>())); break;
-    case 2: IAB_TIMED("k_crt", st, k_crt_g<2><<<cg, 256, 0, st>>>(pr, w->np, w->crt, w->sa.as<int>(), w->sb.as<int>())); break;
-    case 3: IAB_TIMED("k_crt", st, k_crt_g<3><<<cg, 256, 0, st>>>(pr, w->np, w->crt, w->sa.as<int>(), w->sb.as<int>())); break;
-    default: IAB_TIMED("k_crt", st, k_crt_g<4><<<cg, 256, 0, st>>>(pr, w->np, w->crt, w->sa.as<int>(), w->sb.as<int>())); break;
+    if (w->img) {
+        const unsigned ig = (unsigned)std::max<int64_t>(1, std::min<int64_t>(w->units, (int64_t)nsm * 8));
+        switch (w->nc) {
+        case 1: IAB_TIMED("k_crt_img", st, k_crt_img_g<1><<<ig, 256, 0, st>>>(pr, w->np, w->units, w->sa.as<int>(), w->sb.as<int>())); break;
+        case 2: IAB_TIMED("k_crt_img", st, k_crt_img_g<2><<<ig, 256, 0, st>>>(pr, w->np, w->units, w->sa.as<int>(), w->sb.as<int>())); break;
+        case 3: IAB_TIMED("k_crt_img", st, k_crt_img_g<3><<<ig, 256, 0, st>>>(pr, w->np, w->units, w->sa.as<int>(), w->sb.as<int>())); break;
+        default: IAB_TIMED("k_crt_img", st, k_crt_img_g<4><<<ig, 256, 0, st>>>(pr, w->np, w->units, w->sa.as<int>(), w->sb.as<int>())); break;
+        }
+    } else {
+        switch (w->nc) {
+        case 1: IAB_TIMED("k_crt", st, k_crt_g<1><<<cg, 256, 0, st>>>(pr, w->np, w->crt, w->sa.as<int>(), w->sb.as<int>())); break;
+        case 2: IAB_TIMED("k_crt", st, k_crt_g<2><<<cg, 256, 0, st>>>(pr, w->np, w->crt, w->sa.as<int>(), w->sb.as<int>())); break;
+        case 3: IAB_TIMED("k_crt", st, k_crt_g<3><<<cg, 256, 0, st>>>(pr, w->np, w->crt, w->sa.as<int>(), w->sb.as<int>())); break;
+        default: IAB_TIMED("k_crt", st, k_crt_g<4><<<cg, 256, 0, st>>>(pr, w->np, w->crt, w->sa.as<int>(), w->sb.as<int>())); break;
+        }
     }
     IAB_TIMED("k_nonfinite_fix", st, k_nonfinite_fix_g<<<(unsigned)(((w->rows + w->cols) * 32 + 255) / 256), 256, 0, st>>>(
         pr, w->np, w->rows, w->cols, w->sa.as<int>(), w->sb.as<int>()));
