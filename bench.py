@@ -199,6 +199,7 @@ def roofline(kprof, steps, pk, dgemm_tflops, c_cbytes, a_cb, b_cb):
             "k_lz4_encode_par": img + (c_cbytes or img),
             "k_lz4_decode_cta": a_cb + b_cb + 2 * img,          # upper bound: all streams LZ4
             "k_crt": L_MODULI * M * N + img,                    # residue planes in, float64 out
+            "k_crt_img": L_MODULI * M * N + img,                # the same, out as C's encoder image
             "k_residues_rows": img + L_MODULI * M * K,
             "k_residues_cols": img + L_MODULI * K * N,
             "k_scatter_fast": 4 * img, "k_scatter": 4 * img,   # both operands, read + write
