@@ -1804,8 +1804,20 @@ INA_API(ina_rc_t) iarray_b200_opt_gemm_cframes(iarray_context_t *ctx, const uint
         if (split && k > 0) cudaStreamWaitEvent(st, evK.ev[(size_t)k - 1], 0);
         const int64_t r0 = k * gc.chunk[0], mk = row_geom(fa.g, k).shape[0];
         uint8_t *a_k = dA.as<uint8_t>() + r0 * lda * isz, *c_k = dC.as<uint8_t>() + r0 * ldc * isz;
+        const Geom gk = row_geom(gc, k);
+        iab::EncodeWork &w = enc[(size_t)k];
+        // split float64: the band's reconstruction goes straight into its encoder image
+        iab::CImage cimg;
+        if (split && dtype == IARRAY_DATA_TYPE_DOUBLE && iab::encode_image_ok(gk, cc->shuffle, cc->clevel == 0)) {
+            err = iab::encode_image_prepare(gk, &w);
+            if (err) break;
+            cimg.g = gk;
+            cimg.img = w.img.as<uint8_t>();
+            oz[(size_t)k].cimg = &cimg;
+        }
         if (split) {
             err = iab::gemm_f64_ozaki_rows(mk, (const double *)a_k, lda, ob, (double *)c_k, ldc, &oz[(size_t)k], st);
+            oz[(size_t)k].cimg = nullptr;                 // read at launch only
         } else if (dtype == IARRAY_DATA_TYPE_DOUBLE) {
             iab::gemm_f64_native(mk, N, K, (const double *)a_k, lda, dB.as<double>(), ldb, (double *)c_k, ldc, st);
         } else {
@@ -1814,8 +1826,6 @@ INA_API(ina_rc_t) iarray_b200_opt_gemm_cframes(iarray_context_t *ctx, const uint
         if (err) break;
         cudaEventRecord(evP.ev[(size_t)k], st);
         cudaStreamWaitEvent(se, evP.ev[(size_t)k], 0);
-        const Geom gk = row_geom(gc, k);
-        iab::EncodeWork &w = enc[(size_t)k];
         w.exact_lz4 = ctx->encoder == IARRAY_B200_ENCODER_LIBLZ4;
         w.memcpy_only = cc->clevel == 0;
         err = iab::encode_launch(gk, c_k, ldc, cc->shuffle, cc->splitmode, &cbuf[(size_t)k], &w, se);
