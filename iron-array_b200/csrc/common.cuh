@@ -399,6 +399,7 @@ struct OzGroupWork {
     int64_t rows = 0, cols = 0, tasks_r = 0, tiles_c = 0, items = 0, crt = 0;
     bool img = false;                // the reconstruction writes the items' encoder images
     int64_t units = 0;               // its work units (block slices of every image)
+    int slice = 0;                   // rows per work unit
 };
 int gemm_f64_ozaki_grouped_setup(const std::vector<OzGroupItem> &items, int nterms, OzGroupWork *w, cudaStream_t st);
 int gemm_f64_ozaki_grouped_launch(OzGroupWork *w, cudaStream_t st);

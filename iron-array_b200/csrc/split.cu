@@ -910,27 +910,33 @@ __device__ __forceinline__ void crt_quad(int N, const uint8_t *__restrict__ R, i
     }
 }
 
-// Rows of a block per work unit of the image reconstruction.
-constexpr int CRT_SLICE = 128;
+// Rows of a block per work unit of the image reconstruction: up to 128, fewer when the images
+// hold fewer than 128 x 8 x SMs block rows, so that small products still spread over the SMs.
+constexpr int CRT_SLICE_MAX = 128;
+static int crt_slice_rows(int64_t block_rows_total, int nsm)
+{
+    const int64_t s = block_rows_total / ((int64_t)nsm * 8);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(CRT_SLICE_MAX, s));
+}
 
 // The reconstruction written into the output container's shuffled block image (CImage): work
-// units are slices of CRT_SLICE rows of one block; each thread takes 4 consecutive items of a
+// units are slices of `slice` rows of one block; each thread takes 4 consecutive items of a
 // block row (one 4-byte word per byte plane), the logical ones reconstructed, chunk and array
 // padding zero, exactly the image the encoder's gather would write from the dense product.
 // Needs block[1] % 4 == 0 and chunk[1] % 4 == 0 (every quad starts at a column j0 % 4 == 0).
 //
-// One work unit of it: rows [CRT_SLICE sl, CRT_SLICE (sl + 1)) of block t of the output's image
+// One work unit of it: rows [slice sl, slice (sl + 1)) of block t of the output's image
 // (unit un = t x slices-per-block + sl); sA / sB are the product's row and column shifts.
 template <int NC>
 __device__ __forceinline__ void crt_img_unit(const Geom &g, const uint8_t *__restrict__ R, int64_t ldr,
                                              const int *__restrict__ sA, const int *__restrict__ sB,
-                                             uint8_t *__restrict__ img, int64_t un)
+                                             uint8_t *__restrict__ img, int64_t un, int slice)
 {
     const int M = (int)g.shape[0], N = (int)g.shape[1];
     const int64_t plane = (int64_t)M * ldr;
     const int qpr = (int)(g.block[1] / 4);
     const int step_r = (int)blockDim.x / qpr, step_q = (int)blockDim.x - step_r * qpr;
-    const int spb = (int)((g.block[0] + CRT_SLICE - 1) / CRT_SLICE);
+    const int spb = (int)((g.block[0] + slice - 1) / slice);
     const int64_t units = g.nchunks * g.nblocks * spb;
     const bool small = units < (int64_t(1) << 31) && g.cgrid[1] < (int64_t(1) << 31);
     int64_t t, c, b, ci0, ci1, bi0, bi1;
@@ -953,7 +959,7 @@ __device__ __forceinline__ void crt_img_unit(const Geom &g, const uint8_t *__res
     const int nr = (int)max((int64_t)0, min(min(g.block[0], g.chunk[0] - bi0 * g.block[0]), g.shape[0] - row0));
     const int nc = (int)max((int64_t)0, min(min(g.block[1], g.chunk[1] - bi1 * g.block[1]), g.shape[1] - col0));
     uint8_t *blk = img + t * g.blocksize;
-    const int r_lo = sl * CRT_SLICE, r_hi = (int)min((int64_t)r_lo + CRT_SLICE, g.block[0]);
+    const int r_lo = sl * slice, r_hi = (int)min((int64_t)r_lo + slice, g.block[0]);
     const int nq = (r_hi - r_lo) * qpr;
     // (row, quad column) of each thread's quad, advanced by a fixed step per iteration
     int r = r_lo + (int)threadIdx.x / qpr, q = (int)threadIdx.x % qpr;
@@ -981,15 +987,15 @@ __device__ __forceinline__ void crt_img_unit(const Geom &g, const uint8_t *__res
     }
 }
 
-// Work units: slices of CRT_SLICE rows of one block of the image.  Held to 80 registers (three
+// Work units: slices of `slice` rows of one block of the image.  Held to 80 registers (three
 // CTAs per SM): 0.70 ms instead of 0.79 ms at 8192^2 with 102.
 template <int NC>
 __global__ void __launch_bounds__(256, 3) k_crt_img(Geom g, const uint8_t *__restrict__ R, int64_t ldr,
                                                     const int *__restrict__ sA, const int *__restrict__ sB,
-                                                    uint8_t *__restrict__ img)
+                                                    uint8_t *__restrict__ img, int slice)
 {
-    const int64_t units = g.nchunks * g.nblocks * ((g.block[0] + CRT_SLICE - 1) / CRT_SLICE);
-    for (int64_t un = blockIdx.x; un < units; un += gridDim.x) crt_img_unit<NC>(g, R, ldr, sA, sB, img, un);
+    const int64_t units = g.nchunks * g.nblocks * ((g.block[0] + slice - 1) / slice);
+    for (int64_t un = blockIdx.x; un < units; un += gridDim.x) crt_img_unit<NC>(g, R, ldr, sA, sB, img, un, slice);
 }
 
 template <int NC>
@@ -1017,14 +1023,17 @@ static void launch_crt(int nc, unsigned grid, int M, int N, const uint8_t *R, in
     }
 }
 
-static void launch_crt_img(int nc, unsigned grid, const Geom &g, const uint8_t *R, int64_t ldr, const int *sA,
+static void launch_crt_img(int nc, int nsm, const Geom &g, const uint8_t *R, int64_t ldr, const int *sA,
                            const int *sB, uint8_t *img, cudaStream_t st)
 {
+    const int slice = crt_slice_rows(g.nchunks * g.nblocks * g.block[0], nsm);
+    const int64_t units = g.nchunks * g.nblocks * ceil_div(g.block[0], (int64_t)slice);
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(units, (int64_t)nsm * 8));
     switch (nc) {
-    case 1: IAB_TIMED("k_crt_img", st, k_crt_img<1><<<grid, 256, 0, st>>>(g, R, ldr, sA, sB, img)); break;
-    case 2: IAB_TIMED("k_crt_img", st, k_crt_img<2><<<grid, 256, 0, st>>>(g, R, ldr, sA, sB, img)); break;
-    case 3: IAB_TIMED("k_crt_img", st, k_crt_img<3><<<grid, 256, 0, st>>>(g, R, ldr, sA, sB, img)); break;
-    default: IAB_TIMED("k_crt_img", st, k_crt_img<4><<<grid, 256, 0, st>>>(g, R, ldr, sA, sB, img)); break;
+    case 1: IAB_TIMED("k_crt_img", st, k_crt_img<1><<<grid, 256, 0, st>>>(g, R, ldr, sA, sB, img, slice)); break;
+    case 2: IAB_TIMED("k_crt_img", st, k_crt_img<2><<<grid, 256, 0, st>>>(g, R, ldr, sA, sB, img, slice)); break;
+    case 3: IAB_TIMED("k_crt_img", st, k_crt_img<3><<<grid, 256, 0, st>>>(g, R, ldr, sA, sB, img, slice)); break;
+    default: IAB_TIMED("k_crt_img", st, k_crt_img<4><<<grid, 256, 0, st>>>(g, R, ldr, sA, sB, img, slice)); break;
     }
 }
 
@@ -1189,8 +1198,8 @@ int gemm_f64_ozaki_rows_product(int64_t M, const double *A, int64_t lda, const O
     else
         IAB_TIMED("k_i8gemm_mod", st, k_i8gemm_mod<false, false><<<(unsigned)std::min(tiles, nsm), oz::THREADS, oz::SMEM, st>>>(tmA, tmB, prm));
     if (w->cimg) {
-        launch_crt_img(ob.nc, (unsigned)(nsm * 8), w->cimg->g, w->rr.as<uint8_t>(), ldr, w->sa.as<int>(), ob.sb.as<int>(),
-                       w->cimg->img, st);
+        launch_crt_img(ob.nc, nsm, w->cimg->g, w->rr.as<uint8_t>(), ldr, w->sa.as<int>(), ob.sb.as<int>(), w->cimg->img,
+                       st);
     } else {
         launch_crt(ob.nc, (unsigned)(nsm * 8), (int)M, (int)N, w->rr.as<uint8_t>(), ldr, w->sa.as<int>(), ob.sb.as<int>(), C,
                    ldc, st);
@@ -1413,7 +1422,7 @@ __global__ void __launch_bounds__(256) k_crt_g(const OzGProb *__restrict__ pr, i
 // numbered consecutively (unit0), each unit as in k_crt_img.
 template <int NC>
 __global__ void __launch_bounds__(256, 3) k_crt_img_g(const OzGProb *__restrict__ pr, int np, int64_t units,
-                                                      const int *__restrict__ sA, const int *__restrict__ sB)
+                                                      const int *__restrict__ sA, const int *__restrict__ sB, int slice)
 {
     int qh = -1;
     for (int64_t un = blockIdx.x; un < units; un += gridDim.x) {
@@ -1424,7 +1433,7 @@ __global__ void __launch_bounds__(256, 3) k_crt_img_g(const OzGProb *__restrict_
         const uint8_t *R = q.R;
         uint8_t *img = q.cimg;
         const int64_t ldr = q.ldr, row0 = q.row0, col0 = q.col0, unit0 = q.unit0;
-        crt_img_unit<NC>(g, R, ldr, sA + row0, sB + col0, img, un - unit0);
+        crt_img_unit<NC>(g, R, ldr, sA + row0, sB + col0, img, un - unit0, slice);
     }
 }
 
@@ -1487,6 +1496,12 @@ int gemm_f64_ozaki_grouped_setup(const std::vector<OzGroupItem> &items, int nter
     size_t ra_bytes = 0, rb_bytes = 0, r_bytes = 0;
     // image output: every item has one (then no item may be skipped: its image must be written)
     const bool img = !items.empty() && items[0].cimg;
+    int slice = CRT_SLICE_MAX;
+    if (img) {
+        int64_t brows = 0;
+        for (const OzGroupItem &it : items) brows += it.gc.nchunks * it.gc.nblocks * it.gc.block[0];
+        slice = crt_slice_rows(brows, sms());
+    }
     for (const OzGroupItem &it : items) {
         if ((it.cimg != nullptr) != img) return -1;
         if (img && (it.M <= 0 || it.N <= 0 || it.K <= 0 || it.gc.shape[0] != it.M || it.gc.shape[1] != it.N ||
@@ -1505,7 +1520,7 @@ int gemm_f64_ozaki_grouped_setup(const std::vector<OzGroupItem> &items, int nter
             q.gc = it.gc;
             q.cimg = it.cimg;
             q.unit0 = units;
-            units += it.gc.nchunks * it.gc.nblocks * ceil_div(it.gc.block[0], (int64_t)CRT_SLICE);
+            units += it.gc.nchunks * it.gc.nblocks * ceil_div(it.gc.block[0], (int64_t)slice);
         }
         rows += it.M; cols += it.N;
         tr += it.M * (q.Kp / 8);
@@ -1521,6 +1536,7 @@ int gemm_f64_ozaki_grouped_setup(const std::vector<OzGroupItem> &items, int nter
     w->rows = rows; w->cols = cols; w->tasks_r = tr; w->tiles_c = tc; w->items = items_total; w->crt = crt;
     w->img = img;
     w->units = units;
+    w->slice = slice;
     if (hp.empty()) return 0;
     if (!w->ra.allocate(ra_bytes, dev) || !w->rb.allocate(rb_bytes, dev) || !w->rr.allocate(r_bytes, dev) ||
         !w->sa.allocate((size_t)rows * 4, dev) || !w->sb.allocate((size_t)cols * 4, dev) ||
@@ -1589,10 +1605,10 @@ int gemm_f64_ozaki_grouped_launch(OzGroupWork *w, cudaStream_t st)
     if (w->img) {
         const unsigned ig = (unsigned)std::max<int64_t>(1, std::min<int64_t>(w->units, (int64_t)nsm * 8));
         switch (w->nc) {
-        case 1: IAB_TIMED("k_crt_img", st, k_crt_img_g<1><<<ig, 256, 0, st>>>(pr, w->np, w->units, w->sa.as<int>(), w->sb.as<int>())); break;
-        case 2: IAB_TIMED("k_crt_img", st, k_crt_img_g<2><<<ig, 256, 0, st>>>(pr, w->np, w->units, w->sa.as<int>(), w->sb.as<int>())); break;
-        case 3: IAB_TIMED("k_crt_img", st, k_crt_img_g<3><<<ig, 256, 0, st>>>(pr, w->np, w->units, w->sa.as<int>(), w->sb.as<int>())); break;
-        default: IAB_TIMED("k_crt_img", st, k_crt_img_g<4><<<ig, 256, 0, st>>>(pr, w->np, w->units, w->sa.as<int>(), w->sb.as<int>())); break;
+        case 1: IAB_TIMED("k_crt_img", st, k_crt_img_g<1><<<ig, 256, 0, st>>>(pr, w->np, w->units, w->sa.as<int>(), w->sb.as<int>(), w->slice)); break;
+        case 2: IAB_TIMED("k_crt_img", st, k_crt_img_g<2><<<ig, 256, 0, st>>>(pr, w->np, w->units, w->sa.as<int>(), w->sb.as<int>(), w->slice)); break;
+        case 3: IAB_TIMED("k_crt_img", st, k_crt_img_g<3><<<ig, 256, 0, st>>>(pr, w->np, w->units, w->sa.as<int>(), w->sb.as<int>(), w->slice)); break;
+        default: IAB_TIMED("k_crt_img", st, k_crt_img_g<4><<<ig, 256, 0, st>>>(pr, w->np, w->units, w->sa.as<int>(), w->sb.as<int>(), w->slice)); break;
         }
     } else {
         switch (w->nc) {
