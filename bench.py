@@ -737,8 +737,9 @@ def run_kernel_case(args):
     codec: an n x n float64 container (n = --case-n, default 4096) of the product's kind of
     values (gaussian) encoded with the parallel encoder, then an A-like one
     (uniform(-1,1) x 2^U{-8..8}) decoded; three rounds each.  split: the split-precision
-    float64 product n x n x n on device operands (iarray_b200_dense_gemm), two rounds.
-    f32split: the float32 split form (six BF16 products) n x n x n, two rounds.  gemv: the
+    float64 product n x n x n on device operands (iarray_b200_dense_gemm), two rounds.  splitc:
+    the split-precision iarray_opt_gemm on compressed n x n containers (chunk n/2, block 256^2;
+    the product reconstructed into C's encoder image), two rounds.  f32split: the float32 split form (six BF16 products) n x n x n, two rounds.  gemv: the
     plain GEMV workload's smooth float32 matrix at n x n (chunk 4000^2, block 500^2) decoded three
     times, then one iarray_opt_gemv.  f64native: the native FP64 product n x n x n on device
     operands, two rounds.  batch: the first n / 64 problems of the batching workload in the
@@ -805,6 +806,21 @@ def run_kernel_case(args):
         ref = (A[:64] @ B).cpu().numpy()
         err = np.linalg.norm(C[:64].cpu().numpy() - ref) / np.linalg.norm(ref)
         assert err < 1e-14, err
+    elif args.kernel_case == "splitc":
+        # the split-precision iarray_opt_gemm on compressed n x n containers (chunk n/2, block
+        # 256): decode, product reconstructed into C's encoder image, encode; two rounds
+        ctx = ia.Context(form=ia.FORM_SPLIT, encoder=ia.ENCODER_PARALLEL)
+        a = rng.uniform(-1, 1, (n, n)) * np.exp2(rng.integers(-8, 9, (n, n)))
+        b = rng.uniform(-1, 1, (n, n)) * np.exp2(rng.integers(-8, 9, (n, n)))
+        ch, bl = (n // 2, n // 2), (256, 256)
+        Ac, Bc = ia.Container.from_numpy(ctx, a, ch, bl), ia.Container.from_numpy(ctx, b, ch, bl)
+        for _ in range(2):
+            C = ia.opt_gemm(ctx, Ac, Bc, ch, bl)
+            got = C.to_numpy()[:64]
+            C.free()
+        ref = a[:64] @ b
+        err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+        assert err < 1e-14, err
     elif args.kernel_case == "f32split":
         ctx = ia.Context(form=ia.FORM_SPLIT)
         A = torch.from_numpy(rng.standard_normal((n, n)).astype(np.float32)).cuda()
@@ -846,7 +862,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-samples", type=int, default=3, help="whole-product samples of the CPU baseline")
     ap.add_argument("--no-secondary", action="store_true", help="skip the GEMV, float32 and batching workloads")
-    ap.add_argument("--kernel-case", choices=["codec", "split", "f32split", "gemv", "f64native", "batch"], default=None,
+    ap.add_argument("--kernel-case", choices=["codec", "split", "splitc", "f32split", "gemv", "f64native", "batch"], default=None,
                     help="run one small case of one kernel family instead of the benchmark")
     ap.add_argument("--case-n", type=int, default=4096, help="matrix size of --kernel-case")
     args = ap.parse_args()
