@@ -291,3 +291,40 @@ def test_split_f64_output_written_into_encoder_image(ia, M, K, N, ch, bl, encode
     ref = ia.Container.from_numpy(ctx, dense, ch, bl)
     assert C.chunks() == ref.chunks()
     ctx.close()
+
+
+@pytest.mark.parametrize("M,K,N,ch,bl", [
+    (512, 300, 768, (256, 256), (64, 128)),
+    (1024, 200, 512, (512, 512), (128, 256)),
+    (300, 200, 260, (100, 120), (40, 40)),     # chunk and array padding
+])
+def test_split_f32_output_chunks_equal_dense_encode(ia, M, K, N, ch, bl):
+    """float32 split form through iarray_linalg_matmul: C's values are bitwise those of the dense
+    split product on device operands and its chunks byte for byte those of that product encoded
+    from an array, NaN and infinity rows and columns included."""
+    import ctypes
+    import torch
+    rng = np.random.default_rng(M + N + K)
+    a = rng.standard_normal((M, K)).astype(np.float32)
+    b = rng.standard_normal((K, N)).astype(np.float32)
+    a[M // 2, 3] = np.nan
+    b[K - 1, N // 3] = np.inf
+    ctx = ia.Context(form=ia.FORM_SPLIT, encoder=ia.ENCODER_PARALLEL)
+    Ac = ia.Container.from_numpy(ctx, a, ch, bl)
+    Bc = ia.Container.from_numpy(ctx, b, (100, ch[1]), (50, bl[1]))
+    C = ia.matmul(ctx, Ac, Bc, ch, bl)
+    got = C.to_numpy()
+    A = torch.from_numpy(a).cuda()
+    B = torch.from_numpy(b).cuda()
+    D = torch.empty((M, N), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    ia.check(ia.lib().iarray_b200_dense_gemm(ctx.ptr, ia.DTYPE_FLOAT, M, N, K, ctypes.c_void_p(A.data_ptr()), K,
+                                              ctypes.c_void_p(B.data_ptr()), N, ctypes.c_void_p(D.data_ptr()), N),
+             "dense_gemm")
+    ctx.synchronize()
+    dense = D.cpu().numpy()
+    assert got.tobytes() == dense.tobytes()
+    assert np.isnan(got[M // 2]).all() and not np.isfinite(got[:, N // 3]).any()
+    ref = ia.Container.from_numpy(ctx, dense, ch, bl)
+    assert C.chunks() == ref.chunks()
+    ctx.close()
